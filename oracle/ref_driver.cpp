@@ -1,0 +1,285 @@
+/*
+ * C driver for the reference engine compiled in place (oracle tier A).
+ *
+ * TEST INFRASTRUCTURE ONLY: used by tests/ and by bench.py's CPU baseline
+ * leg to run the reference's own CPU code path; the product never loads it.
+ *
+ * Each entry point performs exactly what the reference's Python layer does
+ * for the same user call, but without the Python object model:
+ *   mxref_init            universe_init (src/MxSimulator.cpp:349-420)
+ *   mxref_add_type        particle type defaults (src/MxParticle.cpp:1395-1420,
+ *                         imass = 1/mass at :1266)
+ *   mxref_add_particles   particle_init_ex (src/MxParticle.cpp:2062-2119);
+ *                         positions pass through a float 3-vector first
+ *   mxref_potential_*     the Potential factories (src/mdcore/src/MxPotential.cpp
+ *                         :2459-2473 LJ, :2545-2559 harmonic, :2652-2667 Morse,
+ *                         :2738-2750 DPD)
+ *   mxref_bind            engine_addpot (src/mdcore/src/engine.cpp:960-981)
+ *   mxref_bind_force      MxConstantForce + engine_add_singlebody_force
+ *                         (src/mdcore/src/MxForce.cpp:508-519, engine.cpp:983-1003)
+ *   mxref_add_bonds       _bond_init (src/mdcore/src/bond.cpp:497-529)
+ *   mxref_step            engine_step (src/mdcore/src/engine.cpp:1198)
+ *   mxref_force           engine_force (src/mdcore/src/engine.cpp:1230)
+ * The engine is a process-wide singleton in the reference, so one process
+ * holds one reference engine; tests run each scenario in a fresh process.
+ */
+#include "mdcore_config.h"
+#include "engine.h"
+#include "MxParticle.h"
+#include "MxPotential.h"
+#include "DissapativeParticleDynamics.hpp"
+#include "potential_eval.hpp"
+#include "bond.h"
+#include "task.h"
+#include "MxForce.h"
+#include "../../rendering/NOMStyle.hpp"
+#include <vector>
+
+extern PyTypeObject MxConstantForce_Type;
+MxPotential *potential_create_morse(double d, double a, double r0, double min, double max, double tol);
+MxPotential *potential_create_power(double k, double r0, double alpha, double a, double b, double tol);
+
+static std::vector<NOMStyle *> g_styles;
+
+extern "C" {
+
+int mxref_init(const double *origin, const double *dim, const int *cells_in, double cutoff,
+               const char *bc_x, const char *bc_y, const char *bc_z, double dt,
+               double max_distance, int nr_types_max) {
+    if (engine::types == NULL) {
+        engine::types = (MxParticleType *)calloc(engine::max_type, sizeof(MxParticleType));
+        engine::nr_types = 0;
+    }
+    int cells[3] = {cells_in[0], cells_in[1], cells_in[2]};
+    PyObject *bc = PyDict_New();
+    PyObject *sx = PyUnicode_FromString(bc_x), *sy = PyUnicode_FromString(bc_y), *sz = PyUnicode_FromString(bc_z);
+    PyDict_SetItemString(bc, "x", sx);
+    PyDict_SetItemString(bc, "y", sy);
+    PyDict_SetItemString(bc, "z", sz);
+    Py_DECREF(sx); Py_DECREF(sy); Py_DECREF(sz);
+    int rc = engine_init(&_Engine, origin, dim, cells, cutoff, bc, nr_types_max, engine_flag_none);
+    if (rc != 0) return rc;
+    _Engine.dt = dt;
+    _Engine.temperature = 1;
+    _Engine.integrator = EngineIntegrator::FORWARD_EULER;
+    if (max_distance >= 0) _Engine.particle_max_dist_fraction = max_distance / _Engine.s.h[0];
+    return 0;
+}
+
+int mxref_add_type(double mass, double radius, int dynamics) {
+    int id = engine::nr_types;
+    if (id >= engine::max_type) return -1;
+    MxParticleType *t = &engine::types[id];
+    bzero(t, sizeof(MxParticleType));
+    t->id = id;
+    t->mass = mass;
+    t->imass = 1.0 / mass;
+    t->radius = radius;
+    t->minimum_radius = 0.0;
+    t->dynamics = (unsigned char)dynamics;
+    NOMStyle *st = (NOMStyle *)calloc(1, sizeof(NOMStyle));
+    st->flags = STYLE_VISIBLE;
+    g_styles.push_back(st);
+    t->style = st;
+    engine::nr_types = id + 1;
+    return id;
+}
+
+/* Adds n particles; x and v are n*3 arrays; returns the id of the first. */
+int mxref_add_particles(int n, const double *x, const double *v, const int *type) {
+    int first = -1;
+    for (int k = 0; k < n; ++k) {
+        MxParticleType *t = &engine::types[type[k]];
+        MxParticle part;
+        bzero(&part, sizeof(MxParticle));
+        part.radius = t->radius;
+        part.mass = t->mass;
+        part.imass = t->imass;
+        part.id = engine_next_partid(&_Engine);
+        part.typeId = t->id;
+        part.flags = t->particle_flags;
+        part.creation_time = _Engine.time;
+        part.clusterId = -1;
+        part.position = Magnum::Vector3((float)x[3 * k], (float)x[3 * k + 1], (float)x[3 * k + 2]);
+        part.velocity = Magnum::Vector3((float)v[3 * k], (float)v[3 * k + 1], (float)v[3 * k + 2]);
+        if (part.radius > _Engine.s.cutoff) part.flags |= PARTICLE_LARGE;
+        MxParticle *p = NULL;
+        double pos[] = {part.position[0], part.position[1], part.position[2]};
+        int rc = engine_addpart(&_Engine, &part, pos, &p);
+        if (rc < 0) return rc;
+        if (first < 0) first = p->id;
+        p->clusterId = -1;
+    }
+    return first;
+}
+
+void *mxref_potential_lj126(double a, double b, double A, double B, double tol) {
+    return potential_create_LJ126(a, b, A, B, tol);
+}
+void *mxref_potential_morse(double d, double a, double r0, double min, double max, double tol) {
+    return potential_create_morse(d, a, r0, min, max, tol);
+}
+void *mxref_potential_harmonic(double k, double r0, double min, double max, double tol) {
+    return potential_create_harmonic(min, max, k, r0, tol);
+}
+void *mxref_potential_power(double k, double r0, double alpha, double min, double max, double tol) {
+    return potential_create_power(k, r0, alpha, min, max, tol);
+}
+void *mxref_potential_dpd(double alpha, double gamma, double sigma, double cutoff, int shifted) {
+    return DPDPotential_New((float)alpha, (float)gamma, (float)sigma, (float)cutoff, shifted != 0);
+}
+
+int mxref_potential_info(void *vp, int *n, float *alpha4, float *a, float *b, unsigned *flags,
+                         float *r0_plusone, int *kind) {
+    MxPotential *p = (MxPotential *)vp;
+    if (!p) return -1;
+    *n = p->n;
+    for (int k = 0; k < 4; ++k) alpha4[k] = p->alpha[k];
+    *a = p->a;
+    *b = p->b;
+    *flags = p->flags;
+    *r0_plusone = p->r0_plusone;
+    *kind = (int)p->kind;
+    return 0;
+}
+
+int mxref_potential_coeffs(void *vp, float *out, int cap) {
+    MxPotential *p = (MxPotential *)vp;
+    int len = (p->n + 1) * potential_chunk;
+    if (!p->c) return 0;
+    if (cap < len) return -len;
+    memcpy(out, p->c, sizeof(float) * len);
+    return len;
+}
+
+int mxref_dpd_params(void *vp, float *alpha, float *gamma, float *sigma) {
+    DPDPotential *p = (DPDPotential *)vp;
+    *alpha = p->alpha;
+    *gamma = p->gamma;
+    *sigma = p->sigma;
+    return 0;
+}
+
+/* The reference's inline table evaluators, called on scalars. */
+int mxref_potential_eval_ex(void *vp, float ri, float rj, float r2, float *e, float *f) {
+    return potential_eval_ex((MxPotential *)vp, ri, rj, r2, e, f) ? 1 : 0;
+}
+void mxref_potential_eval(void *vp, float r2, float *e, float *f) {
+    potential_eval((MxPotential *)vp, r2, e, f);
+}
+
+int mxref_bind(void *pot, int ti, int tj) { return engine_addpot(&_Engine, (MxPotential *)pot, ti, tj); }
+
+int mxref_bind_force(int type, float fx, float fy, float fz) {
+    if (PyType_Ready(&MxForce_Type) < 0 || PyType_Ready(&MxConstantForce_Type) < 0) return -1;
+    PyObject *obj = PyType_GenericAlloc(&MxConstantForce_Type, 0);
+    if (!obj) return -1;
+    PyObject *val = Py_BuildValue("[fff]", fx, fy, fz);
+    PyObject *args = PyTuple_Pack(1, val);
+    int rc = MxConstantForce_Type.tp_init(obj, args, NULL);
+    Py_DECREF(args);
+    Py_DECREF(val);
+    if (rc != 0) return -1;
+    return engine_add_singlebody_force(&_Engine, (MxForce *)obj, type, -1);
+}
+
+int mxref_add_bonds(int n, const int *pi, const int *pj, void *pot, double dissociation) {
+    for (int k = 0; k < n; ++k) {
+        MxBond *bond = NULL;
+        int id = engine_bond_alloc(&_Engine, &bond);
+        if (id < 0) return id;
+        bond->flags = 0;
+        bond->i = pi[k];
+        bond->j = pj[k];
+        bond->half_life = 0;
+        bond->dissociation_energy = dissociation;
+        bond->style = NULL;
+        if (bond->i >= 0 && bond->j >= 0) {
+            bond->flags |= BOND_ACTIVE;
+            _Engine.nr_active_bonds++;
+        }
+        bond->potential = (MxPotential *)pot;
+    }
+    return 0;
+}
+
+int mxref_start(int nr_runners) { return engine_start(&_Engine, nr_runners, nr_runners); }
+
+int mxref_step(int nsteps) {
+    for (int k = 0; k < nsteps; ++k) {
+        int rc = engine_step(&_Engine);
+        if (rc != 0) return rc;
+    }
+    return 0;
+}
+
+int mxref_force(void) { return engine_force(&_Engine); }
+
+int mxref_nr_parts(void) { return _Engine.s.nr_parts; }
+
+/* Per-id state: cell-relative position, absolute position (double), velocity,
+ * force, cell index and type. Missing ids get cell = -1. */
+int mxref_get_state(int n, float *xrel, double *xabs, float *v, float *f, int *cell, int *type) {
+    space *s = &_Engine.s;
+    for (int id = 0; id < n; ++id) {
+        MxParticle *p = id < s->nr_parts ? s->partlist[id] : NULL;
+        if (!p) { cell[id] = -1; continue; }
+        space_cell *c = s->celllist[id];
+        cell[id] = (int)(c - s->cells);
+        type[id] = p->typeId;
+        for (int k = 0; k < 3; ++k) {
+            xrel[3 * id + k] = p->x[k];
+            xabs[3 * id + k] = c->origin[k] + p->x[k];
+            v[3 * id + k] = p->v[k];
+            f[3 * id + k] = p->f[k];
+        }
+    }
+    return 0;
+}
+
+int mxref_space_info(int *cdim, double *h, int *nr_cells, int *nr_tasks, unsigned *period) {
+    space *s = &_Engine.s;
+    for (int k = 0; k < 3; ++k) { cdim[k] = s->cdim[k]; h[k] = s->h[k]; }
+    *nr_cells = s->nr_cells;
+    *nr_tasks = s->nr_tasks;
+    *period = s->period;
+    return 0;
+}
+
+/* Task list as rows of (type, flags, i, j). */
+int mxref_get_tasks(int *out, int cap) {
+    space *s = &_Engine.s;
+    if (cap < 4 * s->nr_tasks) return -s->nr_tasks;
+    for (int k = 0; k < s->nr_tasks; ++k) {
+        out[4 * k] = s->tasks[k].type;
+        out[4 * k + 1] = s->tasks[k].flags;
+        out[4 * k + 2] = s->tasks[k].i;
+        out[4 * k + 3] = s->tasks[k].j;
+    }
+    return s->nr_tasks;
+}
+
+int mxref_cell_flags(unsigned *out, double *origin) {
+    space *s = &_Engine.s;
+    for (int c = 0; c < s->nr_cells; ++c) {
+        out[c] = s->cells[c].flags;
+        for (int k = 0; k < 3; ++k) origin[3 * c + k] = s->cells[c].origin[k];
+    }
+    return s->nr_cells;
+}
+
+int mxref_bond_flags(unsigned *out, int n) {
+    for (int k = 0; k < n && k < _Engine.nr_bonds; ++k) out[k] = _Engine.bonds[k].flags;
+    return _Engine.nr_bonds;
+}
+
+void mxref_energies(double *epot, double *epot_nonbond, double *epot_bond, double *ekin) {
+    *epot = _Engine.s.epot;
+    *epot_nonbond = _Engine.s.epot_nonbond;
+    *epot_bond = _Engine.s.epot_bond;
+    *ekin = engine_kinetic_energy(&_Engine);
+}
+
+double mxref_max_dist_fraction(void) { return _Engine.particle_max_dist_fraction; }
+
+}
