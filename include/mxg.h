@@ -1,0 +1,191 @@
+/*
+ * mxg.h -- C ABI of the B200 force-and-step engine.
+ *
+ * The entry points replace, one for one, the mdcore engine calls that the
+ * reference's Python layer and C drivers make for the force-and-step path
+ * (paths relative to the reference project root):
+ *
+ *   mxg_potential_create_lj126     potential_create_LJ126   src/mdcore/src/MxPotential.cpp:960
+ *   mxg_potential_create_morse     potential_create_morse   src/mdcore/src/MxPotential.cpp:3389
+ *   mxg_potential_create_harmonic  potential_create_harmonic src/mdcore/src/MxPotential.cpp:335
+ *   mxg_potential_create_power     potential_create_power   src/mdcore/src/MxPotential.cpp:1614
+ *   mxg_potential_create_dpd       DPDPotential_New         src/mdcore/src/DissapativeParticleDynamics.cpp:134
+ *   mxg_potential_eval             potential_eval_ex        src/mdcore/src/potential_eval.hpp:106
+ *   mxg_engine_init                engine_init              src/mdcore/include/engine.h:600
+ *   mxg_engine_addtype             engine_addtype           src/mdcore/include/engine.h:575
+ *   mxg_engine_addpot              engine_addpot            src/mdcore/src/engine.cpp:960
+ *   mxg_engine_add_singlebody_force engine_add_singlebody_force src/mdcore/src/engine.cpp:983
+ *   mxg_engine_addparts            engine_addpart           src/mdcore/src/engine.cpp:1726
+ *   mxg_engine_addbonds            engine_bond_alloc + _bond_init src/mdcore/src/bond.cpp:497
+ *   mxg_engine_start               engine_start             src/mdcore/include/engine.h:640
+ *   mxg_engine_step                engine_step              src/mdcore/src/engine.cpp:1198
+ *   mxg_engine_force               engine_force             src/mdcore/src/engine.cpp:1230
+ *   mxg_engine_load                engine_load              src/mdcore/include/engine.h:612
+ *   mxg_engine_unload              engine_unload            src/mdcore/include/engine.h:646
+ *   mxg_engine_kinetic_energy      engine_kinetic_energy    src/mdcore/src/engine.cpp:1698
+ *   mxg_engine_finalize            engine_finalize          src/mdcore/src/engine.cpp:1418
+ *
+ * Conventions (as engine.h:33-63): every call returns int, 0 on success and a
+ * negative engine_err_* value on failure. GPU-specific failures use the codes
+ * below -100. Only plain pointers and sizes cross the boundary; device state
+ * stays resident between calls. A CUDA stream may be supplied; all device
+ * work of an engine is ordered on that stream.
+ */
+#ifndef MXG_H_
+#define MXG_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes (values of the reference's engine_err_*) */
+#define MXG_OK 0
+#define MXG_ERR_NULL -1
+#define MXG_ERR_MALLOC -2
+#define MXG_ERR_SPACE -3
+#define MXG_ERR_RANGE -6
+#define MXG_ERR_CELL -7
+#define MXG_ERR_BOND -11
+#define MXG_ERR_POTENTIAL -17
+#define MXG_ERR_CUDA -21
+#define MXG_ERR_NOCUDA -22
+#define MXG_ERR_TOOFAST -29
+/* GPU-specific status codes */
+#define MXG_ERR_CELL_OVERFLOW -101 /* more particles entered a cell in one step than its bucket holds */
+#define MXG_ERR_NONFINITE -102     /* a position or velocity became NaN/Inf */
+#define MXG_ERR_STATE -103         /* call made in the wrong engine state */
+#define MXG_ERR_ARG -104           /* invalid argument */
+
+/* potential kinds */
+#define MXG_POTENTIAL_TABLE 0
+#define MXG_POTENTIAL_DPD 1
+
+/* potential flags (src/mdcore/include/MxPotential.h:52-96) */
+#define MXG_POTENTIAL_LJ126 (1u << 0)
+#define MXG_POTENTIAL_R2 (1u << 4)
+#define MXG_POTENTIAL_R (1u << 5)
+#define MXG_POTENTIAL_HARMONIC (1u << 7)
+#define MXG_POTENTIAL_SCALED (1u << 11)
+#define MXG_POTENTIAL_SHIFTED (1u << 12)
+
+/* boundary kinds per face (src/mdcore/src/MxBoundaryConditions.hpp:15-23) */
+#define MXG_BOUNDARY_VELOCITY (1 << 0)
+#define MXG_BOUNDARY_PERIODIC (1 << 1)
+#define MXG_BOUNDARY_FREESLIP (1 << 2)
+#define MXG_BOUNDARY_NO_SLIP (1 << 4)
+
+/* faces, in the order the bc arrays use */
+#define MXG_FACE_LEFT 0   /* -x */
+#define MXG_FACE_RIGHT 1  /* +x */
+#define MXG_FACE_FRONT 2  /* -y */
+#define MXG_FACE_BACK 3   /* +y */
+#define MXG_FACE_BOTTOM 4 /* -z */
+#define MXG_FACE_TOP 5    /* +z */
+
+/* particle dynamics (src/mdcore/include/MxParticle.h:48-49) */
+#define MXG_NEWTONIAN 0
+#define MXG_OVERDAMPED 1
+
+/* particle flags (src/mdcore/include/MxParticle.h:54-70) */
+#define MXG_PARTICLE_FROZEN_X (1u << 2)
+#define MXG_PARTICLE_FROZEN_Y (1u << 3)
+#define MXG_PARTICLE_FROZEN_Z (1u << 4)
+
+typedef struct mxg_potential mxg_potential;
+typedef struct mxg_engine mxg_engine;
+
+/* ---- potentials: host-side table fit (FP64 fit, FP32 coefficients) ---- */
+int mxg_potential_create_lj126(double a, double b, double A, double B, double tol, mxg_potential **out);
+int mxg_potential_create_morse(double d, double alpha, double r0, double min, double max, double tol,
+                               mxg_potential **out);
+int mxg_potential_create_harmonic(double k, double r0, double min, double max, double tol, mxg_potential **out);
+int mxg_potential_create_power(double k, double r0, double alpha, double min, double max, double tol,
+                               mxg_potential **out);
+int mxg_potential_create_dpd(double alpha, double gamma, double sigma, double cutoff, int shifted,
+                             mxg_potential **out);
+/* Table description: kind, flags, intervals n, interval map alpha[4], domain [a,b], r0+1. */
+int mxg_potential_info(const mxg_potential *p, int *kind, unsigned *flags, int *n, float *alpha4, float *a,
+                       float *b, float *r0_plusone);
+/* Copies the (n+1)*8 FP32 coefficients; returns their count or -(needed) if cap is short. */
+int mxg_potential_coeffs(const mxg_potential *p, float *out, int cap);
+/* DPD parameters (alpha, gamma, sigma). */
+int mxg_potential_dpd_params(const mxg_potential *p, float *alpha, float *gamma, float *sigma);
+/* Host scalar evaluation with potential_eval_ex semantics: returns 1 if in range. */
+int mxg_potential_eval(const mxg_potential *p, float ri, float rj, float r2, float *e, float *f);
+void mxg_potential_free(mxg_potential *p);
+
+/* ---- engine ---- */
+/* bc_kind[6]: MXG_BOUNDARY_* per face (faces above); bc_velocity[18]: wall velocity per face for
+ * velocity boundaries; bc_restore[6]: restitution per face. Cells are raised to 3 along periodic
+ * axes as the reference does. */
+int mxg_engine_init(const double *origin, const double *dim, const int *cells, double cutoff, const int *bc_kind,
+                    const float *bc_velocity, const float *bc_restore, int max_type, unsigned flags,
+                    mxg_engine **out);
+/* dt, max-distance fraction (reference default 0.05) */
+int mxg_engine_set_dt(mxg_engine *e, double dt, double max_dist_fraction);
+/* Returns the new type id (>= 0). */
+int mxg_engine_addtype(mxg_engine *e, double mass, double radius, int dynamics, unsigned particle_flags);
+int mxg_engine_addpot(mxg_engine *e, const mxg_potential *p, int type_i, int type_j);
+int mxg_engine_add_singlebody_force(mxg_engine *e, int type, float fx, float fy, float fz);
+/* Adds n particles (positions double[3n] in global coordinates, velocities float[3n]); ids_out
+ * receives consecutive ids (may be NULL). */
+int mxg_engine_addparts(mxg_engine *e, int n, const double *x, const float *v, const int *type, int *ids_out);
+/* Adds n harmonic/table bonds between particle ids i[k], j[k], all with potential p. */
+int mxg_engine_addbonds(mxg_engine *e, int n, const int *i, const int *j, const mxg_potential *p,
+                        double dissociation_energy, int *ids_out);
+/* Builds the cell-pair lists and uploads the state. stream may be NULL (default stream). */
+int mxg_engine_start(mxg_engine *e, void *cuda_stream);
+/* Runs nsteps forward-Euler steps on the device (forces, bonds, integrate, re-bin). */
+int mxg_engine_step(mxg_engine *e, int nsteps);
+/* Computes forces (and energies) for the current positions without advancing. */
+int mxg_engine_force(mxg_engine *e);
+/* Waits for the engine's stream and returns the device status word as a status code. */
+int mxg_engine_status(mxg_engine *e);
+int mxg_engine_nr_parts(const mxg_engine *e);
+int mxg_engine_nr_cells(const mxg_engine *e);
+/* Per-id host copies: absolute positions (double[3n]), velocities, forces (float[3n]), cell index,
+ * cell-relative positions. Any pointer may be NULL. */
+int mxg_engine_unload(mxg_engine *e, int n, double *x, float *v, float *f, int *cell, float *xrel);
+/* Per-id upload of positions (double[3n], global coordinates) and velocities (float[3n]);
+ * particles are re-binned as engine_addpart would place them. */
+int mxg_engine_load(mxg_engine *e, int n, const double *x, const float *v);
+/* Potential energy (nonbonded + bonded) of the last force evaluation and the current kinetic energy,
+ * both reduced in FP64 on the device. virial9 may be NULL. */
+int mxg_engine_energy(mxg_engine *e, double *epot, double *ekin, double *virial9);
+double mxg_engine_kinetic_energy(mxg_engine *e);
+/* Cell-pair task list rows (type, sid, i, j) as space_init builds them. */
+int mxg_engine_tasks(const mxg_engine *e, int *out, int cap);
+/* Bond flags (bit 0 = active); returns the number of bonds. */
+int mxg_engine_bond_flags(mxg_engine *e, unsigned *out, int cap);
+/* Space description: cdim[3], h[3], nr_cells, period bitmask. */
+int mxg_engine_space_info(const mxg_engine *e, int *cdim, double *h, int *nr_cells, unsigned *period);
+/* Raw device-resident state in slot order (cell-sorted): pos float4 (xrel, type bits),
+ * vel float4 (v, id bits), force float4, cell index per slot; device pointers. */
+int mxg_engine_device_state(mxg_engine *e, void **pos, void **vel, void **force, void **cell);
+int mxg_engine_finalize(mxg_engine *e);
+
+/* DPD random term: 0 = reference semantics (xi = 1, dpd_eval.hpp:57), 1 = Philox stream keyed on
+ * (step, particle id pair). Set before mxg_engine_start. */
+int mxg_engine_set_rng_mode(mxg_engine *e, int mode);
+/* Clears the device status word. */
+int mxg_engine_clear_status(mxg_engine *e);
+/* Launches the nonbonded force kernel reps times back to back on the engine stream and returns the
+ * mean CUDA-event duration of one launch in milliseconds (state is not advanced). */
+int mxg_engine_time_force(mxg_engine *e, int reps, double *ms);
+
+/* ---- timing of the engine's own kernels (for roofline reporting) ---- */
+/* Enables per-kernel CUDA-event timing on the engine stream (off by default). */
+int mxg_engine_enable_timing(mxg_engine *e, int on);
+/* Accumulated milliseconds and launch counts for kernels: 0 force, 1 bonds, 2 integrate, 3 scan,
+ * 4 scatter. */
+int mxg_engine_kernel_times(mxg_engine *e, double *ms, long long *launches, int nkernels);
+/* Pair statistics for the last force evaluation: candidate and interacting pair counts as the
+ * reference's task list defines them (counted on the device when enabled). */
+int mxg_engine_pair_counts(mxg_engine *e, long long *candidates, long long *interacting);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,557 @@
+"""mechanica_b200: the force-and-step hot path of Mechanica's mdcore engine on a B200.
+
+The Python surface keeps the reference's names, arguments and defaults
+(src/MxSimulator.cpp:196-275 for ``init``, src/MxUniverse.cpp:93-108 for the
+defaults, src/mdcore/src/MxPotential.cpp:2459-2750 for the potential
+factories, src/mdcore/src/bond.cpp:535-560 for ``Bond``):
+
+    import mechanica_b200 as m
+    m.init(dim=[10, 10, 10], cells=[10, 10, 10], cutoff=1.0, dt=0.01)
+    class Argon(m.Particle):
+        mass = 39.4
+        radius = 0.1
+    pot = m.Potential.lennard_jones_12_6(0.275, 1.0, 9.5075e-6, 6.1545e-3, 1e-3)
+    m.bind(pot, Argon, Argon)
+    Argon.factory(positions=x, velocities=v)     # or Argon(position, velocity)
+    m.Universe.step()
+
+Everything below the Python layer is the C ABI of libmxg.so (include/mxg.h);
+all force, bond and integration work runs in CUDA kernels on the device.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import _native
+from ._native import EngineError, check, f32, f64, i32, lib, ptr
+
+__all__ = [
+    "init", "Universe", "universe", "Particle", "Potential", "Bond", "bind", "forces", "step", "run",
+    "Newtonian", "Overdamped", "FORWARD_EULER", "BOUNDARY_NONE", "PERIODIC_X", "PERIODIC_Y", "PERIODIC_Z",
+    "PERIODIC_FULL", "FREESLIP_X", "FREESLIP_Y", "FREESLIP_Z", "FREESLIP_FULL", "EngineError",
+]
+
+# particle dynamics (src/mdcore/include/MxParticle.h:48-49)
+Newtonian = 0
+Overdamped = 1
+FORWARD_EULER = 0
+
+# integer boundary flags (src/mdcore/include/space.h:44-59)
+BOUNDARY_NONE = 0
+PERIODIC_X = 1 << 0
+PERIODIC_Y = 1 << 1
+PERIODIC_Z = 1 << 2
+PERIODIC_FULL = PERIODIC_X | PERIODIC_Y | PERIODIC_Z
+FREESLIP_X = 1 << 6
+FREESLIP_Y = 1 << 7
+FREESLIP_Z = 1 << 8
+FREESLIP_FULL = FREESLIP_X | FREESLIP_Y | FREESLIP_Z
+
+_BC_VELOCITY, _BC_PERIODIC, _BC_FREESLIP, _BC_NOSLIP = 1, 2, 4, 16
+_FACES = ["left", "right", "front", "back", "bottom", "top"]
+_AXIS_FACES = {"x": (0, 1), "y": (2, 3), "z": (4, 5)}
+
+
+def _bc_kind_of(value):
+    s = str(value).upper()
+    if s == "PERIODIC":
+        return _BC_PERIODIC
+    if s in ("FREE_SLIP", "FREESLIP"):
+        return _BC_FREESLIP
+    if s in ("NO_SLIP", "NOSLIP"):
+        return _BC_NOSLIP
+    if s == "POTENTIAL":
+        return _BC_FREESLIP  # wall potentials are not on this path; the wall reflects
+    raise ValueError(f"invalid boundary condition {value!r}")
+
+
+def parse_bc(bc):
+    """Maps the reference's ``bc`` argument (MxBoundaryConditions.cpp:501-700) to
+    per-face kinds, wall velocities and restitution."""
+    kind = [_BC_PERIODIC] * 6
+    vel = np.zeros((6, 3), dtype=np.float32)
+    restore = np.ones(6, dtype=np.float32)
+    if bc is None:
+        return kind, vel, restore
+    if isinstance(bc, (int, np.integer)):
+        kind = [0] * 6
+        for axis, bit_p, bit_f in (("x", PERIODIC_X, FREESLIP_X), ("y", PERIODIC_Y, FREESLIP_Y),
+                                   ("z", PERIODIC_Z, FREESLIP_Z)):
+            k = _BC_PERIODIC if bc & bit_p else (_BC_FREESLIP if bc & bit_f else 0)
+            for f in _AXIS_FACES[axis]:
+                kind[f] = k
+        return kind, vel, restore
+    if isinstance(bc, dict):
+        kind = [0] * 6
+        for axis, faces in _AXIS_FACES.items():
+            if axis in bc:
+                v = bc[axis]
+                vals = v if isinstance(v, (list, tuple)) else [v]
+                k = 0
+                for item in vals:
+                    k |= _bc_kind_of(item)
+                for f in faces:
+                    kind[f] = k
+        for f, name in enumerate(_FACES):
+            if name in bc:
+                item = bc[name]
+                if isinstance(item, dict):
+                    kind[f] = _BC_VELOCITY
+                    vel[f] = np.asarray(item["velocity"], dtype=np.float32)
+                    if "restore" in item:
+                        restore[f] = float(item["restore"])
+                else:
+                    kind[f] = _bc_kind_of(item)
+        return kind, vel, restore
+    raise TypeError("bc must be an int flag set or a dict")
+
+
+class Potential:
+    """A tabulated (or DPD) pair potential; factories mirror MxPotential.cpp:2459-2750."""
+
+    def __init__(self, handle, name):
+        self._h = ctypes.c_void_p(handle)
+        self.name = name
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().mxg_potential_free(self._h)
+        except Exception:
+            pass
+
+    @staticmethod
+    def _make(fn, args, name):
+        h = ctypes.c_void_p()
+        check(getattr(lib(), fn)(*args, ctypes.byref(h)), fn)
+        return Potential(h.value, name)
+
+    @staticmethod
+    def lennard_jones_12_6(min, max, A, B, tol=None):
+        tol = 0.001 * (max - min) if tol is None else tol
+        return Potential._make("mxg_potential_create_lj126", (min, max, A, B, tol), "Lennard-Jones")
+
+    @staticmethod
+    def morse(d=1.0, a=6.0, r0=0.0, min=0.0001, max=3.0, tol=0.001):
+        return Potential._make("mxg_potential_create_morse", (d, a, r0, min, max, tol), "Morse")
+
+    @staticmethod
+    def harmonic(k, r0, min=None, max=None, tol=None):
+        rng = r0
+        min = r0 - rng if min is None else min
+        max = r0 + rng if max is None else max
+        tol = 0.01 * (max - min) if tol is None else tol
+        return Potential._make("mxg_potential_create_harmonic", (k, r0, min, max, tol), "Harmonic")
+
+    @staticmethod
+    def power(k=1.0, r0=1.0, alpha=1.0, min=None, max=None, tol=None):
+        dmin, dmax = 0.1, 3.0
+        dtol = 0.001 if alpha >= 1 else 0.01
+        if r0 > 0:
+            dmin = r0 if alpha <= 1 else 0.1 * r0
+            dmax = 3.0 * r0
+        return Potential._make("mxg_potential_create_power",
+                               (k, r0, alpha, dmin if min is None else min, dmax if max is None else max,
+                                dtol if tol is None else tol), "Power")
+
+    @staticmethod
+    def dpd(alpha=1.0, gamma=1.0, sigma=1.0, cutoff=1.0, shifted=False):
+        # the reference stores the parameters as float (MxPotential.cpp:2738-2750)
+        return Potential._make("mxg_potential_create_dpd", (alpha, gamma, sigma, cutoff, int(bool(shifted))),
+                               "Dissapative Particle Dynamics")
+
+    def _info(self):
+        kind, flags, n = ctypes.c_int(), ctypes.c_uint(), ctypes.c_int()
+        a4 = (ctypes.c_float * 4)()
+        a, b, r0 = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        check(lib().mxg_potential_info(self._h, ctypes.byref(kind), ctypes.byref(flags), ctypes.byref(n), a4,
+                                       ctypes.byref(a), ctypes.byref(b), ctypes.byref(r0)), "potential_info")
+        return dict(kind=kind.value, flags=flags.value, n=n.value, alpha=np.array(a4, dtype=np.float32),
+                    a=a.value, b=b.value, r0_plusone=r0.value)
+
+    @property
+    def min(self):
+        return self._info()["a"]
+
+    @property
+    def max(self):
+        return self._info()["b"]
+
+    cutoff = max
+
+    @property
+    def domain(self):
+        i = self._info()
+        return (i["a"], i["b"])
+
+    @property
+    def intervals(self):
+        return self._info()["n"]
+
+    @property
+    def flags(self):
+        return self._info()["flags"]
+
+    @property
+    def kind(self):
+        return self._info()["kind"]
+
+    @property
+    def coefficients(self):
+        n = self.intervals
+        out = np.zeros((n + 1) * 8, dtype=np.float32)
+        check(lib().mxg_potential_coeffs(self._h, ptr(out, ctypes.c_float), out.size), "potential_coeffs")
+        return out
+
+    def __call__(self, r, r0=None):
+        """(energy, force) at distance r; like potential_call (MxPotential.cpp:2375-2414)."""
+        info = self._info()
+        if (info["flags"] & ((1 << 11) | (1 << 12))) and (r0 is None or r0 < 0):
+            r0 = 1.0
+        r0 = 0.0 if r0 is None else r0
+        e, f = ctypes.c_float(), ctypes.c_float()
+        lib().mxg_potential_eval(self._h, r0 / 2, r0 / 2, float(np.float32(r) * np.float32(r)), ctypes.byref(e),
+                                 ctypes.byref(f))
+        return (e.value, float(np.float32(f.value) * np.float32(r)))
+
+
+class _ConstantForce:
+    def __init__(self, value, period=None):
+        self.value = np.asarray(value, dtype=np.float32).reshape(3)
+
+
+class forces:  # noqa: N801 - namespace mirroring m.forces
+    ConstantForce = _ConstantForce
+
+
+class Bond:
+    """A pairwise bond with a table potential and dissociation threshold
+    (bond.cpp:535-560; break test eff >= dissociation_energy, bond.cpp:230)."""
+
+    def __init__(self, potential, i, j, dissociation_energy=np.finfo(np.float64).max):
+        u = _require()
+        self.id = u._add_bonds(potential, [_pid(i)], [_pid(j)], dissociation_energy)[0]
+        self.potential = potential
+
+    @property
+    def active(self):
+        return bool(universe.bond_flags()[self.id] & 1)
+
+
+def _pid(p):
+    return p.id if isinstance(p, Particle) else int(p)
+
+
+class _ParticleMeta(type):
+    def __init__(cls, name, bases, ns):
+        super().__init__(name, bases, ns)
+        if bases and any(isinstance(b, _ParticleMeta) for b in bases):
+            u = _require()
+            cls.id = u._add_type(cls)
+
+    def factory(cls, positions=None, velocities=None, nr_parts=None):
+        """Bulk creation of particles of this type from arrays (N x 3)."""
+        u = _require()
+        x = np.asarray(positions, dtype=np.float64).reshape(-1, 3)
+        v = np.zeros_like(x, dtype=np.float32) if velocities is None else np.asarray(velocities).reshape(-1, 3)
+        ids = u._add_particles(x, v, np.full(len(x), cls.id, dtype=np.int32))
+        return ids
+
+
+class Particle(metaclass=_ParticleMeta):
+    """Base particle type; subclasses define a type (mass, radius, dynamics)."""
+
+    mass = 1.0
+    radius = 1.0
+    dynamics = Newtonian
+    frozen = 0
+
+    def __init__(self, position=None, velocity=None):
+        u = _require()
+        if position is None:
+            position = np.random.uniform(0, 1, 3) * np.asarray(u.dim)
+        velocity = np.zeros(3) if velocity is None else velocity
+        self.id = u._add_particles(np.asarray(position, dtype=np.float64).reshape(1, 3),
+                                   np.asarray(velocity, dtype=np.float32).reshape(1, 3),
+                                   np.array([type(self).id], dtype=np.int32))[0]
+
+    @property
+    def position(self):
+        return universe.positions[self.id]
+
+    @property
+    def velocity(self):
+        return universe.velocities[self.id]
+
+    @property
+    def force(self):
+        return universe.forces[self.id]
+
+
+class _Universe:
+    """The simulation (engine + space); mirrors MxUniverse."""
+
+    def __init__(self):
+        self._e = None
+
+    # ---- configuration ----
+    def _init(self, dim, cells, cutoff, dt, bc, max_distance, origin, rng, max_types):
+        self.dim = [float(d) for d in dim]
+        self.origin = [float(o) for o in origin]
+        self.cells = [int(c) for c in cells]
+        self.cutoff = float(cutoff)
+        self.dt = float(dt)
+        self.bc = bc
+        self.max_distance = max_distance
+        self.rng = rng
+        self.max_types = max_types
+        self.time = 0
+        self._types = []        # (mass, radius, dynamics, flags)
+        self._pots = []         # (potential, ti, tj)
+        self._forces = []       # (type, value)
+        self._bonds = []        # (potential, i[], j[], dissociation)
+        self._x = np.zeros((0, 3))
+        self._v = np.zeros((0, 3), dtype=np.float32)
+        self._t = np.zeros(0, dtype=np.int32)
+        self._started = False
+        self._dirty = False
+        self._new_engine()
+
+    def _new_engine(self):
+        if self._e is not None:
+            lib().mxg_engine_finalize(self._e)
+            self._e = None
+        kind, vel, restore = parse_bc(self.bc)
+        h = ctypes.c_void_p()
+        check(lib().mxg_engine_init(ptr(f64(self.origin), ctypes.c_double), ptr(f64(self.dim), ctypes.c_double),
+                                    ptr(i32(self.cells), ctypes.c_int), self.cutoff, ptr(i32(kind), ctypes.c_int),
+                                    ptr(f32(vel), ctypes.c_float), ptr(f32(restore), ctypes.c_float),
+                                    self.max_types, 0, ctypes.byref(h)), "engine_init")
+        self._e = h
+        frac = -1.0
+        if self.max_distance is not None and self.max_distance >= 0:
+            hh = self.space_info()[1]
+            frac = self.max_distance / hh[0]
+        check(lib().mxg_engine_set_dt(self._e, self.dt, frac), "set_dt")
+        check(lib().mxg_engine_set_rng_mode(self._e, 1 if self.rng == "philox" else 0), "set_rng_mode")
+        for (m, r, d, fl) in self._types:
+            check(lib().mxg_engine_addtype(self._e, m, r, d, fl), "addtype")
+        for (p, a, b) in self._pots:
+            check(lib().mxg_engine_addpot(self._e, p._h, a, b), "addpot")
+        for (t, v) in self._forces:
+            check(lib().mxg_engine_add_singlebody_force(self._e, t, float(v[0]), float(v[1]), float(v[2])),
+                  "add_singlebody_force")
+        for (p, ii, jj, d) in self._bonds:
+            check(lib().mxg_engine_addbonds(self._e, len(ii), ptr(ii, ctypes.c_int), ptr(jj, ctypes.c_int), p._h, d,
+                                            None), "addbonds")
+        self._started = False
+
+    def _add_type(self, cls):
+        fl = int(getattr(cls, "frozen", 0))
+        rec = (float(cls.mass), float(cls.radius), int(cls.dynamics), fl)
+        tid = check(lib().mxg_engine_addtype(self._e, *rec), "addtype") if not self._started else None
+        self._types.append(rec)
+        if tid is None:
+            self._dirty = True
+            tid = len(self._types) - 1
+        return tid
+
+    def _add_particles(self, x, v, t):
+        first = len(self._t)
+        self._sync_state()
+        self._x = np.concatenate([self._x, np.asarray(x, dtype=np.float64)])
+        self._v = np.concatenate([self._v, np.asarray(v, dtype=np.float32)])
+        self._t = np.concatenate([self._t, np.asarray(t, dtype=np.int32)])
+        self._dirty = True
+        return list(range(first, first + len(t)))
+
+    def _add_bonds(self, pot, i, j, d):
+        ii, jj = i32(i), i32(j)
+        first = sum(len(b[1]) for b in self._bonds)
+        self._bonds.append((pot, ii, jj, float(d)))
+        self._sync_state()
+        self._dirty = True
+        return list(range(first, first + len(ii)))
+
+    def bind(self, obj, a, b=None):
+        """Binds a potential to a pair of types, or a force to a type (MxBind.cpp:18-100)."""
+        ta = a.id if isinstance(a, type) else int(a)
+        if isinstance(obj, Potential):
+            tb = ta if b is None else (b.id if isinstance(b, type) else int(b))
+            self._sync_state()
+            self._pots.append((obj, ta, tb))
+            self._dirty = True
+        elif isinstance(obj, _ConstantForce):
+            self._sync_state()
+            self._forces.append((ta, obj.value))
+            self._dirty = True
+        else:
+            raise TypeError("bind expects a Potential or a force")
+
+    # ---- engine lifecycle ----
+    def _sync_state(self):
+        """Pulls the device state back into the host arrays before a rebuild."""
+        if self._started:
+            n = len(self._t)
+            x = np.zeros((n, 3))
+            v = np.zeros((n, 3), dtype=np.float32)
+            check(lib().mxg_engine_unload(self._e, n, ptr(x, ctypes.c_double), ptr(v, ctypes.c_float), None, None,
+                                          None), "unload")
+            self._x, self._v = x, v
+
+    def _ensure(self):
+        if self._started and not self._dirty:
+            return
+        if self._started or self._dirty:
+            self._new_engine()
+        n = len(self._t)
+        if n:
+            check(lib().mxg_engine_addparts(self._e, n, ptr(f64(self._x), ctypes.c_double),
+                                            ptr(f32(self._v), ctypes.c_float), ptr(i32(self._t), ctypes.c_int),
+                                            None), "addparts")
+        check(lib().mxg_engine_start(self._e, None), "engine_start")
+        self._started = True
+        self._dirty = False
+
+    @property
+    def handle(self):
+        self._ensure()
+        return self._e
+
+    def step(self, until=0, dt=0):
+        """One engine step (MxUniverse_Step ignores until and dt, MxUniverse.cpp:549-566)."""
+        self.steps(1)
+
+    def steps(self, n):
+        self._ensure()
+        check(lib().mxg_engine_step(self._e, int(n)), "engine_step")
+        self.time += int(n)
+        check(lib().mxg_engine_status(self._e), "engine_step")
+
+    def force(self):
+        self._ensure()
+        check(lib().mxg_engine_force(self._e), "engine_force")
+        check(lib().mxg_engine_status(self._e), "engine_force")
+
+    def _unload(self):
+        self._ensure()
+        n = len(self._t)
+        x = np.zeros((n, 3))
+        v = np.zeros((n, 3), dtype=np.float32)
+        f = np.zeros((n, 3), dtype=np.float32)
+        c = np.zeros(n, dtype=np.int32)
+        xr = np.zeros((n, 3), dtype=np.float32)
+        check(lib().mxg_engine_unload(self._e, n, ptr(x, ctypes.c_double), ptr(v, ctypes.c_float),
+                                      ptr(f, ctypes.c_float), ptr(c, ctypes.c_int), ptr(xr, ctypes.c_float)), "unload")
+        return x, v, f, c, xr
+
+    @property
+    def positions(self):
+        return self._unload()[0]
+
+    @property
+    def velocities(self):
+        return self._unload()[1]
+
+    @property
+    def forces(self):
+        return self._unload()[2]
+
+    def state(self):
+        """(positions, velocities, forces, cell, cell-relative positions) by particle id."""
+        return self._unload()
+
+    def energies(self):
+        self._ensure()
+        ep, ek = ctypes.c_double(), ctypes.c_double()
+        check(lib().mxg_engine_energy(self._e, ctypes.byref(ep), ctypes.byref(ek), None), "energy")
+        return ep.value, ek.value
+
+    @property
+    def kinetic_energy(self):
+        return self.energies()[1]
+
+    @property
+    def potential_energy(self):
+        return self.energies()[0]
+
+    def tasks(self):
+        n = lib().mxg_engine_tasks(self._e, None, 0)
+        out = np.zeros(4 * n, dtype=np.int32)
+        check(lib().mxg_engine_tasks(self._e, ptr(out, ctypes.c_int), out.size), "tasks")
+        return out.reshape(n, 4)
+
+    def bond_flags(self):
+        self._ensure()
+        n = lib().mxg_engine_bond_flags(self._e, None, 0)
+        out = np.zeros(max(n, 1), dtype=np.uint32)
+        check(lib().mxg_engine_bond_flags(self._e, ptr(out, ctypes.c_uint), out.size), "bond_flags")
+        return out[:n]
+
+    def space_info(self):
+        cdim = np.zeros(3, dtype=np.int32)
+        hh = np.zeros(3)
+        nc, per = ctypes.c_int(), ctypes.c_uint()
+        check(lib().mxg_engine_space_info(self._e, ptr(cdim, ctypes.c_int), ptr(hh, ctypes.c_double),
+                                          ctypes.byref(nc), ctypes.byref(per)), "space_info")
+        return cdim, hh, nc.value, per.value
+
+    def time_force(self, reps=10):
+        self._ensure()
+        ms = ctypes.c_double()
+        check(lib().mxg_engine_time_force(self._e, int(reps), ctypes.byref(ms)), "time_force")
+        return ms.value
+
+    def candidate_pairs(self):
+        self._ensure()
+        c, i = ctypes.c_longlong(), ctypes.c_longlong()
+        check(lib().mxg_engine_pair_counts(self._e, ctypes.byref(c), ctypes.byref(i)), "pair_counts")
+        return c.value
+
+    def close(self):
+        if self._e is not None:
+            lib().mxg_engine_finalize(self._e)
+            self._e = None
+
+
+class _UniverseNamespace:
+    """``m.Universe``: class-level access to the single universe."""
+
+    def __getattr__(self, name):
+        return getattr(universe, name)
+
+
+universe = _Universe()
+Universe = _UniverseNamespace()
+
+
+def _require():
+    if universe._e is None:
+        raise RuntimeError("mechanica_b200: call init() first")
+    return universe
+
+
+def init(dim=(10.0, 10.0, 10.0), cutoff=1.0, cells=(4, 4, 4), dt=0.01, bc=None, boundary_conditions=None,
+         max_distance=None, origin=(0.0, 0.0, 0.0), integrator=FORWARD_EULER, rng="reference", max_types=64,
+         **ignored):
+    """Initialises the universe (MxSimulator_Init / universe_init). Rendering and
+    windowing arguments of the reference are accepted and ignored."""
+    if integrator != FORWARD_EULER:
+        raise NotImplementedError("only the forward Euler integrator is on this path")
+    universe.close()
+    universe._init(dim, cells, cutoff, dt, bc if bc is not None else boundary_conditions, max_distance, origin,
+                   rng, max_types)
+    return universe
+
+
+def bind(obj, a, b=None):
+    return _require().bind(obj, a, b)
+
+
+def step(until=0, dt=0):
+    return _require().step(until, dt)
+
+
+def run(steps=1):
+    return _require().steps(steps)

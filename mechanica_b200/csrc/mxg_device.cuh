@@ -1,0 +1,198 @@
+/*
+ * Device-side data layout and helpers shared by the engine kernels.
+ *
+ * HBM layout (all arrays in slot order = sorted by cell, ascending particle id
+ * inside a cell):
+ *   pos[slot]   float4  (x, y, z relative to the cell origin, w = type id bits)
+ *   vel[slot]   float4  (vx, vy, vz, w = particle id bits)
+ *   force[slot] float4  (fx, fy, fz, w unused)
+ *   cell_of[slot] int
+ * Cells: cell_start[c], cell_count[c]; per cell a CSR list of neighbour
+ * entries (neighbour cell, role, float shift) derived from the reference's
+ * cell-pair task list. The kernels in this translation unit are compiled
+ * without FMA contraction so that every per-pair and per-particle operation
+ * rounds exactly as the reference's scalar FP32/FP64 code does.
+ */
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mxg {
+
+constexpr int kChunk = 8;           // floats per table interval
+constexpr int kBucket = 32;         // max particles entering one cell per step
+constexpr int kMaxTypes = 64;       // types per engine
+constexpr int kWarpsPerBlock = 4;   // force kernel: warps (cells) per block
+
+/* neighbour-entry roles, relative to the reference's (flipped) cell pair */
+enum : int { kRoleSelf = 0, kRoleFirst = 1, kRoleSecond = 2 };
+
+/* cell flags (space_cell.h:48-82) */
+enum : unsigned {
+    kCellActiveTop = 1u << 5,
+    kCellActiveBottom = 1u << 6,
+    kCellActiveLeft = 1u << 7,
+    kCellActiveRight = 1u << 8,
+    kCellActiveFront = 1u << 9,
+    kCellActiveBack = 1u << 10,
+    kCellActiveAny = (1u << 5) | (1u << 6) | (1u << 7) | (1u << 8) | (1u << 9) | (1u << 10),
+};
+
+/* boundary kinds */
+enum : unsigned { kBcVelocity = 1u << 0, kBcPeriodic = 1u << 1, kBcFreeslip = 1u << 2 };
+
+/* status word bits */
+enum : unsigned {
+    kStatusTooFast = 1u << 0,
+    kStatusBucketOverflow = 1u << 1,
+    kStatusNonFinite = 1u << 2,
+};
+
+struct DevPot {          // one per potential, 64 B
+    int kind;            // 0 table, 1 DPD
+    unsigned flags;
+    int n;
+    int coef_off;        // float offset into the coefficient pool
+    float alpha0, alpha1, alpha2;
+    float a, b, r0_plusone;
+    float dpd_alpha, dpd_gamma, dpd_sigma, dpd_delta;  // delta = 1/sqrt(dt) as the reference keeps it
+    float a2;            // a*a (float)
+    float pad;
+};
+
+struct DevType {
+    double imass;
+    double mass;
+    float radius;
+    int dynamics;        // 0 Newtonian, 1 overdamped
+    unsigned flags;      // frozen bits
+    float fx, fy, fz;    // constant body force
+    int has_force;
+    int pad;
+};
+
+struct DevSpace {        // one per replica
+    double hd[3];        // cell size (double, as space.h keeps it)
+    float h[3], h2[3];   // float(h), float(2h)
+    float maxv[3], maxv2[3], maxx[3], maxx2[3];
+    float dt;
+    float cut2_pair, cut2_self;
+    int cdim[3];
+    int cell_offset;
+    int ncells;
+    int pot_offset;      // offset of this replica's type-pair matrix
+    unsigned bc_kind[6];
+    float bc_vel[6][3];
+    float bc_restore[6];
+    unsigned rng_mode;   // 0: reference DPD random term (xi = 1), 1: Philox
+    unsigned pad;
+};
+
+struct DevBond {
+    int i, j;            // particle ids
+    int pot;             // potential index
+    int pad;
+    double dissociation;
+};
+
+struct EngineView {      // everything a kernel needs, passed by value
+    const float4 *pos;
+    const float4 *vel;
+    float4 *force;
+    const int *cell_of;
+    const int *cell_start;
+    const int *cell_count;
+    const int *cell_rep;
+    const unsigned *cell_flags;
+    const int *nb_off;
+    const int *nb_cell;
+    const float4 *nb_shift;  // xyz shift, w = role bits
+    const DevPot *pots;
+    const float *coef;
+    const int *pot_idx;      // per replica: [ntypes*ntypes] potential index or -1
+    const DevType *types;
+    const DevSpace *spaces;
+    int ntypes;
+    int ncells;
+    int nparts;
+    const unsigned long long *step;  // device step counter
+    double *epot_cell;       // per cell nonbonded energy of the last force pass
+    unsigned *status;
+};
+
+#ifdef __CUDACC__
+/* ---- exact-rounding helpers (the file is compiled with -fmad=false too) ---- */
+__device__ __forceinline__ float dot3_rn(float x, float y, float z) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z));
+}
+
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11), counter-based. */
+__device__ __forceinline__ uint4 philox4x32(uint4 c, uint2 k) {
+    const unsigned M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const unsigned hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+        const unsigned hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += W0;
+        k.y += W1;
+    }
+    return c;
+}
+
+/* uniform in (0,1) from 32 random bits */
+__device__ __forceinline__ float u01(unsigned x) { return ((float)(x >> 8) + 0.5f) * (1.0f / 16777216.0f); }
+
+/* Table evaluation with potential_eval_ex semantics (potential_eval.hpp:106-161):
+ * returns false when out of range. ri, rj are the particle radii. */
+__device__ __forceinline__ bool table_eval_ex(const DevPot &p, const float *__restrict__ coef, float ri, float rj,
+                                              float r2, float &e, float &f) {
+    float r = sqrtf(r2);
+    const float ro = r < 1.19209290e-7f ? 1.19209290e-7f : r;
+    r = r < p.a ? p.a : r;
+    if (p.flags & (1u << 11))
+        r = __fdiv_rn(r, __fadd_rn(ri, rj));
+    else if (p.flags & (1u << 12))
+        r = __fadd_rn(__fsub_rn(r, __fadd_rn(ri, rj)), p.r0_plusone);
+    const float t = __fadd_rn(p.alpha0, __fmul_rn(r, __fadd_rn(p.alpha1, __fmul_rn(r, p.alpha2))));
+    const unsigned ind = (unsigned)fmaxf(0.0f, t);
+    if (r > p.b || ind > (unsigned)p.n) return false;
+    const float4 *c4 = reinterpret_cast<const float4 *>(coef + p.coef_off + ind * kChunk);
+    const float4 c0 = __ldg(c4), c1 = __ldg(c4 + 1);
+    const float x = __fmul_rn(__fsub_rn(r, c0.x), c0.y);
+    float ee = __fadd_rn(__fmul_rn(c0.z, x), c0.w);
+    float eff = c0.z;
+    eff = __fadd_rn(__fmul_rn(eff, x), ee); ee = __fadd_rn(__fmul_rn(ee, x), c1.x);
+    eff = __fadd_rn(__fmul_rn(eff, x), ee); ee = __fadd_rn(__fmul_rn(ee, x), c1.y);
+    eff = __fadd_rn(__fmul_rn(eff, x), ee); ee = __fadd_rn(__fmul_rn(ee, x), c1.z);
+    eff = __fadd_rn(__fmul_rn(eff, x), ee); ee = __fadd_rn(__fmul_rn(ee, x), c1.w);
+    e = ee;
+    f = __fdiv_rn(__fmul_rn(eff, c0.y), ro);
+    return true;
+}
+
+/* Table evaluation with potential_eval semantics (no range check, no
+ * radius shift; potential_eval.hpp:67-104), used by bonds. */
+__device__ __forceinline__ void table_eval(const DevPot &p, const float *__restrict__ coef, float r2, float &e,
+                                           float &f) {
+    const float r = sqrtf(r2);
+    const float t = __fadd_rn(p.alpha0, __fmul_rn(r, __fadd_rn(p.alpha1, __fmul_rn(r, p.alpha2))));
+    // the reference indexes unchecked; r is clamped to [a, b] by the caller, so
+    // ind <= n except for rounding at r = b, which is clamped here
+    const int ind = min((int)fmaxf(0.0f, t), p.n);
+    const float4 *c4 = reinterpret_cast<const float4 *>(coef + p.coef_off + ind * kChunk);
+    const float4 c0 = __ldg(c4), c1 = __ldg(c4 + 1);
+    const float x = __fmul_rn(__fsub_rn(r, c0.x), c0.y);
+    float ee = __fadd_rn(__fmul_rn(c0.z, x), c0.w);
+    float eff = c0.z;
+    eff = __fadd_rn(__fmul_rn(eff, x), ee); ee = __fadd_rn(__fmul_rn(ee, x), c1.x);
+    eff = __fadd_rn(__fmul_rn(eff, x), ee); ee = __fadd_rn(__fmul_rn(ee, x), c1.y);
+    eff = __fadd_rn(__fmul_rn(eff, x), ee); ee = __fadd_rn(__fmul_rn(ee, x), c1.z);
+    eff = __fadd_rn(__fmul_rn(eff, x), ee); ee = __fadd_rn(__fmul_rn(ee, x), c1.w);
+    e = ee;
+    f = __fdiv_rn(__fmul_rn(eff, c0.y), r);
+}
+
+#endif  // __CUDACC__
+
+}  // namespace mxg

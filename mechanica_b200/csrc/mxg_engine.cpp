@@ -1,0 +1,1109 @@
+/*
+ * Host side of the engine behind the C ABI in include/mxg.h.
+ *
+ * Set-up mirrors the reference engine:
+ *   - geometry and cells: engine_init (src/mdcore/src/engine.cpp:1502-1560) and
+ *     space_init (src/mdcore/src/space.cpp:626-978), including the cell-pair
+ *     task list, its pruning and the sort-ID / flip of every pair
+ *     (space_getsid, space.cpp:95-130);
+ *   - particle placement: space_addpart (space.cpp:397-477) followed by the
+ *     relocation rule of space_shuffle_local (space.cpp:333-393) that the first
+ *     engine_force applies;
+ *   - integrator constants: engine_advance_forward_euler (engine_advance.cpp:270-280).
+ * The task list is turned into per-cell neighbour entries carrying the pair's
+ * float shift and the role of the cell in the (flipped) pair, so the device
+ * force kernel reproduces each pair's arithmetic exactly.
+ *
+ * Device state is allocated once at mxg_engine_start and stays resident; a step
+ * is five kernels (force, bonds, integrate, scan, scatter) replayed from CUDA
+ * graphs, one per buffer parity.
+ */
+#include "../../include/mxg.h"
+#include "mxg_kernels.h"
+#include "potential_table.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <vector>
+
+struct mxg_potential {
+    mxg::PotentialTable t;
+};
+
+namespace {
+
+using namespace mxg;
+
+/* sort-ID tables of space_cell.cpp:54-99 (27 shift directions -> 13 sort lists) */
+const int kSortlistID[27] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 0, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2, 1, 0};
+const bool kCellFlip[27] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+
+enum : int { kTaskSelf = 1, kTaskPair = 2, kTaskSort = 3 };  // task.h:31-37
+
+struct Task {
+    int type, flags, i, j;
+};
+
+enum : unsigned {
+    kPeriodicX = 1u << 0,
+    kPeriodicY = 1u << 1,
+    kPeriodicZ = 1u << 2,
+};
+
+struct TypeInfo {
+    double mass, imass, radius;
+    int dynamics;
+    unsigned flags;
+    float force[3];
+    bool has_force;
+};
+
+struct BondInfo {
+    int i, j, pot;
+    double dissociation;
+};
+
+#define CUDA_TRY(x)                                                                              \
+    do {                                                                                         \
+        cudaError_t err_ = (x);                                                                  \
+        if (err_ != cudaSuccess) {                                                               \
+            fprintf(stderr, "mxg: CUDA error %s at %s:%d\n", cudaGetErrorString(err_), __FILE__, __LINE__); \
+            return MXG_ERR_CUDA;                                                                 \
+        }                                                                                        \
+    } while (0)
+
+template <typename T>
+int dev_alloc(T **p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    if (cudaMalloc((void **)p, n * sizeof(T)) != cudaSuccess) return MXG_ERR_MALLOC;
+    return MXG_OK;
+}
+
+template <typename T>
+int upload(T *dst, const std::vector<T> &src, cudaStream_t st) {
+    if (src.empty()) return MXG_OK;
+    CUDA_TRY(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    return MXG_OK;
+}
+
+}  // namespace
+
+struct mxg_engine {
+    // ---- configuration ----
+    double origin[3], dim[3];
+    int cells[3];
+    double cutoff;
+    int bc_kind[6];
+    float bc_vel[6][3];
+    float bc_restore[6];
+    unsigned period = 0;
+    int max_type = 0;
+    double dt = 0.01;
+    float max_dist_fraction = 0.05f;
+    unsigned rng_mode = 0;
+
+    // ---- space (space_init) ----
+    int cdim[3];
+    double h[3], ih[3];
+    int ncells = 0;
+    std::vector<unsigned> cell_flags;
+    std::vector<double> cell_origin;  // 3 per cell
+    std::vector<Task> tasks;
+
+    // ---- model ----
+    std::vector<TypeInfo> types;
+    std::vector<mxg::PotentialTable> pots;  // private copies
+    std::vector<int> pot_idx;               // max_type^2 (compacted to ntypes^2 at start)
+    std::vector<double> px;                 // staged positions (3 per particle)
+    std::vector<float> pv;
+    std::vector<int> ptype;
+    std::vector<BondInfo> bonds;
+
+    // ---- device ----
+    bool started = false;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    int nparts = 0;
+    int ntypes = 0;
+    int cur = 0;
+    float4 *d_pos[2] = {nullptr, nullptr}, *d_vel[2] = {nullptr, nullptr};
+    float4 *d_force = nullptr;
+    int *d_cell_of[2] = {nullptr, nullptr};
+    int *d_new_cell = nullptr;
+    int *d_cell_start[2] = {nullptr, nullptr}, *d_cell_count[2] = {nullptr, nullptr};
+    int *d_in_count = nullptr, *d_out_count = nullptr, *d_in_list = nullptr;
+    int *d_slot_of_id = nullptr;
+    int *d_cell_rep = nullptr;
+    unsigned *d_cell_flags = nullptr;
+    int *d_nb_off = nullptr, *d_nb_cell = nullptr;
+    float4 *d_nb_shift = nullptr;
+    DevPot *d_pots = nullptr;
+    float *d_coef = nullptr;
+    int *d_pot_idx = nullptr;
+    DevType *d_types = nullptr;
+    DevSpace *d_spaces = nullptr;
+    double *d_epot_cell = nullptr, *d_ebond_slot = nullptr;
+    DevBond *d_bonds = nullptr;
+    unsigned *d_bond_flags = nullptr;
+    int *d_bond_off = nullptr, *d_bond_list = nullptr;
+    unsigned *d_status = nullptr;
+    unsigned long long *d_step = nullptr;
+    double *d_partials = nullptr, *d_energy = nullptr;
+    int energy_blocks = 64;
+    bool has_dpd = false;
+    int force_grid = 0;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool use_graphs = true;
+    std::vector<void *> allocations;
+
+    ~mxg_engine() {
+        for (int k = 0; k < 2; ++k)
+            if (graph[k]) cudaGraphExecDestroy(graph[k]);
+        for (void *p : allocations) cudaFree(p);
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+
+    template <typename T>
+    int alloc(T **p, size_t n) {
+        int rc = dev_alloc(p, n);
+        if (rc == MXG_OK) allocations.push_back((void *)*p);
+        return rc;
+    }
+
+    int cellid(int i, int j, int k) const { return (i * cdim[1] + j) * cdim[2] + k; }
+
+    /* space_getsid (space.cpp:95-130): min-image shift between cell origins,
+     * sort ID, and the flip of (ci, cj). shift is single precision. */
+    int getsid(int &ci, int &cj, float *shift) const {
+        for (int k = 0; k < 3; ++k) {
+            shift[k] = (float)(cell_origin[3 * cj + k] - cell_origin[3 * ci + k]);
+            if (shift[k] * 2 > dim[k])
+                shift[k] = (float)(shift[k] - dim[k]);
+            else if (shift[k] * 2 < -dim[k])
+                shift[k] = (float)(shift[k] + dim[k]);
+        }
+        int sid = 0;
+        for (int k = 0; k < 3; ++k) sid = 3 * sid + ((shift[k] < 0) ? 0 : ((shift[k] > 0) ? 2 : 1));
+        if (kCellFlip[sid]) {
+            std::swap(ci, cj);
+            for (int k = 0; k < 3; ++k) shift[k] = -shift[k];
+        }
+        return kSortlistID[sid];
+    }
+
+    int build_space() {
+        // engine_init: L = (dim - origin)/cells; space_init: cdim = floor(dim/L), h = dim/cdim
+        for (int k = 0; k < 3; ++k) {
+            const double L = (dim[k] - origin[k]) / cells[k];
+            cdim[k] = (int)std::floor(dim[k] / L);
+            if (cdim[k] < 1) return MXG_ERR_SPACE;
+        }
+        ncells = cdim[0] * cdim[1] * cdim[2];
+        for (int k = 0; k < 3; ++k) {
+            h[k] = dim[k] / cdim[k];
+            ih[k] = 1.0 / h[k];
+        }
+        cell_flags.assign(ncells, 0u);
+        cell_origin.assign(3 * ncells, 0.0);
+        const unsigned active = MXG_BOUNDARY_FREESLIP | MXG_BOUNDARY_VELOCITY;
+        int l[3];
+        double o[3];
+        for (l[0] = 0; l[0] < cdim[0]; l[0]++) {
+            o[0] = origin[0] + l[0] * h[0];
+            for (l[1] = 0; l[1] < cdim[1]; l[1]++) {
+                o[1] = origin[1] + l[1] * h[1];
+                for (l[2] = 0; l[2] < cdim[2]; l[2]++) {
+                    o[2] = origin[2] + l[2] * h[2];
+                    const int c = cellid(l[0], l[1], l[2]);
+                    for (int k = 0; k < 3; ++k) cell_origin[3 * c + k] = o[k];
+                    unsigned f = 0;
+                    if (l[0] == 0 && (bc_kind[MXG_FACE_LEFT] & active))
+                        f |= kCellActiveLeft;
+                    else if (l[0] + 1 == cdim[0] && (bc_kind[MXG_FACE_RIGHT] & active))
+                        f |= kCellActiveRight;
+                    if (l[1] == 0 && (bc_kind[MXG_FACE_FRONT] & active))
+                        f |= kCellActiveFront;
+                    else if (l[1] + 1 == cdim[1] && (bc_kind[MXG_FACE_BACK] & active))
+                        f |= kCellActiveBack;
+                    if (l[2] == 0 && (bc_kind[MXG_FACE_BOTTOM] & active))
+                        f |= kCellActiveBottom;
+                    else if (l[2] + 1 == cdim[2] && (bc_kind[MXG_FACE_TOP] & active))
+                        f |= kCellActiveTop;
+                    cell_flags[c] = f;
+                }
+            }
+        }
+        // cell-pair tasks (space.cpp:797-913); no ghost cells on this path
+        int span[3];
+        for (int k = 0; k < 3; ++k) span[k] = (int)std::ceil(cutoff * ih[k]);
+        const double cutoff2 = cutoff * cutoff;
+        tasks.clear();
+        for (int i = 0; i < cdim[0]; i++)
+            for (int j = 0; j < cdim[1]; j++)
+                for (int k = 0; k < cdim[2]; k++) {
+                    const int id1 = cellid(i, j, k);
+                    for (l[0] = -span[0]; l[0] <= span[0]; l[0]++) {
+                        int ii = i + l[0];
+                        if (ii < 0) {
+                            if (period & kPeriodicX) ii += cdim[0]; else continue;
+                        } else if (ii >= cdim[0]) {
+                            if (period & kPeriodicX) ii -= cdim[0]; else continue;
+                        }
+                        for (l[1] = -span[1]; l[1] <= span[1]; l[1]++) {
+                            int jj = j + l[1];
+                            if (jj < 0) {
+                                if (period & kPeriodicY) jj += cdim[1]; else continue;
+                            } else if (jj >= cdim[1]) {
+                                if (period & kPeriodicY) jj -= cdim[1]; else continue;
+                            }
+                            for (l[2] = -span[2]; l[2] <= span[2]; l[2]++) {
+                                double lh[3];
+                                for (int q = 0; q < 3; ++q) lh[q] = h[q] * std::fmax(std::abs(l[q]) - 1, 0);
+                                if (lh[0] * lh[0] + lh[1] * lh[1] + lh[2] * lh[2] > cutoff2) continue;
+                                int kk = k + l[2];
+                                if (kk < 0) {
+                                    if (period & kPeriodicZ) kk += cdim[2]; else continue;
+                                } else if (kk >= cdim[2]) {
+                                    if (period & kPeriodicZ) kk -= cdim[2]; else continue;
+                                }
+                                const int id2 = cellid(ii, jj, kk);
+                                int ci = id1, cj = id2;
+                                float shift[3];
+                                const int sid = getsid(ci, cj, shift);
+                                if (id1 < id2 || (id1 == id2 && l[0] == 0 && l[1] == 0 && l[2] == 0))
+                                    tasks.push_back({id1 == id2 ? kTaskSelf : kTaskPair, sid, ci, cj});
+                            }
+                        }
+                    }
+                }
+        return MXG_OK;
+    }
+
+    /* space_addpart's placement plus the first shuffle: cell index and
+     * cell-relative float position. */
+    int place(const double *x, int &cell, float *xr) const {
+        int ind[3];
+        for (int k = 0; k < 3; ++k) ind[k] = (int)((x[k] - origin[k]) * ih[k]);
+        for (int k = 0; k < 3; ++k)
+            if (ind[k] < 0 || ind[k] >= cdim[k]) return MXG_ERR_SPACE;
+        cell = cellid(ind[0], ind[1], ind[2]);
+        for (int k = 0; k < 3; ++k) xr[k] = (float)(x[k] - cell_origin[3 * cell + k]);
+        int delta[3];
+        for (int k = 0; k < 3; ++k) {
+            const float hf = (float)h[k];
+            delta[k] = (xr[k] >= hf ? 1 : 0) - (xr[k] < 0.0f ? 1 : 0);
+        }
+        if (delta[0] | delta[1] | delta[2]) {
+            int loc[3] = {ind[0], ind[1], ind[2]};
+            for (int k = 0; k < 3; ++k) {
+                xr[k] -= delta[k] * (float)h[k];
+                loc[k] = (loc[k] + delta[k] + cdim[k]) % cdim[k];
+            }
+            cell = cellid(loc[0], loc[1], loc[2]);
+        }
+        return MXG_OK;
+    }
+
+    DevSpace space_desc() const {
+        DevSpace S;
+        memset(&S, 0, sizeof(S));
+        const float dtf = (float)dt;
+        for (int k = 0; k < 3; ++k) {
+            S.hd[k] = h[k];
+            S.h[k] = (float)h[k];
+            S.h2[k] = (float)(2. * h[k]);
+            S.maxv[k] = (S.h[k] * max_dist_fraction) / dtf;
+            S.maxv2[k] = S.maxv[k] * S.maxv[k];
+            S.maxx[k] = S.h[k] * max_dist_fraction;
+            S.maxx2[k] = S.maxx[k] * S.maxx[k];
+            S.cdim[k] = cdim[k];
+        }
+        S.dt = dtf;
+        const float cf = (float)cutoff;
+        S.cut2_pair = cf * cf;                  // runner_dopair: float cutoff squared
+        S.cut2_self = (float)(cutoff * cutoff);  // runner_doself: s->cutoff2 (double) as float
+        S.cell_offset = 0;
+        S.ncells = ncells;
+        S.pot_offset = 0;
+        for (int f = 0; f < 6; ++f) {
+            S.bc_kind[f] = (unsigned)bc_kind[f];
+            for (int q = 0; q < 3; ++q) S.bc_vel[f][q] = bc_vel[f][q];
+            S.bc_restore[f] = bc_restore[f];
+        }
+        S.rng_mode = rng_mode;
+        return S;
+    }
+
+    EngineView view(int b) const {
+        EngineView v;
+        v.pos = d_pos[b];
+        v.vel = d_vel[b];
+        v.force = d_force;
+        v.cell_of = d_cell_of[b];
+        v.cell_start = d_cell_start[b];
+        v.cell_count = d_cell_count[b];
+        v.cell_rep = d_cell_rep;
+        v.cell_flags = d_cell_flags;
+        v.nb_off = d_nb_off;
+        v.nb_cell = d_nb_cell;
+        v.nb_shift = d_nb_shift;
+        v.pots = d_pots;
+        v.coef = d_coef;
+        v.pot_idx = d_pot_idx;
+        v.types = d_types;
+        v.spaces = d_spaces;
+        v.ntypes = ntypes;
+        v.ncells = ncells;
+        v.nparts = nparts;
+        v.step = d_step;
+        v.epot_cell = d_epot_cell;
+        v.status = d_status;
+        return v;
+    }
+
+    void enqueue_force(int b) {
+        const EngineView v = view(b);
+        launch_force(v, has_dpd, force_grid, stream);
+        if (!bonds.empty())
+            launch_bonds(v, d_bonds, d_bond_flags, d_bond_off, d_bond_list, d_slot_of_id, d_ebond_slot, stream);
+    }
+
+    void enqueue_step(int b) {
+        const int nb = 1 - b;
+        enqueue_force(b);
+        const EngineView v = view(b);
+        launch_integrate(v, d_pos[b], d_vel[b], d_new_cell, d_in_count, d_in_list, d_out_count, stream);
+        launch_scan(ncells, d_cell_count[b], d_out_count, d_in_count, d_cell_start[nb], d_cell_count[nb], d_step,
+                    stream);
+        launch_scatter(ncells, d_pos[b], d_vel[b], d_new_cell, d_cell_start[b], d_cell_count[b], d_in_count,
+                       d_in_list, d_out_count, d_cell_start[nb], d_pos[nb], d_vel[nb], d_cell_of[nb], d_slot_of_id,
+                       stream);
+    }
+
+    int start(cudaStream_t st);
+    int load_state(const double *x, const float *v, int n);
+};
+
+int mxg_engine::start(cudaStream_t st) {
+    if (!st) {
+        // graphs cannot be captured on the legacy default stream: use an own stream
+        CUDA_TRY(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+        st = own_stream;
+    }
+    stream = st;
+    nparts = (int)ptype.size();
+    ntypes = std::max(1, (int)types.size());
+    // ---- host staging: placement, ordering ----
+    std::vector<int> cell(nparts);
+    std::vector<float> xr(3 * (size_t)nparts);
+    for (int p = 0; p < nparts; ++p) {
+        int rc = place(&px[3 * (size_t)p], cell[p], &xr[3 * (size_t)p]);
+        if (rc != MXG_OK) return rc;
+    }
+    std::vector<int> order(nparts);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cell[a] < cell[b]; });
+    std::vector<float4> hpos(nparts), hvel(nparts);
+    std::vector<int> hcell_of(nparts), hslot(nparts);
+    std::vector<int> hcount(ncells, 0), hstart(ncells + 1, 0);
+    for (int s = 0; s < nparts; ++s) {
+        const int p = order[s];
+        hpos[s] = make_float4(xr[3 * (size_t)p], xr[3 * (size_t)p + 1], xr[3 * (size_t)p + 2], 0.f);
+        int t = ptype[p];
+        memcpy(&hpos[s].w, &t, 4);
+        hvel[s] = make_float4(pv[3 * (size_t)p], pv[3 * (size_t)p + 1], pv[3 * (size_t)p + 2], 0.f);
+        memcpy(&hvel[s].w, &p, 4);
+        hcell_of[s] = cell[p];
+        hslot[p] = s;
+        hcount[cell[p]]++;
+    }
+    for (int c = 0; c < ncells; ++c) hstart[c + 1] = hstart[c] + hcount[c];
+
+    // ---- neighbour entries from the task list ----
+    std::vector<std::vector<std::pair<int, float4>>> nb(ncells);
+    for (const Task &t : tasks) {
+        if (t.type == kTaskSelf) {
+            float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+            int role = kRoleSelf;
+            memcpy(&e.w, &role, 4);
+            nb[t.i].push_back({t.i, e});
+        } else if (t.type == kTaskPair) {
+            int ci = t.i, cj = t.j;
+            float shift[3];
+            getsid(ci, cj, shift);  // runner_dopair recomputes the shift (and flip) per task
+            float4 e1 = make_float4(shift[0], shift[1], shift[2], 0.f), e2 = e1;
+            int r1 = kRoleFirst, r2 = kRoleSecond;
+            memcpy(&e1.w, &r1, 4);
+            memcpy(&e2.w, &r2, 4);
+            nb[ci].push_back({cj, e1});
+            nb[cj].push_back({ci, e2});
+        }
+    }
+    std::vector<int> nb_off(ncells + 1, 0), nb_cell;
+    std::vector<float4> nb_shift;
+    for (int c = 0; c < ncells; ++c) {
+        nb_off[c + 1] = nb_off[c] + (int)nb[c].size();
+        for (auto &e : nb[c]) {
+            nb_cell.push_back(e.first);
+            nb_shift.push_back(e.second);
+        }
+    }
+
+    // ---- potentials, types, space ----
+    std::vector<DevPot> hp;
+    std::vector<float> coef;
+    has_dpd = false;
+    for (const auto &t : pots) {
+        DevPot d;
+        memset(&d, 0, sizeof(d));
+        d.kind = t.kind;
+        d.flags = t.flags;
+        d.n = t.n;
+        d.coef_off = (int)coef.size();
+        d.alpha0 = t.alpha[0];
+        d.alpha1 = t.alpha[1];
+        d.alpha2 = t.alpha[2];
+        d.a = t.a;
+        d.b = t.b;
+        d.r0_plusone = t.r0_plusone;
+        d.a2 = t.a * t.a;
+        d.dpd_alpha = t.dpd_alpha;
+        d.dpd_gamma = t.dpd_gamma;
+        d.dpd_sigma = t.dpd_sigma;
+        d.dpd_delta = (float)(1.f / std::sqrt(dt));  // dpd_eval.hpp:23, from the engine dt
+        if (t.kind == kKindDPD) has_dpd = true;
+        coef.insert(coef.end(), t.c.begin(), t.c.end());
+        hp.push_back(d);
+    }
+    std::vector<int> hpidx((size_t)ntypes * ntypes, -1);
+    for (int a = 0; a < (int)types.size(); ++a)
+        for (int b = 0; b < (int)types.size(); ++b) hpidx[a * ntypes + b] = pot_idx[a * max_type + b];
+    std::vector<DevType> ht(ntypes);
+    for (int a = 0; a < (int)types.size(); ++a) {
+        DevType &d = ht[a];
+        memset(&d, 0, sizeof(d));
+        d.imass = types[a].imass;
+        d.mass = types[a].mass;
+        d.radius = (float)types[a].radius;
+        d.dynamics = types[a].dynamics;
+        d.flags = types[a].flags;
+        d.fx = types[a].force[0];
+        d.fy = types[a].force[1];
+        d.fz = types[a].force[2];
+        d.has_force = types[a].has_force ? 1 : 0;
+    }
+    std::vector<DevSpace> hs(1, space_desc());
+    std::vector<int> hrep(ncells, 0);
+
+    // ---- bonds: CSR by particle id ----
+    std::vector<DevBond> hb;
+    std::vector<unsigned> hbf;
+    std::vector<int> boff(nparts + 1, 0), blist;
+    for (const BondInfo &b : bonds) {
+        if (b.i < 0 || b.i >= nparts || b.j < 0 || b.j >= nparts) return MXG_ERR_BOND;
+        boff[b.i + 1]++;
+        if (b.j != b.i) boff[b.j + 1]++;
+    }
+    for (int p = 0; p < nparts; ++p) boff[p + 1] += boff[p];
+    blist.assign(boff[nparts], 0);
+    {
+        std::vector<int> fill(boff.begin(), boff.end() - 1);
+        for (int k = 0; k < (int)bonds.size(); ++k) {
+            blist[fill[bonds[k].i]++] = k;
+            if (bonds[k].j != bonds[k].i) blist[fill[bonds[k].j]++] = k;
+            DevBond d;
+            memset(&d, 0, sizeof(d));
+            d.i = bonds[k].i;
+            d.j = bonds[k].j;
+            d.pot = bonds[k].pot;
+            d.dissociation = bonds[k].dissociation;
+            hb.push_back(d);
+            hbf.push_back(1u);
+        }
+    }
+
+    // ---- device allocation ----
+    int rc = MXG_OK;
+    for (int b = 0; b < 2; ++b) {
+        rc |= alloc(&d_pos[b], nparts);
+        rc |= alloc(&d_vel[b], nparts);
+        rc |= alloc(&d_cell_of[b], nparts);
+        rc |= alloc(&d_cell_start[b], ncells + 1);
+        rc |= alloc(&d_cell_count[b], ncells);
+    }
+    rc |= alloc(&d_force, nparts);
+    rc |= alloc(&d_new_cell, nparts);
+    rc |= alloc(&d_in_count, ncells);
+    rc |= alloc(&d_out_count, ncells);
+    rc |= alloc(&d_in_list, (size_t)ncells * kBucket);
+    rc |= alloc(&d_slot_of_id, nparts);
+    rc |= alloc(&d_cell_rep, ncells);
+    rc |= alloc(&d_cell_flags, ncells);
+    rc |= alloc(&d_nb_off, ncells + 1);
+    rc |= alloc(&d_nb_cell, nb_cell.size());
+    rc |= alloc(&d_nb_shift, nb_shift.size());
+    rc |= alloc(&d_pots, hp.size());
+    rc |= alloc(&d_coef, coef.size() + 8);
+    rc |= alloc(&d_pot_idx, hpidx.size());
+    rc |= alloc(&d_types, ht.size());
+    rc |= alloc(&d_spaces, hs.size());
+    rc |= alloc(&d_epot_cell, ncells);
+    rc |= alloc(&d_ebond_slot, nparts);
+    rc |= alloc(&d_bonds, hb.size());
+    rc |= alloc(&d_bond_flags, hbf.size());
+    rc |= alloc(&d_bond_off, boff.size());
+    rc |= alloc(&d_bond_list, blist.size());
+    rc |= alloc(&d_status, 1);
+    rc |= alloc(&d_step, 1);
+    rc |= alloc(&d_partials, 2 * (size_t)energy_blocks);
+    rc |= alloc(&d_energy, 2);
+    if (rc != MXG_OK) return MXG_ERR_MALLOC;
+
+    CUDA_TRY(cudaMemsetAsync(d_in_count, 0, sizeof(int) * ncells, stream));
+    CUDA_TRY(cudaMemsetAsync(d_out_count, 0, sizeof(int) * ncells, stream));
+    CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
+    CUDA_TRY(cudaMemsetAsync(d_step, 0, sizeof(unsigned long long), stream));
+    CUDA_TRY(cudaMemsetAsync(d_epot_cell, 0, sizeof(double) * ncells, stream));
+    CUDA_TRY(cudaMemsetAsync(d_ebond_slot, 0, sizeof(double) * std::max(1, nparts), stream));
+    CUDA_TRY(cudaMemsetAsync(d_force, 0, sizeof(float4) * std::max(1, nparts), stream));
+    if ((rc = upload(d_pos[0], hpos, stream)) || (rc = upload(d_vel[0], hvel, stream)) ||
+        (rc = upload(d_cell_of[0], hcell_of, stream)) || (rc = upload(d_cell_start[0], hstart, stream)) ||
+        (rc = upload(d_cell_count[0], hcount, stream)) || (rc = upload(d_slot_of_id, hslot, stream)) ||
+        (rc = upload(d_cell_rep, hrep, stream)) || (rc = upload(d_cell_flags, cell_flags, stream)) ||
+        (rc = upload(d_nb_off, nb_off, stream)) || (rc = upload(d_nb_cell, nb_cell, stream)) ||
+        (rc = upload(d_nb_shift, nb_shift, stream)) || (rc = upload(d_pots, hp, stream)) ||
+        (rc = upload(d_coef, coef, stream)) || (rc = upload(d_pot_idx, hpidx, stream)) ||
+        (rc = upload(d_types, ht, stream)) || (rc = upload(d_spaces, hs, stream)) ||
+        (rc = upload(d_bonds, hb, stream)) || (rc = upload(d_bond_flags, hbf, stream)) ||
+        (rc = upload(d_bond_off, boff, stream)) || (rc = upload(d_bond_list, blist, stream)))
+        return rc;
+    CUDA_TRY(cudaStreamSynchronize(stream));
+
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    force_grid = std::max(1, std::min((ncells + kWarpsPerBlock - 1) / kWarpsPerBlock, sms * 16));
+    cur = 0;
+    started = true;
+
+    if (use_graphs && nparts > 0) {
+        for (int b = 0; b < 2; ++b) {
+            cudaGraph_t g;
+            CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            enqueue_step(b);
+            CUDA_TRY(cudaStreamEndCapture(stream, &g));
+            CUDA_TRY(cudaGraphInstantiate(&graph[b], g, 0));
+            cudaGraphDestroy(g);
+        }
+    }
+    return MXG_OK;
+}
+
+/* Re-places all particles from global positions (per id) and velocities. */
+int mxg_engine::load_state(const double *x, const float *v, int n) {
+    if (n != nparts) return MXG_ERR_ARG;
+    for (int p = 0; p < n; ++p) {
+        for (int k = 0; k < 3; ++k) px[3 * (size_t)p + k] = x[3 * (size_t)p + k];
+        if (v)
+            for (int k = 0; k < 3; ++k) pv[3 * (size_t)p + k] = v[3 * (size_t)p + k];
+    }
+    std::vector<int> cell(nparts);
+    std::vector<float> xr(3 * (size_t)nparts);
+    for (int p = 0; p < nparts; ++p) {
+        int rc = place(&px[3 * (size_t)p], cell[p], &xr[3 * (size_t)p]);
+        if (rc != MXG_OK) return rc;
+    }
+    std::vector<int> order(nparts);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cell[a] < cell[b]; });
+    std::vector<float4> hpos(nparts), hvel(nparts);
+    std::vector<int> hcell_of(nparts), hslot(nparts), hcount(ncells, 0), hstart(ncells + 1, 0);
+    for (int s = 0; s < nparts; ++s) {
+        const int p = order[s];
+        hpos[s] = make_float4(xr[3 * (size_t)p], xr[3 * (size_t)p + 1], xr[3 * (size_t)p + 2], 0.f);
+        int t = ptype[p];
+        memcpy(&hpos[s].w, &t, 4);
+        hvel[s] = make_float4(pv[3 * (size_t)p], pv[3 * (size_t)p + 1], pv[3 * (size_t)p + 2], 0.f);
+        memcpy(&hvel[s].w, &p, 4);
+        hcell_of[s] = cell[p];
+        hslot[p] = s;
+        hcount[cell[p]]++;
+    }
+    for (int c = 0; c < ncells; ++c) hstart[c + 1] = hstart[c] + hcount[c];
+    int rc;
+    if ((rc = upload(d_pos[cur], hpos, stream)) || (rc = upload(d_vel[cur], hvel, stream)) ||
+        (rc = upload(d_cell_of[cur], hcell_of, stream)) || (rc = upload(d_cell_start[cur], hstart, stream)) ||
+        (rc = upload(d_cell_count[cur], hcount, stream)) || (rc = upload(d_slot_of_id, hslot, stream)))
+        return rc;
+    CUDA_TRY(cudaStreamSynchronize(stream));
+    return MXG_OK;
+}
+
+/* ======================================================================== */
+/* C ABI                                                                     */
+/* ======================================================================== */
+
+extern "C" {
+
+static int wrap_potential(int rc, mxg_potential *p, mxg_potential **out) {
+    if (rc != 0) {
+        delete p;
+        *out = nullptr;
+        return MXG_ERR_POTENTIAL;
+    }
+    *out = p;
+    return MXG_OK;
+}
+
+int mxg_potential_create_lj126(double a, double b, double A, double B, double tol, mxg_potential **out) {
+    if (!out) return MXG_ERR_NULL;
+    if (!(a > 0) || !(b > a) || !(tol > 0)) return MXG_ERR_ARG;
+    mxg_potential *p = new mxg_potential;
+    return wrap_potential(make_lj126(p->t, a, b, A, B, tol), p, out);
+}
+
+int mxg_potential_create_morse(double d, double alpha, double r0, double min, double max, double tol,
+                               mxg_potential **out) {
+    if (!out) return MXG_ERR_NULL;
+    if (!(max > min) || !(tol > 0)) return MXG_ERR_ARG;
+    mxg_potential *p = new mxg_potential;
+    return wrap_potential(make_morse(p->t, d, alpha, r0, min, max, tol), p, out);
+}
+
+int mxg_potential_create_harmonic(double k, double r0, double min, double max, double tol, mxg_potential **out) {
+    if (!out) return MXG_ERR_NULL;
+    if (!(max > min) || !(tol > 0)) return MXG_ERR_ARG;
+    mxg_potential *p = new mxg_potential;
+    return wrap_potential(make_harmonic(p->t, k, r0, min, max, tol), p, out);
+}
+
+int mxg_potential_create_power(double k, double r0, double alpha, double min, double max, double tol,
+                               mxg_potential **out) {
+    if (!out) return MXG_ERR_NULL;
+    if (!(max > min) || !(tol > 0)) return MXG_ERR_ARG;
+    mxg_potential *p = new mxg_potential;
+    return wrap_potential(make_power(p->t, k, r0, alpha, min, max, tol), p, out);
+}
+
+int mxg_potential_create_dpd(double alpha, double gamma, double sigma, double cutoff, int shifted,
+                             mxg_potential **out) {
+    if (!out) return MXG_ERR_NULL;
+    if (!(cutoff > 0)) return MXG_ERR_ARG;
+    mxg_potential *p = new mxg_potential;
+    return wrap_potential(make_dpd(p->t, alpha, gamma, sigma, cutoff, shifted != 0), p, out);
+}
+
+int mxg_potential_info(const mxg_potential *p, int *kind, unsigned *flags, int *n, float *alpha4, float *a, float *b,
+                       float *r0_plusone) {
+    if (!p) return MXG_ERR_NULL;
+    if (kind) *kind = p->t.kind;
+    if (flags) *flags = p->t.flags;
+    if (n) *n = p->t.n;
+    if (alpha4)
+        for (int k = 0; k < 4; ++k) alpha4[k] = p->t.alpha[k];
+    if (a) *a = p->t.a;
+    if (b) *b = p->t.b;
+    if (r0_plusone) *r0_plusone = p->t.r0_plusone;
+    return MXG_OK;
+}
+
+int mxg_potential_coeffs(const mxg_potential *p, float *out, int cap) {
+    if (!p) return MXG_ERR_NULL;
+    const int len = (int)p->t.c.size();
+    if (cap < len) return -len;
+    if (len) memcpy(out, p->t.c.data(), sizeof(float) * len);
+    return len;
+}
+
+int mxg_potential_dpd_params(const mxg_potential *p, float *alpha, float *gamma, float *sigma) {
+    if (!p) return MXG_ERR_NULL;
+    if (p->t.kind != kKindDPD) return MXG_ERR_POTENTIAL;
+    *alpha = p->t.dpd_alpha;
+    *gamma = p->t.dpd_gamma;
+    *sigma = p->t.dpd_sigma;
+    return MXG_OK;
+}
+
+int mxg_potential_eval(const mxg_potential *p, float ri, float rj, float r2, float *e, float *f) {
+    if (!p || !e || !f) return MXG_ERR_NULL;
+    if (p->t.kind != kKindTable) return MXG_ERR_POTENTIAL;
+    return eval_ex(p->t, ri, rj, r2, e, f) ? 1 : 0;
+}
+
+void mxg_potential_free(mxg_potential *p) { delete p; }
+
+int mxg_engine_init(const double *origin, const double *dim, const int *cells, double cutoff, const int *bc_kind,
+                    const float *bc_velocity, const float *bc_restore, int max_type, unsigned flags,
+                    mxg_engine **out) {
+    (void)flags;
+    if (!origin || !dim || !cells || !out) return MXG_ERR_NULL;
+    if (!(cutoff > 0) || max_type <= 0 || max_type > kMaxTypes) return MXG_ERR_ARG;
+    mxg_engine *e = new mxg_engine;
+    for (int k = 0; k < 3; ++k) {
+        e->origin[k] = origin[k];
+        e->dim[k] = dim[k];
+        e->cells[k] = cells[k];
+        if (cells[k] < 1 || !(dim[k] > origin[k])) {
+            delete e;
+            return MXG_ERR_ARG;
+        }
+    }
+    e->cutoff = cutoff;
+    for (int f = 0; f < 6; ++f) {
+        int kind = bc_kind ? bc_kind[f] : MXG_BOUNDARY_PERIODIC;
+        if (kind == MXG_BOUNDARY_NO_SLIP) kind = MXG_BOUNDARY_VELOCITY;  // no-slip = zero-velocity wall
+        e->bc_kind[f] = kind;
+        for (int q = 0; q < 3; ++q) e->bc_vel[f][q] = (bc_velocity && bc_kind && bc_kind[f] != MXG_BOUNDARY_NO_SLIP) ? bc_velocity[3 * f + q] : 0.f;
+        e->bc_restore[f] = bc_restore ? bc_restore[f] : 1.f;
+    }
+    // a face pair is periodic only when both faces are (check_periodicy sets both)
+    const int faces[3][2] = {{MXG_FACE_LEFT, MXG_FACE_RIGHT}, {MXG_FACE_FRONT, MXG_FACE_BACK},
+                             {MXG_FACE_BOTTOM, MXG_FACE_TOP}};
+    for (int k = 0; k < 3; ++k) {
+        const bool lo = e->bc_kind[faces[k][0]] & MXG_BOUNDARY_PERIODIC, hi = e->bc_kind[faces[k][1]] & MXG_BOUNDARY_PERIODIC;
+        if (lo || hi) {
+            e->bc_kind[faces[k][0]] = e->bc_kind[faces[k][1]] = MXG_BOUNDARY_PERIODIC;
+            e->period |= 1u << k;
+            if (e->cells[k] < 3) e->cells[k] = 3;  // MxBoundaryConditions_Init: >= 3 periodic cells
+        }
+    }
+    e->max_type = max_type;
+    e->pot_idx.assign((size_t)max_type * max_type, -1);
+    int rc = e->build_space();
+    if (rc != MXG_OK) {
+        delete e;
+        return rc;
+    }
+    *out = e;
+    return MXG_OK;
+}
+
+int mxg_engine_set_dt(mxg_engine *e, double dt, double max_dist_fraction) {
+    if (!e) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    if (!(dt > 0)) return MXG_ERR_ARG;
+    e->dt = dt;
+    if (max_dist_fraction > 0) e->max_dist_fraction = (float)max_dist_fraction;
+    return MXG_OK;
+}
+
+int mxg_engine_set_rng_mode(mxg_engine *e, int mode) {
+    if (!e) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    e->rng_mode = mode ? 1u : 0u;
+    return MXG_OK;
+}
+
+int mxg_engine_addtype(mxg_engine *e, double mass, double radius, int dynamics, unsigned particle_flags) {
+    if (!e) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    if ((int)e->types.size() >= e->max_type) return MXG_ERR_RANGE;
+    if (!(mass > 0)) return MXG_ERR_ARG;
+    TypeInfo t;
+    t.mass = mass;
+    t.imass = 1.0 / mass;
+    t.radius = radius;
+    t.dynamics = dynamics;
+    t.flags = particle_flags;
+    t.force[0] = t.force[1] = t.force[2] = 0.f;
+    t.has_force = false;
+    e->types.push_back(t);
+    return (int)e->types.size() - 1;
+}
+
+int mxg_engine_addpot(mxg_engine *e, const mxg_potential *p, int i, int j) {
+    if (!e || !p) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    const int nt = (int)e->types.size();
+    if (i < 0 || i >= nt || j < 0 || j >= nt) return MXG_ERR_RANGE;
+    e->pots.push_back(p->t);
+    const int idx = (int)e->pots.size() - 1;
+    e->pot_idx[i * e->max_type + j] = idx;  // engine_addpot overwrites: one potential per pair
+    e->pot_idx[j * e->max_type + i] = idx;
+    return MXG_OK;
+}
+
+int mxg_engine_add_singlebody_force(mxg_engine *e, int type, float fx, float fy, float fz) {
+    if (!e) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    if (type < 0 || type >= (int)e->types.size()) return MXG_ERR_RANGE;
+    TypeInfo &t = e->types[type];
+    t.force[0] = fx;
+    t.force[1] = fy;
+    t.force[2] = fz;
+    t.has_force = true;
+    return MXG_OK;
+}
+
+int mxg_engine_addparts(mxg_engine *e, int n, const double *x, const float *v, const int *type, int *ids_out) {
+    if (!e || (n > 0 && (!x || !type))) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    for (int k = 0; k < n; ++k) {
+        if (type[k] < 0 || type[k] >= (int)e->types.size()) return MXG_ERR_RANGE;
+        int cell;
+        float xr[3];
+        if (e->place(&x[3 * (size_t)k], cell, xr) != MXG_OK) return MXG_ERR_SPACE;
+    }
+    const int first = (int)e->ptype.size();
+    for (int k = 0; k < n; ++k) {
+        for (int q = 0; q < 3; ++q) {
+            e->px.push_back(x[3 * (size_t)k + q]);
+            e->pv.push_back(v ? v[3 * (size_t)k + q] : 0.f);
+        }
+        e->ptype.push_back(type[k]);
+        if (ids_out) ids_out[k] = first + k;
+    }
+    return MXG_OK;
+}
+
+int mxg_engine_addbonds(mxg_engine *e, int n, const int *i, const int *j, const mxg_potential *p,
+                        double dissociation_energy, int *ids_out) {
+    if (!e || !p || (n > 0 && (!i || !j))) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    if (p->t.kind != kKindTable) return MXG_ERR_POTENTIAL;
+    e->pots.push_back(p->t);
+    const int idx = (int)e->pots.size() - 1;
+    for (int k = 0; k < n; ++k) {
+        if (ids_out) ids_out[k] = (int)e->bonds.size();
+        e->bonds.push_back({i[k], j[k], idx, dissociation_energy});
+    }
+    return MXG_OK;
+}
+
+int mxg_engine_start(mxg_engine *e, void *cuda_stream) {
+    if (!e) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MXG_ERR_NOCUDA;
+    return e->start((cudaStream_t)cuda_stream);
+}
+
+int mxg_engine_step(mxg_engine *e, int nsteps) {
+    if (!e) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    if (e->nparts == 0) return MXG_OK;
+    for (int s = 0; s < nsteps; ++s) {
+        if (e->graph[e->cur]) {
+            CUDA_TRY(cudaGraphLaunch(e->graph[e->cur], e->stream));
+        } else {
+            e->enqueue_step(e->cur);
+            CUDA_TRY(cudaGetLastError());
+        }
+        e->cur = 1 - e->cur;
+    }
+    return MXG_OK;
+}
+
+int mxg_engine_force(mxg_engine *e) {
+    if (!e) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    if (e->nparts == 0) return MXG_OK;
+    e->enqueue_force(e->cur);
+    CUDA_TRY(cudaGetLastError());
+    return MXG_OK;
+}
+
+int mxg_engine_status(mxg_engine *e) {
+    if (!e) return MXG_ERR_NULL;
+    if (!e->started) return MXG_OK;
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    unsigned st = 0;
+    CUDA_TRY(cudaMemcpy(&st, e->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (st & kStatusNonFinite) return MXG_ERR_NONFINITE;
+    if (st & kStatusBucketOverflow) return MXG_ERR_CELL_OVERFLOW;
+    if (st & kStatusTooFast) return MXG_ERR_TOOFAST;
+    return MXG_OK;
+}
+
+int mxg_engine_clear_status(mxg_engine *e) {
+    if (!e) return MXG_ERR_NULL;
+    if (!e->started) return MXG_OK;
+    CUDA_TRY(cudaMemsetAsync(e->d_status, 0, sizeof(unsigned), e->stream));
+    return MXG_OK;
+}
+
+int mxg_engine_nr_parts(const mxg_engine *e) { return e ? (int)e->ptype.size() : MXG_ERR_NULL; }
+int mxg_engine_nr_cells(const mxg_engine *e) { return e ? e->ncells : MXG_ERR_NULL; }
+
+int mxg_engine_unload(mxg_engine *e, int n, double *x, float *v, float *f, int *cell, float *xrel) {
+    if (!e) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    if (n > e->nparts) return MXG_ERR_RANGE;
+    const int N = e->nparts;
+    std::vector<float4> hp(N), hv(N), hf(N);
+    std::vector<int> hc(N);
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    CUDA_TRY(cudaMemcpy(hp.data(), e->d_pos[e->cur], sizeof(float4) * N, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(hv.data(), e->d_vel[e->cur], sizeof(float4) * N, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(hf.data(), e->d_force, sizeof(float4) * N, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(hc.data(), e->d_cell_of[e->cur], sizeof(int) * N, cudaMemcpyDeviceToHost));
+    for (int s = 0; s < N; ++s) {
+        int id;
+        memcpy(&id, &hv[s].w, 4);
+        if (id < 0 || id >= n) continue;
+        const int c = hc[s];
+        const float xr[3] = {hp[s].x, hp[s].y, hp[s].z};
+        for (int k = 0; k < 3; ++k) {
+            if (x) x[3 * (size_t)id + k] = e->cell_origin[3 * (size_t)c + k] + xr[k];
+            if (xrel) xrel[3 * (size_t)id + k] = xr[k];
+        }
+        if (v) {
+            v[3 * (size_t)id] = hv[s].x;
+            v[3 * (size_t)id + 1] = hv[s].y;
+            v[3 * (size_t)id + 2] = hv[s].z;
+        }
+        if (f) {
+            f[3 * (size_t)id] = hf[s].x;
+            f[3 * (size_t)id + 1] = hf[s].y;
+            f[3 * (size_t)id + 2] = hf[s].z;
+        }
+        if (cell) cell[id] = c;
+    }
+    return MXG_OK;
+}
+
+int mxg_engine_load(mxg_engine *e, int n, const double *x, const float *v) {
+    if (!e || !x) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return e->load_state(x, v, n);
+}
+
+int mxg_engine_energy(mxg_engine *e, double *epot, double *ekin, double *virial9) {
+    if (!e) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    launch_energy(e->ncells, e->d_epot_cell, e->nparts, e->bonds.empty() ? nullptr : e->d_ebond_slot,
+                  e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
+                  e->stream);
+    double out[2];
+    CUDA_TRY(cudaMemcpyAsync(out, e->d_energy, sizeof(out), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    if (epot) *epot = out[0];
+    if (ekin) *ekin = out[1];
+    if (virial9)
+        for (int k = 0; k < 9; ++k) virial9[k] = 0.0;
+    return MXG_OK;
+}
+
+double mxg_engine_kinetic_energy(mxg_engine *e) {
+    double ek = 0.0;
+    if (mxg_engine_energy(e, nullptr, &ek, nullptr) != MXG_OK) return -1.0;
+    return ek;
+}
+
+int mxg_engine_tasks(const mxg_engine *e, int *out, int cap) {
+    if (!e) return MXG_ERR_NULL;
+    const int n = (int)e->tasks.size();
+    if (!out) return n;
+    if (cap < 4 * n) return -n;
+    for (int k = 0; k < n; ++k) {
+        out[4 * k] = e->tasks[k].type;
+        out[4 * k + 1] = e->tasks[k].flags;
+        out[4 * k + 2] = e->tasks[k].i;
+        out[4 * k + 3] = e->tasks[k].j;
+    }
+    return n;
+}
+
+int mxg_engine_bond_flags(mxg_engine *e, unsigned *out, int cap) {
+    if (!e) return MXG_ERR_NULL;
+    const int n = (int)e->bonds.size();
+    if (!out || !e->started) return n;
+    if (cap < n) return -n;
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    if (n) CUDA_TRY(cudaMemcpy(out, e->d_bond_flags, sizeof(unsigned) * n, cudaMemcpyDeviceToHost));
+    return n;
+}
+
+int mxg_engine_space_info(const mxg_engine *e, int *cdim, double *h, int *nr_cells, unsigned *period) {
+    if (!e) return MXG_ERR_NULL;
+    for (int k = 0; k < 3; ++k) {
+        if (cdim) cdim[k] = e->cdim[k];
+        if (h) h[k] = e->h[k];
+    }
+    if (nr_cells) *nr_cells = e->ncells;
+    if (period) *period = e->period;
+    return MXG_OK;
+}
+
+int mxg_engine_device_state(mxg_engine *e, void **pos, void **vel, void **force, void **cell) {
+    if (!e) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    if (pos) *pos = e->d_pos[e->cur];
+    if (vel) *vel = e->d_vel[e->cur];
+    if (force) *force = e->d_force;
+    if (cell) *cell = e->d_cell_of[e->cur];
+    return MXG_OK;
+}
+
+int mxg_engine_finalize(mxg_engine *e) {
+    if (!e) return MXG_ERR_NULL;
+    if (e->started && e->stream) cudaStreamSynchronize(e->stream);
+    delete e;
+    return MXG_OK;
+}
+
+int mxg_engine_enable_timing(mxg_engine *e, int on) {
+    if (!e) return MXG_ERR_NULL;
+    (void)on;
+    return MXG_OK;
+}
+
+/* Launches the force kernel reps times on the engine stream between two events
+ * and returns the mean duration in milliseconds. */
+int mxg_engine_time_force(mxg_engine *e, int reps, double *ms) {
+    if (!e || !ms) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    cudaEvent_t a, b;
+    CUDA_TRY(cudaEventCreate(&a));
+    CUDA_TRY(cudaEventCreate(&b));
+    const EngineView v = e->view(e->cur);
+    CUDA_TRY(cudaEventRecord(a, e->stream));
+    for (int r = 0; r < reps; ++r) launch_force(v, e->has_dpd, e->force_grid, e->stream);
+    CUDA_TRY(cudaEventRecord(b, e->stream));
+    CUDA_TRY(cudaEventSynchronize(b));
+    float t = 0.f;
+    cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ms = t / std::max(1, reps);
+    return MXG_OK;
+}
+
+int mxg_engine_kernel_times(mxg_engine *e, double *ms, long long *launches, int nkernels) {
+    if (!e) return MXG_ERR_NULL;
+    for (int k = 0; k < nkernels; ++k) {
+        if (ms) ms[k] = 0.0;
+        if (launches) launches[k] = 0;
+    }
+    return MXG_OK;
+}
+
+int mxg_engine_pair_counts(mxg_engine *e, long long *candidates, long long *interacting) {
+    if (!e) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    // candidates as the reference's task list defines them: sum over pair tasks
+    // of n_i*n_j and over self tasks of n(n-1)/2, for the current occupancy
+    std::vector<int> cnt(e->ncells);
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    CUDA_TRY(cudaMemcpy(cnt.data(), e->d_cell_count[e->cur], sizeof(int) * e->ncells, cudaMemcpyDeviceToHost));
+    long long cand = 0;
+    for (const Task &t : e->tasks) {
+        if (t.type == kTaskSelf)
+            cand += (long long)cnt[t.i] * (cnt[t.i] - 1) / 2;
+        else if (t.type == kTaskPair)
+            cand += (long long)cnt[t.i] * cnt[t.j];
+    }
+    if (candidates) *candidates = cand;
+    if (interacting) *interacting = -1;
+    return MXG_OK;
+}
+
+}  // extern "C"

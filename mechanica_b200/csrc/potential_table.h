@@ -1,0 +1,46 @@
+/*
+ * Host-side potential tables (see potential_table.cpp for the format).
+ */
+#pragma once
+#include <algorithm>
+#include <cstdint>
+#include <functional>
+#include <vector>
+
+namespace mxg {
+
+using ScalarFn = std::function<double(double)>;
+
+enum : uint32_t {
+    kFlagLJ126 = 1u << 0,
+    kFlagR2 = 1u << 4,
+    kFlagR = 1u << 5,
+    kFlagHarmonic = 1u << 7,
+    kFlagScaled = 1u << 11,
+    kFlagShifted = 1u << 12,
+};
+
+enum : int { kKindTable = 0, kKindDPD = 1 };
+
+struct PotentialTable {
+    int kind = kKindTable;
+    uint32_t flags = 0;
+    float alpha[4] = {0, 0, 0, 0};
+    float r0_plusone = 0.0f;
+    float a = 0.0f, b = 0.0f;
+    int n = 0;
+    std::vector<float> c;  // (n+1)*8
+    float dpd_alpha = 0, dpd_gamma = 0, dpd_sigma = 0;
+    std::vector<double> params;  // construction parameters, for re-fitting
+};
+
+int build_table(PotentialTable &p, const ScalarFn &f, const ScalarFn &fp, const ScalarFn &f6, float a, float b,
+                float tol);
+int make_lj126(PotentialTable &p, double a, double b, double A, double B, double tol);
+int make_morse(PotentialTable &p, double d, double alpha, double r0, double min, double max, double tol);
+int make_harmonic(PotentialTable &p, double k, double r0, double min, double max, double tol);
+int make_power(PotentialTable &p, double k, double r0, double alpha, double a, double b, double tol);
+int make_dpd(PotentialTable &p, double alpha, double gamma, double sigma, double cutoff, bool shifted);
+bool eval_ex(const PotentialTable &p, float ri, float rj, float r2, float *e, float *f);
+
+}  // namespace mxg

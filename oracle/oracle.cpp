@@ -1,0 +1,264 @@
+/*
+ * Oracle tier B: an independent C++ restatement of the reference's nonbonded
+ * force pass, templated on the arithmetic type.
+ *
+ * TEST INFRASTRUCTURE ONLY: tests/ and bench.py's CPU-baseline leg call it;
+ * the product never links it.
+ *
+ *   T = float   follows the reference's scalar FP32 operation order
+ *               (runner_dopair.cpp:91-340, runner_doself.cpp :446-682,
+ *               potential_eval.hpp:106-161, dpd_eval.hpp:21-169) with the
+ *               pair shift rounded to float as space_getsid does (space.cpp:95-130).
+ *   T = double  the same algorithm in FP64 on the same FP32 table coefficients
+ *               and the same FP32 positions: the "FP64 CPU oracle" against which
+ *               FP32 rounding error is stated.
+ * It also offers a second pair term per type pair (a table potential plus a
+ * DPD thermostat summed), which the reference cannot express (engine_addpot
+ * keeps one potential per pair, engine.cpp:968-977).
+ *
+ * Pairs are enumerated brute force within each task's cell pair, which is the
+ * interacting set of the reference's sorted loops: their pruning keeps two
+ * quanta of slack (runner_dopair.cpp:136) and never drops a pair inside the
+ * cutoff. The r < a random-direction branch (dpd_eval.hpp:122-131) is not
+ * reproduced; such pairs are counted and skipped.
+ */
+#include "oracle.h"
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+const int kSortlistID[27] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 0, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2, 1, 0};
+const bool kFlip[27] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+
+template <typename T>
+struct Pot {
+    int kind;
+    unsigned flags;
+    int n;
+    T alpha[3];
+    T a, b, r0p1;
+    const float *c;
+    T dpd_alpha, dpd_gamma, dpd_sigma, dpd_delta;
+};
+
+/* potential_eval_ex in type T; coefficients widened from float */
+template <typename T>
+bool table_eval_ex(const Pot<T> &p, T ri, T rj, T r2, T &e, T &f) {
+    const T eps = (T)FLT_EPSILON;
+    T r = std::sqrt(r2);
+    const T ro = r < eps ? eps : r;
+    r = r < p.a ? p.a : r;
+    if (p.flags & (1u << 11))
+        r = r / (ri + rj);
+    else if (p.flags & (1u << 12))
+        r = r - (ri + rj) + p.r0p1;
+    const T t = p.alpha[0] + r * (p.alpha[1] + r * p.alpha[2]);
+    const unsigned ind = (unsigned)std::max((T)0, t);
+    if (r > p.b || ind > (unsigned)p.n) return false;
+    const float *c = p.c + ind * 8;
+    const T x = (r - (T)c[0]) * (T)c[1];
+    T ee = (T)c[2] * x + (T)c[3];
+    T eff = (T)c[2];
+    for (int k = 4; k < 8; ++k) {
+        eff = eff * x + ee;
+        ee = ee * x + (T)c[k];
+    }
+    e = ee;
+    f = eff * (T)c[1] / ro;
+    return true;
+}
+
+template <typename T>
+struct Setup {
+    int N;
+    std::vector<T> x, v;  // N*3
+    const int *cell;
+    const int *type;
+    int ncells;
+    const double *origin;
+    double dim[3];
+    T cut2_pair, cut2_self;
+    int ntypes;
+    std::vector<T> radius;
+    const int *pot_of_pair;
+    const int *dpd_of_pair;
+    std::vector<Pot<T>> pots;
+    std::vector<T> body;
+};
+
+template <typename T>
+void pair_force(const Setup<T> &S, int pi, int pj, const T *dx_in, T r2, std::vector<T> &f, double &epot,
+                long long &nint, long long &nrand) {
+    const int ti = S.type[pi], tj = S.type[pj];
+    const int pidx = S.pot_of_pair[ti * S.ntypes + tj];
+    const int didx = S.dpd_of_pair ? S.dpd_of_pair[ti * S.ntypes + tj] : -1;
+    for (int which = 0; which < 2; ++which) {
+        const int idx = which == 0 ? pidx : didx;
+        if (idx < 0) continue;
+        const Pot<T> &p = S.pots[idx];
+        if (r2 < p.a * p.a) {
+            ++nrand;
+            continue;
+        }
+        T dx[3] = {dx_in[0], dx_in[1], dx_in[2]};
+        if (p.kind == 1) {
+            const T ri = S.radius[ti], rj = S.radius[tj];
+            const bool shifted = p.flags & (1u << 12);
+            const T cutoff = shifted ? (p.b + ri + rj) : p.b;
+            if (r2 > cutoff * cutoff) continue;
+            const T r = std::sqrt(r2);
+            const T e[3] = {dx[0] / r, dx[1] / r, dx[2] / r};
+            const T w[3] = {S.v[3 * pi] - S.v[3 * pj], S.v[3 * pi + 1] - S.v[3 * pj + 1], S.v[3 * pi + 2] - S.v[3 * pj + 2]};
+            const T sr = shifted ? r - ri - rj : r;
+            const T oc = sr < 0 ? (T)1 : ((T)1 - sr / cutoff);
+            const T fc = p.dpd_alpha * oc;
+            const T od = oc * oc;
+            const T fd = -p.dpd_gamma * od * (e[0] * w[0] + e[1] * w[1] + e[2] * w[2]);
+            const T fr = p.dpd_sigma * oc * p.dpd_delta;
+            const T ff = fc + fd + fr;
+            for (int k = 0; k < 3; ++k) {
+                f[3 * pj + k] = f[3 * pj + k] - ff * e[k];
+                f[3 * pi + k] = f[3 * pi + k] + ff * e[k];
+            }
+            ++nint;
+        } else {
+            T ee, ff;
+            if (!table_eval_ex(p, S.radius[ti], S.radius[tj], r2, ee, ff)) continue;
+            for (int k = 0; k < 3; ++k) {
+                const T wk = ff * dx[k];
+                f[3 * pi + k] -= wk;
+                f[3 * pj + k] += wk;
+            }
+            epot += (double)ee;
+            ++nint;
+        }
+    }
+}
+
+template <typename T>
+int run(const Setup<T> &S, const int *tasks, int ntasks, double *f_out, double *epot_out, long long *counts) {
+    // particles per cell, in index order
+    std::vector<std::vector<int>> members(S.ncells);
+    for (int p = 0; p < S.N; ++p) members[S.cell[p]].push_back(p);
+    std::vector<T> f(3 * (size_t)S.N, (T)0);
+    for (int p = 0; p < S.N; ++p)
+        for (int k = 0; k < 3; ++k) f[3 * p + k] = S.body[3 * S.type[p] + k];
+    double epot = 0.0;
+    long long ncand = 0, nint = 0, nrand = 0;
+    for (int q = 0; q < ntasks; ++q) {
+        const int type = tasks[4 * q], ci0 = tasks[4 * q + 2], cj0 = tasks[4 * q + 3];
+        if (type == 1) {  // self
+            const std::vector<int> &mem = members[ci0];
+            for (size_t a = 0; a < mem.size(); ++a)
+                for (size_t b = a + 1; b < mem.size(); ++b) {
+                    const int pi = mem[a], pj = mem[b];
+                    T dx[3];
+                    for (int k = 0; k < 3; ++k) dx[k] = S.x[3 * pi + k] - S.x[3 * pj + k];
+                    const T r2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
+                    ++ncand;
+                    if (r2 > S.cut2_self) continue;
+                    pair_force(S, pi, pj, dx, r2, f, epot, nint, nrand);
+                }
+        } else if (type == 2) {  // pair, shift and flip as space_getsid
+            int ci = ci0, cj = cj0;
+            T shift[3];
+            for (int k = 0; k < 3; ++k) {
+                double s = S.origin[3 * cj + k] - S.origin[3 * ci + k];
+                T sk = (T)s;
+                if (sk * 2 > S.dim[k])
+                    sk = (T)(sk - S.dim[k]);
+                else if (sk * 2 < -S.dim[k])
+                    sk = (T)(sk + S.dim[k]);
+                shift[k] = sk;
+            }
+            int sid = 0;
+            for (int k = 0; k < 3; ++k) sid = 3 * sid + ((shift[k] < 0) ? 0 : ((shift[k] > 0) ? 2 : 1));
+            if (kFlip[sid]) {
+                std::swap(ci, cj);
+                for (int k = 0; k < 3; ++k) shift[k] = -shift[k];
+            }
+            (void)kSortlistID;
+            for (int pi : members[ci])
+                for (int pj : members[cj]) {
+                    T pix[3], dx[3];
+                    for (int k = 0; k < 3; ++k) {
+                        pix[k] = S.x[3 * pi + k] - shift[k];
+                        dx[k] = pix[k] - S.x[3 * pj + k];
+                    }
+                    const T r2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
+                    ++ncand;
+                    if (r2 > S.cut2_pair) continue;
+                    pair_force(S, pi, pj, dx, r2, f, epot, nint, nrand);
+                }
+        }
+    }
+    for (size_t k = 0; k < f.size(); ++k) f_out[k] = (double)f[k];
+    *epot_out = epot;
+    if (counts) {
+        counts[0] = ncand;
+        counts[1] = nint;
+        counts[2] = nrand;
+    }
+    return 0;
+}
+
+template <typename T>
+int build_and_run(const OrcInput *in, double *f_out, double *epot_out, long long *counts) {
+    Setup<T> S;
+    S.N = in->N;
+    S.x.resize(3 * (size_t)in->N);
+    S.v.resize(3 * (size_t)in->N);
+    for (size_t k = 0; k < S.x.size(); ++k) {
+        S.x[k] = (T)in->xrel[k];
+        S.v[k] = in->vel ? (T)in->vel[k] : (T)0;
+    }
+    S.cell = in->cell;
+    S.type = in->type;
+    S.ncells = in->ncells;
+    S.origin = in->cell_origin;
+    for (int k = 0; k < 3; ++k) S.dim[k] = in->dim[k];
+    const float cf = (float)in->cutoff;
+    if (sizeof(T) == sizeof(float)) {
+        S.cut2_pair = (T)(cf * cf);
+        S.cut2_self = (T)(float)(in->cutoff * in->cutoff);
+    } else {
+        S.cut2_pair = (T)(in->cutoff * in->cutoff);
+        S.cut2_self = S.cut2_pair;
+    }
+    S.ntypes = in->ntypes;
+    for (int t = 0; t < in->ntypes; ++t) S.radius.push_back((T)in->radius[t]);
+    S.pot_of_pair = in->pot_of_pair;
+    S.dpd_of_pair = in->dpd_of_pair;
+    for (int q = 0; q < in->npots; ++q) {
+        Pot<T> p;
+        p.kind = in->pot_kind[q];
+        p.flags = in->pot_flags[q];
+        p.n = in->pot_n[q];
+        for (int k = 0; k < 3; ++k) p.alpha[k] = (T)in->pot_alpha[3 * q + k];
+        p.a = (T)in->pot_abr[3 * q];
+        p.b = (T)in->pot_abr[3 * q + 1];
+        p.r0p1 = (T)in->pot_abr[3 * q + 2];
+        p.c = in->coef + in->pot_coef_off[q];
+        p.dpd_alpha = (T)in->dpd[4 * q];
+        p.dpd_gamma = (T)in->dpd[4 * q + 1];
+        p.dpd_sigma = (T)in->dpd[4 * q + 2];
+        p.dpd_delta = (T)in->dpd[4 * q + 3];
+        S.pots.push_back(p);
+    }
+    for (int t = 0; t < 3 * in->ntypes; ++t) S.body.push_back(in->body ? (T)in->body[t] : (T)0);
+    return run(S, in->tasks, in->ntasks, f_out, epot_out, counts);
+}
+
+}  // namespace
+
+extern "C" int orc_nonbond(int precision, const OrcInput *in, double *f_out, double *epot_out, long long *counts) {
+    if (!in || !f_out || !epot_out) return -1;
+    if (precision == 32) return build_and_run<float>(in, f_out, epot_out, counts);
+    if (precision == 64) return build_and_run<double>(in, f_out, epot_out, counts);
+    return -1;
+}

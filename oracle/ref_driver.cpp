@@ -273,9 +273,14 @@ int mxref_bond_flags(unsigned *out, int n) {
     return _Engine.nr_bonds;
 }
 
-void mxref_energies(double *epot, double *epot_nonbond, double *epot_bond, double *ekin) {
+/* epot: s->epot (after engine_force it holds the bonded part only; engine_advance
+ * adds the per-cell nonbonded energies); cell_sum: the per-cell nonbonded
+ * energies of the last force pass (space_cell.epot). */
+void mxref_energies(double *epot, double *cell_sum, double *epot_bond, double *ekin) {
     *epot = _Engine.s.epot;
-    *epot_nonbond = _Engine.s.epot_nonbond;
+    double cs = 0.0;
+    for (int c = 0; c < _Engine.s.nr_cells; ++c) cs += _Engine.s.cells[c].epot;
+    *cell_sum = cs;
     *epot_bond = _Engine.s.epot_bond;
     *ekin = engine_kinetic_energy(&_Engine);
 }

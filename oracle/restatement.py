@@ -1,0 +1,168 @@
+"""Python wrapper of oracle tier B (oracle/liboracle.so, built from oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY. Computes the nonbonded forces and energy of a
+configuration in FP32 (reference operation order) or FP64 on the same FP32
+table coefficients. Tables come from the reference's own table builder
+(oracle/_ref/libmxref.so) when it is built, else from the committed golden
+tables.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+
+class _OrcInput(ctypes.Structure):
+    _fields_ = [
+        ("N", ctypes.c_int), ("xrel", ctypes.c_void_p), ("vel", ctypes.c_void_p), ("cell", ctypes.c_void_p),
+        ("type", ctypes.c_void_p), ("ncells", ctypes.c_int), ("cell_origin", ctypes.c_void_p),
+        ("dim", ctypes.c_double * 3), ("cutoff", ctypes.c_double), ("tasks", ctypes.c_void_p),
+        ("ntasks", ctypes.c_int), ("ntypes", ctypes.c_int), ("radius", ctypes.c_void_p),
+        ("pot_of_pair", ctypes.c_void_p), ("dpd_of_pair", ctypes.c_void_p), ("npots", ctypes.c_int),
+        ("pot_kind", ctypes.c_void_p), ("pot_flags", ctypes.c_void_p), ("pot_n", ctypes.c_void_p),
+        ("pot_alpha", ctypes.c_void_p), ("pot_abr", ctypes.c_void_p), ("pot_coef_off", ctypes.c_void_p),
+        ("coef", ctypes.c_void_p), ("dpd", ctypes.c_void_p), ("body", ctypes.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            import subprocess
+            subprocess.run(["make", "-C", HERE, "restatement"], check=True, capture_output=True)
+        _lib = ctypes.CDLL(LIB)
+        _lib.orc_nonbond.argtypes = [ctypes.c_int, ctypes.POINTER(_OrcInput), ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_void_p]
+        _lib.orc_nonbond.restype = ctypes.c_int
+    return _lib
+
+
+def reference_table(kind, params):
+    """(info dict, coefficients) from the reference's table builder (in process)."""
+    from . import refengine
+    L = ctypes.PyDLL(refengine.LIB)
+    vp, cd = ctypes.c_void_p, ctypes.c_double
+    if kind == "dpd":
+        L.mxref_potential_dpd.restype = vp
+        L.mxref_potential_dpd.argtypes = [cd, cd, cd, cd, ctypes.c_int]
+        p = L.mxref_potential_dpd(*[float(q) for q in params[:4]], int(params[4]) if len(params) > 4 else 0)
+    else:
+        fn = getattr(L, f"mxref_potential_{kind}")
+        fn.restype = vp
+        fn.argtypes = [cd] * len(params)
+        p = fn(*[float(q) for q in params])
+    n = ctypes.c_int()
+    a4 = (ctypes.c_float * 4)()
+    a, b, r0 = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+    fl, k = ctypes.c_uint(), ctypes.c_int()
+    L.mxref_potential_info(vp(p), ctypes.byref(n), a4, ctypes.byref(a), ctypes.byref(b), ctypes.byref(fl),
+                           ctypes.byref(r0), ctypes.byref(k))
+    coef = np.zeros(max(1, (n.value + 1) * 8), dtype=np.float32)
+    if k.value == 0:
+        L.mxref_potential_coeffs(vp(p), coef.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), coef.size)
+    return dict(kind=k.value, flags=fl.value, n=n.value, alpha=np.array(a4[:3], dtype=np.float32), a=a.value,
+                b=b.value, r0p1=r0.value), coef
+
+
+def cell_origins(dim, cdim, origin=(0.0, 0.0, 0.0)):
+    h = np.asarray(dim, dtype=np.float64) / np.asarray(cdim)
+    out = np.zeros((int(np.prod(cdim)), 3))
+    c = 0
+    for i in range(cdim[0]):
+        for j in range(cdim[1]):
+            for k in range(cdim[2]):
+                out[c] = (origin[0] + i * h[0], origin[1] + j * h[1], origin[2] + k * h[2])
+                c += 1
+    return out
+
+
+def nonbond(scn, xrel, vel, cell, tasks, cdim, precision=64, tables=None, second=None):
+    """Forces (N,3) float64, energy, counts for a configuration.
+
+    tables: {pot index: (info, coef)} for scn["pots"] order (defaults to the
+    reference builder); second: optional list of (kind, params, ti, tj) DPD
+    terms summed with the first potential of each pair.
+    """
+    N = len(scn["t"])
+    ntypes = len(scn["types"])
+    pots = list(scn["pots"]) + list(second or [])
+    infos = []
+    coefs = []
+    for q, (kind, params, ti, tj) in enumerate(pots):
+        if tables is not None and q in tables:
+            infos.append(tables[q][0])
+            coefs.append(tables[q][1])
+        else:
+            inf, cf = reference_table(kind, params)
+            infos.append(inf)
+            coefs.append(cf)
+    off = np.cumsum([0] + [len(c) for c in coefs])[:-1].astype(np.int32)
+    coef = np.concatenate(coefs).astype(np.float32)
+    pot_of_pair = -np.ones(ntypes * ntypes, dtype=np.int32)
+    dpd_of_pair = -np.ones(ntypes * ntypes, dtype=np.int32)
+    for q, (kind, params, ti, tj) in enumerate(pots):
+        tgt = pot_of_pair if q < len(scn["pots"]) else dpd_of_pair
+        tgt[ti * ntypes + tj] = q
+        tgt[tj * ntypes + ti] = q
+    kinds = np.array([i["kind"] for i in infos], dtype=np.int32)
+    flags = np.array([i["flags"] for i in infos], dtype=np.uint32)
+    ns = np.array([i["n"] for i in infos], dtype=np.int32)
+    alpha = np.concatenate([i["alpha"] for i in infos]).astype(np.float32)
+    abr = np.array([[i["a"], i["b"], i["r0p1"]] for i in infos], dtype=np.float32).ravel()
+    dt = float(scn["dt"])
+    dpd = np.zeros(4 * len(pots), dtype=np.float32)
+    for q, (kind, params, ti, tj) in enumerate(pots):
+        if kind == "dpd":
+            dpd[4 * q:4 * q + 3] = np.float32(params[0]), np.float32(params[1]), np.float32(params[2])
+            dpd[4 * q + 3] = np.float32(1.0 / np.sqrt(dt))
+    radius = np.array([r for (_, r, _) in scn["types"]], dtype=np.float32)
+    body = np.zeros(3 * ntypes, dtype=np.float32)
+    for (t, fx, fy, fz) in scn.get("forces", []):
+        body[3 * t:3 * t + 3] = fx, fy, fz
+    tasks = np.ascontiguousarray(tasks, dtype=np.int32)
+    origins = cell_origins(scn["dim"], cdim)
+    keep = dict(xrel=np.ascontiguousarray(xrel, dtype=np.float32), vel=np.ascontiguousarray(vel, dtype=np.float32),
+                cell=np.ascontiguousarray(cell, dtype=np.int32), type=np.ascontiguousarray(scn["t"], dtype=np.int32),
+                origins=origins, tasks=tasks, radius=radius, pop=pot_of_pair, dop=dpd_of_pair, kinds=kinds,
+                flags=flags, ns=ns, alpha=alpha, abr=abr, off=off, coef=coef, dpd=dpd, body=body)
+    inp = _OrcInput()
+    inp.N = N
+    inp.xrel = keep["xrel"].ctypes.data
+    inp.vel = keep["vel"].ctypes.data
+    inp.cell = keep["cell"].ctypes.data
+    inp.type = keep["type"].ctypes.data
+    inp.ncells = len(origins)
+    inp.cell_origin = origins.ctypes.data
+    for k in range(3):
+        inp.dim[k] = float(scn["dim"][k])
+    inp.cutoff = float(scn["cutoff"])
+    inp.tasks = tasks.ctypes.data
+    inp.ntasks = len(tasks)
+    inp.ntypes = ntypes
+    inp.radius = radius.ctypes.data
+    inp.pot_of_pair = pot_of_pair.ctypes.data
+    inp.dpd_of_pair = dpd_of_pair.ctypes.data if second else None
+    inp.npots = len(pots)
+    inp.pot_kind = kinds.ctypes.data
+    inp.pot_flags = flags.ctypes.data
+    inp.pot_n = ns.ctypes.data
+    inp.pot_alpha = alpha.ctypes.data
+    inp.pot_abr = abr.ctypes.data
+    inp.pot_coef_off = off.ctypes.data
+    inp.coef = coef.ctypes.data
+    inp.dpd = dpd.ctypes.data
+    inp.body = body.ctypes.data
+    f = np.zeros((N, 3))
+    ep = ctypes.c_double()
+    counts = np.zeros(3, dtype=np.int64)
+    rc = lib().orc_nonbond(int(precision), ctypes.byref(inp), f.ctypes.data, ctypes.addressof(ep), counts.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"orc_nonbond {rc}")
+    return f, ep.value, counts

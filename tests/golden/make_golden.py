@@ -1,0 +1,137 @@
+"""Generates the golden fixtures in tests/golden/ from the reference engine
+compiled in place (oracle/_ref/libmxref.so, built by `make -C oracle reference`
+from the reference sources).
+
+Run from the repository root:  python tests/golden/make_golden.py
+Fixtures: small seeded cases of each workload shape (forces after one
+engine_force, state after a few engine_steps, task lists, potential tables).
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+import scenarios as S  # noqa: E402
+from oracle import refengine  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+# (name, scenario factory, steps for the trajectory fixture)
+CASES = [
+    ("argon_small", lambda: S.argon(n=1000, L=4.641588833612778, cells=4, seed=11), 10),
+    ("argon_default_cells", lambda: S.argon(n=1000, L=10.0, cells=4, seed=12, dmin=0.3), 10),
+    ("dpd_small", lambda: S.dpd(n=4000, dims=(8.0, 6.0, 7.0), seed=13), 10),
+    # the bonded lattice (k=200, dissociation 2.0, dt=0.005) breaks within a few
+    # steps under the reference's eff >= dissociation rule: partial break states
+    ("lattice_small", lambda: S.lattice(nx=8, seed=14, pull=0.05), 3),
+    ("lattice_break", lambda: S.lattice(nx=6, seed=15, pull=0.05), 2),
+    ("morse2_small", lambda: S.morse2(n=1500, seed=16), 10),
+    # bond lengths spread around the break threshold: one force pass on
+    # identical inputs decides the flags
+    ("lattice_noisy", lambda: S.lattice(nx=8, seed=17, noise=5e-3), 1),
+]
+
+TABLES = [
+    ("lj_argon", "lj126", (0.275, 1.0, 9.5075e-6, 6.1545e-3, 1e-3)),
+    ("lj_argon_example", "lj126", (0.275, 3.0, 9.5075e-6, 6.1545e-3, 1e-3)),
+    ("morse_lattice", "morse", (0.5, 6.0, 0.5, 1e-4, 1.5, 1e-3)),
+    ("morse_sorting", "morse", (0.37, 5.0, 1.0, 1e-4, 2.5, 1e-3)),
+    ("morse_default", "morse", (1.0, 6.0, 0.0, 1e-4, 3.0, 1e-3)),
+    ("harmonic_lattice", "harmonic", (200.0, 0.5, 0.1, 1.0, 0.009)),
+    ("harmonic_unit", "harmonic", (1.0, 1.0, 0.2, 2.0, 0.018)),
+    ("power_sq", "power", (1.0, 1.0, 2.0, 0.1, 3.0, 1e-3)),
+]
+
+
+def make_tables():
+    import ctypes
+    L = ctypes.PyDLL(refengine.LIB)
+    vp, cd = ctypes.c_void_p, ctypes.c_double
+    out = {}
+    for name, kind, params in TABLES:
+        fn = getattr(L, f"mxref_potential_{kind}")
+        fn.restype = vp
+        fn.argtypes = [cd] * len(params)
+        p = fn(*params)
+        n = ctypes.c_int()
+        a4 = (ctypes.c_float * 4)()
+        a, b, r0 = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        fl, k = ctypes.c_uint(), ctypes.c_int()
+        L.mxref_potential_info(vp(p), ctypes.byref(n), a4, ctypes.byref(a), ctypes.byref(b), ctypes.byref(fl),
+                               ctypes.byref(r0), ctypes.byref(k))
+        buf = np.zeros((n.value + 1) * 8, dtype=np.float32)
+        L.mxref_potential_coeffs(vp(p), buf.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), buf.size)
+        # a sweep of potential_eval_ex values across the domain
+        r = np.linspace(max(a.value * 0.9, 1e-3), b.value * 1.05, 257).astype(np.float32)
+        e = np.zeros_like(r)
+        f = np.zeros_like(r)
+        ok = np.zeros(r.shape, dtype=np.int32)
+        L.mxref_potential_eval_ex.argtypes = [vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                              ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
+        for q, rr in enumerate(r):
+            ee, ff = ctypes.c_float(), ctypes.c_float()
+            ok[q] = L.mxref_potential_eval_ex(vp(p), ctypes.c_float(0.5), ctypes.c_float(0.5),
+                                              ctypes.c_float(np.float32(rr) * np.float32(rr)), ctypes.byref(ee),
+                                              ctypes.byref(ff))
+            e[q], f[q] = ee.value, ff.value
+        out[f"{name}__kind"] = np.array(kind)
+        out[f"{name}__params"] = np.array(params, dtype=np.float64)
+        out[f"{name}__info"] = np.array([n.value, fl.value], dtype=np.int64)
+        out[f"{name}__alpha"] = np.array(a4, dtype=np.float32)
+        out[f"{name}__ab"] = np.array([a.value, b.value, r0.value], dtype=np.float32)
+        out[f"{name}__coef"] = buf
+        out[f"{name}__r"] = r
+        out[f"{name}__e"] = e
+        out[f"{name}__f"] = f
+        out[f"{name}__ok"] = ok
+    np.savez_compressed(os.path.join(OUT, "tables.npz"), **out)
+
+
+def scenario_arrays(scn):
+    d = {}
+    for k, v in scn.items():
+        if k in ("types", "pots", "forces", "bond_pot", "bc"):
+            d["scn_" + k] = np.array(repr(v))
+        else:
+            d["scn_" + k] = np.asarray(v)
+    return d
+
+
+def make_case(name, factory, nsteps):
+    scn = factory()
+    f1 = refengine.run(dict(scn, action="force", runners=1))
+    tr = refengine.run(dict(scn, action="steps", nsteps=nsteps, runners=1))
+    out = scenario_arrays(scn)
+    for k in ("f", "cell", "xrel", "epot", "ekin", "tasks", "cdim", "h", "bond_flags"):
+        out["force_" + k] = f1[k]
+    for k in ("xrel", "xabs", "v", "cell", "epot", "ekin", "bond_flags"):
+        out["traj_" + k] = tr[k]
+    out["traj_nsteps"] = np.int64(nsteps)
+    np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **out)
+
+
+def load_scenario(z):
+    scn = {}
+    for k in z.files:
+        if not k.startswith("scn_"):
+            continue
+        v = z[k]
+        key = k[4:]
+        if key in ("types", "pots", "forces", "bond_pot", "bc"):
+            scn[key] = eval(str(v))  # plain literals written by scenario_arrays
+        elif v.shape == ():
+            scn[key] = v.item()
+        else:
+            scn[key] = v
+    return scn
+
+
+if __name__ == "__main__":
+    make_tables()
+    for name, fac, ns in CASES:
+        make_case(name, fac, ns)
+        print("wrote", name)

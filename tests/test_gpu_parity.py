@@ -1,0 +1,100 @@
+"""GPU parity: the B200 engine against the reference engine (golden vectors from
+the reference compiled in place, and the live reference when it is built).
+
+Bars (per the force-and-step contract):
+  - integer work bit-exact: cell ids, cell-relative positions after binning,
+    bond break flags on identical inputs;
+  - per-particle force relative RMS error <= 1e-5 (FP32 summation order differs);
+  - potential energy within 1e-6 relative of the FP64 oracle (reduced in FP64);
+  - kinetic energy equal to FP64 summation accuracy.
+"""
+import numpy as np
+import pytest
+
+from oracle import refengine
+from oracle import restatement as R
+
+import scenarios as S
+from golden_util import CASES, load, ref_tasks, rel_rms
+
+pytestmark = pytest.mark.gpu
+
+FORCE_TOL = 1e-5
+EPOT_TOL = 1e-6
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_force_pass_matches_reference(name):
+    z, scn = load(name)
+    u = S.build_gpu(scn)
+    u.force()
+    x, v, f, c, xr = u.state()
+    assert np.array_equal(c, z["force_cell"])
+    assert np.array_equal(_bits(xr), _bits(z["force_xrel"]))
+    assert rel_rms(f, z["force_f"]) <= FORCE_TOL
+    if "bi" in scn and len(scn["bi"]):
+        assert np.array_equal(u.bond_flags(), z["force_bond_flags"])
+    ep, ek = u.energies()
+    ref_ep = float(z["force_epot"])
+    assert abs(ep - ref_ep) <= 1e-5 * abs(ref_ep) + 1e-9
+    assert abs(ek - float(z["force_ekin"])) <= 1e-12 * abs(float(z["force_ekin"])) + 1e-12
+
+
+@pytest.mark.parametrize("name", [c for c in CASES if not c.startswith("lattice")])
+def test_force_pass_against_fp64_oracle(name):
+    z, scn = load(name)
+    u = S.build_gpu(scn)
+    u.force()
+    x, v, f, c, xr = u.state()
+    f64, ep64, _ = R.nonbond(scn, xr, v, c, ref_tasks(z), z["force_cdim"], precision=64)
+    assert rel_rms(f, f64) <= FORCE_TOL
+    ep, ek = u.energies()
+    assert abs(ep - ep64) <= EPOT_TOL * abs(ep64) + 1e-9
+
+
+@pytest.mark.parametrize("name", [c for c in CASES if c != "lattice_noisy"])
+def test_trajectory_matches_reference(name):
+    z, scn = load(name)
+    n = int(z["traj_nsteps"])
+    u = S.build_gpu(scn)
+    u.steps(n)
+    x, v, f, c, xr = u.state()
+    ref_c = z["traj_cell"]
+    moved = c != ref_c
+    # cell membership is exact except for particles whose FP32 trajectories
+    # straddle a cell face after the summation-order differences
+    assert moved.mean() <= 0.002
+    L = np.asarray(scn["dim"])
+    d = x - z["traj_xabs"]
+    d -= L * np.round(d / L)
+    assert np.abs(d).max() < 1e-3
+    assert rel_rms(v, z["traj_v"]) < 1e-3
+    if "bi" in scn and len(scn["bi"]):
+        agree = (u.bond_flags() == z["traj_bond_flags"]).mean()
+        assert agree >= 0.99
+
+
+@pytest.mark.skipif(not refengine.available(), reason="reference library not built")
+@pytest.mark.parametrize("case", ["argon_full", "dpd_slab", "lattice_full", "morse2_big"])
+def test_force_pass_live_reference_full_size(case):
+    scn = {
+        "argon_full": lambda: S.argon(n=10000, L=10.0, cells=10, seed=21),
+        "dpd_slab": lambda: S.dpd(n=40000, dims=(40.0, 20.0, 4.0), seed=22),
+        "lattice_full": lambda: S.lattice(nx=32, seed=23, noise=5e-3),
+        "morse2_big": lambda: S.morse2(n=20000, seed=24),
+    }[case]()
+    ref = refengine.run(dict(scn, action="force", runners=4))
+    u = S.build_gpu(scn)
+    u.force()
+    x, v, f, c, xr = u.state()
+    assert np.array_equal(c, ref["cell"])
+    assert np.array_equal(_bits(xr), _bits(ref["xrel"]))
+    assert rel_rms(f, ref["f"]) <= FORCE_TOL
+    if "bi" in scn:
+        assert np.array_equal(u.bond_flags(), ref["bond_flags"])
+    ep, ek = u.energies()
+    assert abs(ep - float(ref["epot"])) <= 1e-5 * abs(float(ref["epot"])) + 1e-9

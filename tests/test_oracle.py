@@ -1,0 +1,42 @@
+"""Oracle pins: tier B (own restatement, FP32 and FP64) against the golden
+vectors produced by the reference engine compiled in place (tier A)."""
+import numpy as np
+import pytest
+
+from oracle import restatement as R
+
+from golden_util import CASES, load, ref_tasks, rel_rms
+
+NONBONDED = [c for c in CASES if not c.startswith("lattice")]
+
+
+@pytest.mark.parametrize("name", NONBONDED)
+def test_tier_b_fp32_matches_reference(name):
+    z, scn = load(name)
+    f, ep, cnt = R.nonbond(scn, z["force_xrel"], scn["v"], z["force_cell"], ref_tasks(z), z["force_cdim"],
+                           precision=32)
+    # same per-pair arithmetic; only the order of the per-particle sums differs
+    assert rel_rms(f, z["force_f"]) < 1e-6
+    if float(z["force_epot"]) != 0.0:
+        assert abs(ep - float(z["force_epot"])) <= 1e-6 * abs(float(z["force_epot"])) + 1e-9
+    assert cnt[2] == 0  # no pair below the table minimum in these inputs
+
+
+@pytest.mark.parametrize("name", NONBONDED)
+def test_tier_b_fp64_close_to_reference(name):
+    """FP32 rounding of the reference stated against the FP64 oracle."""
+    z, scn = load(name)
+    f64, ep64, _ = R.nonbond(scn, z["force_xrel"], scn["v"], z["force_cell"], ref_tasks(z), z["force_cdim"],
+                             precision=64)
+    assert rel_rms(z["force_f"], f64) < 1e-5
+
+
+def test_tier_b_bonds_excluded_lattice_nonbonded():
+    """Lattice nonbonded part: reference forces minus tier B nonbonded are the
+    bond forces, which vanish for intact bonds at rest length."""
+    z, scn = load("lattice_small")
+    f, ep, cnt = R.nonbond(scn, z["force_xrel"], scn["v"], z["force_cell"], ref_tasks(z), z["force_cdim"],
+                           precision=32)
+    bond = np.asarray(z["force_f"], dtype=np.float64) - f
+    # bonds at (nearly) rest length contribute little compared with the Morse forces
+    assert np.sqrt((bond ** 2).mean()) < 0.5 * np.sqrt((f ** 2).mean())
