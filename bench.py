@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Benchmark of the force-and-step path on B200: particle-steps/s.
+
+Default workload (N=1): the DPD fluid with a body force -- 200,000 particles in a
+40x20x20 box, periodic in x/y, no-slip walls in z, DPD a=25, gamma=4.5,
+sigma=3, cutoff 1, constant force 0.02 in +x, dt=0.01 -- seeded synthetic
+positions (uniform) and velocities (Maxwell-Boltzmann, kT=1).
+
+One step = one engine_step: nonbonded forces, integrator, re-binning (four
+kernels replayed from a CUDA graph). value = particles x timed steps / device
+time (per-step CUDA events on the engine stream, L2 flushed between steps with
+a 256 MiB write). e2e = the same metric through the C ABI with host buffers:
+every step uploads the state from pinned host memory, steps, downloads the
+state and the FP64 energies.
+
+--impl reference times the reference's own CPU engine (compiled in place from
+the reference sources, oracle/_ref) on this host's cores for the same workload.
+With torchrun (N > 1) each rank runs an independent replica (weak scaling); the
+reported time is the max over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s (1 B200) plain vs batched/adjoint; force rel-err <=1e-5"
+WORKLOAD = ("DPD fluid with body force: 200,000 particles, 40x20x20 box, periodic x/y, no-slip z; "
+            "DPD a=25 gamma=4.5 sigma=3 rc=1 kT=1; constant force 0.02 +x; FP32, dt=0.01")
+# algorithmic FP32 operations per candidate pair and per interacting DPD pair
+# (counted from the reference's scalar pair loop and dpd_eval)
+F_CAND = 9
+F_INT_DPD = 40
+F_INT_TABLE = 44
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=200000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    return ap.parse_args()
+
+
+def workload(n):
+    from mechanica_b200 import workloads as W
+    scale = (n / 200000.0) ** (1.0 / 3.0)
+    dims = (40.0 * scale, 20.0 * scale, 20.0 * scale) if n != 200000 else (40.0, 20.0, 20.0)
+    return W.dpd(n=n, dims=dims, seed=2)
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", delete=False, suffix=".csv")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, name in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(name)
+            except Exception:
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+def cpu_baseline(scn, seconds):
+    """The reference's own CPU engine on this host, a bounded sample of the workload."""
+    from oracle import refengine
+    if not refengine.available():
+        return None, None
+    cores = os.cpu_count() or 1
+    probe = refengine.run(dict(scn, action="steps", nsteps=2, warmup=1, runners=cores))
+    per = max(float(probe["seconds"]) / 2, 1e-4)
+    nsteps = int(max(3, min(500, seconds / per)))
+    r = refengine.run(dict(scn, action="steps", nsteps=nsteps, warmup=1, runners=cores))
+    n = len(scn["t"])
+    val = n * nsteps / float(r["seconds"])
+    return {"value": val, "unit": "particle-steps/s", "cores": cores, "kind": "reference",
+            "sample": f"{nsteps} engine_step calls of the full {n}-particle workload after 1 warm-up step, "
+                      f"nr_runners = {cores} pthreads (reference engine compiled from its own sources)"}, r
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    scn = workload(args.n)
+    from oracle import refengine
+    if not refengine.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference engine library (oracle/_ref) not built"}))
+        return
+    cores = os.cpu_count() or 1
+    n = len(scn["t"])
+    probe = refengine.run(dict(scn, action="steps", nsteps=1, warmup=0, runners=cores))
+    per = max(float(probe["seconds"]), 1e-4)
+    budget = 120.0
+    steps = int(max(1, min(args.steps, budget / per)))
+    r = refengine.run(dict(scn, action="steps", nsteps=steps, warmup=args.warmup if args.warmup <= 5 else 3,
+                           runners=cores))
+    secs = float(r["seconds"])
+    val = n * steps / secs
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "particle-steps/s", "n_gpus": 0,
+            "steps": steps, "warmup": min(args.warmup, 5), "ms_per_step": 1e3 * secs / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded uniform positions, Maxwell-Boltzmann velocities)",
+            "config": {"workload": WORKLOAD, "steps_requested": args.steps},
+            "cpu_baseline": {"value": val, "unit": "particle-steps/s", "cores": cores, "kind": "reference",
+                             "sample": f"{steps} of {args.steps} requested engine_step calls (bounded to ~{budget:.0f} s), "
+                                       f"nr_runners = {cores}"},
+            "e2e": {"value": val, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+
+    import mechanica_b200 as m
+    from mechanica_b200 import workloads as W
+    from mechanica_b200._native import lib, check
+
+    scn = workload(args.n)
+    n = len(scn["t"])
+    stream = torch.cuda.Stream(device=dev)
+    # build through the public API on our stream
+    bc = {"x": scn["bc"][0], "y": scn["bc"][1], "z": scn["bc"][2]}
+    W.build_gpu(scn)
+    u = m.universe
+    u.stream = stream.cuda_stream
+    u._dirty = True
+    u._ensure()
+    e = u._e
+    L = lib()
+
+    # accuracy on the initial configuration: GPU force pass (the reference leg
+    # below compares it against the reference engine)
+    check(L.mxg_engine_force(e), "force")
+    x0, v0, f_gpu, c0, xr0 = u.state()
+    cand = ctypes.c_longlong()
+    inter = ctypes.c_longlong()
+    check(L.mxg_engine_pair_counts(e, ctypes.byref(cand), ctypes.byref(inter)), "pair_counts")
+
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    # ---- warm-up ----
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            check(L.mxg_engine_step(e, 1), "step")
+    barrier()
+    check(L.mxg_engine_status(e), "warmup status")
+
+    # ---- timed region: device-resident ----
+    K = args.steps
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    clk = Clocks(local)
+    clk.start()
+    barrier()
+    t_wall = time.perf_counter()
+    with torch.cuda.stream(stream):
+        for k in range(K):
+            starts[k].record(stream)
+            L.mxg_engine_step(e, 1)
+            ends[k].record(stream)
+            flush.zero_()
+    barrier()
+    t_wall = time.perf_counter() - t_wall
+    clocks = clk.stop()
+    rc = L.mxg_engine_status(e)
+    if rc < 0:
+        raise RuntimeError(f"engine status {rc} after the timed steps")
+    ms = sum(s.elapsed_time(t) for s, t in zip(starts, ends))
+    if world > 1:
+        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * n * K / (ms / 1e3)
+
+    # ---- e2e through the C ABI with pinned host buffers ----
+    hpos = torch.empty(n * 16, dtype=torch.uint8, pin_memory=True)
+    hvel = torch.empty(n * 16, dtype=torch.uint8, pin_memory=True)
+    hen = torch.zeros(2, dtype=torch.float64, pin_memory=True)
+    pe = ctypes.c_void_p(hpos.data_ptr())
+    ve = ctypes.c_void_p(hvel.data_ptr())
+    ee = ctypes.cast(ctypes.c_void_p(hen.data_ptr()), ctypes.POINTER(ctypes.c_double))
+    check(L.mxg_engine_copy_state(e, pe, ve, 0), "copy_state")
+    Ke = max(1, min(K, 500))
+    s2 = [torch.cuda.Event(enable_timing=True) for _ in range(Ke)]
+    e2 = [torch.cuda.Event(enable_timing=True) for _ in range(Ke)]
+    barrier()
+    with torch.cuda.stream(stream):
+        for k in range(Ke):
+            s2[k].record(stream)
+            L.mxg_engine_copy_state(e, pe, ve, 1)
+            L.mxg_engine_step(e, 1)
+            L.mxg_engine_copy_state(e, pe, ve, 0)
+            L.mxg_engine_energy_async(e, ee)
+            e2[k].record(stream)
+            flush.zero_()
+    barrier()
+    ms_e2e = sum(s.elapsed_time(t) for s, t in zip(s2, e2))
+    if world > 1:
+        tt = torch.tensor([ms_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_e2e = float(tt.item())
+    e2e = world * n * Ke / (ms_e2e / 1e3)
+
+    # ---- roofline of the dominant kernel (nonbonded forces) ----
+    R = 50
+    fs = [torch.cuda.Event(enable_timing=True) for _ in range(R)]
+    fe = [torch.cuda.Event(enable_timing=True) for _ in range(R)]
+    barrier()
+    with torch.cuda.stream(stream):
+        for k in range(R):
+            flush.zero_()
+            fs[k].record(stream)
+            L.mxg_engine_force(e)
+            fe[k].record(stream)
+    barrier()
+    force_ms = sum(a.elapsed_time(b) for a, b in zip(fs, fe)) / R
+    flops = F_CAND * cand.value + F_INT_DPD * inter.value
+    peaks = measured_peaks()
+    sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
+    max_mhz = (peaks or {}).get("sm_max_mhz", 1965.0)
+    fp32_peak = sm_count * 128 * 2 * max_mhz * 1e6 / 1e12  # TFLOP/s, nominal (no measured FP32 figure)
+    achieved = flops / (force_ms / 1e3) / 1e12
+    roofline = {"bound": "fp32", "kernel": "force_kernel (nonbonded cell-pair forces)", "achieved": achieved,
+                "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                "peak_source": f"nominal FP32 pipe: {sm_count} SMs x 128 lanes x 2 x {max_mhz:.0f} MHz "
+                               "(MEASURED_PEAKS.json holds no FP32 figure)",
+                "algorithmic_flops_per_launch": flops, "candidate_pairs": cand.value,
+                "interacting_pairs": inter.value,
+                "flops_per_pair": {"candidate": F_CAND, "interacting_dpd": F_INT_DPD},
+                "force_ms_per_launch": force_ms, "traffic": None}
+
+    # ---- CPU baseline and accuracy (reference engine, rank 0, N=1 only) ----
+    cpu = None
+    accuracy = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import refengine
+            if refengine.available():
+                ref = refengine.run(dict(scn, action="force", runners=os.cpu_count() or 1))
+                d = f_gpu.astype(np.float64) - ref["f"]
+                accuracy = {"force_rel_rms_vs_reference": float(np.sqrt((d ** 2).sum() / (ref["f"].astype(np.float64) ** 2).sum())),
+                            "cells_equal": bool(np.array_equal(c0, ref["cell"])), "tolerance": 1e-5}
+                cpu, _ = cpu_baseline(scn, args.cpu_seconds)
+        except Exception as exc:  # the baseline is reported, not required
+            cpu = {"error": str(exc)[:300]}
+
+    line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded uniform positions, Maxwell-Boltzmann velocities, kT=1)",
+            "config": {"workload": WORKLOAD, "particles_per_gpu": n, "cells": scn["cells"],
+                       "l2": "flushed between steps (256 MiB write outside the per-step CUDA events)",
+                       "rng": "reference DPD random term (xi = 1)", "parallelism": f"replicas x{world}"},
+            "clocks": clocks, "gpu_launches": 4 * K,
+            "e2e": {"value": e2e, "unit": "particle-steps/s", "steps": Ke, "h2d_bytes_per_step": 32 * n,
+                    "d2h_bytes_per_step": 32 * n + 16,
+                    "path": "mxg_engine_copy_state (pinned host -> device), mxg_engine_step, "
+                            "mxg_engine_copy_state (device -> pinned host), mxg_engine_energy_async"},
+            "roofline": roofline, "cpu_baseline": cpu, "accuracy": accuracy,
+            "wall_s_timed_region": t_wall}
+    if rank == 0:
+        print(json.dumps(line))
+    m.universe.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -164,11 +164,26 @@ int mxg_engine_space_info(const mxg_engine *e, int *cdim, double *h, int *nr_cel
 /* Raw device-resident state in slot order (cell-sorted): pos float4 (xrel, type bits),
  * vel float4 (v, id bits), force float4, cell index per slot; device pointers. */
 int mxg_engine_device_state(mxg_engine *e, void **pos, void **vel, void **force, void **cell);
+/* Asynchronous copy of the raw slot-order state (pos, vel float4 arrays of nr_parts entries) between
+ * host memory (pinned for full speed) and the device, ordered on the engine stream. The layout is the
+ * device's own, so a download followed by an upload restores the state exactly. */
+int mxg_engine_copy_state(mxg_engine *e, void *host_pos, void *host_vel, int to_device);
+/* Enqueues the FP64 energy reduction and an asynchronous copy of (epot, ekin) into host_out2. */
+int mxg_engine_energy_async(mxg_engine *e, double *host_out2);
 int mxg_engine_finalize(mxg_engine *e);
 
 /* DPD random term: 0 = reference semantics (xi = 1, dpd_eval.hpp:57), 1 = Philox stream keyed on
  * (step, particle id pair). Set before mxg_engine_start. */
 int mxg_engine_set_rng_mode(mxg_engine *e, int mode);
+/* Pair pruning of cell pairs as the reference's sorted loops do it (runner_dopair.cpp:132-182):
+ * (a) a candidate pair is skipped when the quantised projections of the two particles on the pair's
+ * sort axis, plus the shift length, differ by dmaxdist or more; with cubic cells this never drops a
+ * pair inside the cutoff, with non-cubic cells it does; (b) the whole cell pair is skipped when the
+ * largest key of its first cell and the smallest key of its second give a difference below zero
+ * (unsigned wrap) or above dmaxdist, which happens when particles sit within one key quantum of the
+ * shared face. mode 0 (default): (a) on non-cubic grids, (b) always -- the reference's result;
+ * 1: (a) and (b) on every grid; 2: neither (every pair inside the cutoff). Set before start. */
+int mxg_engine_set_pair_pruning(mxg_engine *e, int mode);
 /* Clears the device status word. */
 int mxg_engine_clear_status(mxg_engine *e);
 /* Launches the nonbonded force kernel reps times back to back on the engine stream and returns the

@@ -296,7 +296,9 @@ class _Universe:
         self._e = None
 
     # ---- configuration ----
-    def _init(self, dim, cells, cutoff, dt, bc, max_distance, origin, rng, max_types):
+    def _init(self, dim, cells, cutoff, dt, bc, max_distance, origin, rng, max_types, stream=None, pair_pruning=0):
+        self.stream = stream
+        self.pair_pruning = pair_pruning
         self.dim = [float(d) for d in dim]
         self.origin = [float(o) for o in origin]
         self.cells = [int(c) for c in cells]
@@ -335,6 +337,7 @@ class _Universe:
             frac = self.max_distance / hh[0]
         check(lib().mxg_engine_set_dt(self._e, self.dt, frac), "set_dt")
         check(lib().mxg_engine_set_rng_mode(self._e, 1 if self.rng == "philox" else 0), "set_rng_mode")
+        check(lib().mxg_engine_set_pair_pruning(self._e, int(self.pair_pruning)), "set_pair_pruning")
         for (m, r, d, fl) in self._types:
             check(lib().mxg_engine_addtype(self._e, m, r, d, fl), "addtype")
         for (p, a, b) in self._pots:
@@ -410,7 +413,8 @@ class _Universe:
             check(lib().mxg_engine_addparts(self._e, n, ptr(f64(self._x), ctypes.c_double),
                                             ptr(f32(self._v), ctypes.c_float), ptr(i32(self._t), ctypes.c_int),
                                             None), "addparts")
-        check(lib().mxg_engine_start(self._e, None), "engine_start")
+        check(lib().mxg_engine_start(self._e, ctypes.c_void_p(self.stream) if self.stream else None),
+              "engine_start")
         self._started = True
         self._dirty = False
 
@@ -534,14 +538,20 @@ def _require():
 
 def init(dim=(10.0, 10.0, 10.0), cutoff=1.0, cells=(4, 4, 4), dt=0.01, bc=None, boundary_conditions=None,
          max_distance=None, origin=(0.0, 0.0, 0.0), integrator=FORWARD_EULER, rng="reference", max_types=64,
-         **ignored):
+         stream=None, pair_pruning=0, **ignored):
     """Initialises the universe (MxSimulator_Init / universe_init). Rendering and
-    windowing arguments of the reference are accepted and ignored."""
+    windowing arguments of the reference are accepted and ignored.
+
+    rng: "reference" keeps the reference's deterministic DPD random term
+    (dpd_eval.hpp:57); "philox" draws it from a counter-based stream.
+    stream: optional CUDA stream handle (int) on which the engine runs.
+    pair_pruning: 0 reproduces the reference's sorted-loop pruning (default),
+    2 evaluates every pair inside the cutoff (see mxg_engine_set_pair_pruning)."""
     if integrator != FORWARD_EULER:
         raise NotImplementedError("only the forward Euler integrator is on this path")
     universe.close()
     universe._init(dim, cells, cutoff, dt, bc if bc is not None else boundary_conditions, max_distance, origin,
-                   rng, max_types)
+                   rng, max_types, stream, pair_pruning)
     return universe
 
 

@@ -67,6 +67,7 @@ _SIGS = {
                          ctypes.c_int, ctypes.c_uint, _vpp], ctypes.c_int),
     "mxg_engine_set_dt": ([_vp, ctypes.c_double, ctypes.c_double], ctypes.c_int),
     "mxg_engine_set_rng_mode": ([_vp, ctypes.c_int], ctypes.c_int),
+    "mxg_engine_set_pair_pruning": ([_vp, ctypes.c_int], ctypes.c_int),
     "mxg_engine_addtype": ([_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_uint], ctypes.c_int),
     "mxg_engine_addpot": ([_vp, _vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "mxg_engine_add_singlebody_force": ([_vp, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float],
@@ -89,6 +90,8 @@ _SIGS = {
     "mxg_engine_bond_flags": ([_vp, _c_uint_p, ctypes.c_int], ctypes.c_int),
     "mxg_engine_space_info": ([_vp, _c_int_p, _c_double_p, _c_int_p, _c_uint_p], ctypes.c_int),
     "mxg_engine_device_state": ([_vp, _vpp, _vpp, _vpp, _vpp], ctypes.c_int),
+    "mxg_engine_copy_state": ([_vp, _vp, _vp, ctypes.c_int], ctypes.c_int),
+    "mxg_engine_energy_async": ([_vp, _c_double_p], ctypes.c_int),
     "mxg_engine_finalize": ([_vp], ctypes.c_int),
     "mxg_engine_enable_timing": ([_vp, ctypes.c_int], ctypes.c_int),
     "mxg_engine_time_force": ([_vp, ctypes.c_int, _c_double_p], ctypes.c_int),

@@ -85,7 +85,16 @@ struct DevSpace {        // one per replica
     float bc_vel[6][3];
     float bc_restore[6];
     unsigned rng_mode;   // 0: reference DPD random term (xi = 1), 1: Philox
-    unsigned pad;
+    int prune;           // bit 0: per-pair projection test, bit 1: cell-pair exit test (runner_dopair)
+    float sort_bias;     // |h| (runner_dopair.cpp:132)
+    float sort_dscale;   // SHRT_MAX / (2 |h|)
+    int dmaxdist;        // 2 + dscale * cutoff
+    int pad2;
+};
+
+/* normalised sort directions of the 13 sort lists (space_cell.cpp:82-96) */
+struct SortAxes {
+    float n[13][3];
 };
 
 struct DevBond {
@@ -106,7 +115,7 @@ struct EngineView {      // everything a kernel needs, passed by value
     const unsigned *cell_flags;
     const int *nb_off;
     const int *nb_cell;
-    const float4 *nb_shift;  // xyz shift, w = role bits
+    const float4 *nb_shift;  // xyz shift, w = bits of role | sid << 2 | dnshift << 8
     const DevPot *pots;
     const float *coef;
     const int *pot_idx;      // per replica: [ntypes*ntypes] potential index or -1
@@ -116,8 +125,11 @@ struct EngineView {      // everything a kernel needs, passed by value
     int ncells;
     int nparts;
     const unsigned long long *step;  // device step counter
+    const SortAxes *axes;
+    int2 *sort_bounds;               // per cell and sort axis: (min key, max key)
     double *epot_cell;       // per cell nonbonded energy of the last force pass
     unsigned *status;
+    unsigned long long *pair_stats;  // non-null only for the statistics launch
 };
 
 #ifdef __CUDACC__
@@ -138,6 +150,13 @@ __device__ __forceinline__ uint4 philox4x32(uint4 c, uint2 k) {
         k.y += W1;
     }
     return c;
+}
+
+/* The reference's projection key of a particle along sort direction n
+ * (runner_dosort.cpp:133-136): (unsigned)(dscale * (bias + x.n)) in FP32. */
+__device__ __forceinline__ int sort_key(float x, float y, float z, const float *n, float bias, float dscale) {
+    const float proj = __fadd_rn(__fadd_rn(__fadd_rn(bias, __fmul_rn(x, n[0])), __fmul_rn(y, n[1])), __fmul_rn(z, n[2]));
+    return (int)(unsigned)__fmul_rn(dscale, proj);
 }
 
 /* uniform in (0,1) from 32 random bits */

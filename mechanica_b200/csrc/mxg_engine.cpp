@@ -46,6 +46,23 @@ const bool kCellFlip[27] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0, 0, 0, 0
 
 enum : int { kTaskSelf = 1, kTaskPair = 2, kTaskSort = 3 };  // task.h:31-37
 
+/* normalised shift vector of each of the 13 sort lists (space_cell.cpp:82-96) */
+const double kCellShift[13][3] = {
+    {5.773502691896258e-01, 5.773502691896258e-01, 5.773502691896258e-01},
+    {7.071067811865475e-01, 7.071067811865475e-01, 0.0},
+    {5.773502691896258e-01, 5.773502691896258e-01, -5.773502691896258e-01},
+    {7.071067811865475e-01, 0.0, 7.071067811865475e-01},
+    {1.0, 0.0, 0.0},
+    {7.071067811865475e-01, 0.0, -7.071067811865475e-01},
+    {5.773502691896258e-01, -5.773502691896258e-01, 5.773502691896258e-01},
+    {7.071067811865475e-01, -7.071067811865475e-01, 0.0},
+    {5.773502691896258e-01, -5.773502691896258e-01, -5.773502691896258e-01},
+    {0.0, 7.071067811865475e-01, 7.071067811865475e-01},
+    {0.0, 1.0, 0.0},
+    {0.0, 7.071067811865475e-01, -7.071067811865475e-01},
+    {0.0, 0.0, 1.0},
+};
+
 struct Task {
     int type, flags, i, j;
 };
@@ -108,6 +125,7 @@ struct mxg_engine {
     double dt = 0.01;
     float max_dist_fraction = 0.05f;
     unsigned rng_mode = 0;
+    int pruning = 0;  // 0: the reference's pruning, 1: same with the per-pair test on every grid, 2: none
 
     // ---- space (space_init) ----
     int cdim[3];
@@ -149,6 +167,8 @@ struct mxg_engine {
     int *d_pot_idx = nullptr;
     DevType *d_types = nullptr;
     DevSpace *d_spaces = nullptr;
+    SortAxes *d_axes = nullptr;
+    int2 *d_sort_bounds = nullptr;
     double *d_epot_cell = nullptr, *d_ebond_slot = nullptr;
     DevBond *d_bonds = nullptr;
     unsigned *d_bond_flags = nullptr;
@@ -338,7 +358,24 @@ struct mxg_engine {
             S.bc_restore[f] = bc_restore[f];
         }
         S.rng_mode = rng_mode;
+        // the per-pair projection test can only drop a pair inside the cutoff when
+        // the cells are not cubic; the cell-pair exit test applies to every grid
+        const bool cubic = h[0] == h[1] && h[1] == h[2];
+        S.prune = pruning == 2 ? 0 : (2 | ((pruning == 1 || !cubic) ? 1 : 0));
+        S.dmaxdist = dmaxdist();
+        S.sort_bias = sort_bias();
+        S.sort_dscale = sort_dscale();
         return S;
+    }
+
+    /* runner_dopair.cpp:132-136: bias = |h|, dscale = SHRT_MAX/(2 bias),
+     * dmaxdist = 2 + dscale*(cutoff + 2*maxdx) with maxdx = 0; FP32. */
+    float sort_bias() const { return (float)std::sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]); }
+    float sort_dscale() const { return (float)32767 / (2 * sort_bias()); }
+    int dmaxdist() const { return (int)(2 + sort_dscale() * ((float)cutoff + 2 * 0.0f)); }
+    int dnshift(const float *shift) const {
+        const float ns = std::sqrt(shift[0] * shift[0] + shift[1] * shift[1] + shift[2] * shift[2]);
+        return (int)(sort_dscale() * ns);
     }
 
     EngineView view(int b) const {
@@ -363,8 +400,11 @@ struct mxg_engine {
         v.ncells = ncells;
         v.nparts = nparts;
         v.step = d_step;
+        v.axes = d_axes;
+        v.sort_bounds = d_sort_bounds;
         v.epot_cell = d_epot_cell;
         v.status = d_status;
+        v.pair_stats = nullptr;
         return v;
     }
 
@@ -437,9 +477,10 @@ int mxg_engine::start(cudaStream_t st) {
         } else if (t.type == kTaskPair) {
             int ci = t.i, cj = t.j;
             float shift[3];
-            getsid(ci, cj, shift);  // runner_dopair recomputes the shift (and flip) per task
+            const int sid = getsid(ci, cj, shift);  // runner_dopair recomputes the shift (and flip) per task
+            const int dn = dnshift(shift);
             float4 e1 = make_float4(shift[0], shift[1], shift[2], 0.f), e2 = e1;
-            int r1 = kRoleFirst, r2 = kRoleSecond;
+            int r1 = kRoleFirst | (sid << 2) | (dn << 8), r2 = kRoleSecond | (sid << 2) | (dn << 8);
             memcpy(&e1.w, &r1, 4);
             memcpy(&e2.w, &r2, 4);
             nb[ci].push_back({cj, e1});
@@ -500,6 +541,9 @@ int mxg_engine::start(cudaStream_t st) {
         d.has_force = types[a].has_force ? 1 : 0;
     }
     std::vector<DevSpace> hs(1, space_desc());
+    std::vector<SortAxes> haxes(1);
+    for (int q = 0; q < 13; ++q)
+        for (int k = 0; k < 3; ++k) haxes[0].n[q][k] = (float)kCellShift[q][k];
     std::vector<int> hrep(ncells, 0);
 
     // ---- bonds: CSR by particle id ----
@@ -554,6 +598,8 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_pot_idx, hpidx.size());
     rc |= alloc(&d_types, ht.size());
     rc |= alloc(&d_spaces, hs.size());
+    rc |= alloc(&d_axes, 1);
+    rc |= alloc(&d_sort_bounds, (size_t)ncells * 13);
     rc |= alloc(&d_epot_cell, ncells);
     rc |= alloc(&d_ebond_slot, nparts);
     rc |= alloc(&d_bonds, hb.size());
@@ -580,7 +626,7 @@ int mxg_engine::start(cudaStream_t st) {
         (rc = upload(d_nb_off, nb_off, stream)) || (rc = upload(d_nb_cell, nb_cell, stream)) ||
         (rc = upload(d_nb_shift, nb_shift, stream)) || (rc = upload(d_pots, hp, stream)) ||
         (rc = upload(d_coef, coef, stream)) || (rc = upload(d_pot_idx, hpidx, stream)) ||
-        (rc = upload(d_types, ht, stream)) || (rc = upload(d_spaces, hs, stream)) ||
+        (rc = upload(d_types, ht, stream)) || (rc = upload(d_spaces, hs, stream)) || (rc = upload(d_axes, haxes, stream)) ||
         (rc = upload(d_bonds, hb, stream)) || (rc = upload(d_bond_flags, hbf, stream)) ||
         (rc = upload(d_bond_off, boff, stream)) || (rc = upload(d_bond_list, blist, stream)))
         return rc;
@@ -798,6 +844,14 @@ int mxg_engine_set_rng_mode(mxg_engine *e, int mode) {
     if (!e) return MXG_ERR_NULL;
     if (e->started) return MXG_ERR_STATE;
     e->rng_mode = mode ? 1u : 0u;
+    return MXG_OK;
+}
+
+int mxg_engine_set_pair_pruning(mxg_engine *e, int mode) {
+    if (!e) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    if (mode < 0 || mode > 2) return MXG_ERR_ARG;
+    e->pruning = mode;
     return MXG_OK;
 }
 
@@ -1043,6 +1097,30 @@ int mxg_engine_device_state(mxg_engine *e, void **pos, void **vel, void **force,
     return MXG_OK;
 }
 
+int mxg_engine_copy_state(mxg_engine *e, void *host_pos, void *host_vel, int to_device) {
+    if (!e || !host_pos || !host_vel) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    const size_t bytes = sizeof(float4) * (size_t)e->nparts;
+    if (to_device) {
+        CUDA_TRY(cudaMemcpyAsync(e->d_pos[e->cur], host_pos, bytes, cudaMemcpyHostToDevice, e->stream));
+        CUDA_TRY(cudaMemcpyAsync(e->d_vel[e->cur], host_vel, bytes, cudaMemcpyHostToDevice, e->stream));
+    } else {
+        CUDA_TRY(cudaMemcpyAsync(host_pos, e->d_pos[e->cur], bytes, cudaMemcpyDeviceToHost, e->stream));
+        CUDA_TRY(cudaMemcpyAsync(host_vel, e->d_vel[e->cur], bytes, cudaMemcpyDeviceToHost, e->stream));
+    }
+    return MXG_OK;
+}
+
+int mxg_engine_energy_async(mxg_engine *e, double *host_out2) {
+    if (!e || !host_out2) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    launch_energy(e->ncells, e->d_epot_cell, e->nparts, e->bonds.empty() ? nullptr : e->d_ebond_slot,
+                  e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
+                  e->stream);
+    CUDA_TRY(cudaMemcpyAsync(host_out2, e->d_energy, 2 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    return MXG_OK;
+}
+
 int mxg_engine_finalize(mxg_engine *e) {
     if (!e) return MXG_ERR_NULL;
     if (e->started && e->stream) cudaStreamSynchronize(e->stream);
@@ -1102,7 +1180,21 @@ int mxg_engine_pair_counts(mxg_engine *e, long long *candidates, long long *inte
             cand += (long long)cnt[t.i] * cnt[t.j];
     }
     if (candidates) *candidates = cand;
-    if (interacting) *interacting = -1;
+    if (interacting) {
+        // one statistics launch of the force kernel counts the interacting pairs
+        // (each pair once, in the reference's orientation)
+        unsigned long long *d_cnt = nullptr;
+        CUDA_TRY(cudaMalloc(&d_cnt, sizeof(unsigned long long)));
+        CUDA_TRY(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), e->stream));
+        EngineView v = e->view(e->cur);
+        v.pair_stats = d_cnt;
+        launch_force(v, e->has_dpd, e->force_grid, e->stream);
+        unsigned long long n = 0;
+        CUDA_TRY(cudaMemcpyAsync(&n, d_cnt, sizeof(n), cudaMemcpyDeviceToHost, e->stream));
+        CUDA_TRY(cudaStreamSynchronize(e->stream));
+        cudaFree(d_cnt);
+        *interacting = (long long)n;
+    }
     return MXG_OK;
 }
 

@@ -54,6 +54,43 @@ __device__ __forceinline__ float philox_pair_xi(unsigned long long step, unsigne
 }  // namespace
 
 /* ------------------------------------------------------------------------ */
+/* sort-key bounds                                                           */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Per cell and per sort direction, the smallest and largest projection key of
+ * its particles (runner_dosort.cpp:133-141 computes the keys; runner_dopair
+ * reads the largest key of its first cell and the smallest of its second,
+ * runner_dopair.cpp:167-171). One warp per cell.
+ */
+__global__ void sort_bounds_kernel(EngineView v) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < v.ncells; c += warps) {
+        const int n = v.cell_count[c];
+        if (n == 0) continue;
+        const int start = v.cell_start[c];
+        const DevSpace &S = v.spaces[v.cell_rep[c]];
+        const float bias = S.sort_bias, dscale = S.sort_dscale;
+        for (int sid = 0; sid < 13; ++sid) {
+            const float *ax = v.axes->n[sid];
+            int kmin = 0x7fffffff, kmax = -1;
+            for (int k = lane; k < n; k += 32) {
+                const float4 q = v.pos[start + k];
+                const int key = sort_key(q.x, q.y, q.z, ax, bias, dscale);
+                kmin = min(kmin, key);
+                kmax = max(kmax, key);
+            }
+            for (int off = 16; off > 0; off >>= 1) {
+                kmin = min(kmin, __shfl_xor_sync(kFull, kmin, off));
+                kmax = max(kmax, __shfl_xor_sync(kFull, kmax, off));
+            }
+            if (lane == 0) v.sort_bounds[c * 13 + sid] = make_int2(kmin, kmax);
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
 /* nonbonded forces                                                          */
 /* ------------------------------------------------------------------------ */
 
@@ -72,10 +109,12 @@ __device__ __forceinline__ float philox_pair_xi(unsigned long long step, unsigne
  * dx = (x_j - shift) - x_i with i as its second particle. Computing dx in the
  * reference's orientation makes r2 and the per-pair force bit-identical.
  */
-template <bool kDPD>
+template <bool kDPD, bool kStats>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) force_kernel(EngineView v) {
+    unsigned long long npair = 0;  // interacting pairs counted once (statistics launch only)
     __shared__ float4 sp[kWarpsPerBlock][32];
     __shared__ float4 sv[kWarpsPerBlock][kDPD ? 32 : 1];
+    __shared__ int skey[kWarpsPerBlock][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int c = blockIdx.x * kWarpsPerBlock + w; c < v.ncells; c += gridDim.x * kWarpsPerBlock) {
         const int n = v.cell_count[c];
@@ -86,6 +125,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) force_kernel(EngineView v
             const int pot_base = S.pot_offset;
             const float cut2_pair = S.cut2_pair, cut2_self = S.cut2_self;
             const unsigned rng_mode = S.rng_mode;
+            const bool prune = (S.prune & 1) != 0;       // per-pair projection test
+            const bool exit_test = (S.prune & 2) != 0;   // cell-pair exit test
+            const float sbias = S.sort_bias, sdscale = S.sort_dscale;
+            const int dmaxdist = S.dmaxdist;
             const int P = n >= 32 ? 32 : next_pow2(n);
             const int G = 32 / P;
             const int il = lane & (P - 1), g = lane / P;
@@ -115,7 +158,27 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) force_kernel(EngineView v
                     if (jn == 0) continue;
                     const int js = v.cell_start[nc];
                     const float4 sh = v.nb_shift[e];
-                    const int role = __float_as_int(sh.w);
+                    const int packed = __float_as_int(sh.w);
+                    const int role = packed & 3;
+                    // runner_dopair's pruning: a pair (first i, second j) is evaluated only
+                    // when key_j + dnshift - key_i < dmaxdist (runner_dopair.cpp:167-182)
+                    const bool prune_e = prune && role != kRoleSelf;
+                    const int sid = (packed >> 2) & 15;
+                    const float *axis = v.axes->n[sid];
+                    const int dnshift = packed >> 8;
+                    if (exit_test && role != kRoleSelf) {
+                        // runner_dopair's first-iteration exit (runner_dopair.cpp:167-171): with the
+                        // largest key of the first cell and the smallest of the second, the unsigned
+                        // difference kmin + dnshift - kmax exceeds dmaxdist (or wraps below zero)
+                        // and the whole cell pair is skipped
+                        const int2 bi = v.sort_bounds[c * 13 + sid], bj = v.sort_bounds[nc * 13 + sid];
+                        const int kmax_first = role == kRoleFirst ? bi.y : bj.y;
+                        const int kmin_second = role == kRoleFirst ? bj.x : bi.x;
+                        const int gap = kmin_second + dnshift - kmax_first;
+                        if (gap < 0 || gap > dmaxdist) continue;
+                    }
+                    int mykey = 0;
+                    if (prune_e) mykey = sort_key(xi.x, xi.y, xi.z, axis, sbias, sdscale);
                     float ax = xi.x, ay = xi.y, az = xi.z;
                     if (role == kRoleFirst) {
                         ax = __fsub_rn(xi.x, sh.x);
@@ -128,6 +191,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) force_kernel(EngineView v
                         __syncwarp();
                         if (lane < cnt) {
                             float4 q = v.pos[js + j0 + lane];
+                            if (prune_e) skey[w][lane] = sort_key(q.x, q.y, q.z, axis, sbias, sdscale);
                             if (role == kRoleSecond) {
                                 q.x = __fsub_rn(q.x, sh.x);
                                 q.y = __fsub_rn(q.y, sh.y);
@@ -141,6 +205,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) force_kernel(EngineView v
                         for (int t = g; t < cnt; t += G) {
                             const int j = j0 + t;
                             if (role == kRoleSelf && j == i) continue;
+                            if (prune_e) {
+                                const int kf = role == kRoleFirst ? mykey : skey[w][t];
+                                const int ks = role == kRoleFirst ? skey[w][t] : mykey;
+                                if (!(ks + dnshift - kf < dmaxdist)) continue;
+                            }
                             const float4 q = sp[w][t];
                             // dx in the reference's orientation
                             float dx, dy, dz;
@@ -152,6 +221,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) force_kernel(EngineView v
                                 dx = __fsub_rn(ax, q.x);
                                 dy = __fsub_rn(ay, q.y);
                                 dz = __fsub_rn(az, q.z);
+                                if (role == kRoleSelf && j < i) {
+                                    // the reference's first particle of a self pair is the earlier
+                                    // one; x_j - x_i is the exact negation of x_i - x_j
+                                    dx = -dx;
+                                    dy = -dy;
+                                    dz = -dz;
+                                }
                             }
                             float r2 = dot3_rn(dx, dy, dz);
                             if (r2 > cut2) continue;
@@ -221,6 +297,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) force_kernel(EngineView v
                                     fz = __fsub_rn(fz, __fmul_rn(f, ez));
                                 }
                                 // the reference tabulates zero energy for DPD
+                                if (kStats && i_first) ++npair;
                             } else {
                                 const float radj = v.types[tj].radius;
                                 float pe, pf;
@@ -236,7 +313,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) force_kernel(EngineView v
                                     fy = __fadd_rn(fy, wy);
                                     fz = __fadd_rn(fz, wz);
                                 }
-                                if (role == kRoleFirst || (role == kRoleSelf && i < j)) eacc += (double)pe;
+                                if (role == kRoleFirst || (role == kRoleSelf && i < j)) {
+                                    eacc += (double)pe;
+                                    if (kStats) ++npair;
+                                }
                             }
                         }
                     }
@@ -254,6 +334,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) force_kernel(EngineView v
         }
         for (int off = 16; off > 0; off >>= 1) ecell += __shfl_xor_sync(kFull, ecell, off);
         if (lane == 0) v.epot_cell[c] = ecell;
+    }
+    if (kStats) {
+        for (int off = 16; off > 0; off >>= 1) npair += __shfl_xor_sync(kFull, npair, off);
+        if (lane == 0) atomicAdd(v.pair_stats, npair);
     }
 }
 
@@ -607,10 +691,19 @@ __global__ void reduce_final_kernel(int nblocks, const double *partials, double 
 /* ------------------------------------------------------------------------ */
 
 void launch_force(const EngineView &v, bool has_dpd, int grid, cudaStream_t st) {
-    if (has_dpd)
-        force_kernel<true><<<grid, kWarpsPerBlock * 32, 0, st>>>(v);
-    else
-        force_kernel<false><<<grid, kWarpsPerBlock * 32, 0, st>>>(v);
+    const bool stats = v.pair_stats != nullptr;
+    sort_bounds_kernel<<<(v.ncells * 32 + 255) / 256, 256, 0, st>>>(v);
+    if (has_dpd) {
+        if (stats)
+            force_kernel<true, true><<<grid, kWarpsPerBlock * 32, 0, st>>>(v);
+        else
+            force_kernel<true, false><<<grid, kWarpsPerBlock * 32, 0, st>>>(v);
+    } else {
+        if (stats)
+            force_kernel<false, true><<<grid, kWarpsPerBlock * 32, 0, st>>>(v);
+        else
+            force_kernel<false, false><<<grid, kWarpsPerBlock * 32, 0, st>>>(v);
+    }
 }
 
 void launch_bonds(const EngineView &v, const DevBond *bonds, unsigned *bond_flags, const int *bond_off,

@@ -16,10 +16,16 @@
  * DPD thermostat summed), which the reference cannot express (engine_addpot
  * keeps one potential per pair, engine.cpp:968-977).
  *
- * Pairs are enumerated brute force within each task's cell pair, which is the
- * interacting set of the reference's sorted loops: their pruning keeps two
- * quanta of slack (runner_dopair.cpp:136) and never drops a pair inside the
- * cutoff. The r < a random-direction branch (dpd_eval.hpp:122-131) is not
+ * Pairs are enumerated within each task's cell pair and filtered by the
+ * reference's sorted-projection test (runner_dosort.cpp:133-136,
+ * runner_dopair.cpp:132-182): a pair is evaluated only when
+ * key_j + dnshift - key_i < dmaxdist. With cubic cells the test keeps two
+ * quanta of slack and never drops a pair inside the cutoff; with non-cubic
+ * cells it does (it uses |shift| where the projection of the shift belongs),
+ * and the oracle reproduces that. The whole cell pair is also skipped when the
+ * loop's first exit test underflows (unsigned arithmetic, runner_dopair.cpp:167-171),
+ * which happens for particles within one key quantum of the shared face.
+ * pruning = 0 or 1 applies both tests (the reference), 2 applies neither. The r < a random-direction branch (dpd_eval.hpp:122-131) is not
  * reproduced; such pairs are counted and skipped.
  */
 #include "oracle.h"
@@ -31,6 +37,22 @@
 #include <vector>
 
 namespace {
+
+const double kCellShift[13][3] = {
+    {5.773502691896258e-01, 5.773502691896258e-01, 5.773502691896258e-01},
+    {7.071067811865475e-01, 7.071067811865475e-01, 0.0},
+    {5.773502691896258e-01, 5.773502691896258e-01, -5.773502691896258e-01},
+    {7.071067811865475e-01, 0.0, 7.071067811865475e-01},
+    {1.0, 0.0, 0.0},
+    {7.071067811865475e-01, 0.0, -7.071067811865475e-01},
+    {5.773502691896258e-01, -5.773502691896258e-01, 5.773502691896258e-01},
+    {7.071067811865475e-01, -7.071067811865475e-01, 0.0},
+    {5.773502691896258e-01, -5.773502691896258e-01, -5.773502691896258e-01},
+    {0.0, 7.071067811865475e-01, 7.071067811865475e-01},
+    {0.0, 1.0, 0.0},
+    {0.0, 7.071067811865475e-01, -7.071067811865475e-01},
+    {0.0, 0.0, 1.0},
+};
 
 const int kSortlistID[27] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 0, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2, 1, 0};
 const bool kFlip[27] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -89,6 +111,11 @@ struct Setup {
     const int *dpd_of_pair;
     std::vector<Pot<T>> pots;
     std::vector<T> body;
+    std::vector<float> xf;  // FP32 positions for the pruning keys
+    bool prune;
+    float bias, dscale;
+    int dmaxdist;
+    float axes[13][3];
 };
 
 template <typename T>
@@ -182,9 +209,43 @@ int run(const Setup<T> &S, const int *tasks, int ntasks, double *f_out, double *
                 std::swap(ci, cj);
                 for (int k = 0; k < 3; ++k) shift[k] = -shift[k];
             }
-            (void)kSortlistID;
+            // the reference's sorted-projection pruning, always in FP32
+            // (runner_dosort.cpp:133-136, runner_dopair.cpp:132-182)
+            float fshift[3];
+            for (int k = 0; k < 3; ++k) {
+                const double sd = S.origin[3 * cj + k] - S.origin[3 * ci + k];
+                float sk = (float)sd;
+                if (sk * 2 > S.dim[k])
+                    sk = (float)(sk - S.dim[k]);
+                else if (sk * 2 < -S.dim[k])
+                    sk = (float)(sk + S.dim[k]);
+                fshift[k] = sk;
+            }
+            const float *nax = S.axes[kSortlistID[sid]];
+            const float nsh = std::sqrt(fshift[0] * fshift[0] + fshift[1] * fshift[1] + fshift[2] * fshift[2]);
+            const int dnshift = (int)(S.dscale * nsh);
+            auto key = [&](int p) {
+                const float proj = S.bias + S.xf[3 * p] * nax[0] + S.xf[3 * p + 1] * nax[1] + S.xf[3 * p + 2] * nax[2];
+                return (int)(unsigned)(S.dscale * proj);
+            };
+            if (S.prune && !members[ci].empty() && !members[cj].empty()) {
+                // first-iteration exit of the sorted loop (runner_dopair.cpp:167-171): the
+                // largest key of cell i against the smallest of cell j, unsigned arithmetic
+                int kmax = -1, kmin = 0x7fffffff;
+                for (int pi : members[ci]) kmax = std::max(kmax, key(pi));
+                for (int pj : members[cj]) kmin = std::min(kmin, key(pj));
+                const unsigned gap = (unsigned)kmin + (unsigned)dnshift - (unsigned)kmax;
+                if (gap > (unsigned)S.dmaxdist) {
+                    ncand += (long long)members[ci].size() * members[cj].size();
+                    continue;
+                }
+            }
             for (int pi : members[ci])
                 for (int pj : members[cj]) {
+                    if (S.prune && !((unsigned)key(pj) + (unsigned)dnshift - (unsigned)key(pi) < (unsigned)S.dmaxdist)) {
+                        ++ncand;
+                        continue;
+                    }
                     T pix[3], dx[3];
                     for (int k = 0; k < 3; ++k) {
                         pix[k] = S.x[3 * pi + k] - shift[k];
@@ -251,6 +312,16 @@ int build_and_run(const OrcInput *in, double *f_out, double *epot_out, long long
         S.pots.push_back(p);
     }
     for (int t = 0; t < 3 * in->ntypes; ++t) S.body.push_back(in->body ? (T)in->body[t] : (T)0);
+    S.xf.assign(in->xrel, in->xrel + 3 * (size_t)in->N);
+    double h[3];
+    int cdim[3] = {in->cdim[0], in->cdim[1], in->cdim[2]};
+    for (int k = 0; k < 3; ++k) h[k] = in->dim[k] / cdim[k];
+    S.bias = (float)std::sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+    S.dscale = (float)32767 / (2 * S.bias);
+    S.dmaxdist = (int)(2 + S.dscale * ((float)in->cutoff + 2 * 0.0f));
+    S.prune = in->pruning != 2;
+    for (int q = 0; q < 13; ++q)
+        for (int k = 0; k < 3; ++k) S.axes[q][k] = (float)kCellShift[q][k];
     return run(S, in->tasks, in->ntasks, f_out, epot_out, counts);
 }
 

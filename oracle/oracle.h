@@ -30,6 +30,8 @@ typedef struct OrcInput {
     const float *coef;
     const float *dpd;         /* npots*4: alpha, gamma, sigma, 1/sqrt(dt) */
     const float *body;        /* ntypes*3 constant force, may be NULL */
+    int cdim[3];              /* cells per axis */
+    int pruning;              /* 0: reference pruning on non-cubic cells, 1: always, 2: never */
 } OrcInput;
 
 /* precision 32 or 64; f_out N*3; counts[3] = candidates, interacting, r<a skipped */

@@ -25,6 +25,7 @@ class _OrcInput(ctypes.Structure):
         ("pot_kind", ctypes.c_void_p), ("pot_flags", ctypes.c_void_p), ("pot_n", ctypes.c_void_p),
         ("pot_alpha", ctypes.c_void_p), ("pot_abr", ctypes.c_void_p), ("pot_coef_off", ctypes.c_void_p),
         ("coef", ctypes.c_void_p), ("dpd", ctypes.c_void_p), ("body", ctypes.c_void_p),
+        ("cdim", ctypes.c_int * 3), ("pruning", ctypes.c_int),
     ]
 
 
@@ -83,7 +84,7 @@ def cell_origins(dim, cdim, origin=(0.0, 0.0, 0.0)):
     return out
 
 
-def nonbond(scn, xrel, vel, cell, tasks, cdim, precision=64, tables=None, second=None):
+def nonbond(scn, xrel, vel, cell, tasks, cdim, precision=64, tables=None, second=None, pruning=0):
     """Forces (N,3) float64, energy, counts for a configuration.
 
     tables: {pot index: (info, coef)} for scn["pots"] order (defaults to the
@@ -159,6 +160,9 @@ def nonbond(scn, xrel, vel, cell, tasks, cdim, precision=64, tables=None, second
     inp.coef = coef.ctypes.data
     inp.dpd = dpd.ctypes.data
     inp.body = body.ctypes.data
+    for k in range(3):
+        inp.cdim[k] = int(cdim[k])
+    inp.pruning = int(pruning)
     f = np.zeros((N, 3))
     ep = ctypes.c_double()
     counts = np.zeros(3, dtype=np.int64)

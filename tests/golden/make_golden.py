@@ -111,6 +111,10 @@ def make_case(name, factory, nsteps):
     for k in ("xrel", "xabs", "v", "cell", "epot", "ekin", "bond_flags"):
         out["traj_" + k] = tr[k]
     out["traj_nsteps"] = np.int64(nsteps)
+    for ns in (1, 2):
+        t = refengine.run(dict(scn, action="steps", nsteps=ns, runners=1))
+        for k in ("xrel", "xabs", "v", "cell", "epot", "ekin", "bond_flags"):
+            out[f"step{ns}_" + k] = t[k]
     np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **out)
 
 

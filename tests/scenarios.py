@@ -1,173 +1,3 @@
-"""Seeded synthetic inputs shaped like the benchmark configurations, and helpers
-that build the same scenario in the B200 engine (through the Python surface)
-and in the reference engine (oracle tier A).
-
-Shapes follow the five workloads of the force-and-step path:
-  argon   LJ 12-6 fluid, one type, mass 39.4, periodic cube, density 10
-  dpd     DPD fluid with a constant body force, periodic x/y, no-slip z walls
-  lattice simple-cubic harmonic-bonded lattice with Morse nonbonded, overdamped
-  morse2  two-type Morse mixture, overdamped, periodic (batched replicas)
-Sizes are parameters so tests run small cases and the bench runs full ones.
-"""
-import numpy as np
-
-import mechanica_b200 as m
-
-
-def _reject_close(x, L, dmin, rng):
-    """Replaces points closer than dmin to an earlier point (periodic cube)."""
-    n = len(x)
-    ncell = max(1, int(L // max(dmin, 1e-9)))
-    h = L / ncell
-    for _ in range(200):
-        idx = np.floor(x / h).astype(np.int64) % ncell
-        key = (idx[:, 0] * ncell + idx[:, 1]) * ncell + idx[:, 2]
-        order = np.argsort(key, kind="stable")
-        bad = np.zeros(n, dtype=bool)
-        # compare against the 27 neighbouring cells
-        buckets = {}
-        for p in order:
-            buckets.setdefault(int(key[p]), []).append(p)
-        for p in range(n):
-            i, j, k = idx[p]
-            for di in (-1, 0, 1):
-                for dj in (-1, 0, 1):
-                    for dk in (-1, 0, 1):
-                        kk = (((i + di) % ncell) * ncell + (j + dj) % ncell) * ncell + (k + dk) % ncell
-                        for q in buckets.get(int(kk), ()):
-                            if q < p:
-                                d = x[p] - x[q]
-                                d -= L * np.round(d / L)
-                                if d @ d < dmin * dmin:
-                                    bad[p] = True
-                                    break
-                        if bad[p]:
-                            break
-                    if bad[p]:
-                        break
-                if bad[p]:
-                    break
-        if not bad.any():
-            return x
-        x[bad] = rng.uniform(0, L, size=(int(bad.sum()), 3))
-    raise RuntimeError("rejection sampling did not converge")
-
-
-def argon(n=10000, L=10.0, cells=10, seed=1, dmin=0.3, temperature=100.0, mass=39.4, dt=0.01):
-    rng = np.random.default_rng(seed)
-    x = rng.uniform(0, L, size=(n, 3))
-    if dmin > 0:
-        x = _reject_close(x, L, dmin, rng)
-    x = x.astype(np.float32).astype(np.float64)
-    v = rng.normal(0, np.sqrt(temperature / mass), size=(n, 3))
-    v -= v.mean(axis=0)
-    v = v.astype(np.float32).astype(np.float64)
-    return dict(dim=[L, L, L], cells=[cells] * 3, cutoff=1.0, dt=dt, bc=("periodic", "periodic", "periodic"),
-                types=[(mass, 0.1, m.Newtonian)],
-                pots=[("lj126", (0.275, 1.0, 9.5075e-6, 6.1545e-3, 1e-3), 0, 0)],
-                forces=[], x=x, v=v, t=np.zeros(n, dtype=np.int32))
-
-
-def dpd(n=200000, dims=(40.0, 20.0, 20.0), seed=2, body=0.02, dt=0.01):
-    rng = np.random.default_rng(seed)
-    d = np.asarray(dims)
-    x = rng.uniform(0, 1, size=(n, 3)) * d
-    x = np.minimum(x, d * (1 - 1e-6)).astype(np.float32).astype(np.float64)
-    v = rng.normal(0, 1.0, size=(n, 3))
-    v -= v.mean(axis=0)
-    v = v.astype(np.float32).astype(np.float64)
-    cells = [int(c) for c in d]  # cutoff 1.0
-    return dict(dim=list(d), cells=cells, cutoff=1.0, dt=dt, bc=("periodic", "periodic", "no_slip"),
-                types=[(1.0, 0.5, m.Newtonian)],
-                pots=[("dpd", (25.0, 4.5, 3.0, 1.0, 0), 0, 0)],
-                forces=[(0, body, 0.0, 0.0)], x=x, v=v, t=np.zeros(n, dtype=np.int32))
-
-
-def lattice(nx=32, spacing=0.5, seed=3, dt=0.005, pull=0.05, dissociation=2.0, k=200.0, margin=2.0, noise=1e-4,
-            radius=0.5):
-    """nx^3 simple-cubic lattice, harmonic bonds to the 6 nearest neighbours,
-    Morse nonbonded (d=0.5, a=6, r0=0.5, cutoff 1.5); the top layer is a
-    separate type pulled by a constant force in +z. Free-slip walls."""
-    rng = np.random.default_rng(seed)
-    g = np.arange(nx) * spacing + spacing / 2 + margin / 2
-    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
-    x = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
-    x += rng.normal(0, noise * spacing, size=x.shape)
-    x = x.astype(np.float32).astype(np.float64)
-    n = len(x)
-    idx = np.arange(n).reshape(nx, nx, nx)
-    t = np.zeros(n, dtype=np.int32)
-    t[idx[:, :, -1].ravel()] = 1
-    bi, bj = [], []
-    for ax in range(3):
-        sl_a = [slice(None)] * 3
-        sl_b = [slice(None)] * 3
-        sl_a[ax] = slice(0, nx - 1)
-        sl_b[ax] = slice(1, nx)
-        bi.append(idx[tuple(sl_a)].ravel())
-        bj.append(idx[tuple(sl_b)].ravel())
-    bi = np.concatenate(bi).astype(np.int32)
-    bj = np.concatenate(bj).astype(np.int32)
-    L = nx * spacing + margin
-    cut = 1.5
-    cells = int(L // cut)
-    return dict(dim=[L, L, L + 2.0], cells=[cells, cells, int((L + 2.0) // cut)], cutoff=cut, dt=dt,
-                bc=("free_slip", "free_slip", "free_slip"),
-                types=[(1.0, radius, m.Overdamped), (1.0, radius, m.Overdamped)],
-                pots=[("morse", (0.5, 6.0, 0.5, 1e-4, cut, 1e-3), 0, 0), ("morse", (0.5, 6.0, 0.5, 1e-4, cut, 1e-3), 0, 1),
-                      ("morse", (0.5, 6.0, 0.5, 1e-4, cut, 1e-3), 1, 1)],
-                forces=[(1, 0.0, 0.0, pull)], x=x, v=np.zeros_like(x), t=t,
-                bi=bi, bj=bj, bond_pot=("harmonic", (k, spacing, 0.1, 1.0, 0.009)), dissociation=dissociation)
-
-
-def morse2(n=4000, density=0.8, seed=4, dt=0.01, d=(0.6, 0.3, 0.8), cut=2.5):
-    rng = np.random.default_rng(seed)
-    L = (n / density) ** (1.0 / 3.0)
-    x = rng.uniform(0, L, size=(n, 3))
-    x = _reject_close(x, L, 0.6, rng).astype(np.float32).astype(np.float64)
-    t = (np.arange(n) % 2).astype(np.int32)
-    cells = max(3, int(L // cut))
-    dAA, dAB, dBB = d
-    return dict(dim=[L, L, L], cells=[cells] * 3, cutoff=cut, dt=dt, bc=("periodic", "periodic", "periodic"),
-                types=[(1.0, 1.0, m.Overdamped), (1.0, 1.0, m.Overdamped)],
-                pots=[("morse", (dAA, 5.0, 1.0, 1e-4, cut, 1e-3), 0, 0), ("morse", (dAB, 5.0, 1.0, 1e-4, cut, 1e-3), 0, 1),
-                      ("morse", (dBB, 5.0, 1.0, 1e-4, cut, 1e-3), 1, 1)],
-                forces=[], x=x, v=np.zeros_like(x), t=t)
-
-
-def make_potential(kind, params):
-    if kind == "lj126":
-        return m.Potential.lennard_jones_12_6(*params)
-    if kind == "morse":
-        return m.Potential.morse(*params)
-    if kind == "harmonic":
-        k, r0, mn, mx, tol = params
-        return m.Potential.harmonic(k, r0, mn, mx, tol)
-    if kind == "power":
-        return m.Potential.power(*params)
-    if kind == "dpd":
-        return m.Potential.dpd(*params[:4], shifted=bool(params[4]) if len(params) > 4 else False)
-    raise ValueError(kind)
-
-
-def build_gpu(scn, rng_mode="reference"):
-    """Builds the scenario in the B200 engine through the Python surface."""
-    bc = {"x": scn["bc"][0], "y": scn["bc"][1], "z": scn["bc"][2]}
-    m.init(dim=scn["dim"], cells=scn["cells"], cutoff=scn["cutoff"], dt=scn["dt"], bc=bc, rng=rng_mode,
-           max_distance=scn.get("max_distance"))
-    types = []
-    for k, (mass, radius, dyn) in enumerate(scn["types"]):
-        types.append(type(f"T{k}", (m.Particle,), {"mass": mass, "radius": radius, "dynamics": dyn}))
-    for (kind, params, ti, tj) in scn["pots"]:
-        m.bind(make_potential(kind, params), types[ti], types[tj])
-    for (ti, fx, fy, fz) in scn["forces"]:
-        m.bind(m.forces.ConstantForce([fx, fy, fz]), types[ti])
-    x, v, t = scn["x"], scn["v"], scn["t"]
-    # create in id order, type by type, keeping ids equal to the scenario's indices
-    assert np.all(np.diff(np.flatnonzero(t == t[0])) >= 1)
-    u = m.universe
-    u._add_particles(np.asarray(x), np.asarray(v, dtype=np.float32), np.asarray(t, dtype=np.int32))
-    if "bi" in scn and len(scn["bi"]):
-        kind, params = scn["bond_pot"]
-        u._add_bonds(make_potential(kind, params), scn["bi"], scn["bj"], scn["dissociation"])
-    return u
+"""Test-side alias of the seeded workloads (mechanica_b200/workloads.py)."""
+from mechanica_b200.workloads import *  # noqa: F401,F403
+from mechanica_b200.workloads import _reject_close, argon, build_gpu, dpd, lattice, make_potential, morse2  # noqa: F401
