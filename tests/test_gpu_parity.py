@@ -68,14 +68,50 @@ def test_steps_match_reference(name, nsteps):
     u.steps(nsteps)
     x, v, f, c, xr = u.state()
     k = f"step{nsteps}_"
-    assert np.array_equal(c, z[k + "cell"])
+    # Pairs closer than the table minimum get a random direction in the
+    # reference (per-cell mt19937, dpd_eval.hpp:122-131) and a Philox draw here;
+    # particles in such pairs at the start of a step are excluded, and counted.
+    keep = np.ones(len(x), dtype=bool)
+    if nsteps == 2:
+        keep = ~_close_pairs(scn, z["step1_xabs"])
+    assert keep.mean() > 0.98
+    assert np.array_equal(c[keep], z[k + "cell"][keep])
     L = np.asarray(scn["dim"])
     d = x - z[k + "xabs"]
     d -= L * np.round(d / L)
-    assert np.abs(d).max() < 1e-5
-    assert rel_rms(v, z[k + "v"]) <= 1e-5 or np.abs(v - z[k + "v"]).max() < 1e-5
+    assert np.abs(d[keep]).max() < 1e-5
+    vr = z[k + "v"][keep]
+    assert rel_rms(v[keep], vr) <= 1e-5 or np.abs(v[keep] - vr).max() < 1e-5
     if "bi" in scn and len(scn["bi"]):
         assert np.array_equal(u.bond_flags(), z[k + "bond_flags"])
+
+
+def _close_pairs(scn, xabs):
+    """Particles with a neighbour closer than the minimum of their pair's table."""
+    from scipy.spatial import cKDTree
+    amin = {}
+    for (kind, params, ti, tj) in scn["pots"]:
+        a = {"lj126": params[0], "morse": params[3], "harmonic": params[2], "power": params[3],
+             "dpd": float(np.sqrt(np.float32(np.finfo(np.float32).eps)))}[kind]
+        amin[(ti, tj)] = amin[(tj, ti)] = a
+    if not amin:
+        return np.zeros(len(xabs), dtype=bool)
+    L = np.asarray(scn["dim"], dtype=np.float64)
+    periodic = all(b == "periodic" for b in scn["bc"])
+    pts = np.mod(xabs, L) if periodic else xabs
+    tree = cKDTree(pts, boxsize=L if periodic else None)
+    bad = np.zeros(len(xabs), dtype=bool)
+    for i, j in tree.query_pairs(max(amin.values())):
+        ti, tj = scn["t"][i], scn["t"][j]
+        a = amin.get((ti, tj))
+        if a is None:
+            continue
+        d = pts[i] - pts[j]
+        if periodic:
+            d -= L * np.round(d / L)
+        if d @ d < a * a:
+            bad[i] = bad[j] = True
+    return bad
 
 
 @pytest.mark.parametrize("name", [c for c in CASES if c != "lattice_noisy"])
