@@ -200,6 +200,23 @@ int mxg_engine_kernel_times(mxg_engine *e, double *ms, long long *launches, int 
  * reference's task list defines them (counted on the device when enabled). */
 int mxg_engine_pair_counts(mxg_engine *e, long long *candidates, long long *interacting);
 
+/* ---- allocation-free entry point ---- */
+/* No counterpart in the reference. Kinetic energy of nparts particles, computed like
+ * engine_kinetic_energy (float e = 0.5*mass*|v|^2 per particle, summed in FP64), for callers
+ * that cannot call cudaMalloc -- an application whose device memory is reserved by another
+ * allocator, or a latency-critical loop that must not take an allocation's implicit device
+ * synchronisation. vel and pos are device arrays of nparts float4 in the engine's layout (pos.w
+ * holds the type id bits, see mxg_engine_device_state); type_mass is a device array of ntypes
+ * doubles; out is a device array of 1 + ntypes doubles receiving the total and the per-type sums.
+ * Work is enqueued on stream (NULL = default stream). The reduction's scratch is a file-scope
+ * device array of 256 x 64 doubles (128 KiB, held by every GPU that loads the library until the
+ * process exits): ntypes above 64 is rejected with MXG_ERR_RANGE. The first call on a device looks
+ * the array's address up for that device (cudaGetSymbolAddress); make that first call before any
+ * stream capture. Calls that overlap on the GPU share the array and race; serialise them. Nothing
+ * is allocated: no cudaMalloc, cudaFree or allocating library routine is called. */
+int mxg_kinetic_energy_noalloc(const void *vel, const void *pos, int nparts, const double *type_mass, int ntypes,
+                               double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

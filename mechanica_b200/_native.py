@@ -98,6 +98,7 @@ _SIGS = {
     "mxg_engine_kernel_times": ([_vp, _c_double_p, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int], ctypes.c_int),
     "mxg_engine_pair_counts": ([_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)],
                                ctypes.c_int),
+    "mxg_kinetic_energy_noalloc": ([_vp, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp], ctypes.c_int),
 }
 
 _lib = None
