@@ -123,6 +123,23 @@ void mxg_potential_free(mxg_potential *p);
 int mxg_engine_init(const double *origin, const double *dim, const int *cells, double cutoff, const int *bc_kind,
                     const float *bc_velocity, const float *bc_restore, int max_type, unsigned flags,
                     mxg_engine **out);
+/* ---- independent replicas in one engine (batched ensembles) ---- */
+/* Adds another simulation box with its own geometry and boundaries to the engine (before
+ * mxg_engine_start); returns its replica index. mxg_engine_init creates replica 0. All replicas
+ * share the cutoff, dt, particle types and pruning mode; each has its own potentials per type pair,
+ * particles and cell grid, and every step advances all of them with the same kernel launches.
+ * No counterpart in the reference, which holds one engine per process (engine.h:708). */
+int mxg_engine_add_replica(mxg_engine *e, const double *origin, const double *dim, const int *cells,
+                           const int *bc_kind, const float *bc_velocity, const float *bc_restore);
+int mxg_engine_nr_replicas(const mxg_engine *e);
+/* engine_addpot / engine_addpart for one replica (the plain forms act on replica 0). */
+int mxg_engine_addpot_replica(mxg_engine *e, int replica, const mxg_potential *p, int type_i, int type_j);
+int mxg_engine_addparts_replica(mxg_engine *e, int replica, int n, const double *x, const float *v,
+                                const int *type, int *ids_out);
+/* Chooses the force kernel's grid (CTAs per SM) by timing candidate launches on the current state;
+ * returns the chosen blocks per SM. Call after mxg_engine_start. */
+int mxg_engine_autotune(mxg_engine *e);
+
 /* dt, max-distance fraction (reference default 0.05) */
 int mxg_engine_set_dt(mxg_engine *e, double dt, double max_dist_fraction);
 /* Returns the new type id (>= 0). */

@@ -250,12 +250,12 @@ class _ParticleMeta(type):
             u = _require()
             cls.id = u._add_type(cls)
 
-    def factory(cls, positions=None, velocities=None, nr_parts=None):
+    def factory(cls, positions=None, velocities=None, nr_parts=None, replica=0):
         """Bulk creation of particles of this type from arrays (N x 3)."""
         u = _require()
         x = np.asarray(positions, dtype=np.float64).reshape(-1, 3)
         v = np.zeros_like(x, dtype=np.float32) if velocities is None else np.asarray(velocities).reshape(-1, 3)
-        ids = u._add_particles(x, v, np.full(len(x), cls.id, dtype=np.int32))
+        ids = u._add_particles(x, v, np.full(len(x), cls.id, dtype=np.int32), replica)
         return ids
 
 
@@ -310,12 +310,14 @@ class _Universe:
         self.max_types = max_types
         self.time = 0
         self._types = []        # (mass, radius, dynamics, flags)
-        self._pots = []         # (potential, ti, tj)
+        self._pots = []         # (potential, ti, tj, replica)
+        self._replicas = []     # extra boxes: (origin, dim, cells, bc)
         self._forces = []       # (type, value)
         self._bonds = []        # (potential, i[], j[], dissociation)
         self._x = np.zeros((0, 3))
         self._v = np.zeros((0, 3), dtype=np.float32)
         self._t = np.zeros(0, dtype=np.int32)
+        self._r = np.zeros(0, dtype=np.int32)
         self._started = False
         self._dirty = False
         self._new_engine()
@@ -338,10 +340,16 @@ class _Universe:
         check(lib().mxg_engine_set_dt(self._e, self.dt, frac), "set_dt")
         check(lib().mxg_engine_set_rng_mode(self._e, 1 if self.rng == "philox" else 0), "set_rng_mode")
         check(lib().mxg_engine_set_pair_pruning(self._e, int(self.pair_pruning)), "set_pair_pruning")
+        for (o, d, c, b) in self._replicas:
+            kind, vel, restore = parse_bc(b)
+            check(lib().mxg_engine_add_replica(self._e, ptr(f64(o), ctypes.c_double), ptr(f64(d), ctypes.c_double),
+                                               ptr(i32(c), ctypes.c_int), ptr(i32(kind), ctypes.c_int),
+                                               ptr(f32(vel), ctypes.c_float), ptr(f32(restore), ctypes.c_float)),
+                  "add_replica")
         for (m, r, d, fl) in self._types:
             check(lib().mxg_engine_addtype(self._e, m, r, d, fl), "addtype")
-        for (p, a, b) in self._pots:
-            check(lib().mxg_engine_addpot(self._e, p._h, a, b), "addpot")
+        for (p, a, b, rep) in self._pots:
+            check(lib().mxg_engine_addpot_replica(self._e, rep, p._h, a, b), "addpot")
         for (t, v) in self._forces:
             check(lib().mxg_engine_add_singlebody_force(self._e, t, float(v[0]), float(v[1]), float(v[2])),
                   "add_singlebody_force")
@@ -360,14 +368,23 @@ class _Universe:
             tid = len(self._types) - 1
         return tid
 
-    def _add_particles(self, x, v, t):
+    def _add_particles(self, x, v, t, replica=0):
         first = len(self._t)
         self._sync_state()
         self._x = np.concatenate([self._x, np.asarray(x, dtype=np.float64)])
         self._v = np.concatenate([self._v, np.asarray(v, dtype=np.float32)])
         self._t = np.concatenate([self._t, np.asarray(t, dtype=np.int32)])
+        self._r = np.concatenate([self._r, np.full(len(t), int(replica), dtype=np.int32)])
         self._dirty = True
         return list(range(first, first + len(t)))
+
+    def add_replica(self, dim, cells, bc=None, origin=(0.0, 0.0, 0.0)):
+        """Adds an independent simulation box that steps together with the others
+        (batched ensembles); returns its replica index. Types, cutoff and dt are shared."""
+        self._sync_state()
+        self._replicas.append((list(origin), list(dim), list(cells), bc))
+        self._dirty = True
+        return len(self._replicas)
 
     def _add_bonds(self, pot, i, j, d):
         ii, jj = i32(i), i32(j)
@@ -377,13 +394,13 @@ class _Universe:
         self._dirty = True
         return list(range(first, first + len(ii)))
 
-    def bind(self, obj, a, b=None):
+    def bind(self, obj, a, b=None, replica=0):
         """Binds a potential to a pair of types, or a force to a type (MxBind.cpp:18-100)."""
         ta = a.id if isinstance(a, type) else int(a)
         if isinstance(obj, Potential):
             tb = ta if b is None else (b.id if isinstance(b, type) else int(b))
             self._sync_state()
-            self._pots.append((obj, ta, tb))
+            self._pots.append((obj, ta, tb, int(replica)))
             self._dirty = True
         elif isinstance(obj, _ConstantForce):
             self._sync_state()
@@ -409,10 +426,17 @@ class _Universe:
         if self._started or self._dirty:
             self._new_engine()
         n = len(self._t)
-        if n:
-            check(lib().mxg_engine_addparts(self._e, n, ptr(f64(self._x), ctypes.c_double),
-                                            ptr(f32(self._v), ctypes.c_float), ptr(i32(self._t), ctypes.c_int),
-                                            None), "addparts")
+        # particles go in id order; consecutive runs of one replica are added together
+        k = 0
+        while k < n:
+            rep = int(self._r[k])
+            e = k
+            while e < n and self._r[e] == rep:
+                e += 1
+            check(lib().mxg_engine_addparts_replica(self._e, rep, e - k, ptr(f64(self._x[k:e]), ctypes.c_double),
+                                                    ptr(f32(self._v[k:e]), ctypes.c_float),
+                                                    ptr(i32(self._t[k:e]), ctypes.c_int), None), "addparts")
+            k = e
         check(lib().mxg_engine_start(self._e, ctypes.c_void_p(self.stream) if self.stream else None),
               "engine_start")
         self._started = True
@@ -507,6 +531,11 @@ class _Universe:
         check(lib().mxg_engine_time_force(self._e, int(reps), ctypes.byref(ms)), "time_force")
         return ms.value
 
+    def autotune(self):
+        """Picks the force kernel's grid by timing candidates on the current state."""
+        self._ensure()
+        return check(lib().mxg_engine_autotune(self._e), "autotune")
+
     def candidate_pairs(self):
         self._ensure()
         c, i = ctypes.c_longlong(), ctypes.c_longlong()
@@ -555,8 +584,8 @@ def init(dim=(10.0, 10.0, 10.0), cutoff=1.0, cells=(4, 4, 4), dt=0.01, bc=None, 
     return universe
 
 
-def bind(obj, a, b=None):
-    return _require().bind(obj, a, b)
+def bind(obj, a, b=None, replica=0):
+    return _require().bind(obj, a, b, replica)
 
 
 def step(until=0, dt=0):

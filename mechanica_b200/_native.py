@@ -98,6 +98,13 @@ _SIGS = {
     "mxg_engine_kernel_times": ([_vp, _c_double_p, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int], ctypes.c_int),
     "mxg_engine_pair_counts": ([_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)],
                                ctypes.c_int),
+    "mxg_engine_add_replica": ([_vp, _c_double_p, _c_double_p, _c_int_p, _c_int_p, _c_float_p, _c_float_p],
+                               ctypes.c_int),
+    "mxg_engine_nr_replicas": ([_vp], ctypes.c_int),
+    "mxg_engine_addpot_replica": ([_vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "mxg_engine_addparts_replica": ([_vp, ctypes.c_int, ctypes.c_int, _c_double_p, _c_float_p, _c_int_p, _c_int_p],
+                                    ctypes.c_int),
+    "mxg_engine_autotune": ([_vp], ctypes.c_int),
     "mxg_kinetic_energy_noalloc": ([_vp, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp], ctypes.c_int),
 }
 

@@ -112,90 +112,24 @@ int upload(T *dst, const std::vector<T> &src, cudaStream_t st) {
 
 }  // namespace
 
-struct mxg_engine {
-    // ---- configuration ----
+/* One simulation box (a replica): the reference's space (space.h:136-263) with its
+ * cell grid, boundary kinds, cell-pair task list and the global index of its
+ * first cell in the engine's concatenated cell array. */
+struct Space {
     double origin[3], dim[3];
     int cells[3];
-    double cutoff;
     int bc_kind[6];
     float bc_vel[6][3];
     float bc_restore[6];
     unsigned period = 0;
-    int max_type = 0;
-    double dt = 0.01;
-    float max_dist_fraction = 0.05f;
-    unsigned rng_mode = 0;
-    int pruning = 0;  // 0: the reference's pruning, 1: same with the per-pair test on every grid, 2: none
-
-    // ---- space (space_init) ----
     int cdim[3];
     double h[3], ih[3];
     int ncells = 0;
+    int cell_offset = 0;
     std::vector<unsigned> cell_flags;
     std::vector<double> cell_origin;  // 3 per cell
-    std::vector<Task> tasks;
-
-    // ---- model ----
-    std::vector<TypeInfo> types;
-    std::vector<mxg::PotentialTable> pots;  // private copies
-    std::vector<int> pot_idx;               // max_type^2 (compacted to ntypes^2 at start)
-    std::vector<double> px;                 // staged positions (3 per particle)
-    std::vector<float> pv;
-    std::vector<int> ptype;
-    std::vector<BondInfo> bonds;
-
-    // ---- device ----
-    bool started = false;
-    cudaStream_t stream = nullptr;
-    cudaStream_t own_stream = nullptr;
-    int nparts = 0;
-    int ntypes = 0;
-    int cur = 0;
-    float4 *d_pos[2] = {nullptr, nullptr}, *d_vel[2] = {nullptr, nullptr};
-    float4 *d_force = nullptr;
-    int *d_cell_of[2] = {nullptr, nullptr};
-    int *d_new_cell = nullptr;
-    int *d_cell_start[2] = {nullptr, nullptr}, *d_cell_count[2] = {nullptr, nullptr};
-    int *d_in_count = nullptr, *d_out_count = nullptr, *d_in_list = nullptr;
-    int *d_slot_of_id = nullptr;
-    int *d_cell_rep = nullptr;
-    unsigned *d_cell_flags = nullptr;
-    int *d_nb_off = nullptr, *d_nb_cell = nullptr;
-    float4 *d_nb_shift = nullptr;
-    DevPot *d_pots = nullptr;
-    float *d_coef = nullptr;
-    int *d_pot_idx = nullptr;
-    DevType *d_types = nullptr;
-    DevSpace *d_spaces = nullptr;
-    SortAxes *d_axes = nullptr;
-    int2 *d_sort_bounds = nullptr;
-    double *d_epot_cell = nullptr, *d_ebond_slot = nullptr;
-    DevBond *d_bonds = nullptr;
-    unsigned *d_bond_flags = nullptr;
-    int *d_bond_off = nullptr, *d_bond_list = nullptr;
-    unsigned *d_status = nullptr;
-    unsigned long long *d_step = nullptr;
-    double *d_partials = nullptr, *d_energy = nullptr;
-    int energy_blocks = 64;
-    bool has_dpd = false;
-    int force_grid = 0;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    bool use_graphs = true;
-    std::vector<void *> allocations;
-
-    ~mxg_engine() {
-        for (int k = 0; k < 2; ++k)
-            if (graph[k]) cudaGraphExecDestroy(graph[k]);
-        for (void *p : allocations) cudaFree(p);
-        if (own_stream) cudaStreamDestroy(own_stream);
-    }
-
-    template <typename T>
-    int alloc(T **p, size_t n) {
-        int rc = dev_alloc(p, n);
-        if (rc == MXG_OK) allocations.push_back((void *)*p);
-        return rc;
-    }
+    std::vector<Task> tasks;          // local cell indices
+    std::vector<int> pot_idx;         // max_type^2 potential index per type pair (-1 none)
 
     int cellid(int i, int j, int k) const { return (i * cdim[1] + j) * cdim[2] + k; }
 
@@ -218,7 +152,40 @@ struct mxg_engine {
         return kSortlistID[sid];
     }
 
-    int build_space() {
+    /* engine_init / MxBoundaryConditions_Init: boundary kinds, periodicity and the
+     * raise of periodic axes to 3 cells. */
+    int configure(const double *o, const double *d, const int *c, const int *kinds, const float *vel,
+                  const float *restore) {
+        for (int k = 0; k < 3; ++k) {
+            origin[k] = o[k];
+            dim[k] = d[k];
+            cells[k] = c[k];
+            if (c[k] < 1 || !(d[k] > o[k])) return MXG_ERR_ARG;
+        }
+        for (int f = 0; f < 6; ++f) {
+            int kind = kinds ? kinds[f] : MXG_BOUNDARY_PERIODIC;
+            const bool noslip = kind == MXG_BOUNDARY_NO_SLIP;
+            if (noslip) kind = MXG_BOUNDARY_VELOCITY;  // no-slip = zero-velocity wall
+            bc_kind[f] = kind;
+            for (int q = 0; q < 3; ++q) bc_vel[f][q] = (vel && !noslip) ? vel[3 * f + q] : 0.f;
+            bc_restore[f] = restore ? restore[f] : 1.f;
+        }
+        // a face pair is periodic when either face is (check_periodicy sets both)
+        const int faces[3][2] = {{MXG_FACE_LEFT, MXG_FACE_RIGHT}, {MXG_FACE_FRONT, MXG_FACE_BACK},
+                                 {MXG_FACE_BOTTOM, MXG_FACE_TOP}};
+        period = 0;
+        for (int k = 0; k < 3; ++k) {
+            const bool lo = bc_kind[faces[k][0]] & MXG_BOUNDARY_PERIODIC, hi = bc_kind[faces[k][1]] & MXG_BOUNDARY_PERIODIC;
+            if (lo || hi) {
+                bc_kind[faces[k][0]] = bc_kind[faces[k][1]] = MXG_BOUNDARY_PERIODIC;
+                period |= 1u << k;
+                if (cells[k] < 3) cells[k] = 3;  // MxBoundaryConditions_Init: >= 3 periodic cells
+            }
+        }
+        return MXG_OK;
+    }
+
+    int build(double cutoff) {
         // engine_init: L = (dim - origin)/cells; space_init: cdim = floor(dim/L), h = dim/cdim
         for (int k = 0; k < 3; ++k) {
             const double L = (dim[k] - origin[k]) / cells[k];
@@ -306,7 +273,7 @@ struct mxg_engine {
         return MXG_OK;
     }
 
-    /* space_addpart's placement plus the first shuffle: cell index and
+    /* space_addpart's placement plus the first shuffle: local cell index and
      * cell-relative float position. */
     int place(const double *x, int &cell, float *xr) const {
         int ind[3];
@@ -331,51 +298,167 @@ struct mxg_engine {
         return MXG_OK;
     }
 
-    DevSpace space_desc() const {
+    /* runner_dopair.cpp:132-136: bias = |h|, dscale = SHRT_MAX/(2 bias),
+     * dmaxdist = 2 + dscale*(cutoff + 2*maxdx) with maxdx = 0; FP32. */
+    float sort_bias() const { return (float)std::sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]); }
+    float sort_dscale() const { return (float)32767 / (2 * sort_bias()); }
+    int dmaxdist(double cutoff) const { return (int)(2 + sort_dscale() * ((float)cutoff + 2 * 0.0f)); }
+    int dnshift(const float *shift) const {
+        const float ns = std::sqrt(shift[0] * shift[0] + shift[1] * shift[1] + shift[2] * shift[2]);
+        return (int)(sort_dscale() * ns);
+    }
+};
+
+struct mxg_engine {
+    // ---- configuration shared by all replicas ----
+    double cutoff;
+    int max_type = 0;
+    double dt = 0.01;
+    float max_dist_fraction = 0.05f;
+    unsigned rng_mode = 0;
+    int pruning = 0;  // 0: the reference's pruning, 1: same with the per-pair test on every grid, 2: none
+
+    // ---- replicas ----
+    std::vector<Space> spaces;
+    int ncells = 0;  // all replicas
+
+    // ---- model ----
+    std::vector<TypeInfo> types;
+    std::vector<mxg::PotentialTable> pots;  // private copies
+    std::vector<double> px;                 // staged positions (3 per particle)
+    std::vector<float> pv;
+    std::vector<int> ptype;
+    std::vector<int> prep;                  // replica of each particle
+    std::vector<BondInfo> bonds;
+
+    // ---- device ----
+    bool started = false;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    int nparts = 0;
+    int ntypes = 0;
+    int cur = 0;
+    float4 *d_pos[2] = {nullptr, nullptr}, *d_vel[2] = {nullptr, nullptr};
+    float4 *d_force = nullptr;
+    int *d_cell_of[2] = {nullptr, nullptr};
+    int *d_new_cell = nullptr;
+    int *d_cell_start[2] = {nullptr, nullptr}, *d_cell_count[2] = {nullptr, nullptr};
+    int *d_in_count = nullptr, *d_out_count = nullptr, *d_in_list = nullptr;
+    int *d_slot_of_id = nullptr;
+    int *d_cell_rep = nullptr;
+    unsigned *d_cell_flags = nullptr;
+    int *d_nb_off = nullptr, *d_nb_cell = nullptr;
+    float4 *d_nb_shift = nullptr;
+    DevPot *d_pots = nullptr;
+    float *d_coef = nullptr;
+    int *d_pot_idx = nullptr;
+    DevType *d_types = nullptr;
+    DevSpace *d_spaces = nullptr;
+    SortAxes *d_axes = nullptr;
+    int2 *d_sort_bounds = nullptr;
+    double *d_epot_cell = nullptr, *d_ebond_slot = nullptr;
+    DevBond *d_bonds = nullptr;
+    unsigned *d_bond_flags = nullptr;
+    int *d_bond_off = nullptr, *d_bond_list = nullptr;
+    unsigned *d_status = nullptr;
+    unsigned long long *d_step = nullptr;
+    double *d_partials = nullptr, *d_energy = nullptr;
+    int energy_blocks = 64;
+    bool has_dpd = false;
+    int force_grid = 0;
+    int num_sms = 148;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool use_graphs = true;
+    std::vector<void *> allocations;
+
+    ~mxg_engine() {
+        for (int k = 0; k < 2; ++k)
+            if (graph[k]) cudaGraphExecDestroy(graph[k]);
+        for (void *p : allocations) cudaFree(p);
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+
+    template <typename T>
+    int alloc(T **p, size_t n) {
+        int rc = dev_alloc(p, n);
+        if (rc == MXG_OK) allocations.push_back((void *)*p);
+        return rc;
+    }
+
+    DevSpace space_desc(int r, int pot_offset) const {
+        const Space &sp = spaces[r];
         DevSpace S;
         memset(&S, 0, sizeof(S));
         const float dtf = (float)dt;
         for (int k = 0; k < 3; ++k) {
-            S.hd[k] = h[k];
-            S.h[k] = (float)h[k];
-            S.h2[k] = (float)(2. * h[k]);
+            S.hd[k] = sp.h[k];
+            S.h[k] = (float)sp.h[k];
+            S.h2[k] = (float)(2. * sp.h[k]);
             S.maxv[k] = (S.h[k] * max_dist_fraction) / dtf;
             S.maxv2[k] = S.maxv[k] * S.maxv[k];
             S.maxx[k] = S.h[k] * max_dist_fraction;
             S.maxx2[k] = S.maxx[k] * S.maxx[k];
-            S.cdim[k] = cdim[k];
+            S.cdim[k] = sp.cdim[k];
         }
         S.dt = dtf;
         const float cf = (float)cutoff;
         S.cut2_pair = cf * cf;                  // runner_dopair: float cutoff squared
         S.cut2_self = (float)(cutoff * cutoff);  // runner_doself: s->cutoff2 (double) as float
-        S.cell_offset = 0;
-        S.ncells = ncells;
-        S.pot_offset = 0;
+        S.cell_offset = sp.cell_offset;
+        S.ncells = sp.ncells;
+        S.pot_offset = pot_offset;
         for (int f = 0; f < 6; ++f) {
-            S.bc_kind[f] = (unsigned)bc_kind[f];
-            for (int q = 0; q < 3; ++q) S.bc_vel[f][q] = bc_vel[f][q];
-            S.bc_restore[f] = bc_restore[f];
+            S.bc_kind[f] = (unsigned)sp.bc_kind[f];
+            for (int q = 0; q < 3; ++q) S.bc_vel[f][q] = sp.bc_vel[f][q];
+            S.bc_restore[f] = sp.bc_restore[f];
         }
         S.rng_mode = rng_mode;
         // the per-pair projection test can only drop a pair inside the cutoff when
         // the cells are not cubic; the cell-pair exit test applies to every grid
-        const bool cubic = h[0] == h[1] && h[1] == h[2];
+        const bool cubic = sp.h[0] == sp.h[1] && sp.h[1] == sp.h[2];
         S.prune = pruning == 2 ? 0 : (2 | ((pruning == 1 || !cubic) ? 1 : 0));
-        S.dmaxdist = dmaxdist();
-        S.sort_bias = sort_bias();
-        S.sort_dscale = sort_dscale();
+        S.dmaxdist = sp.dmaxdist(cutoff);
+        S.sort_bias = sp.sort_bias();
+        S.sort_dscale = sp.sort_dscale();
         return S;
     }
 
-    /* runner_dopair.cpp:132-136: bias = |h|, dscale = SHRT_MAX/(2 bias),
-     * dmaxdist = 2 + dscale*(cutoff + 2*maxdx) with maxdx = 0; FP32. */
-    float sort_bias() const { return (float)std::sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]); }
-    float sort_dscale() const { return (float)32767 / (2 * sort_bias()); }
-    int dmaxdist() const { return (int)(2 + sort_dscale() * ((float)cutoff + 2 * 0.0f)); }
-    int dnshift(const float *shift) const {
-        const float ns = std::sqrt(shift[0] * shift[0] + shift[1] * shift[1] + shift[2] * shift[2]);
-        return (int)(sort_dscale() * ns);
+    /* Places every staged particle in its replica (global cell index and
+     * cell-relative position) and orders them by cell, then id. */
+    int stage(std::vector<float4> &hpos, std::vector<float4> &hvel, std::vector<int> &hcell_of,
+              std::vector<int> &hslot, std::vector<int> &hcount, std::vector<int> &hstart) const {
+        const int n = (int)ptype.size();
+        std::vector<int> cell(n);
+        std::vector<float> xr(3 * (size_t)n);
+        for (int p = 0; p < n; ++p) {
+            const Space &sp = spaces[prep[p]];
+            int lc;
+            int rc = sp.place(&px[3 * (size_t)p], lc, &xr[3 * (size_t)p]);
+            if (rc != MXG_OK) return rc;
+            cell[p] = sp.cell_offset + lc;
+        }
+        std::vector<int> order(n);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cell[a] < cell[b]; });
+        hpos.assign(n, make_float4(0.f, 0.f, 0.f, 0.f));
+        hvel.assign(n, make_float4(0.f, 0.f, 0.f, 0.f));
+        hcell_of.assign(n, 0);
+        hslot.assign(n, 0);
+        hcount.assign(ncells, 0);
+        hstart.assign(ncells + 1, 0);
+        for (int s = 0; s < n; ++s) {
+            const int p = order[s];
+            hpos[s] = make_float4(xr[3 * (size_t)p], xr[3 * (size_t)p + 1], xr[3 * (size_t)p + 2], 0.f);
+            int t = ptype[p];
+            memcpy(&hpos[s].w, &t, 4);
+            hvel[s] = make_float4(pv[3 * (size_t)p], pv[3 * (size_t)p + 1], pv[3 * (size_t)p + 2], 0.f);
+            memcpy(&hvel[s].w, &p, 4);
+            hcell_of[s] = cell[p];
+            hslot[p] = s;
+            hcount[cell[p]]++;
+        }
+        for (int c = 0; c < ncells; ++c) hstart[c + 1] = hstart[c] + hcount[c];
+        return MXG_OK;
     }
 
     EngineView view(int b) const {
@@ -428,6 +511,7 @@ struct mxg_engine {
     }
 
     int start(cudaStream_t st);
+    int build_graphs();
     int load_state(const double *x, const float *v, int n);
 };
 
@@ -441,50 +525,40 @@ int mxg_engine::start(cudaStream_t st) {
     nparts = (int)ptype.size();
     ntypes = std::max(1, (int)types.size());
     // ---- host staging: placement, ordering ----
-    std::vector<int> cell(nparts);
-    std::vector<float> xr(3 * (size_t)nparts);
-    for (int p = 0; p < nparts; ++p) {
-        int rc = place(&px[3 * (size_t)p], cell[p], &xr[3 * (size_t)p]);
-        if (rc != MXG_OK) return rc;
-    }
-    std::vector<int> order(nparts);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cell[a] < cell[b]; });
-    std::vector<float4> hpos(nparts), hvel(nparts);
-    std::vector<int> hcell_of(nparts), hslot(nparts);
-    std::vector<int> hcount(ncells, 0), hstart(ncells + 1, 0);
-    for (int s = 0; s < nparts; ++s) {
-        const int p = order[s];
-        hpos[s] = make_float4(xr[3 * (size_t)p], xr[3 * (size_t)p + 1], xr[3 * (size_t)p + 2], 0.f);
-        int t = ptype[p];
-        memcpy(&hpos[s].w, &t, 4);
-        hvel[s] = make_float4(pv[3 * (size_t)p], pv[3 * (size_t)p + 1], pv[3 * (size_t)p + 2], 0.f);
-        memcpy(&hvel[s].w, &p, 4);
-        hcell_of[s] = cell[p];
-        hslot[p] = s;
-        hcount[cell[p]]++;
-    }
-    for (int c = 0; c < ncells; ++c) hstart[c + 1] = hstart[c] + hcount[c];
+    std::vector<float4> hpos, hvel;
+    std::vector<int> hcell_of, hslot, hcount, hstart;
+    int rc = stage(hpos, hvel, hcell_of, hslot, hcount, hstart);
+    if (rc != MXG_OK) return rc;
 
-    // ---- neighbour entries from the task list ----
+    // ---- neighbour entries from each replica's task list (global cell indices) ----
     std::vector<std::vector<std::pair<int, float4>>> nb(ncells);
-    for (const Task &t : tasks) {
-        if (t.type == kTaskSelf) {
-            float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
-            int role = kRoleSelf;
-            memcpy(&e.w, &role, 4);
-            nb[t.i].push_back({t.i, e});
-        } else if (t.type == kTaskPair) {
-            int ci = t.i, cj = t.j;
-            float shift[3];
-            const int sid = getsid(ci, cj, shift);  // runner_dopair recomputes the shift (and flip) per task
-            const int dn = dnshift(shift);
-            float4 e1 = make_float4(shift[0], shift[1], shift[2], 0.f), e2 = e1;
-            int r1 = kRoleFirst | (sid << 2) | (dn << 8), r2 = kRoleSecond | (sid << 2) | (dn << 8);
-            memcpy(&e1.w, &r1, 4);
-            memcpy(&e2.w, &r2, 4);
-            nb[ci].push_back({cj, e1});
-            nb[cj].push_back({ci, e2});
+    std::vector<int> hrep(ncells, 0);
+    std::vector<unsigned> hcflags(ncells, 0u);
+    for (int r = 0; r < (int)spaces.size(); ++r) {
+        const Space &sp = spaces[r];
+        const int off = sp.cell_offset;
+        for (int c = 0; c < sp.ncells; ++c) {
+            hrep[off + c] = r;
+            hcflags[off + c] = sp.cell_flags[c];
+        }
+        for (const Task &t : sp.tasks) {
+            if (t.type == kTaskSelf) {
+                float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+                int role = kRoleSelf;
+                memcpy(&e.w, &role, 4);
+                nb[off + t.i].push_back({off + t.i, e});
+            } else if (t.type == kTaskPair) {
+                int ci = t.i, cj = t.j;
+                float shift[3];
+                const int sid = sp.getsid(ci, cj, shift);  // runner_dopair recomputes the shift (and flip)
+                const int dn = sp.dnshift(shift);
+                float4 e1 = make_float4(shift[0], shift[1], shift[2], 0.f), e2 = e1;
+                int r1 = kRoleFirst | (sid << 2) | (dn << 8), r2 = kRoleSecond | (sid << 2) | (dn << 8);
+                memcpy(&e1.w, &r1, 4);
+                memcpy(&e2.w, &r2, 4);
+                nb[off + ci].push_back({off + cj, e1});
+                nb[off + cj].push_back({off + ci, e2});
+            }
         }
     }
     std::vector<int> nb_off(ncells + 1, 0), nb_cell;
@@ -497,7 +571,7 @@ int mxg_engine::start(cudaStream_t st) {
         }
     }
 
-    // ---- potentials, types, space ----
+    // ---- potentials, types, replicas ----
     std::vector<DevPot> hp;
     std::vector<float> coef;
     has_dpd = false;
@@ -523,9 +597,15 @@ int mxg_engine::start(cudaStream_t st) {
         coef.insert(coef.end(), t.c.begin(), t.c.end());
         hp.push_back(d);
     }
-    std::vector<int> hpidx((size_t)ntypes * ntypes, -1);
-    for (int a = 0; a < (int)types.size(); ++a)
-        for (int b = 0; b < (int)types.size(); ++b) hpidx[a * ntypes + b] = pot_idx[a * max_type + b];
+    const int tt = ntypes * ntypes;
+    std::vector<int> hpidx((size_t)tt * spaces.size(), -1);
+    std::vector<DevSpace> hs;
+    for (int r = 0; r < (int)spaces.size(); ++r) {
+        for (int a = 0; a < (int)types.size(); ++a)
+            for (int b = 0; b < (int)types.size(); ++b)
+                hpidx[(size_t)r * tt + a * ntypes + b] = spaces[r].pot_idx[a * max_type + b];
+        hs.push_back(space_desc(r, r * tt));
+    }
     std::vector<DevType> ht(ntypes);
     for (int a = 0; a < (int)types.size(); ++a) {
         DevType &d = ht[a];
@@ -540,11 +620,9 @@ int mxg_engine::start(cudaStream_t st) {
         d.fz = types[a].force[2];
         d.has_force = types[a].has_force ? 1 : 0;
     }
-    std::vector<DevSpace> hs(1, space_desc());
     std::vector<SortAxes> haxes(1);
     for (int q = 0; q < 13; ++q)
         for (int k = 0; k < 3; ++k) haxes[0].n[q][k] = (float)kCellShift[q][k];
-    std::vector<int> hrep(ncells, 0);
 
     // ---- bonds: CSR by particle id ----
     std::vector<DevBond> hb;
@@ -552,6 +630,7 @@ int mxg_engine::start(cudaStream_t st) {
     std::vector<int> boff(nparts + 1, 0), blist;
     for (const BondInfo &b : bonds) {
         if (b.i < 0 || b.i >= nparts || b.j < 0 || b.j >= nparts) return MXG_ERR_BOND;
+        if (prep[b.i] != prep[b.j]) return MXG_ERR_BOND;  // a bond cannot span two replicas
         boff[b.i + 1]++;
         if (b.j != b.i) boff[b.j + 1]++;
     }
@@ -574,7 +653,7 @@ int mxg_engine::start(cudaStream_t st) {
     }
 
     // ---- device allocation ----
-    int rc = MXG_OK;
+    rc = MXG_OK;
     for (int b = 0; b < 2; ++b) {
         rc |= alloc(&d_pos[b], nparts);
         rc |= alloc(&d_vel[b], nparts);
@@ -622,7 +701,7 @@ int mxg_engine::start(cudaStream_t st) {
     if ((rc = upload(d_pos[0], hpos, stream)) || (rc = upload(d_vel[0], hvel, stream)) ||
         (rc = upload(d_cell_of[0], hcell_of, stream)) || (rc = upload(d_cell_start[0], hstart, stream)) ||
         (rc = upload(d_cell_count[0], hcount, stream)) || (rc = upload(d_slot_of_id, hslot, stream)) ||
-        (rc = upload(d_cell_rep, hrep, stream)) || (rc = upload(d_cell_flags, cell_flags, stream)) ||
+        (rc = upload(d_cell_rep, hrep, stream)) || (rc = upload(d_cell_flags, hcflags, stream)) ||
         (rc = upload(d_nb_off, nb_off, stream)) || (rc = upload(d_nb_cell, nb_cell, stream)) ||
         (rc = upload(d_nb_shift, nb_shift, stream)) || (rc = upload(d_pots, hp, stream)) ||
         (rc = upload(d_coef, coef, stream)) || (rc = upload(d_pot_idx, hpidx, stream)) ||
@@ -635,10 +714,20 @@ int mxg_engine::start(cudaStream_t st) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    num_sms = sms;
+    configure_force_kernels();
     force_grid = std::max(1, std::min((ncells + kWarpsPerBlock - 1) / kWarpsPerBlock, sms * 16));
     cur = 0;
     started = true;
+    return build_graphs();
+}
 
+int mxg_engine::build_graphs() {
+    for (int k = 0; k < 2; ++k)
+        if (graph[k]) {
+            cudaGraphExecDestroy(graph[k]);
+            graph[k] = nullptr;
+        }
     if (use_graphs && nparts > 0) {
         for (int b = 0; b < 2; ++b) {
             cudaGraph_t g;
@@ -660,30 +749,10 @@ int mxg_engine::load_state(const double *x, const float *v, int n) {
         if (v)
             for (int k = 0; k < 3; ++k) pv[3 * (size_t)p + k] = v[3 * (size_t)p + k];
     }
-    std::vector<int> cell(nparts);
-    std::vector<float> xr(3 * (size_t)nparts);
-    for (int p = 0; p < nparts; ++p) {
-        int rc = place(&px[3 * (size_t)p], cell[p], &xr[3 * (size_t)p]);
-        if (rc != MXG_OK) return rc;
-    }
-    std::vector<int> order(nparts);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cell[a] < cell[b]; });
-    std::vector<float4> hpos(nparts), hvel(nparts);
-    std::vector<int> hcell_of(nparts), hslot(nparts), hcount(ncells, 0), hstart(ncells + 1, 0);
-    for (int s = 0; s < nparts; ++s) {
-        const int p = order[s];
-        hpos[s] = make_float4(xr[3 * (size_t)p], xr[3 * (size_t)p + 1], xr[3 * (size_t)p + 2], 0.f);
-        int t = ptype[p];
-        memcpy(&hpos[s].w, &t, 4);
-        hvel[s] = make_float4(pv[3 * (size_t)p], pv[3 * (size_t)p + 1], pv[3 * (size_t)p + 2], 0.f);
-        memcpy(&hvel[s].w, &p, 4);
-        hcell_of[s] = cell[p];
-        hslot[p] = s;
-        hcount[cell[p]]++;
-    }
-    for (int c = 0; c < ncells; ++c) hstart[c + 1] = hstart[c] + hcount[c];
-    int rc;
+    std::vector<float4> hpos, hvel;
+    std::vector<int> hcell_of, hslot, hcount, hstart;
+    int rc = stage(hpos, hvel, hcell_of, hslot, hcount, hstart);
+    if (rc != MXG_OK) return rc;
     if ((rc = upload(d_pos[cur], hpos, stream)) || (rc = upload(d_vel[cur], hvel, stream)) ||
         (rc = upload(d_cell_of[cur], hcell_of, stream)) || (rc = upload(d_cell_start[cur], hstart, stream)) ||
         (rc = upload(d_cell_count[cur], hcount, stream)) || (rc = upload(d_slot_of_id, hslot, stream)))
@@ -792,44 +861,33 @@ int mxg_engine_init(const double *origin, const double *dim, const int *cells, d
     if (!origin || !dim || !cells || !out) return MXG_ERR_NULL;
     if (!(cutoff > 0) || max_type <= 0 || max_type > kMaxTypes) return MXG_ERR_ARG;
     mxg_engine *e = new mxg_engine;
-    for (int k = 0; k < 3; ++k) {
-        e->origin[k] = origin[k];
-        e->dim[k] = dim[k];
-        e->cells[k] = cells[k];
-        if (cells[k] < 1 || !(dim[k] > origin[k])) {
-            delete e;
-            return MXG_ERR_ARG;
-        }
-    }
     e->cutoff = cutoff;
-    for (int f = 0; f < 6; ++f) {
-        int kind = bc_kind ? bc_kind[f] : MXG_BOUNDARY_PERIODIC;
-        if (kind == MXG_BOUNDARY_NO_SLIP) kind = MXG_BOUNDARY_VELOCITY;  // no-slip = zero-velocity wall
-        e->bc_kind[f] = kind;
-        for (int q = 0; q < 3; ++q) e->bc_vel[f][q] = (bc_velocity && bc_kind && bc_kind[f] != MXG_BOUNDARY_NO_SLIP) ? bc_velocity[3 * f + q] : 0.f;
-        e->bc_restore[f] = bc_restore ? bc_restore[f] : 1.f;
-    }
-    // a face pair is periodic only when both faces are (check_periodicy sets both)
-    const int faces[3][2] = {{MXG_FACE_LEFT, MXG_FACE_RIGHT}, {MXG_FACE_FRONT, MXG_FACE_BACK},
-                             {MXG_FACE_BOTTOM, MXG_FACE_TOP}};
-    for (int k = 0; k < 3; ++k) {
-        const bool lo = e->bc_kind[faces[k][0]] & MXG_BOUNDARY_PERIODIC, hi = e->bc_kind[faces[k][1]] & MXG_BOUNDARY_PERIODIC;
-        if (lo || hi) {
-            e->bc_kind[faces[k][0]] = e->bc_kind[faces[k][1]] = MXG_BOUNDARY_PERIODIC;
-            e->period |= 1u << k;
-            if (e->cells[k] < 3) e->cells[k] = 3;  // MxBoundaryConditions_Init: >= 3 periodic cells
-        }
-    }
     e->max_type = max_type;
-    e->pot_idx.assign((size_t)max_type * max_type, -1);
-    int rc = e->build_space();
-    if (rc != MXG_OK) {
+    const int rc = mxg_engine_add_replica(e, origin, dim, cells, bc_kind, bc_velocity, bc_restore);
+    if (rc < 0) {
         delete e;
         return rc;
     }
     *out = e;
     return MXG_OK;
 }
+
+int mxg_engine_add_replica(mxg_engine *e, const double *origin, const double *dim, const int *cells,
+                           const int *bc_kind, const float *bc_velocity, const float *bc_restore) {
+    if (!e || !origin || !dim || !cells) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    Space sp;
+    int rc = sp.configure(origin, dim, cells, bc_kind, bc_velocity, bc_restore);
+    if (rc != MXG_OK) return rc;
+    if ((rc = sp.build(e->cutoff)) != MXG_OK) return rc;
+    sp.cell_offset = e->ncells;
+    sp.pot_idx.assign((size_t)e->max_type * e->max_type, -1);
+    e->ncells += sp.ncells;
+    e->spaces.push_back(std::move(sp));
+    return (int)e->spaces.size() - 1;
+}
+
+int mxg_engine_nr_replicas(const mxg_engine *e) { return e ? (int)e->spaces.size() : MXG_ERR_NULL; }
 
 int mxg_engine_set_dt(mxg_engine *e, double dt, double max_dist_fraction) {
     if (!e) return MXG_ERR_NULL;
@@ -872,16 +930,21 @@ int mxg_engine_addtype(mxg_engine *e, double mass, double radius, int dynamics, 
     return (int)e->types.size() - 1;
 }
 
-int mxg_engine_addpot(mxg_engine *e, const mxg_potential *p, int i, int j) {
+int mxg_engine_addpot_replica(mxg_engine *e, int rep, const mxg_potential *p, int i, int j) {
     if (!e || !p) return MXG_ERR_NULL;
     if (e->started) return MXG_ERR_STATE;
     const int nt = (int)e->types.size();
-    if (i < 0 || i >= nt || j < 0 || j >= nt) return MXG_ERR_RANGE;
+    if (i < 0 || i >= nt || j < 0 || j >= nt || rep < 0 || rep >= (int)e->spaces.size()) return MXG_ERR_RANGE;
     e->pots.push_back(p->t);
     const int idx = (int)e->pots.size() - 1;
-    e->pot_idx[i * e->max_type + j] = idx;  // engine_addpot overwrites: one potential per pair
-    e->pot_idx[j * e->max_type + i] = idx;
+    std::vector<int> &m = e->spaces[rep].pot_idx;
+    m[i * e->max_type + j] = idx;  // engine_addpot overwrites: one potential per pair
+    m[j * e->max_type + i] = idx;
     return MXG_OK;
+}
+
+int mxg_engine_addpot(mxg_engine *e, const mxg_potential *p, int i, int j) {
+    return mxg_engine_addpot_replica(e, 0, p, i, j);
 }
 
 int mxg_engine_add_singlebody_force(mxg_engine *e, int type, float fx, float fy, float fz) {
@@ -896,14 +959,17 @@ int mxg_engine_add_singlebody_force(mxg_engine *e, int type, float fx, float fy,
     return MXG_OK;
 }
 
-int mxg_engine_addparts(mxg_engine *e, int n, const double *x, const float *v, const int *type, int *ids_out) {
+int mxg_engine_addparts_replica(mxg_engine *e, int rep, int n, const double *x, const float *v, const int *type,
+                                int *ids_out) {
     if (!e || (n > 0 && (!x || !type))) return MXG_ERR_NULL;
     if (e->started) return MXG_ERR_STATE;
+    if (rep < 0 || rep >= (int)e->spaces.size()) return MXG_ERR_RANGE;
+    const Space &sp = e->spaces[rep];
     for (int k = 0; k < n; ++k) {
         if (type[k] < 0 || type[k] >= (int)e->types.size()) return MXG_ERR_RANGE;
         int cell;
         float xr[3];
-        if (e->place(&x[3 * (size_t)k], cell, xr) != MXG_OK) return MXG_ERR_SPACE;
+        if (sp.place(&x[3 * (size_t)k], cell, xr) != MXG_OK) return MXG_ERR_SPACE;
     }
     const int first = (int)e->ptype.size();
     for (int k = 0; k < n; ++k) {
@@ -912,9 +978,14 @@ int mxg_engine_addparts(mxg_engine *e, int n, const double *x, const float *v, c
             e->pv.push_back(v ? v[3 * (size_t)k + q] : 0.f);
         }
         e->ptype.push_back(type[k]);
+        e->prep.push_back(rep);
         if (ids_out) ids_out[k] = first + k;
     }
     return MXG_OK;
+}
+
+int mxg_engine_addparts(mxg_engine *e, int n, const double *x, const float *v, const int *type, int *ids_out) {
+    return mxg_engine_addparts_replica(e, 0, n, x, v, type, ids_out);
 }
 
 int mxg_engine_addbonds(mxg_engine *e, int n, const int *i, const int *j, const mxg_potential *p,
@@ -1003,9 +1074,11 @@ int mxg_engine_unload(mxg_engine *e, int n, double *x, float *v, float *f, int *
         memcpy(&id, &hv[s].w, 4);
         if (id < 0 || id >= n) continue;
         const int c = hc[s];
+        const Space &sp = e->spaces[e->prep[id]];
+        const int lc = c - sp.cell_offset;
         const float xr[3] = {hp[s].x, hp[s].y, hp[s].z};
         for (int k = 0; k < 3; ++k) {
-            if (x) x[3 * (size_t)id + k] = e->cell_origin[3 * (size_t)c + k] + xr[k];
+            if (x) x[3 * (size_t)id + k] = sp.cell_origin[3 * (size_t)lc + k] + xr[k];
             if (xrel) xrel[3 * (size_t)id + k] = xr[k];
         }
         if (v) {
@@ -1054,14 +1127,15 @@ double mxg_engine_kinetic_energy(mxg_engine *e) {
 
 int mxg_engine_tasks(const mxg_engine *e, int *out, int cap) {
     if (!e) return MXG_ERR_NULL;
-    const int n = (int)e->tasks.size();
+    const std::vector<Task> &tasks = e->spaces[0].tasks;
+    const int n = (int)tasks.size();
     if (!out) return n;
     if (cap < 4 * n) return -n;
     for (int k = 0; k < n; ++k) {
-        out[4 * k] = e->tasks[k].type;
-        out[4 * k + 1] = e->tasks[k].flags;
-        out[4 * k + 2] = e->tasks[k].i;
-        out[4 * k + 3] = e->tasks[k].j;
+        out[4 * k] = tasks[k].type;
+        out[4 * k + 1] = tasks[k].flags;
+        out[4 * k + 2] = tasks[k].i;
+        out[4 * k + 3] = tasks[k].j;
     }
     return n;
 }
@@ -1078,12 +1152,13 @@ int mxg_engine_bond_flags(mxg_engine *e, unsigned *out, int cap) {
 
 int mxg_engine_space_info(const mxg_engine *e, int *cdim, double *h, int *nr_cells, unsigned *period) {
     if (!e) return MXG_ERR_NULL;
+    const Space &sp = e->spaces[0];
     for (int k = 0; k < 3; ++k) {
-        if (cdim) cdim[k] = e->cdim[k];
-        if (h) h[k] = e->h[k];
+        if (cdim) cdim[k] = sp.cdim[k];
+        if (h) h[k] = sp.h[k];
     }
-    if (nr_cells) *nr_cells = e->ncells;
-    if (period) *period = e->period;
+    if (nr_cells) *nr_cells = sp.ncells;
+    if (period) *period = sp.period;
     return MXG_OK;
 }
 
@@ -1155,6 +1230,44 @@ int mxg_engine_time_force(mxg_engine *e, int reps, double *ms) {
     return MXG_OK;
 }
 
+/* A small autotuner for the force kernel's grid: candidate CTAs per SM are
+ * timed on the current state (mean of a few launches each) and the fastest is
+ * kept; the step graphs are re-captured with it. */
+int mxg_engine_autotune(mxg_engine *e) {
+    if (!e) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    if (e->nparts == 0) return MXG_OK;
+    const int cands[] = {2, 4, 6, 8, 12, 16, 24, 32};
+    const int max_grid = (e->ncells + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    int best = e->force_grid, best_per_sm = 0;
+    float best_ms = 1e30f;
+    cudaEvent_t a, b;
+    CUDA_TRY(cudaEventCreate(&a));
+    CUDA_TRY(cudaEventCreate(&b));
+    const EngineView v = e->view(e->cur);
+    for (int per_sm : cands) {
+        const int grid = std::max(1, std::min(max_grid, e->num_sms * per_sm));
+        launch_force(v, e->has_dpd, grid, e->stream);  // warm
+        CUDA_TRY(cudaEventRecord(a, e->stream));
+        for (int r = 0; r < 5; ++r) launch_force(v, e->has_dpd, grid, e->stream);
+        CUDA_TRY(cudaEventRecord(b, e->stream));
+        CUDA_TRY(cudaEventSynchronize(b));
+        float t = 0.f;
+        cudaEventElapsedTime(&t, a, b);
+        if (t < best_ms) {
+            best_ms = t;
+            best = grid;
+            best_per_sm = per_sm;
+        }
+        if (grid == max_grid) break;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    e->force_grid = best;
+    const int rc = e->build_graphs();
+    return rc != MXG_OK ? rc : best_per_sm;
+}
+
 int mxg_engine_kernel_times(mxg_engine *e, double *ms, long long *launches, int nkernels) {
     if (!e) return MXG_ERR_NULL;
     for (int k = 0; k < nkernels; ++k) {
@@ -1173,12 +1286,14 @@ int mxg_engine_pair_counts(mxg_engine *e, long long *candidates, long long *inte
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     CUDA_TRY(cudaMemcpy(cnt.data(), e->d_cell_count[e->cur], sizeof(int) * e->ncells, cudaMemcpyDeviceToHost));
     long long cand = 0;
-    for (const Task &t : e->tasks) {
-        if (t.type == kTaskSelf)
-            cand += (long long)cnt[t.i] * (cnt[t.i] - 1) / 2;
-        else if (t.type == kTaskPair)
-            cand += (long long)cnt[t.i] * cnt[t.j];
-    }
+    for (const Space &sp : e->spaces)
+        for (const Task &t : sp.tasks) {
+            const int a = sp.cell_offset + t.i, b = sp.cell_offset + t.j;
+            if (t.type == kTaskSelf)
+                cand += (long long)cnt[a] * (cnt[a] - 1) / 2;
+            else if (t.type == kTaskPair)
+                cand += (long long)cnt[a] * cnt[b];
+        }
     if (candidates) *candidates = cand;
     if (interacting) {
         // one statistics launch of the force kernel counts the interacting pairs

@@ -25,12 +25,6 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-__device__ __forceinline__ int next_pow2(int n) {
-    int p = 1;
-    while (p < n) p <<= 1;
-    return p;
-}
-
 /* Three normal deviates from one Philox draw (Box-Muller on two pairs). */
 __device__ __forceinline__ void philox_normal3(unsigned long long step, unsigned a, unsigned b, float &g0,
                                                float &g1, float &g2) {
@@ -95,27 +89,197 @@ __global__ void sort_bounds_kernel(EngineView v) {
 /* ------------------------------------------------------------------------ */
 
 /*
- * One warp per cell i (grid-stride). The warp's lanes are split into G groups
- * of P = next_pow2(count) lanes: lane (il, g) owns particle il of the cell and
- * the g-th share of every neighbour cell's particles. Neighbour particles are
- * staged 32 at a time in shared memory (coalesced float4 loads) and read back
- * as broadcasts; each lane accumulates the force on its own particle in
- * registers and the G partial sums are combined with warp shuffles, so no
- * global atomics are needed and the result is deterministic.
+ * One warp per cell (grid-stride). The warp stages up to kOwn of the cell's
+ * particles and then, region by region, up to kCap particles of its neighbour
+ * entries (whole entries where they fit) in shared memory. Each own particle
+ * is tested against the staged neighbours one per lane, 32 candidates per
+ * step, for the cutoff, the reference's pruning and the existence of a
+ * potential (pass 1). Interacting candidates are appended, in candidate order,
+ * to a per-warp queue with a ballot; every 32 queued pairs are evaluated with
+ * one pair per lane (pass 2), so the expensive pair arithmetic runs with the
+ * warp's lanes full. The queue is ordered by own particle, so the per-particle
+ * sums of a batch are formed by a segmented shuffle scan in a fixed order and
+ * added to the particle's force in shared memory by the segment's last lane:
+ * no atomics, deterministic results.
  *
- * Each neighbour entry carries the role of cell i in the reference's flipped
+ * Each neighbour entry carries the role of the cell in the reference's flipped
  * cell pair (runner_dopair.cpp:91-340, runner_doself :446-682): FIRST means the
  * reference computes dx = (x_i - shift) - x_j; SECOND means it computes
- * dx = (x_j - shift) - x_i with i as its second particle. Computing dx in the
- * reference's orientation makes r2 and the per-pair force bit-identical.
+ * dx = (x_j - shift) - x_i with i as its second particle. Neighbour positions
+ * of SECOND entries are staged pre-shifted and FIRST entries stage their shift
+ * beside each particle, so every candidate computes d = (x_i - s) - b with one
+ * formula; the reference's dx is d or its exact negation, which makes r2 and
+ * the per-pair force bit-identical to the reference's.
  */
+template <bool kDPD>
+__device__ __forceinline__ void pair_contribution(const EngineView &v, const DevPot &p, int role, bool i_first,
+                                                  float dx, float dy, float dz, float r2, float radi, float radj,
+                                                  const float4 &vi, const float4 &vj, unsigned rng_mode,
+                                                  float &cx, float &cy, float &cz, float &pe, bool &counted) {
+    cx = cy = cz = 0.f;
+    pe = 0.f;
+    counted = false;
+    if (kDPD && p.kind == 1) {
+        // dpd_eval (dpd_eval.hpp:21-69), in the reference's orientation
+        const float r_first = i_first ? radi : radj;
+        const float r_second = i_first ? radj : radi;
+        const bool shifted = p.flags & (1u << 12);
+        const float cutoff = shifted ? __fadd_rn(__fadd_rn(p.b, r_first), r_second) : p.b;
+        if (r2 > __fmul_rn(cutoff, cutoff)) return;
+        const float r = sqrtf(r2);
+        const float ex = __fdiv_rn(dx, r), ey = __fdiv_rn(dy, r), ez = __fdiv_rn(dz, r);
+        float wx, wy, wz;  // v_first - v_second
+        if (i_first) {
+            wx = __fsub_rn(vi.x, vj.x);
+            wy = __fsub_rn(vi.y, vj.y);
+            wz = __fsub_rn(vi.z, vj.z);
+        } else {
+            wx = __fsub_rn(vj.x, vi.x);
+            wy = __fsub_rn(vj.y, vi.y);
+            wz = __fsub_rn(vj.z, vi.z);
+        }
+        const float sr = shifted ? __fsub_rn(__fsub_rn(r, r_first), r_second) : r;
+        const float oc = sr < 0.f ? 1.f : __fsub_rn(1.0f, __fdiv_rn(sr, cutoff));
+        const float fc = __fmul_rn(p.dpd_alpha, oc);
+        const float od = __fmul_rn(oc, oc);
+        const float ev = __fadd_rn(__fadd_rn(__fmul_rn(ex, wx), __fmul_rn(ey, wy)), __fmul_rn(ez, wz));
+        const float fd = __fmul_rn(__fmul_rn(-p.dpd_gamma, od), ev);
+        float fr = __fmul_rn(__fmul_rn(p.dpd_sigma, oc), p.dpd_delta);
+        if (rng_mode) {
+            const unsigned idi = __float_as_uint(vi.w), idj = __float_as_uint(vj.w);
+            fr = fr * philox_pair_xi(*v.step, idi < idj ? idi : idj, idi < idj ? idj : idi);
+        }
+        const float f = __fadd_rn(__fadd_rn(fc, fd), fr);
+        // first particle gets +f e, second -f e; the reference tabulates zero energy for DPD
+        const float sg = i_first ? 1.0f : -1.0f;
+        cx = sg * __fmul_rn(f, ex);
+        cy = sg * __fmul_rn(f, ey);
+        cz = sg * __fmul_rn(f, ez);
+        counted = i_first;
+    } else {
+        float e, f;
+        if (!table_eval_ex(p, v.coef, i_first ? radi : radj, i_first ? radj : radi, r2, e, f)) return;
+        // first particle gets -f dx, second +f dx
+        const float sg = i_first ? -1.0f : 1.0f;
+        cx = sg * __fmul_rn(f, dx);
+        cy = sg * __fmul_rn(f, dy);
+        cz = sg * __fmul_rn(f, dz);
+        if (i_first) pe = e;
+        counted = i_first;
+    }
+}
+
+constexpr int kOwn = 32;    // own particles staged at a time
+constexpr int kCap = 128;   // neighbour particles staged at a time
+
+template <bool kDPD>
+struct ForceSmem {
+    float4 nb_x[kCap];              // position (pre-shifted for SECOND entries); w = type
+    float4 nb_s[kCap];              // shift of FIRST entries, else 0; w = role | entry << 2 | index << 8
+    float4 nb_v[kDPD ? kCap : 1];   // velocity; w = id
+    float4 own_x[kOwn];
+    float4 own_v[kDPD ? kOwn : 1];
+    float4 own_f[kOwn];
+    float4 ent_sh[32];              // region entries: shift, w = packed role/sort direction/key shift
+    int ent_beg[33];                // first staged index of each region entry
+    int ent_slot[32];               // slot of the entry cell's first particle
+    int ent_jb[32];                 // index (within its cell) of the entry's first staged particle
+    int own_mask[kOwn];             // bit t: a potential exists for (own type, t), types < 32
+    int nb_key[kCap];               // sort key of the unshifted neighbour (per-pair pruning)
+    int queue[64];                  // own index << 16 | staged index, in candidate order
+};
+
+/* Pass 2 over queue[0, nb): one interacting pair per lane, segmented sums into
+ * own_f. Returns the pairs counted once (statistics launch). */
+template <bool kDPD, bool kStats>
+__device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD> &sm, int nb, int i0, int own_start,
+                                           int pot_base, unsigned rng_mode, double &ecell,
+                                           unsigned long long &npair) {
+    const int lane = threadIdx.x & 31;
+    float cx = 0.f, cy = 0.f, cz = 0.f;
+    int il = -1;
+    if (lane < nb) {
+        const int cd = sm.queue[lane];
+        il = cd >> 16;
+        const int jj = cd & 0xffff;
+        const int i = i0 + il;
+        const float4 xi = sm.own_x[il];
+        const float4 b = sm.nb_x[jj];
+        const float4 s = sm.nb_s[jj];
+        const int meta = __float_as_int(s.w);
+        const int role = meta & 3, jl = meta >> 8;
+        float dx = __fsub_rn(__fsub_rn(xi.x, s.x), b.x);
+        float dy = __fsub_rn(__fsub_rn(xi.y, s.y), b.y);
+        float dz = __fsub_rn(__fsub_rn(xi.z, s.z), b.z);
+        // SECOND: the reference's dx is b - x_i; SELF with the neighbour first: x_j - x_i
+        if (role == kRoleSecond || (role == kRoleSelf && jl < i)) {
+            dx = -dx;
+            dy = -dy;
+            dz = -dz;
+        }
+        float r2 = dot3_rn(dx, dy, dz);
+        const int ti = __float_as_int(xi.w), tj = __float_as_int(b.w);
+        const DevPot &p = v.pots[v.pot_idx[pot_base + ti * v.ntypes + tj]];
+        const bool i_first = role == kRoleFirst || (role == kRoleSelf && i < jl);
+        if (r2 < p.a2) {
+            // potential_eval_super_ex (dpd_eval.hpp:122-131): random direction of
+            // length a; here a Philox draw keyed on the step and the id pair
+            const unsigned idi = __float_as_uint(kDPD ? sm.own_v[il].w : v.vel[own_start + i].w);
+            const unsigned idj =
+                __float_as_uint(kDPD ? sm.nb_v[jj].w : v.vel[sm.ent_slot[(meta >> 2) & 63] + jl].w);
+            const unsigned lo = idi < idj ? idi : idj, hi = idi < idj ? idj : idi;
+            float g0, g1, g2;
+            philox_normal3(*v.step, lo, hi, g0, g1, g2);
+            const float len = sqrtf(g0 * g0 + g1 * g1 + g2 * g2);
+            // the draw is the displacement first-minus-second for (lo, hi)
+            const float sgn = ((idi == lo) == i_first) ? 1.0f : -1.0f;
+            dx = sgn * g0 * p.a / len;
+            dy = sgn * g1 * p.a / len;
+            dz = sgn * g2 * p.a / len;
+            r2 = p.a2;
+        }
+        const float4 vi = kDPD ? sm.own_v[il] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 vj = kDPD ? sm.nb_v[jj] : make_float4(0.f, 0.f, 0.f, 0.f);
+        float pe;
+        bool counted;
+        pair_contribution<kDPD>(v, p, role, i_first, dx, dy, dz, r2, v.types[ti].radius, v.types[tj].radius, vi,
+                                vj, rng_mode, cx, cy, cz, pe, counted);
+        ecell += (double)pe;
+        if (kStats && counted) ++npair;
+    }
+    // segmented inclusive scan: segments are runs of equal own index
+    const int il_prev = __shfl_up_sync(kFull, il, 1);
+    const unsigned heads = __ballot_sync(kFull, lane == 0 || il != il_prev);
+    const int seg0 = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+    for (int off = 1; off < 32; off <<= 1) {
+        const float ox = __shfl_up_sync(kFull, cx, off);
+        const float oy = __shfl_up_sync(kFull, cy, off);
+        const float oz = __shfl_up_sync(kFull, cz, off);
+        if (lane - off >= seg0) {
+            cx = ox + cx;
+            cy = oy + cy;
+            cz = oz + cz;
+        }
+    }
+    const bool seg_end = lane == 31 || ((heads >> (lane + 1)) & 1u);
+    if (il >= 0 && seg_end) {
+        float4 f = sm.own_f[il];
+        f.x += cx;
+        f.y += cy;
+        f.z += cz;
+        sm.own_f[il] = f;
+    }
+}
+
 template <bool kDPD, bool kStats>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) force_kernel(EngineView v) {
     unsigned long long npair = 0;  // interacting pairs counted once (statistics launch only)
-    __shared__ float4 sp[kWarpsPerBlock][32];
-    __shared__ float4 sv[kWarpsPerBlock][kDPD ? 32 : 1];
-    __shared__ int skey[kWarpsPerBlock][32];
+    __shared__ ForceSmem<kDPD> smem_all[kWarpsPerBlock];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    ForceSmem<kDPD> &sm = smem_all[w];
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const int ntypes = v.ntypes;
+    const bool use_mask = ntypes <= 32;
     for (int c = blockIdx.x * kWarpsPerBlock + w; c < v.ncells; c += gridDim.x * kWarpsPerBlock) {
         const int n = v.cell_count[c];
         double ecell = 0.0;
@@ -125,211 +289,170 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) force_kernel(EngineView v
             const int pot_base = S.pot_offset;
             const float cut2_pair = S.cut2_pair, cut2_self = S.cut2_self;
             const unsigned rng_mode = S.rng_mode;
-            const bool prune = (S.prune & 1) != 0;       // per-pair projection test
-            const bool exit_test = (S.prune & 2) != 0;   // cell-pair exit test
+            const bool prune = (S.prune & 1) != 0;      // per-pair projection test
+            const bool exit_test = (S.prune & 2) != 0;  // cell-pair exit test
             const float sbias = S.sort_bias, sdscale = S.sort_dscale;
             const int dmaxdist = S.dmaxdist;
-            const int P = n >= 32 ? 32 : next_pow2(n);
-            const int G = 32 / P;
-            const int il = lane & (P - 1), g = lane / P;
             const int nb0 = v.nb_off[c], nb1 = v.nb_off[c + 1];
-            for (int i0 = 0; i0 < n; i0 += 32) {
-                const int i = i0 + il;
-                const bool live = i < n;
-                float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
-                float4 vi = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (live) {
-                    xi = v.pos[start + i];
-                    if (kDPD) vi = v.vel[start + i];
-                }
-                const int ti = __float_as_int(xi.w);
-                const DevType &T = v.types[live ? ti : 0];
-                const float radi = T.radius;
-                float fx = 0.f, fy = 0.f, fz = 0.f;
-                if (live && g == 0 && T.has_force) {  // constant_force (MxForce.cpp:339-344), scale 1
-                    fx = T.fx;
-                    fy = T.fy;
-                    fz = T.fz;
-                }
-                double eacc = 0.0;
-                for (int e = nb0; e < nb1; ++e) {
-                    const int nc = v.nb_cell[e];
-                    const int jn = v.cell_count[nc];
-                    if (jn == 0) continue;
-                    const int js = v.cell_start[nc];
-                    const float4 sh = v.nb_shift[e];
-                    const int packed = __float_as_int(sh.w);
-                    const int role = packed & 3;
-                    // runner_dopair's pruning: a pair (first i, second j) is evaluated only
-                    // when key_j + dnshift - key_i < dmaxdist (runner_dopair.cpp:167-182)
-                    const bool prune_e = prune && role != kRoleSelf;
-                    const int sid = (packed >> 2) & 15;
-                    const float *axis = v.axes->n[sid];
-                    const int dnshift = packed >> 8;
-                    if (exit_test && role != kRoleSelf) {
-                        // runner_dopair's first-iteration exit (runner_dopair.cpp:167-171): with the
-                        // largest key of the first cell and the smallest of the second, the unsigned
-                        // difference kmin + dnshift - kmax exceeds dmaxdist (or wraps below zero)
-                        // and the whole cell pair is skipped
-                        const int2 bi = v.sort_bounds[c * 13 + sid], bj = v.sort_bounds[nc * 13 + sid];
-                        const int kmax_first = role == kRoleFirst ? bi.y : bj.y;
-                        const int kmin_second = role == kRoleFirst ? bj.x : bi.x;
-                        const int gap = kmin_second + dnshift - kmax_first;
-                        if (gap < 0 || gap > dmaxdist) continue;
+            for (int i0 = 0; i0 < n; i0 += kOwn) {
+                const int ni = min(kOwn, n - i0);
+                __syncwarp();
+                if (lane < ni) {
+                    const float4 x = v.pos[start + i0 + lane];
+                    sm.own_x[lane] = x;
+                    const int ti = __float_as_int(x.w);
+                    const DevType &T = v.types[ti];
+                    // constant_force (MxForce.cpp:339-344), scale 1
+                    sm.own_f[lane] = T.has_force ? make_float4(T.fx, T.fy, T.fz, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (kDPD) sm.own_v[lane] = v.vel[start + i0 + lane];
+                    if (use_mask) {
+                        int mk = 0;
+                        for (int t = 0; t < ntypes; ++t)
+                            if (v.pot_idx[pot_base + ti * ntypes + t] >= 0) mk |= 1 << t;
+                        sm.own_mask[lane] = mk;
                     }
-                    int mykey = 0;
-                    if (prune_e) mykey = sort_key(xi.x, xi.y, xi.z, axis, sbias, sdscale);
-                    float ax = xi.x, ay = xi.y, az = xi.z;
-                    if (role == kRoleFirst) {
-                        ax = __fsub_rn(xi.x, sh.x);
-                        ay = __fsub_rn(xi.y, sh.y);
-                        az = __fsub_rn(xi.z, sh.z);
-                    }
-                    const float cut2 = role == kRoleSelf ? cut2_self : cut2_pair;
-                    for (int j0 = 0; j0 < jn; j0 += 32) {
-                        const int cnt = min(32, jn - j0);
-                        __syncwarp();
-                        if (lane < cnt) {
-                            float4 q = v.pos[js + j0 + lane];
-                            if (prune_e) skey[w][lane] = sort_key(q.x, q.y, q.z, axis, sbias, sdscale);
-                            if (role == kRoleSecond) {
-                                q.x = __fsub_rn(q.x, sh.x);
-                                q.y = __fsub_rn(q.y, sh.y);
-                                q.z = __fsub_rn(q.z, sh.z);
-                            }
-                            sp[w][lane] = q;
-                            if (kDPD) sv[w][lane] = v.vel[js + j0 + lane];
+                }
+                int e = nb0, jpos = 0;
+                while (e < nb1) {
+                    // ---- region: lane k describes entry e + k
+                    const int ek = e + lane;
+                    int cnt = 0, cstart = 0, pk = 0;
+                    float4 sh = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (ek < nb1) {
+                        const int nc = v.nb_cell[ek];
+                        sh = v.nb_shift[ek];
+                        pk = __float_as_int(sh.w);
+                        cnt = v.cell_count[nc];
+                        cstart = v.cell_start[nc];
+                        const int role = pk & 3;
+                        if (cnt > 0 && exit_test && role != kRoleSelf) {
+                            // runner_dopair.cpp:167-171: kmin(second) + dnshift - kmax(first) in
+                            // unsigned arithmetic; above dmaxdist or wrapped, the pair is skipped
+                            const int sid = (pk >> 2) & 15;
+                            const int2 bc = v.sort_bounds[c * 13 + sid], bn = v.sort_bounds[nc * 13 + sid];
+                            const int kmax_first = role == kRoleFirst ? bc.y : bn.y;
+                            const int kmin_second = role == kRoleFirst ? bn.x : bc.x;
+                            const int gap = kmin_second + (pk >> 8) - kmax_first;
+                            if (gap < 0 || gap > dmaxdist) cnt = 0;
                         }
-                        __syncwarp();
-                        if (!live) continue;
-                        for (int t = g; t < cnt; t += G) {
-                            const int j = j0 + t;
-                            if (role == kRoleSelf && j == i) continue;
-                            if (prune_e) {
-                                const int kf = role == kRoleFirst ? mykey : skey[w][t];
-                                const int ks = role == kRoleFirst ? skey[w][t] : mykey;
-                                if (!(ks + dnshift - kf < dmaxdist)) continue;
-                            }
-                            const float4 q = sp[w][t];
-                            // dx in the reference's orientation
-                            float dx, dy, dz;
-                            if (role == kRoleSecond) {
-                                dx = __fsub_rn(q.x, xi.x);
-                                dy = __fsub_rn(q.y, xi.y);
-                                dz = __fsub_rn(q.z, xi.z);
-                            } else {
-                                dx = __fsub_rn(ax, q.x);
-                                dy = __fsub_rn(ay, q.y);
-                                dz = __fsub_rn(az, q.z);
-                                if (role == kRoleSelf && j < i) {
-                                    // the reference's first particle of a self pair is the earlier
-                                    // one; x_j - x_i is the exact negation of x_i - x_j
-                                    dx = -dx;
-                                    dy = -dy;
-                                    dz = -dz;
+                    }
+                    const int jb = lane == 0 ? jpos : 0;
+                    const int rem = max(cnt - jb, 0);
+                    int incl = rem;
+                    for (int off = 1; off < 32; off <<= 1) {
+                        const int o = __shfl_up_sync(kFull, incl, off);
+                        if (lane >= off) incl += o;
+                    }
+                    const int nfit = __popc(__ballot_sync(kFull, ek < nb1 && incl <= kCap));
+                    int nent, M;
+                    if (nfit == 0) {  // the first entry alone holds more than kCap particles
+                        nent = 1;
+                        M = kCap;
+                        jpos += kCap;
+                    } else {
+                        nent = nfit;
+                        M = __shfl_sync(kFull, incl, nfit - 1);
+                        e += nfit;
+                        jpos = 0;
+                    }
+                    __syncwarp();
+                    if (lane < nent) {
+                        sm.ent_beg[lane] = incl - rem;
+                        sm.ent_slot[lane] = cstart;
+                        sm.ent_jb[lane] = jb;
+                        sm.ent_sh[lane] = sh;
+                    }
+                    if (lane == 0) sm.ent_beg[nent] = M;
+                    __syncwarp();
+                    if (M == 0) continue;
+                    // ---- stage the region's neighbour particles
+                    for (int idx = lane; idx < M; idx += 32) {
+                        int k = 0;
+                        for (int step = 16; step > 0; step >>= 1)
+                            if (k + step < nent && sm.ent_beg[k + step] <= idx) k += step;
+                        const int jl = sm.ent_jb[k] + idx - sm.ent_beg[k];
+                        const int slot = sm.ent_slot[k] + jl;
+                        const float4 es = sm.ent_sh[k];
+                        const int epk = __float_as_int(es.w);
+                        const int role = epk & 3;
+                        float4 q = v.pos[slot];
+                        if (prune) sm.nb_key[idx] = sort_key(q.x, q.y, q.z, v.axes->n[(epk >> 2) & 15], sbias, sdscale);
+                        float4 s4 = make_float4(0.f, 0.f, 0.f, __int_as_float(role | (k << 2) | (jl << 8)));
+                        if (role == kRoleSecond) {
+                            q.x = __fsub_rn(q.x, es.x);
+                            q.y = __fsub_rn(q.y, es.y);
+                            q.z = __fsub_rn(q.z, es.z);
+                        } else if (role == kRoleFirst) {
+                            s4.x = es.x;
+                            s4.y = es.y;
+                            s4.z = es.z;
+                        }
+                        sm.nb_x[idx] = q;
+                        sm.nb_s[idx] = s4;
+                        if (kDPD) sm.nb_v[idx] = v.vel[slot];
+                    }
+                    __syncwarp();
+                    // ---- pass 1 (candidates) and pass 2 (full batches)
+                    int qlen = 0;
+                    for (int il = 0; il < ni; ++il) {
+                        const float4 xi = sm.own_x[il];
+                        const int i = i0 + il;
+                        const int ti = __float_as_int(xi.w);
+                        const int mk = use_mask ? sm.own_mask[il] : 0;
+                        for (int jb0 = 0; jb0 < M; jb0 += 32) {
+                            const int jj = jb0 + lane;
+                            bool hit = false;
+                            if (jj < M) {
+                                const float4 b = sm.nb_x[jj];
+                                const float4 s = sm.nb_s[jj];
+                                const int meta = __float_as_int(s.w);
+                                const int role = meta & 3;
+                                const float dx = __fsub_rn(__fsub_rn(xi.x, s.x), b.x);
+                                const float dy = __fsub_rn(__fsub_rn(xi.y, s.y), b.y);
+                                const float dz = __fsub_rn(__fsub_rn(xi.z, s.z), b.z);
+                                const float r2 = dot3_rn(dx, dy, dz);
+                                const int tj = __float_as_int(b.w);
+                                hit = r2 <= (role == kRoleSelf ? cut2_self : cut2_pair);
+                                hit = hit && (use_mask ? ((mk >> tj) & 1) != 0
+                                                       : v.pot_idx[pot_base + ti * ntypes + tj] >= 0);
+                                if (role == kRoleSelf) hit = hit && (meta >> 8) != i;
+                                if (prune && hit && role != kRoleSelf) {
+                                    // runner_dopair's pruning: a pair (first, second) is evaluated
+                                    // only when key_second + dnshift - key_first < dmaxdist
+                                    // (runner_dopair.cpp:167-182)
+                                    const int epk = __float_as_int(sm.ent_sh[(meta >> 2) & 63].w);
+                                    const int okey =
+                                        sort_key(xi.x, xi.y, xi.z, v.axes->n[(epk >> 2) & 15], sbias, sdscale);
+                                    const int kf = role == kRoleFirst ? okey : sm.nb_key[jj];
+                                    const int ks = role == kRoleFirst ? sm.nb_key[jj] : okey;
+                                    hit = ks + (epk >> 8) - kf < dmaxdist;
                                 }
                             }
-                            float r2 = dot3_rn(dx, dy, dz);
-                            if (r2 > cut2) continue;
-                            const int tj = __float_as_int(q.w);
-                            const int pidx = v.pot_idx[pot_base + ti * v.ntypes + tj];
-                            if (pidx < 0) continue;
-                            const DevPot &p = v.pots[pidx];
-                            // which of the two is the reference's first particle
-                            const bool i_first = role == kRoleFirst || (role == kRoleSelf && i < j);
-                            if (r2 < p.a2) {
-                                // potential_eval_super_ex (dpd_eval.hpp:122-131): random direction of
-                                // length a; here a Philox draw keyed on the step and the id pair
-                                const unsigned idi = __float_as_uint(v.vel[start + i].w);
-                                const unsigned idj = __float_as_uint(v.vel[js + j].w);
-                                const unsigned lo = idi < idj ? idi : idj, hi = idi < idj ? idj : idi;
-                                float g0, g1, g2;
-                                philox_normal3(*v.step, lo, hi, g0, g1, g2);
-                                const float len = sqrtf(g0 * g0 + g1 * g1 + g2 * g2);
-                                // the draw is the displacement first-minus-second for (lo, hi)
-                                const bool sign = ((idi == lo) == i_first);
-                                const float s = sign ? 1.0f : -1.0f;
-                                dx = s * g0 * p.a / len;
-                                dy = s * g1 * p.a / len;
-                                dz = s * g2 * p.a / len;
-                                r2 = p.a2;
-                            }
-                            if (kDPD && p.kind == 1) {
-                                // dpd_eval (dpd_eval.hpp:21-69), in the reference's orientation
-                                const DevType &Tj = v.types[tj];
-                                const float r_first = i_first ? radi : Tj.radius;
-                                const float r_second = i_first ? Tj.radius : radi;
-                                const bool shifted = p.flags & (1u << 12);
-                                const float cutoff = shifted ? __fadd_rn(__fadd_rn(p.b, r_first), r_second) : p.b;
-                                if (r2 > __fmul_rn(cutoff, cutoff)) continue;
-                                const float r = sqrtf(r2);
-                                const float ex = __fdiv_rn(dx, r), ey = __fdiv_rn(dy, r), ez = __fdiv_rn(dz, r);
-                                const float4 vj = sv[w][t];
-                                float wx, wy, wz;  // v_first - v_second
-                                if (i_first) {
-                                    wx = __fsub_rn(vi.x, vj.x);
-                                    wy = __fsub_rn(vi.y, vj.y);
-                                    wz = __fsub_rn(vi.z, vj.z);
-                                } else {
-                                    wx = __fsub_rn(vj.x, vi.x);
-                                    wy = __fsub_rn(vj.y, vi.y);
-                                    wz = __fsub_rn(vj.z, vi.z);
-                                }
-                                const float sr = shifted ? __fsub_rn(__fsub_rn(r, r_first), r_second) : r;
-                                const float oc = sr < 0.f ? 1.f : __fsub_rn(1.0f, __fdiv_rn(sr, cutoff));
-                                const float fc = __fmul_rn(p.dpd_alpha, oc);
-                                const float od = __fmul_rn(oc, oc);
-                                const float ev = __fadd_rn(__fadd_rn(__fmul_rn(ex, wx), __fmul_rn(ey, wy)), __fmul_rn(ez, wz));
-                                const float fd = __fmul_rn(__fmul_rn(-p.dpd_gamma, od), ev);
-                                float fr = __fmul_rn(__fmul_rn(p.dpd_sigma, oc), p.dpd_delta);
-                                if (rng_mode) {
-                                    const unsigned idi = __float_as_uint(vi.w), idj = __float_as_uint(vj.w);
-                                    fr = fr * philox_pair_xi(*v.step, idi < idj ? idi : idj, idi < idj ? idj : idi);
-                                }
-                                const float f = __fadd_rn(__fadd_rn(fc, fd), fr);
-                                if (i_first) {
-                                    fx = __fadd_rn(fx, __fmul_rn(f, ex));
-                                    fy = __fadd_rn(fy, __fmul_rn(f, ey));
-                                    fz = __fadd_rn(fz, __fmul_rn(f, ez));
-                                } else {
-                                    fx = __fsub_rn(fx, __fmul_rn(f, ex));
-                                    fy = __fsub_rn(fy, __fmul_rn(f, ey));
-                                    fz = __fsub_rn(fz, __fmul_rn(f, ez));
-                                }
-                                // the reference tabulates zero energy for DPD
-                                if (kStats && i_first) ++npair;
-                            } else {
-                                const float radj = v.types[tj].radius;
-                                float pe, pf;
-                                if (!table_eval_ex(p, v.coef, i_first ? radi : radj, i_first ? radj : radi, r2, pe, pf))
-                                    continue;
-                                const float wx = __fmul_rn(pf, dx), wy = __fmul_rn(pf, dy), wz = __fmul_rn(pf, dz);
-                                if (i_first) {
-                                    fx = __fsub_rn(fx, wx);
-                                    fy = __fsub_rn(fy, wy);
-                                    fz = __fsub_rn(fz, wz);
-                                } else {
-                                    fx = __fadd_rn(fx, wx);
-                                    fy = __fadd_rn(fy, wy);
-                                    fz = __fadd_rn(fz, wz);
-                                }
-                                if (role == kRoleFirst || (role == kRoleSelf && i < j)) {
-                                    eacc += (double)pe;
-                                    if (kStats) ++npair;
-                                }
+                            const unsigned hb = __ballot_sync(kFull, hit);
+                            if (hit) sm.queue[qlen + __popc(hb & lt_mask)] = (il << 16) | jj;
+                            qlen += __popc(hb);
+                            if (qlen >= 32) {
+                                __syncwarp();
+                                eval_batch<kDPD, kStats>(v, sm, 32, i0, start, pot_base, rng_mode, ecell, npair);
+                                qlen -= 32;
+                                const int moved = lane < qlen ? sm.queue[32 + lane] : 0;
+                                __syncwarp();
+                                if (lane < qlen) sm.queue[lane] = moved;
+                                __syncwarp();
                             }
                         }
                     }
+                    if (qlen > 0) {
+                        __syncwarp();
+                        eval_batch<kDPD, kStats>(v, sm, qlen, i0, start, pot_base, rng_mode, ecell, npair);
+                    }
+                    __syncwarp();
                 }
-                // combine the G partial sums of each particle
-                for (int off = P; off < 32; off <<= 1) {
-                    fx += __shfl_xor_sync(kFull, fx, off);
-                    fy += __shfl_xor_sync(kFull, fy, off);
-                    fz += __shfl_xor_sync(kFull, fz, off);
-                    eacc += __shfl_xor_sync(kFull, eacc, off);
+                __syncwarp();
+                if (lane < ni) {
+                    const float4 f = sm.own_f[lane];
+                    v.force[start + i0 + lane] = make_float4(f.x, f.y, f.z, 0.f);
                 }
-                if (live && g == 0) v.force[start + i] = make_float4(fx, fy, fz, 0.f);
-                if (g == 0) ecell += eacc;
             }
         }
         for (int off = 16; off > 0; off >>= 1) ecell += __shfl_xor_sync(kFull, ecell, off);
@@ -689,6 +812,16 @@ __global__ void reduce_final_kernel(int nblocks, const double *partials, double 
 /* ------------------------------------------------------------------------ */
 /* launchers                                                                 */
 /* ------------------------------------------------------------------------ */
+
+void configure_force_kernels() {
+    // the force kernel's occupancy is bounded by shared memory: ask for the
+    // largest shared-memory carveout of the unified L1/shared storage
+    const int carve = cudaSharedmemCarveoutMaxShared;
+    cudaFuncSetAttribute(force_kernel<true, true>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+    cudaFuncSetAttribute(force_kernel<true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+    cudaFuncSetAttribute(force_kernel<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+    cudaFuncSetAttribute(force_kernel<false, false>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+}
 
 void launch_force(const EngineView &v, bool has_dpd, int grid, cudaStream_t st) {
     const bool stats = v.pair_stats != nullptr;

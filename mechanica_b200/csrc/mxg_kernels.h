@@ -4,6 +4,7 @@
 
 namespace mxg {
 
+void configure_force_kernels();
 void launch_force(const EngineView &v, bool has_dpd, int grid, cudaStream_t st);
 void launch_bonds(const EngineView &v, const DevBond *bonds, unsigned *bond_flags, const int *bond_off,
                   const int *bond_list, const int *slot_of_id, double *ebond_slot, cudaStream_t st);

@@ -171,3 +171,47 @@ def build_gpu(scn, rng_mode="reference"):
         kind, params = scn["bond_pot"]
         u._add_bonds(make_potential(kind, params), scn["bi"], scn["bj"], scn["dissociation"])
     return u
+
+
+def cell_sorting_specs(nrep=256, seed=5, nmin=1000, nmax=20000, density=0.8, cut=2.5, dt=0.01, a=5.0, r0=1.0):
+    """Replicas of the two-type cell-sorting mixture: particle counts uniform in
+    [nmin, nmax], cubic periodic boxes at the given density, 50/50 types, Morse
+    per type pair with d_AA, d_BB ~ U(0.2, 1.0), d_AB ~ U(0.05, 0.5), overdamped."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for r in range(nrep):
+        n = int(rng.integers(nmin, nmax + 1))
+        L = (n / density) ** (1.0 / 3.0)
+        x = rng.uniform(0, L, size=(n, 3)).astype(np.float32).astype(np.float64)
+        x = np.minimum(x, np.float32(L) * (1 - 1e-6))
+        t = np.zeros(n, dtype=np.int32)
+        t[rng.permutation(n)[: n // 2]] = 1
+        cells = max(3, int(L // cut))
+        dAA, dBB = rng.uniform(0.2, 1.0, size=2)
+        dAB = rng.uniform(0.05, 0.5)
+        specs.append(dict(dim=[L, L, L], cells=[cells] * 3, cutoff=cut, dt=dt, bc=("periodic", "periodic", "periodic"),
+                          types=[(1.0, 1.0, m.Overdamped), (1.0, 1.0, m.Overdamped)],
+                          pots=[("morse", (float(dAA), a, r0, 1e-4, cut, 1e-3), 0, 0),
+                                ("morse", (float(dAB), a, r0, 1e-4, cut, 1e-3), 0, 1),
+                                ("morse", (float(dBB), a, r0, 1e-4, cut, 1e-3), 1, 1)],
+                          forces=[], x=x, v=np.zeros_like(x), t=t))
+    return specs
+
+
+def build_gpu_batch(specs, stream=None):
+    """All replicas in one engine (one set of kernel launches per step). Types
+    come from the first spec and are shared; potentials are per replica."""
+    s0 = specs[0]
+    bc0 = {"x": s0["bc"][0], "y": s0["bc"][1], "z": s0["bc"][2]}
+    m.init(dim=s0["dim"], cells=s0["cells"], cutoff=s0["cutoff"], dt=s0["dt"], bc=bc0, stream=stream)
+    u = m.universe
+    types = [type(f"T{k}", (m.Particle,), {"mass": ms, "radius": rad, "dynamics": dyn})
+             for k, (ms, rad, dyn) in enumerate(s0["types"])]
+    for r, sc in enumerate(specs):
+        rep = 0 if r == 0 else u.add_replica(sc["dim"], sc["cells"],
+                                             bc={"x": sc["bc"][0], "y": sc["bc"][1], "z": sc["bc"][2]})
+        for (kind, params, ti, tj) in sc["pots"]:
+            u.bind(make_potential(kind, params), types[ti], types[tj], replica=rep)
+        u._add_particles(np.asarray(sc["x"]), np.asarray(sc["v"], dtype=np.float32),
+                         np.asarray(sc["t"], dtype=np.int32), rep)
+    return u
