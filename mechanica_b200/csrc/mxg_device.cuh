@@ -130,6 +130,9 @@ struct EngineView {      // everything a kernel needs, passed by value
     double *epot_cell;       // per cell nonbonded energy of the last force pass
     unsigned *status;
     unsigned long long *pair_stats;  // non-null only for the statistics launch
+    const int *nb_rev;       // FIRST entries: the pair's plane in the neighbour's received sums
+    const int *sec_count;    // per cell: SECOND entries, i.e. planes of received sums
+    float4 *planes;          // [plane][slot] neighbour-side force sums of once-evaluated pairs
 };
 
 #ifdef __CUDACC__

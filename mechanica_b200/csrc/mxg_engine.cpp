@@ -347,8 +347,10 @@ struct mxg_engine {
     int *d_slot_of_id = nullptr;
     int *d_cell_rep = nullptr;
     unsigned *d_cell_flags = nullptr;
-    int *d_nb_off = nullptr, *d_nb_cell = nullptr;
+    int *d_nb_off = nullptr, *d_nb_cell = nullptr, *d_nb_rev = nullptr, *d_sec_count = nullptr;
     float4 *d_nb_shift = nullptr;
+    float4 *d_planes = nullptr;
+    int nplanes = 0;
     DevPot *d_pots = nullptr;
     float *d_coef = nullptr;
     int *d_pot_idx = nullptr;
@@ -488,27 +490,40 @@ struct mxg_engine {
         v.epot_cell = d_epot_cell;
         v.status = d_status;
         v.pair_stats = nullptr;
+        v.nb_rev = d_nb_rev;
+        v.sec_count = d_sec_count;
+        v.planes = d_planes;
         return v;
     }
 
+    /* The force pass alone (engine_force): the bond kernel, or the combine
+     * kernel when there are no bonds, adds the received planes. */
     void enqueue_force(int b) {
         const EngineView v = view(b);
-        launch_force(v, has_dpd, force_grid, stream);
+        launch_force(v, has_dpd, force_grid, bonds.empty(), stream);
         if (!bonds.empty())
             launch_bonds(v, d_bonds, d_bond_flags, d_bond_off, d_bond_list, d_slot_of_id, d_ebond_slot, stream);
     }
 
+    /* One step (engine_step): force pass, bonds, integrator and re-binning; the
+     * received planes are added by the bond kernel or, without bonds, by the
+     * integrator; the re-binning pass computes the new key bounds. */
     void enqueue_step(int b) {
         const int nb = 1 - b;
-        enqueue_force(b);
         const EngineView v = view(b);
-        launch_integrate(v, d_pos[b], d_vel[b], d_new_cell, d_in_count, d_in_list, d_out_count, stream);
+        launch_force(v, has_dpd, force_grid, false, stream);
+        if (!bonds.empty())
+            launch_bonds(v, d_bonds, d_bond_flags, d_bond_off, d_bond_list, d_slot_of_id, d_ebond_slot, stream);
+        launch_integrate(v, d_pos[b], d_vel[b], d_new_cell, d_in_count, d_in_list, d_out_count, bonds.empty(),
+                         stream);
         launch_scan(ncells, d_cell_count[b], d_out_count, d_in_count, d_cell_start[nb], d_cell_count[nb], d_step,
                     stream);
-        launch_scatter(ncells, d_pos[b], d_vel[b], d_new_cell, d_cell_start[b], d_cell_count[b], d_in_count,
-                       d_in_list, d_out_count, d_cell_start[nb], d_pos[nb], d_vel[nb], d_cell_of[nb], d_slot_of_id,
-                       stream);
+        launch_scatter(v, d_pos[b], d_vel[b], d_new_cell, d_cell_start[b], d_cell_count[b], d_in_count, d_in_list,
+                       d_out_count, d_cell_start[nb], d_pos[nb], d_vel[nb], d_cell_of[nb], d_slot_of_id, stream);
     }
+
+    /* Key bounds for a state that did not come from the re-binning pass. */
+    void refresh_bounds() { launch_sort_bounds(view(cur), stream); }
 
     int start(cudaStream_t st);
     int build_graphs();
@@ -531,7 +546,16 @@ int mxg_engine::start(cudaStream_t st) {
     if (rc != MXG_OK) return rc;
 
     // ---- neighbour entries from each replica's task list (global cell indices) ----
-    std::vector<std::vector<std::pair<int, float4>>> nb(ncells);
+    // Each pair task is evaluated once, by the cell in the reference's FIRST role; the
+    // forces on the SECOND cell's particles go to one plane of received sums per SECOND
+    // entry of that cell (rev), added in plane order after the force pass.
+    struct NbEntry {
+        int cell;
+        float4 shift;
+        int rev;
+    };
+    std::vector<std::vector<NbEntry>> nb(ncells);
+    std::vector<int> hsec(ncells, 0);
     std::vector<int> hrep(ncells, 0);
     std::vector<unsigned> hcflags(ncells, 0u);
     for (int r = 0; r < (int)spaces.size(); ++r) {
@@ -546,7 +570,7 @@ int mxg_engine::start(cudaStream_t st) {
                 float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
                 int role = kRoleSelf;
                 memcpy(&e.w, &role, 4);
-                nb[off + t.i].push_back({off + t.i, e});
+                nb[off + t.i].push_back({off + t.i, e, -1});
             } else if (t.type == kTaskPair) {
                 int ci = t.i, cj = t.j;
                 float shift[3];
@@ -556,20 +580,24 @@ int mxg_engine::start(cudaStream_t st) {
                 int r1 = kRoleFirst | (sid << 2) | (dn << 8), r2 = kRoleSecond | (sid << 2) | (dn << 8);
                 memcpy(&e1.w, &r1, 4);
                 memcpy(&e2.w, &r2, 4);
-                nb[off + ci].push_back({off + cj, e1});
-                nb[off + cj].push_back({off + ci, e2});
+                nb[off + ci].push_back({off + cj, e1, hsec[off + cj]});
+                nb[off + cj].push_back({off + ci, e2, -1});
+                ++hsec[off + cj];
             }
         }
     }
-    std::vector<int> nb_off(ncells + 1, 0), nb_cell;
+    std::vector<int> nb_off(ncells + 1, 0), nb_cell, nb_rev;
     std::vector<float4> nb_shift;
     for (int c = 0; c < ncells; ++c) {
         nb_off[c + 1] = nb_off[c] + (int)nb[c].size();
         for (auto &e : nb[c]) {
-            nb_cell.push_back(e.first);
-            nb_shift.push_back(e.second);
+            nb_cell.push_back(e.cell);
+            nb_shift.push_back(e.shift);
+            nb_rev.push_back(e.rev);
         }
     }
+    nplanes = 0;
+    for (int c = 0; c < ncells; ++c) nplanes = std::max(nplanes, hsec[c]);
 
     // ---- potentials, types, replicas ----
     std::vector<DevPot> hp;
@@ -672,6 +700,9 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_nb_off, ncells + 1);
     rc |= alloc(&d_nb_cell, nb_cell.size());
     rc |= alloc(&d_nb_shift, nb_shift.size());
+    rc |= alloc(&d_nb_rev, nb_rev.size());
+    rc |= alloc(&d_sec_count, ncells);
+    rc |= alloc(&d_planes, (size_t)nplanes * nparts);
     rc |= alloc(&d_pots, hp.size());
     rc |= alloc(&d_coef, coef.size() + 8);
     rc |= alloc(&d_pot_idx, hpidx.size());
@@ -703,7 +734,8 @@ int mxg_engine::start(cudaStream_t st) {
         (rc = upload(d_cell_count[0], hcount, stream)) || (rc = upload(d_slot_of_id, hslot, stream)) ||
         (rc = upload(d_cell_rep, hrep, stream)) || (rc = upload(d_cell_flags, hcflags, stream)) ||
         (rc = upload(d_nb_off, nb_off, stream)) || (rc = upload(d_nb_cell, nb_cell, stream)) ||
-        (rc = upload(d_nb_shift, nb_shift, stream)) || (rc = upload(d_pots, hp, stream)) ||
+        (rc = upload(d_nb_shift, nb_shift, stream)) || (rc = upload(d_nb_rev, nb_rev, stream)) ||
+        (rc = upload(d_sec_count, hsec, stream)) || (rc = upload(d_pots, hp, stream)) ||
         (rc = upload(d_coef, coef, stream)) || (rc = upload(d_pot_idx, hpidx, stream)) ||
         (rc = upload(d_types, ht, stream)) || (rc = upload(d_spaces, hs, stream)) || (rc = upload(d_axes, haxes, stream)) ||
         (rc = upload(d_bonds, hb, stream)) || (rc = upload(d_bond_flags, hbf, stream)) ||
@@ -719,6 +751,7 @@ int mxg_engine::start(cudaStream_t st) {
     force_grid = std::max(1, std::min((ncells + kWarpsPerBlock - 1) / kWarpsPerBlock, sms * 16));
     cur = 0;
     started = true;
+    refresh_bounds();
     return build_graphs();
 }
 
@@ -757,6 +790,7 @@ int mxg_engine::load_state(const double *x, const float *v, int n) {
         (rc = upload(d_cell_of[cur], hcell_of, stream)) || (rc = upload(d_cell_start[cur], hstart, stream)) ||
         (rc = upload(d_cell_count[cur], hcount, stream)) || (rc = upload(d_slot_of_id, hslot, stream)))
         return rc;
+    refresh_bounds();
     CUDA_TRY(cudaStreamSynchronize(stream));
     return MXG_OK;
 }
@@ -1179,6 +1213,7 @@ int mxg_engine_copy_state(mxg_engine *e, void *host_pos, void *host_vel, int to_
     if (to_device) {
         CUDA_TRY(cudaMemcpyAsync(e->d_pos[e->cur], host_pos, bytes, cudaMemcpyHostToDevice, e->stream));
         CUDA_TRY(cudaMemcpyAsync(e->d_vel[e->cur], host_vel, bytes, cudaMemcpyHostToDevice, e->stream));
+        e->refresh_bounds();
     } else {
         CUDA_TRY(cudaMemcpyAsync(host_pos, e->d_pos[e->cur], bytes, cudaMemcpyDeviceToHost, e->stream));
         CUDA_TRY(cudaMemcpyAsync(host_vel, e->d_vel[e->cur], bytes, cudaMemcpyDeviceToHost, e->stream));
@@ -1219,7 +1254,7 @@ int mxg_engine_time_force(mxg_engine *e, int reps, double *ms) {
     CUDA_TRY(cudaEventCreate(&b));
     const EngineView v = e->view(e->cur);
     CUDA_TRY(cudaEventRecord(a, e->stream));
-    for (int r = 0; r < reps; ++r) launch_force(v, e->has_dpd, e->force_grid, e->stream);
+    for (int r = 0; r < reps; ++r) launch_force(v, e->has_dpd, e->force_grid, true, e->stream);
     CUDA_TRY(cudaEventRecord(b, e->stream));
     CUDA_TRY(cudaEventSynchronize(b));
     float t = 0.f;
@@ -1247,9 +1282,9 @@ int mxg_engine_autotune(mxg_engine *e) {
     const EngineView v = e->view(e->cur);
     for (int per_sm : cands) {
         const int grid = std::max(1, std::min(max_grid, e->num_sms * per_sm));
-        launch_force(v, e->has_dpd, grid, e->stream);  // warm
+        launch_force(v, e->has_dpd, grid, true, e->stream);  // warm
         CUDA_TRY(cudaEventRecord(a, e->stream));
-        for (int r = 0; r < 5; ++r) launch_force(v, e->has_dpd, grid, e->stream);
+        for (int r = 0; r < 5; ++r) launch_force(v, e->has_dpd, grid, true, e->stream);
         CUDA_TRY(cudaEventRecord(b, e->stream));
         CUDA_TRY(cudaEventSynchronize(b));
         float t = 0.f;
@@ -1303,7 +1338,7 @@ int mxg_engine_pair_counts(mxg_engine *e, long long *candidates, long long *inte
         CUDA_TRY(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), e->stream));
         EngineView v = e->view(e->cur);
         v.pair_stats = d_cnt;
-        launch_force(v, e->has_dpd, e->force_grid, e->stream);
+        launch_force(v, e->has_dpd, e->force_grid, true, e->stream);
         unsigned long long n = 0;
         CUDA_TRY(cudaMemcpyAsync(&n, d_cnt, sizeof(n), cudaMemcpyDeviceToHost, e->stream));
         CUDA_TRY(cudaStreamSynchronize(e->stream));

@@ -55,32 +55,46 @@ __device__ __forceinline__ float philox_pair_xi(unsigned long long step, unsigne
  * Per cell and per sort direction, the smallest and largest projection key of
  * its particles (runner_dosort.cpp:133-141 computes the keys; runner_dopair
  * reads the largest key of its first cell and the smallest of its second,
- * runner_dopair.cpp:167-171). One warp per cell.
+ * runner_dopair.cpp:167-171). Called by one warp for one cell.
  */
-__global__ void sort_bounds_kernel(EngineView v) {
+__device__ __forceinline__ void cell_sort_bounds(const float4 *__restrict__ pos, int start, int n, float bias,
+                                                 float dscale, const SortAxes *axes, int2 *out) {
     const int lane = threadIdx.x & 31;
+    if (n <= 32) {  // one particle per lane
+        const bool live = lane < n;
+        const float4 q = live ? pos[start + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int sid = 0; sid < 13; ++sid) {
+            const int key = sort_key(q.x, q.y, q.z, axes->n[sid], bias, dscale);
+            const int kmin = __reduce_min_sync(kFull, live ? key : 0x7fffffff);
+            const int kmax = __reduce_max_sync(kFull, live ? key : -1);
+            if (lane == 0) out[sid] = make_int2(kmin, kmax);
+        }
+        return;
+    }
+    for (int sid = 0; sid < 13; ++sid) {
+        int kmin = 0x7fffffff, kmax = -1;
+        for (int k = lane; k < n; k += 32) {
+            const float4 q = pos[start + k];
+            const int key = sort_key(q.x, q.y, q.z, axes->n[sid], bias, dscale);
+            kmin = min(kmin, key);
+            kmax = max(kmax, key);
+        }
+        kmin = __reduce_min_sync(kFull, kmin);
+        kmax = __reduce_max_sync(kFull, kmax);
+        if (lane == 0) out[sid] = make_int2(kmin, kmax);
+    }
+}
+
+/* Key bounds of every cell of the current state, for states that did not come
+ * from the re-binning pass (which computes them itself). One warp per cell. */
+__global__ void sort_bounds_kernel(EngineView v) {
     const int warps = (gridDim.x * blockDim.x) >> 5;
     for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < v.ncells; c += warps) {
         const int n = v.cell_count[c];
         if (n == 0) continue;
-        const int start = v.cell_start[c];
         const DevSpace &S = v.spaces[v.cell_rep[c]];
-        const float bias = S.sort_bias, dscale = S.sort_dscale;
-        for (int sid = 0; sid < 13; ++sid) {
-            const float *ax = v.axes->n[sid];
-            int kmin = 0x7fffffff, kmax = -1;
-            for (int k = lane; k < n; k += 32) {
-                const float4 q = v.pos[start + k];
-                const int key = sort_key(q.x, q.y, q.z, ax, bias, dscale);
-                kmin = min(kmin, key);
-                kmax = max(kmax, key);
-            }
-            for (int off = 16; off > 0; off >>= 1) {
-                kmin = min(kmin, __shfl_xor_sync(kFull, kmin, off));
-                kmax = max(kmax, __shfl_xor_sync(kFull, kmax, off));
-            }
-            if (lane == 0) v.sort_bounds[c * 13 + sid] = make_int2(kmin, kmax);
-        }
+        if (!(S.prune & 2)) continue;
+        cell_sort_bounds(v.pos, v.cell_start[c], n, S.sort_bias, S.sort_dscale, v.axes, v.sort_bounds + c * 13);
     }
 }
 
@@ -89,27 +103,31 @@ __global__ void sort_bounds_kernel(EngineView v) {
 /* ------------------------------------------------------------------------ */
 
 /*
- * One warp per cell (grid-stride). The warp stages up to kOwn of the cell's
- * particles and then, region by region, up to kCap particles of its neighbour
- * entries (whole entries where they fit) in shared memory. Each own particle
- * is tested against the staged neighbours one per lane, 32 candidates per
- * step, for the cutoff, the reference's pruning and the existence of a
- * potential (pass 1). Interacting candidates are appended, in candidate order,
- * to a per-warp queue with a ballot; every 32 queued pairs are evaluated with
- * one pair per lane (pass 2), so the expensive pair arithmetic runs with the
- * warp's lanes full. The queue is ordered by own particle, so the per-particle
- * sums of a batch are formed by a segmented shuffle scan in a fixed order and
- * added to the particle's force in shared memory by the segment's last lane:
- * no atomics, deterministic results.
+ * One warp per cell (grid-stride). Every cell pair is evaluated once, by the
+ * cell that is FIRST in the reference's flipped pair (runner_dopair.cpp:91-340);
+ * the cell's own pairs (runner_doself, :446-682) are evaluated from both sides.
+ * The warp stages up to kOwn of the cell's particles and then, region by
+ * region, up to kCap particles of its SELF and FIRST neighbour entries (whole
+ * entries where they fit) in shared memory. Each own particle is tested
+ * against the staged neighbours one per lane, 32 candidates per step, for the
+ * cutoff, the reference's pruning and the existence of a potential (pass 1).
+ * Interacting candidates are appended, in candidate order, to a per-warp queue
+ * with a ballot; every 32 queued pairs are evaluated with one pair per lane
+ * (pass 2), so the expensive pair arithmetic runs with the warp's lanes full.
  *
- * Each neighbour entry carries the role of the cell in the reference's flipped
- * cell pair (runner_dopair.cpp:91-340, runner_doself :446-682): FIRST means the
- * reference computes dx = (x_i - shift) - x_j; SECOND means it computes
- * dx = (x_j - shift) - x_i with i as its second particle. Neighbour positions
- * of SECOND entries are staged pre-shifted and FIRST entries stage their shift
- * beside each particle, so every candidate computes d = (x_i - s) - b with one
- * formula; the reference's dx is d or its exact negation, which makes r2 and
- * the per-pair force bit-identical to the reference's.
+ * The queue is ordered by own particle: the own-side sums of a batch are formed
+ * by a segmented shuffle scan and added to the particle's force in shared
+ * memory by the segment's last lane; the neighbour-side contributions (the
+ * exact negations) are added to per-neighbour sums one segment after another
+ * (inside a segment the neighbours are distinct). At the end of a region the
+ * neighbour sums are stored in the plane that the neighbour cell reserves for
+ * this pair; after the pass, combine_kernel adds each particle's planes in
+ * plane order. Every sum has a fixed order: no atomics, deterministic results.
+ *
+ * FIRST entries stage their shift beside each neighbour particle, so every
+ * candidate computes d = (x_i - s) - x_j, the reference's dx for the pair (or
+ * its exact negation for a self pair whose first particle is j): r2 and the
+ * per-pair force are bit-identical to the reference's.
  */
 template <bool kDPD>
 __device__ __forceinline__ void pair_contribution(const EngineView &v, const DevPot &p, int role, bool i_first,
@@ -169,39 +187,46 @@ __device__ __forceinline__ void pair_contribution(const EngineView &v, const Dev
     }
 }
 
-constexpr int kOwn = 32;    // own particles staged at a time
-constexpr int kCap = 128;   // neighbour particles staged at a time
+constexpr int kOwn = 32;            // own particles staged at a time
+constexpr int kCap = 128;           // neighbour particles staged at a time
+constexpr int kChunks = kCap / 32;  // candidate steps per own particle
+constexpr int kQueue = 256;         // ring buffer of queued pairs (holds kCap + 31)
+constexpr int kEnt = 32;            // neighbour entries cached at a time
 
 template <bool kDPD>
 struct ForceSmem {
-    float4 nb_x[kCap];              // position (pre-shifted for SECOND entries); w = type
+    float4 nb_x[kCap];              // neighbour position; w = type
     float4 nb_s[kCap];              // shift of FIRST entries, else 0; w = role | entry << 2 | index << 8
+    float4 nb_f[kCap];              // neighbour-side force sums of the region
     float4 nb_v[kDPD ? kCap : 1];   // velocity; w = id
     float4 own_x[kOwn];
     float4 own_v[kDPD ? kOwn : 1];
     float4 own_f[kOwn];
-    float4 ent_sh[32];              // region entries: shift, w = packed role/sort direction/key shift
-    int ent_beg[33];                // first staged index of each region entry
-    int ent_slot[32];               // slot of the entry cell's first particle
-    int ent_jb[32];                 // index (within its cell) of the entry's first staged particle
-    int own_mask[kOwn];             // bit t: a potential exists for (own type, t), types < 32
-    int nb_key[kCap];               // sort key of the unshifted neighbour (per-pair pruning)
-    int queue[64];                  // own index << 16 | staged index, in candidate order
+    float4 ent_sh[kEnt];            // staged entries: shift, w = packed role/sort direction/key shift
+    int ent_slot[kEnt];             // slot of the entry cell's first particle
+    int ent_cnt[kEnt];              // particles of the entry cell
+    int ent_rev[kEnt];              // plane of the entry cell's received sums (FIRST entries)
+    int reg_beg[kEnt + 1];          // region: first staged index of each region entry
+    int reg_jb[kEnt];               // region: index within its cell of the entry's first staged particle
+    unsigned long long own_mask[kOwn];  // bit t: a potential exists for (own type, t)
+    int nb_key[kCap];               // sort key of the neighbour (per-pair pruning)
+    unsigned short queue[kQueue];   // own index << 8 | staged index, in candidate order
 };
 
-/* Pass 2 over queue[0, nb): one interacting pair per lane, segmented sums into
- * own_f. Returns the pairs counted once (statistics launch). */
+/* Pass 2 over the nb <= 32 queued pairs from qhead: one interacting pair per
+ * lane; own-side segmented sums into own_f, neighbour-side sums into nb_f. */
 template <bool kDPD, bool kStats>
-__device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD> &sm, int nb, int i0, int own_start,
-                                           int pot_base, unsigned rng_mode, double &ecell,
-                                           unsigned long long &npair) {
+__device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD> &sm, const float4 *tinfo, int qhead,
+                                           int nb, int i0, int own_start, int pot_base, unsigned rng_mode,
+                                           double &ecell, unsigned long long &npair) {
     const int lane = threadIdx.x & 31;
     float cx = 0.f, cy = 0.f, cz = 0.f;
-    int il = -1;
+    int il = -1, jj = 0;
+    bool nbside = false;
     if (lane < nb) {
-        const int cd = sm.queue[lane];
-        il = cd >> 16;
-        const int jj = cd & 0xffff;
+        const int cd = sm.queue[(qhead + lane) & (kQueue - 1)];
+        il = cd >> 8;
+        jj = cd & 0xff;
         const int i = i0 + il;
         const float4 xi = sm.own_x[il];
         const float4 b = sm.nb_x[jj];
@@ -211,8 +236,8 @@ __device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD> 
         float dx = __fsub_rn(__fsub_rn(xi.x, s.x), b.x);
         float dy = __fsub_rn(__fsub_rn(xi.y, s.y), b.y);
         float dz = __fsub_rn(__fsub_rn(xi.z, s.z), b.z);
-        // SECOND: the reference's dx is b - x_i; SELF with the neighbour first: x_j - x_i
-        if (role == kRoleSecond || (role == kRoleSelf && jl < i)) {
+        // a self pair whose first particle is j: the reference's dx is x_j - x_i
+        if (role == kRoleSelf && jl < i) {
             dx = -dx;
             dy = -dy;
             dz = -dz;
@@ -221,12 +246,13 @@ __device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD> 
         const int ti = __float_as_int(xi.w), tj = __float_as_int(b.w);
         const DevPot &p = v.pots[v.pot_idx[pot_base + ti * v.ntypes + tj]];
         const bool i_first = role == kRoleFirst || (role == kRoleSelf && i < jl);
+        nbside = role == kRoleFirst;
         if (r2 < p.a2) {
             // potential_eval_super_ex (dpd_eval.hpp:122-131): random direction of
             // length a; here a Philox draw keyed on the step and the id pair
             const unsigned idi = __float_as_uint(kDPD ? sm.own_v[il].w : v.vel[own_start + i].w);
             const unsigned idj =
-                __float_as_uint(kDPD ? sm.nb_v[jj].w : v.vel[sm.ent_slot[(meta >> 2) & 63] + jl].w);
+                __float_as_uint(kDPD ? sm.nb_v[jj].w : v.vel[sm.ent_slot[(meta >> 2) & 31] + jl].w);
             const unsigned lo = idi < idj ? idi : idj, hi = idi < idj ? idj : idi;
             float g0, g1, g2;
             philox_normal3(*v.step, lo, hi, g0, g1, g2);
@@ -242,14 +268,30 @@ __device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD> 
         const float4 vj = kDPD ? sm.nb_v[jj] : make_float4(0.f, 0.f, 0.f, 0.f);
         float pe;
         bool counted;
-        pair_contribution<kDPD>(v, p, role, i_first, dx, dy, dz, r2, v.types[ti].radius, v.types[tj].radius, vi,
-                                vj, rng_mode, cx, cy, cz, pe, counted);
+        pair_contribution<kDPD>(v, p, role, i_first, dx, dy, dz, r2, tinfo[ti].w, tinfo[tj].w, vi, vj, rng_mode,
+                                cx, cy, cz, pe, counted);
         ecell += (double)pe;
         if (kStats && counted) ++npair;
     }
-    // segmented inclusive scan: segments are runs of equal own index
+    // segments: runs of equal own index (inactive lanes form the last one)
     const int il_prev = __shfl_up_sync(kFull, il, 1);
     const unsigned heads = __ballot_sync(kFull, lane == 0 || il != il_prev);
+    // neighbour side, one segment after another (neighbours are distinct inside one)
+    unsigned segs = heads & (nb == 32 ? kFull : ((1u << nb) - 1u));
+    while (segs) {
+        const int h = __ffs(segs) - 1;
+        segs &= segs - 1;
+        const int next = segs ? __ffs(segs) - 1 : nb;
+        if (nbside && lane >= h && lane < next) {
+            float4 f = sm.nb_f[jj];
+            f.x = __fsub_rn(f.x, cx);
+            f.y = __fsub_rn(f.y, cy);
+            f.z = __fsub_rn(f.z, cz);
+            sm.nb_f[jj] = f;
+        }
+        __syncwarp();
+    }
+    // own side: segmented inclusive scan, the segment's last lane adds
     const int seg0 = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
     for (int off = 1; off < 32; off <<= 1) {
         const float ox = __shfl_up_sync(kFull, cx, off);
@@ -271,19 +313,47 @@ __device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD> 
     }
 }
 
+/* Zeroes the plane a cell owes a FIRST neighbour when it evaluates none of the
+ * pair's candidates (the cell is empty, or the reference's exit test skips the
+ * pair). */
+__device__ __forceinline__ void zero_plane(const EngineView &v, int rev, int nstart, int ncount) {
+    const int lane = threadIdx.x & 31;
+    float4 *dst = v.planes + (size_t)rev * v.nparts + nstart;
+    for (int k = lane; k < ncount; k += 32) dst[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+template <bool kDPD>
+constexpr size_t force_smem_bytes() {
+    return sizeof(ForceSmem<kDPD>) * kWarpsPerBlock;
+}
+
 template <bool kDPD, bool kStats>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) force_kernel(EngineView v) {
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) force_kernel(EngineView v) {
     unsigned long long npair = 0;  // interacting pairs counted once (statistics launch only)
-    __shared__ ForceSmem<kDPD> smem_all[kWarpsPerBlock];
+    extern __shared__ float4 force_smem[];
+    __shared__ float4 tinfo[kMaxTypes];  // per type: constant force (zero if none), radius
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    ForceSmem<kDPD> &sm = smem_all[w];
+    ForceSmem<kDPD> &sm = reinterpret_cast<ForceSmem<kDPD> *>(force_smem)[w];
     const unsigned lt_mask = (1u << lane) - 1u;
     const int ntypes = v.ntypes;
-    const bool use_mask = ntypes <= 32;
+    for (int t = threadIdx.x; t < ntypes; t += blockDim.x) {
+        const DevType &T = v.types[t];
+        // constant_force (MxForce.cpp:339-344), scale 1
+        tinfo[t] = T.has_force ? make_float4(T.fx, T.fy, T.fz, T.radius) : make_float4(0.f, 0.f, 0.f, T.radius);
+    }
+    __syncthreads();
     for (int c = blockIdx.x * kWarpsPerBlock + w; c < v.ncells; c += gridDim.x * kWarpsPerBlock) {
         const int n = v.cell_count[c];
+        const int nb0 = v.nb_off[c], nb1 = v.nb_off[c + 1];
         double ecell = 0.0;
-        if (n > 0) {
+        if (n == 0) {
+            for (int e = nb0; e < nb1; ++e) {
+                const int pk = __float_as_int(v.nb_shift[e].w);
+                if ((pk & 3) != kRoleFirst) continue;
+                const int nc = v.nb_cell[e];
+                zero_plane(v, v.nb_rev[e], v.cell_start[nc], v.cell_count[nc]);
+            }
+        } else {
             const int start = v.cell_start[c];
             const DevSpace &S = v.spaces[v.cell_rep[c]];
             const int pot_base = S.pot_offset;
@@ -293,7 +363,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) force_kernel(EngineView v
             const bool exit_test = (S.prune & 2) != 0;  // cell-pair exit test
             const float sbias = S.sort_bias, sdscale = S.sort_dscale;
             const int dmaxdist = S.dmaxdist;
-            const int nb0 = v.nb_off[c], nb1 = v.nb_off[c + 1];
             for (int i0 = 0; i0 < n; i0 += kOwn) {
                 const int ni = min(kOwn, n - i0);
                 __syncwarp();
@@ -301,152 +370,207 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) force_kernel(EngineView v
                     const float4 x = v.pos[start + i0 + lane];
                     sm.own_x[lane] = x;
                     const int ti = __float_as_int(x.w);
-                    const DevType &T = v.types[ti];
-                    // constant_force (MxForce.cpp:339-344), scale 1
-                    sm.own_f[lane] = T.has_force ? make_float4(T.fx, T.fy, T.fz, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    const float4 T = tinfo[ti];
+                    sm.own_f[lane] = make_float4(T.x, T.y, T.z, 0.f);
                     if (kDPD) sm.own_v[lane] = v.vel[start + i0 + lane];
-                    if (use_mask) {
-                        int mk = 0;
-                        for (int t = 0; t < ntypes; ++t)
-                            if (v.pot_idx[pot_base + ti * ntypes + t] >= 0) mk |= 1 << t;
-                        sm.own_mask[lane] = mk;
-                    }
+                    unsigned long long mk = 0ull;
+                    for (int t = 0; t < ntypes; ++t)
+                        if (v.pot_idx[pot_base + ti * ntypes + t] >= 0) mk |= 1ull << t;
+                    sm.own_mask[lane] = mk;
                 }
-                int e = nb0, jpos = 0;
-                while (e < nb1) {
-                    // ---- region: lane k describes entry e + k
-                    const int ek = e + lane;
-                    int cnt = 0, cstart = 0, pk = 0;
+                for (int g0 = nb0; g0 < nb1; g0 += kEnt) {
+                    // ---- entries g0 .. g0+31: lane k loads entry g0 + k; SELF and FIRST entries
+                    // with particles are staged (compacted in entry order)
+                    const int ek = g0 + lane;
+                    int cnt = 0, cstart = 0, rev = -1, skipped = 0;
                     float4 sh = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (ek < nb1) {
-                        const int nc = v.nb_cell[ek];
                         sh = v.nb_shift[ek];
-                        pk = __float_as_int(sh.w);
-                        cnt = v.cell_count[nc];
-                        cstart = v.cell_start[nc];
+                        const int pk = __float_as_int(sh.w);
                         const int role = pk & 3;
-                        if (cnt > 0 && exit_test && role != kRoleSelf) {
-                            // runner_dopair.cpp:167-171: kmin(second) + dnshift - kmax(first) in
-                            // unsigned arithmetic; above dmaxdist or wrapped, the pair is skipped
-                            const int sid = (pk >> 2) & 15;
-                            const int2 bc = v.sort_bounds[c * 13 + sid], bn = v.sort_bounds[nc * 13 + sid];
-                            const int kmax_first = role == kRoleFirst ? bc.y : bn.y;
-                            const int kmin_second = role == kRoleFirst ? bn.x : bc.x;
-                            const int gap = kmin_second + (pk >> 8) - kmax_first;
-                            if (gap < 0 || gap > dmaxdist) cnt = 0;
-                        }
-                    }
-                    const int jb = lane == 0 ? jpos : 0;
-                    const int rem = max(cnt - jb, 0);
-                    int incl = rem;
-                    for (int off = 1; off < 32; off <<= 1) {
-                        const int o = __shfl_up_sync(kFull, incl, off);
-                        if (lane >= off) incl += o;
-                    }
-                    const int nfit = __popc(__ballot_sync(kFull, ek < nb1 && incl <= kCap));
-                    int nent, M;
-                    if (nfit == 0) {  // the first entry alone holds more than kCap particles
-                        nent = 1;
-                        M = kCap;
-                        jpos += kCap;
-                    } else {
-                        nent = nfit;
-                        M = __shfl_sync(kFull, incl, nfit - 1);
-                        e += nfit;
-                        jpos = 0;
-                    }
-                    __syncwarp();
-                    if (lane < nent) {
-                        sm.ent_beg[lane] = incl - rem;
-                        sm.ent_slot[lane] = cstart;
-                        sm.ent_jb[lane] = jb;
-                        sm.ent_sh[lane] = sh;
-                    }
-                    if (lane == 0) sm.ent_beg[nent] = M;
-                    __syncwarp();
-                    if (M == 0) continue;
-                    // ---- stage the region's neighbour particles
-                    for (int idx = lane; idx < M; idx += 32) {
-                        int k = 0;
-                        for (int step = 16; step > 0; step >>= 1)
-                            if (k + step < nent && sm.ent_beg[k + step] <= idx) k += step;
-                        const int jl = sm.ent_jb[k] + idx - sm.ent_beg[k];
-                        const int slot = sm.ent_slot[k] + jl;
-                        const float4 es = sm.ent_sh[k];
-                        const int epk = __float_as_int(es.w);
-                        const int role = epk & 3;
-                        float4 q = v.pos[slot];
-                        if (prune) sm.nb_key[idx] = sort_key(q.x, q.y, q.z, v.axes->n[(epk >> 2) & 15], sbias, sdscale);
-                        float4 s4 = make_float4(0.f, 0.f, 0.f, __int_as_float(role | (k << 2) | (jl << 8)));
-                        if (role == kRoleSecond) {
-                            q.x = __fsub_rn(q.x, es.x);
-                            q.y = __fsub_rn(q.y, es.y);
-                            q.z = __fsub_rn(q.z, es.z);
-                        } else if (role == kRoleFirst) {
-                            s4.x = es.x;
-                            s4.y = es.y;
-                            s4.z = es.z;
-                        }
-                        sm.nb_x[idx] = q;
-                        sm.nb_s[idx] = s4;
-                        if (kDPD) sm.nb_v[idx] = v.vel[slot];
-                    }
-                    __syncwarp();
-                    // ---- pass 1 (candidates) and pass 2 (full batches)
-                    int qlen = 0;
-                    for (int il = 0; il < ni; ++il) {
-                        const float4 xi = sm.own_x[il];
-                        const int i = i0 + il;
-                        const int ti = __float_as_int(xi.w);
-                        const int mk = use_mask ? sm.own_mask[il] : 0;
-                        for (int jb0 = 0; jb0 < M; jb0 += 32) {
-                            const int jj = jb0 + lane;
-                            bool hit = false;
-                            if (jj < M) {
-                                const float4 b = sm.nb_x[jj];
-                                const float4 s = sm.nb_s[jj];
-                                const int meta = __float_as_int(s.w);
-                                const int role = meta & 3;
-                                const float dx = __fsub_rn(__fsub_rn(xi.x, s.x), b.x);
-                                const float dy = __fsub_rn(__fsub_rn(xi.y, s.y), b.y);
-                                const float dz = __fsub_rn(__fsub_rn(xi.z, s.z), b.z);
-                                const float r2 = dot3_rn(dx, dy, dz);
-                                const int tj = __float_as_int(b.w);
-                                hit = r2 <= (role == kRoleSelf ? cut2_self : cut2_pair);
-                                hit = hit && (use_mask ? ((mk >> tj) & 1) != 0
-                                                       : v.pot_idx[pot_base + ti * ntypes + tj] >= 0);
-                                if (role == kRoleSelf) hit = hit && (meta >> 8) != i;
-                                if (prune && hit && role != kRoleSelf) {
-                                    // runner_dopair's pruning: a pair (first, second) is evaluated
-                                    // only when key_second + dnshift - key_first < dmaxdist
-                                    // (runner_dopair.cpp:167-182)
-                                    const int epk = __float_as_int(sm.ent_sh[(meta >> 2) & 63].w);
-                                    const int okey =
-                                        sort_key(xi.x, xi.y, xi.z, v.axes->n[(epk >> 2) & 15], sbias, sdscale);
-                                    const int kf = role == kRoleFirst ? okey : sm.nb_key[jj];
-                                    const int ks = role == kRoleFirst ? sm.nb_key[jj] : okey;
-                                    hit = ks + (epk >> 8) - kf < dmaxdist;
+                        if (role != kRoleSecond) {
+                            const int nc = v.nb_cell[ek];
+                            cnt = v.cell_count[nc];
+                            cstart = v.cell_start[nc];
+                            rev = v.nb_rev[ek];
+                            if (cnt > 0 && exit_test && role == kRoleFirst) {
+                                // runner_dopair.cpp:167-171: kmin(second) + dnshift - kmax(first) in
+                                // unsigned arithmetic; above dmaxdist or wrapped, the pair is skipped
+                                const int sid = (pk >> 2) & 15;
+                                const int2 bc = v.sort_bounds[c * 13 + sid], bn = v.sort_bounds[nc * 13 + sid];
+                                const int gap = bn.x + (pk >> 8) - bc.y;
+                                if (gap < 0 || gap > dmaxdist) {
+                                    skipped = cnt;
+                                    cnt = 0;
                                 }
                             }
-                            const unsigned hb = __ballot_sync(kFull, hit);
-                            if (hit) sm.queue[qlen + __popc(hb & lt_mask)] = (il << 16) | jj;
-                            qlen += __popc(hb);
-                            if (qlen >= 32) {
-                                __syncwarp();
-                                eval_batch<kDPD, kStats>(v, sm, 32, i0, start, pot_base, rng_mode, ecell, npair);
-                                qlen -= 32;
-                                const int moved = lane < qlen ? sm.queue[32 + lane] : 0;
-                                __syncwarp();
-                                if (lane < qlen) sm.queue[lane] = moved;
-                                __syncwarp();
-                            }
                         }
                     }
-                    if (qlen > 0) {
-                        __syncwarp();
-                        eval_batch<kDPD, kStats>(v, sm, qlen, i0, start, pot_base, rng_mode, ecell, npair);
+                    // skipped pairs owe their neighbour a zero plane (written by the first own chunk)
+                    unsigned zmask = __ballot_sync(kFull, skipped > 0 && i0 == 0);
+                    while (zmask) {
+                        const int k = __ffs(zmask) - 1;
+                        zmask &= zmask - 1;
+                        zero_plane(v, __shfl_sync(kFull, rev, k), __shfl_sync(kFull, cstart, k),
+                                   __shfl_sync(kFull, skipped, k));
+                    }
+                    const unsigned staged = __ballot_sync(kFull, cnt > 0);
+                    const int nst = __popc(staged);
+                    __syncwarp();
+                    if (cnt > 0) {
+                        const int k = __popc(staged & lt_mask);
+                        sm.ent_sh[k] = sh;
+                        sm.ent_slot[k] = cstart;
+                        sm.ent_cnt[k] = cnt;
+                        sm.ent_rev[k] = rev;
                     }
                     __syncwarp();
+                    // ---- regions: consecutive staged entries holding at most kCap particles
+                    int ce = 0, jpos = 0;
+                    while (ce < nst) {
+                        const int rce = ce;
+                        const int k = ce + lane;
+                        const int jb = lane == 0 ? jpos : 0;
+                        const int rem = k < nst ? sm.ent_cnt[k] - jb : 0;
+                        int incl = rem;
+                        for (int off = 1; off < 32; off <<= 1) {
+                            const int o = __shfl_up_sync(kFull, incl, off);
+                            if (lane >= off) incl += o;
+                        }
+                        const int nfit = __popc(__ballot_sync(kFull, k < nst && incl <= kCap));
+                        int nent, M;
+                        if (nfit == 0) {  // the first entry alone holds more than kCap particles
+                            nent = 1;
+                            M = kCap;
+                            jpos += kCap;
+                        } else {
+                            nent = nfit;
+                            M = __shfl_sync(kFull, incl, nfit - 1);
+                            ce += nfit;
+                            jpos = 0;
+                        }
+                        __syncwarp();
+                        if (lane < nent) {
+                            sm.reg_beg[lane] = incl - rem;
+                            sm.reg_jb[lane] = jb;
+                        }
+                        if (lane == 0) sm.reg_beg[nent] = M;
+                        __syncwarp();
+                        // ---- stage the region's neighbour particles; lane's chunk-u neighbour
+                        // (staged index u * 32 + lane) is also kept in registers for pass 1
+                        float rbx[kChunks], rby[kChunks], rbz[kChunks], rsx[kChunks], rsy[kChunks], rsz[kChunks];
+                        float rc2[kChunks];   // cutoff squared; -1 for an empty position
+                        int rself[kChunks];   // index of a SELF neighbour within the cell, else -1
+                        int rtj[kChunks];     // neighbour type
+#pragma unroll
+                        for (int u = 0; u < kChunks; ++u) {
+                            const int idx = u * 32 + lane;
+                            rbx[u] = rby[u] = rbz[u] = rsx[u] = rsy[u] = rsz[u] = 0.f;
+                            rc2[u] = -1.f;
+                            rself[u] = -1;
+                            rtj[u] = 0;
+                            if (idx < M) {
+                                int r = 0;
+                                for (int step = 16; step > 0; step >>= 1)
+                                    if (r + step < nent && sm.reg_beg[r + step] <= idx) r += step;
+                                const int ke = rce + r;
+                                const int jl = sm.reg_jb[r] + idx - sm.reg_beg[r];
+                                const int slot = sm.ent_slot[ke] + jl;
+                                const float4 es = sm.ent_sh[ke];
+                                const int epk = __float_as_int(es.w);
+                                const int role = epk & 3;
+                                const float4 q = v.pos[slot];
+                                if (prune)
+                                    sm.nb_key[idx] =
+                                        sort_key(q.x, q.y, q.z, v.axes->n[(epk >> 2) & 15], sbias, sdscale);
+                                float4 s4 = make_float4(0.f, 0.f, 0.f, __int_as_float(role | (ke << 2) | (jl << 8)));
+                                if (role == kRoleFirst) {
+                                    s4.x = es.x;
+                                    s4.y = es.y;
+                                    s4.z = es.z;
+                                }
+                                sm.nb_x[idx] = q;
+                                sm.nb_s[idx] = s4;
+                                sm.nb_f[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+                                if (kDPD) sm.nb_v[idx] = v.vel[slot];
+                                rbx[u] = q.x;
+                                rby[u] = q.y;
+                                rbz[u] = q.z;
+                                rsx[u] = s4.x;
+                                rsy[u] = s4.y;
+                                rsz[u] = s4.z;
+                                rc2[u] = role == kRoleSelf ? cut2_self : cut2_pair;
+                                rself[u] = role == kRoleSelf ? jl : -1;
+                                rtj[u] = __float_as_int(q.w);
+                            }
+                        }
+                        __syncwarp();
+                        // ---- pass 1: each own particle against the region, kChunks steps of
+                        // 32 candidates, then pass 2 on every full batch of 32 queued pairs
+                        int qhead = 0, qtail = 0;
+                        for (int il = 0; il < ni; ++il) {
+                            const float4 xi = sm.own_x[il];
+                            const int i = i0 + il;
+                            const unsigned long long mk = sm.own_mask[il];
+                            unsigned hb[kChunks];
+#pragma unroll
+                            for (int u = 0; u < kChunks; ++u) {
+                                hb[u] = 0u;
+                                if (u * 32 < M) {
+                                    const float dx = __fsub_rn(__fsub_rn(xi.x, rsx[u]), rbx[u]);
+                                    const float dy = __fsub_rn(__fsub_rn(xi.y, rsy[u]), rby[u]);
+                                    const float dz = __fsub_rn(__fsub_rn(xi.z, rsz[u]), rbz[u]);
+                                    const float r2 = dot3_rn(dx, dy, dz);
+                                    bool hit = (r2 <= rc2[u]) & (((mk >> rtj[u]) & 1ull) != 0ull) & (rself[u] != i);
+                                    if (prune && hit && rself[u] < 0) {
+                                        // runner_dopair's pruning: a pair (first, second) is evaluated
+                                        // only when key_second + dnshift - key_first < dmaxdist
+                                        // (runner_dopair.cpp:167-182)
+                                        const int jj = u * 32 + lane;
+                                        const int meta = __float_as_int(sm.nb_s[jj].w);
+                                        const int epk = __float_as_int(sm.ent_sh[(meta >> 2) & 31].w);
+                                        const int okey =
+                                            sort_key(xi.x, xi.y, xi.z, v.axes->n[(epk >> 2) & 15], sbias, sdscale);
+                                        hit = sm.nb_key[jj] + (epk >> 8) - okey < dmaxdist;
+                                    }
+                                    hb[u] = __ballot_sync(kFull, hit);
+                                }
+                            }
+#pragma unroll
+                            for (int u = 0; u < kChunks; ++u) {
+                                if ((hb[u] >> lane) & 1u)
+                                    sm.queue[(qtail + __popc(hb[u] & lt_mask)) & (kQueue - 1)] =
+                                        (unsigned short)((il << 8) | (u * 32 + lane));
+                                qtail += __popc(hb[u]);
+                            }
+                            while (qtail - qhead >= 32) {
+                                __syncwarp();
+                                eval_batch<kDPD, kStats>(v, sm, tinfo, qhead, 32, i0, start, pot_base, rng_mode,
+                                                         ecell, npair);
+                                qhead += 32;
+                            }
+                        }
+                        if (qtail > qhead) {
+                            __syncwarp();
+                            eval_batch<kDPD, kStats>(v, sm, tinfo, qhead, qtail - qhead, i0, start, pot_base,
+                                                     rng_mode, ecell, npair);
+                        }
+                        __syncwarp();
+                        // ---- neighbour-side sums of FIRST entries into their planes
+                        for (int idx = lane; idx < M; idx += 32) {
+                            const int meta = __float_as_int(sm.nb_s[idx].w);
+                            if ((meta & 3) != kRoleFirst) continue;
+                            const int ke = (meta >> 2) & 31;
+                            float4 *dst = v.planes + (size_t)sm.ent_rev[ke] * v.nparts + sm.ent_slot[ke] + (meta >> 8);
+                            float4 f = sm.nb_f[idx];
+                            if (i0 > 0) {  // later own chunks add to the first chunk's sums
+                                const float4 o = *dst;
+                                f = make_float4(o.x + f.x, o.y + f.y, o.z + f.z, 0.f);
+                            }
+                            *dst = f;
+                        }
+                        __syncwarp();
+                    }
                 }
                 __syncwarp();
                 if (lane < ni) {
@@ -462,6 +586,28 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) force_kernel(EngineView v
         for (int off = 16; off > 0; off >>= 1) npair += __shfl_xor_sync(kFull, npair, off);
         if (lane == 0) atomicAdd(v.pair_stats, npair);
     }
+}
+
+/* A particle's own-side force plus the sums its cell received from the cells
+ * that evaluated their shared pairs, in plane order. */
+__device__ __forceinline__ float4 total_force(const EngineView &v, int s) {
+    float4 f = v.force[s];
+    const int np = v.sec_count[v.cell_of[s]];
+    for (int k = 0; k < np; ++k) {
+        const float4 g = v.planes[(size_t)k * v.nparts + s];
+        f.x += g.x;
+        f.y += g.y;
+        f.z += g.z;
+    }
+    return f;
+}
+
+/* Completes the force pass when neither the bond kernel nor the integrator
+ * follows it: force = total_force. */
+__global__ void combine_kernel(EngineView v) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= v.nparts) return;
+    v.force[s] = total_force(v, s);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -483,8 +629,8 @@ __global__ void bond_kernel(EngineView v, const DevBond *__restrict__ bonds, uns
     const int id = __float_as_int(v.vel[s].w);
     const int k0 = bond_off[id], k1 = bond_off[id + 1];
     double eb = 0.0;
+    float4 f = total_force(v, s);  // the bond pass completes the nonbonded force
     if (k0 < k1) {
-        float4 f = v.force[s];
         for (int k = k0; k < k1; ++k) {
             const int b = bond_list[k];
             if (!(bond_flags[b] & 1u)) continue;
@@ -531,8 +677,8 @@ __global__ void bond_kernel(EngineView v, const DevBond *__restrict__ bonds, uns
                 f.z = __fadd_rn(f.z, wz);
             }
         }
-        v.force[s] = f;
     }
+    v.force[s] = f;
     ebond_slot[s] = eb;
 }
 
@@ -553,14 +699,15 @@ __device__ __forceinline__ int cell_delta(float x, float h) { return (x >= h ? 1
  * counted implicitly (count_old - out + in).
  */
 __global__ void integrate_kernel(EngineView v, float4 *pos, float4 *vel, int *new_cell, int *in_count,
-                                 int *in_list, int *out_count) {
+                                 int *in_list, int *out_count, bool add_planes) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= v.nparts) return;
     const int c = v.cell_of[s];
     const DevSpace &S = v.spaces[v.cell_rep[c]];
     float4 x = pos[s];
     float4 u = vel[s];
-    const float4 f = v.force[s];
+    const float4 f = add_planes ? total_force(v, s) : v.force[s];
+    if (add_planes) v.force[s] = f;  // the integrator completes the nonbonded force
     const DevType &T = v.types[__float_as_int(x.w)];
     const unsigned fz_all = (1u << 2) | (1u << 3) | (1u << 4);
     int dest = c;
@@ -662,35 +809,58 @@ __global__ void integrate_kernel(EngineView v, float4 *pos, float4 *vel, int *ne
 /* ------------------------------------------------------------------------ */
 
 /* New occupancy count_old - out + in, exclusive scan into new_start; single
- * block, each thread scans a contiguous run of cells. */
+ * block, each thread scans a contiguous run of cells (loads issued eight at a
+ * time), warp-shuffle scans across the threads. */
 __global__ void __launch_bounds__(1024) scan_kernel(int ncells, const int *__restrict__ old_count,
                                                    const int *__restrict__ out_count, const int *__restrict__ in_count,
                                                    int *new_start, int *new_count, unsigned long long *step) {
-    __shared__ int part[1024];
-    const int t = threadIdx.x;
+    __shared__ int warp_total[32];
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
     const int per = (ncells + blockDim.x - 1) / blockDim.x;
     const int b = t * per, e = min(ncells, b + per);
     int sum = 0;
-    for (int c = b; c < e; ++c) {
-        const int n = old_count[c] - out_count[c] + min(in_count[c], kBucket);
-        new_count[c] = n;
-        sum += n;
+    for (int c0 = b; c0 < e; c0 += 8) {
+        int nv[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int c = c0 + k;
+            nv[k] = c < e ? old_count[c] - out_count[c] + min(in_count[c], kBucket) : 0;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (c0 + k < e) new_count[c0 + k] = nv[k];
+            sum += nv[k];
+        }
     }
-    part[t] = sum;
+    int incl = sum;
+    for (int off = 1; off < 32; off <<= 1) {
+        const int o = __shfl_up_sync(kFull, incl, off);
+        if (lane >= off) incl += o;
+    }
+    if (lane == 31) warp_total[wid] = incl;
     __syncthreads();
-    for (int off = 1; off < blockDim.x; off <<= 1) {  // Hillis-Steele inclusive scan
-        const int add = t >= off ? part[t - off] : 0;
-        __syncthreads();
-        part[t] += add;
-        __syncthreads();
+    if (wid == 0) {
+        int x = lane < (int)(blockDim.x >> 5) ? warp_total[lane] : 0;
+        for (int off = 1; off < 32; off <<= 1) {
+            const int o = __shfl_up_sync(kFull, x, off);
+            if (lane >= off) x += o;
+        }
+        warp_total[lane] = x;
     }
-    int run = part[t] - sum;
-    for (int c = b; c < e; ++c) {
-        new_start[c] = run;
-        run += new_count[c];
+    __syncthreads();
+    int run = (wid > 0 ? warp_total[wid - 1] : 0) + incl - sum;
+    for (int c0 = b; c0 < e; c0 += 8) {
+        int nv[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) nv[k] = c0 + k < e ? new_count[c0 + k] : 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (c0 + k < e) new_start[c0 + k] = run;
+            run += nv[k];
+        }
     }
-    if (t == blockDim.x - 1) {
-        new_start[ncells] = part[t];
+    if (t == (int)blockDim.x - 1) {
+        new_start[ncells] = warp_total[31];
         *step += 1;  // the step counter keying the Philox streams
     }
 }
@@ -698,9 +868,10 @@ __global__ void __launch_bounds__(1024) scan_kernel(int ncells, const int *__res
 /*
  * One warp per destination cell. Stayers keep their relative order (ascending
  * id); movers are merged in by id, so every cell stays sorted by id and the
- * layout is independent of thread scheduling.
+ * layout is independent of thread scheduling. The warp then computes the new
+ * cell's projection-key bounds for the next force pass.
  */
-__global__ void scatter_kernel(int ncells, const float4 *__restrict__ pos, const float4 *__restrict__ vel,
+__global__ void scatter_kernel(EngineView v, int ncells, const float4 *__restrict__ pos, const float4 *__restrict__ vel,
                                const int *__restrict__ new_cell, const int *__restrict__ old_start,
                                const int *__restrict__ old_count, int *in_count, const int *__restrict__ in_list,
                                int *out_count, const int *__restrict__ new_start, float4 *pos_out, float4 *vel_out,
@@ -758,6 +929,11 @@ __global__ void scatter_kernel(int ncells, const float4 *__restrict__ pos, const
             in_count[c] = 0;
             out_count[c] = 0;
         }
+        // the next force pass's cell-pair exit test reads the new cell's key bounds
+        const int nn = new_start[c + 1] - base;
+        const DevSpace &S = v.spaces[v.cell_rep[c]];
+        if (nn > 0 && (S.prune & 2))
+            cell_sort_bounds(pos_out, base, nn, S.sort_bias, S.sort_dscale, v.axes, v.sort_bounds + c * 13);
     }
 }
 
@@ -814,29 +990,39 @@ __global__ void reduce_final_kernel(int nblocks, const double *partials, double 
 /* ------------------------------------------------------------------------ */
 
 void configure_force_kernels() {
-    // the force kernel's occupancy is bounded by shared memory: ask for the
-    // largest shared-memory carveout of the unified L1/shared storage
+    // the force kernel's occupancy is bounded by shared memory: allow its dynamic
+    // shared memory and ask for the largest carveout of the unified L1/shared storage
     const int carve = cudaSharedmemCarveoutMaxShared;
+    const int bd = (int)force_smem_bytes<true>(), bn = (int)force_smem_bytes<false>();
+    cudaFuncSetAttribute(force_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bd);
+    cudaFuncSetAttribute(force_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bd);
+    cudaFuncSetAttribute(force_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bn);
+    cudaFuncSetAttribute(force_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bn);
     cudaFuncSetAttribute(force_kernel<true, true>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
     cudaFuncSetAttribute(force_kernel<true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
     cudaFuncSetAttribute(force_kernel<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
     cudaFuncSetAttribute(force_kernel<false, false>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
 }
 
-void launch_force(const EngineView &v, bool has_dpd, int grid, cudaStream_t st) {
-    const bool stats = v.pair_stats != nullptr;
+void launch_sort_bounds(const EngineView &v, cudaStream_t st) {
     sort_bounds_kernel<<<(v.ncells * 32 + 255) / 256, 256, 0, st>>>(v);
+}
+
+void launch_force(const EngineView &v, bool has_dpd, int grid, bool combine, cudaStream_t st) {
+    const bool stats = v.pair_stats != nullptr;
+    const size_t bd = force_smem_bytes<true>(), bn = force_smem_bytes<false>();
     if (has_dpd) {
         if (stats)
-            force_kernel<true, true><<<grid, kWarpsPerBlock * 32, 0, st>>>(v);
+            force_kernel<true, true><<<grid, kWarpsPerBlock * 32, bd, st>>>(v);
         else
-            force_kernel<true, false><<<grid, kWarpsPerBlock * 32, 0, st>>>(v);
+            force_kernel<true, false><<<grid, kWarpsPerBlock * 32, bd, st>>>(v);
     } else {
         if (stats)
-            force_kernel<false, true><<<grid, kWarpsPerBlock * 32, 0, st>>>(v);
+            force_kernel<false, true><<<grid, kWarpsPerBlock * 32, bn, st>>>(v);
         else
-            force_kernel<false, false><<<grid, kWarpsPerBlock * 32, 0, st>>>(v);
+            force_kernel<false, false><<<grid, kWarpsPerBlock * 32, bn, st>>>(v);
     }
+    if (combine) combine_kernel<<<(v.nparts + 255) / 256, 256, 0, st>>>(v);
 }
 
 void launch_bonds(const EngineView &v, const DevBond *bonds, unsigned *bond_flags, const int *bond_off,
@@ -847,9 +1033,10 @@ void launch_bonds(const EngineView &v, const DevBond *bonds, unsigned *bond_flag
 }
 
 void launch_integrate(const EngineView &v, float4 *pos, float4 *vel, int *new_cell, int *in_count, int *in_list,
-                      int *out_count, cudaStream_t st) {
+                      int *out_count, bool add_planes, cudaStream_t st) {
     const int tb = 256;
-    integrate_kernel<<<(v.nparts + tb - 1) / tb, tb, 0, st>>>(v, pos, vel, new_cell, in_count, in_list, out_count);
+    integrate_kernel<<<(v.nparts + tb - 1) / tb, tb, 0, st>>>(v, pos, vel, new_cell, in_count, in_list, out_count,
+                                                             add_planes);
 }
 
 void launch_scan(int ncells, const int *old_count, const int *out_count, const int *in_count, int *new_start,
@@ -857,12 +1044,13 @@ void launch_scan(int ncells, const int *old_count, const int *out_count, const i
     scan_kernel<<<1, 1024, 0, st>>>(ncells, old_count, out_count, in_count, new_start, new_count, step);
 }
 
-void launch_scatter(int ncells, const float4 *pos, const float4 *vel, const int *new_cell, const int *old_start,
-                    const int *old_count, int *in_count, const int *in_list, int *out_count, const int *new_start,
-                    float4 *pos_out, float4 *vel_out, int *cell_out, int *slot_of_id, cudaStream_t st) {
+void launch_scatter(const EngineView &v, const float4 *pos, const float4 *vel, const int *new_cell,
+                    const int *old_start, const int *old_count, int *in_count, const int *in_list, int *out_count,
+                    const int *new_start, float4 *pos_out, float4 *vel_out, int *cell_out, int *slot_of_id,
+                    cudaStream_t st) {
     const int tb = 256;
-    const int grid = (ncells * 32 + tb - 1) / tb;
-    scatter_kernel<<<grid, tb, 0, st>>>(ncells, pos, vel, new_cell, old_start, old_count, in_count, in_list,
+    const int grid = (v.ncells * 32 + tb - 1) / tb;
+    scatter_kernel<<<grid, tb, 0, st>>>(v, v.ncells, pos, vel, new_cell, old_start, old_count, in_count, in_list,
                                          out_count, new_start, pos_out, vel_out, cell_out, slot_of_id);
 }
 

@@ -5,16 +5,19 @@
 namespace mxg {
 
 void configure_force_kernels();
-void launch_force(const EngineView &v, bool has_dpd, int grid, cudaStream_t st);
+void launch_sort_bounds(const EngineView &v, cudaStream_t st);
+/* combine: add the received planes here (no bond or integrator pass follows) */
+void launch_force(const EngineView &v, bool has_dpd, int grid, bool combine, cudaStream_t st);
 void launch_bonds(const EngineView &v, const DevBond *bonds, unsigned *bond_flags, const int *bond_off,
                   const int *bond_list, const int *slot_of_id, double *ebond_slot, cudaStream_t st);
 void launch_integrate(const EngineView &v, float4 *pos, float4 *vel, int *new_cell, int *in_count, int *in_list,
-                      int *out_count, cudaStream_t st);
+                      int *out_count, bool add_planes, cudaStream_t st);
 void launch_scan(int ncells, const int *old_count, const int *out_count, const int *in_count, int *new_start,
                  int *new_count, unsigned long long *step, cudaStream_t st);
-void launch_scatter(int ncells, const float4 *pos, const float4 *vel, const int *new_cell, const int *old_start,
-                    const int *old_count, int *in_count, const int *in_list, int *out_count, const int *new_start,
-                    float4 *pos_out, float4 *vel_out, int *cell_out, int *slot_of_id, cudaStream_t st);
+void launch_scatter(const EngineView &v, const float4 *pos, const float4 *vel, const int *new_cell,
+                    const int *old_start, const int *old_count, int *in_count, const int *in_list, int *out_count,
+                    const int *new_start, float4 *pos_out, float4 *vel_out, int *cell_out, int *slot_of_id,
+                    cudaStream_t st);
 void launch_energy(int ncells, const double *epot_cell, int nparts, const double *ebond_slot, const float4 *vel,
                    const float4 *pos, const DevType *types, double *partials, int nblocks, double *out,
                    cudaStream_t st);
