@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--n", type=int, default=200000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-forms", action="store_true", help="skip the other configurations (batched, LJ, lattice)")
     return ap.parse_args()
 
 
@@ -165,6 +166,97 @@ def reference_arm(args):
                                        f"nr_runners = {cores}"},
             "e2e": {"value": val, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def _time_steps(L, e, K, stream, flush):
+    """Device time (ms) of K single steps of engine e, L2 flushed between steps
+    outside the per-step events."""
+    import torch
+    a = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    b = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    with torch.cuda.stream(stream):
+        for k in range(K):
+            flush.zero_()
+            a[k].record(stream)
+            L.mxg_engine_step(e, 1)
+            b[k].record(stream)
+    torch.cuda.synchronize()
+    return sum(x.elapsed_time(y) for x, y in zip(a, b))
+
+
+def _plain(u, stream):
+    """Moves a universe built by the workload helpers onto the bench stream."""
+    u.stream = stream.cuda_stream
+    u._dirty = True
+    u._ensure()
+    return u._e
+
+
+def forms_and_configs(args, stream, flush):
+    """The other configurations on the same GPU: the LJ argon fluid and the
+    bonded lattice (plain engine), and the batched ensemble of 256 cell-sorting
+    replicas against the same replicas run one after another."""
+    import mechanica_b200 as m
+    from mechanica_b200 import workloads as W
+    from mechanica_b200._native import lib, check
+    L = lib()
+    out = {}
+    K = max(10, min(args.steps, 200))
+    for name, build in (("lj_argon_10k", lambda: W.argon(n=10000, L=10.0, cells=10, seed=21)),
+                        ("lattice_32k", lambda: W.lattice(nx=32, seed=23))):
+        scn = build()
+        W.build_gpu(scn)
+        e = _plain(m.universe, stream)
+        with torch_stream(stream):
+            check(L.mxg_engine_step(e, 3), "warm-up")
+        ms = _time_steps(L, e, K, stream, flush)
+        check(L.mxg_engine_status(e), name)
+        n = len(scn["t"])
+        out[name] = {"value": n * K / (ms / 1e3), "unit": "particle-steps/s", "particles": n, "steps": K,
+                     "ms_per_step": ms / K}
+        m.universe.close()
+
+    # batched ensemble: all replicas in one engine, one set of launches per step
+    specs = W.cell_sorting_specs(nrep=256, seed=5)
+    ntot = sum(len(sc["t"]) for sc in specs)
+    Kb = max(5, min(args.steps, 50))
+    u = W.build_gpu_batch(specs, stream=stream.cuda_stream)
+    u._ensure()
+    per_sm = u.autotune()
+    e = u._e
+    with torch_stream(stream):
+        check(L.mxg_engine_step(e, 3), "warm-up")
+    ms_b = _time_steps(L, e, Kb, stream, flush)
+    check(L.mxg_engine_status(e), "batched")
+    u.close()
+    # the same replicas, one plain engine each, run one after another
+    ms_s = 0.0
+    for sc in specs:
+        W.build_gpu(sc)
+        e = _plain(m.universe, stream)
+        with torch_stream(stream):
+            check(L.mxg_engine_step(e, 3), "warm-up")
+        ms_s += _time_steps(L, e, Kb, stream, flush)
+        check(L.mxg_engine_status(e), "sequential")
+        m.universe.close()
+    out["batched_256"] = {"value": ntot * Kb / (ms_b / 1e3), "unit": "particle-steps/s", "replicas": len(specs),
+                          "particles": ntot, "steps": Kb, "ms_per_step": ms_b / Kb,
+                          "force_ctas_per_sm": per_sm,
+                          "sequential_plain_value": ntot * Kb / (ms_s / 1e3),
+                          "speedup_vs_sequential": ms_s / ms_b}
+    return out
+
+
+class torch_stream:
+    def __init__(self, stream):
+        import torch
+        self.ctx = torch.cuda.stream(stream)
+
+    def __enter__(self):
+        return self.ctx.__enter__()
+
+    def __exit__(self, *a):
+        return self.ctx.__exit__(*a)
 
 
 def main():
@@ -323,6 +415,11 @@ def main():
         except Exception as exc:  # the baseline is reported, not required
             cpu = {"error": str(exc)[:300]}
 
+    m.universe.close()
+    forms = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        forms = forms_and_configs(args, stream, flush)
+
     line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": K,
             "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
@@ -336,10 +433,9 @@ def main():
                     "path": "mxg_engine_copy_state (pinned host -> device), mxg_engine_step, "
                             "mxg_engine_copy_state (device -> pinned host), mxg_engine_energy_async"},
             "roofline": roofline, "cpu_baseline": cpu, "accuracy": accuracy,
-            "wall_s_timed_region": t_wall}
+            "forms": forms, "wall_s_timed_region": t_wall}
     if rank == 0:
         print(json.dumps(line))
-    m.universe.close()
     if world > 1:
         dist.destroy_process_group()
 

@@ -22,7 +22,8 @@ namespace mxg {
 constexpr int kChunk = 8;           // floats per table interval
 constexpr int kBucket = 32;         // max particles entering one cell per step
 constexpr int kMaxTypes = 64;       // types per engine
-constexpr int kWarpsPerBlock = 4;   // force kernel: warps (cells) per block
+constexpr int kWarpsPerBlock = 4;   // force kernel: warps (work items) per block
+constexpr int kMaxCellParts = 4;    // force work items per cell at most
 
 /* neighbour-entry roles, relative to the reference's (flipped) cell pair */
 enum : int { kRoleSelf = 0, kRoleFirst = 1, kRoleSecond = 2 };
@@ -127,12 +128,15 @@ struct EngineView {      // everything a kernel needs, passed by value
     const unsigned long long *step;  // device step counter
     const SortAxes *axes;
     int2 *sort_bounds;               // per cell and sort axis: (min key, max key)
-    double *epot_cell;       // per cell nonbonded energy of the last force pass
+    double *epot_cell;       // per force work item: nonbonded energy of the last force pass
     unsigned *status;
     unsigned long long *pair_stats;  // non-null only for the statistics launch
     const int *nb_rev;       // FIRST entries: the pair's plane in the neighbour's received sums
     const int *sec_count;    // per cell: SECOND entries, i.e. planes of received sums
+    const int *cell_planes;  // per cell: received planes plus own-side planes of its later work items
     float4 *planes;          // [plane][slot] neighbour-side force sums of once-evaluated pairs
+    const int4 *items;       // force work items: (cell, first entry, end entry, part)
+    int nitems;
 };
 
 #ifdef __CUDACC__

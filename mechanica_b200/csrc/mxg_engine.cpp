@@ -351,6 +351,9 @@ struct mxg_engine {
     float4 *d_nb_shift = nullptr;
     float4 *d_planes = nullptr;
     int nplanes = 0;
+    int4 *d_items = nullptr;            // force work items: (cell, first entry, end entry, part)
+    int *d_cell_planes = nullptr;       // planes summed into each cell's forces
+    int nitems = 0;
     DevPot *d_pots = nullptr;
     float *d_coef = nullptr;
     int *d_pot_idx = nullptr;
@@ -492,6 +495,9 @@ struct mxg_engine {
         v.pair_stats = nullptr;
         v.nb_rev = d_nb_rev;
         v.sec_count = d_sec_count;
+        v.cell_planes = d_cell_planes;
+        v.items = d_items;
+        v.nitems = nitems;
         v.planes = d_planes;
         return v;
     }
@@ -586,18 +592,48 @@ int mxg_engine::start(cudaStream_t st) {
             }
         }
     }
-    std::vector<int> nb_off(ncells + 1, 0), nb_cell, nb_rev;
-    std::vector<float4> nb_shift;
-    for (int c = 0; c < ncells; ++c) {
-        nb_off[c + 1] = nb_off[c] + (int)nb[c].size();
-        for (auto &e : nb[c]) {
-            nb_cell.push_back(e.cell);
-            nb_shift.push_back(e.shift);
-            nb_rev.push_back(e.rev);
-        }
+    // ---- work items: each cell's SELF and FIRST entries split into up to `parts`
+    // groups (one warp each) when there are too few cells to fill the GPU. Item k > 0
+    // of a cell sums its own-side forces into plane sec_count + k - 1 of the cell.
+    {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        num_sms = sms;
     }
+    const int want_warps = num_sms * 32;
+    const int parts = std::max(1, std::min(kMaxCellParts, (want_warps + ncells - 1) / std::max(1, ncells)));
+    std::vector<int> nb_off(ncells + 1, 0), nb_cell, nb_rev, hplanes(ncells, 0);
+    std::vector<float4> nb_shift;
+    std::vector<int4> hitems;
+    for (int c = 0; c < ncells; ++c) {
+        std::vector<const NbEntry *> self_e, first_e, second_e;
+        for (auto &e : nb[c]) {
+            int pk;
+            memcpy(&pk, &e.shift.w, 4);
+            ((pk & 3) == kRoleSelf ? self_e : (pk & 3) == kRoleFirst ? first_e : second_e).push_back(&e);
+        }
+        const int nf = (int)first_e.size();
+        const int groups = std::max(1, std::min(parts, nf));
+        auto push = [&](const NbEntry *e) {
+            nb_cell.push_back(e->cell);
+            nb_shift.push_back(e->shift);
+            nb_rev.push_back(e->rev);
+        };
+        for (int g = 0; g < groups; ++g) {
+            const int e0 = (int)nb_cell.size();
+            if (g == 0)
+                for (auto *e : self_e) push(e);
+            for (int k = g * nf / groups; k < (g + 1) * nf / groups; ++k) push(first_e[k]);
+            hitems.push_back(make_int4(c, e0, (int)nb_cell.size(), g));
+        }
+        for (auto *e : second_e) push(e);
+        nb_off[c + 1] = (int)nb_cell.size();
+        hplanes[c] = hsec[c] + groups - 1;
+    }
+    nitems = (int)hitems.size();
     nplanes = 0;
-    for (int c = 0; c < ncells; ++c) nplanes = std::max(nplanes, hsec[c]);
+    for (int c = 0; c < ncells; ++c) nplanes = std::max(nplanes, hplanes[c]);
 
     // ---- potentials, types, replicas ----
     std::vector<DevPot> hp;
@@ -702,6 +738,8 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_nb_shift, nb_shift.size());
     rc |= alloc(&d_nb_rev, nb_rev.size());
     rc |= alloc(&d_sec_count, ncells);
+    rc |= alloc(&d_cell_planes, ncells);
+    rc |= alloc(&d_items, hitems.size());
     rc |= alloc(&d_planes, (size_t)nplanes * nparts);
     rc |= alloc(&d_pots, hp.size());
     rc |= alloc(&d_coef, coef.size() + 8);
@@ -710,7 +748,7 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_spaces, hs.size());
     rc |= alloc(&d_axes, 1);
     rc |= alloc(&d_sort_bounds, (size_t)ncells * 13);
-    rc |= alloc(&d_epot_cell, ncells);
+    rc |= alloc(&d_epot_cell, nitems);
     rc |= alloc(&d_ebond_slot, nparts);
     rc |= alloc(&d_bonds, hb.size());
     rc |= alloc(&d_bond_flags, hbf.size());
@@ -726,7 +764,7 @@ int mxg_engine::start(cudaStream_t st) {
     CUDA_TRY(cudaMemsetAsync(d_out_count, 0, sizeof(int) * ncells, stream));
     CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
     CUDA_TRY(cudaMemsetAsync(d_step, 0, sizeof(unsigned long long), stream));
-    CUDA_TRY(cudaMemsetAsync(d_epot_cell, 0, sizeof(double) * ncells, stream));
+    CUDA_TRY(cudaMemsetAsync(d_epot_cell, 0, sizeof(double) * std::max(1, nitems), stream));
     CUDA_TRY(cudaMemsetAsync(d_ebond_slot, 0, sizeof(double) * std::max(1, nparts), stream));
     CUDA_TRY(cudaMemsetAsync(d_force, 0, sizeof(float4) * std::max(1, nparts), stream));
     if ((rc = upload(d_pos[0], hpos, stream)) || (rc = upload(d_vel[0], hvel, stream)) ||
@@ -735,7 +773,8 @@ int mxg_engine::start(cudaStream_t st) {
         (rc = upload(d_cell_rep, hrep, stream)) || (rc = upload(d_cell_flags, hcflags, stream)) ||
         (rc = upload(d_nb_off, nb_off, stream)) || (rc = upload(d_nb_cell, nb_cell, stream)) ||
         (rc = upload(d_nb_shift, nb_shift, stream)) || (rc = upload(d_nb_rev, nb_rev, stream)) ||
-        (rc = upload(d_sec_count, hsec, stream)) || (rc = upload(d_pots, hp, stream)) ||
+        (rc = upload(d_sec_count, hsec, stream)) || (rc = upload(d_cell_planes, hplanes, stream)) ||
+        (rc = upload(d_items, hitems, stream)) || (rc = upload(d_pots, hp, stream)) ||
         (rc = upload(d_coef, coef, stream)) || (rc = upload(d_pot_idx, hpidx, stream)) ||
         (rc = upload(d_types, ht, stream)) || (rc = upload(d_spaces, hs, stream)) || (rc = upload(d_axes, haxes, stream)) ||
         (rc = upload(d_bonds, hb, stream)) || (rc = upload(d_bond_flags, hbf, stream)) ||
@@ -743,12 +782,8 @@ int mxg_engine::start(cudaStream_t st) {
         return rc;
     CUDA_TRY(cudaStreamSynchronize(stream));
 
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    num_sms = sms;
     configure_force_kernels();
-    force_grid = std::max(1, std::min((ncells + kWarpsPerBlock - 1) / kWarpsPerBlock, sms * 16));
+    force_grid = std::max(1, std::min((nitems + kWarpsPerBlock - 1) / kWarpsPerBlock, num_sms * 16));
     cur = 0;
     started = true;
     refresh_bounds();
@@ -1140,7 +1175,7 @@ int mxg_engine_load(mxg_engine *e, int n, const double *x, const float *v) {
 int mxg_engine_energy(mxg_engine *e, double *epot, double *ekin, double *virial9) {
     if (!e) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
-    launch_energy(e->ncells, e->d_epot_cell, e->nparts, e->bonds.empty() ? nullptr : e->d_ebond_slot,
+    launch_energy(e->nitems, e->d_epot_cell, e->nparts, e->bonds.empty() ? nullptr : e->d_ebond_slot,
                   e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
                   e->stream);
     double out[2];
@@ -1224,7 +1259,7 @@ int mxg_engine_copy_state(mxg_engine *e, void *host_pos, void *host_vel, int to_
 int mxg_engine_energy_async(mxg_engine *e, double *host_out2) {
     if (!e || !host_out2) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
-    launch_energy(e->ncells, e->d_epot_cell, e->nparts, e->bonds.empty() ? nullptr : e->d_ebond_slot,
+    launch_energy(e->nitems, e->d_epot_cell, e->nparts, e->bonds.empty() ? nullptr : e->d_ebond_slot,
                   e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
                   e->stream);
     CUDA_TRY(cudaMemcpyAsync(host_out2, e->d_energy, 2 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
@@ -1273,7 +1308,7 @@ int mxg_engine_autotune(mxg_engine *e) {
     if (!e->started) return MXG_ERR_STATE;
     if (e->nparts == 0) return MXG_OK;
     const int cands[] = {2, 4, 6, 8, 12, 16, 24, 32};
-    const int max_grid = (e->ncells + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    const int max_grid = (e->nitems + kWarpsPerBlock - 1) / kWarpsPerBlock;
     int best = e->force_grid, best_per_sm = 0;
     float best_ms = 1e30f;
     cudaEvent_t a, b;

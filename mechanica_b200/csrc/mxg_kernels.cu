@@ -342,9 +342,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) force_kernel(EngineVie
         tinfo[t] = T.has_force ? make_float4(T.fx, T.fy, T.fz, T.radius) : make_float4(0.f, 0.f, 0.f, T.radius);
     }
     __syncthreads();
-    for (int c = blockIdx.x * kWarpsPerBlock + w; c < v.ncells; c += gridDim.x * kWarpsPerBlock) {
+    for (int it = blockIdx.x * kWarpsPerBlock + w; it < v.nitems; it += gridDim.x * kWarpsPerBlock) {
+        const int4 item = v.items[it];
+        const int c = item.x, nb0 = item.y, nb1 = item.z, part = item.w;
         const int n = v.cell_count[c];
-        const int nb0 = v.nb_off[c], nb1 = v.nb_off[c + 1];
         double ecell = 0.0;
         if (n == 0) {
             for (int e = nb0; e < nb1; ++e) {
@@ -370,8 +371,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) force_kernel(EngineVie
                     const float4 x = v.pos[start + i0 + lane];
                     sm.own_x[lane] = x;
                     const int ti = __float_as_int(x.w);
-                    const float4 T = tinfo[ti];
-                    sm.own_f[lane] = make_float4(T.x, T.y, T.z, 0.f);
+                    const float4 T = tinfo[ti];  // the body force goes with the cell's first work item
+                    sm.own_f[lane] = part == 0 ? make_float4(T.x, T.y, T.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
                     if (kDPD) sm.own_v[lane] = v.vel[start + i0 + lane];
                     unsigned long long mk = 0ull;
                     for (int t = 0; t < ntypes; ++t)
@@ -575,12 +576,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) force_kernel(EngineVie
                 __syncwarp();
                 if (lane < ni) {
                     const float4 f = sm.own_f[lane];
-                    v.force[start + i0 + lane] = make_float4(f.x, f.y, f.z, 0.f);
+                    // the cell's first work item writes the force, later ones their own plane
+                    float4 *dst = part == 0 ? v.force : v.planes + (size_t)(v.sec_count[c] + part - 1) * v.nparts;
+                    dst[start + i0 + lane] = make_float4(f.x, f.y, f.z, 0.f);
                 }
             }
         }
         for (int off = 16; off > 0; off >>= 1) ecell += __shfl_xor_sync(kFull, ecell, off);
-        if (lane == 0) v.epot_cell[c] = ecell;
+        if (lane == 0) v.epot_cell[it] = ecell;
     }
     if (kStats) {
         for (int off = 16; off > 0; off >>= 1) npair += __shfl_xor_sync(kFull, npair, off);
@@ -588,11 +591,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) force_kernel(EngineVie
     }
 }
 
-/* A particle's own-side force plus the sums its cell received from the cells
- * that evaluated their shared pairs, in plane order. */
+/* A particle's own-side force plus, in plane order, the sums its cell received
+ * from the cells that evaluated their shared pairs and the own-side sums of its
+ * cell's later work items. */
 __device__ __forceinline__ float4 total_force(const EngineView &v, int s) {
     float4 f = v.force[s];
-    const int np = v.sec_count[v.cell_of[s]];
+    const int np = v.cell_planes[v.cell_of[s]];
     for (int k = 0; k < np; ++k) {
         const float4 g = v.planes[(size_t)k * v.nparts + s];
         f.x += g.x;
