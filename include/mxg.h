@@ -34,6 +34,7 @@
 #ifndef MXG_H_
 #define MXG_H_
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -115,6 +116,21 @@ int mxg_potential_dpd_params(const mxg_potential *p, float *alpha, float *gamma,
 /* Host scalar evaluation with potential_eval_ex semantics: returns 1 if in range. */
 int mxg_potential_eval(const mxg_potential *p, float ri, float rj, float r2, float *e, float *f);
 void mxg_potential_free(mxg_potential *p);
+/* Frozen-node re-fit of a table potential at new construction parameters (layout as in
+ * mxg_engine_set_pot_params); the interval count, map and nodes stay those of the first fit. For a
+ * DPD potential the three coefficients change (cutoff and shift flag must stay). */
+int mxg_potential_refit(mxg_potential *p, const double *params, int nparams);
+/* The table's coefficients before their rounding to float (FP64, same layout as
+ * mxg_potential_coeffs); returns their number. No counterpart in the reference. */
+int mxg_potential_coeffs64(const mxg_potential *p, double *out, int cap);
+/* The construction parameters of a potential (layout as in mxg_engine_set_pot_params); returns
+ * their number, copying at most cap into out (out may be NULL). */
+int mxg_potential_params(const mxg_potential *p, double *out, int cap);
+/* The table (same nodes, map and interval count) of dV/dtheta_k for construction parameter k of a
+ * table potential: LJ A (k=2), B (3); Morse d (0), alpha (1); harmonic k (0), r0 (1). Returns
+ * MXG_ERR_ARG for parameters that do not change the tabulated function (Morse r0 only shifts the
+ * argument). No counterpart in the reference. */
+int mxg_potential_param_table(const mxg_potential *p, int k, mxg_potential **out);
 
 /* ---- engine ---- */
 /* bc_kind[6]: MXG_BOUNDARY_* per face (faces above); bc_velocity[18]: wall velocity per face for
@@ -136,6 +152,21 @@ int mxg_engine_nr_replicas(const mxg_engine *e);
 int mxg_engine_addpot_replica(mxg_engine *e, int replica, const mxg_potential *p, int type_i, int type_j);
 int mxg_engine_addparts_replica(mxg_engine *e, int replica, int n, const double *x, const float *v,
                                 const int *type, int *ids_out);
+/* A second potential on a type pair, summed with the pair's first one (a table potential plus a
+ * DPD thermostat, say); each term keeps its own cutoff and table. No counterpart in the reference,
+ * whose engine_addpot keeps one potential per type pair (engine.cpp:968-977). */
+int mxg_engine_addpot_second(mxg_engine *e, int replica, const mxg_potential *p, int type_i, int type_j);
+/* The engine's index of the potential bound to (type_i, type_j) of a replica: which = 0 for the
+ * pair's potential, 1 for the summed second one; -1 in *idx when there is none. */
+int mxg_engine_pot_index(mxg_engine *e, int replica, int type_i, int type_j, int which, int *idx);
+/* New construction parameters for the engine's potential idx (the layout the create call takes,
+ * minus the trailing output: LJ (a, b, A, B, tol), Morse (d, alpha, r0, min, max, tol), harmonic
+ * (k, r0, min, max, tol), DPD (alpha, gamma, sigma, cutoff, shifted)). Tables are re-fitted on their
+ * frozen nodes (same interval count and map), so a table's coefficients are a linear function of
+ * the sampled potential and parameter derivatives are exact for the tabulated model; on a started
+ * engine the device copy is updated in place, ordered on the engine stream. No counterpart in the
+ * reference. */
+int mxg_engine_set_pot_params(mxg_engine *e, int idx, const double *params, int nparams);
 /* Chooses the force kernel's grid (CTAs per SM) by timing candidate launches on the current state;
  * returns the chosen blocks per SM. Call after mxg_engine_start. */
 int mxg_engine_autotune(mxg_engine *e);
@@ -188,6 +219,39 @@ int mxg_engine_copy_state(mxg_engine *e, void *host_pos, void *host_vel, int to_
 /* Enqueues the FP64 energy reduction and an asynchronous copy of (epot, ekin) into host_out2. */
 int mxg_engine_energy_async(mxg_engine *e, double *host_out2);
 int mxg_engine_finalize(mxg_engine *e);
+
+/* ---- adjoint (reverse-mode gradients of trajectories) ---- No counterpart in the reference. ---- */
+/* Bytes of a state snapshot (positions, velocities, cell lists, id map, step counter, bond flags). */
+int mxg_engine_snapshot_bytes(const mxg_engine *e, size_t *bytes);
+/* save = 1: copies the current state into dev_buf (device memory, 16-byte aligned); save = 0: makes
+ * dev_buf's state current. Ordered on the engine stream; restoring then stepping reproduces the
+ * trajectory bit for bit (the step counter that keys the Philox streams is part of the state). */
+int mxg_engine_snapshot(mxg_engine *e, void *dev_buf, int save);
+/* Registers the differentiated parameters: entry k adds d loss / d (parameter param[k] of the
+ * engine's potential pot[k]) into gradient slot slot[k] (< 16; several entries may share a slot).
+ * Parameters use the construction layout of mxg_engine_set_pot_params: LJ A (2), B (3); Morse d (0),
+ * alpha (1), r0 (2); harmonic k (0), r0 (1); DPD alpha (0), gamma (1), sigma (2). */
+int mxg_engine_adjoint_params(mxg_engine *e, int n, const int *pot, const int *param, const int *slot);
+/* Vector-Jacobian product of one step taken from the current state. lam_x, lam_v: device float4
+ * arrays indexed by particle id, holding the adjoints of the positions and velocities after the step;
+ * on return (stream-ordered) they hold the adjoints of the state before it. grad: device double array
+ * of the gradient slots, to which the step's parameter terms are added. Periodic boxes, nonbonded
+ * potentials (tables, DPD, summed pairs) and constant forces; bonds are refused (MXG_ERR_ARG). */
+int mxg_engine_vjp_step(mxg_engine *e, void *lam_x, void *lam_v, double *grad);
+/* Device float4 arrays by particle id: absolute positions (x, y, z, type bits) and velocities
+ * (v, id bits); either pointer may be NULL. Stream-ordered. */
+int mxg_engine_positions(mxg_engine *e, void *x4, void *v4);
+/* Sets the step counter that keys the Philox streams (after a load, to replay a trajectory). */
+int mxg_engine_set_step_counter(mxg_engine *e, unsigned long long step);
+/* Gaussian-smoothed pair histogram of particle types (type_a, type_b) in a periodic box:
+ * hist[b] += 2^32 * sum over pairs (i of type_a, j of type_b, i != j) of K(r_ij - (b + 1/2) dr),
+ * K a Gaussian of width sigma (normalised, minus its value at 4 sigma) cut at |r - centre| > 4 sigma, as uint64 fixed point (device array of
+ * nbins <= 256; the sums do not depend on the order of the additions). With coef (device double per
+ * bin) and grad4 (device float4 per particle): grad4[i] = d(sum_b coef[b] hist[b]) / d x_i, unscaled.
+ * x4: device float4 (x, y, z, type bits) per particle; box: host double[3]. The workload's loss
+ * (an A-B radial distribution) is built on it. No counterpart in the reference. */
+int mxg_rdf(const void *x4, int n, const double *box, int type_a, int type_b, int nbins, double dr, double sigma,
+            void *hist, const double *coef, void *grad4, void *stream);
 
 /* DPD random term: 0 = reference semantics (xi = 1, dpd_eval.hpp:57), 1 = Philox stream keyed on
  * (step, particle id pair). Set before mxg_engine_start. */

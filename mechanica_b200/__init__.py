@@ -107,6 +107,14 @@ def parse_bc(bc):
     raise TypeError("bc must be an int flag set or a dict")
 
 
+class PotentialSum:
+    """Two potentials summed on the same type pairs (Potential.__add__)."""
+
+    def __init__(self, first, second):
+        self.terms = (first, second)
+        self.name = f"{first.name} + {second.name}"
+
+
 class Potential:
     """A tabulated (or DPD) pair potential; factories mirror MxPotential.cpp:2459-2750."""
 
@@ -160,6 +168,26 @@ class Potential:
         # the reference stores the parameters as float (MxPotential.cpp:2738-2750)
         return Potential._make("mxg_potential_create_dpd", (alpha, gamma, sigma, cutoff, int(bool(shifted))),
                                "Dissapative Particle Dynamics")
+
+    def __add__(self, other):
+        """p1 + p2: both potentials act on the pairs they are bound to, summed
+        (a table potential plus a DPD thermostat, say). No counterpart in the
+        reference, which binds one potential per type pair."""
+        if not isinstance(other, Potential):
+            return NotImplemented
+        return PotentialSum(self, other)
+
+    def refit(self, params):
+        """Frozen-node re-fit at new construction parameters (same nodes and
+        interval count), so the coefficients are linear in the sampled potential."""
+        q = np.ascontiguousarray(params, dtype=np.float64)
+        check(lib().mxg_potential_refit(self._h, ptr(q, ctypes.c_double), len(q)), "potential_refit")
+
+    def param_table(self, k):
+        """The table of dV/dtheta_k on this table's nodes (see mxg_potential_param_table)."""
+        h = ctypes.c_void_p()
+        check(lib().mxg_potential_param_table(self._h, int(k), ctypes.byref(h)), "potential_param_table")
+        return Potential(h.value, self.name + f" d/dparam{k}")
 
     def _info(self):
         kind, flags, n = ctypes.c_int(), ctypes.c_uint(), ctypes.c_int()
@@ -348,8 +376,11 @@ class _Universe:
                   "add_replica")
         for (m, r, d, fl) in self._types:
             check(lib().mxg_engine_addtype(self._e, m, r, d, fl), "addtype")
-        for (p, a, b, rep) in self._pots:
-            check(lib().mxg_engine_addpot_replica(self._e, rep, p._h, a, b), "addpot")
+        for (p, a, b, rep, which) in self._pots:
+            if which == 0:
+                check(lib().mxg_engine_addpot_replica(self._e, rep, p._h, a, b), "addpot")
+            else:
+                check(lib().mxg_engine_addpot_second(self._e, rep, p._h, a, b), "addpot_second")
         for (t, v) in self._forces:
             check(lib().mxg_engine_add_singlebody_force(self._e, t, float(v[0]), float(v[1]), float(v[2])),
                   "add_singlebody_force")
@@ -397,10 +428,12 @@ class _Universe:
     def bind(self, obj, a, b=None, replica=0):
         """Binds a potential to a pair of types, or a force to a type (MxBind.cpp:18-100)."""
         ta = a.id if isinstance(a, type) else int(a)
-        if isinstance(obj, Potential):
+        if isinstance(obj, (Potential, PotentialSum)):
             tb = ta if b is None else (b.id if isinstance(b, type) else int(b))
             self._sync_state()
-            self._pots.append((obj, ta, tb, int(replica)))
+            terms = obj.terms if isinstance(obj, PotentialSum) else (obj,)
+            for which, p in enumerate(terms):
+                self._pots.append((p, ta, tb, int(replica), which))
             self._dirty = True
         elif isinstance(obj, _ConstantForce):
             self._sync_state()
@@ -408,6 +441,29 @@ class _Universe:
             self._dirty = True
         else:
             raise TypeError("bind expects a Potential or a force")
+
+    def potential_index(self, a, b, replica=0, which=0):
+        """The engine's index of the potential bound to types (a, b)."""
+        self._ensure()
+        ta = a.id if isinstance(a, type) else int(a)
+        tb = b.id if isinstance(b, type) else int(b)
+        idx = ctypes.c_int()
+        check(lib().mxg_engine_pot_index(self._e, int(replica), ta, tb, int(which), ctypes.byref(idx)), "pot_index")
+        return idx.value
+
+    def set_potential_params(self, pot, params):
+        """New construction parameters for a bound potential: the host object is
+        re-fitted on its frozen nodes and every engine copy of it is updated in place."""
+        q = np.ascontiguousarray(params, dtype=np.float64)
+        pot.refit(q)
+        if self._e is None or self._dirty or not self._started:
+            self._dirty = True
+            return
+        for (p, a, b, rep, which) in self._pots:
+            if p is pot:
+                idx = self.potential_index(a, b, rep, which)
+                check(lib().mxg_engine_set_pot_params(self._e, idx, ptr(q, ctypes.c_double), len(q)),
+                      "set_pot_params")
 
     # ---- engine lifecycle ----
     def _sync_state(self):

@@ -102,6 +102,22 @@ _SIGS = {
                                ctypes.c_int),
     "mxg_engine_nr_replicas": ([_vp], ctypes.c_int),
     "mxg_engine_addpot_replica": ([_vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "mxg_engine_addpot_second": ([_vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "mxg_engine_pot_index": ([_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _c_int_p],
+                             ctypes.c_int),
+    "mxg_engine_set_pot_params": ([_vp, ctypes.c_int, _c_double_p, ctypes.c_int], ctypes.c_int),
+    "mxg_engine_snapshot_bytes": ([_vp, ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
+    "mxg_engine_snapshot": ([_vp, _vp, ctypes.c_int], ctypes.c_int),
+    "mxg_engine_adjoint_params": ([_vp, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p], ctypes.c_int),
+    "mxg_engine_vjp_step": ([_vp, _vp, _vp, _vp], ctypes.c_int),
+    "mxg_engine_positions": ([_vp, _vp, _vp], ctypes.c_int),
+    "mxg_engine_set_step_counter": ([_vp, ctypes.c_ulonglong], ctypes.c_int),
+    "mxg_rdf": ([_vp, ctypes.c_int, _c_double_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                 ctypes.c_double, _vp, _vp, _vp, _vp], ctypes.c_int),
+    "mxg_potential_params": ([_vp, _c_double_p, ctypes.c_int], ctypes.c_int),
+    "mxg_potential_coeffs64": ([_vp, _c_double_p, ctypes.c_int], ctypes.c_int),
+    "mxg_potential_refit": ([_vp, _c_double_p, ctypes.c_int], ctypes.c_int),
+    "mxg_potential_param_table": ([_vp, ctypes.c_int, _vpp], ctypes.c_int),
     "mxg_engine_addparts_replica": ([_vp, ctypes.c_int, ctypes.c_int, _c_double_p, _c_float_p, _c_int_p, _c_int_p],
                                     ctypes.c_int),
     "mxg_engine_autotune": ([_vp], ctypes.c_int),

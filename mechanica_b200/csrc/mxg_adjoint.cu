@@ -1,0 +1,632 @@
+/*
+ * Adjoint (reverse-mode) kernels of the force-and-step path.
+ *
+ * One forward-Euler step maps (x, v) to (x', v'):
+ *     v'_k = clamp(mask_k (v_k + dt f_k(x, v; theta) imass))       (Newtonian)
+ *     x'   = x + dt v'
+ * or, overdamped, x'_k = x_k + clamp(mask_k dt f_k imass) with v unchanged
+ * (engine_advance.cpp:126-239). Given the adjoints (lx, lv) of (x', v'), the
+ * step's vector-Jacobian product is
+ *     g      = lv + dt lx            (adjoint of v', Newtonian)
+ *     gpre_k = clamped_k ? 0 : g_k   (through the speed clamp and the frozen mask)
+ *     w      = dt imass gpre         (adjoint of the force on the particle)
+ *     lx_in  = lx + sum_pairs J_x^T (w_i - w_j)
+ *     lv_in  = gpre + sum_pairs J_v^T (w_i - w_j)
+ *     dL/dtheta += sum_pairs (dF_ij/dtheta) . (w_i - w_j)
+ * where F_ij is the force of j on i. The pair sums are taken by vjp_pair_kernel
+ * over the same cell-pair lists as the force pass, but from both sides (each
+ * cell sums its own particles' terms from all 27 neighbour entries), so no
+ * cross-warp sums are needed. Parameter gradients are counted once per pair
+ * (on the side with the smaller particle id) in FP64.
+ *
+ * The derivative of a tabulated potential is that of the piecewise polynomial
+ * itself, and parameter derivatives use tables of dV/dtheta fitted on the same
+ * frozen nodes (the fit is linear in the sampled function), so the gradients
+ * are those of the tabulated model the forward pass integrates. Wall
+ * reflections and bonds are not differentiated (the adjoint covers periodic
+ * boxes and nonbonded potentials plus constant forces).
+ */
+#include "mxg_adjoint.h"
+#include "mxg_device.cuh"
+
+namespace mxg {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kOwnA = 32;              // own particles staged at a time
+constexpr int kCapA = 64;              // neighbour particles staged at a time
+constexpr int kChunksA = kCapA / 32;
+constexpr int kQueueA = 128;           // ring buffer of queued pairs (holds kCapA + 31)
+constexpr int kEntA = 32;              // neighbour entries cached at a time
+constexpr int kWarpsA = 4;             // warps (cells) per block
+
+struct AdjSmem {
+    float4 nb_x[kCapA];   // neighbour position (SECOND entries pre-shifted); w = type
+    float4 nb_s[kCapA];   // shift of FIRST entries, else 0; w = role | entry << 2 | index << 8
+    float4 nb_v[kCapA];   // velocity; w = id
+    float4 nb_w[kCapA];   // force adjoint
+    float4 own_x[kOwnA];
+    float4 own_v[kOwnA];
+    float4 own_w[kOwnA];
+    float4 own_gx[kOwnA];
+    float4 own_gv[kOwnA];
+    float4 ent_sh[kEntA];
+    int ent_slot[kEntA];
+    int ent_cnt[kEntA];
+    int reg_beg[kEntA + 1];
+    int reg_jb[kEntA];
+    unsigned long long own_mask[kOwnA];
+    unsigned short queue[kQueueA];
+};
+
+constexpr size_t adj_smem_bytes() {
+    return (sizeof(AdjSmem) + 32 * kMaxGradSlots * sizeof(double)) * kWarpsA;
+}
+
+/* P(x), P'(x), P''(x) of an interval polynomial c[2] x^5 + ... + c[7]. */
+__device__ __forceinline__ void poly3(const float *c, float x, float &p, float &dp, float &ddp) {
+    p = c[2];
+    dp = 0.f;
+    float d2 = 0.f;
+#pragma unroll
+    for (int k = 3; k < 8; ++k) {
+        d2 = d2 * x + dp;
+        dp = dp * x + p;
+        p = p * x + c[k];
+    }
+    ddp = 2.f * d2;
+}
+
+/* Table term: adds J_x^T u to gx and the parameter terms (if count) into g. */
+__device__ __forceinline__ void table_vjp(const EngineView &v, const AdjointView &a, int pidx, const DevPot &p,
+                                          float radi, float radj, const float3 &d, float r2, const float3 &u,
+                                          bool count, float3 &gx, double *g) {
+    const float r = sqrtf(r2);
+    const float ro = r < 1.19209290e-7f ? 1.19209290e-7f : r;
+    const bool clamped = r < p.a;
+    const float rr = clamped ? p.a : r;
+    float s = rr, dsdr = 1.f;
+    if (p.flags & (1u << 11)) {
+        s = rr / (radi + radj);
+        dsdr = 1.f / (radi + radj);
+    } else if (p.flags & (1u << 12)) {
+        s = rr - (radi + radj) + p.r0_plusone;
+    }
+    if (clamped) dsdr = 0.f;
+    const float t = p.alpha0 + s * (p.alpha1 + s * p.alpha2);
+    const unsigned ind = (unsigned)fmaxf(0.0f, t);
+    if (s > p.b || ind > (unsigned)p.n) return;
+    const float *c = v.coef + p.coef_off + ind * kChunk;
+    const float x = (s - c[0]) * c[1];
+    float P, dP, ddP;
+    poly3(c, x, P, dP, ddP);
+    const float vp = dP * c[1], vpp = ddP * c[1] * c[1];
+    const float f = vp / ro;
+    const float dfdr = vpp * dsdr / ro - (r >= 1.19209290e-7f ? vp / (ro * ro) : 0.f);
+    const float du = d.x * u.x + d.y * u.y + d.z * u.z;
+    const float k = r > 0.f ? dfdr / r * du : 0.f;
+    // F_i = -f d:  J^T u = -(f u + (df/dr / r)(d.u) d)
+    gx.x -= f * u.x + k * d.x;
+    gx.y -= f * u.y + k * d.y;
+    gx.z -= f * u.z + k * d.z;
+    if (!count) return;
+    const DevPotGrad &pg = a.pot_grad[pidx];
+    for (int q = 0; q < pg.n; ++q) {
+        float fth = 0.f;
+        if (pg.mode[q] == kGradTable) {
+            const float *cd = a.dcoef + pg.coef_off[q] + ind * kChunk;
+            float Pq, dPq, ddPq;
+            poly3(cd, x, Pq, dPq, ddPq);
+            fth = dPq * c[1] / ro;
+        } else if (pg.mode[q] == kGradShift) {
+            fth = vpp / ro;  // d s / d r0 = 1
+        } else {
+            continue;
+        }
+        g[pg.slot[q]] += (double)(-fth * du);
+    }
+}
+
+/* DPD term (dpd_eval.hpp:21-69 with xi): adds J_x^T u, J_v^T u and the
+ * parameter terms. */
+__device__ __forceinline__ void dpd_vjp(const EngineView &v, const AdjointView &a, int pidx, const DevPot &p,
+                                        float radi, float radj, const float3 &d, float r2, const float3 &vij,
+                                        float xi_rand, const float3 &u, bool count, float3 &gx, float3 &gv,
+                                        double *g) {
+    const bool shifted = p.flags & (1u << 12);
+    const float cutoff = shifted ? p.b + radi + radj : p.b;
+    if (r2 > cutoff * cutoff || r2 <= 0.f) return;
+    const float r = sqrtf(r2);
+    const float ir = 1.f / r;
+    const float3 e = make_float3(d.x * ir, d.y * ir, d.z * ir);
+    const float sr = shifted ? r - radi - radj : r;
+    const bool inner = sr < 0.f;
+    const float om = inner ? 1.f : 1.f - sr / cutoff;
+    const float domdr = inner ? 0.f : -1.f / cutoff;
+    const float sv = e.x * vij.x + e.y * vij.y + e.z * vij.z;
+    const float eu = e.x * u.x + e.y * u.y + e.z * u.z;
+    const float rnd = p.dpd_sigma * xi_rand * p.dpd_delta;
+    const float h = p.dpd_alpha * om - p.dpd_gamma * om * om * sv + rnd * om;
+    const float dhdr = (p.dpd_alpha - 2.f * p.dpd_gamma * om * sv + rnd) * domdr;
+    const float dhds = -p.dpd_gamma * om * om;
+    // d(u.F)/dd = dh/dr (e.u) e + dh/ds (e.u) (v - s e)/r + h (u - (e.u) e)/r
+    const float a1 = dhdr * eu, a2 = dhds * eu * ir, a3 = h * ir;
+    gx.x += a1 * e.x + a2 * (vij.x - sv * e.x) + a3 * (u.x - eu * e.x);
+    gx.y += a1 * e.y + a2 * (vij.y - sv * e.y) + a3 * (u.y - eu * e.y);
+    gx.z += a1 * e.z + a2 * (vij.z - sv * e.z) + a3 * (u.z - eu * e.z);
+    gv.x += dhds * eu * e.x;
+    gv.y += dhds * eu * e.y;
+    gv.z += dhds * eu * e.z;
+    if (!count) return;
+    const DevPotGrad &pg = a.pot_grad[pidx];
+    for (int q = 0; q < pg.n; ++q) {
+        float dth;
+        if (pg.mode[q] == kGradDpdAlpha)
+            dth = om * eu;
+        else if (pg.mode[q] == kGradDpdGamma)
+            dth = -om * om * sv * eu;
+        else if (pg.mode[q] == kGradDpdSigma)
+            dth = om * xi_rand * p.dpd_delta * eu;
+        else
+            continue;
+        g[pg.slot[q]] += (double)dth;
+    }
+}
+
+__device__ __forceinline__ void term_vjp(const EngineView &v, const AdjointView &a, int pidx, float radi,
+                                         float radj, const float3 &d, float r2, const float3 &vij, unsigned ida,
+                                         unsigned idb, unsigned rng_mode, const float3 &u, bool count, float3 &gx,
+                                         float3 &gv, double *g) {
+    const DevPot &p = v.pots[pidx];
+    if (r2 < p.a2) return;  // the random-direction branch is not differentiated
+    if (p.kind == 1) {
+        float xr = 1.0f;
+        if (rng_mode) {
+            const unsigned lo = ida < idb ? ida : idb, hi = ida < idb ? idb : ida;
+            xr = philox_pair_xi(*v.step, lo, hi);
+        }
+        dpd_vjp(v, a, pidx, p, radi, radj, d, r2, vij, xr, u, count, gx, gv, g);
+    } else {
+        table_vjp(v, a, pidx, p, radi, radj, d, r2, u, count, gx, g);
+    }
+}
+
+/* Per slot: the adjoint through the integrator; w = dt imass gpre is the
+ * adjoint of the particle's force. f must hold the forces of the state. */
+__global__ void adj_prep_kernel(EngineView v, AdjointView a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= v.nparts) return;
+    const float4 x = v.pos[s], u = v.vel[s], f = v.force[s];
+    const int id = __float_as_int(u.w);
+    const DevType &T = v.types[__float_as_int(x.w)];
+    const DevSpace &S = v.spaces[v.cell_rep[v.cell_of[s]]];
+    const float4 lx = a.lam_x[id], lv = a.lam_v[id];
+    const float lxv[3] = {lx.x, lx.y, lx.z}, lvv[3] = {lv.x, lv.y, lv.z};
+    const float uv[3] = {u.x, u.y, u.z}, fv[3] = {f.x, f.y, f.z};
+    float w[3] = {0.f, 0.f, 0.f}, gv[3] = {lvv[0], lvv[1], lvv[2]};
+    const unsigned fz_all = (1u << 2) | (1u << 3) | (1u << 4);
+    if ((T.flags & fz_all) != fz_all) {
+        const float dt = S.dt;
+        for (int k = 0; k < 3; ++k) {
+            const bool frozen = T.flags & (1u << (2 + k));
+            if (T.dynamics == 0) {
+                // a frozen component gets v' = 0 (the mask), so nothing flows back through it
+                const float vk = (float)((double)uv[k] + (double)(dt * fv[k]) * T.imass);
+                const bool clamped = frozen || vk * vk > S.maxv2[k];
+                const float gk = lvv[k] + dt * lxv[k];
+                const float gpre = clamped ? 0.f : gk;
+                gv[k] = gpre;
+                w[k] = (float)((double)(gpre * dt) * T.imass);
+            } else {
+                const float dxk = (float)((double)(dt * fv[k]) * T.imass);
+                const bool clamped = frozen || dxk * dxk > S.maxx2[k];
+                w[k] = clamped ? 0.f : (float)((double)(lxv[k] * dt) * T.imass);
+            }
+        }
+    }
+    a.w[s] = make_float4(w[0], w[1], w[2], 0.f);
+    a.gx[s] = make_float4(lxv[0], lxv[1], lxv[2], 0.f);
+    a.gv[s] = make_float4(gv[0], gv[1], gv[2], 0.f);
+}
+
+/* Pair terms of the step's VJP. One warp per cell, full shell (SELF, FIRST and
+ * SECOND entries); the structure follows force_kernel: staged regions, a
+ * candidate pass one neighbour per lane, then the interacting pairs 32 at a
+ * time with per-particle segmented sums. */
+__global__ void __launch_bounds__(kWarpsA * 32, 4) vjp_pair_kernel(EngineView v, AdjointView a) {
+    extern __shared__ float4 adj_smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    AdjSmem &sm = reinterpret_cast<AdjSmem *>(adj_smem)[w];
+    double *gl = reinterpret_cast<double *>(reinterpret_cast<AdjSmem *>(adj_smem) + kWarpsA) +
+                 (size_t)(w * 32 + lane) * kMaxGradSlots;  // this lane's parameter sums
+    for (int q = 0; q < kMaxGradSlots; ++q) gl[q] = 0.0;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const int ntypes = v.ntypes;
+    for (int c = blockIdx.x * kWarpsA + w; c < v.ncells; c += gridDim.x * kWarpsA) {
+        const int n = v.cell_count[c];
+        if (n == 0) continue;
+        const int start = v.cell_start[c];
+        const DevSpace &S = v.spaces[v.cell_rep[c]];
+        const int pot_base = S.pot_offset;
+        const float cut2_pair = S.cut2_pair, cut2_self = S.cut2_self;
+        const unsigned rng_mode = S.rng_mode;
+        const int nb0 = v.nb_off[c], nb1 = v.nb_off[c + 1];
+        for (int i0 = 0; i0 < n; i0 += kOwnA) {
+            const int ni = min(kOwnA, n - i0);
+            __syncwarp();
+            if (lane < ni) {
+                const int sl = start + i0 + lane;
+                const float4 x = v.pos[sl];
+                sm.own_x[lane] = x;
+                sm.own_v[lane] = v.vel[sl];
+                sm.own_w[lane] = a.w[sl];
+                sm.own_gx[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+                sm.own_gv[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+                const int ti = __float_as_int(x.w);
+                unsigned long long mk = 0ull;
+                for (int t = 0; t < ntypes; ++t)
+                    if (v.pot_idx[pot_base + ti * ntypes + t] >= 0) mk |= 1ull << t;
+                sm.own_mask[lane] = mk;
+            }
+            for (int g0 = nb0; g0 < nb1; g0 += kEntA) {
+                const int ek = g0 + lane;
+                int cnt = 0, cstart = 0;
+                float4 sh = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (ek < nb1) {
+                    sh = v.nb_shift[ek];
+                    const int nc = v.nb_cell[ek];
+                    cnt = v.cell_count[nc];
+                    cstart = v.cell_start[nc];
+                }
+                const unsigned staged = __ballot_sync(kFull, cnt > 0);
+                const int nst = __popc(staged);
+                __syncwarp();
+                if (cnt > 0) {
+                    const int k = __popc(staged & lt_mask);
+                    sm.ent_sh[k] = sh;
+                    sm.ent_slot[k] = cstart;
+                    sm.ent_cnt[k] = cnt;
+                }
+                __syncwarp();
+                int ce = 0, jpos = 0;
+                while (ce < nst) {
+                    const int rce = ce;
+                    const int k = ce + lane;
+                    const int jb = lane == 0 ? jpos : 0;
+                    const int rem = k < nst ? sm.ent_cnt[k] - jb : 0;
+                    int incl = rem;
+                    for (int off = 1; off < 32; off <<= 1) {
+                        const int o = __shfl_up_sync(kFull, incl, off);
+                        if (lane >= off) incl += o;
+                    }
+                    const int nfit = __popc(__ballot_sync(kFull, k < nst && incl <= kCapA));
+                    int nent, M;
+                    if (nfit == 0) {
+                        nent = 1;
+                        M = kCapA;
+                        jpos += kCapA;
+                    } else {
+                        nent = nfit;
+                        M = __shfl_sync(kFull, incl, nfit - 1);
+                        ce += nfit;
+                        jpos = 0;
+                    }
+                    __syncwarp();
+                    if (lane < nent) {
+                        sm.reg_beg[lane] = incl - rem;
+                        sm.reg_jb[lane] = jb;
+                    }
+                    if (lane == 0) sm.reg_beg[nent] = M;
+                    __syncwarp();
+                    for (int idx = lane; idx < M; idx += 32) {
+                        int r = 0;
+                        for (int step = 16; step > 0; step >>= 1)
+                            if (r + step < nent && sm.reg_beg[r + step] <= idx) r += step;
+                        const int ke = rce + r;
+                        const int jl = sm.reg_jb[r] + idx - sm.reg_beg[r];
+                        const int slot = sm.ent_slot[ke] + jl;
+                        const float4 es = sm.ent_sh[ke];
+                        const int role = __float_as_int(es.w) & 3;
+                        float4 q = v.pos[slot];
+                        float4 s4 = make_float4(0.f, 0.f, 0.f, __int_as_float(role | (ke << 2) | (jl << 8)));
+                        if (role == kRoleSecond) {
+                            q.x -= es.x;
+                            q.y -= es.y;
+                            q.z -= es.z;
+                        } else if (role == kRoleFirst) {
+                            s4.x = es.x;
+                            s4.y = es.y;
+                            s4.z = es.z;
+                        }
+                        sm.nb_x[idx] = q;
+                        sm.nb_s[idx] = s4;
+                        sm.nb_v[idx] = v.vel[slot];
+                        sm.nb_w[idx] = a.w[slot];
+                    }
+                    __syncwarp();
+                    int qhead = 0, qtail = 0;
+                    auto drain = [&](int nb) {
+                        float3 gx = make_float3(0.f, 0.f, 0.f), gv = make_float3(0.f, 0.f, 0.f);
+                        int il = -1;
+                        if (lane < nb) {
+                            const int cd = sm.queue[(qhead + lane) & (kQueueA - 1)];
+                            il = cd >> 8;
+                            const int jj = cd & 0xff;
+                            const float4 xi = sm.own_x[il], b = sm.nb_x[jj], s = sm.nb_s[jj];
+                            const float3 d = make_float3((xi.x - s.x) - b.x, (xi.y - s.y) - b.y, (xi.z - s.z) - b.z);
+                            const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+                            const float4 vi = sm.own_v[il], vj = sm.nb_v[jj];
+                            const float4 wi = sm.own_w[il], wj = sm.nb_w[jj];
+                            const float3 u = make_float3(wi.x - wj.x, wi.y - wj.y, wi.z - wj.z);
+                            const float3 vij = make_float3(vi.x - vj.x, vi.y - vj.y, vi.z - vj.z);
+                            const int ti = __float_as_int(xi.w), tj = __float_as_int(b.w);
+                            const unsigned ida = __float_as_uint(vi.w), idb = __float_as_uint(vj.w);
+                            const bool count = ida < idb;
+                            const float radi = v.types[ti].radius, radj = v.types[tj].radius;
+                            const int p1 = v.pot_idx[pot_base + ti * ntypes + tj];
+                            term_vjp(v, a, p1, radi, radj, d, r2, vij, ida, idb, rng_mode, u, count, gx, gv, gl);
+                            if (v.pot_idx2) {
+                                const int p2 = v.pot_idx2[pot_base + ti * ntypes + tj];
+                                if (p2 >= 0)
+                                    term_vjp(v, a, p2, radi, radj, d, r2, vij, ida, idb, rng_mode, u, count, gx, gv,
+                                             gl);
+                            }
+                        }
+                        const int il_prev = __shfl_up_sync(kFull, il, 1);
+                        const unsigned heads = __ballot_sync(kFull, lane == 0 || il != il_prev);
+                        const int seg0 = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+                        for (int off = 1; off < 32; off <<= 1) {
+                            const float o0 = __shfl_up_sync(kFull, gx.x, off), o1 = __shfl_up_sync(kFull, gx.y, off);
+                            const float o2 = __shfl_up_sync(kFull, gx.z, off), o3 = __shfl_up_sync(kFull, gv.x, off);
+                            const float o4 = __shfl_up_sync(kFull, gv.y, off), o5 = __shfl_up_sync(kFull, gv.z, off);
+                            if (lane - off >= seg0) {
+                                gx.x = o0 + gx.x;
+                                gx.y = o1 + gx.y;
+                                gx.z = o2 + gx.z;
+                                gv.x = o3 + gv.x;
+                                gv.y = o4 + gv.y;
+                                gv.z = o5 + gv.z;
+                            }
+                        }
+                        const bool seg_end = lane == 31 || ((heads >> (lane + 1)) & 1u);
+                        if (il >= 0 && seg_end) {
+                            float4 t = sm.own_gx[il];
+                            sm.own_gx[il] = make_float4(t.x + gx.x, t.y + gx.y, t.z + gx.z, 0.f);
+                            t = sm.own_gv[il];
+                            sm.own_gv[il] = make_float4(t.x + gv.x, t.y + gv.y, t.z + gv.z, 0.f);
+                        }
+                    };
+                    for (int il = 0; il < ni; ++il) {
+                        const float4 xi = sm.own_x[il];
+                        const int i = i0 + il;
+                        const unsigned long long mk = sm.own_mask[il];
+#pragma unroll
+                        for (int u = 0; u < kChunksA; ++u) {
+                            const int jj = u * 32 + lane;
+                            bool hit = false;
+                            if (jj < M) {
+                                const float4 b = sm.nb_x[jj], s = sm.nb_s[jj];
+                                const int meta = __float_as_int(s.w);
+                                const float dx = (xi.x - s.x) - b.x, dy = (xi.y - s.y) - b.y, dz = (xi.z - s.z) - b.z;
+                                const float r2 = dx * dx + dy * dy + dz * dz;
+                                const bool self = (meta & 3) == kRoleSelf;
+                                hit = r2 <= (self ? cut2_self : cut2_pair) && ((mk >> __float_as_int(b.w)) & 1ull) &&
+                                      !(self && (meta >> 8) == i);
+                            }
+                            const unsigned hb = __ballot_sync(kFull, hit);
+                            if (hit) sm.queue[(qtail + __popc(hb & lt_mask)) & (kQueueA - 1)] = (unsigned short)((il << 8) | jj);
+                            qtail += __popc(hb);
+                        }
+                        while (qtail - qhead >= 32) {
+                            __syncwarp();
+                            drain(32);
+                            qhead += 32;
+                            __syncwarp();
+                        }
+                    }
+                    if (qtail > qhead) {
+                        __syncwarp();
+                        drain(qtail - qhead);
+                    }
+                    __syncwarp();
+                }
+            }
+            __syncwarp();
+            if (lane < ni) {
+                const int sl = start + i0 + lane;
+                const float4 gx = sm.own_gx[lane], gv = sm.own_gv[lane];
+                const float4 bx = a.gx[sl], bv = a.gv[sl];
+                a.gx[sl] = make_float4(bx.x + gx.x, bx.y + gx.y, bx.z + gx.z, 0.f);
+                a.gv[sl] = make_float4(bv.x + gv.x, bv.y + gv.y, bv.z + gv.z, 0.f);
+            }
+        }
+    }
+    // this warp's parameter sums, lanes in order
+    __syncwarp();
+    if (lane < kMaxGradSlots && lane < a.nslots) {
+        double* base = reinterpret_cast<double *>(reinterpret_cast<AdjSmem *>(adj_smem) + kWarpsA) +
+                       (size_t)(w * 32) * kMaxGradSlots;
+        double t = 0.0;
+        for (int l = 0; l < 32; ++l) t += base[(size_t)l * kMaxGradSlots + lane];
+        a.partials[(size_t)(blockIdx.x * kWarpsA + w) * kMaxGradSlots + lane] = t;
+    }
+}
+
+/* Per slot: the adjoints back into id order. */
+__global__ void adj_finish_kernel(EngineView v, AdjointView a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= v.nparts) return;
+    const int id = __float_as_int(v.vel[s].w);
+    a.lam_x[id] = a.gx[s];
+    a.lam_v[id] = a.gv[s];
+}
+
+/* grad[k] += sum of the warps' partials, in warp order. */
+__global__ void adj_grad_kernel(AdjointView a, int nwarps, double *grad) {
+    const int k = threadIdx.x;
+    if (k >= a.nslots) return;
+    double t = 0.0;
+    for (int q = 0; q < nwarps; ++q) t += a.partials[(size_t)q * kMaxGradSlots + k];
+    grad[k] += t;
+}
+
+/* Absolute positions (x, y, z, type bits) and velocities (v, id bits) by id;
+ * the position is the cell origin (double, space.cpp:431-451) plus the
+ * cell-relative coordinate. */
+__global__ void positions_kernel(EngineView v, float4 *x_out, float4 *v_out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= v.nparts) return;
+    const float4 q = v.pos[s], u = v.vel[s];
+    const int id = __float_as_int(u.w);
+    const int c = v.cell_of[s];
+    const DevSpace &S = v.spaces[v.cell_rep[c]];
+    const int l = c - S.cell_offset;
+    const int loc[3] = {l / (S.cdim[1] * S.cdim[2]), (l / S.cdim[2]) % S.cdim[1], l % S.cdim[2]};
+    const float xr[3] = {q.x, q.y, q.z};
+    float xa[3];
+    for (int k = 0; k < 3; ++k) xa[k] = (float)(S.origin[k] + loc[k] * S.hd[k] + (double)xr[k]);
+    if (x_out) x_out[id] = make_float4(xa[0], xa[1], xa[2], q.w);
+    if (v_out) v_out[id] = u;
+}
+
+/* Gaussian kernel of width sigma at distance t from a bin centre, lowered by
+ * its value at 4 sigma so that the cut there is continuous (the loss then has
+ * no jumps as pair distances cross a cut). */
+__device__ __forceinline__ double rdf_kernel_value(double t, double sigma) {
+    return (exp(-0.5 * (t / sigma) * (t / sigma)) - 3.3546262790251185e-04) * (0.3989422804014327 / sigma);
+}
+
+constexpr int kRdfTile = 256;
+constexpr int kRdfMaxBins = 256;
+constexpr double kRdfFixed = 4294967296.0;  // histogram fixed point: 2^32 per unit
+
+/* hist[b] += sum over (i of type ta, j of type tb, i != j) of K(r_ij - c_b),
+ * c_b = (b + 1/2) dr, minimum image in the periodic box, terms with
+ * |r - c_b| > 4 sigma left out. Fixed-point sums make the result independent
+ * of the order of the additions. One thread per particle i. */
+__global__ void rdf_hist_kernel(const float4 *__restrict__ x, int n, double3 box, int ta, int tb, int nbins,
+                                double dr, double sigma, unsigned long long *hist) {
+    __shared__ float4 tile[kRdfTile];
+    __shared__ unsigned long long h[kRdfMaxBins];
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x) h[b] = 0ull;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
+    bool active = false;
+    if (i < n) {
+        xi = x[i];
+        active = __float_as_int(xi.w) == ta;
+    }
+    const double rmax = nbins * dr + 4 * sigma;
+    __syncthreads();
+    for (int t0 = 0; t0 < n; t0 += kRdfTile) {
+        const int j = t0 + threadIdx.x;
+        tile[threadIdx.x] = j < n ? x[j] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+        __syncthreads();
+        if (active) {
+            const int m = min(kRdfTile, n - t0);
+            for (int k = 0; k < m; ++k) {
+                const float4 xj = tile[k];
+                if (__float_as_int(xj.w) != tb || t0 + k == i) continue;
+                double d[3] = {(double)xi.x - xj.x, (double)xi.y - xj.y, (double)xi.z - xj.z};
+                const double L[3] = {box.x, box.y, box.z};
+                for (int q = 0; q < 3; ++q) d[q] -= L[q] * rint(d[q] / L[q]);
+                const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+                if (r >= rmax) continue;
+                const int b0 = max(0, (int)floor((r - 4 * sigma) / dr)), b1 = min(nbins - 1, (int)floor((r + 4 * sigma) / dr));
+                for (int b = b0; b <= b1; ++b) {
+                    const double t = r - (b + 0.5) * dr;
+                    if (fabs(t) > 4 * sigma) continue;
+                    atomicAdd(&h[b], (unsigned long long)llrint(rdf_kernel_value(t, sigma) * kRdfFixed));
+                }
+            }
+        }
+        __syncthreads();
+    }
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x)
+        if (h[b]) atomicAdd(&hist[b], h[b]);
+}
+
+/* grad[i] = sum over partners j of sum_b coef[b] dK(r_ij - c_b)/dr (x_i - x_j)/r
+ * for i of type ta (partners tb) and of type tb (partners ta): d loss / d x_i
+ * for loss = sum_b G_b(hist) with coef[b] = dG/dhist_b. One thread per particle. */
+__global__ void rdf_grad_kernel(const float4 *__restrict__ x, int n, double3 box, int ta, int tb, int nbins,
+                                double dr, double sigma, const double *__restrict__ coef, float4 *grad) {
+    __shared__ float4 tile[kRdfTile];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
+    int partner = -2;
+    if (i < n) {
+        xi = x[i];
+        const int ti = __float_as_int(xi.w);
+        partner = ti == ta ? tb : (ti == tb ? ta : -2);
+    }
+    const double rmax = nbins * dr + 4 * sigma;
+    double g[3] = {0.0, 0.0, 0.0};
+    for (int t0 = 0; t0 < n; t0 += kRdfTile) {
+        const int j = t0 + threadIdx.x;
+        tile[threadIdx.x] = j < n ? x[j] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+        __syncthreads();
+        if (partner != -2) {
+            const int m = min(kRdfTile, n - t0);
+            for (int k = 0; k < m; ++k) {
+                const float4 xj = tile[k];
+                if (__float_as_int(xj.w) != partner || t0 + k == i) continue;
+                double d[3] = {(double)xi.x - xj.x, (double)xi.y - xj.y, (double)xi.z - xj.z};
+                const double L[3] = {box.x, box.y, box.z};
+                for (int q = 0; q < 3; ++q) d[q] -= L[q] * rint(d[q] / L[q]);
+                const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+                if (r >= rmax || r <= 0.0) continue;
+                const int b0 = max(0, (int)floor((r - 4 * sigma) / dr)), b1 = min(nbins - 1, (int)floor((r + 4 * sigma) / dr));
+                double s = 0.0;
+                for (int b = b0; b <= b1; ++b) {
+                    const double t = r - (b + 0.5) * dr;
+                    if (fabs(t) > 4 * sigma) continue;
+                    s += coef[b] * exp(-0.5 * (t / sigma) * (t / sigma)) * (0.3989422804014327 / sigma) *
+                         (-t / (sigma * sigma));
+                }
+                // ta == tb counts each unordered pair twice in hist, as i and as j
+                const double f = s / r * (ta == tb ? 2.0 : 1.0);
+                for (int q = 0; q < 3; ++q) g[q] += f * d[q];
+            }
+        }
+        __syncthreads();
+    }
+    if (i < n) grad[i] = make_float4((float)g[0], (float)g[1], (float)g[2], 0.f);
+}
+
+}  // namespace
+
+void launch_positions(const EngineView &v, float4 *x_out, float4 *v_out, cudaStream_t st) {
+    positions_kernel<<<(v.nparts + 255) / 256, 256, 0, st>>>(v, x_out, v_out);
+}
+
+int launch_rdf(const float4 *x, int n, const double *box, int ta, int tb, int nbins, double dr, double sigma,
+               unsigned long long *hist, const double *coef, float4 *grad, cudaStream_t st) {
+    if (nbins < 1 || nbins > kRdfMaxBins) return -1;
+    const double3 b = make_double3(box[0], box[1], box[2]);
+    const int grid = (n + kRdfTile - 1) / kRdfTile;
+    if (hist) rdf_hist_kernel<<<grid, kRdfTile, 0, st>>>(x, n, b, ta, tb, nbins, dr, sigma, hist);
+    if (grad) rdf_grad_kernel<<<grid, kRdfTile, 0, st>>>(x, n, b, ta, tb, nbins, dr, sigma, coef, grad);
+    return 0;
+}
+
+int adjoint_grid(int num_sms) { return num_sms * 4; }
+int adjoint_partials(int num_sms) { return adjoint_grid(num_sms) * kWarpsA; }
+
+void configure_adjoint_kernels() {
+    cudaFuncSetAttribute(vjp_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_smem_bytes());
+    cudaFuncSetAttribute(vjp_pair_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+}
+
+void launch_vjp_step(const EngineView &v, const AdjointView &a, int num_sms, double *grad, cudaStream_t st) {
+    const int tb = 256;
+    adj_prep_kernel<<<(v.nparts + tb - 1) / tb, tb, 0, st>>>(v, a);
+    const int grid = adjoint_grid(num_sms);
+    vjp_pair_kernel<<<grid, kWarpsA * 32, adj_smem_bytes(), st>>>(v, a);
+    adj_finish_kernel<<<(v.nparts + tb - 1) / tb, tb, 0, st>>>(v, a);
+    adj_grad_kernel<<<1, 64, 0, st>>>(a, grid * kWarpsA, grad);
+}
+
+}  // namespace mxg

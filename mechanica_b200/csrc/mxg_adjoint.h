@@ -1,0 +1,37 @@
+/* Adjoint (vector-Jacobian product) of one engine step (mxg_adjoint.cu). */
+#pragma once
+#include "mxg_device.cuh"
+
+namespace mxg {
+
+constexpr int kMaxGradSlots = 16;  // parameter-gradient slots per engine
+constexpr int kMaxPotGrads = 4;    // differentiated parameters per potential
+
+enum : int { kGradTable = 0, kGradShift = 1, kGradDpdAlpha = 2, kGradDpdGamma = 3, kGradDpdSigma = 4 };
+
+struct DevPotGrad {      // the differentiated parameters of one potential
+    int n;
+    int mode[kMaxPotGrads];      // kGrad*
+    int slot[kMaxPotGrads];      // gradient slot the parameter adds to
+    int coef_off[kMaxPotGrads];  // kGradTable: offset of dV/dtheta's table in the derivative pool
+};
+
+struct AdjointView {
+    float4 *lam_x, *lam_v;       // [id] adjoints of positions and velocities (in: after the step; out: before)
+    float4 *w, *gx, *gv;         // [slot] scratch: force adjoint and the partial sums
+    const DevPotGrad *pot_grad;  // per potential
+    const float *dcoef;          // derivative tables' coefficient pool
+    double *partials;            // [warp][kMaxGradSlots] FP64 parameter sums
+    int nslots;
+};
+
+void launch_positions(const EngineView &v, float4 *x_out, float4 *v_out, cudaStream_t st);
+/* Smoothed pair histogram of types (ta, tb) and/or its gradient (see mxg_rdf). */
+int launch_rdf(const float4 *x, int n, const double *box, int ta, int tb, int nbins, double dr, double sigma,
+               unsigned long long *hist, const double *coef, float4 *grad, cudaStream_t st);
+int adjoint_partials(int num_sms);
+void configure_adjoint_kernels();
+/* Enqueues the VJP of one step at the engine's current state, whose forces v.force must hold. */
+void launch_vjp_step(const EngineView &v, const AdjointView &a, int num_sms, double *grad, cudaStream_t st);
+
+}  // namespace mxg

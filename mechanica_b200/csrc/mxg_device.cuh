@@ -73,6 +73,7 @@ struct DevType {
 };
 
 struct DevSpace {        // one per replica
+    double origin[3];    // the box's lower corner
     double hd[3];        // cell size (double, as space.h keeps it)
     float h[3], h2[3];   // float(h), float(2h)
     float maxv[3], maxv2[3], maxx[3], maxx2[3];
@@ -120,6 +121,7 @@ struct EngineView {      // everything a kernel needs, passed by value
     const DevPot *pots;
     const float *coef;
     const int *pot_idx;      // per replica: [ntypes*ntypes] potential index or -1
+    const int *pot_idx2;     // per replica: second (summed) potential index or -1; null if none
     const DevType *types;
     const DevSpace *spaces;
     int ntypes;
@@ -168,6 +170,27 @@ __device__ __forceinline__ int sort_key(float x, float y, float z, const float *
 
 /* uniform in (0,1) from 32 random bits */
 __device__ __forceinline__ float u01(unsigned x) { return ((float)(x >> 8) + 0.5f) * (1.0f / 16777216.0f); }
+
+/* Three normal deviates from one Philox draw (Box-Muller on two pairs). */
+__device__ __forceinline__ void philox_normal3(unsigned long long step, unsigned a, unsigned b, float &g0,
+                                               float &g1, float &g2) {
+    const uint4 r = philox4x32(make_uint4(a, b, (unsigned)step, (unsigned)(step >> 32)), make_uint2(0x4d584731u, 0x5f524e44u));
+    const float u0 = u01(r.x), u1 = u01(r.y), u2 = u01(r.z), u3 = u01(r.w);
+    const float m0 = sqrtf(-2.0f * logf(u0)), m1 = sqrtf(-2.0f * logf(u2));
+    float s0, c0, s1, c1;
+    sincospif(2.0f * u1, &s0, &c0);
+    sincospif(2.0f * u3, &s1, &c1);
+    g0 = m0 * c0;
+    g1 = m0 * s0;
+    g2 = m1 * c1;
+}
+
+/* Zero-mean, unit-variance DPD random number for the unordered pair (a, b). */
+__device__ __forceinline__ float philox_pair_xi(unsigned long long step, unsigned lo, unsigned hi) {
+    const uint4 r = philox4x32(make_uint4(lo, hi, (unsigned)step, (unsigned)(step >> 32)), make_uint2(0x44504431u, 0x58495f31u));
+    return 1.7320508075688772f * (2.0f * u01(r.x) - 1.0f);
+}
+
 
 /* Table evaluation with potential_eval_ex semantics (potential_eval.hpp:106-161):
  * returns false when out of range. ri, rj are the particle radii. */

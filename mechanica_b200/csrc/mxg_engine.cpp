@@ -19,6 +19,7 @@
  * graphs, one per buffer parity.
  */
 #include "../../include/mxg.h"
+#include "mxg_adjoint.h"
 #include "mxg_kernels.h"
 #include "potential_table.h"
 
@@ -130,6 +131,7 @@ struct Space {
     std::vector<double> cell_origin;  // 3 per cell
     std::vector<Task> tasks;          // local cell indices
     std::vector<int> pot_idx;         // max_type^2 potential index per type pair (-1 none)
+    std::vector<int> pot2_idx;        // max_type^2 second (summed) potential per type pair (-1 none)
 
     int cellid(int i, int j, int k) const { return (i * cdim[1] + j) * cdim[2] + k; }
 
@@ -357,6 +359,8 @@ struct mxg_engine {
     DevPot *d_pots = nullptr;
     float *d_coef = nullptr;
     int *d_pot_idx = nullptr;
+    int *d_pot_idx2 = nullptr;   // second summed potential per type pair, or -1
+    bool has_second = false;
     DevType *d_types = nullptr;
     DevSpace *d_spaces = nullptr;
     SortAxes *d_axes = nullptr;
@@ -364,6 +368,18 @@ struct mxg_engine {
     double *d_epot_cell = nullptr, *d_ebond_slot = nullptr;
     DevBond *d_bonds = nullptr;
     unsigned *d_bond_flags = nullptr;
+    // ---- adjoint ----
+    struct GradReg {
+        int pot, param, slot;
+    };
+    std::vector<GradReg> grad_regs;        // differentiated (potential, parameter) -> gradient slot
+    int grad_slots = 0;
+    bool adjoint_stale = true;             // derivative tables need a rebuild
+    DevPotGrad *d_pot_grad = nullptr;
+    float *d_dcoef = nullptr;
+    size_t dcoef_cap = 0;
+    float4 *d_adj_w = nullptr, *d_adj_gx = nullptr, *d_adj_gv = nullptr;
+    double *d_adj_partials = nullptr;
     int *d_bond_off = nullptr, *d_bond_list = nullptr;
     unsigned *d_status = nullptr;
     unsigned long long *d_step = nullptr;
@@ -381,6 +397,35 @@ struct mxg_engine {
             if (graph[k]) cudaGraphExecDestroy(graph[k]);
         for (void *p : allocations) cudaFree(p);
         if (own_stream) cudaStreamDestroy(own_stream);
+    }
+
+    /* Device form of the potentials: one DevPot each and the pooled coefficients. */
+    void pot_arrays(std::vector<DevPot> &hp, std::vector<float> &coef) {
+        hp.clear();
+        coef.clear();
+        has_dpd = false;
+        for (const auto &t : pots) {
+            DevPot d;
+            memset(&d, 0, sizeof(d));
+            d.kind = t.kind;
+            d.flags = t.flags;
+            d.n = t.n;
+            d.coef_off = (int)coef.size();
+            d.alpha0 = t.alpha[0];
+            d.alpha1 = t.alpha[1];
+            d.alpha2 = t.alpha[2];
+            d.a = t.a;
+            d.b = t.b;
+            d.r0_plusone = t.r0_plusone;
+            d.a2 = t.a * t.a;
+            d.dpd_alpha = t.dpd_alpha;
+            d.dpd_gamma = t.dpd_gamma;
+            d.dpd_sigma = t.dpd_sigma;
+            d.dpd_delta = (float)(1.f / std::sqrt(dt));  // dpd_eval.hpp:23, from the engine dt
+            if (t.kind == kKindDPD) has_dpd = true;
+            coef.insert(coef.end(), t.c.begin(), t.c.end());
+            hp.push_back(d);
+        }
     }
 
     template <typename T>
@@ -404,6 +449,7 @@ struct mxg_engine {
             S.maxx[k] = S.h[k] * max_dist_fraction;
             S.maxx2[k] = S.maxx[k] * S.maxx[k];
             S.cdim[k] = sp.cdim[k];
+            S.origin[k] = sp.origin[k];
         }
         S.dt = dtf;
         const float cf = (float)cutoff;
@@ -482,6 +528,7 @@ struct mxg_engine {
         v.pots = d_pots;
         v.coef = d_coef;
         v.pot_idx = d_pot_idx;
+        v.pot_idx2 = has_second ? d_pot_idx2 : nullptr;
         v.types = d_types;
         v.spaces = d_spaces;
         v.ntypes = ntypes;
@@ -530,6 +577,76 @@ struct mxg_engine {
 
     /* Key bounds for a state that did not come from the re-binning pass. */
     void refresh_bounds() { launch_sort_bounds(view(cur), stream); }
+
+    /* Derivative tables and per-potential parameter descriptors for the VJP. */
+    int build_adjoint() {
+        std::vector<DevPotGrad> hg(std::max<size_t>(1, pots.size()));
+        for (auto &g : hg) memset(&g, 0, sizeof(g));
+        std::vector<float> dcoef;
+        for (const GradReg &r : grad_regs) {
+            const mxg::PotentialTable &t = pots[r.pot];
+            DevPotGrad &g = hg[r.pot];
+            if (g.n >= kMaxPotGrads) return MXG_ERR_RANGE;
+            int mode = -1, off = 0;
+            if (t.kind == kKindDPD) {
+                mode = r.param == 0 ? kGradDpdAlpha : r.param == 1 ? kGradDpdGamma : r.param == 2 ? kGradDpdSigma : -1;
+            } else if (t.form == mxg::kFormMorse && r.param == 2) {
+                mode = kGradShift;  // r0 shifts the table's argument
+            } else {
+                mxg::PotentialTable d;
+                if (mxg::param_derivative_table(t, r.param, d) != 0) return MXG_ERR_ARG;
+                mode = kGradTable;
+                off = (int)dcoef.size();
+                dcoef.insert(dcoef.end(), d.c.begin(), d.c.end());
+            }
+            if (mode < 0) return MXG_ERR_ARG;
+            g.mode[g.n] = mode;
+            g.slot[g.n] = r.slot;
+            g.coef_off[g.n] = off;
+            ++g.n;
+        }
+        if (!d_pot_grad) {
+            int rc = alloc(&d_pot_grad, hg.size());
+            rc |= alloc(&d_adj_w, (size_t)nparts);
+            rc |= alloc(&d_adj_gx, (size_t)nparts);
+            rc |= alloc(&d_adj_gv, (size_t)nparts);
+            rc |= alloc(&d_adj_partials, (size_t)adjoint_partials(num_sms) * kMaxGradSlots);
+            if (rc != MXG_OK) return MXG_ERR_MALLOC;
+            configure_adjoint_kernels();
+        }
+        if (dcoef.size() + 8 > dcoef_cap) {
+            dcoef_cap = dcoef.size() + 8;
+            if (alloc(&d_dcoef, dcoef_cap) != MXG_OK) return MXG_ERR_MALLOC;
+        }
+        int rc;
+        if ((rc = upload(d_pot_grad, hg, stream)) || (rc = upload(d_dcoef, dcoef, stream))) return rc;
+        adjoint_stale = false;
+        return MXG_OK;
+    }
+
+    /* Layout of a state snapshot: byte offsets of its sections (16-byte aligned). */
+    struct SnapLayout {
+        size_t pos, vel, cell_of, slot_of_id, start, count, step, bonds, total;
+    };
+    SnapLayout snap_layout() const {
+        SnapLayout L;
+        size_t o = 0;
+        auto take = [&](size_t bytes) {
+            const size_t at = o;
+            o += (bytes + 15) & ~(size_t)15;
+            return at;
+        };
+        L.pos = take(sizeof(float4) * (size_t)nparts);
+        L.vel = take(sizeof(float4) * (size_t)nparts);
+        L.cell_of = take(sizeof(int) * (size_t)nparts);
+        L.slot_of_id = take(sizeof(int) * (size_t)nparts);
+        L.start = take(sizeof(int) * (size_t)(ncells + 1));
+        L.count = take(sizeof(int) * (size_t)ncells);
+        L.step = take(sizeof(unsigned long long));
+        L.bonds = take(sizeof(unsigned) * bonds.size());
+        L.total = o;
+        return L;
+    }
 
     int start(cudaStream_t st);
     int build_graphs();
@@ -638,36 +755,20 @@ int mxg_engine::start(cudaStream_t st) {
     // ---- potentials, types, replicas ----
     std::vector<DevPot> hp;
     std::vector<float> coef;
-    has_dpd = false;
-    for (const auto &t : pots) {
-        DevPot d;
-        memset(&d, 0, sizeof(d));
-        d.kind = t.kind;
-        d.flags = t.flags;
-        d.n = t.n;
-        d.coef_off = (int)coef.size();
-        d.alpha0 = t.alpha[0];
-        d.alpha1 = t.alpha[1];
-        d.alpha2 = t.alpha[2];
-        d.a = t.a;
-        d.b = t.b;
-        d.r0_plusone = t.r0_plusone;
-        d.a2 = t.a * t.a;
-        d.dpd_alpha = t.dpd_alpha;
-        d.dpd_gamma = t.dpd_gamma;
-        d.dpd_sigma = t.dpd_sigma;
-        d.dpd_delta = (float)(1.f / std::sqrt(dt));  // dpd_eval.hpp:23, from the engine dt
-        if (t.kind == kKindDPD) has_dpd = true;
-        coef.insert(coef.end(), t.c.begin(), t.c.end());
-        hp.push_back(d);
-    }
+    pot_arrays(hp, coef);
     const int tt = ntypes * ntypes;
-    std::vector<int> hpidx((size_t)tt * spaces.size(), -1);
+    std::vector<int> hpidx((size_t)tt * spaces.size(), -1), hpidx2((size_t)tt * spaces.size(), -1);
     std::vector<DevSpace> hs;
+    has_second = false;
     for (int r = 0; r < (int)spaces.size(); ++r) {
         for (int a = 0; a < (int)types.size(); ++a)
-            for (int b = 0; b < (int)types.size(); ++b)
-                hpidx[(size_t)r * tt + a * ntypes + b] = spaces[r].pot_idx[a * max_type + b];
+            for (int b = 0; b < (int)types.size(); ++b) {
+                int p1 = spaces[r].pot_idx[a * max_type + b], p2 = spaces[r].pot2_idx[a * max_type + b];
+                if (p1 < 0) std::swap(p1, p2);  // a lone second term acts as the pair's potential
+                hpidx[(size_t)r * tt + a * ntypes + b] = p1;
+                hpidx2[(size_t)r * tt + a * ntypes + b] = p2;
+                if (p2 >= 0) has_second = true;
+            }
         hs.push_back(space_desc(r, r * tt));
     }
     std::vector<DevType> ht(ntypes);
@@ -744,6 +845,7 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_pots, hp.size());
     rc |= alloc(&d_coef, coef.size() + 8);
     rc |= alloc(&d_pot_idx, hpidx.size());
+    rc |= alloc(&d_pot_idx2, hpidx2.size());
     rc |= alloc(&d_types, ht.size());
     rc |= alloc(&d_spaces, hs.size());
     rc |= alloc(&d_axes, 1);
@@ -776,6 +878,7 @@ int mxg_engine::start(cudaStream_t st) {
         (rc = upload(d_sec_count, hsec, stream)) || (rc = upload(d_cell_planes, hplanes, stream)) ||
         (rc = upload(d_items, hitems, stream)) || (rc = upload(d_pots, hp, stream)) ||
         (rc = upload(d_coef, coef, stream)) || (rc = upload(d_pot_idx, hpidx, stream)) ||
+        (rc = upload(d_pot_idx2, hpidx2, stream)) ||
         (rc = upload(d_types, ht, stream)) || (rc = upload(d_spaces, hs, stream)) || (rc = upload(d_axes, haxes, stream)) ||
         (rc = upload(d_bonds, hb, stream)) || (rc = upload(d_bond_flags, hbf, stream)) ||
         (rc = upload(d_bond_off, boff, stream)) || (rc = upload(d_bond_list, blist, stream)))
@@ -951,6 +1054,7 @@ int mxg_engine_add_replica(mxg_engine *e, const double *origin, const double *di
     if ((rc = sp.build(e->cutoff)) != MXG_OK) return rc;
     sp.cell_offset = e->ncells;
     sp.pot_idx.assign((size_t)e->max_type * e->max_type, -1);
+    sp.pot2_idx.assign((size_t)e->max_type * e->max_type, -1);
     e->ncells += sp.ncells;
     e->spaces.push_back(std::move(sp));
     return (int)e->spaces.size() - 1;
@@ -1009,6 +1113,90 @@ int mxg_engine_addpot_replica(mxg_engine *e, int rep, const mxg_potential *p, in
     std::vector<int> &m = e->spaces[rep].pot_idx;
     m[i * e->max_type + j] = idx;  // engine_addpot overwrites: one potential per pair
     m[j * e->max_type + i] = idx;
+    return MXG_OK;
+}
+
+namespace {
+/* New construction parameters for a potential: a frozen-node re-fit for tables;
+ * for DPD the three coefficients (the cutoff and the shift flag stay). */
+int set_params(mxg::PotentialTable &t, const double *params, int nparams) {
+    if (nparams != (int)t.params.size()) return MXG_ERR_ARG;
+    if (t.kind == kKindDPD) {
+        if (params[3] != t.params[3] || params[4] != t.params[4]) return MXG_ERR_ARG;
+        t.dpd_alpha = (float)params[0];
+        t.dpd_gamma = (float)params[1];
+        t.dpd_sigma = (float)params[2];
+        t.params.assign(params, params + nparams);
+        return MXG_OK;
+    }
+    std::vector<double> q(params, params + nparams);
+    return mxg::refit_frozen(t, q) == 0 ? MXG_OK : MXG_ERR_ARG;
+}
+}  // namespace
+
+int mxg_potential_coeffs64(const mxg_potential *p, double *out, int cap) {
+    if (!p || !out) return MXG_ERR_NULL;
+    const int n = (int)p->t.c64.size();
+    for (int k = 0; k < n && k < cap; ++k) out[k] = p->t.c64[k];
+    return n;
+}
+
+int mxg_potential_params(const mxg_potential *p, double *out, int cap) {
+    if (!p) return MXG_ERR_NULL;
+    const int n = (int)p->t.params.size();
+    for (int k = 0; k < n && k < cap && out; ++k) out[k] = p->t.params[k];
+    return n;
+}
+
+int mxg_potential_refit(mxg_potential *p, const double *params, int nparams) {
+    if (!p || !params) return MXG_ERR_NULL;
+    return set_params(p->t, params, nparams);
+}
+
+int mxg_potential_param_table(const mxg_potential *p, int k, mxg_potential **out) {
+    if (!p || !out) return MXG_ERR_NULL;
+    mxg_potential *q = new mxg_potential;
+    if (mxg::param_derivative_table(p->t, k, q->t) != 0) {
+        delete q;
+        return MXG_ERR_ARG;
+    }
+    *out = q;
+    return MXG_OK;
+}
+
+int mxg_engine_addpot_second(mxg_engine *e, int rep, const mxg_potential *p, int i, int j) {
+    if (!e || !p) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    const int nt = (int)e->types.size();
+    if (i < 0 || i >= nt || j < 0 || j >= nt || rep < 0 || rep >= (int)e->spaces.size()) return MXG_ERR_RANGE;
+    e->pots.push_back(p->t);
+    const int idx = (int)e->pots.size() - 1;
+    std::vector<int> &m = e->spaces[rep].pot2_idx;
+    m[i * e->max_type + j] = idx;
+    m[j * e->max_type + i] = idx;
+    return MXG_OK;
+}
+
+int mxg_engine_pot_index(mxg_engine *e, int rep, int i, int j, int which, int *idx) {
+    if (!e || !idx) return MXG_ERR_NULL;
+    const int nt = (int)e->types.size();
+    if (i < 0 || i >= nt || j < 0 || j >= nt || rep < 0 || rep >= (int)e->spaces.size() || which < 0 || which > 1)
+        return MXG_ERR_RANGE;
+    const std::vector<int> &m = which == 0 ? e->spaces[rep].pot_idx : e->spaces[rep].pot2_idx;
+    *idx = m[i * e->max_type + j];
+    return MXG_OK;
+}
+
+int mxg_engine_set_pot_params(mxg_engine *e, int idx, const double *params, int nparams) {
+    if (!e || !params) return MXG_ERR_NULL;
+    if (idx < 0 || idx >= (int)e->pots.size()) return MXG_ERR_RANGE;
+    int rc = set_params(e->pots[idx], params, nparams);
+    e->adjoint_stale = true;  // dV/dtheta tables depend on the parameters
+    if (rc != MXG_OK || !e->started) return rc;
+    std::vector<DevPot> hp;
+    std::vector<float> coef;
+    e->pot_arrays(hp, coef);  // same sizes: a frozen-node refit keeps every table's length
+    if ((rc = upload(e->d_pots, hp, e->stream)) || (rc = upload(e->d_coef, coef, e->stream))) return rc;
     return MXG_OK;
 }
 
@@ -1263,6 +1451,117 @@ int mxg_engine_energy_async(mxg_engine *e, double *host_out2) {
                   e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
                   e->stream);
     CUDA_TRY(cudaMemcpyAsync(host_out2, e->d_energy, 2 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    return MXG_OK;
+}
+
+int mxg_engine_snapshot_bytes(const mxg_engine *e, size_t *bytes) {
+    if (!e || !bytes) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    *bytes = e->snap_layout().total;
+    return MXG_OK;
+}
+
+int mxg_engine_snapshot(mxg_engine *e, void *dev_buf, int save) {
+    if (!e || !dev_buf) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    if (((uintptr_t)dev_buf) & 15) return MXG_ERR_ARG;
+    const auto L = e->snap_layout();
+    char *b = static_cast<char *>(dev_buf);
+    const int c = e->cur;
+    struct Sec {
+        void *dev;
+        size_t off, bytes;
+    } secs[] = {
+        {e->d_pos[c], L.pos, sizeof(float4) * (size_t)e->nparts},
+        {e->d_vel[c], L.vel, sizeof(float4) * (size_t)e->nparts},
+        {e->d_cell_of[c], L.cell_of, sizeof(int) * (size_t)e->nparts},
+        {e->d_slot_of_id, L.slot_of_id, sizeof(int) * (size_t)e->nparts},
+        {e->d_cell_start[c], L.start, sizeof(int) * (size_t)(e->ncells + 1)},
+        {e->d_cell_count[c], L.count, sizeof(int) * (size_t)e->ncells},
+        {e->d_step, L.step, sizeof(unsigned long long)},
+        {e->d_bond_flags, L.bonds, sizeof(unsigned) * e->bonds.size()},
+    };
+    for (const Sec &q : secs) {
+        if (q.bytes == 0) continue;
+        if (save)
+            CUDA_TRY(cudaMemcpyAsync(b + q.off, q.dev, q.bytes, cudaMemcpyDeviceToDevice, e->stream));
+        else
+            CUDA_TRY(cudaMemcpyAsync(q.dev, b + q.off, q.bytes, cudaMemcpyDeviceToDevice, e->stream));
+    }
+    if (!save) e->refresh_bounds();
+    return MXG_OK;
+}
+
+int mxg_engine_adjoint_params(mxg_engine *e, int n, const int *pot, const int *param, const int *slot) {
+    if (!e || (n > 0 && (!pot || !param || !slot))) return MXG_ERR_NULL;
+    std::vector<mxg_engine::GradReg> regs;
+    int nslots = 0;
+    for (int k = 0; k < n; ++k) {
+        if (pot[k] < 0 || pot[k] >= (int)e->pots.size() || slot[k] < 0 || slot[k] >= kMaxGradSlots)
+            return MXG_ERR_RANGE;
+        regs.push_back({pot[k], param[k], slot[k]});
+        nslots = std::max(nslots, slot[k] + 1);
+    }
+    e->grad_regs = regs;
+    e->grad_slots = nslots;
+    e->adjoint_stale = true;
+    if (e->started) return e->build_adjoint();
+    return MXG_OK;
+}
+
+int mxg_engine_vjp_step(mxg_engine *e, void *lam_x, void *lam_v, double *grad) {
+    if (!e || !lam_x || !lam_v || !grad) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    if (!e->bonds.empty()) return MXG_ERR_ARG;  // bonded forces are not differentiated
+    if (e->nparts == 0) return MXG_OK;
+    if (e->adjoint_stale) {
+        const int rc = e->build_adjoint();
+        if (rc != MXG_OK) return rc;
+    }
+    const EngineView v = e->view(e->cur);
+    launch_force(v, e->has_dpd, e->force_grid, true, e->stream);  // forces of the step's state
+    AdjointView a;
+    a.lam_x = static_cast<float4 *>(lam_x);
+    a.lam_v = static_cast<float4 *>(lam_v);
+    a.w = e->d_adj_w;
+    a.gx = e->d_adj_gx;
+    a.gv = e->d_adj_gv;
+    a.pot_grad = e->d_pot_grad;
+    a.dcoef = e->d_dcoef;
+    a.partials = e->d_adj_partials;
+    a.nslots = e->grad_slots;
+    launch_vjp_step(v, a, e->num_sms, grad, e->stream);
+    CUDA_TRY(cudaGetLastError());
+    return MXG_OK;
+}
+
+int mxg_engine_positions(mxg_engine *e, void *x4, void *v4) {
+    if (!e) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    if (e->nparts == 0) return MXG_OK;
+    launch_positions(e->view(e->cur), static_cast<float4 *>(x4), static_cast<float4 *>(v4), e->stream);
+    CUDA_TRY(cudaGetLastError());
+    return MXG_OK;
+}
+
+int mxg_engine_set_step_counter(mxg_engine *e, unsigned long long step) {
+    if (!e) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    CUDA_TRY(cudaMemcpyAsync(e->d_step, &step, sizeof(step), cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return MXG_OK;
+}
+
+int mxg_rdf(const void *x4, int n, const double *box, int type_a, int type_b, int nbins, double dr, double sigma,
+            void *hist, const double *coef, void *grad4, void *stream) {
+    if (!x4 || !box || (!hist && !grad4) || (grad4 && !coef)) return MXG_ERR_NULL;
+    if (n < 0 || !(dr > 0) || !(sigma > 0)) return MXG_ERR_ARG;
+    if (n == 0) return MXG_OK;
+    if (launch_rdf(static_cast<const float4 *>(x4), n, box, type_a, type_b, nbins, dr, sigma,
+                   static_cast<unsigned long long *>(hist), coef, static_cast<float4 *>(grad4),
+                   static_cast<cudaStream_t>(stream)) != 0)
+        return MXG_ERR_RANGE;
+    CUDA_TRY(cudaGetLastError());
     return MXG_OK;
 }
 

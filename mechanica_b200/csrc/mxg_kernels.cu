@@ -25,26 +25,6 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-/* Three normal deviates from one Philox draw (Box-Muller on two pairs). */
-__device__ __forceinline__ void philox_normal3(unsigned long long step, unsigned a, unsigned b, float &g0,
-                                               float &g1, float &g2) {
-    const uint4 r = philox4x32(make_uint4(a, b, (unsigned)step, (unsigned)(step >> 32)), make_uint2(0x4d584731u, 0x5f524e44u));
-    const float u0 = u01(r.x), u1 = u01(r.y), u2 = u01(r.z), u3 = u01(r.w);
-    const float m0 = sqrtf(-2.0f * logf(u0)), m1 = sqrtf(-2.0f * logf(u2));
-    float s0, c0, s1, c1;
-    sincospif(2.0f * u1, &s0, &c0);
-    sincospif(2.0f * u3, &s1, &c1);
-    g0 = m0 * c0;
-    g1 = m0 * s0;
-    g2 = m1 * c1;
-}
-
-/* Zero-mean, unit-variance DPD random number for the unordered pair (a, b). */
-__device__ __forceinline__ float philox_pair_xi(unsigned long long step, unsigned lo, unsigned hi) {
-    const uint4 r = philox4x32(make_uint4(lo, hi, (unsigned)step, (unsigned)(step >> 32)), make_uint2(0x44504431u, 0x58495f31u));
-    return 1.7320508075688772f * (2.0f * u01(r.x) - 1.0f);
-}
-
 }  // namespace
 
 /* ------------------------------------------------------------------------ */
@@ -243,6 +223,7 @@ __device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD> 
             dz = -dz;
         }
         float r2 = dot3_rn(dx, dy, dz);
+        const float dxo = dx, dyo = dy, dzo = dz;  // before the r < a substitution
         const int ti = __float_as_int(xi.w), tj = __float_as_int(b.w);
         const DevPot &p = v.pots[v.pot_idx[pot_base + ti * v.ntypes + tj]];
         const bool i_first = role == kRoleFirst || (role == kRoleSelf && i < jl);
@@ -272,6 +253,25 @@ __device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD> 
                                 cx, cy, cz, pe, counted);
         ecell += (double)pe;
         if (kStats && counted) ++npair;
+        if (v.pot_idx2) {
+            // a second potential summed on the same pair (a table potential plus a DPD
+            // thermostat), evaluated on the pair's own displacement
+            const int q2 = v.pot_idx2[pot_base + ti * v.ntypes + tj];
+            if (q2 >= 0) {
+                const DevPot &p2 = v.pots[q2];
+                float r2b = dot3_rn(dxo, dyo, dzo);
+                if (!(r2b < p2.a2)) {
+                    float c2x, c2y, c2z, pe2;
+                    bool counted2;
+                    pair_contribution<kDPD>(v, p2, role, i_first, dxo, dyo, dzo, r2b, tinfo[ti].w, tinfo[tj].w, vi,
+                                            vj, rng_mode, c2x, c2y, c2z, pe2, counted2);
+                    cx = cx + c2x;
+                    cy = cy + c2y;
+                    cz = cz + c2z;
+                    ecell += (double)pe2;
+                }
+            }
+        }
     }
     // segments: runs of equal own index (inactive lanes form the last one)
     const int il_prev = __shfl_up_sync(kFull, il, 1);
@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) force_kernel(EngineVie
                     if (kDPD) sm.own_v[lane] = v.vel[start + i0 + lane];
                     unsigned long long mk = 0ull;
                     for (int t = 0; t < ntypes; ++t)
-                        if (v.pot_idx[pot_base + ti * ntypes + t] >= 0) mk |= 1ull << t;
+                        if (v.pot_idx[pot_base + ti * ntypes + t] >= 0) mk |= 1ull << t;  // a lone second term is moved here
                     sm.own_mask[lane] = mk;
                 }
                 for (int g0 = nb0; g0 < nb1; g0 += kEnt) {

@@ -122,8 +122,10 @@ void solve_node_slopes(const ScalarFn &f, double fpa, double fpb, int n, const f
 }
 
 /* Fills the n interval chunks at c (each kChunk floats) for the nodes xi and
- * returns the largest interval error relative to max(|V|, 1) through err. */
-void fit_intervals(const ScalarFn &f, const ScalarFn &fprime, const float *xi, int n, float *c, float *err) {
+ * returns the largest interval error relative to max(|V|, 1) through err. If
+ * c64 is not null it receives the same coefficients before rounding to float. */
+void fit_intervals(const ScalarFn &f, const ScalarFn &fprime, const float *xi, int n, float *c, double *c64,
+                   float *err) {
     const std::vector<float> &ck = cheb_cos_table();
     std::vector<double> fnode(n + 1), slope(n + 1);
     double samples[kSamples];
@@ -172,6 +174,17 @@ void fit_intervals(const ScalarFn &f, const ScalarFn &fprime, const float *xi, i
         out[2] = 16 * t[5];
         out[1] = 1.0 / h;
         out[0] = m;
+        if (c64) {
+            double *o = c64 + i * kChunk;
+            o[7] = t[0] / 2 - t[2] + t[4];
+            o[6] = t[1] - 3 * t[3] + 5 * t[5];
+            o[5] = 2 * t[2] - 8 * t[4];
+            o[4] = 4 * t[3] - 20 * t[5];
+            o[3] = 8 * t[4];
+            o[2] = 16 * t[5];
+            o[1] = 1.0 / h;
+            o[0] = m;
+        }
 
         double vmax = 0.0, emax = 0.0;
         for (int k = 1; k < kSamples; ++k) {
@@ -247,7 +260,139 @@ void place_nodes(const float *map, float a, float b, int n, std::vector<float> &
     }
 }
 
+/* Interval 0: the linear continuation of interval 1's left end, x = (r - a)/a. */
+template <typename T>
+void fill_interval0(T *c, float a) {
+    c[0] = a;
+    c[1] = 1.0 / a;
+    double coef[kDegree], deriv[kDegree];
+    for (int k = 0; k < kDegree; ++k) {
+        coef[k] = c[2 * kChunk - 1 - k];
+        deriv[k] = 0.0;
+    }
+    for (int i = 0; i < kDegree; ++i)
+        for (int k = kDegree - 1; k >= i; --k) {
+            deriv[i] = coef[k] + (-1.0) * deriv[i];
+            coef[k] *= (k - i) * c[kChunk + 1] * a;
+        }
+    c[kChunk - 1] = deriv[0];
+    c[kChunk - 2] = deriv[1];
+    c[kChunk - 3] = 0.5 * deriv[2];
+    for (int k = 3; k <= kDegree; ++k) c[kChunk - 1 - k] = 0.0;
+}
+
+/* The analytic form of a table kind: value and first derivative at the
+ * construction parameters (the layout of PotentialTable::params). */
+bool form_functions(int form, const std::vector<double> &q, ScalarFn &f, ScalarFn &fp) {
+    switch (form) {
+    case kFormLJ126: {
+        const double A = q[2], B = q[3];
+        f = [A, B](double r) {
+            const double ir = 1.0 / r, ir2 = ir * ir, ir6 = ir2 * ir2 * ir2, ir12 = ir6 * ir6;
+            return A * ir12 - B * ir6;
+        };
+        fp = [A, B](double r) {
+            const double ir = 1.0 / r, ir2 = ir * ir, ir4 = ir2 * ir2, ir12 = ir4 * ir4 * ir4;
+            return 6.0 * ir * (-2.0 * A * ir12 + B * ir4 * ir2);
+        };
+        return true;
+    }
+    case kFormMorse: {
+        const double d = q[0], al = q[1];
+        f = [d, al](double r) { return d * (std::pow(M_E, -2 * al * (-1 + r)) - 2 / std::pow(M_E, al * (-1 + r))); };
+        fp = [d, al](double r) {
+            return d * ((-2 * al) / std::pow(M_E, 2 * al * (-1 + r)) + (2 * al) / std::pow(M_E, al * (-1 + r)));
+        };
+        return true;
+    }
+    case kFormHarmonic: {
+        const double k = q[0], r0 = q[1];
+        f = [k, r0](double r) { return k * (r - r0) * (r - r0); };
+        fp = [k, r0](double r) { return 2.0 * k * (r - r0); };
+        return true;
+    }
+    default:
+        return false;
+    }
+}
+
+/* d/dtheta_k of the analytic form (value and first derivative). */
+bool form_param_derivative(int form, const std::vector<double> &q, int k, ScalarFn &f, ScalarFn &fp) {
+    if (form == kFormLJ126 && (k == 2 || k == 3)) {
+        if (k == 2) {  // dV/dA = r^-12
+            f = [](double r) { return std::pow(r, -12.0); };
+            fp = [](double r) { return -12.0 * std::pow(r, -13.0); };
+        } else {  // dV/dB = -r^-6
+            f = [](double r) { return -std::pow(r, -6.0); };
+            fp = [](double r) { return 6.0 * std::pow(r, -7.0); };
+        }
+        return true;
+    }
+    if (form == kFormMorse && (k == 0 || k == 1)) {
+        const double d = q[0], al = q[1];
+        if (k == 0) {  // V is linear in d
+            f = [al](double r) { return std::exp(-2 * al * (r - 1)) - 2 * std::exp(-al * (r - 1)); };
+            fp = [al](double r) { return -2 * al * std::exp(-2 * al * (r - 1)) + 2 * al * std::exp(-al * (r - 1)); };
+        } else {
+            f = [d, al](double r) {
+                const double u = r - 1;
+                return d * (-2 * u * std::exp(-2 * al * u) + 2 * u * std::exp(-al * u));
+            };
+            fp = [d, al](double r) {
+                const double u = r - 1, e2 = std::exp(-2 * al * u), e1 = std::exp(-al * u);
+                return d * (-2 * e2 + 4 * al * u * e2 + 2 * e1 - 2 * al * u * e1);
+            };
+        }
+        return true;
+    }
+    if (form == kFormHarmonic && (k == 0 || k == 1)) {
+        const double kk = q[0], r0 = q[1];
+        if (k == 0) {
+            f = [r0](double r) { return (r - r0) * (r - r0); };
+            fp = [r0](double r) { return 2.0 * (r - r0); };
+        } else {
+            f = [kk, r0](double r) { return -2.0 * kk * (r - r0); };
+            fp = [kk](double) { return -2.0 * kk; };
+        }
+        return true;
+    }
+    return false;
+}
+
+/* Refit of p's coefficient array for the function f (end slopes from fp) on
+ * p's frozen nodes. */
+void refit_on_nodes(PotentialTable &p, const ScalarFn &f, const ScalarFn &fp) {
+    const int n = p.n;
+    std::vector<float> c((size_t)(n + 1) * kChunk, 0.0f);
+    std::vector<double> c64((size_t)(n + 1) * kChunk, 0.0);
+    float err = 0.0f;
+    fit_intervals(f, fp, p.nodes.data(), n, c.data() + kChunk, c64.data() + kChunk, &err);
+    fill_interval0(c.data(), p.nodes[0]);
+    fill_interval0(c64.data(), p.nodes[0]);
+    p.c.swap(c);
+    p.c64.swap(c64);
+}
+
 }  // namespace
+
+int refit_frozen(PotentialTable &p, const std::vector<double> &params) {
+    if (p.kind != kKindTable || p.nodes.empty() || params.size() != p.params.size()) return -1;
+    ScalarFn f, fp;
+    if (!form_functions(p.form, params, f, fp)) return -1;
+    refit_on_nodes(p, f, fp);
+    p.params = params;
+    if (p.form == kFormMorse) p.r0_plusone = (float)(params[2] + 1);
+    return 0;
+}
+
+int param_derivative_table(const PotentialTable &p, int k, PotentialTable &out) {
+    if (p.kind != kKindTable || p.nodes.empty()) return -1;
+    ScalarFn f, fp;
+    if (!form_param_derivative(p.form, p.params, k, f, fp)) return -1;
+    out = p;
+    refit_on_nodes(out, f, fp);
+    return 0;
+}
 
 int build_table(PotentialTable &p, const ScalarFn &f, const ScalarFn &fp, const ScalarFn &f6, float a, float b,
                 float tol) {
@@ -274,7 +419,7 @@ int build_table(PotentialTable &p, const ScalarFn &f, const ScalarFn &fp, const 
         std::vector<float> xi;
         place_nodes(map, a, b, n, xi);
         c.assign((size_t)(n + 1) * kChunk, 0.0f);
-        fit_intervals(f, fp, xi.data(), n, c.data() + kChunk, &err);
+        fit_intervals(f, fp, xi.data(), n, c.data() + kChunk, nullptr, &err);
     };
 
     int l = kIvalsFirstLeft, r = kIvalsFirstRight;
@@ -320,25 +465,14 @@ int build_table(PotentialTable &p, const ScalarFn &f, const ScalarFn &fp, const 
     p.alpha[2] = map[2] * n;
     p.alpha[3] = map[3];
     p.alpha[0] += 1.0;
-
-    // interval 0: linear continuation of interval 1's left end, x = (r - a)/a
-    float *c = p.c.data();
-    c[0] = a;
-    c[1] = 1.0 / a;
-    double coef[kDegree], deriv[kDegree];
-    for (int k = 0; k < kDegree; ++k) {
-        coef[k] = c[2 * kChunk - 1 - k];
-        deriv[k] = 0.0;
-    }
-    for (int i = 0; i < kDegree; ++i)
-        for (int k = kDegree - 1; k >= i; --k) {
-            deriv[i] = coef[k] + (-1.0) * deriv[i];
-            coef[k] *= (k - i) * c[kChunk + 1] * a;
-        }
-    c[kChunk - 1] = deriv[0];
-    c[kChunk - 2] = deriv[1];
-    c[kChunk - 3] = 0.5 * deriv[2];
-    for (int k = 3; k <= kDegree; ++k) c[kChunk - 1 - k] = 0.0;
+    place_nodes(map, a, b, n, p.nodes);
+    fill_interval0(p.c.data(), a);
+    // the unrounded coefficients of the same fit
+    std::vector<float> c32(p.c.size(), 0.0f);
+    p.c64.assign(p.c.size(), 0.0);
+    float err = 0.0f;
+    fit_intervals(f, fp, p.nodes.data(), n, c32.data() + kChunk, p.c64.data() + kChunk, &err);
+    fill_interval0(p.c64.data(), a);
     return 0;
 }
 
@@ -360,6 +494,7 @@ int make_lj126(PotentialTable &p, double a, double b, double A, double B, double
         return 10080.0 * ir12 * (884.0 * A * ir6 - 33.0 * B);
     };
     p.params = {a, b, A, B, tol};
+    p.form = kFormLJ126;
     return build_table(p, f, fp, f6, (float)a, (float)b, (float)tol);
 }
 
@@ -377,6 +512,7 @@ int make_morse(PotentialTable &p, double d, double al, double r0, double min, do
                     (2 * std::pow(al, 6)) / std::pow(M_E, al * (-1 + r)));
     };
     p.params = {d, al, r0, min, max, tol};
+    p.form = kFormMorse;
     return build_table(p, f, fp, f6, (float)min, (float)max, (float)tol);
 }
 
@@ -387,6 +523,7 @@ int make_harmonic(PotentialTable &p, double k, double r0, double min, double max
     ScalarFn fp = [k, r0](double r) { return 2.0 * k * (r - r0); };
     ScalarFn f6 = [](double) { return 0.0; };
     p.params = {k, r0, min, max, tol};
+    p.form = kFormHarmonic;
     return build_table(p, f, fp, f6, (float)min, (float)max, (float)tol);
 }
 

@@ -30,9 +30,24 @@ struct PotentialTable {
     float a = 0.0f, b = 0.0f;
     int n = 0;
     std::vector<float> c;  // (n+1)*8
+    std::vector<double> c64;  // the same coefficients before rounding to float
     float dpd_alpha = 0, dpd_gamma = 0, dpd_sigma = 0;
     std::vector<double> params;  // construction parameters, for re-fitting
+    int form = 0;                // analytic form (kForm*), for frozen-node re-fits
+    std::vector<float> nodes;    // the fit's n+1 interval nodes (stretched domain)
 };
+
+enum : int { kFormNone = 0, kFormLJ126 = 1, kFormMorse = 2, kFormHarmonic = 3, kFormPower = 4 };
+
+/* Frozen-node re-fit: the table of p's analytic form at new parameters, on p's
+ * nodes and interval map (same n), so the coefficients depend linearly on the
+ * sampled function. params has the construction parameters' layout. */
+int refit_frozen(PotentialTable &p, const std::vector<double> &params);
+/* Table (same nodes, map and n as p) of dV/dtheta_k: the derivative of p's
+ * coefficients with respect to construction parameter k at p.params. Only
+ * parameters that change the tabulated function have one (LJ A, B; Morse d, a;
+ * harmonic k, r0); returns -1 otherwise. */
+int param_derivative_table(const PotentialTable &p, int k, PotentialTable &out);
 
 int build_table(PotentialTable &p, const ScalarFn &f, const ScalarFn &fp, const ScalarFn &f6, float a, float b,
                 float tol);

@@ -215,3 +215,64 @@ def build_gpu_batch(specs, stream=None):
         u._add_particles(np.asarray(sc["x"]), np.asarray(sc["v"], dtype=np.float32),
                          np.asarray(sc["t"], dtype=np.int32), rep)
     return u
+
+
+def adjoint_spec(n=32768, seed=7, density=0.8, cut=2.5, dt=0.01, a=5.0, r0=1.0, gamma=1.0, sigma=1.0, jitter=0.15):
+    """Two-type Morse mixture (parameters drawn as the cell-sorting replicas') plus
+    a DPD thermostat summed on every type pair (alpha 0, gamma, sigma; kT =
+    sigma^2 / (2 gamma)), Newtonian, mass 1, periodic cube at the given density.
+    Positions: a jittered simple-cubic lattice of k^3 >= n sites, first n kept."""
+    rng = np.random.default_rng(seed)
+    k = int(np.ceil(n ** (1.0 / 3.0) - 1e-9))
+    L = (n / density) ** (1.0 / 3.0)
+    sp = L / k
+    g = (np.arange(k) + 0.5) * sp
+    x = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)[:n]
+    x = x + rng.uniform(-jitter, jitter, size=x.shape) * sp
+    x = np.mod(x, L)
+    x = np.minimum(x, L * (1 - 1e-6)).astype(np.float32).astype(np.float64)
+    t = np.zeros(n, dtype=np.int32)
+    t[rng.permutation(n)[: n // 2]] = 1
+    kT = sigma * sigma / (2 * gamma)
+    v = rng.normal(0, np.sqrt(kT), size=(n, 3))
+    v -= v.mean(axis=0)
+    dAA, dBB = rng.uniform(0.2, 1.0, size=2)
+    dAB = rng.uniform(0.05, 0.5)
+    cells = max(3, int(L // cut))
+    morse = {(0, 0): [float(dAA), a, r0, 1e-4, cut, 1e-3], (0, 1): [float(dAB), a, r0, 1e-4, cut, 1e-3],
+             (1, 1): [float(dBB), a, r0, 1e-4, cut, 1e-3]}
+    return dict(dim=[L, L, L], cells=[cells] * 3, cutoff=cut, dt=dt, bc=("periodic",) * 3,
+                types=[(1.0, 1.0, m.Newtonian), (1.0, 1.0, m.Newtonian)], morse=morse,
+                dpd=[0.0, float(gamma), float(sigma), cut, 0.0], x=x, v=v.astype(np.float32), t=t)
+
+
+def rdf_target(nbins=64, rmax=2.5, seed=11):
+    """A seeded smooth target for the A-B radial distribution: 1 plus a few
+    random sine modes, damped near r = 0."""
+    rng = np.random.default_rng(seed)
+    c = (np.arange(nbins) + 0.5) * rmax / nbins
+    g = 1.0 + sum(rng.normal(0, 0.3) * np.sin((k + 1) * np.pi * c / rmax) for k in range(4))
+    return np.clip(g, 0.0, None) * (1 - np.exp(-(c / 0.9) ** 8))
+
+
+def build_adjoint(spec, stream=None):
+    """The adjoint workload in the engine (Philox DPD stream); returns the
+    universe and the ten differentiated parameters: Morse (d, a, r0) of AA, AB,
+    BB and the DPD gamma shared by the three pairs."""
+    from . import adjoint as A
+    bc = {"x": spec["bc"][0], "y": spec["bc"][1], "z": spec["bc"][2]}
+    m.init(dim=spec["dim"], cells=spec["cells"], cutoff=spec["cutoff"], dt=spec["dt"], bc=bc, rng="philox",
+           stream=stream)
+    types = [type(f"T{k}", (m.Particle,), {"mass": ms, "radius": rad, "dynamics": dyn})
+             for k, (ms, rad, dyn) in enumerate(spec["types"])]
+    u = m.universe
+    slots, dpds = [], []
+    for (ti, tj), q in spec["morse"].items():
+        mp = m.Potential.morse(*q)
+        dp = m.Potential.dpd(*spec["dpd"][:4], shifted=bool(spec["dpd"][4]))
+        u.bind(mp + dp, types[ti], types[tj])
+        slots += [[(mp, 0)], [(mp, 1)], [(mp, 2)]]
+        dpds.append((dp, 1))
+    slots.append(dpds)
+    u._add_particles(np.asarray(spec["x"]), np.asarray(spec["v"], dtype=np.float32), np.asarray(spec["t"], dtype=np.int32))
+    return u, A.Parameters(u, slots)
