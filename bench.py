@@ -239,11 +239,55 @@ def forms_and_configs(args, stream, flush):
         ms_s += _time_steps(L, e, Kb, stream, flush)
         check(L.mxg_engine_status(e), "sequential")
         m.universe.close()
+    out["adjoint_32k"] = adjoint_form(stream)
     out["batched_256"] = {"value": ntot * Kb / (ms_b / 1e3), "unit": "particle-steps/s", "replicas": len(specs),
                           "particles": ntot, "steps": Kb, "ms_per_step": ms_b / Kb,
                           "force_ctas_per_sm": per_sm,
                           "sequential_plain_value": ntot * Kb / (ms_s / 1e3),
                           "speedup_vs_sequential": ms_s / ms_b}
+    return out
+
+
+def adjoint_form(stream, nsteps=200, every=20):
+    """The adjoint workload: 32,768-particle two-type Morse mixture with a summed
+    DPD thermostat (Philox), 200 steps, snapshots every 20, RDF loss; gradients of
+    the loss with respect to the ten potential parameters and the initial state.
+    Timed with CUDA events on the engine's stream around forward + loss +
+    backward (segment recompute included)."""
+    import torch
+    import mechanica_b200 as m
+    from mechanica_b200 import adjoint as A
+    from mechanica_b200 import workloads as W
+    spec = W.adjoint_spec(n=32768, seed=7)
+    with torch.cuda.stream(stream):
+        u, P = W.build_adjoint(spec, stream=stream.cuda_stream)
+        sim = A.Simulation(u, P, nsteps=nsteps, checkpoint_every=every, step0=0)
+        tgt = torch.tensor(W.rdf_target(), dtype=torch.float64, device="cuda")
+        theta = torch.tensor(P.theta(), dtype=torch.float64, requires_grad=True)
+        x0 = torch.tensor(spec["x"], dtype=torch.float64, requires_grad=True)
+        v0 = torch.tensor(spec["v"], dtype=torch.float64, requires_grad=True)
+        # warm-up (builds the engine, derivative tables and graphs)
+        x4 = A.trajectory(theta, x0, v0, A.Simulation(u, P, nsteps=every, checkpoint_every=every, step0=0))
+        A.rdf_loss(x4, tgt, spec["dim"], 0, 1)[0].backward()
+        theta.grad = None
+        torch.cuda.synchronize()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        x4 = A.trajectory(theta, x0, v0, sim)
+        loss, _ = A.rdf_loss(x4, tgt, spec["dim"], 0, 1)
+        e1.record(stream)
+        loss.backward()
+        e2.record(stream)
+        torch.cuda.synchronize()
+    fwd, tot = e0.elapsed_time(e1), e0.elapsed_time(e2)
+    n = len(spec["t"])
+    out = {"value": n * nsteps / (tot / 1e3), "unit": "particle-steps/s (forward + backward)", "particles": n,
+           "steps": nsteps, "checkpoint_every": every, "ms_forward": fwd, "ms_forward_backward": tot,
+           "forward_value": n * nsteps / (fwd / 1e3), "loss": float(loss.item()),
+           "grad_theta": [float(g) for g in theta.grad.numpy()],
+           "params": "Morse (d, a, r0) of AA, AB, BB; DPD gamma shared",
+           "check": "gradients vs FP64 central differences: tests/test_gpu_adjoint.py (512 particles, 12 steps)"}
+    u.close()
     return out
 
 
