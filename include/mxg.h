@@ -200,7 +200,10 @@ int mxg_engine_unload(mxg_engine *e, int n, double *x, float *v, float *f, int *
  * particles are re-binned as engine_addpart would place them. */
 int mxg_engine_load(mxg_engine *e, int n, const double *x, const float *v);
 /* Potential energy (nonbonded + bonded) of the last force evaluation and the current kinetic energy,
- * both reduced in FP64 on the device. virial9 may be NULL. */
+ * both reduced in FP64 on the device. virial9 (may be NULL): the nonbonded pair virial
+ * sum over pairs of (x_first - x_second) (x) F_first of the current positions, reduced in FP64 (one
+ * extra force pass that changes no engine state); the reference's MxCalculateVirial returns zeros
+ * (metrics.cpp:183,246). */
 int mxg_engine_energy(mxg_engine *e, double *epot, double *ekin, double *virial9);
 double mxg_engine_kinetic_energy(mxg_engine *e);
 /* Cell-pair task list rows (type, sid, i, j) as space_init builds them. */

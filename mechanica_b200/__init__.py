@@ -546,6 +546,14 @@ class _Universe:
         """(positions, velocities, forces, cell, cell-relative positions) by particle id."""
         return self._unload()
 
+    def virial(self):
+        """The nonbonded pair virial (3x3, FP64) of the current positions."""
+        self._ensure()
+        out = np.zeros(9)
+        check(lib().mxg_engine_energy(self._e, None, None, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+              "virial")
+        return out.reshape(3, 3)
+
     def energies(self):
         self._ensure()
         ep, ek = ctypes.c_double(), ctypes.c_double()

@@ -133,6 +133,7 @@ struct EngineView {      // everything a kernel needs, passed by value
     double *epot_cell;       // per force work item: nonbonded energy of the last force pass
     unsigned *status;
     unsigned long long *pair_stats;  // non-null only for the statistics launch
+    double *virial_partials;         // non-null only for the virial launch: [warp][6]
     const int *nb_rev;       // FIRST entries: the pair's plane in the neighbour's received sums
     const int *sec_count;    // per cell: SECOND entries, i.e. planes of received sums
     const int *cell_planes;  // per cell: received planes plus own-side planes of its later work items

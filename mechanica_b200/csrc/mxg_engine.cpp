@@ -380,6 +380,8 @@ struct mxg_engine {
     size_t dcoef_cap = 0;
     float4 *d_adj_w = nullptr, *d_adj_gx = nullptr, *d_adj_gv = nullptr;
     double *d_adj_partials = nullptr;
+    double *d_virial_partials = nullptr, *d_virial_out = nullptr;
+    int virial_cap = 0;
     int *d_bond_off = nullptr, *d_bond_list = nullptr;
     unsigned *d_status = nullptr;
     unsigned long long *d_step = nullptr;
@@ -540,6 +542,7 @@ struct mxg_engine {
         v.epot_cell = d_epot_cell;
         v.status = d_status;
         v.pair_stats = nullptr;
+        v.virial_partials = nullptr;
         v.nb_rev = d_nb_rev;
         v.sec_count = d_sec_count;
         v.cell_planes = d_cell_planes;
@@ -1371,8 +1374,23 @@ int mxg_engine_energy(mxg_engine *e, double *epot, double *ekin, double *virial9
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     if (epot) *epot = out[0];
     if (ekin) *ekin = out[1];
-    if (virial9)
-        for (int k = 0; k < 9; ++k) virial9[k] = 0.0;
+    if (virial9) {
+        // the pair virial of the current positions: a force pass in the kernel's
+        // virial mode, which writes only its per-warp FP64 partials
+        const int nwarps = e->force_grid * kWarpsPerBlock;
+        if (nwarps > e->virial_cap) {
+            if (e->alloc(&e->d_virial_partials, (size_t)nwarps * 6) != MXG_OK) return MXG_ERR_MALLOC;
+            if (!e->d_virial_out && e->alloc(&e->d_virial_out, 9) != MXG_OK) return MXG_ERR_MALLOC;
+            e->virial_cap = nwarps;
+        }
+        EngineView v = e->view(e->cur);
+        v.virial_partials = e->d_virial_partials;
+        launch_force(v, e->has_dpd, e->force_grid, false, e->stream);
+        launch_virial_reduce(e->d_virial_partials, nwarps, e->d_virial_out, e->stream);
+        CUDA_TRY(cudaMemcpyAsync(virial9, e->d_virial_out, 9 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+        CUDA_TRY(cudaStreamSynchronize(e->stream));
+        CUDA_TRY(cudaGetLastError());
+    }
     return MXG_OK;
 }
 

@@ -194,11 +194,13 @@ struct ForceSmem {
 };
 
 /* Pass 2 over the nb <= 32 queued pairs from qhead: one interacting pair per
- * lane; own-side segmented sums into own_f, neighbour-side sums into nb_f. */
-template <bool kDPD, bool kStats>
+ * lane; own-side segmented sums into own_f, neighbour-side sums into nb_f.
+ * kMode 1 counts the pairs (once each), kMode 2 sums the pair virial
+ * (x_first - x_second) (x) F_first in FP64 (xx, yy, zz, xy, xz, yz). */
+template <bool kDPD, int kMode>
 __device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD> &sm, const float4 *tinfo, int qhead,
                                            int nb, int i0, int own_start, int pot_base, unsigned rng_mode,
-                                           double &ecell, unsigned long long &npair) {
+                                           double &ecell, unsigned long long &npair, double *vir) {
     const int lane = threadIdx.x & 31;
     float cx = 0.f, cy = 0.f, cz = 0.f;
     int il = -1, jj = 0;
@@ -252,7 +254,7 @@ __device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD> 
         pair_contribution<kDPD>(v, p, role, i_first, dx, dy, dz, r2, tinfo[ti].w, tinfo[tj].w, vi, vj, rng_mode,
                                 cx, cy, cz, pe, counted);
         ecell += (double)pe;
-        if (kStats && counted) ++npair;
+        if (kMode == 1 && counted) ++npair;
         if (v.pot_idx2) {
             // a second potential summed on the same pair (a table potential plus a DPD
             // thermostat), evaluated on the pair's own displacement
@@ -271,6 +273,14 @@ __device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD> 
                     ecell += (double)pe2;
                 }
             }
+        }
+        if (kMode == 2 && i_first) {
+            vir[0] += (double)dxo * cx;
+            vir[1] += (double)dyo * cy;
+            vir[2] += (double)dzo * cz;
+            vir[3] += (double)dxo * cy;
+            vir[4] += (double)dxo * cz;
+            vir[5] += (double)dyo * cz;
         }
     }
     // segments: runs of equal own index (inactive lanes form the last one)
@@ -327,9 +337,10 @@ constexpr size_t force_smem_bytes() {
     return sizeof(ForceSmem<kDPD>) * kWarpsPerBlock;
 }
 
-template <bool kDPD, bool kStats>
+template <bool kDPD, int kMode>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) force_kernel(EngineView v) {
     unsigned long long npair = 0;  // interacting pairs counted once (statistics launch only)
+    double vir[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // pair virial (virial launch only)
     extern __shared__ float4 force_smem[];
     __shared__ float4 tinfo[kMaxTypes];  // per type: constant force (zero if none), radius
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -348,7 +359,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) force_kernel(EngineVie
         const int n = v.cell_count[c];
         double ecell = 0.0;
         if (n == 0) {
-            for (int e = nb0; e < nb1; ++e) {
+            for (int e = nb0; e < nb1 && kMode != 2; ++e) {
                 const int pk = __float_as_int(v.nb_shift[e].w);
                 if ((pk & 3) != kRoleFirst) continue;
                 const int nc = v.nb_cell[e];
@@ -408,7 +419,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) force_kernel(EngineVie
                         }
                     }
                     // skipped pairs owe their neighbour a zero plane (written by the first own chunk)
-                    unsigned zmask = __ballot_sync(kFull, skipped > 0 && i0 == 0);
+                    unsigned zmask = __ballot_sync(kFull, skipped > 0 && i0 == 0 && kMode != 2);
                     while (zmask) {
                         const int k = __ffs(zmask) - 1;
                         zmask &= zmask - 1;
@@ -546,19 +557,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) force_kernel(EngineVie
                             }
                             while (qtail - qhead >= 32) {
                                 __syncwarp();
-                                eval_batch<kDPD, kStats>(v, sm, tinfo, qhead, 32, i0, start, pot_base, rng_mode,
-                                                         ecell, npair);
+                                eval_batch<kDPD, kMode>(v, sm, tinfo, qhead, 32, i0, start, pot_base, rng_mode,
+                                                        ecell, npair, vir);
                                 qhead += 32;
                             }
                         }
                         if (qtail > qhead) {
                             __syncwarp();
-                            eval_batch<kDPD, kStats>(v, sm, tinfo, qhead, qtail - qhead, i0, start, pot_base,
-                                                     rng_mode, ecell, npair);
+                            eval_batch<kDPD, kMode>(v, sm, tinfo, qhead, qtail - qhead, i0, start, pot_base,
+                                                    rng_mode, ecell, npair, vir);
                         }
                         __syncwarp();
                         // ---- neighbour-side sums of FIRST entries into their planes
-                        for (int idx = lane; idx < M; idx += 32) {
+                        for (int idx = lane; idx < M && kMode != 2; idx += 32) {
                             const int meta = __float_as_int(sm.nb_s[idx].w);
                             if ((meta & 3) != kRoleFirst) continue;
                             const int ke = (meta >> 2) & 31;
@@ -578,17 +589,35 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) force_kernel(EngineVie
                     const float4 f = sm.own_f[lane];
                     // the cell's first work item writes the force, later ones their own plane
                     float4 *dst = part == 0 ? v.force : v.planes + (size_t)(v.sec_count[c] + part - 1) * v.nparts;
-                    dst[start + i0 + lane] = make_float4(f.x, f.y, f.z, 0.f);
+                    if (kMode != 2) dst[start + i0 + lane] = make_float4(f.x, f.y, f.z, 0.f);
                 }
             }
         }
         for (int off = 16; off > 0; off >>= 1) ecell += __shfl_xor_sync(kFull, ecell, off);
-        if (lane == 0) v.epot_cell[it] = ecell;
+        if (lane == 0 && kMode != 2) v.epot_cell[it] = ecell;
     }
-    if (kStats) {
+    if (kMode == 1) {
         for (int off = 16; off > 0; off >>= 1) npair += __shfl_xor_sync(kFull, npair, off);
         if (lane == 0) atomicAdd(v.pair_stats, npair);
     }
+    if (kMode == 2) {  // this warp's virial, lanes summed in a fixed tree (the launch writes nothing else)
+        for (int k = 0; k < 6; ++k) {
+            double t = vir[k];
+            for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(kFull, t, off);
+            if (lane == 0) v.virial_partials[(size_t)(blockIdx.x * kWarpsPerBlock + w) * 6 + k] = t;
+        }
+    }
+}
+
+/* The 3x3 pair virial from the warps' partials, in warp order. */
+__global__ void virial_reduce_kernel(const double *partials, int nwarps, double *out9) {
+    const int k = threadIdx.x;
+    if (k >= 6) return;
+    double t = 0.0;
+    for (int q = 0; q < nwarps; ++q) t += partials[(size_t)q * 6 + k];
+    const int rc[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+    out9[rc[k][0] * 3 + rc[k][1]] = t;
+    out9[rc[k][1] * 3 + rc[k][0]] = t;
 }
 
 /* A particle's own-side force plus, in plane order, the sums its cell received
@@ -812,59 +841,67 @@ __global__ void integrate_kernel(EngineView v, float4 *pos, float4 *vel, int *ne
 /* re-binning                                                                */
 /* ------------------------------------------------------------------------ */
 
-/* New occupancy count_old - out + in, exclusive scan into new_start; single
- * block, each thread scans a contiguous run of cells (loads issued eight at a
- * time), warp-shuffle scans across the threads. */
+/* New occupancy count_old - out + in, exclusive scan into new_start. One block
+ * of 1024 threads walks the cells in chunks of kScanChunk: the counts go
+ * through shared memory so that every global load and store is coalesced; each
+ * thread scans eight consecutive cells of the chunk, warp-shuffle scans join
+ * the threads, and a carry joins the chunks. */
+constexpr int kScanChunk = 8192;
+__device__ __forceinline__ int scan_pad(int i) { return i + (i >> 5); }  // conflict-free 8-cell runs
+
 __global__ void __launch_bounds__(1024) scan_kernel(int ncells, const int *__restrict__ old_count,
                                                    const int *__restrict__ out_count, const int *__restrict__ in_count,
                                                    int *new_start, int *new_count, unsigned long long *step) {
+    __shared__ int cnt[kScanChunk + kScanChunk / 32];
     __shared__ int warp_total[32];
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-    const int per = (ncells + blockDim.x - 1) / blockDim.x;
-    const int b = t * per, e = min(ncells, b + per);
-    int sum = 0;
-    for (int c0 = b; c0 < e; c0 += 8) {
-        int nv[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
+    int carry = 0;
+    for (int c0 = 0; c0 < ncells; c0 += kScanChunk) {
+        const int m = min(kScanChunk, ncells - c0);
+        for (int k = t; k < m; k += blockDim.x) {
             const int c = c0 + k;
-            nv[k] = c < e ? old_count[c] - out_count[c] + min(in_count[c], kBucket) : 0;
+            const int n = old_count[c] - out_count[c] + min(in_count[c], kBucket);
+            new_count[c] = n;
+            cnt[scan_pad(k)] = n;
         }
+        __syncthreads();
+        int v[8], sum = 0;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            if (c0 + k < e) new_count[c0 + k] = nv[k];
-            sum += nv[k];
+        for (int q = 0; q < 8; ++q) {
+            const int idx = 8 * t + q;
+            v[q] = idx < m ? cnt[scan_pad(idx)] : 0;
+            sum += v[q];
         }
-    }
-    int incl = sum;
-    for (int off = 1; off < 32; off <<= 1) {
-        const int o = __shfl_up_sync(kFull, incl, off);
-        if (lane >= off) incl += o;
-    }
-    if (lane == 31) warp_total[wid] = incl;
-    __syncthreads();
-    if (wid == 0) {
-        int x = lane < (int)(blockDim.x >> 5) ? warp_total[lane] : 0;
+        int incl = sum;
         for (int off = 1; off < 32; off <<= 1) {
-            const int o = __shfl_up_sync(kFull, x, off);
-            if (lane >= off) x += o;
+            const int o = __shfl_up_sync(kFull, incl, off);
+            if (lane >= off) incl += o;
         }
-        warp_total[lane] = x;
-    }
-    __syncthreads();
-    int run = (wid > 0 ? warp_total[wid - 1] : 0) + incl - sum;
-    for (int c0 = b; c0 < e; c0 += 8) {
-        int nv[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) nv[k] = c0 + k < e ? new_count[c0 + k] : 0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            if (c0 + k < e) new_start[c0 + k] = run;
-            run += nv[k];
+        if (lane == 31) warp_total[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            int x = lane < (int)(blockDim.x >> 5) ? warp_total[lane] : 0;
+            for (int off = 1; off < 32; off <<= 1) {
+                const int o = __shfl_up_sync(kFull, x, off);
+                if (lane >= off) x += o;
+            }
+            warp_total[lane] = x;
         }
+        __syncthreads();
+        int run = carry + (wid > 0 ? warp_total[wid - 1] : 0) + incl - sum;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = 8 * t + q;
+            if (idx < m) cnt[scan_pad(idx)] = run;
+            run += v[q];
+        }
+        carry += warp_total[31];
+        __syncthreads();
+        for (int k = t; k < m; k += blockDim.x) new_start[c0 + k] = cnt[scan_pad(k)];
+        __syncthreads();
     }
-    if (t == (int)blockDim.x - 1) {
-        new_start[ncells] = warp_total[31];
+    if (t == 0) {
+        new_start[ncells] = carry;
         *step += 1;  // the step counter keying the Philox streams
     }
 }
@@ -993,40 +1030,50 @@ __global__ void reduce_final_kernel(int nblocks, const double *partials, double 
 /* launchers                                                                 */
 /* ------------------------------------------------------------------------ */
 
+template <bool kDPD, int kMode>
+void configure_one() {
+    const int bytes = (int)force_smem_bytes<kDPD>();
+    cudaFuncSetAttribute(force_kernel<kDPD, kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(force_kernel<kDPD, kMode>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+}
+
 void configure_force_kernels() {
     // the force kernel's occupancy is bounded by shared memory: allow its dynamic
     // shared memory and ask for the largest carveout of the unified L1/shared storage
-    const int carve = cudaSharedmemCarveoutMaxShared;
-    const int bd = (int)force_smem_bytes<true>(), bn = (int)force_smem_bytes<false>();
-    cudaFuncSetAttribute(force_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bd);
-    cudaFuncSetAttribute(force_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bd);
-    cudaFuncSetAttribute(force_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bn);
-    cudaFuncSetAttribute(force_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bn);
-    cudaFuncSetAttribute(force_kernel<true, true>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
-    cudaFuncSetAttribute(force_kernel<true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
-    cudaFuncSetAttribute(force_kernel<false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
-    cudaFuncSetAttribute(force_kernel<false, false>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+    configure_one<true, 0>();
+    configure_one<true, 1>();
+    configure_one<true, 2>();
+    configure_one<false, 0>();
+    configure_one<false, 1>();
+    configure_one<false, 2>();
 }
 
 void launch_sort_bounds(const EngineView &v, cudaStream_t st) {
     sort_bounds_kernel<<<(v.ncells * 32 + 255) / 256, 256, 0, st>>>(v);
 }
 
+template <bool kDPD>
+void launch_force_mode(const EngineView &v, int grid, cudaStream_t st) {
+    const size_t bytes = force_smem_bytes<kDPD>();
+    if (v.pair_stats)
+        force_kernel<kDPD, 1><<<grid, kWarpsPerBlock * 32, bytes, st>>>(v);
+    else if (v.virial_partials)
+        force_kernel<kDPD, 2><<<grid, kWarpsPerBlock * 32, bytes, st>>>(v);
+    else
+        force_kernel<kDPD, 0><<<grid, kWarpsPerBlock * 32, bytes, st>>>(v);
+}
+
 void launch_force(const EngineView &v, bool has_dpd, int grid, bool combine, cudaStream_t st) {
-    const bool stats = v.pair_stats != nullptr;
-    const size_t bd = force_smem_bytes<true>(), bn = force_smem_bytes<false>();
-    if (has_dpd) {
-        if (stats)
-            force_kernel<true, true><<<grid, kWarpsPerBlock * 32, bd, st>>>(v);
-        else
-            force_kernel<true, false><<<grid, kWarpsPerBlock * 32, bd, st>>>(v);
-    } else {
-        if (stats)
-            force_kernel<false, true><<<grid, kWarpsPerBlock * 32, bn, st>>>(v);
-        else
-            force_kernel<false, false><<<grid, kWarpsPerBlock * 32, bn, st>>>(v);
-    }
+    if (has_dpd)
+        launch_force_mode<true>(v, grid, st);
+    else
+        launch_force_mode<false>(v, grid, st);
     if (combine) combine_kernel<<<(v.nparts + 255) / 256, 256, 0, st>>>(v);
+}
+
+void launch_virial_reduce(const double *partials, int nwarps, double *out9, cudaStream_t st) {
+    virial_reduce_kernel<<<1, 32, 0, st>>>(partials, nwarps, out9);
 }
 
 void launch_bonds(const EngineView &v, const DevBond *bonds, unsigned *bond_flags, const int *bond_off,

@@ -6,6 +6,7 @@ namespace mxg {
 
 void configure_force_kernels();
 void launch_sort_bounds(const EngineView &v, cudaStream_t st);
+void launch_virial_reduce(const double *partials, int nwarps, double *out9, cudaStream_t st);
 /* combine: add the received planes here (no bond or integrator pass follows) */
 void launch_force(const EngineView &v, bool has_dpd, int grid, bool combine, cudaStream_t st);
 void launch_bonds(const EngineView &v, const DevBond *bonds, unsigned *bond_flags, const int *bond_off,

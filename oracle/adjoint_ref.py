@@ -141,6 +141,22 @@ def run(x0, v0, types, ids, box, mass, radius, terms, cutoff, dt, nsteps, step0,
     return x
 
 
+def run_velocities(x0, v0, types, ids, box, mass, radius, terms, cutoff, dt, nsteps, step0, maxv, every=1,
+                   philox=True):
+    """As run(), returning the velocities every `every` steps (including step 0)."""
+    x = np.array(x0, dtype=np.float64)
+    v = np.array(v0, dtype=np.float64)
+    imass = 1.0 / mass[types]
+    out = [v.copy()]
+    for s in range(nsteps):
+        f = forces(x, v, types, ids, box, radius, terms, cutoff, step0 + s, philox)
+        v = np.clip(v + dt * f * imass[:, None], -maxv, maxv)
+        x = x + dt * v
+        if (s + 1) % every == 0:
+            out.append(v.copy())
+    return np.array(out)
+
+
 def rdf(x, types, box, ta, tb, nbins, rmax, sigma):
     """The smoothed A-B radial distribution of the engine's mxg_rdf, in FP64
     (Gaussian minus its value at the 4 sigma cut)."""

@@ -120,7 +120,7 @@ struct Setup {
 
 template <typename T>
 void pair_force(const Setup<T> &S, int pi, int pj, const T *dx_in, T r2, std::vector<T> &f, double &epot,
-                long long &nint, long long &nrand) {
+                long long &nint, long long &nrand, double *vir) {
     const int ti = S.type[pi], tj = S.type[pj];
     const int pidx = S.pot_of_pair[ti * S.ntypes + tj];
     const int didx = S.dpd_of_pair ? S.dpd_of_pair[ti * S.ntypes + tj] : -1;
@@ -152,6 +152,9 @@ void pair_force(const Setup<T> &S, int pi, int pj, const T *dx_in, T r2, std::ve
                 f[3 * pj + k] = f[3 * pj + k] - ff * e[k];
                 f[3 * pi + k] = f[3 * pi + k] + ff * e[k];
             }
+            if (vir)  // (x_i - x_j) (x) F_i
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b) vir[3 * a + b] += (double)dx[a] * (double)(ff * e[b]);
             ++nint;
         } else {
             T ee, ff;
@@ -161,6 +164,9 @@ void pair_force(const Setup<T> &S, int pi, int pj, const T *dx_in, T r2, std::ve
                 f[3 * pi + k] -= wk;
                 f[3 * pj + k] += wk;
             }
+            if (vir)
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b) vir[3 * a + b] -= (double)dx[a] * (double)(ff * dx[b]);
             epot += (double)ee;
             ++nint;
         }
@@ -168,7 +174,10 @@ void pair_force(const Setup<T> &S, int pi, int pj, const T *dx_in, T r2, std::ve
 }
 
 template <typename T>
-int run(const Setup<T> &S, const int *tasks, int ntasks, double *f_out, double *epot_out, long long *counts) {
+int run(const Setup<T> &S, const int *tasks, int ntasks, double *f_out, double *epot_out, long long *counts,
+        double *vir) {
+    if (vir)
+        for (int k = 0; k < 9; ++k) vir[k] = 0.0;
     // particles per cell, in index order
     std::vector<std::vector<int>> members(S.ncells);
     for (int p = 0; p < S.N; ++p) members[S.cell[p]].push_back(p);
@@ -189,7 +198,7 @@ int run(const Setup<T> &S, const int *tasks, int ntasks, double *f_out, double *
                     const T r2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
                     ++ncand;
                     if (r2 > S.cut2_self) continue;
-                    pair_force(S, pi, pj, dx, r2, f, epot, nint, nrand);
+                    pair_force(S, pi, pj, dx, r2, f, epot, nint, nrand, vir);
                 }
         } else if (type == 2) {  // pair, shift and flip as space_getsid
             int ci = ci0, cj = cj0;
@@ -254,7 +263,7 @@ int run(const Setup<T> &S, const int *tasks, int ntasks, double *f_out, double *
                     const T r2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
                     ++ncand;
                     if (r2 > S.cut2_pair) continue;
-                    pair_force(S, pi, pj, dx, r2, f, epot, nint, nrand);
+                    pair_force(S, pi, pj, dx, r2, f, epot, nint, nrand, vir);
                 }
         }
     }
@@ -269,7 +278,7 @@ int run(const Setup<T> &S, const int *tasks, int ntasks, double *f_out, double *
 }
 
 template <typename T>
-int build_and_run(const OrcInput *in, double *f_out, double *epot_out, long long *counts) {
+int build_and_run(const OrcInput *in, double *f_out, double *epot_out, long long *counts, double *vir) {
     Setup<T> S;
     S.N = in->N;
     S.x.resize(3 * (size_t)in->N);
@@ -322,14 +331,22 @@ int build_and_run(const OrcInput *in, double *f_out, double *epot_out, long long
     S.prune = in->pruning != 2;
     for (int q = 0; q < 13; ++q)
         for (int k = 0; k < 3; ++k) S.axes[q][k] = (float)kCellShift[q][k];
-    return run(S, in->tasks, in->ntasks, f_out, epot_out, counts);
+    return run(S, in->tasks, in->ntasks, f_out, epot_out, counts, vir);
 }
 
 }  // namespace
 
+extern "C" int orc_nonbond_virial(int precision, const OrcInput *in, double *f_out, double *epot_out,
+                                  long long *counts, double *virial_out) {
+    if (!in || !f_out || !epot_out) return -1;
+    if (precision == 32) return build_and_run<float>(in, f_out, epot_out, counts, virial_out);
+    if (precision == 64) return build_and_run<double>(in, f_out, epot_out, counts, virial_out);
+    return -1;
+}
+
 extern "C" int orc_nonbond(int precision, const OrcInput *in, double *f_out, double *epot_out, long long *counts) {
     if (!in || !f_out || !epot_out) return -1;
-    if (precision == 32) return build_and_run<float>(in, f_out, epot_out, counts);
-    if (precision == 64) return build_and_run<double>(in, f_out, epot_out, counts);
+    if (precision == 32) return build_and_run<float>(in, f_out, epot_out, counts, nullptr);
+    if (precision == 64) return build_and_run<double>(in, f_out, epot_out, counts, nullptr);
     return -1;
 }

@@ -36,6 +36,9 @@ typedef struct OrcInput {
 
 /* precision 32 or 64; f_out N*3; counts[3] = candidates, interacting, r<a skipped */
 int orc_nonbond(int precision, const OrcInput *in, double *f_out, double *epot_out, long long *counts);
+/* the same, plus the pair virial sum (x_first - x_second) (x) F_first, 9 doubles row-major */
+int orc_nonbond_virial(int precision, const OrcInput *in, double *f_out, double *epot_out, long long *counts,
+                       double *virial_out);
 
 #ifdef __cplusplus
 }

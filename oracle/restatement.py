@@ -42,6 +42,9 @@ def lib():
         _lib.orc_nonbond.argtypes = [ctypes.c_int, ctypes.POINTER(_OrcInput), ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_void_p]
         _lib.orc_nonbond.restype = ctypes.c_int
+        _lib.orc_nonbond_virial.argtypes = [ctypes.c_int, ctypes.POINTER(_OrcInput), ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        _lib.orc_nonbond_virial.restype = ctypes.c_int
     return _lib
 
 
@@ -84,7 +87,7 @@ def cell_origins(dim, cdim, origin=(0.0, 0.0, 0.0)):
     return out
 
 
-def nonbond(scn, xrel, vel, cell, tasks, cdim, precision=64, tables=None, second=None, pruning=0):
+def nonbond(scn, xrel, vel, cell, tasks, cdim, precision=64, tables=None, second=None, pruning=0, virial=False):
     """Forces (N,3) float64, energy, counts for a configuration.
 
     tables: {pot index: (info, coef)} for scn["pots"] order (defaults to the
@@ -166,6 +169,13 @@ def nonbond(scn, xrel, vel, cell, tasks, cdim, precision=64, tables=None, second
     f = np.zeros((N, 3))
     ep = ctypes.c_double()
     counts = np.zeros(3, dtype=np.int64)
+    if virial:
+        vir = np.zeros(9)
+        rc = lib().orc_nonbond_virial(int(precision), ctypes.byref(inp), f.ctypes.data, ctypes.addressof(ep),
+                                      counts.ctypes.data, vir.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"orc_nonbond_virial {rc}")
+        return f, ep.value, counts, vir.reshape(3, 3)
     rc = lib().orc_nonbond(int(precision), ctypes.byref(inp), f.ctypes.data, ctypes.addressof(ep), counts.ctypes.data)
     if rc != 0:
         raise RuntimeError(f"orc_nonbond {rc}")
