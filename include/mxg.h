@@ -256,6 +256,13 @@ int mxg_engine_set_step_counter(mxg_engine *e, unsigned long long step);
 int mxg_rdf(const void *x4, int n, const double *box, int type_a, int type_b, int nbins, double dr, double sigma,
             void *hist, const double *coef, void *grad4, void *stream);
 
+/* The integrator (engine.h EngineIntegrator, set by universe_init from the `integrator` keyword,
+ * src/MxSimulator.cpp:218-230): 0 forward Euler (engine_advance_forward_euler), 1 Runge-Kutta 4
+ * (engine_advance_runge_kutta_4, engine_advance.cpp:443-698). Set before mxg_engine_start. The RK4
+ * stages keep the step's cell frame (the reference re-bins between stages and leaves the stage
+ * origin in the old cell's frame, so a particle crossing a face mid-step lands a cell edge away
+ * there). */
+int mxg_engine_set_integrator(mxg_engine *e, int kind);
 /* DPD random term: 0 = reference semantics (xi = 1, dpd_eval.hpp:57), 1 = Philox stream keyed on
  * (step, particle id pair). Set before mxg_engine_start. */
 int mxg_engine_set_rng_mode(mxg_engine *e, int mode);

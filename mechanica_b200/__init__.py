@@ -28,7 +28,7 @@ from ._native import EngineError, check, f32, f64, i32, lib, ptr
 
 __all__ = [
     "init", "Universe", "universe", "Particle", "Potential", "Bond", "bind", "forces", "step", "run",
-    "Newtonian", "Overdamped", "FORWARD_EULER", "BOUNDARY_NONE", "PERIODIC_X", "PERIODIC_Y", "PERIODIC_Z",
+    "Newtonian", "Overdamped", "FORWARD_EULER", "RUNGE_KUTTA_4", "BOUNDARY_NONE", "PERIODIC_X", "PERIODIC_Y", "PERIODIC_Z",
     "PERIODIC_FULL", "FREESLIP_X", "FREESLIP_Y", "FREESLIP_Z", "FREESLIP_FULL", "EngineError",
 ]
 
@@ -36,6 +36,7 @@ __all__ = [
 Newtonian = 0
 Overdamped = 1
 FORWARD_EULER = 0
+RUNGE_KUTTA_4 = 1
 
 # integer boundary flags (src/mdcore/include/space.h:44-59)
 BOUNDARY_NONE = 0
@@ -324,8 +325,10 @@ class _Universe:
         self._e = None
 
     # ---- configuration ----
-    def _init(self, dim, cells, cutoff, dt, bc, max_distance, origin, rng, max_types, stream=None, pair_pruning=0):
+    def _init(self, dim, cells, cutoff, dt, bc, max_distance, origin, rng, max_types, stream=None, pair_pruning=0,
+              integrator=FORWARD_EULER):
         self.stream = stream
+        self.integrator = int(integrator)
         self.pair_pruning = pair_pruning
         self.dim = [float(d) for d in dim]
         self.origin = [float(o) for o in origin]
@@ -368,6 +371,7 @@ class _Universe:
         check(lib().mxg_engine_set_dt(self._e, self.dt, frac), "set_dt")
         check(lib().mxg_engine_set_rng_mode(self._e, 1 if self.rng == "philox" else 0), "set_rng_mode")
         check(lib().mxg_engine_set_pair_pruning(self._e, int(self.pair_pruning)), "set_pair_pruning")
+        check(lib().mxg_engine_set_integrator(self._e, int(self.integrator)), "set_integrator")
         for (o, d, c, b) in self._replicas:
             kind, vel, restore = parse_bc(b)
             check(lib().mxg_engine_add_replica(self._e, ptr(f64(o), ctypes.c_double), ptr(f64(d), ctypes.c_double),
@@ -639,12 +643,13 @@ def init(dim=(10.0, 10.0, 10.0), cutoff=1.0, cells=(4, 4, 4), dt=0.01, bc=None, 
     (dpd_eval.hpp:57); "philox" draws it from a counter-based stream.
     stream: optional CUDA stream handle (int) on which the engine runs.
     pair_pruning: 0 reproduces the reference's sorted-loop pruning (default),
-    2 evaluates every pair inside the cutoff (see mxg_engine_set_pair_pruning)."""
-    if integrator != FORWARD_EULER:
-        raise NotImplementedError("only the forward Euler integrator is on this path")
+    2 evaluates every pair inside the cutoff (see mxg_engine_set_pair_pruning).
+    integrator: FORWARD_EULER or RUNGE_KUTTA_4 (MxSimulator.cpp:218-230)."""
+    if integrator not in (FORWARD_EULER, RUNGE_KUTTA_4):
+        raise ValueError(f"invalid integrator kind: {integrator}")
     universe.close()
     universe._init(dim, cells, cutoff, dt, bc if bc is not None else boundary_conditions, max_distance, origin,
-                   rng, max_types, stream, pair_pruning)
+                   rng, max_types, stream, pair_pruning, integrator)
     return universe
 
 

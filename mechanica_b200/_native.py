@@ -102,6 +102,7 @@ _SIGS = {
                                ctypes.c_int),
     "mxg_engine_nr_replicas": ([_vp], ctypes.c_int),
     "mxg_engine_addpot_replica": ([_vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "mxg_engine_set_integrator": ([_vp, ctypes.c_int], ctypes.c_int),
     "mxg_engine_addpot_second": ([_vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "mxg_engine_pot_index": ([_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _c_int_p],
                              ctypes.c_int),

@@ -388,6 +388,8 @@ struct mxg_engine {
     double *d_partials = nullptr, *d_energy = nullptr;
     int energy_blocks = 64;
     bool has_dpd = false;
+    int integrator = 0;                 // 0 forward Euler, 1 Runge-Kutta 4 (engine.h EngineIntegrator)
+    float4 *d_rk[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // RK4 per-slot stage state
     int force_grid = 0;
     int num_sms = 148;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -565,6 +567,10 @@ struct mxg_engine {
      * received planes are added by the bond kernel or, without bonds, by the
      * integrator; the re-binning pass computes the new key bounds. */
     void enqueue_step(int b) {
+        if (integrator == 1) {
+            enqueue_step_rk4(b);
+            return;
+        }
         const int nb = 1 - b;
         const EngineView v = view(b);
         launch_force(v, has_dpd, force_grid, false, stream);
@@ -572,6 +578,31 @@ struct mxg_engine {
             launch_bonds(v, d_bonds, d_bond_flags, d_bond_off, d_bond_list, d_slot_of_id, d_ebond_slot, stream);
         launch_integrate(v, d_pos[b], d_vel[b], d_new_cell, d_in_count, d_in_list, d_out_count, bonds.empty(),
                          stream);
+        launch_scan(ncells, d_cell_count[b], d_out_count, d_in_count, d_cell_start[nb], d_cell_count[nb], d_step,
+                    stream);
+        launch_scatter(v, d_pos[b], d_vel[b], d_new_cell, d_cell_start[b], d_cell_count[b], d_in_count, d_in_list,
+                       d_out_count, d_cell_start[nb], d_pos[nb], d_vel[nb], d_cell_of[nb], d_slot_of_id, stream);
+    }
+
+    /* One Runge-Kutta 4 step (engine_advance_runge_kutta_4): four force passes (with
+     * bonds when present), stage updates in the step's cell frame with fresh key
+     * bounds before each intermediate pass, then the final update, re-binning as
+     * for Euler. */
+    void enqueue_step_rk4(int b) {
+        const int nb = 1 - b;
+        const EngineView v = view(b);
+        for (int stage = 0; stage < 4; ++stage) {
+            launch_force(v, has_dpd, force_grid, false, stream);
+            if (!bonds.empty())
+                launch_bonds(v, d_bonds, d_bond_flags, d_bond_off, d_bond_list, d_slot_of_id, d_ebond_slot, stream);
+            if (stage < 3) {
+                launch_rk_stage(v, d_pos[b], d_rk, stage, bonds.empty(), stream);
+                launch_sort_bounds(v, stream);
+            } else {
+                launch_rk_final(v, d_pos[b], d_vel[b], d_rk, d_new_cell, d_in_count, d_in_list, d_out_count,
+                                bonds.empty(), stream);
+            }
+        }
         launch_scan(ncells, d_cell_count[b], d_out_count, d_in_count, d_cell_start[nb], d_cell_count[nb], d_step,
                     stream);
         launch_scatter(v, d_pos[b], d_vel[b], d_new_cell, d_cell_start[b], d_cell_count[b], d_in_count, d_in_list,
@@ -830,6 +861,8 @@ int mxg_engine::start(cudaStream_t st) {
         rc |= alloc(&d_cell_count[b], ncells);
     }
     rc |= alloc(&d_force, nparts);
+    if (integrator == 1)
+        for (int k = 0; k < 5; ++k) rc |= alloc(&d_rk[k], nparts);
     rc |= alloc(&d_new_cell, nparts);
     rc |= alloc(&d_in_count, ncells);
     rc |= alloc(&d_out_count, ncells);
@@ -1164,6 +1197,14 @@ int mxg_potential_param_table(const mxg_potential *p, int k, mxg_potential **out
         return MXG_ERR_ARG;
     }
     *out = q;
+    return MXG_OK;
+}
+
+int mxg_engine_set_integrator(mxg_engine *e, int kind) {
+    if (!e) return MXG_ERR_NULL;
+    if (kind != 0 && kind != 1) return MXG_ERR_ARG;
+    if (e->started) return MXG_ERR_STATE;
+    e->integrator = kind;
     return MXG_OK;
 }
 

@@ -722,6 +722,34 @@ __global__ void bond_kernel(EngineView v, const DevBond *__restrict__ bonds, uns
 /* space_shuffle_local's rule (space.cpp:352-371): delta = (x >= h) - (x < 0). */
 __device__ __forceinline__ int cell_delta(float x, float h) { return (x >= h ? 1 : 0) - (x < 0.0f ? 1 : 0); }
 
+/* The move of a particle that left cell c by delta (engine_advance.cpp:204-211):
+ * x -= delta*h and the destination by the periodic wrap; then the next force
+ * pass's shuffle rule (space.cpp:333-393) once more. Returns the destination. */
+__device__ __forceinline__ int relocate(const DevSpace &S, int c, float *xv, int *delta) {
+    const int l = c - S.cell_offset;
+    int loc[3] = {l / (S.cdim[1] * S.cdim[2]), (l / S.cdim[2]) % S.cdim[1], l % S.cdim[2]};
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int k = 0; k < 3; ++k) {
+            xv[k] = __fsub_rn(xv[k], __fmul_rn((float)delta[k], S.h[k]));
+            loc[k] = (loc[k] + delta[k] + S.cdim[k]) % S.cdim[k];
+        }
+        for (int k = 0; k < 3; ++k) delta[k] = cell_delta(xv[k], S.h[k]);
+        if (!(delta[0] | delta[1] | delta[2])) break;
+    }
+    return S.cell_offset + (loc[0] * S.cdim[1] + loc[1]) * S.cdim[2] + loc[2];
+}
+
+/* Appends a particle that moved from cell c to dest to dest's bucket. */
+__device__ __forceinline__ void bucket_move(const EngineView &v, int s, int c, int dest, int *in_count, int *in_list,
+                                            int *out_count) {
+    const int k = atomicAdd(&in_count[dest], 1);
+    if (k < kBucket)
+        in_list[dest * kBucket + k] = s;
+    else
+        atomicOr(v.status, kStatusBucketOverflow);
+    atomicAdd(&out_count[c], 1);
+}
+
 /*
  * Forward Euler for one particle (engine_advance.cpp:126-239): velocity update
  * in FP64 rounded to FP32, per-component speed (or step) clamp, position update,
@@ -806,20 +834,7 @@ __global__ void integrate_kernel(EngineView v, float4 *pos, float4 *vel, int *ne
             }
             if (enforced)
                 for (int k = 0; k < 3; ++k) delta[k] = cell_delta(xv[k], S.h[k]);
-            if (delta[0] | delta[1] | delta[2]) {
-                const int l = c - S.cell_offset;
-                int loc[3] = {l / (S.cdim[1] * S.cdim[2]), (l / S.cdim[2]) % S.cdim[1], l % S.cdim[2]};
-                for (int pass = 0; pass < 2; ++pass) {
-                    for (int k = 0; k < 3; ++k) {
-                        xv[k] = __fsub_rn(xv[k], __fmul_rn((float)delta[k], S.h[k]));
-                        loc[k] = (loc[k] + delta[k] + S.cdim[k]) % S.cdim[k];
-                    }
-                    // the next force pass's shuffle (space.cpp:333-393) on the moved particle
-                    for (int k = 0; k < 3; ++k) delta[k] = cell_delta(xv[k], S.h[k]);
-                    if (!(delta[0] | delta[1] | delta[2])) break;
-                }
-                dest = S.cell_offset + (loc[0] * S.cdim[1] + loc[1]) * S.cdim[2] + loc[2];
-            }
+            if (delta[0] | delta[1] | delta[2]) dest = relocate(S, c, xv, delta);
         }
         x.x = xv[0]; x.y = xv[1]; x.z = xv[2];
         u.x = vv[0]; u.y = vv[1]; u.z = vv[2];
@@ -827,14 +842,110 @@ __global__ void integrate_kernel(EngineView v, float4 *pos, float4 *vel, int *ne
         vel[s] = u;
     }
     new_cell[s] = dest;
-    if (dest != c) {
-        const int k = atomicAdd(&in_count[dest], 1);
-        if (k < kBucket)
-            in_list[dest * kBucket + k] = s;
-        else
-            atomicOr(v.status, kStatusBucketOverflow);
-        atomicAdd(&out_count[c], 1);
+    if (dest != c) bucket_move(v, s, c, dest, in_count, in_list, out_count);
+}
+
+/*
+ * Runge-Kutta 4 (engine_advance_runge_kutta_4, engine_advance.cpp:443-698), in
+ * the reference's FP32 expression order: the force of stage k gives
+ * vk = f imass and xk (v0, v0 + dt/2 vk_{k-1}, ..., or f imass when
+ * overdamped); the weighted sums xk0 + 2 xk1 + 2 xk2 + xk3 (and vk) accumulate
+ * in that order. Stage positions p0 + dt/2 xk (p0 + dt xk2 for the last) stay
+ * in the step's starting cell, whose frame p0 belongs to. (The reference's
+ * engine_force re-bins between stages and leaves p0 in the old cell's frame,
+ * so there a particle that crosses a face mid-step lands a cell edge away;
+ * here the stages keep one frame.) Velocities change only at the end; like
+ * the reference, no speed clamp, no frozen mask and no wall reflection.
+ */
+struct RkState {
+    float4 *p0, *v0;       // step start
+    float4 *accx, *accv;   // weighted sums of the stages so far
+    float4 *vkp;           // previous stage's vk
+};
+
+__global__ void rk_stage_kernel(EngineView v, float4 *pos, RkState rk, int stage, bool add_planes) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= v.nparts) return;
+    const DevSpace &S = v.spaces[v.cell_rep[v.cell_of[s]]];
+    const float4 x = pos[s];
+    const float4 f = add_planes ? total_force(v, s) : v.force[s];
+    if (add_planes) v.force[s] = f;
+    const DevType &T = v.types[__float_as_int(x.w)];
+    const float imf = (float)T.imass;
+    const float dtf = S.dt;
+    const float hdt = (float)(0.5 * (double)dtf);
+    const bool newton = T.dynamics == 0;
+    float4 p0, v0, vkp = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (stage == 0) {
+        p0 = x;
+        v0 = v.vel[s];
+        rk.p0[s] = p0;
+        rk.v0[s] = v0;
+    } else {
+        p0 = rk.p0[s];
+        v0 = rk.v0[s];
+        vkp = rk.vkp[s];
     }
+    const float fv[3] = {f.x, f.y, f.z}, pv[3] = {p0.x, p0.y, p0.z}, vv[3] = {v0.x, v0.y, v0.z};
+    const float kv[3] = {vkp.x, vkp.y, vkp.z};
+    float vk[3], xk[3], nx[3];
+    bool toofast = false;
+    const float4 ax = stage ? rk.accx[s] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 av = stage ? rk.accv[s] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float axv[3] = {ax.x, ax.y, ax.z}, avv[3] = {av.x, av.y, av.z};
+    float nax[3], nav[3];
+    const float step = stage == 2 ? dtf : hdt;
+    for (int k = 0; k < 3; ++k) {
+        vk[k] = __fmul_rn(fv[k], imf);
+        xk[k] = newton ? (stage == 0 ? vv[k] : __fadd_rn(vv[k], __fmul_rn(hdt, kv[k]))) : vk[k];
+        nax[k] = stage == 0 ? xk[k] : __fadd_rn(axv[k], __fmul_rn(2.0f, xk[k]));
+        nav[k] = stage == 0 ? vk[k] : __fadd_rn(avv[k], __fmul_rn(2.0f, vk[k]));
+        nx[k] = __fadd_rn(pv[k], __fmul_rn(step, xk[k]));
+        toofast = toofast || nx[k] >= S.h2[k] || nx[k] <= -S.h[k];  // CHECK_TOOFAST (:424-431)
+    }
+    if (toofast) atomicOr(v.status, kStatusTooFast);
+    rk.accx[s] = make_float4(nax[0], nax[1], nax[2], 0.f);
+    rk.accv[s] = make_float4(nav[0], nav[1], nav[2], 0.f);
+    rk.vkp[s] = make_float4(vk[0], vk[1], vk[2], 0.f);
+    pos[s] = make_float4(nx[0], nx[1], nx[2], x.w);
+}
+
+__global__ void rk_final_kernel(EngineView v, float4 *pos, float4 *vel, RkState rk, int *new_cell, int *in_count,
+                                int *in_list, int *out_count, bool add_planes) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= v.nparts) return;
+    const int c = v.cell_of[s];
+    const DevSpace &S = v.spaces[v.cell_rep[c]];
+    const float4 f = add_planes ? total_force(v, s) : v.force[s];
+    if (add_planes) v.force[s] = f;
+    const float4 x = pos[s];
+    const DevType &T = v.types[__float_as_int(x.w)];
+    const float imf = (float)T.imass;
+    const float dtf = S.dt;
+    const float sixth = (float)((double)dtf / 6.);
+    const bool newton = T.dynamics == 0;
+    const float4 p0 = rk.p0[s], v0 = rk.v0[s], vkp = rk.vkp[s], ax = rk.accx[s], av = rk.accv[s];
+    const float fv[3] = {f.x, f.y, f.z}, pv[3] = {p0.x, p0.y, p0.z}, vv[3] = {v0.x, v0.y, v0.z};
+    const float kv[3] = {vkp.x, vkp.y, vkp.z}, axv[3] = {ax.x, ax.y, ax.z}, avv[3] = {av.x, av.y, av.z};
+    float xv[3], nv[3] = {vv[0], vv[1], vv[2]};
+    bool toofast = false;
+    int delta[3];
+    for (int k = 0; k < 3; ++k) {
+        const float vk = __fmul_rn(imf, fv[k]);
+        const float xk = newton ? __fadd_rn(vv[k], __fmul_rn(dtf, kv[k])) : vk;
+        if (newton) nv[k] = __fadd_rn(vv[k], __fmul_rn(sixth, __fadd_rn(avv[k], vk)));
+        xv[k] = __fadd_rn(pv[k], __fmul_rn(sixth, __fadd_rn(axv[k], xk)));
+        delta[k] = cell_delta(xv[k], S.h[k]);
+        toofast = toofast || xv[k] >= S.h2[k] || xv[k] <= -S.h[k];
+    }
+    if (toofast) atomicOr(v.status, kStatusTooFast);
+    if (!(isfinite(xv[0]) && isfinite(xv[1]) && isfinite(xv[2]))) atomicOr(v.status, kStatusNonFinite);
+    int dest = c;
+    if (delta[0] | delta[1] | delta[2]) dest = relocate(S, c, xv, delta);
+    pos[s] = make_float4(xv[0], xv[1], xv[2], x.w);
+    vel[s] = make_float4(nv[0], nv[1], nv[2], v0.w);
+    new_cell[s] = dest;
+    if (dest != c) bucket_move(v, s, c, dest, in_count, in_list, out_count);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1088,6 +1199,19 @@ void launch_integrate(const EngineView &v, float4 *pos, float4 *vel, int *new_ce
     const int tb = 256;
     integrate_kernel<<<(v.nparts + tb - 1) / tb, tb, 0, st>>>(v, pos, vel, new_cell, in_count, in_list, out_count,
                                                              add_planes);
+}
+
+void launch_rk_stage(const EngineView &v, float4 *pos, float4 *const *rk, int stage, bool add_planes,
+                     cudaStream_t st) {
+    const RkState r{rk[0], rk[1], rk[2], rk[3], rk[4]};
+    rk_stage_kernel<<<(v.nparts + 255) / 256, 256, 0, st>>>(v, pos, r, stage, add_planes);
+}
+
+void launch_rk_final(const EngineView &v, float4 *pos, float4 *vel, float4 *const *rk, int *new_cell, int *in_count,
+                     int *in_list, int *out_count, bool add_planes, cudaStream_t st) {
+    const RkState r{rk[0], rk[1], rk[2], rk[3], rk[4]};
+    rk_final_kernel<<<(v.nparts + 255) / 256, 256, 0, st>>>(v, pos, vel, r, new_cell, in_count, in_list, out_count,
+                                                           add_planes);
 }
 
 void launch_scan(int ncells, const int *old_count, const int *out_count, const int *in_count, int *new_start,

@@ -13,6 +13,11 @@ void launch_bonds(const EngineView &v, const DevBond *bonds, unsigned *bond_flag
                   const int *bond_list, const int *slot_of_id, double *ebond_slot, cudaStream_t st);
 void launch_integrate(const EngineView &v, float4 *pos, float4 *vel, int *new_cell, int *in_count, int *in_list,
                       int *out_count, bool add_planes, cudaStream_t st);
+/* Runge-Kutta 4: rk[5] = p0, v0, accx, accv, vk of the previous stage (per slot). */
+void launch_rk_stage(const EngineView &v, float4 *pos, float4 *const *rk, int stage, bool add_planes,
+                     cudaStream_t st);
+void launch_rk_final(const EngineView &v, float4 *pos, float4 *vel, float4 *const *rk, int *new_cell, int *in_count,
+                     int *in_list, int *out_count, bool add_planes, cudaStream_t st);
 void launch_scan(int ncells, const int *old_count, const int *out_count, const int *in_count, int *new_start,
                  int *new_count, unsigned long long *step, cudaStream_t st);
 void launch_scatter(const EngineView &v, const float4 *pos, const float4 *vel, const int *new_cell,

@@ -154,7 +154,7 @@ def build_gpu(scn, rng_mode="reference"):
     """Builds the scenario in the B200 engine through the Python surface."""
     bc = {"x": scn["bc"][0], "y": scn["bc"][1], "z": scn["bc"][2]}
     m.init(dim=scn["dim"], cells=scn["cells"], cutoff=scn["cutoff"], dt=scn["dt"], bc=bc, rng=rng_mode,
-           max_distance=scn.get("max_distance"))
+           max_distance=scn.get("max_distance"), integrator=scn.get("integrator", m.FORWARD_EULER))
     types = []
     for k, (mass, radius, dyn) in enumerate(scn["types"]):
         types.append(type(f"T{k}", (m.Particle,), {"mass": mass, "radius": radius, "dynamics": dyn}))

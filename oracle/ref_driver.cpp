@@ -215,6 +215,13 @@ int mxref_step(int nsteps) {
 
 int mxref_force(void) { return engine_force(&_Engine); }
 
+/* EngineIntegrator (engine.h): 0 forward Euler, 1 Runge-Kutta 4, as universe_init sets it
+ * from the integrator keyword (src/MxSimulator.cpp:218-230,380). */
+int mxref_set_integrator(int kind) {
+    _Engine.integrator = kind == 1 ? EngineIntegrator::RUNGE_KUTTA_4 : EngineIntegrator::FORWARD_EULER;
+    return 0;
+}
+
 int mxref_nr_parts(void) { return _Engine.s.nr_parts; }
 
 /* Per-id state: cell-relative position, absolute position (double), velocity,

@@ -14,7 +14,8 @@ A scenario is a dict:
     pots [(kind, params, ti, tj)] with kind in lj126/morse/harmonic/power/dpd,
     forces [(type, fx, fy, fz)], x (N,3) float64, v (N,3), t (N,) int,
     bonds (optional): bi, bj, bond_pot (kind, params), dissociation,
-    action: "force" | "steps", nsteps, runners (threads), time_it (bool)
+    action: "force" | "steps", nsteps, runners (threads), time_it (bool),
+    integrator (0 forward Euler, 1 Runge-Kutta 4)
 Results: xabs, xrel, v, f, cell (per id), tasks (rows type, sid, i, j),
     cdim, h, epot, ekin, bond_flags, seconds (wall time of the steps).
 """
@@ -108,6 +109,8 @@ def _execute(scn):
                       float(scn.get("max_distance", -1.0)), 64)
     if rc != 0:
         raise RuntimeError(f"mxref_init {rc}")
+    if scn.get("integrator", 0):
+        L.mxref_set_integrator(int(scn["integrator"]))
     for (m, r, d) in scn["types"]:
         L.mxref_add_type(float(m), float(r), int(d))
 
