@@ -177,6 +177,20 @@ int mxg_engine_set_dt(mxg_engine *e, double dt, double max_dist_fraction);
 int mxg_engine_addtype(mxg_engine *e, double mass, double radius, int dynamics, unsigned particle_flags);
 int mxg_engine_addpot(mxg_engine *e, const mxg_potential *p, int type_i, int type_j);
 int mxg_engine_add_singlebody_force(mxg_engine *e, int type, float fx, float fy, float fz);
+/* The other single-body forces of the forces module (engine_add_singlebody_force, engine.cpp:983-1003,
+ * with the forces of src/mdcore/src/MxForce.cpp:308-419); like the reference, a type keeps one.
+ *   kind 2, Berendsen thermostat (berenderson_tstat): params {tau}; f += (1/tau)(T0/KE_type - 1) v with
+ *          KE_type the type's summed kinetic energy (see mxg_engine_set_target_temperature for T0);
+ *   kind 3, random (random): params {mean, std, duration}; a persistent force N(mean, std) in a uniformly
+ *          random direction, redrawn every ceil(duration/dt) steps (when time + id is a multiple);
+ *   kind 4, friction (friction): params {coef, mean, std, duration}; f += -coef |v|^2 v + a persistent
+ *          random force as for kind 3.
+ * The random draws come from a Philox stream keyed on (time, particle id) instead of the reference's
+ * global mt19937. */
+int mxg_engine_add_singlebody_force_kind(mxg_engine *e, int type, int kind, const float *params);
+/* The type's target temperature (MxParticle.cpp:543-560), which the Berendsen force compares with the
+ * type's summed kinetic energy. */
+int mxg_engine_set_target_temperature(mxg_engine *e, int type, double temperature);
 /* Adds n particles (positions double[3n] in global coordinates, velocities float[3n]); ids_out
  * receives consecutive ids (may be NULL). */
 int mxg_engine_addparts(mxg_engine *e, int n, const double *x, const float *v, const int *type, int *ids_out);

@@ -250,8 +250,39 @@ class _ConstantForce:
         self.value = np.asarray(value, dtype=np.float32).reshape(3)
 
 
+class _SingleBodyForce:
+    """The forces module's other one-body forces (MxForce.cpp:213-259); kind and
+    params as mxg_engine_add_singlebody_force_kind takes them."""
+
+    def __init__(self, kind, params):
+        self.kind = kind
+        self.params = np.asarray(list(params) + [0.0] * (4 - len(params)), dtype=np.float32)
+
+
+def _berenderson_tstat(tau):
+    """Berendsen thermostat force (1/tau)(T0/KE_type - 1) v with T0 the type's target_temperature."""
+    return _SingleBodyForce(2, [tau])
+
+
+def _random(std, mean, durration=0.01):
+    """A persistent random force in a random direction, redrawn every durration.
+    As in the reference, the module passes (std, mean) into parameters declared
+    (mean, std) (MxForce.cpp:18,226-233), so the magnitude is drawn from a normal
+    distribution with mean `std` and standard deviation `mean`."""
+    return _SingleBodyForce(3, [std, mean, durration])
+
+
+def _friction(coef, std=0.0, mean=0.0, durration=0.01):
+    """-coef |v|^2 v plus a persistent random force as for random(), with the
+    reference's same (std, mean) exchange (MxForce.cpp:19,239-247)."""
+    return _SingleBodyForce(4, [coef, std, mean, durration])
+
+
 class forces:  # noqa: N801 - namespace mirroring m.forces
     ConstantForce = _ConstantForce
+    berenderson_tstat = staticmethod(_berenderson_tstat)
+    random = staticmethod(_random)
+    friction = staticmethod(_friction)
 
 
 class Bond:
@@ -343,7 +374,8 @@ class _Universe:
         self._types = []        # (mass, radius, dynamics, flags)
         self._pots = []         # (potential, ti, tj, replica)
         self._replicas = []     # extra boxes: (origin, dim, cells, bc)
-        self._forces = []       # (type, value)
+        self._forces = []       # (type, force object), one per type
+        self._targets = {}      # type -> target temperature
         self._bonds = []        # (potential, i[], j[], dissociation)
         self._x = np.zeros((0, 3))
         self._v = np.zeros((0, 3), dtype=np.float32)
@@ -385,9 +417,16 @@ class _Universe:
                 check(lib().mxg_engine_addpot_replica(self._e, rep, p._h, a, b), "addpot")
             else:
                 check(lib().mxg_engine_addpot_second(self._e, rep, p._h, a, b), "addpot_second")
-        for (t, v) in self._forces:
-            check(lib().mxg_engine_add_singlebody_force(self._e, t, float(v[0]), float(v[1]), float(v[2])),
-                  "add_singlebody_force")
+        for (t, f) in self._forces:
+            if isinstance(f, _SingleBodyForce):
+                check(lib().mxg_engine_add_singlebody_force_kind(self._e, t, f.kind, ptr(f.params, ctypes.c_float)),
+                      "add_singlebody_force")
+            else:
+                v = f.value
+                check(lib().mxg_engine_add_singlebody_force(self._e, t, float(v[0]), float(v[1]), float(v[2])),
+                      "add_singlebody_force")
+        for t, temp in self._targets.items():
+            check(lib().mxg_engine_set_target_temperature(self._e, t, float(temp)), "set_target_temperature")
         for (p, ii, jj, d) in self._bonds:
             check(lib().mxg_engine_addbonds(self._e, len(ii), ptr(ii, ctypes.c_int), ptr(jj, ctypes.c_int), p._h, d,
                                             None), "addbonds")
@@ -401,6 +440,12 @@ class _Universe:
         if tid is None:
             self._dirty = True
             tid = len(self._types) - 1
+        if getattr(cls, "target_temperature", None) is not None:
+            self._targets[tid] = float(cls.target_temperature)
+            if self._started:
+                self._dirty = True
+            else:
+                check(lib().mxg_engine_set_target_temperature(self._e, tid, self._targets[tid]), "target_temperature")
         return tid
 
     def _add_particles(self, x, v, t, replica=0):
@@ -439,9 +484,10 @@ class _Universe:
             for which, p in enumerate(terms):
                 self._pots.append((p, ta, tb, int(replica), which))
             self._dirty = True
-        elif isinstance(obj, _ConstantForce):
+        elif isinstance(obj, (_ConstantForce, _SingleBodyForce)):
             self._sync_state()
-            self._forces.append((ta, obj.value))
+            self._forces = [(t, f) for (t, f) in self._forces if t != ta]  # one single-body force per type
+            self._forces.append((ta, obj))
             self._dirty = True
         else:
             raise TypeError("bind expects a Potential or a force")

@@ -103,6 +103,8 @@ _SIGS = {
     "mxg_engine_nr_replicas": ([_vp], ctypes.c_int),
     "mxg_engine_addpot_replica": ([_vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "mxg_engine_set_integrator": ([_vp, ctypes.c_int], ctypes.c_int),
+    "mxg_engine_add_singlebody_force_kind": ([_vp, ctypes.c_int, ctypes.c_int, _c_float_p], ctypes.c_int),
+    "mxg_engine_set_target_temperature": ([_vp, ctypes.c_int, ctypes.c_double], ctypes.c_int),
     "mxg_engine_addpot_second": ([_vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "mxg_engine_pot_index": ([_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _c_int_p],
                              ctypes.c_int),

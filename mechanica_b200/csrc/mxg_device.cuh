@@ -70,6 +70,11 @@ struct DevType {
     float fx, fy, fz;    // constant body force
     int has_force;
     int pad;
+    // other single-body force (MxForce.cpp:308-419): 0 none, 2 Berendsen, 3 random, 4 friction
+    int sb_kind;
+    int sb_steps;        // random/friction: redraw interval in steps, ceil(duration / dt)
+    float sb_a, sb_b, sb_c, sb_pad;  // Berendsen: 1/tau; random: mean, std; friction: coef, mean, std
+    double target;       // Berendsen: the type's target temperature
 };
 
 struct DevSpace {        // one per replica
@@ -134,6 +139,9 @@ struct EngineView {      // everything a kernel needs, passed by value
     unsigned *status;
     unsigned long long *pair_stats;  // non-null only for the statistics launch
     double *virial_partials;         // non-null only for the virial launch: [warp][6]
+    int has_sb;                      // some type has a Berendsen, random or friction force
+    const double *type_ke;           // per type: summed kinetic energy of the state (Berendsen)
+    const float4 *persist;           // per particle id: persistent random force (random, friction)
     const int *nb_rev;       // FIRST entries: the pair's plane in the neighbour's received sums
     const int *sec_count;    // per cell: SECOND entries, i.e. planes of received sums
     const int *cell_planes;  // per cell: received planes plus own-side planes of its later work items

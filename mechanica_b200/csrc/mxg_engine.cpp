@@ -80,6 +80,9 @@ struct TypeInfo {
     unsigned flags;
     float force[3];
     bool has_force;
+    int sb_kind = 0;            // 2 Berendsen, 3 random, 4 friction (the type's one single-body force)
+    float sb[4] = {0, 0, 0, 0};  // Berendsen: tau; random: mean, std, duration; friction: coef, mean, std, duration
+    double target = 0.0;        // target temperature (Berendsen)
 };
 
 struct BondInfo {
@@ -388,7 +391,11 @@ struct mxg_engine {
     double *d_partials = nullptr, *d_energy = nullptr;
     int energy_blocks = 64;
     bool has_dpd = false;
+    bool has_sb = false;                // a type has a Berendsen, random or friction force
+    double *d_type_ke = nullptr;
+    float4 *d_persist = nullptr;
     int integrator = 0;                 // 0 forward Euler, 1 Runge-Kutta 4 (engine.h EngineIntegrator)
+    int force_layout = 0;               // the buffer whose slot order the force array follows
     float4 *d_rk[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // RK4 per-slot stage state
     int force_grid = 0;
     int num_sms = 148;
@@ -545,6 +552,9 @@ struct mxg_engine {
         v.status = d_status;
         v.pair_stats = nullptr;
         v.virial_partials = nullptr;
+        v.has_sb = has_sb ? 1 : 0;
+        v.type_ke = d_type_ke;
+        v.persist = d_persist;
         v.nb_rev = d_nb_rev;
         v.sec_count = d_sec_count;
         v.cell_planes = d_cell_planes;
@@ -557,7 +567,9 @@ struct mxg_engine {
     /* The force pass alone (engine_force): the bond kernel, or the combine
      * kernel when there are no bonds, adds the received planes. */
     void enqueue_force(int b) {
+        force_layout = b;
         const EngineView v = view(b);
+        if (has_sb) launch_singlebody_prep(v, ntypes, d_type_ke, d_persist, false, stream);
         launch_force(v, has_dpd, force_grid, bonds.empty(), stream);
         if (!bonds.empty())
             launch_bonds(v, d_bonds, d_bond_flags, d_bond_off, d_bond_list, d_slot_of_id, d_ebond_slot, stream);
@@ -573,6 +585,7 @@ struct mxg_engine {
         }
         const int nb = 1 - b;
         const EngineView v = view(b);
+        if (has_sb) launch_singlebody_prep(v, ntypes, d_type_ke, d_persist, true, stream);
         launch_force(v, has_dpd, force_grid, false, stream);
         if (!bonds.empty())
             launch_bonds(v, d_bonds, d_bond_flags, d_bond_off, d_bond_list, d_slot_of_id, d_ebond_slot, stream);
@@ -592,6 +605,8 @@ struct mxg_engine {
         const int nb = 1 - b;
         const EngineView v = view(b);
         for (int stage = 0; stage < 4; ++stage) {
+            // persistent random forces are redrawn in the first stage only (INTEGRATOR_UPDATE_PERSISTENTFORCE)
+            if (has_sb) launch_singlebody_prep(v, ntypes, d_type_ke, d_persist, stage == 0, stream);
             launch_force(v, has_dpd, force_grid, false, stream);
             if (!bonds.empty())
                 launch_bonds(v, d_bonds, d_bond_flags, d_bond_off, d_bond_list, d_slot_of_id, d_ebond_slot, stream);
@@ -805,6 +820,7 @@ int mxg_engine::start(cudaStream_t st) {
             }
         hs.push_back(space_desc(r, r * tt));
     }
+    has_sb = false;
     std::vector<DevType> ht(ntypes);
     for (int a = 0; a < (int)types.size(); ++a) {
         DevType &d = ht[a];
@@ -818,6 +834,19 @@ int mxg_engine::start(cudaStream_t st) {
         d.fy = types[a].force[1];
         d.fz = types[a].force[2];
         d.has_force = types[a].has_force ? 1 : 0;
+        const TypeInfo &ti = types[a];
+        d.sb_kind = ti.sb_kind;
+        d.target = ti.target;
+        if (ti.sb_kind == 2) {
+            d.sb_a = 1 / ti.sb[0];  // berenderson_create keeps 1/tau (MxForce.cpp:388-395)
+        } else if (ti.sb_kind == 3 || ti.sb_kind == 4) {
+            d.sb_a = ti.sb[0];
+            d.sb_b = ti.sb[1];
+            d.sb_c = ti.sb[2];
+            const float dur = ti.sb_kind == 3 ? ti.sb[2] : ti.sb[3];
+            d.sb_steps = std::max(1, (int)std::ceil(dur / dt));  // durration_steps (MxForce.cpp:403,417)
+        }
+        if (ti.sb_kind) has_sb = true;
     }
     std::vector<SortAxes> haxes(1);
     for (int q = 0; q < 13; ++q)
@@ -883,6 +912,8 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_pot_idx, hpidx.size());
     rc |= alloc(&d_pot_idx2, hpidx2.size());
     rc |= alloc(&d_types, ht.size());
+    rc |= alloc(&d_type_ke, ht.size());
+    rc |= alloc(&d_persist, (size_t)nparts);
     rc |= alloc(&d_spaces, hs.size());
     rc |= alloc(&d_axes, 1);
     rc |= alloc(&d_sort_bounds, (size_t)ncells * 13);
@@ -905,6 +936,8 @@ int mxg_engine::start(cudaStream_t st) {
     CUDA_TRY(cudaMemsetAsync(d_epot_cell, 0, sizeof(double) * std::max(1, nitems), stream));
     CUDA_TRY(cudaMemsetAsync(d_ebond_slot, 0, sizeof(double) * std::max(1, nparts), stream));
     CUDA_TRY(cudaMemsetAsync(d_force, 0, sizeof(float4) * std::max(1, nparts), stream));
+    CUDA_TRY(cudaMemsetAsync(d_persist, 0, sizeof(float4) * std::max(1, nparts), stream));
+    CUDA_TRY(cudaMemsetAsync(d_type_ke, 0, sizeof(double) * ht.size(), stream));
     if ((rc = upload(d_pos[0], hpos, stream)) || (rc = upload(d_vel[0], hvel, stream)) ||
         (rc = upload(d_cell_of[0], hcell_of, stream)) || (rc = upload(d_cell_start[0], hstart, stream)) ||
         (rc = upload(d_cell_count[0], hcount, stream)) || (rc = upload(d_slot_of_id, hslot, stream)) ||
@@ -1200,6 +1233,27 @@ int mxg_potential_param_table(const mxg_potential *p, int k, mxg_potential **out
     return MXG_OK;
 }
 
+int mxg_engine_add_singlebody_force_kind(mxg_engine *e, int type, int kind, const float *params) {
+    if (!e || !params) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    if (type < 0 || type >= (int)e->types.size()) return MXG_ERR_RANGE;
+    if (kind < 2 || kind > 4) return MXG_ERR_ARG;
+    if (kind == 2 && !(params[0] != 0.f)) return MXG_ERR_ARG;
+    TypeInfo &t = e->types[type];
+    t.has_force = false;  // engine_add_singlebody_force keeps one force per type
+    t.sb_kind = kind;
+    for (int k = 0; k < 4; ++k) t.sb[k] = params[k];
+    return MXG_OK;
+}
+
+int mxg_engine_set_target_temperature(mxg_engine *e, int type, double temperature) {
+    if (!e) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    if (type < 0 || type >= (int)e->types.size()) return MXG_ERR_RANGE;
+    e->types[type].target = temperature;
+    return MXG_OK;
+}
+
 int mxg_engine_set_integrator(mxg_engine *e, int kind) {
     if (!e) return MXG_ERR_NULL;
     if (kind != 0 && kind != 1) return MXG_ERR_ARG;
@@ -1253,6 +1307,7 @@ int mxg_engine_add_singlebody_force(mxg_engine *e, int type, float fx, float fy,
     if (e->started) return MXG_ERR_STATE;
     if (type < 0 || type >= (int)e->types.size()) return MXG_ERR_RANGE;
     TypeInfo &t = e->types[type];
+    t.sb_kind = 0;  // one single-body force per type
     t.force[0] = fx;
     t.force[1] = fy;
     t.force[2] = fz;
@@ -1323,6 +1378,7 @@ int mxg_engine_step(mxg_engine *e, int nsteps) {
             CUDA_TRY(cudaGetLastError());
         }
         e->cur = 1 - e->cur;
+        e->force_layout = 1 - e->cur;
     }
     return MXG_OK;
 }
@@ -1363,13 +1419,25 @@ int mxg_engine_unload(mxg_engine *e, int n, double *x, float *v, float *f, int *
     if (!e->started) return MXG_ERR_STATE;
     if (n > e->nparts) return MXG_ERR_RANGE;
     const int N = e->nparts;
-    std::vector<float4> hp(N), hv(N), hf(N);
+    std::vector<float4> hp(N), hv(N), hf(N), hfv(N);
     std::vector<int> hc(N);
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     CUDA_TRY(cudaMemcpy(hp.data(), e->d_pos[e->cur], sizeof(float4) * N, cudaMemcpyDeviceToHost));
     CUDA_TRY(cudaMemcpy(hv.data(), e->d_vel[e->cur], sizeof(float4) * N, cudaMemcpyDeviceToHost));
     CUDA_TRY(cudaMemcpy(hf.data(), e->d_force, sizeof(float4) * N, cudaMemcpyDeviceToHost));
     CUDA_TRY(cudaMemcpy(hc.data(), e->d_cell_of[e->cur], sizeof(int) * N, cudaMemcpyDeviceToHost));
+    // after a step the forces are in the slot order of the step's starting buffer, whose
+    // velocity array still carries the ids in that order
+    CUDA_TRY(cudaMemcpy(hfv.data(), e->d_vel[e->force_layout], sizeof(float4) * N, cudaMemcpyDeviceToHost));
+    if (f)
+        for (int s = 0; s < N; ++s) {
+            int id;
+            memcpy(&id, &hfv[s].w, 4);
+            if (id < 0 || id >= n) continue;
+            f[3 * (size_t)id] = hf[s].x;
+            f[3 * (size_t)id + 1] = hf[s].y;
+            f[3 * (size_t)id + 2] = hf[s].z;
+        }
     for (int s = 0; s < N; ++s) {
         int id;
         memcpy(&id, &hv[s].w, 4);
@@ -1386,11 +1454,6 @@ int mxg_engine_unload(mxg_engine *e, int n, double *x, float *v, float *f, int *
             v[3 * (size_t)id] = hv[s].x;
             v[3 * (size_t)id + 1] = hv[s].y;
             v[3 * (size_t)id + 2] = hv[s].z;
-        }
-        if (f) {
-            f[3 * (size_t)id] = hf[s].x;
-            f[3 * (size_t)id + 1] = hf[s].y;
-            f[3 * (size_t)id + 2] = hf[s].z;
         }
         if (cell) cell[id] = c;
     }
@@ -1571,7 +1634,7 @@ int mxg_engine_adjoint_params(mxg_engine *e, int n, const int *pot, const int *p
 int mxg_engine_vjp_step(mxg_engine *e, void *lam_x, void *lam_v, double *grad) {
     if (!e || !lam_x || !lam_v || !grad) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
-    if (!e->bonds.empty()) return MXG_ERR_ARG;  // bonded forces are not differentiated
+    if (!e->bonds.empty() || e->has_sb) return MXG_ERR_ARG;  // bonds and single-body forces are not differentiated
     if (e->nparts == 0) return MXG_OK;
     if (e->adjoint_stale) {
         const int rc = e->build_adjoint();
@@ -1579,6 +1642,7 @@ int mxg_engine_vjp_step(mxg_engine *e, void *lam_x, void *lam_v, double *grad) {
     }
     const EngineView v = e->view(e->cur);
     launch_force(v, e->has_dpd, e->force_grid, true, e->stream);  // forces of the step's state
+    e->force_layout = e->cur;
     AdjointView a;
     a.lam_x = static_cast<float4 *>(lam_x);
     a.lam_v = static_cast<float4 *>(lam_v);
@@ -1648,6 +1712,7 @@ int mxg_engine_time_force(mxg_engine *e, int reps, double *ms) {
     const EngineView v = e->view(e->cur);
     CUDA_TRY(cudaEventRecord(a, e->stream));
     for (int r = 0; r < reps; ++r) launch_force(v, e->has_dpd, e->force_grid, true, e->stream);
+    e->force_layout = e->cur;
     CUDA_TRY(cudaEventRecord(b, e->stream));
     CUDA_TRY(cudaEventSynchronize(b));
     float t = 0.f;
@@ -1676,6 +1741,7 @@ int mxg_engine_autotune(mxg_engine *e) {
     for (int per_sm : cands) {
         const int grid = std::max(1, std::min(max_grid, e->num_sms * per_sm));
         launch_force(v, e->has_dpd, grid, true, e->stream);  // warm
+        e->force_layout = e->cur;
         CUDA_TRY(cudaEventRecord(a, e->stream));
         for (int r = 0; r < 5; ++r) launch_force(v, e->has_dpd, grid, true, e->stream);
         CUDA_TRY(cudaEventRecord(b, e->stream));
@@ -1732,6 +1798,7 @@ int mxg_engine_pair_counts(mxg_engine *e, long long *candidates, long long *inte
         EngineView v = e->view(e->cur);
         v.pair_stats = d_cnt;
         launch_force(v, e->has_dpd, e->force_grid, true, e->stream);
+        e->force_layout = e->cur;
         unsigned long long n = 0;
         CUDA_TRY(cudaMemcpyAsync(&n, d_cnt, sizeof(n), cudaMemcpyDeviceToHost, e->stream));
         CUDA_TRY(cudaStreamSynchronize(e->stream));

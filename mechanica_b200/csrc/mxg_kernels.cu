@@ -632,7 +632,84 @@ __device__ __forceinline__ float4 total_force(const EngineView &v, int s) {
         f.y += g.y;
         f.z += g.z;
     }
+    if (v.has_sb) {
+        // the velocity-dependent and random single-body forces (MxForce.cpp:330-386)
+        const int ti = __float_as_int(v.pos[s].w);
+        const DevType &T = v.types[ti];
+        if (T.sb_kind >= 2) {
+            const float4 u = v.vel[s];
+            const int id = __float_as_int(u.w);
+            float sx = 0.f, sy = 0.f, sz = 0.f, px = 0.f, py = 0.f, pz = 0.f;
+            if (T.sb_kind == 2) {  // berendsen_force: itau ((T0 / KE_type) - 1) v
+                const float scale = (float)((double)T.sb_a * ((T.target / v.type_ke[ti]) - 1.0));
+                sx = __fmul_rn(scale, u.x);
+                sy = __fmul_rn(scale, u.y);
+                sz = __fmul_rn(scale, u.z);
+            } else {
+                const float4 pf = v.persist[id];
+                px = pf.x;
+                py = pf.y;
+                pz = pf.z;
+                if (T.sb_kind == 4) {  // friction_force: -coef |v|^2 v
+                    const float v2 = __fadd_rn(__fadd_rn(__fmul_rn(u.x, u.x), __fmul_rn(u.y, u.y)), __fmul_rn(u.z, u.z));
+                    const float scale = (float)(-1. * (double)T.sb_a * (double)v2);
+                    sx = __fmul_rn(scale, u.x);
+                    sy = __fmul_rn(scale, u.y);
+                    sz = __fmul_rn(scale, u.z);
+                }
+            }
+            f.x += __fadd_rn(sx, px);
+            f.y += __fadd_rn(sy, py);
+            f.z += __fadd_rn(sz, pz);
+        }
+    }
     return f;
+}
+
+/* Per type: the summed kinetic energy 0.5 m v^2 (each particle's term in FP32,
+ * summed in FP64, engine_kinetic_energy, engine.cpp:1698-1719), the quantity
+ * berendsen_force reads. One block per type, fixed summation order. */
+__global__ void type_ke_kernel(EngineView v, double *out) {
+    __shared__ double part[256];
+    const int t = blockIdx.x;
+    const double mass = v.types[t].mass;
+    double acc = 0.0;
+    for (int s = threadIdx.x; s < v.nparts; s += blockDim.x) {
+        if (__float_as_int(v.pos[s].w) != t) continue;
+        const float4 u = v.vel[s];
+        const float e = (float)(0.5 * mass * (double)(u.x * u.x + u.y * u.y + u.z * u.z));
+        acc += (double)e;
+    }
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+        if ((int)threadIdx.x < off) part[threadIdx.x] += part[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[t] = part[0];
+}
+
+/* Redraws the persistent random force of particles whose (time + id) is a
+ * multiple of their type's interval (gaussian_force / friction_force,
+ * MxForce.cpp:356-381): a normal magnitude N(mean, std) in a uniformly random
+ * direction, as MxRandomVector builds it (MxParticle.cpp:1782-1793), drawn from
+ * a Philox stream keyed on (time, id) instead of the global mt19937. */
+__global__ void persist_kernel(EngineView v, float4 *persist) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= v.nparts) return;
+    const DevType &T = v.types[__float_as_int(v.pos[s].w)];
+    if (T.sb_kind != 3 && T.sb_kind != 4) return;
+    const unsigned id = __float_as_uint(v.vel[s].w);
+    const unsigned long long time = *v.step + 1;  // engine_step advances the time before the step
+    if ((time + id) % (unsigned long long)T.sb_steps != 0) return;
+    const uint4 r = philox4x32(make_uint4(id, 0x52414e44u, (unsigned)time, (unsigned)(time >> 32)),
+                               make_uint2(0x46524345u, 0x50455253u));
+    const float mean = T.sb_kind == 3 ? T.sb_a : T.sb_b, sd = T.sb_kind == 3 ? T.sb_b : T.sb_c;
+    const float g = sqrtf(-2.0f * logf(u01(r.x))) * cospif(2.0f * u01(r.y));
+    const float mag = mean + sd * g;
+    const float theta = 2.0f * (float)M_PI * u01(r.z);
+    const float phi = acosf(1.0f - 2.0f * u01(r.w));
+    persist[id] = make_float4(mag * sinf(phi) * cosf(theta), mag * sinf(phi) * sinf(theta), mag * cosf(phi), 0.f);
 }
 
 /* Completes the force pass when neither the bond kernel nor the integrator
@@ -1181,6 +1258,12 @@ void launch_force(const EngineView &v, bool has_dpd, int grid, bool combine, cud
     else
         launch_force_mode<false>(v, grid, st);
     if (combine) combine_kernel<<<(v.nparts + 255) / 256, 256, 0, st>>>(v);
+}
+
+void launch_singlebody_prep(const EngineView &v, int ntypes, double *type_ke, float4 *persist, bool redraw,
+                            cudaStream_t st) {
+    type_ke_kernel<<<ntypes, 256, 0, st>>>(v, type_ke);
+    if (redraw) persist_kernel<<<(v.nparts + 255) / 256, 256, 0, st>>>(v, persist);
 }
 
 void launch_virial_reduce(const double *partials, int nwarps, double *out9, cudaStream_t st) {

@@ -6,6 +6,10 @@ namespace mxg {
 
 void configure_force_kernels();
 void launch_sort_bounds(const EngineView &v, cudaStream_t st);
+/* Before a force pass: the per-type kinetic energy (Berendsen) and, when redraw is set (the
+ * step's first force pass), the persistent random forces due at this step. */
+void launch_singlebody_prep(const EngineView &v, int ntypes, double *type_ke, float4 *persist, bool redraw,
+                            cudaStream_t st);
 void launch_virial_reduce(const double *partials, int nwarps, double *out9, cudaStream_t st);
 /* combine: add the received planes here (no bond or integrator pass follows) */
 void launch_force(const EngineView &v, bool has_dpd, int grid, bool combine, cudaStream_t st);

@@ -183,6 +183,33 @@ int mxref_bind_force(int type, float fx, float fy, float fz) {
     return engine_add_singlebody_force(&_Engine, (MxForce *)obj, type, -1);
 }
 
+extern "C" PyObject *mxref_make_berendsen(float tau);
+extern "C" PyObject *mxref_make_random(float std, float mean, float durration);
+extern "C" PyObject *mxref_make_friction(float coef, float std, float mean, float durration);
+
+/* The other single-body forces of MxForce.cpp:308-419 (berendsen_force,
+ * gaussian_force, friction_force), created as the forces module creates them
+ * (MxForce.cpp:213-259) and bound with engine_add_singlebody_force
+ * (engine.cpp:983-1003), with the module's arguments:
+ * kind 1: berenderson_tstat(a = tau); 2: random(a = std, b = mean, c = durration);
+ * 3: friction(a = coef, b = std, c = mean, d = durration). */
+int mxref_bind_singlebody(int type, int kind, float a, float b, float c, float d) {
+    // engine_add_singlebody_force type-checks against MxConstantForce_Type
+    if (PyType_Ready(&MxForce_Type) < 0 || PyType_Ready(&MxConstantForce_Type) < 0) return -1;
+    PyObject *obj = kind == 1 ? mxref_make_berendsen(a) : kind == 2 ? mxref_make_random(a, b, c)
+                                                                    : mxref_make_friction(a, b, c, d);
+    if (!obj) return -1;
+    return engine_add_singlebody_force(&_Engine, (MxForce *)obj, type, -1);
+}
+
+/* The type's target temperature, which berendsen_force compares with the type's
+ * summed kinetic energy (MxParticle.cpp:543-560). */
+int mxref_set_target_temperature(int type, double t) {
+    if (type < 0 || type >= engine::nr_types) return -1;
+    engine::types[type].target_energy = t;
+    return 0;
+}
+
 int mxref_add_bonds(int n, const int *pi, const int *pj, void *pot, double dissociation) {
     for (int k = 0; k < n; ++k) {
         MxBond *bond = NULL;

@@ -12,6 +12,8 @@
  * links; none of them is reached by the configurations the oracle runs
  * (no clusters, fluxes, angles, dihedrals, exclusions, rigids or events).
  */
+#include <random>
+
 #include "mdcore_config.h"
 #include "engine.h"
 #include "MxParticle.h"
@@ -67,5 +69,18 @@ CMulticastTimeEvent *CMulticastTimeEvent_New() { return nullptr; }
 HRESULT CMulticastTimeEvent_Invoke(CMulticastTimeEvent *, double) { return S_OK; }
 PyObject *MxPotential_Bind(MxPotential *, PyObject *, PyObject *) { Py_RETURN_NONE; }
 int MxParticle_Check(PyObject *) { return 0; }
-Magnum::Vector3 MxRandomVector(float, float) { return Magnum::Vector3(); }
+/* MxRandomVector (src/mdcore/src/MxParticle.cpp:1782-1793, a file this build
+ * does not compile): a normal magnitude N(mean, std) in a uniformly random
+ * direction, restated with the same construction on a default-seeded mt19937
+ * standing in for carbon's global generator (the random-force tests compare
+ * statistics, not draws). */
+static std::mt19937 g_random;
+Magnum::Vector3 MxRandomVector(float mean, float std) {
+    std::normal_distribution<> dist{mean, std};
+    std::uniform_real_distribution<double> uniform01(0.0, 1.0);
+    float theta = 2 * M_PI * uniform01(g_random);
+    float phi = acos(1 - 2 * uniform01(g_random));
+    float r = dist(g_random);
+    return Magnum::Vector3{r * sinf(phi) * cosf(theta), r * sinf(phi) * sinf(theta), r * cosf(phi)};
+}
 MxBody::MxBody() {}

@@ -15,7 +15,11 @@ A scenario is a dict:
     forces [(type, fx, fy, fz)], x (N,3) float64, v (N,3), t (N,) int,
     bonds (optional): bi, bj, bond_pot (kind, params), dissociation,
     action: "force" | "steps", nsteps, runners (threads), time_it (bool),
-    integrator (0 forward Euler, 1 Runge-Kutta 4)
+    integrator (0 forward Euler, 1 Runge-Kutta 4),
+    sbforces [(type, "berendsen" | "random" | "friction", params)] with the forces module's
+    arguments: berenderson_tstat(tau), random(std, mean, durration),
+    friction(coef, std, mean, durration) (MxForce.cpp:213-259),
+    target_temperature {type: T}
 Results: xabs, xrel, v, f, cell (per id), tasks (rows type, sid, i, j),
     cdim, h, epot, ekin, bond_flags, seconds (wall time of the steps).
 """
@@ -39,7 +43,7 @@ def available():
 def _pack(scn):
     flat = {}
     for k, v in scn.items():
-        if k in ("types", "pots", "forces", "bond_pot", "bc"):
+        if k in ("types", "pots", "forces", "bond_pot", "bc", "sbforces", "target_temperature"):
             flat[k] = np.array(repr(v))
         else:
             flat[k] = np.asarray(v)
@@ -50,7 +54,7 @@ def _unpack(npz):
     out = {}
     for k in npz.files:
         v = npz[k]
-        if k in ("types", "pots", "forces", "bond_pot", "bc"):
+        if k in ("types", "pots", "forces", "bond_pot", "bc", "sbforces", "target_temperature"):
             out[k] = eval(str(v))  # written by _pack from plain literals
         elif v.shape == ():
             out[k] = v.item()
@@ -131,6 +135,15 @@ def _execute(scn):
     for (t, fx, fy, fz) in scn.get("forces", []):
         if L.mxref_bind_force(int(t), float(fx), float(fy), float(fz)) < 0:
             raise RuntimeError("mxref_bind_force")
+    L.mxref_bind_singlebody.argtypes = [ci] * 2 + [ctypes.c_float] * 4
+    L.mxref_set_target_temperature.argtypes = [ci, cd]
+    for (t, kind, params) in scn.get("sbforces", []):
+        code = {"berendsen": 1, "random": 2, "friction": 3}[kind]
+        q = list(params) + [0.0] * (4 - len(params))
+        if L.mxref_bind_singlebody(int(t), code, *[float(v) for v in q]) < 0:
+            raise RuntimeError("mxref_bind_singlebody")
+    for t, temp in scn.get("target_temperature", {}).items():
+        L.mxref_set_target_temperature(int(t), float(temp))
     x = np.ascontiguousarray(scn["x"], dtype=np.float64)
     v = np.ascontiguousarray(scn["v"], dtype=np.float64)
     t = np.ascontiguousarray(scn["t"], dtype=np.int32)
