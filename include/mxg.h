@@ -9,6 +9,7 @@
  *   mxg_potential_create_morse     potential_create_morse   src/mdcore/src/MxPotential.cpp:3389
  *   mxg_potential_create_harmonic  potential_create_harmonic src/mdcore/src/MxPotential.cpp:335
  *   mxg_potential_create_power     potential_create_power   src/mdcore/src/MxPotential.cpp:1614
+ *   mxg_potential_create_harmonic_angle potential_create_harmonic_angle src/mdcore/src/MxPotential.cpp:557
  *   mxg_potential_create_dpd       DPDPotential_New         src/mdcore/src/DissapativeParticleDynamics.cpp:134
  *   mxg_potential_eval             potential_eval_ex        src/mdcore/src/potential_eval.hpp:106
  *   mxg_engine_init                engine_init              src/mdcore/include/engine.h:600
@@ -17,6 +18,7 @@
  *   mxg_engine_add_singlebody_force engine_add_singlebody_force src/mdcore/src/engine.cpp:983
  *   mxg_engine_addparts            engine_addpart           src/mdcore/src/engine.cpp:1726
  *   mxg_engine_addbonds            engine_bond_alloc + _bond_init src/mdcore/src/bond.cpp:497
+ *   mxg_engine_addangles           engine_angle_alloc + angle_init src/mdcore/src/angle.cpp:659-707
  *   mxg_engine_start               engine_start             src/mdcore/include/engine.h:640
  *   mxg_engine_step                engine_step              src/mdcore/src/engine.cpp:1198
  *   mxg_engine_force               engine_force             src/mdcore/src/engine.cpp:1230
@@ -104,6 +106,11 @@ int mxg_potential_create_morse(double d, double alpha, double r0, double min, do
 int mxg_potential_create_harmonic(double k, double r0, double min, double max, double tol, mxg_potential **out);
 int mxg_potential_create_power(double k, double r0, double alpha, double min, double max, double tol,
                                mxg_potential **out);
+/* k (acos(c) - theta0)^2 tabulated in c = cos(theta) on [cos(max), cos(min)], min clipped to >= 0 and
+ * max to <= pi, fitted without an analytic derivative (Potential.harmonic_angle,
+ * src/mdcore/src/MxPotential.cpp:2577-2590, 557-594). */
+int mxg_potential_create_harmonic_angle(double k, double theta0, double min, double max, double tol,
+                                        mxg_potential **out);
 int mxg_potential_create_dpd(double alpha, double gamma, double sigma, double cutoff, int shifted,
                              mxg_potential **out);
 /* Table description: kind, flags, intervals n, interval map alpha[4], domain [a,b], r0+1. */
@@ -197,6 +204,11 @@ int mxg_engine_addparts(mxg_engine *e, int n, const double *x, const float *v, c
 /* Adds n harmonic/table bonds between particle ids i[k], j[k], all with potential p. */
 int mxg_engine_addbonds(mxg_engine *e, int n, const int *i, const int *j, const mxg_potential *p,
                         double dissociation_energy, int *ids_out);
+/* Adds n angles i[q]-j[q]-k[q] (vertex j), all with table potential p in cos(theta), evaluated each
+ * force pass after the bonds as angle_eval does (src/mdcore/src/angle.cpp:92-352); the vertex carries
+ * the energy. ids_out receives consecutive angle indices (may be NULL). */
+int mxg_engine_addangles(mxg_engine *e, int n, const int *i, const int *j, const int *k, const mxg_potential *p,
+                         int *ids_out);
 /* Builds the cell-pair lists and uploads the state. stream may be NULL (default stream). */
 int mxg_engine_start(mxg_engine *e, void *cuda_stream);
 /* Runs nsteps forward-Euler steps on the device (forces, bonds, integrate, re-bin). */

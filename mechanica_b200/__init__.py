@@ -27,7 +27,7 @@ from . import _native
 from ._native import EngineError, check, f32, f64, i32, lib, ptr
 
 __all__ = [
-    "init", "Universe", "universe", "Particle", "Potential", "Bond", "bind", "forces", "step", "run",
+    "init", "Universe", "universe", "Particle", "Potential", "Bond", "Angle", "bind", "forces", "step", "run",
     "Newtonian", "Overdamped", "FORWARD_EULER", "RUNGE_KUTTA_4", "BOUNDARY_NONE", "PERIODIC_X", "PERIODIC_Y", "PERIODIC_Z",
     "PERIODIC_FULL", "FREESLIP_X", "FREESLIP_Y", "FREESLIP_Z", "FREESLIP_FULL", "EngineError",
 ]
@@ -152,6 +152,12 @@ class Potential:
         max = r0 + rng if max is None else max
         tol = 0.01 * (max - min) if tol is None else tol
         return Potential._make("mxg_potential_create_harmonic", (k, r0, min, max, tol), "Harmonic")
+
+    @staticmethod
+    def harmonic_angle(k, theta0, min=0.0, max=math.pi, tol=None):
+        """k (theta - theta0)^2, tabulated in cos(theta) (MxPotential.cpp:2577-2590)."""
+        tol = 0.005 * abs(max - min) if tol is None else tol
+        return Potential._make("mxg_potential_create_harmonic_angle", (k, theta0, min, max, tol), "Harmonic Angle")
 
     @staticmethod
     def power(k=1.0, r0=1.0, alpha=1.0, min=None, max=None, tol=None):
@@ -299,6 +305,20 @@ class Bond:
         return bool(universe.bond_flags()[self.id] & 1)
 
 
+class Angle:
+    """An angle p1-p2-p3 with its vertex at p2 and a potential in cos(theta)
+    (angle.cpp:659-707); evaluated every force pass after the bonds
+    (angle_eval, angle.cpp:92-352)."""
+
+    def __init__(self, potential, p1, p2, p3):
+        if not isinstance(potential, Potential):
+            raise TypeError("potential is not a instance of Potential")
+        u = _require()
+        self.i, self.j, self.k = _pid(p1), _pid(p2), _pid(p3)
+        self.id = u._add_angles(potential, [self.i], [self.j], [self.k])[0]
+        self.potential = potential
+
+
 def _pid(p):
     return p.id if isinstance(p, Particle) else int(p)
 
@@ -377,6 +397,7 @@ class _Universe:
         self._forces = []       # (type, force object), one per type
         self._targets = {}      # type -> target temperature
         self._bonds = []        # (potential, i[], j[], dissociation)
+        self._angles = []       # (potential, i[], j[], k[])
         self._x = np.zeros((0, 3))
         self._v = np.zeros((0, 3), dtype=np.float32)
         self._t = np.zeros(0, dtype=np.int32)
@@ -430,6 +451,9 @@ class _Universe:
         for (p, ii, jj, d) in self._bonds:
             check(lib().mxg_engine_addbonds(self._e, len(ii), ptr(ii, ctypes.c_int), ptr(jj, ctypes.c_int), p._h, d,
                                             None), "addbonds")
+        for (p, ii, jj, kk) in self._angles:
+            check(lib().mxg_engine_addangles(self._e, len(ii), ptr(ii, ctypes.c_int), ptr(jj, ctypes.c_int),
+                                             ptr(kk, ctypes.c_int), p._h, None), "addangles")
         self._started = False
 
     def _add_type(self, cls):
@@ -470,6 +494,14 @@ class _Universe:
         ii, jj = i32(i), i32(j)
         first = sum(len(b[1]) for b in self._bonds)
         self._bonds.append((pot, ii, jj, float(d)))
+        self._sync_state()
+        self._dirty = True
+        return list(range(first, first + len(ii)))
+
+    def _add_angles(self, pot, i, j, k):
+        ii, jj, kk = i32(i), i32(j), i32(k)
+        first = sum(len(a[1]) for a in self._angles)
+        self._angles.append((pot, ii, jj, kk))
         self._sync_state()
         self._dirty = True
         return list(range(first, first + len(ii)))

@@ -111,6 +111,25 @@ struct DevBond {
     double dissociation;
 };
 
+struct DevAngle {
+    int i, j, k;         // particle ids; j is the vertex
+    int pot;             // potential index (a table in cos(theta))
+};
+
+/* Bonded interactions, CSR by particle id. bond_list holds bond indices;
+ * angle_list holds angle * 4 + role (0: i, 1: j, 2: k). */
+struct BondedView {
+    const DevBond *bonds;
+    unsigned *bond_flags;
+    const int *bond_off;
+    const int *bond_list;
+    const DevAngle *angles;
+    const int *angle_off;
+    const int *angle_list;
+    const int *slot_of_id;
+    double *e_slot;      // per slot: bonded energy of the last pass
+};
+
 struct EngineView {      // everything a kernel needs, passed by value
     const float4 *pos;
     const float4 *vel;
@@ -249,6 +268,26 @@ __device__ __forceinline__ void table_eval(const DevPot &p, const float *__restr
     eff = __fadd_rn(__fmul_rn(eff, x), ee); ee = __fadd_rn(__fmul_rn(ee, x), c1.w);
     e = ee;
     f = __fdiv_rn(__fmul_rn(eff, c0.y), r);
+}
+
+/* Table evaluation with potential_eval_r semantics (potential_eval.hpp:180-207):
+ * the table at r itself, f = dV/dr (not divided by r). Used by angles with
+ * r = cos(theta) clamped to [a, b] by the caller; the index is clamped to n. */
+__device__ __forceinline__ void table_eval_r(const DevPot &p, const float *__restrict__ coef, float r, float &e,
+                                             float &f) {
+    const float t = __fadd_rn(p.alpha0, __fmul_rn(r, __fadd_rn(p.alpha1, __fmul_rn(r, p.alpha2))));
+    const int ind = min((int)fmaxf(0.0f, t), p.n);
+    const float4 *c4 = reinterpret_cast<const float4 *>(coef + p.coef_off + ind * kChunk);
+    const float4 c0 = __ldg(c4), c1 = __ldg(c4 + 1);
+    const float x = __fmul_rn(__fsub_rn(r, c0.x), c0.y);
+    float ee = __fadd_rn(__fmul_rn(c0.z, x), c0.w);
+    float eff = c0.z;
+    eff = __fadd_rn(__fmul_rn(eff, x), ee); ee = __fadd_rn(__fmul_rn(ee, x), c1.x);
+    eff = __fadd_rn(__fmul_rn(eff, x), ee); ee = __fadd_rn(__fmul_rn(ee, x), c1.y);
+    eff = __fadd_rn(__fmul_rn(eff, x), ee); ee = __fadd_rn(__fmul_rn(ee, x), c1.z);
+    eff = __fadd_rn(__fmul_rn(eff, x), ee); ee = __fadd_rn(__fmul_rn(ee, x), c1.w);
+    e = ee;
+    f = __fmul_rn(eff, c0.y);
 }
 
 #endif  // __CUDACC__

@@ -90,6 +90,10 @@ struct BondInfo {
     double dissociation;
 };
 
+struct AngleInfo {
+    int i, j, k, pot;
+};
+
 #define CUDA_TRY(x)                                                                              \
     do {                                                                                         \
         cudaError_t err_ = (x);                                                                  \
@@ -335,6 +339,7 @@ struct mxg_engine {
     std::vector<int> ptype;
     std::vector<int> prep;                  // replica of each particle
     std::vector<BondInfo> bonds;
+    std::vector<AngleInfo> angles;
 
     // ---- device ----
     bool started = false;
@@ -386,6 +391,8 @@ struct mxg_engine {
     double *d_virial_partials = nullptr, *d_virial_out = nullptr;
     int virial_cap = 0;
     int *d_bond_off = nullptr, *d_bond_list = nullptr;
+    DevAngle *d_angles = nullptr;
+    int *d_angle_off = nullptr, *d_angle_list = nullptr;
     unsigned *d_status = nullptr;
     unsigned long long *d_step = nullptr;
     double *d_partials = nullptr, *d_energy = nullptr;
@@ -564,20 +571,36 @@ struct mxg_engine {
         return v;
     }
 
-    /* The force pass alone (engine_force): the bond kernel, or the combine
-     * kernel when there are no bonds, adds the received planes. */
+    bool has_bonded() const { return !bonds.empty() || !angles.empty(); }
+
+    BondedView bonded_view() const {
+        BondedView bv;
+        bv.bonds = d_bonds;
+        bv.bond_flags = d_bond_flags;
+        bv.bond_off = d_bond_off;
+        bv.bond_list = d_bond_list;
+        bv.angles = d_angles;
+        bv.angle_off = d_angle_off;
+        bv.angle_list = d_angle_list;
+        bv.slot_of_id = d_slot_of_id;
+        bv.e_slot = d_ebond_slot;
+        return bv;
+    }
+
+    /* The force pass alone (engine_force): the bonded kernel, or the combine
+     * kernel when there are no bonded interactions, adds the received planes. */
     void enqueue_force(int b) {
         force_layout = b;
         const EngineView v = view(b);
         if (has_sb) launch_singlebody_prep(v, ntypes, d_type_ke, d_persist, false, stream);
-        launch_force(v, has_dpd, force_grid, bonds.empty(), stream);
-        if (!bonds.empty())
-            launch_bonds(v, d_bonds, d_bond_flags, d_bond_off, d_bond_list, d_slot_of_id, d_ebond_slot, stream);
+        launch_force(v, has_dpd, force_grid, !has_bonded(), stream);
+        if (has_bonded()) launch_bonded(v, bonded_view(), stream);
     }
 
-    /* One step (engine_step): force pass, bonds, integrator and re-binning; the
-     * received planes are added by the bond kernel or, without bonds, by the
-     * integrator; the re-binning pass computes the new key bounds. */
+    /* One step (engine_step): force pass, bonded pass, integrator and re-binning;
+     * the received planes are added by the bonded kernel or, without bonded
+     * interactions, by the integrator; the re-binning pass computes the new key
+     * bounds. */
     void enqueue_step(int b) {
         if (integrator == 1) {
             enqueue_step_rk4(b);
@@ -587,9 +610,8 @@ struct mxg_engine {
         const EngineView v = view(b);
         if (has_sb) launch_singlebody_prep(v, ntypes, d_type_ke, d_persist, true, stream);
         launch_force(v, has_dpd, force_grid, false, stream);
-        if (!bonds.empty())
-            launch_bonds(v, d_bonds, d_bond_flags, d_bond_off, d_bond_list, d_slot_of_id, d_ebond_slot, stream);
-        launch_integrate(v, d_pos[b], d_vel[b], d_new_cell, d_in_count, d_in_list, d_out_count, bonds.empty(),
+        if (has_bonded()) launch_bonded(v, bonded_view(), stream);
+        launch_integrate(v, d_pos[b], d_vel[b], d_new_cell, d_in_count, d_in_list, d_out_count, !has_bonded(),
                          stream);
         launch_scan(ncells, d_cell_count[b], d_out_count, d_in_count, d_cell_start[nb], d_cell_count[nb], d_step,
                     stream);
@@ -598,7 +620,7 @@ struct mxg_engine {
     }
 
     /* One Runge-Kutta 4 step (engine_advance_runge_kutta_4): four force passes (with
-     * bonds when present), stage updates in the step's cell frame with fresh key
+     * the bonded pass when present), stage updates in the step's cell frame with fresh key
      * bounds before each intermediate pass, then the final update, re-binning as
      * for Euler. */
     void enqueue_step_rk4(int b) {
@@ -608,14 +630,13 @@ struct mxg_engine {
             // persistent random forces are redrawn in the first stage only (INTEGRATOR_UPDATE_PERSISTENTFORCE)
             if (has_sb) launch_singlebody_prep(v, ntypes, d_type_ke, d_persist, stage == 0, stream);
             launch_force(v, has_dpd, force_grid, false, stream);
-            if (!bonds.empty())
-                launch_bonds(v, d_bonds, d_bond_flags, d_bond_off, d_bond_list, d_slot_of_id, d_ebond_slot, stream);
+            if (has_bonded()) launch_bonded(v, bonded_view(), stream);
             if (stage < 3) {
-                launch_rk_stage(v, d_pos[b], d_rk, stage, bonds.empty(), stream);
+                launch_rk_stage(v, d_pos[b], d_rk, stage, !has_bonded(), stream);
                 launch_sort_bounds(v, stream);
             } else {
                 launch_rk_final(v, d_pos[b], d_vel[b], d_rk, d_new_cell, d_in_count, d_in_list, d_out_count,
-                                bonds.empty(), stream);
+                                !has_bonded(), stream);
             }
         }
         launch_scan(ncells, d_cell_count[b], d_out_count, d_in_count, d_cell_start[nb], d_cell_count[nb], d_step,
@@ -880,6 +901,27 @@ int mxg_engine::start(cudaStream_t st) {
         }
     }
 
+    // ---- angles: CSR by particle id, entries angle * 4 + role ----
+    std::vector<DevAngle> ha;
+    std::vector<int> aoff(nparts + 1, 0), alist;
+    for (const AngleInfo &a : angles) {
+        const int ids[3] = {a.i, a.j, a.k};
+        for (int r = 0; r < 3; ++r)
+            if (ids[r] < 0 || ids[r] >= nparts) return MXG_ERR_BOND;
+        if (prep[a.i] != prep[a.j] || prep[a.k] != prep[a.j]) return MXG_ERR_BOND;
+        for (int r = 0; r < 3; ++r) aoff[ids[r] + 1]++;
+    }
+    for (int p = 0; p < nparts; ++p) aoff[p + 1] += aoff[p];
+    alist.assign(aoff[nparts], 0);
+    {
+        std::vector<int> fill(aoff.begin(), aoff.end() - 1);
+        for (int k = 0; k < (int)angles.size(); ++k) {
+            const int ids[3] = {angles[k].i, angles[k].j, angles[k].k};
+            for (int r = 0; r < 3; ++r) alist[fill[ids[r]]++] = k * 4 + r;
+            ha.push_back({angles[k].i, angles[k].j, angles[k].k, angles[k].pot});
+        }
+    }
+
     // ---- device allocation ----
     rc = MXG_OK;
     for (int b = 0; b < 2; ++b) {
@@ -923,6 +965,9 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_bond_flags, hbf.size());
     rc |= alloc(&d_bond_off, boff.size());
     rc |= alloc(&d_bond_list, blist.size());
+    rc |= alloc(&d_angles, ha.size());
+    rc |= alloc(&d_angle_off, aoff.size());
+    rc |= alloc(&d_angle_list, alist.size());
     rc |= alloc(&d_status, 1);
     rc |= alloc(&d_step, 1);
     rc |= alloc(&d_partials, 2 * (size_t)energy_blocks);
@@ -950,7 +995,9 @@ int mxg_engine::start(cudaStream_t st) {
         (rc = upload(d_pot_idx2, hpidx2, stream)) ||
         (rc = upload(d_types, ht, stream)) || (rc = upload(d_spaces, hs, stream)) || (rc = upload(d_axes, haxes, stream)) ||
         (rc = upload(d_bonds, hb, stream)) || (rc = upload(d_bond_flags, hbf, stream)) ||
-        (rc = upload(d_bond_off, boff, stream)) || (rc = upload(d_bond_list, blist, stream)))
+        (rc = upload(d_bond_off, boff, stream)) || (rc = upload(d_bond_list, blist, stream)) ||
+        (rc = upload(d_angles, ha, stream)) || (rc = upload(d_angle_off, aoff, stream)) ||
+        (rc = upload(d_angle_list, alist, stream)))
         return rc;
     CUDA_TRY(cudaStreamSynchronize(stream));
 
@@ -1038,6 +1085,14 @@ int mxg_potential_create_harmonic(double k, double r0, double min, double max, d
     if (!(max > min) || !(tol > 0)) return MXG_ERR_ARG;
     mxg_potential *p = new mxg_potential;
     return wrap_potential(make_harmonic(p->t, k, r0, min, max, tol), p, out);
+}
+
+int mxg_potential_create_harmonic_angle(double k, double theta0, double min, double max, double tol,
+                                       mxg_potential **out) {
+    if (!out) return MXG_ERR_NULL;
+    if (!(max > min) || !(tol > 0)) return MXG_ERR_ARG;
+    mxg_potential *p = new mxg_potential;
+    return wrap_potential(make_harmonic_angle(p->t, k, theta0, min, max, tol), p, out);
 }
 
 int mxg_potential_create_power(double k, double r0, double alpha, double min, double max, double tol,
@@ -1358,6 +1413,20 @@ int mxg_engine_addbonds(mxg_engine *e, int n, const int *i, const int *j, const 
     return MXG_OK;
 }
 
+int mxg_engine_addangles(mxg_engine *e, int n, const int *i, const int *j, const int *k, const mxg_potential *p,
+                         int *ids_out) {
+    if (!e || !p || (n > 0 && (!i || !j || !k))) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    if (p->t.kind != kKindTable) return MXG_ERR_POTENTIAL;
+    e->pots.push_back(p->t);
+    const int idx = (int)e->pots.size() - 1;
+    for (int q = 0; q < n; ++q) {
+        if (ids_out) ids_out[q] = (int)e->angles.size();
+        e->angles.push_back({i[q], j[q], k[q], idx});
+    }
+    return MXG_OK;
+}
+
 int mxg_engine_start(mxg_engine *e, void *cuda_stream) {
     if (!e) return MXG_ERR_NULL;
     if (e->started) return MXG_ERR_STATE;
@@ -1470,7 +1539,7 @@ int mxg_engine_load(mxg_engine *e, int n, const double *x, const float *v) {
 int mxg_engine_energy(mxg_engine *e, double *epot, double *ekin, double *virial9) {
     if (!e) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
-    launch_energy(e->nitems, e->d_epot_cell, e->nparts, e->bonds.empty() ? nullptr : e->d_ebond_slot,
+    launch_energy(e->nitems, e->d_epot_cell, e->nparts, e->has_bonded() ? e->d_ebond_slot : nullptr,
                   e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
                   e->stream);
     double out[2];
@@ -1569,7 +1638,7 @@ int mxg_engine_copy_state(mxg_engine *e, void *host_pos, void *host_vel, int to_
 int mxg_engine_energy_async(mxg_engine *e, double *host_out2) {
     if (!e || !host_out2) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
-    launch_energy(e->nitems, e->d_epot_cell, e->nparts, e->bonds.empty() ? nullptr : e->d_ebond_slot,
+    launch_energy(e->nitems, e->d_epot_cell, e->nparts, e->has_bonded() ? e->d_ebond_slot : nullptr,
                   e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
                   e->stream);
     CUDA_TRY(cudaMemcpyAsync(host_out2, e->d_energy, 2 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
@@ -1634,7 +1703,7 @@ int mxg_engine_adjoint_params(mxg_engine *e, int n, const int *pot, const int *p
 int mxg_engine_vjp_step(mxg_engine *e, void *lam_x, void *lam_v, double *grad) {
     if (!e || !lam_x || !lam_v || !grad) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
-    if (!e->bonds.empty() || e->has_sb) return MXG_ERR_ARG;  // bonds and single-body forces are not differentiated
+    if (e->has_bonded() || e->has_sb) return MXG_ERR_ARG;  // bonded and single-body forces are not differentiated
     if (e->nparts == 0) return MXG_OK;
     if (e->adjoint_stale) {
         const int rc = e->build_adjoint();

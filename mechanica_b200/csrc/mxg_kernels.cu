@@ -3,7 +3,7 @@
  *
  *   force_kernel      nonbonded cell-pair forces (tables, DPD), single-body
  *                     forces, per-cell FP64 energy. One warp per cell.
- *   bond_kernel       harmonic/table bonds with dissociation flags.
+ *   bonded_kernel     harmonic/table bonds with dissociation flags, angles.
  *   integrate_kernel  forward Euler (Newtonian / overdamped), speed clamp,
  *                     wall reflection, relocation; counts the next binning.
  *   scan_kernel       exclusive scan of the new cell occupancy.
@@ -724,72 +724,170 @@ __global__ void combine_kernel(EngineView v) {
 /* bonds                                                                     */
 /* ------------------------------------------------------------------------ */
 
+/* Cell coordinates of global cell c in its replica's grid. */
+__device__ __forceinline__ void cell_loc(const DevSpace &S, int c, int loc[3]) {
+    const int l = c - S.cell_offset;
+    loc[0] = l / (S.cdim[1] * S.cdim[2]);
+    loc[1] = (l / S.cdim[2]) % S.cdim[1];
+    loc[2] = l % S.cdim[2];
+}
+
+/* The bonded code's neighbour-cell shift (bond.cpp:163-170, angle.cpp:155-168):
+ * a cell difference of more than one is a periodic wrap. */
+__device__ __forceinline__ int wrap_shift(int d) { return d > 1 ? -1 : (d < -1 ? 1 : d); }
+
+/* x + shift*h formed in double and rounded to float, as the reference writes
+ * the double product into a float position. */
+__device__ __forceinline__ float shifted(float x, int sh, double h) {
+    return (float)__dadd_rn((double)x, __dmul_rn(h, (double)sh));
+}
+
 /*
- * One thread per particle slot; each thread evaluates every bond its particle
- * takes part in, from the bond's first particle's point of view exactly as
- * bond_eval does (bond.cpp:99-312), and applies its own half of the force.
- * Both ends therefore compute the same force/r and the same break decision
- * eff >= dissociation_energy; the first end clears the bond's active flag.
+ * The force terms of angle aid exactly as angle_eval computes them
+ * (angle.cpp:92-352): positions relative to the vertex j's cell, cos(theta)
+ * at j clamped to [-1, 1], the derivatives of cos(theta) with respect to x_i
+ * and x_k, the table's [a, b] clamp, and potential_eval_r on the cosine.
+ * Returns wi = eff * dcos/dx_i and wk = eff * dcos/dx_k, or false when one of
+ * the ids is absent. At cos(theta) = 0 or -1 the reference replaces both
+ * derivatives with one random unit vector (a uniform draw in [-1, 1]^3 minus
+ * its projection on x_i - x_k, normalised); that draw comes from a Philox
+ * stream keyed on (angle, step) here instead of the global mt19937.
  */
-__global__ void bond_kernel(EngineView v, const DevBond *__restrict__ bonds, unsigned *bond_flags,
-                            const int *__restrict__ bond_off, const int *__restrict__ bond_list,
-                            const int *__restrict__ slot_of_id, double *__restrict__ ebond_slot) {
+__device__ bool angle_terms(const EngineView &v, const BondedView &bv, int aid, float wi[3], float wk[3],
+                            float &ee) {
+    const DevAngle A = bv.angles[aid];
+    if (A.pot < 0) return false;
+    const int si = bv.slot_of_id[A.i], sj = bv.slot_of_id[A.j], sk = bv.slot_of_id[A.k];
+    if (si < 0 || sj < 0 || sk < 0) return false;
+    const int cj = v.cell_of[sj];
+    const DevSpace &S = v.spaces[v.cell_rep[cj]];
+    int loci[3], locj[3], lock[3];
+    cell_loc(S, v.cell_of[si], loci);
+    cell_loc(S, cj, locj);
+    cell_loc(S, v.cell_of[sk], lock);
+    const float4 pi = v.pos[si], pj = v.pos[sj], pk = v.pos[sk];
+    const float xiv[3] = {pi.x, pi.y, pi.z}, xj[3] = {pj.x, pj.y, pj.z}, xkv[3] = {pk.x, pk.y, pk.z};
+    float xi[3], xk[3], rji[3], rjk[3];
+    for (int q = 0; q < 3; ++q) {
+        xi[q] = shifted(xiv[q], wrap_shift(loci[q] - locj[q]), S.hd[q]);
+        xk[q] = shifted(xkv[q], wrap_shift(lock[q] - locj[q]), S.hd[q]);
+        rji[q] = __fsub_rn(xi[q], xj[q]);
+        rjk[q] = __fsub_rn(xk[q], xj[q]);
+    }
+    const float dprod =
+        __fadd_rn(__fadd_rn(__fmul_rn(rji[0], rjk[0]), __fmul_rn(rji[1], rjk[1])), __fmul_rn(rji[2], rjk[2]));
+    const float inji = __fdiv_rn(1.0f, __fsqrt_rn(dot3_rn(rji[0], rji[1], rji[2])));
+    const float injk = __fdiv_rn(1.0f, __fsqrt_rn(dot3_rn(rjk[0], rjk[1], rjk[2])));
+    float ct = fmaxf(-1.0f, fminf(1.0f, __fmul_rn(__fmul_rn(dprod, inji), injk)));
+    float dxi[3], dxk[3];
+    if (ct == 0.0f || ct == -1.0f) {
+        const unsigned long long step = *v.step;
+        const uint4 r = philox4x32(make_uint4((unsigned)aid, 0x414e474cu, (unsigned)step, (unsigned)(step >> 32)),
+                                   make_uint2(0x504c414eu, 0x45524e44u));
+        float x[3] = {__fsub_rn(__fmul_rn(2.0f, u01(r.x)), 1.0f), __fsub_rn(__fmul_rn(2.0f, u01(r.y)), 1.0f),
+                      __fsub_rn(__fmul_rn(2.0f, u01(r.z)), 1.0f)};
+        const float vik[3] = {__fsub_rn(xi[0], xk[0]), __fsub_rn(xi[1], xk[1]), __fsub_rn(xi[2], xk[2])};
+        const float d = __fadd_rn(__fadd_rn(__fmul_rn(x[0], vik[0]), __fmul_rn(x[1], vik[1])), __fmul_rn(x[2], vik[2]));
+        for (int q = 0; q < 3; ++q) x[q] = __fsub_rn(x[q], __fmul_rn(d, vik[q]));
+        const float len = __fsqrt_rn(dot3_rn(x[0], x[1], x[2]));
+        for (int q = 0; q < 3; ++q) dxi[q] = dxk[q] = __fdiv_rn(x[q], len);
+    } else {
+        for (int q = 0; q < 3; ++q) {
+            dxi[q] = __fmul_rn(__fsub_rn(__fmul_rn(rjk[q], injk), __fmul_rn(__fmul_rn(ct, rji[q]), inji)), inji);
+            dxk[q] = __fmul_rn(__fsub_rn(__fmul_rn(rji[q], inji), __fmul_rn(__fmul_rn(ct, rjk[q]), injk)), injk);
+        }
+    }
+    const DevPot &p = v.pots[A.pot];
+    if (ct < p.a || ct > p.b) ct = fmaxf(p.a, fminf(p.b, ct));
+    float eff;
+    table_eval_r(p, v.coef, ct, ee, eff);
+    for (int q = 0; q < 3; ++q) {
+        wi[q] = __fmul_rn(eff, dxi[q]);
+        wk[q] = __fmul_rn(eff, dxk[q]);
+    }
+    return true;
+}
+
+/*
+ * The bonded pass (engine_bonded_eval, engine_bonded.cpp:1373-1543: bonds,
+ * then angles). One thread per particle slot; each thread evaluates every
+ * bond and angle its particle takes part in and applies its own share, in the
+ * bonded lists' index order, so its force receives the same sequence of
+ * updates as in the reference's serial loops.
+ *
+ * Bonds (bond.cpp:99-312) are evaluated from the bond's first particle's point
+ * of view; both ends compute the same force/r and the same break decision
+ * eff >= dissociation_energy, and the first end clears the active flag.
+ * Angles: f_i -= wi, f_k -= wk, f_j += wi + wk; the vertex carries the energy.
+ */
+__global__ void bonded_kernel(EngineView v, BondedView bv) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= v.nparts) return;
     const int id = __float_as_int(v.vel[s].w);
-    const int k0 = bond_off[id], k1 = bond_off[id + 1];
     double eb = 0.0;
-    float4 f = total_force(v, s);  // the bond pass completes the nonbonded force
-    if (k0 < k1) {
-        for (int k = k0; k < k1; ++k) {
-            const int b = bond_list[k];
-            if (!(bond_flags[b] & 1u)) continue;
-            const DevBond B = bonds[b];
-            const int si = slot_of_id[B.i], sj = slot_of_id[B.j];
-            if (si < 0 || sj < 0) continue;
-            const int ci = v.cell_of[si], cj = v.cell_of[sj];
-            const DevSpace &S = v.spaces[v.cell_rep[ci]];
-            const int li = ci - S.cell_offset, lj = cj - S.cell_offset;
-            const int loci[3] = {li / (S.cdim[1] * S.cdim[2]), (li / S.cdim[2]) % S.cdim[1], li % S.cdim[2]};
-            const int locj[3] = {lj / (S.cdim[1] * S.cdim[2]), (lj / S.cdim[2]) % S.cdim[1], lj % S.cdim[2]};
-            const float4 xi = v.pos[si], xj = v.pos[sj];
-            const float xiv[3] = {xi.x, xi.y, xi.z}, xjv[3] = {xj.x, xj.y, xj.z};
-            float d[3];
-            for (int q = 0; q < 3; ++q) {
-                int sh = loci[q] - locj[q];
-                if (sh > 1)
-                    sh = -1;
-                else if (sh < -1)
-                    sh = 1;
-                const float pix = (float)__dadd_rn((double)xiv[q], __dmul_rn(S.hd[q], (double)sh));
-                d[q] = __fsub_rn(pix, xjv[q]);
-            }
-            float r2 = dot3_rn(d[0], d[1], d[2]);
-            const DevPot &p = v.pots[B.pot];
-            const float a2 = __fmul_rn(p.a, p.a), b2 = __fmul_rn(p.b, p.b);
-            if (r2 < a2 || r2 > b2) r2 = fmaxf(a2, fminf(b2, r2));
-            float ee, eff;
-            table_eval(p, v.coef, r2, ee, eff);
-            const bool first = (s == si);
-            if ((double)eff >= B.dissociation) {
-                if (first) bond_flags[b] = 0u;  // MxBond_Destroy (bond.cpp:1001-1013)
-                continue;
-            }
-            const float wx = __fmul_rn(eff, d[0]), wy = __fmul_rn(eff, d[1]), wz = __fmul_rn(eff, d[2]);
-            if (first) {
-                f.x = __fsub_rn(f.x, wx);
-                f.y = __fsub_rn(f.y, wy);
-                f.z = __fsub_rn(f.z, wz);
-                eb += (double)ee;
-            } else {
-                f.x = __fadd_rn(f.x, wx);
-                f.y = __fadd_rn(f.y, wy);
-                f.z = __fadd_rn(f.z, wz);
-            }
+    float4 f = total_force(v, s);  // the bonded pass completes the nonbonded force
+    const int k0 = bv.bond_off[id], k1 = bv.bond_off[id + 1];
+    for (int k = k0; k < k1; ++k) {
+        const int b = bv.bond_list[k];
+        if (!(bv.bond_flags[b] & 1u)) continue;
+        const DevBond B = bv.bonds[b];
+        const int si = bv.slot_of_id[B.i], sj = bv.slot_of_id[B.j];
+        if (si < 0 || sj < 0) continue;
+        const int ci = v.cell_of[si], cj = v.cell_of[sj];
+        const DevSpace &S = v.spaces[v.cell_rep[ci]];
+        int loci[3], locj[3];
+        cell_loc(S, ci, loci);
+        cell_loc(S, cj, locj);
+        const float4 xi = v.pos[si], xj = v.pos[sj];
+        const float xiv[3] = {xi.x, xi.y, xi.z}, xjv[3] = {xj.x, xj.y, xj.z};
+        float d[3];
+        for (int q = 0; q < 3; ++q) d[q] = __fsub_rn(shifted(xiv[q], wrap_shift(loci[q] - locj[q]), S.hd[q]), xjv[q]);
+        float r2 = dot3_rn(d[0], d[1], d[2]);
+        const DevPot &p = v.pots[B.pot];
+        const float a2 = __fmul_rn(p.a, p.a), b2 = __fmul_rn(p.b, p.b);
+        if (r2 < a2 || r2 > b2) r2 = fmaxf(a2, fminf(b2, r2));
+        float ee, eff;
+        table_eval(p, v.coef, r2, ee, eff);
+        const bool first = (s == si);
+        if ((double)eff >= B.dissociation) {
+            if (first) bv.bond_flags[b] = 0u;  // MxBond_Destroy (bond.cpp:1001-1013)
+            continue;
+        }
+        const float wx = __fmul_rn(eff, d[0]), wy = __fmul_rn(eff, d[1]), wz = __fmul_rn(eff, d[2]);
+        if (first) {
+            f.x = __fsub_rn(f.x, wx);
+            f.y = __fsub_rn(f.y, wy);
+            f.z = __fsub_rn(f.z, wz);
+            eb += (double)ee;
+        } else {
+            f.x = __fadd_rn(f.x, wx);
+            f.y = __fadd_rn(f.y, wy);
+            f.z = __fadd_rn(f.z, wz);
+        }
+    }
+    const int a0 = bv.angle_off[id], a1 = bv.angle_off[id + 1];
+    for (int k = a0; k < a1; ++k) {
+        const int code = bv.angle_list[k];
+        const int role = code & 3;
+        float wi[3], wk[3], ee;
+        if (!angle_terms(v, bv, code >> 2, wi, wk, ee)) continue;
+        if (role == 0) {
+            f.x = __fsub_rn(f.x, wi[0]);
+            f.y = __fsub_rn(f.y, wi[1]);
+            f.z = __fsub_rn(f.z, wi[2]);
+        } else if (role == 2) {
+            f.x = __fsub_rn(f.x, wk[0]);
+            f.y = __fsub_rn(f.y, wk[1]);
+            f.z = __fsub_rn(f.z, wk[2]);
+        } else {
+            f.x = __fadd_rn(f.x, __fadd_rn(wi[0], wk[0]));
+            f.y = __fadd_rn(f.y, __fadd_rn(wi[1], wk[1]));
+            f.z = __fadd_rn(f.z, __fadd_rn(wi[2], wk[2]));
+            eb += (double)ee;
         }
     }
     v.force[s] = f;
-    ebond_slot[s] = eb;
+    bv.e_slot[s] = eb;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1270,11 +1368,9 @@ void launch_virial_reduce(const double *partials, int nwarps, double *out9, cuda
     virial_reduce_kernel<<<1, 32, 0, st>>>(partials, nwarps, out9);
 }
 
-void launch_bonds(const EngineView &v, const DevBond *bonds, unsigned *bond_flags, const int *bond_off,
-                  const int *bond_list, const int *slot_of_id, double *ebond_slot, cudaStream_t st) {
+void launch_bonded(const EngineView &v, const BondedView &bv, cudaStream_t st) {
     const int tb = 256;
-    bond_kernel<<<(v.nparts + tb - 1) / tb, tb, 0, st>>>(v, bonds, bond_flags, bond_off, bond_list, slot_of_id,
-                                                        ebond_slot);
+    bonded_kernel<<<(v.nparts + tb - 1) / tb, tb, 0, st>>>(v, bv);
 }
 
 void launch_integrate(const EngineView &v, float4 *pos, float4 *vel, int *new_cell, int *in_count, int *in_list,

@@ -13,8 +13,8 @@ void launch_singlebody_prep(const EngineView &v, int ntypes, double *type_ke, fl
 void launch_virial_reduce(const double *partials, int nwarps, double *out9, cudaStream_t st);
 /* combine: add the received planes here (no bond or integrator pass follows) */
 void launch_force(const EngineView &v, bool has_dpd, int grid, bool combine, cudaStream_t st);
-void launch_bonds(const EngineView &v, const DevBond *bonds, unsigned *bond_flags, const int *bond_off,
-                  const int *bond_list, const int *slot_of_id, double *ebond_slot, cudaStream_t st);
+/* bonds then angles; also adds the received planes (the force pass ran without combine) */
+void launch_bonded(const EngineView &v, const BondedView &bv, cudaStream_t st);
 void launch_integrate(const EngineView &v, float4 *pos, float4 *vel, int *new_cell, int *in_count, int *in_list,
                       int *out_count, bool add_planes, cudaStream_t st);
 /* Runge-Kutta 4: rk[5] = p0, v0, accx, accv, vk of the previous stage (per slot). */

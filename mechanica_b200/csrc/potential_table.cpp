@@ -8,7 +8,8 @@
  * V's sixth derivative. Interval 0 is a linear continuation of interval 1 below
  * a. This is the table format of the reference's potential_init
  * (src/mdcore/src/MxPotential.cpp:1690-1930) and its helpers
- * potential_getfp_fixend (:2032-2113), potential_getcoeffs (:2139-2260) and
+ * potential_getfp (:1949-2030), potential_getfp_fixend (:2032-2113),
+ * potential_getcoeffs (:2139-2260) and
  * potential_getalpha (:2277-2338); the GPU kernels consume exactly this format.
  *
  * The fit reproduces the reference's FP32 coefficient arrays bit for bit, so
@@ -68,10 +69,13 @@ const SlopeQuadrature &slope_quadrature() {
     return q;
 }
 
-/* Interior node slopes that minimise the L2 misfit of the piecewise cubic
- * Hermite interpolant, with the end slopes pinned to V'(a), V'(b): a
- * tridiagonal system over the n+1 nodes. */
-void solve_node_slopes(const ScalarFn &f, double fpa, double fpb, int n, const float *x, double *fp) {
+/* Node slopes that minimise the L2 misfit of the piecewise cubic Hermite
+ * interpolant: a tridiagonal system over the n+1 nodes. With fixed_ends the
+ * end slopes are pinned to fpa, fpb (potential_getfp_fixend); otherwise the
+ * end rows are the misfit's own normal equations (potential_getfp, used when
+ * a potential has no analytic derivative). */
+void solve_node_slopes(const ScalarFn &f, bool fixed_ends, double fpa, double fpb, int n, const float *x,
+                       double *fp) {
     // inner products of the Hermite cardinal functions on [-1,1]
     const double cl1[4] = {0.25, -0.25, -0.25, 0.25};
     const double cr1[4] = {-0.25, -0.25, 0.25, 0.25};
@@ -100,18 +104,30 @@ void solve_node_slopes(const ScalarFn &f, double fpa, double fpb, int n, const f
         pl[i] = sl / (kSamples - 2);
         pr[i] = sr / (kSamples - 2);
     }
-    diag[0] = 1.0;
-    up[0] = 0.0;
-    rhs[0] = fpa;
+    if (fixed_ends) {
+        diag[0] = 1.0;
+        up[0] = 0.0;
+        rhs[0] = fpa;
+    } else {
+        diag[0] = l1l1 * hx[0];
+        up[0] = l1r1 * hx[0];
+        rhs[0] = 2 * (pl[0] - fx[0] * l0l1 - fx[1] * l1r0);
+    }
     for (int i = 1; i < n; ++i) {
         lo[i] = l1r1 * hx[i - 1];
         diag[i] = r1r1 * hx[i - 1] + l1l1 * hx[i];
         up[i] = l1r1 * hx[i];
         rhs[i] = 2 * (pr[i - 1] - fx[i - 1] * l0r1 - fx[i] * r0r1) + 2 * (pl[i] - fx[i] * l0l1 - fx[i + 1] * l1r0);
     }
-    lo[n] = 0.0;
-    diag[n] = 1.0;
-    rhs[n] = fpb;
+    if (fixed_ends) {
+        lo[n] = 0.0;
+        diag[n] = 1.0;
+        rhs[n] = fpb;
+    } else {
+        lo[n] = l1r1 * hx[n - 1];
+        diag[n] = r1r1 * hx[n - 1];
+        rhs[n] = 2 * (pr[n - 1] - fx[n - 1] * l0r1 - fx[n] * r0r1);
+    }
     for (int i = 1; i <= n; ++i) {  // forward elimination
         const double m = lo[i] / diag[i - 1];
         diag[i] = diag[i] - m * up[i - 1];
@@ -123,14 +139,18 @@ void solve_node_slopes(const ScalarFn &f, double fpa, double fpb, int n, const f
 
 /* Fills the n interval chunks at c (each kChunk floats) for the nodes xi and
  * returns the largest interval error relative to max(|V|, 1) through err. If
- * c64 is not null it receives the same coefficients before rounding to float. */
+ * c64 is not null it receives the same coefficients before rounding to float.
+ * An empty fprime selects the free-end slope solve. */
 void fit_intervals(const ScalarFn &f, const ScalarFn &fprime, const float *xi, int n, float *c, double *c64,
                    float *err) {
     const std::vector<float> &ck = cheb_cos_table();
     std::vector<double> fnode(n + 1), slope(n + 1);
     double samples[kSamples];
     for (int k = 0; k <= n; ++k) fnode[k] = f(xi[k]);
-    solve_node_slopes(f, fprime(xi[0]), fprime(xi[n]), n, xi, slope.data());
+    if (fprime)
+        solve_node_slopes(f, true, fprime(xi[0]), fprime(xi[n]), n, xi, slope.data());
+    else
+        solve_node_slopes(f, false, 0.0, 0.0, n, xi, slope.data());
 
     *err = 0.0f;
     for (int i = 0; i < n; ++i) {
@@ -527,6 +547,24 @@ int make_harmonic(PotentialTable &p, double k, double r0, double min, double max
     return build_table(p, f, fp, f6, (float)min, (float)max, (float)tol);
 }
 
+int make_harmonic_angle(PotentialTable &p, double k, double theta0, double min, double max, double tol) {
+    p = PotentialTable();
+    p.flags = kFlagAngle | kFlagHarmonic;
+    // V(c) = k (acos(c) - theta0)^2 in the cosine c, fitted without an analytic
+    // derivative (MxPotential.cpp:519-540, 557-594)
+    ScalarFn f = [k, theta0](double r) {
+        r = std::fmin(1.0, std::fmax(-1.0, r));
+        const double theta = std::acos(r);
+        return k * (theta - theta0) * (theta - theta0);
+    };
+    ScalarFn f6 = [](double) { return 0.0; };
+    if (min < 0.0) min = 0.0;
+    if (max > M_PI) max = M_PI;
+    p.params = {k, theta0, min, max, tol};
+    p.form = kFormHarmonicAngle;
+    return build_table(p, f, ScalarFn(), f6, (float)std::cos(max), (float)std::cos(min), (float)tol);
+}
+
 int make_power(PotentialTable &p, double k, double r0, double alpha, double a, double b, double tol) {
     p = PotentialTable();
     p.flags = kFlagR2 | kFlagScaled;
@@ -561,6 +599,22 @@ int make_dpd(PotentialTable &p, double alpha, double gamma, double sigma, double
     if (shifted) p.flags |= kFlagShifted;
     p.params = {alpha, gamma, sigma, cutoff, shifted ? 1.0 : 0.0};
     return 0;
+}
+
+/* Scalar evaluation with the reference's potential_eval_r semantics
+ * (potential_eval.hpp:180-207): the table at r itself, f = dV/dr. */
+void eval_r(const PotentialTable &p, float r, float *e, float *f) {
+    const int ind = (int)std::max(0.0f, p.alpha[0] + r * (p.alpha[1] + r * p.alpha[2]));
+    const float *c = p.c.data() + std::min(ind, p.n) * kChunk;
+    const float x = (r - c[0]) * c[1];
+    float ee = c[2] * x + c[3];
+    float eff = c[2];
+    for (int k = 4; k < kChunk; ++k) {
+        eff = eff * x + ee;
+        ee = ee * x + c[k];
+    }
+    *e = ee;
+    *f = eff * c[1];
 }
 
 /* Scalar evaluation with the reference's potential_eval_ex semantics. */

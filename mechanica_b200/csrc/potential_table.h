@@ -15,6 +15,7 @@ enum : uint32_t {
     kFlagLJ126 = 1u << 0,
     kFlagR2 = 1u << 4,
     kFlagR = 1u << 5,
+    kFlagAngle = 1u << 6,
     kFlagHarmonic = 1u << 7,
     kFlagScaled = 1u << 11,
     kFlagShifted = 1u << 12,
@@ -37,7 +38,8 @@ struct PotentialTable {
     std::vector<float> nodes;    // the fit's n+1 interval nodes (stretched domain)
 };
 
-enum : int { kFormNone = 0, kFormLJ126 = 1, kFormMorse = 2, kFormHarmonic = 3, kFormPower = 4 };
+enum : int { kFormNone = 0, kFormLJ126 = 1, kFormMorse = 2, kFormHarmonic = 3, kFormPower = 4,
+             kFormHarmonicAngle = 5 };
 
 /* Frozen-node re-fit: the table of p's analytic form at new parameters, on p's
  * nodes and interval map (same n), so the coefficients depend linearly on the
@@ -55,7 +57,10 @@ int make_lj126(PotentialTable &p, double a, double b, double A, double B, double
 int make_morse(PotentialTable &p, double d, double alpha, double r0, double min, double max, double tol);
 int make_harmonic(PotentialTable &p, double k, double r0, double min, double max, double tol);
 int make_power(PotentialTable &p, double k, double r0, double alpha, double a, double b, double tol);
+/* k (acos(c) - theta0)^2 on cos(max) <= c <= cos(min), with min clipped to >= 0 and max to <= pi. */
+int make_harmonic_angle(PotentialTable &p, double k, double theta0, double min, double max, double tol);
 int make_dpd(PotentialTable &p, double alpha, double gamma, double sigma, double cutoff, bool shifted);
 bool eval_ex(const PotentialTable &p, float ri, float rj, float r2, float *e, float *f);
+void eval_r(const PotentialTable &p, float r, float *e, float *f);
 
 }  // namespace mxg

@@ -120,6 +120,52 @@ def lattice(nx=32, spacing=0.5, seed=3, dt=0.005, pull=0.05, dissociation=2.0, k
                 bi=bi, bj=bj, bond_pot=("harmonic", (k, spacing, 0.1, 1.0, 0.009)), dissociation=dissociation)
 
 
+def chains(nchains=64, length=32, bond=0.5, L=8.0, seed=5, dt=0.002, k_bond=100.0, k_angle=5.0, theta0=2.0,
+           pair=None, cut=1.0, temperature=0.1):
+    """Bead-spring chains in a periodic cube: harmonic bonds between consecutive
+    beads (k_bond (r - bond)^2, never breaking) and harmonic angles on
+    consecutive triples (k_angle (theta - theta0)^2, vertex at the middle bead).
+    Chains are random walks with bond-length steps whose turning angle stays
+    near pi - theta0, wrapped into the box, so bonds and angles cross the
+    periodic faces. pair: None (bonded forces only) or the parameters of a Morse
+    potential bound on the bead type. Newtonian, mass 1."""
+    rng = np.random.default_rng(seed)
+    xs = []
+    for _ in range(nchains):
+        p = rng.uniform(0, L, size=3)
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        pts = [p]
+        for _ in range(length - 1):
+            # turn by pi - theta0 (jittered) about a random axis perpendicular to d
+            ax = np.cross(d, rng.normal(size=3))
+            ax /= np.linalg.norm(ax)
+            turn = (np.pi - theta0) + rng.normal(0, 0.15)
+            d = d * np.cos(turn) + np.cross(ax, d) * np.sin(turn)
+            d /= np.linalg.norm(d)
+            p = p + bond * (1 + rng.normal(0, 0.05)) * d
+            pts.append(p)
+        xs.append(np.array(pts))
+    x = np.mod(np.concatenate(xs), L)
+    x = np.minimum(x, L * (1 - 1e-6)).astype(np.float32).astype(np.float64)
+    n = len(x)
+    idx = np.arange(n).reshape(nchains, length)
+    bi = idx[:, :-1].ravel().astype(np.int32)
+    bj = idx[:, 1:].ravel().astype(np.int32)
+    ai = idx[:, :-2].ravel().astype(np.int32)
+    aj = idx[:, 1:-1].ravel().astype(np.int32)
+    ak = idx[:, 2:].ravel().astype(np.int32)
+    v = rng.normal(0, np.sqrt(temperature), size=(n, 3))
+    v -= v.mean(axis=0)
+    cells = int(L // cut)
+    pots = [] if pair is None else [("morse", tuple(pair), 0, 0)]
+    return dict(dim=[L, L, L], cells=[cells] * 3, cutoff=cut, dt=dt, bc=("periodic", "periodic", "periodic"),
+                types=[(1.0, 0.25, m.Newtonian)], pots=pots, forces=[], x=x, v=v, t=np.zeros(n, dtype=np.int32),
+                bi=bi, bj=bj, bond_pot=("harmonic", (k_bond, bond, 0.1, 1.0, 0.009)),
+                dissociation=float(np.finfo(np.float64).max),
+                ai=ai, aj=aj, ak=ak, angle_pot=("harmonic_angle", (k_angle, theta0, 0.0, np.pi, 0.005 * np.pi)))
+
+
 def morse2(n=4000, density=0.8, seed=4, dt=0.01, d=(0.6, 0.3, 0.8), cut=2.5):
     rng = np.random.default_rng(seed)
     L = (n / density) ** (1.0 / 3.0)
@@ -147,6 +193,8 @@ def make_potential(kind, params):
         return m.Potential.power(*params)
     if kind == "dpd":
         return m.Potential.dpd(*params[:4], shifted=bool(params[4]) if len(params) > 4 else False)
+    if kind == "harmonic_angle":
+        return m.Potential.harmonic_angle(*params)
     raise ValueError(kind)
 
 
@@ -170,6 +218,8 @@ def build_gpu(scn, rng_mode="reference"):
     if "bi" in scn and len(scn["bi"]):
         kind, params = scn["bond_pot"]
         u._add_bonds(make_potential(kind, params), scn["bi"], scn["bj"], scn["dissociation"])
+    if "ai" in scn and len(scn["ai"]):
+        u._add_angles(make_potential(*scn["angle_pot"]), scn["ai"], scn["aj"], scn["ak"])
     return u
 
 

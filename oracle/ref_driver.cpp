@@ -18,6 +18,7 @@
  *   mxref_bind_force      MxConstantForce + engine_add_singlebody_force
  *                         (src/mdcore/src/MxForce.cpp:508-519, engine.cpp:983-1003)
  *   mxref_add_bonds       _bond_init (src/mdcore/src/bond.cpp:497-529)
+ *   mxref_add_angles      angle_init (src/mdcore/src/angle.cpp:659-707)
  *   mxref_step            engine_step (src/mdcore/src/engine.cpp:1198)
  *   mxref_force           engine_force (src/mdcore/src/engine.cpp:1230)
  * The engine is a process-wide singleton in the reference, so one process
@@ -30,12 +31,14 @@
 #include "DissapativeParticleDynamics.hpp"
 #include "potential_eval.hpp"
 #include "bond.h"
+#include "angle.h"
 #include "task.h"
 #include "MxForce.h"
 #include "../../rendering/NOMStyle.hpp"
 #include <vector>
 
 extern PyTypeObject MxConstantForce_Type;
+extern PyTypeObject MxAngle_Type;
 MxPotential *potential_create_morse(double d, double a, double r0, double min, double max, double tol);
 MxPotential *potential_create_power(double k, double r0, double alpha, double a, double b, double tol);
 
@@ -121,6 +124,10 @@ void *mxref_potential_morse(double d, double a, double r0, double min, double ma
 }
 void *mxref_potential_harmonic(double k, double r0, double min, double max, double tol) {
     return potential_create_harmonic(min, max, k, r0, tol);
+}
+/* Potential.harmonic_angle(k, theta0, min, max, tol) (MxPotential.cpp:2577-2590) */
+void *mxref_potential_harmonic_angle(double k, double theta0, double min, double max, double tol) {
+    return potential_create_harmonic_angle(min, max, k, theta0, tol);
 }
 void *mxref_potential_power(double k, double r0, double alpha, double min, double max, double tol) {
     return potential_create_power(k, r0, alpha, min, max, tol);
@@ -229,6 +236,26 @@ int mxref_add_bonds(int n, const int *pi, const int *pj, void *pot, double disso
     }
     return 0;
 }
+
+/* Angle(potential, p1, p2, p3) (src/mdcore/src/angle.cpp:659-707): an engine-owned
+ * record from engine_angle_alloc (engine_bonded.cpp:1087-1129) holding the three
+ * ids and the potential. */
+int mxref_add_angles(int n, const int *pi, const int *pj, const int *pk, void *pot) {
+    if (PyType_Ready(&MxAngle_Type) < 0) return -1;
+    for (int k = 0; k < n; ++k) {
+        MxAngle *a = NULL;
+        int rc = engine_angle_alloc(&_Engine, &MxAngle_Type, &a);
+        if (rc < 0) return rc;
+        a->i = pi[k];
+        a->j = pj[k];
+        a->k = pk[k];
+        a->potential = (MxPotential *)pot;
+    }
+    return 0;
+}
+
+/* The angle part of the last bonded pass (s->epot_angle, engine_bonded.cpp:1525-1528). */
+double mxref_epot_angle(void) { return _Engine.s.epot_angle; }
 
 int mxref_start(int nr_runners) { return engine_start(&_Engine, nr_runners, nr_runners); }
 

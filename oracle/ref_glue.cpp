@@ -4,13 +4,13 @@
  * TEST INFRASTRUCTURE ONLY. Nothing in the product links or loads this.
  *
  * The reference's hot-path translation units (space, runners, pair loops,
- * integrator, bonds, potentials) are compiled unmodified from the reference
- * checkout. They reference a handful of symbols that live in subsystems that
- * are outside the force-and-step path (rendering styles, clusters, fluxes,
- * events, timers, rigid constraints, angles/dihedrals/exclusions, Verlet
- * lists). This file defines those symbols as inert stand-ins so the engine
- * links; none of them is reached by the configurations the oracle runs
- * (no clusters, fluxes, angles, dihedrals, exclusions, rigids or events).
+ * integrator, bonds, angles, potentials) are compiled unmodified from the
+ * reference checkout. They reference a handful of symbols that live in
+ * subsystems that are outside the force-and-step path (rendering styles,
+ * clusters, fluxes, events, timers, rigid constraints, dihedrals/exclusions,
+ * Verlet lists). This file defines those symbols as inert stand-ins so the
+ * engine links; none of them is reached by the configurations the oracle runs
+ * (no clusters, fluxes, dihedrals, exclusions, rigids or events).
  */
 #include <random>
 
@@ -40,7 +40,6 @@ double MxWallTime() { return 0.0; }
 
 extern "C" int exclusion_eval(struct exclusion *, int, struct engine *, double *) { return 0; }
 extern "C" int dihedral_eval(struct dihedral *, int, struct engine *, double *) { return 0; }
-int angle_eval(struct MxAngle *, int, struct engine *, double *) { return 0; }
 int engine_rigid_eval(struct engine *) { return 0; }
 extern "C" int runner_verlet_fill(struct runner *, struct space_cell *, struct space_cell *, FPTYPE *) { return 0; }
 extern "C" int runner_verlet_eval(struct runner *, struct space_cell *, FPTYPE *) { return 0; }
@@ -72,15 +71,15 @@ int MxParticle_Check(PyObject *) { return 0; }
 /* MxRandomVector (src/mdcore/src/MxParticle.cpp:1782-1793, a file this build
  * does not compile): a normal magnitude N(mean, std) in a uniformly random
  * direction, restated with the same construction on a default-seeded mt19937
- * standing in for carbon's global generator (the random-force tests compare
+ * as carbon's global generator (the random-force tests compare
  * statistics, not draws). */
-static std::mt19937 g_random;
+std::mt19937 CRandom;
 Magnum::Vector3 MxRandomVector(float mean, float std) {
     std::normal_distribution<> dist{mean, std};
     std::uniform_real_distribution<double> uniform01(0.0, 1.0);
-    float theta = 2 * M_PI * uniform01(g_random);
-    float phi = acos(1 - 2 * uniform01(g_random));
-    float r = dist(g_random);
+    float theta = 2 * M_PI * uniform01(CRandom);
+    float phi = acos(1 - 2 * uniform01(CRandom));
+    float r = dist(CRandom);
     return Magnum::Vector3{r * sinf(phi) * cosf(theta), r * sinf(phi) * sinf(theta), r * cosf(phi)};
 }
 MxBody::MxBody() {}

@@ -10,10 +10,14 @@
 #include <string>
 #include <stdexcept>
 #include <iostream>
+#include <random>
 
 #define CAPI_FUNC(RTYPE) RTYPE
 #define CAPI_DATA(RTYPE) extern RTYPE
 #define CAPI_STRUCT(NAME) struct NAME
+
+/* carbon's process-wide generator (defined in ref_glue.cpp) */
+extern std::mt19937 CRandom;
 
 typedef int32_t HRESULT;
 #define S_OK ((HRESULT)0)

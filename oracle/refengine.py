@@ -14,6 +14,7 @@ A scenario is a dict:
     pots [(kind, params, ti, tj)] with kind in lj126/morse/harmonic/power/dpd,
     forces [(type, fx, fy, fz)], x (N,3) float64, v (N,3), t (N,) int,
     bonds (optional): bi, bj, bond_pot (kind, params), dissociation,
+    angles (optional): ai, aj, ak (vertex aj), angle_pot ("harmonic_angle", (k, theta0, min, max, tol)),
     action: "force" | "steps", nsteps, runners (threads), time_it (bool),
     integrator (0 forward Euler, 1 Runge-Kutta 4),
     sbforces [(type, "berendsen" | "random" | "friction", params)] with the forces module's
@@ -21,7 +22,7 @@ A scenario is a dict:
     friction(coef, std, mean, durration) (MxForce.cpp:213-259),
     target_temperature {type: T}
 Results: xabs, xrel, v, f, cell (per id), tasks (rows type, sid, i, j),
-    cdim, h, epot, ekin, bond_flags, seconds (wall time of the steps).
+    cdim, h, epot, epot_angle, ekin, bond_flags, seconds (wall time of the steps).
 """
 import ctypes
 import os
@@ -43,7 +44,7 @@ def available():
 def _pack(scn):
     flat = {}
     for k, v in scn.items():
-        if k in ("types", "pots", "forces", "bond_pot", "bc", "sbforces", "target_temperature"):
+        if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "bc", "sbforces", "target_temperature"):
             flat[k] = np.array(repr(v))
         else:
             flat[k] = np.asarray(v)
@@ -54,7 +55,7 @@ def _unpack(npz):
     out = {}
     for k in npz.files:
         v = npz[k]
-        if k in ("types", "pots", "forces", "bond_pot", "bc", "sbforces", "target_temperature"):
+        if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "bc", "sbforces", "target_temperature"):
             out[k] = eval(str(v))  # written by _pack from plain literals
         elif v.shape == ():
             out[k] = v.item()
@@ -89,7 +90,7 @@ def _execute(scn):
     L.mxref_add_type.argtypes = [cd, cd, ci]
     L.mxref_add_particles.argtypes = [ci, P(cd), P(cd), P(ci)]
     for fn, n in (("mxref_potential_lj126", 5), ("mxref_potential_morse", 6), ("mxref_potential_harmonic", 5),
-                  ("mxref_potential_power", 6)):
+                  ("mxref_potential_power", 6), ("mxref_potential_harmonic_angle", 5)):
         getattr(L, fn).restype = vp
         getattr(L, fn).argtypes = [cd] * n
     L.mxref_potential_dpd.restype = vp
@@ -121,7 +122,7 @@ def _execute(scn):
     def make_pot(kind, params):
         fn = {"lj126": L.mxref_potential_lj126, "morse": L.mxref_potential_morse,
               "harmonic": L.mxref_potential_harmonic, "power": L.mxref_potential_power,
-              "dpd": L.mxref_potential_dpd}[kind]
+              "harmonic_angle": L.mxref_potential_harmonic_angle, "dpd": L.mxref_potential_dpd}[kind]
         if kind == "dpd":
             return fn(*[float(p) for p in params[:4]], int(params[4]) if len(params) > 4 else 0)
         return fn(*[float(p) for p in params])
@@ -155,6 +156,12 @@ def _execute(scn):
         bp = make_pot(*scn["bond_pot"])
         keep.append(bp)
         L.mxref_add_bonds(len(scn["bi"]), a(scn["bi"], ci), a(scn["bj"], ci), bp, float(scn["dissociation"]))
+    if "ai" in scn and len(scn["ai"]):
+        ap = make_pot(*scn["angle_pot"])
+        keep.append(ap)
+        L.mxref_add_angles.argtypes = [ci, P(ci), P(ci), P(ci), vp]
+        if L.mxref_add_angles(len(scn["ai"]), a(scn["ai"], ci), a(scn["aj"], ci), a(scn["ak"], ci), ap) != 0:
+            raise RuntimeError("mxref_add_angles")
     L.mxref_start(int(scn.get("runners", 1)))
     t0 = time.perf_counter()
     if scn.get("action", "force") == "force":
@@ -202,6 +209,8 @@ def _execute(scn):
     out["epot_nonbond"] = np.float64(e[1].value)
     out["epot_bond"] = np.float64(e[2].value)
     out["ekin"] = np.float64(e[3].value)
+    L.mxref_epot_angle.restype = cd
+    out["epot_angle"] = np.float64(L.mxref_epot_angle())
     return out
 
 

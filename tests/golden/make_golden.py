@@ -33,6 +33,10 @@ CASES = [
     # bond lengths spread around the break threshold: one force pass on
     # identical inputs decides the flags
     ("lattice_noisy", lambda: S.lattice(nx=8, seed=17, noise=5e-3), 1),
+    # bead-spring chains with harmonic angles: bonded forces only (bit-exact
+    # forces and trajectories), and with a Morse pair potential
+    ("chains_bonded", lambda: S.chains(nchains=16, length=24, seed=21), 10),
+    ("chains_morse", lambda: S.chains(nchains=16, length=24, seed=22, pair=(0.2, 6.0, 0.5, 1e-4, 1.0, 1e-3)), 10),
 ]
 
 TABLES = [
@@ -44,6 +48,8 @@ TABLES = [
     ("harmonic_lattice", "harmonic", (200.0, 0.5, 0.1, 1.0, 0.009)),
     ("harmonic_unit", "harmonic", (1.0, 1.0, 0.2, 2.0, 0.018)),
     ("power_sq", "power", (1.0, 1.0, 2.0, 0.1, 3.0, 1e-3)),
+    ("angle_default", "harmonic_angle", (5.0, 2.0, 0.0, 3.141592653589793, 0.005 * 3.141592653589793)),
+    ("angle_narrow", "harmonic_angle", (20.0, 1.9, 1.0, 2.8, 0.009)),
 ]
 
 
@@ -94,7 +100,7 @@ def make_tables():
 def scenario_arrays(scn):
     d = {}
     for k, v in scn.items():
-        if k in ("types", "pots", "forces", "bond_pot", "bc"):
+        if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "bc"):
             d["scn_" + k] = np.array(repr(v))
         else:
             d["scn_" + k] = np.asarray(v)
@@ -106,7 +112,7 @@ def make_case(name, factory, nsteps):
     f1 = refengine.run(dict(scn, action="force", runners=1))
     tr = refengine.run(dict(scn, action="steps", nsteps=nsteps, runners=1))
     out = scenario_arrays(scn)
-    for k in ("f", "cell", "xrel", "epot", "ekin", "tasks", "cdim", "h", "bond_flags"):
+    for k in ("f", "cell", "xrel", "epot", "ekin", "tasks", "cdim", "h", "bond_flags", "epot_angle"):
         out["force_" + k] = f1[k]
     for k in ("xrel", "xabs", "v", "cell", "epot", "ekin", "bond_flags"):
         out["traj_" + k] = tr[k]
@@ -125,7 +131,7 @@ def load_scenario(z):
             continue
         v = z[k]
         key = k[4:]
-        if key in ("types", "pots", "forces", "bond_pot", "bc"):
+        if key in ("types", "pots", "forces", "bond_pot", "angle_pot", "bc"):
             scn[key] = eval(str(v))  # plain literals written by scenario_arrays
         elif v.shape == ():
             scn[key] = v.item()
@@ -135,7 +141,11 @@ def load_scenario(z):
 
 
 if __name__ == "__main__":
-    make_tables()
+    # no arguments: everything; otherwise the named cases ("tables" for the tables)
+    want = set(sys.argv[1:])
+    if not want or "tables" in want:
+        make_tables()
     for name, fac, ns in CASES:
-        make_case(name, fac, ns)
-        print("wrote", name)
+        if not want or name in want:
+            make_case(name, fac, ns)
+            print("wrote", name)

@@ -81,10 +81,15 @@ def test_tables_random_parameters_live():
         cases.append(("lj126", (lo, float(rng.uniform(1.0, 3.0)), A, B, 1e-3)))
         k, r0 = float(rng.uniform(1, 300)), float(rng.uniform(0.3, 1.5))
         cases.append(("harmonic", (k, r0, 0.2 * r0, 2 * r0, 0.018 * r0)))
+        lo, hi = float(rng.uniform(0.0, 1.2)), float(rng.uniform(2.0, 3.4))
+        cases.append(("harmonic_angle", (float(rng.uniform(0.5, 50)), float(rng.uniform(lo, hi)), lo, hi,
+                                         0.005 * (hi - lo))))
     for kind, params in cases:
         info, coef = reference_table(kind, params)
         p = S.make_potential(kind, params)
         mine = p._info()
         assert mine["n"] == info["n"], (kind, params)
+        assert mine["flags"] == info["flags"], (kind, params)
+        assert np.float32(mine["a"]) == np.float32(info["a"]) and np.float32(mine["b"]) == np.float32(info["b"])
         assert np.array_equal(_bits(mine["alpha"][:3]), _bits(info["alpha"])), (kind, params)
         assert np.array_equal(_bits(p.coefficients), _bits(coef)), (kind, params)
