@@ -10,6 +10,7 @@
  *   mxg_potential_create_harmonic  potential_create_harmonic src/mdcore/src/MxPotential.cpp:335
  *   mxg_potential_create_power     potential_create_power   src/mdcore/src/MxPotential.cpp:1614
  *   mxg_potential_create_harmonic_angle potential_create_harmonic_angle src/mdcore/src/MxPotential.cpp:557
+ *   mxg_potential_create_harmonic_dihedral potential_create_harmonic_dihedral src/mdcore/src/MxPotential.cpp:484
  *   mxg_potential_create_dpd       DPDPotential_New         src/mdcore/src/DissapativeParticleDynamics.cpp:134
  *   mxg_potential_eval             potential_eval_ex        src/mdcore/src/potential_eval.hpp:106
  *   mxg_engine_init                engine_init              src/mdcore/include/engine.h:600
@@ -19,6 +20,8 @@
  *   mxg_engine_addparts            engine_addpart           src/mdcore/src/engine.cpp:1726
  *   mxg_engine_addbonds            engine_bond_alloc + _bond_init src/mdcore/src/bond.cpp:497
  *   mxg_engine_addangles           engine_angle_alloc + angle_init src/mdcore/src/angle.cpp:659-707
+ *   mxg_engine_adddihedrals        engine_dihedral_addpot + engine_dihedral_add
+ *                                  src/mdcore/src/engine_bonded.cpp:1049-1080, 1967-1991
  *   mxg_engine_start               engine_start             src/mdcore/include/engine.h:640
  *   mxg_engine_step                engine_step              src/mdcore/src/engine.cpp:1198
  *   mxg_engine_force               engine_force             src/mdcore/src/engine.cpp:1230
@@ -111,6 +114,10 @@ int mxg_potential_create_power(double k, double r0, double alpha, double min, do
  * src/mdcore/src/MxPotential.cpp:2577-2590, 557-594). */
 int mxg_potential_create_harmonic_angle(double k, double theta0, double min, double max, double tol,
                                         mxg_potential **out);
+/* k (1 + cos(n phi - delta)) tabulated in c = cos(phi) on [-1, 1] (pulled in by sqrt(FLT_EPSILON) when
+ * delta is not a multiple of pi), n >= 1, fitted without an analytic derivative
+ * (Potential.harmonic_dihedral, src/mdcore/src/MxPotential.cpp:2595-2607, 423-516). */
+int mxg_potential_create_harmonic_dihedral(double k, int n, double delta, double tol, mxg_potential **out);
 int mxg_potential_create_dpd(double alpha, double gamma, double sigma, double cutoff, int shifted,
                              mxg_potential **out);
 /* Table description: kind, flags, intervals n, interval map alpha[4], domain [a,b], r0+1. */
@@ -209,6 +216,11 @@ int mxg_engine_addbonds(mxg_engine *e, int n, const int *i, const int *j, const 
  * the energy. ids_out receives consecutive angle indices (may be NULL). */
 int mxg_engine_addangles(mxg_engine *e, int n, const int *i, const int *j, const int *k, const mxg_potential *p,
                          int *ids_out);
+/* Adds n dihedrals i[q]-j[q]-k[q]-l[q], all with table potential p in cos(phi), evaluated each force pass
+ * after the angles as dihedral_eval does (src/mdcore/src/dihedral.cpp:81-392): the forces on i, j and l
+ * are balanced on k, which carries the energy. ids_out receives consecutive dihedral indices (may be NULL). */
+int mxg_engine_adddihedrals(mxg_engine *e, int n, const int *i, const int *j, const int *k, const int *l,
+                            const mxg_potential *p, int *ids_out);
 /* Builds the cell-pair lists and uploads the state. stream may be NULL (default stream). */
 int mxg_engine_start(mxg_engine *e, void *cuda_stream);
 /* Runs nsteps forward-Euler steps on the device (forces, bonds, integrate, re-bin). */

@@ -27,7 +27,7 @@ from . import _native
 from ._native import EngineError, check, f32, f64, i32, lib, ptr
 
 __all__ = [
-    "init", "Universe", "universe", "Particle", "Potential", "Bond", "Angle", "bind", "forces", "step", "run",
+    "init", "Universe", "universe", "Particle", "Potential", "Bond", "Angle", "Dihedral", "bind", "forces", "step", "run",
     "Newtonian", "Overdamped", "FORWARD_EULER", "RUNGE_KUTTA_4", "BOUNDARY_NONE", "PERIODIC_X", "PERIODIC_Y", "PERIODIC_Z",
     "PERIODIC_FULL", "FREESLIP_X", "FREESLIP_Y", "FREESLIP_Z", "FREESLIP_FULL", "EngineError",
 ]
@@ -158,6 +158,11 @@ class Potential:
         """k (theta - theta0)^2, tabulated in cos(theta) (MxPotential.cpp:2577-2590)."""
         tol = 0.005 * abs(max - min) if tol is None else tol
         return Potential._make("mxg_potential_create_harmonic_angle", (k, theta0, min, max, tol), "Harmonic Angle")
+
+    @staticmethod
+    def harmonic_dihedral(k, n, delta, tol=0.001):
+        """k (1 + cos(n phi - delta)), tabulated in cos(phi) (MxPotential.cpp:2595-2607)."""
+        return Potential._make("mxg_potential_create_harmonic_dihedral", (k, int(n), delta, tol), "Harmonic Dihedral")
 
     @staticmethod
     def power(k=1.0, r0=1.0, alpha=1.0, min=None, max=None, tol=None):
@@ -319,6 +324,22 @@ class Angle:
         self.potential = potential
 
 
+class Dihedral:
+    """A dihedral p1-p2-p3-p4 with a potential in cos(phi) between the planes
+    (p1, p2, p3) and (p2, p3, p4), evaluated every force pass after the angles
+    (dihedral_eval, dihedral.cpp:81-392). The reference reaches dihedrals through
+    engine_dihedral_addpot / engine_dihedral_add (engine_bonded.cpp:1049-1080,
+    1967-1991) and its file readers; it has no Python constructor for them."""
+
+    def __init__(self, potential, p1, p2, p3, p4):
+        if not isinstance(potential, Potential):
+            raise TypeError("potential is not a instance of Potential")
+        u = _require()
+        self.i, self.j, self.k, self.l = _pid(p1), _pid(p2), _pid(p3), _pid(p4)
+        self.id = u._add_dihedrals(potential, [self.i], [self.j], [self.k], [self.l])[0]
+        self.potential = potential
+
+
 def _pid(p):
     return p.id if isinstance(p, Particle) else int(p)
 
@@ -398,6 +419,7 @@ class _Universe:
         self._targets = {}      # type -> target temperature
         self._bonds = []        # (potential, i[], j[], dissociation)
         self._angles = []       # (potential, i[], j[], k[])
+        self._dihedrals = []    # (potential, i[], j[], k[], l[])
         self._x = np.zeros((0, 3))
         self._v = np.zeros((0, 3), dtype=np.float32)
         self._t = np.zeros(0, dtype=np.int32)
@@ -454,6 +476,10 @@ class _Universe:
         for (p, ii, jj, kk) in self._angles:
             check(lib().mxg_engine_addangles(self._e, len(ii), ptr(ii, ctypes.c_int), ptr(jj, ctypes.c_int),
                                              ptr(kk, ctypes.c_int), p._h, None), "addangles")
+        for (p, ii, jj, kk, ll) in self._dihedrals:
+            check(lib().mxg_engine_adddihedrals(self._e, len(ii), ptr(ii, ctypes.c_int), ptr(jj, ctypes.c_int),
+                                                ptr(kk, ctypes.c_int), ptr(ll, ctypes.c_int), p._h, None),
+                  "adddihedrals")
         self._started = False
 
     def _add_type(self, cls):
@@ -502,6 +528,14 @@ class _Universe:
         ii, jj, kk = i32(i), i32(j), i32(k)
         first = sum(len(a[1]) for a in self._angles)
         self._angles.append((pot, ii, jj, kk))
+        self._sync_state()
+        self._dirty = True
+        return list(range(first, first + len(ii)))
+
+    def _add_dihedrals(self, pot, i, j, k, l):
+        ii, jj, kk, ll = i32(i), i32(j), i32(k), i32(l)
+        first = sum(len(d[1]) for d in self._dihedrals)
+        self._dihedrals.append((pot, ii, jj, kk, ll))
         self._sync_state()
         self._dirty = True
         return list(range(first, first + len(ii)))

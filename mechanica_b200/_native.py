@@ -56,6 +56,8 @@ _SIGS = {
     "mxg_potential_create_harmonic": ([ctypes.c_double] * 5 + [_vpp], ctypes.c_int),
     "mxg_potential_create_power": ([ctypes.c_double] * 6 + [_vpp], ctypes.c_int),
     "mxg_potential_create_harmonic_angle": ([ctypes.c_double] * 5 + [_vpp], ctypes.c_int),
+    "mxg_potential_create_harmonic_dihedral": ([ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double, _vpp],
+                                               ctypes.c_int),
     "mxg_potential_create_dpd": ([ctypes.c_double] * 4 + [ctypes.c_int, _vpp], ctypes.c_int),
     "mxg_potential_info": ([_vp, _c_int_p, _c_uint_p, _c_int_p, _c_float_p, _c_float_p, _c_float_p, _c_float_p],
                            ctypes.c_int),
@@ -76,6 +78,8 @@ _SIGS = {
     "mxg_engine_addparts": ([_vp, ctypes.c_int, _c_double_p, _c_float_p, _c_int_p, _c_int_p], ctypes.c_int),
     "mxg_engine_addbonds": ([_vp, ctypes.c_int, _c_int_p, _c_int_p, _vp, ctypes.c_double, _c_int_p], ctypes.c_int),
     "mxg_engine_addangles": ([_vp, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p, _vp, _c_int_p], ctypes.c_int),
+    "mxg_engine_adddihedrals": ([_vp, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p, _c_int_p, _vp, _c_int_p],
+                                ctypes.c_int),
     "mxg_engine_start": ([_vp, _vp], ctypes.c_int),
     "mxg_engine_step": ([_vp, ctypes.c_int], ctypes.c_int),
     "mxg_engine_force": ([_vp], ctypes.c_int),

@@ -116,8 +116,15 @@ struct DevAngle {
     int pot;             // potential index (a table in cos(theta))
 };
 
+struct DevDihedral {
+    int i, j, k, l;      // particle ids; the k end carries the balancing force
+    int pot;             // potential index (a table in cos(phi))
+    int pad[3];
+};
+
 /* Bonded interactions, CSR by particle id. bond_list holds bond indices;
- * angle_list holds angle * 4 + role (0: i, 1: j, 2: k). */
+ * angle_list holds angle * 4 + role (0: i, 1: j, 2: k); dihedral_list holds
+ * dihedral * 4 + role (0: i, 1: j, 2: k, 3: l). */
 struct BondedView {
     const DevBond *bonds;
     unsigned *bond_flags;
@@ -126,6 +133,9 @@ struct BondedView {
     const DevAngle *angles;
     const int *angle_off;
     const int *angle_list;
+    const DevDihedral *dihedrals;
+    const int *dihedral_off;
+    const int *dihedral_list;
     const int *slot_of_id;
     double *e_slot;      // per slot: bonded energy of the last pass
 };

@@ -94,6 +94,10 @@ struct AngleInfo {
     int i, j, k, pot;
 };
 
+struct DihedralInfo {
+    int i, j, k, l, pot;
+};
+
 #define CUDA_TRY(x)                                                                              \
     do {                                                                                         \
         cudaError_t err_ = (x);                                                                  \
@@ -340,6 +344,7 @@ struct mxg_engine {
     std::vector<int> prep;                  // replica of each particle
     std::vector<BondInfo> bonds;
     std::vector<AngleInfo> angles;
+    std::vector<DihedralInfo> dihedrals;
 
     // ---- device ----
     bool started = false;
@@ -393,6 +398,8 @@ struct mxg_engine {
     int *d_bond_off = nullptr, *d_bond_list = nullptr;
     DevAngle *d_angles = nullptr;
     int *d_angle_off = nullptr, *d_angle_list = nullptr;
+    DevDihedral *d_dihedrals = nullptr;
+    int *d_dihedral_off = nullptr, *d_dihedral_list = nullptr;
     unsigned *d_status = nullptr;
     unsigned long long *d_step = nullptr;
     double *d_partials = nullptr, *d_energy = nullptr;
@@ -571,7 +578,7 @@ struct mxg_engine {
         return v;
     }
 
-    bool has_bonded() const { return !bonds.empty() || !angles.empty(); }
+    bool has_bonded() const { return !bonds.empty() || !angles.empty() || !dihedrals.empty(); }
 
     BondedView bonded_view() const {
         BondedView bv;
@@ -582,6 +589,9 @@ struct mxg_engine {
         bv.angles = d_angles;
         bv.angle_off = d_angle_off;
         bv.angle_list = d_angle_list;
+        bv.dihedrals = d_dihedrals;
+        bv.dihedral_off = d_dihedral_off;
+        bv.dihedral_list = d_dihedral_list;
         bv.slot_of_id = d_slot_of_id;
         bv.e_slot = d_ebond_slot;
         return bv;
@@ -922,6 +932,36 @@ int mxg_engine::start(cudaStream_t st) {
         }
     }
 
+    // ---- dihedrals: CSR by particle id, entries dihedral * 4 + role ----
+    std::vector<DevDihedral> hd;
+    std::vector<int> doff(nparts + 1, 0), dlist;
+    for (const DihedralInfo &d : dihedrals) {
+        const int ids[4] = {d.i, d.j, d.k, d.l};
+        for (int r = 0; r < 4; ++r) {
+            if (ids[r] < 0 || ids[r] >= nparts) return MXG_ERR_BOND;
+            if (prep[ids[r]] != prep[d.j]) return MXG_ERR_BOND;
+        }
+        for (int r = 0; r < 4; ++r) doff[ids[r] + 1]++;
+    }
+    for (int p = 0; p < nparts; ++p) doff[p + 1] += doff[p];
+    dlist.assign(doff[nparts], 0);
+    {
+        std::vector<int> fill(doff.begin(), doff.end() - 1);
+        for (int k = 0; k < (int)dihedrals.size(); ++k) {
+            const DihedralInfo &d = dihedrals[k];
+            const int ids[4] = {d.i, d.j, d.k, d.l};
+            for (int r = 0; r < 4; ++r) dlist[fill[ids[r]]++] = k * 4 + r;
+            DevDihedral dd;
+            memset(&dd, 0, sizeof(dd));
+            dd.i = d.i;
+            dd.j = d.j;
+            dd.k = d.k;
+            dd.l = d.l;
+            dd.pot = d.pot;
+            hd.push_back(dd);
+        }
+    }
+
     // ---- device allocation ----
     rc = MXG_OK;
     for (int b = 0; b < 2; ++b) {
@@ -968,6 +1008,9 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_angles, ha.size());
     rc |= alloc(&d_angle_off, aoff.size());
     rc |= alloc(&d_angle_list, alist.size());
+    rc |= alloc(&d_dihedrals, hd.size());
+    rc |= alloc(&d_dihedral_off, doff.size());
+    rc |= alloc(&d_dihedral_list, dlist.size());
     rc |= alloc(&d_status, 1);
     rc |= alloc(&d_step, 1);
     rc |= alloc(&d_partials, 2 * (size_t)energy_blocks);
@@ -997,7 +1040,8 @@ int mxg_engine::start(cudaStream_t st) {
         (rc = upload(d_bonds, hb, stream)) || (rc = upload(d_bond_flags, hbf, stream)) ||
         (rc = upload(d_bond_off, boff, stream)) || (rc = upload(d_bond_list, blist, stream)) ||
         (rc = upload(d_angles, ha, stream)) || (rc = upload(d_angle_off, aoff, stream)) ||
-        (rc = upload(d_angle_list, alist, stream)))
+        (rc = upload(d_angle_list, alist, stream)) || (rc = upload(d_dihedrals, hd, stream)) ||
+        (rc = upload(d_dihedral_off, doff, stream)) || (rc = upload(d_dihedral_list, dlist, stream)))
         return rc;
     CUDA_TRY(cudaStreamSynchronize(stream));
 
@@ -1093,6 +1137,13 @@ int mxg_potential_create_harmonic_angle(double k, double theta0, double min, dou
     if (!(max > min) || !(tol > 0)) return MXG_ERR_ARG;
     mxg_potential *p = new mxg_potential;
     return wrap_potential(make_harmonic_angle(p->t, k, theta0, min, max, tol), p, out);
+}
+
+int mxg_potential_create_harmonic_dihedral(double k, int n, double delta, double tol, mxg_potential **out) {
+    if (!out) return MXG_ERR_NULL;
+    if (n < 1 || !(tol > 0)) return MXG_ERR_ARG;
+    mxg_potential *p = new mxg_potential;
+    return wrap_potential(make_harmonic_dihedral(p->t, k, n, delta, tol), p, out);
 }
 
 int mxg_potential_create_power(double k, double r0, double alpha, double min, double max, double tol,
@@ -1423,6 +1474,20 @@ int mxg_engine_addangles(mxg_engine *e, int n, const int *i, const int *j, const
     for (int q = 0; q < n; ++q) {
         if (ids_out) ids_out[q] = (int)e->angles.size();
         e->angles.push_back({i[q], j[q], k[q], idx});
+    }
+    return MXG_OK;
+}
+
+int mxg_engine_adddihedrals(mxg_engine *e, int n, const int *i, const int *j, const int *k, const int *l,
+                            const mxg_potential *p, int *ids_out) {
+    if (!e || !p || (n > 0 && (!i || !j || !k || !l))) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    if (p->t.kind != kKindTable) return MXG_ERR_POTENTIAL;
+    e->pots.push_back(p->t);
+    const int idx = (int)e->pots.size() - 1;
+    for (int q = 0; q < n; ++q) {
+        if (ids_out) ids_out[q] = (int)e->dihedrals.size();
+        e->dihedrals.push_back({i[q], j[q], k[q], l[q], idx});
     }
     return MXG_OK;
 }

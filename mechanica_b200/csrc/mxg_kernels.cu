@@ -809,8 +809,91 @@ __device__ bool angle_terms(const EngineView &v, const BondedView &bv, int aid, 
 }
 
 /*
+ * The force terms of dihedral did exactly as dihedral_eval computes them
+ * (dihedral.cpp:81-392): positions relative to j's cell, the rays
+ * b1 = x_i - x_j, b2 = x_k - x_j, b3 = x_l - x_k, cos(phi) between the planes
+ * (i, j, k) and (j, k, l) and its derivatives with respect to x_i, x_j and x_l
+ * in the reference's expression order, the clamp to [-1, 1] and to the table's
+ * [a, b], and potential_eval_r on the cosine. Returns w = eff * dcos/dx for
+ * i, j and l (the k end receives the negated sum), or false when an id is
+ * absent.
+ */
+__device__ bool dihedral_terms(const EngineView &v, const BondedView &bv, int did, float wi[3], float wj[3],
+                               float wl[3], float &ee) {
+    const DevDihedral D = bv.dihedrals[did];
+    if (D.pot < 0) return false;
+    const int si = bv.slot_of_id[D.i], sj = bv.slot_of_id[D.j], sk = bv.slot_of_id[D.k], sl = bv.slot_of_id[D.l];
+    if (si < 0 || sj < 0 || sk < 0 || sl < 0) return false;
+    const int cj = v.cell_of[sj];
+    const DevSpace &S = v.spaces[v.cell_rep[cj]];
+    int loci[3], locj[3], lock[3], locl[3];
+    cell_loc(S, v.cell_of[si], loci);
+    cell_loc(S, cj, locj);
+    cell_loc(S, v.cell_of[sk], lock);
+    cell_loc(S, v.cell_of[sl], locl);
+    const float4 pi = v.pos[si], pj = v.pos[sj], pk = v.pos[sk], pl = v.pos[sl];
+    const float xiv[3] = {pi.x, pi.y, pi.z}, xj[3] = {pj.x, pj.y, pj.z};
+    const float xkv[3] = {pk.x, pk.y, pk.z}, xlv[3] = {pl.x, pl.y, pl.z};
+    float xi[3], xk[3], xl[3], b1[3], b2[3], b3[3];
+    for (int q = 0; q < 3; ++q) {
+        xi[q] = shifted(xiv[q], wrap_shift(loci[q] - locj[q]), S.hd[q]);
+        xk[q] = shifted(xkv[q], wrap_shift(lock[q] - locj[q]), S.hd[q]);
+        xl[q] = shifted(xlv[q], wrap_shift(locl[q] - locj[q]), S.hd[q]);
+        b1[q] = __fsub_rn(xi[q], xj[q]);
+        b2[q] = __fsub_rn(xk[q], xj[q]);
+        b3[q] = __fsub_rn(xl[q], xk[q]);
+    }
+#define M(a, b) __fmul_rn(a, b)
+#define A(a, b) __fadd_rn(a, b)
+#define S_(a, b) __fsub_rn(a, b)
+    const float n33 = dot3_rn(b3[0], b3[1], b3[2]);
+    const float n22 = dot3_rn(b2[0], b2[1], b2[2]);
+    const float n11 = dot3_rn(b1[0], b1[1], b1[2]);
+    const float d32 = A(A(M(b3[0], b2[0]), M(b3[1], b2[1])), M(b3[2], b2[2]));      // b3.b2
+    const float m12 = S_(S_(M(-b1[0], b2[0]), M(b1[1], b2[1])), M(b1[2], b2[2]));   // -b1.b2
+    const float m13 = S_(S_(M(-b1[0], b3[0]), M(b1[1], b3[1])), M(b1[2], b3[2]));   // -b1.b3
+    const float g23 = S_(M(n22, n33), M(d32, d32));  // |b2 x b3|^2
+    const float g12 = S_(M(n11, n22), M(m12, m12));  // |b1 x b2|^2
+    const float g = M(g12, g23);
+    const float rg = __fdiv_rn(1.0f, __fsqrt_rn(g));
+    const float cphi0 = M(S_(M(m12, d32), M(m13, n22)), rg);
+    const float m13x2 = M(2.0f, m13);
+    const float pa = M(g12, d32), pb = M(m12, g23), pc = M(g12, n33);
+    const float qv = S_(-m12, n22);
+    const float rgc = M(__fdiv_rn(1.0f, g), cphi0);
+    const float s23 = M(g23, rgc), s12 = M(g12, rgc);
+    float u[3], w[3], b1n[3], ddi[3], ddj[3], ddl[3];
+    for (int q = 0; q < 3; ++q) {
+        b1n[q] = M(b1[q], n22);
+        u[q] = A(M(-d32, b2[q]), M(b3[q], n22));   // (b3 n22 - d32 b2)
+        w[q] = A(M(m12, b2[q]), b1n[q]);          // (b1 n22 + m12 b2)
+    }
+    for (int q = 0; q < 3; ++q) {
+        const float t = A(S_(xk[q], M(2.0f, xj[q])), xi[q]);  // x_k - 2 x_j + x_i
+        ddi[q] = S_(M(u[q], rg), M(w[q], s23));
+        ddj[q] = S_(M(A(A(M(t, d32), M(b2[q], m13x2)), M(qv, b3[q])), rg),
+                    M(S_(A(A(M(-t, pb), M(b3[q], pa)), M(S_(-b1n[q], M(n11, b2[q])), g23)), M(b2[q], pc)), rgc));
+        ddl[q] = S_(M(w[q], rg), M(u[q], s12));
+    }
+#undef M
+#undef A
+#undef S_
+    float c = fmaxf(-1.0f, fminf(1.0f, cphi0));
+    const DevPot &p = v.pots[D.pot];
+    if (c < p.a || c > p.b) c = fmaxf(p.a, fminf(p.b, c));
+    float eff;
+    table_eval_r(p, v.coef, c, ee, eff);
+    for (int q = 0; q < 3; ++q) {
+        wi[q] = __fmul_rn(eff, ddi[q]);
+        wj[q] = __fmul_rn(eff, ddj[q]);
+        wl[q] = __fmul_rn(eff, ddl[q]);
+    }
+    return true;
+}
+
+/*
  * The bonded pass (engine_bonded_eval, engine_bonded.cpp:1373-1543: bonds,
- * then angles). One thread per particle slot; each thread evaluates every
+ * then angles, then dihedrals). One thread per particle slot; each thread evaluates every
  * bond and angle its particle takes part in and applies its own share, in the
  * bonded lists' index order, so its force receives the same sequence of
  * updates as in the reference's serial loops.
@@ -819,6 +902,8 @@ __device__ bool angle_terms(const EngineView &v, const BondedView &bv, int aid, 
  * of view; both ends compute the same force/r and the same break decision
  * eff >= dissociation_energy, and the first end clears the active flag.
  * Angles: f_i -= wi, f_k -= wk, f_j += wi + wk; the vertex carries the energy.
+ * Dihedrals: f_i -= wi, f_j -= wj, f_l -= wl, f_k += wi + wj + wl; the k end
+ * carries the energy.
  */
 __global__ void bonded_kernel(EngineView v, BondedView bv) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -884,6 +969,24 @@ __global__ void bonded_kernel(EngineView v, BondedView bv) {
             f.y = __fadd_rn(f.y, __fadd_rn(wi[1], wk[1]));
             f.z = __fadd_rn(f.z, __fadd_rn(wi[2], wk[2]));
             eb += (double)ee;
+        }
+    }
+    const int d0 = bv.dihedral_off[id], d1 = bv.dihedral_off[id + 1];
+    for (int k = d0; k < d1; ++k) {
+        const int code = bv.dihedral_list[k];
+        const int role = code & 3;
+        float wi[3], wj[3], wl[3], ee;
+        if (!dihedral_terms(v, bv, code >> 2, wi, wj, wl, ee)) continue;
+        if (role == 2) {
+            f.x = __fadd_rn(f.x, __fadd_rn(__fadd_rn(wi[0], wj[0]), wl[0]));
+            f.y = __fadd_rn(f.y, __fadd_rn(__fadd_rn(wi[1], wj[1]), wl[1]));
+            f.z = __fadd_rn(f.z, __fadd_rn(__fadd_rn(wi[2], wj[2]), wl[2]));
+            eb += (double)ee;
+        } else {
+            const float *w = role == 0 ? wi : (role == 1 ? wj : wl);
+            f.x = __fsub_rn(f.x, w[0]);
+            f.y = __fsub_rn(f.y, w[1]);
+            f.z = __fsub_rn(f.z, w[2]);
         }
     }
     v.force[s] = f;

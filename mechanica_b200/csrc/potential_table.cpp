@@ -565,6 +565,41 @@ int make_harmonic_angle(PotentialTable &p, double k, double theta0, double min, 
     return build_table(p, f, ScalarFn(), f6, (float)std::cos(max), (float)std::cos(min), (float)tol);
 }
 
+int make_harmonic_dihedral(PotentialTable &p, double K, int n, double delta, double tol) {
+    p = PotentialTable();
+    if (n < 1) return -1;
+    p.flags = kFlagR | kFlagHarmonic | kFlagDihedral;
+    // V(c) = K (1 + cos(n phi - delta)) in c = cos(phi), phi in [0, pi]:
+    // cos(n phi) = T_n(c), sin(n phi) = U_{n-1}(c) sin(phi) (Chebyshev recurrences),
+    // fitted without an analytic derivative (MxPotential.cpp:423-447, 484-516)
+    ScalarFn f = [K, n, delta](double r) {
+        const double cd = std::cos(delta), sd = std::sin(delta);
+        double t0 = 1.0, t1 = r, u0 = 1.0, u1 = 2 * r;
+        for (int k = 2; k <= n; ++k) {
+            const double t2 = 2 * r * t1 - t0, u2 = 2 * r * u1 - u0;
+            t0 = t1;
+            t1 = t2;
+            u0 = u1;
+            u1 = u2;
+        }
+        const double tn = t1, un1 = u0;  // T_n and U_{n-1}
+        if (delta == 0.0) return K * (1.0 + tn);
+        if (delta == M_PI) return K * (1.0 - tn);
+        if (std::fabs(r) < 1.0) return K * (1.0 + tn * cd + un1 * std::sqrt(1.0 - r * r) * sd);
+        return K * (1.0 + tn * cd);
+    };
+    ScalarFn f6 = [](double) { return 0.0; };
+    // end points pulled inside [-1, 1] when delta is not a multiple of pi
+    double a = -1.0, b = 1.0;
+    if (std::fmod(delta, M_PI) != 0) {
+        a = -1.0 / (1.0 + std::sqrt(FLT_EPSILON));
+        b = 1.0 / (1.0 + std::sqrt(FLT_EPSILON));
+    }
+    p.params = {K, (double)n, delta, tol};
+    p.form = kFormHarmonicDihedral;
+    return build_table(p, f, ScalarFn(), f6, (float)a, (float)b, (float)tol);
+}
+
 int make_power(PotentialTable &p, double k, double r0, double alpha, double a, double b, double tol) {
     p = PotentialTable();
     p.flags = kFlagR2 | kFlagScaled;

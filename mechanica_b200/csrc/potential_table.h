@@ -17,6 +17,7 @@ enum : uint32_t {
     kFlagR = 1u << 5,
     kFlagAngle = 1u << 6,
     kFlagHarmonic = 1u << 7,
+    kFlagDihedral = 1u << 8,
     kFlagScaled = 1u << 11,
     kFlagShifted = 1u << 12,
 };
@@ -39,7 +40,7 @@ struct PotentialTable {
 };
 
 enum : int { kFormNone = 0, kFormLJ126 = 1, kFormMorse = 2, kFormHarmonic = 3, kFormPower = 4,
-             kFormHarmonicAngle = 5 };
+             kFormHarmonicAngle = 5, kFormHarmonicDihedral = 6 };
 
 /* Frozen-node re-fit: the table of p's analytic form at new parameters, on p's
  * nodes and interval map (same n), so the coefficients depend linearly on the
@@ -59,6 +60,9 @@ int make_harmonic(PotentialTable &p, double k, double r0, double min, double max
 int make_power(PotentialTable &p, double k, double r0, double alpha, double a, double b, double tol);
 /* k (acos(c) - theta0)^2 on cos(max) <= c <= cos(min), with min clipped to >= 0 and max to <= pi. */
 int make_harmonic_angle(PotentialTable &p, double k, double theta0, double min, double max, double tol);
+/* K (1 + cos(n phi - delta)) in c = cos(phi) on [-1, 1] (pulled in by sqrt(eps) unless delta is a
+ * multiple of pi); n >= 1. */
+int make_harmonic_dihedral(PotentialTable &p, double K, int n, double delta, double tol);
 int make_dpd(PotentialTable &p, double alpha, double gamma, double sigma, double cutoff, bool shifted);
 bool eval_ex(const PotentialTable &p, float ri, float rj, float r2, float *e, float *f);
 void eval_r(const PotentialTable &p, float r, float *e, float *f);

@@ -121,14 +121,15 @@ def lattice(nx=32, spacing=0.5, seed=3, dt=0.005, pull=0.05, dissociation=2.0, k
 
 
 def chains(nchains=64, length=32, bond=0.5, L=8.0, seed=5, dt=0.002, k_bond=100.0, k_angle=5.0, theta0=2.0,
-           pair=None, cut=1.0, temperature=0.1):
+           pair=None, cut=1.0, temperature=0.1, dihedral=None):
     """Bead-spring chains in a periodic cube: harmonic bonds between consecutive
     beads (k_bond (r - bond)^2, never breaking) and harmonic angles on
     consecutive triples (k_angle (theta - theta0)^2, vertex at the middle bead).
     Chains are random walks with bond-length steps whose turning angle stays
     near pi - theta0, wrapped into the box, so bonds and angles cross the
     periodic faces. pair: None (bonded forces only) or the parameters of a Morse
-    potential bound on the bead type. Newtonian, mass 1."""
+    potential bound on the bead type. dihedral: None or (k, n, delta, tol) of a
+    harmonic dihedral on consecutive quadruples. Newtonian, mass 1."""
     rng = np.random.default_rng(seed)
     xs = []
     for _ in range(nchains):
@@ -159,7 +160,13 @@ def chains(nchains=64, length=32, bond=0.5, L=8.0, seed=5, dt=0.002, k_bond=100.
     v -= v.mean(axis=0)
     cells = int(L // cut)
     pots = [] if pair is None else [("morse", tuple(pair), 0, 0)]
-    return dict(dim=[L, L, L], cells=[cells] * 3, cutoff=cut, dt=dt, bc=("periodic", "periodic", "periodic"),
+    extra = {}
+    if dihedral is not None:
+        kd, nd, dd, tol = dihedral
+        extra = dict(di=idx[:, :-3].ravel().astype(np.int32), dj=idx[:, 1:-2].ravel().astype(np.int32),
+                     dk=idx[:, 2:-1].ravel().astype(np.int32), dl=idx[:, 3:].ravel().astype(np.int32),
+                     dihedral_pot=("harmonic_dihedral", (float(kd), int(nd), float(dd), float(tol))))
+    return dict(**extra, dim=[L, L, L], cells=[cells] * 3, cutoff=cut, dt=dt, bc=("periodic", "periodic", "periodic"),
                 types=[(1.0, 0.25, m.Newtonian)], pots=pots, forces=[], x=x, v=v, t=np.zeros(n, dtype=np.int32),
                 bi=bi, bj=bj, bond_pot=("harmonic", (k_bond, bond, 0.1, 1.0, 0.009)),
                 dissociation=float(np.finfo(np.float64).max),
@@ -195,6 +202,9 @@ def make_potential(kind, params):
         return m.Potential.dpd(*params[:4], shifted=bool(params[4]) if len(params) > 4 else False)
     if kind == "harmonic_angle":
         return m.Potential.harmonic_angle(*params)
+    if kind == "harmonic_dihedral":
+        k, n, delta, tol = params
+        return m.Potential.harmonic_dihedral(k, int(n), delta, tol)
     raise ValueError(kind)
 
 
@@ -220,6 +230,8 @@ def build_gpu(scn, rng_mode="reference"):
         u._add_bonds(make_potential(kind, params), scn["bi"], scn["bj"], scn["dissociation"])
     if "ai" in scn and len(scn["ai"]):
         u._add_angles(make_potential(*scn["angle_pot"]), scn["ai"], scn["aj"], scn["ak"])
+    if "di" in scn and len(scn["di"]):
+        u._add_dihedrals(make_potential(*scn["dihedral_pot"]), scn["di"], scn["dj"], scn["dk"], scn["dl"])
     return u
 
 

@@ -19,6 +19,8 @@
  *                         (src/mdcore/src/MxForce.cpp:508-519, engine.cpp:983-1003)
  *   mxref_add_bonds       _bond_init (src/mdcore/src/bond.cpp:497-529)
  *   mxref_add_angles      angle_init (src/mdcore/src/angle.cpp:659-707)
+ *   mxref_add_dihedrals   engine_dihedral_addpot + engine_dihedral_add
+ *                         (src/mdcore/src/engine_bonded.cpp:1049-1080, 1967-1991)
  *   mxref_step            engine_step (src/mdcore/src/engine.cpp:1198)
  *   mxref_force           engine_force (src/mdcore/src/engine.cpp:1230)
  * The engine is a process-wide singleton in the reference, so one process
@@ -256,6 +258,25 @@ int mxref_add_angles(int n, const int *pi, const int *pj, const int *pk, void *p
 
 /* The angle part of the last bonded pass (s->epot_angle, engine_bonded.cpp:1525-1528). */
 double mxref_epot_angle(void) { return _Engine.s.epot_angle; }
+
+/* Potential.harmonic_dihedral(k, n, delta, tol) (MxPotential.cpp:2595-2607) */
+void *mxref_potential_harmonic_dihedral(double k, int n, double delta, double tol) {
+    return potential_create_harmonic_dihedral(k, n, delta, tol);
+}
+
+/* engine_dihedral_addpot (engine_bonded.cpp:1967-1991) once, then engine_dihedral_add
+ * (engine_bonded.cpp:1049-1080) per dihedral i-j-k-l. */
+int mxref_add_dihedrals(int n, const int *pi, const int *pj, const int *pk, const int *pl, void *pot) {
+    int pid = engine_dihedral_addpot(&_Engine, (MxPotential *)pot);
+    if (pid < 0) return pid;
+    for (int q = 0; q < n; ++q) {
+        int rc = engine_dihedral_add(&_Engine, pi[q], pj[q], pk[q], pl[q], pid);
+        if (rc < 0) return rc;
+    }
+    return 0;
+}
+
+double mxref_epot_dihedral(void) { return _Engine.s.epot_dihedral; }
 
 int mxref_start(int nr_runners) { return engine_start(&_Engine, nr_runners, nr_runners); }
 

@@ -15,6 +15,7 @@ A scenario is a dict:
     forces [(type, fx, fy, fz)], x (N,3) float64, v (N,3), t (N,) int,
     bonds (optional): bi, bj, bond_pot (kind, params), dissociation,
     angles (optional): ai, aj, ak (vertex aj), angle_pot ("harmonic_angle", (k, theta0, min, max, tol)),
+    dihedrals (optional): di, dj, dk, dl, dihedral_pot ("harmonic_dihedral", (k, n, delta, tol)),
     action: "force" | "steps", nsteps, runners (threads), time_it (bool),
     integrator (0 forward Euler, 1 Runge-Kutta 4),
     sbforces [(type, "berendsen" | "random" | "friction", params)] with the forces module's
@@ -22,7 +23,7 @@ A scenario is a dict:
     friction(coef, std, mean, durration) (MxForce.cpp:213-259),
     target_temperature {type: T}
 Results: xabs, xrel, v, f, cell (per id), tasks (rows type, sid, i, j),
-    cdim, h, epot, epot_angle, ekin, bond_flags, seconds (wall time of the steps).
+    cdim, h, epot, epot_angle, epot_dihedral, ekin, bond_flags, seconds (wall time of the steps).
 """
 import ctypes
 import os
@@ -44,7 +45,8 @@ def available():
 def _pack(scn):
     flat = {}
     for k, v in scn.items():
-        if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "bc", "sbforces", "target_temperature"):
+        if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc", "sbforces",
+                 "target_temperature"):
             flat[k] = np.array(repr(v))
         else:
             flat[k] = np.asarray(v)
@@ -55,7 +57,8 @@ def _unpack(npz):
     out = {}
     for k in npz.files:
         v = npz[k]
-        if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "bc", "sbforces", "target_temperature"):
+        if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc", "sbforces",
+                 "target_temperature"):
             out[k] = eval(str(v))  # written by _pack from plain literals
         elif v.shape == ():
             out[k] = v.item()
@@ -122,9 +125,14 @@ def _execute(scn):
     def make_pot(kind, params):
         fn = {"lj126": L.mxref_potential_lj126, "morse": L.mxref_potential_morse,
               "harmonic": L.mxref_potential_harmonic, "power": L.mxref_potential_power,
-              "harmonic_angle": L.mxref_potential_harmonic_angle, "dpd": L.mxref_potential_dpd}[kind]
+              "harmonic_angle": L.mxref_potential_harmonic_angle, "dpd": L.mxref_potential_dpd,
+              "harmonic_dihedral": L.mxref_potential_harmonic_dihedral}[kind]
         if kind == "dpd":
             return fn(*[float(p) for p in params[:4]], int(params[4]) if len(params) > 4 else 0)
+        if kind == "harmonic_dihedral":
+            fn.restype = vp
+            fn.argtypes = [cd, ci, cd, cd]
+            return fn(float(params[0]), int(params[1]), float(params[2]), float(params[3]))
         return fn(*[float(p) for p in params])
 
     keep = []
@@ -162,6 +170,13 @@ def _execute(scn):
         L.mxref_add_angles.argtypes = [ci, P(ci), P(ci), P(ci), vp]
         if L.mxref_add_angles(len(scn["ai"]), a(scn["ai"], ci), a(scn["aj"], ci), a(scn["ak"], ci), ap) != 0:
             raise RuntimeError("mxref_add_angles")
+    if "di" in scn and len(scn["di"]):
+        dp = make_pot(*scn["dihedral_pot"])
+        keep.append(dp)
+        L.mxref_add_dihedrals.argtypes = [ci, P(ci), P(ci), P(ci), P(ci), vp]
+        if L.mxref_add_dihedrals(len(scn["di"]), a(scn["di"], ci), a(scn["dj"], ci), a(scn["dk"], ci),
+                                 a(scn["dl"], ci), dp) != 0:
+            raise RuntimeError("mxref_add_dihedrals")
     L.mxref_start(int(scn.get("runners", 1)))
     t0 = time.perf_counter()
     if scn.get("action", "force") == "force":
@@ -211,6 +226,8 @@ def _execute(scn):
     out["ekin"] = np.float64(e[3].value)
     L.mxref_epot_angle.restype = cd
     out["epot_angle"] = np.float64(L.mxref_epot_angle())
+    L.mxref_epot_dihedral.restype = cd
+    out["epot_dihedral"] = np.float64(L.mxref_epot_dihedral())
     return out
 
 

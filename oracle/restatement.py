@@ -60,8 +60,14 @@ def reference_table(kind, params):
     else:
         fn = getattr(L, f"mxref_potential_{kind}")
         fn.restype = vp
-        fn.argtypes = [cd] * len(params)
-        p = fn(*[float(q) for q in params])
+        if kind == "harmonic_dihedral":  # (k, n, delta, tol) with an int multiplicity
+            fn.argtypes = [cd, ctypes.c_int, cd, cd]
+            p = fn(float(params[0]), int(params[1]), float(params[2]), float(params[3]))
+        else:
+            fn.argtypes = [cd] * len(params)
+            p = fn(*[float(q) for q in params])
+    if not p:
+        return None, None  # the reference's potential_init failed
     n = ctypes.c_int()
     a4 = (ctypes.c_float * 4)()
     a, b, r0 = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()

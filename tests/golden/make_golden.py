@@ -37,6 +37,13 @@ CASES = [
     # forces and trajectories), and with a Morse pair potential
     ("chains_bonded", lambda: S.chains(nchains=16, length=24, seed=21), 10),
     ("chains_morse", lambda: S.chains(nchains=16, length=24, seed=22, pair=(0.2, 6.0, 0.5, 1e-4, 1.0, 1e-3)), 10),
+    # the same with harmonic dihedrals on consecutive quadruples: n = 3, delta = 0;
+    # and n = 2, delta = 1 with a Morse pair term (a phase that is not a multiple
+    # of pi needs tol 0.01: at the default 0.001 the fit exceeds its interval limit
+    # in the reference and here alike)
+    ("chains_dihedral", lambda: S.chains(nchains=16, length=24, seed=23, dihedral=(1.5, 3, 0.0, 0.001)), 10),
+    ("chains_dihedral_shift", lambda: S.chains(nchains=16, length=24, seed=24, dihedral=(0.8, 2, 1.0, 0.01),
+                                               pair=(0.2, 6.0, 0.5, 1e-4, 1.0, 1e-3)), 10),
 ]
 
 TABLES = [
@@ -50,6 +57,9 @@ TABLES = [
     ("power_sq", "power", (1.0, 1.0, 2.0, 0.1, 3.0, 1e-3)),
     ("angle_default", "harmonic_angle", (5.0, 2.0, 0.0, 3.141592653589793, 0.005 * 3.141592653589793)),
     ("angle_narrow", "harmonic_angle", (20.0, 1.9, 1.0, 2.8, 0.009)),
+    ("dihedral_n3", "harmonic_dihedral", (1.5, 3, 0.0, 0.001)),
+    ("dihedral_shift", "harmonic_dihedral", (0.8, 2, 1.0, 0.01)),
+    ("dihedral_pi", "harmonic_dihedral", (2.0, 1, 3.141592653589793, 0.001)),
 ]
 
 
@@ -62,7 +72,11 @@ def make_tables():
         fn = getattr(L, f"mxref_potential_{kind}")
         fn.restype = vp
         fn.argtypes = [cd] * len(params)
+        if kind == "harmonic_dihedral":  # (k, n, delta, tol) with an int multiplicity
+            fn.argtypes = [cd, ctypes.c_int, cd, cd]
         p = fn(*params)
+        if not p:
+            raise RuntimeError(f"reference table {name} failed")
         n = ctypes.c_int()
         a4 = (ctypes.c_float * 4)()
         a, b, r0 = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
@@ -100,7 +114,7 @@ def make_tables():
 def scenario_arrays(scn):
     d = {}
     for k, v in scn.items():
-        if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "bc"):
+        if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc"):
             d["scn_" + k] = np.array(repr(v))
         else:
             d["scn_" + k] = np.asarray(v)
@@ -112,7 +126,8 @@ def make_case(name, factory, nsteps):
     f1 = refengine.run(dict(scn, action="force", runners=1))
     tr = refengine.run(dict(scn, action="steps", nsteps=nsteps, runners=1))
     out = scenario_arrays(scn)
-    for k in ("f", "cell", "xrel", "epot", "ekin", "tasks", "cdim", "h", "bond_flags", "epot_angle"):
+    for k in ("f", "cell", "xrel", "epot", "ekin", "tasks", "cdim", "h", "bond_flags", "epot_angle",
+              "epot_dihedral"):
         out["force_" + k] = f1[k]
     for k in ("xrel", "xabs", "v", "cell", "epot", "ekin", "bond_flags"):
         out["traj_" + k] = tr[k]
@@ -131,7 +146,7 @@ def load_scenario(z):
             continue
         v = z[k]
         key = k[4:]
-        if key in ("types", "pots", "forces", "bond_pot", "angle_pot", "bc"):
+        if key in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc"):
             scn[key] = eval(str(v))  # plain literals written by scenario_arrays
         elif v.shape == ():
             scn[key] = v.item()

@@ -144,3 +144,84 @@ def test_angle_energy_matches_analytic():
     fi = -2 * k * (theta - th0) * dth
     assert np.linalg.norm(f[0] - fi) <= 5e-3 * np.linalg.norm(fi)
     assert np.abs(f.sum(axis=0)).max() <= 1e-5 * np.abs(f).max()
+
+
+# ---- dihedrals (dihedral_eval, src/mdcore/src/dihedral.cpp:81-392) ----
+
+def test_dihedral_force_pass_and_trajectory_are_bit_exact():
+    """Bonds, angles and n = 3 dihedrals on every consecutive quadruple, no pair
+    term: forces of one pass and a 10-step trajectory bit for bit."""
+    z, scn = load("chains_dihedral")
+    u = S.build_gpu(scn)
+    u.force()
+    x, v, f, c, xr = u.state()
+    assert np.array_equal(c, z["force_cell"])
+    assert np.array_equal(_bits(f), _bits(z["force_f"]))
+    ep, _ = u.energies()
+    ref = float(z["force_epot"])
+    assert abs(ep - ref) <= 1e-12 * abs(ref)
+    u.steps(int(z["traj_nsteps"]))
+    x, v, f, c, xr = u.state()
+    assert np.array_equal(c, z["traj_cell"])
+    assert np.array_equal(_bits(xr), _bits(z["traj_xrel"]))
+    assert np.array_equal(_bits(v), _bits(z["traj_v"]))
+
+
+def test_phase_shifted_dihedrals_with_pair_potential():
+    z, scn = load("chains_dihedral_shift")
+    u = S.build_gpu(scn)
+    u.force()
+    x, v, f, c, xr = u.state()
+    assert rel_rms(f, z["force_f"]) <= 1e-5
+    ep, _ = u.energies()
+    ref = float(z["force_epot"])
+    assert abs(ep - ref) <= 1e-6 * abs(ref)
+    u.steps(int(z["traj_nsteps"]))
+    x, v, f, c, xr = u.state()
+    assert np.array_equal(c, z["traj_cell"])
+    L = np.asarray(scn["dim"])
+    d = x - z["traj_xabs"]
+    d -= L * np.round(d / L)
+    assert np.abs(d).max() < 1e-5
+
+
+def _dihedral_energy(x, K, n, delta):
+    b1, b2, b3 = x[0] - x[1], x[2] - x[1], x[3] - x[2]
+    n1, n2 = np.cross(b1, b2), np.cross(b2, b3)
+    c = -(n1 @ n2) / np.linalg.norm(n1) / np.linalg.norm(n2)
+    phi = np.arccos(np.clip(c, -1, 1))
+    return K * (1 + np.cos(n * phi - delta)), c
+
+
+def test_single_dihedral_against_central_differences():
+    """Energy and forces of one dihedral against K (1 + cos(n phi - delta)) and
+    its FP64 central-difference gradient; momentum is conserved (the k end
+    takes the negated sum)."""
+    K, n, delta = 2.0, 2, 0.0
+    pot = m.Potential.harmonic_dihedral(K, n, delta)
+    m.init(dim=[6.0, 6.0, 6.0], cells=[3, 3, 3], cutoff=2.0, dt=0.001)
+
+    class Bead(m.Particle):
+        mass = 1.0
+        radius = 0.1
+
+    x0 = np.array([[2.6, 2.5, 3.0], [3.0, 3.1, 3.05], [3.5, 3.0, 2.9], [3.7, 3.3, 2.4]])
+    u = m.universe
+    u._add_particles(x0, np.zeros((4, 3), dtype=np.float32), np.zeros(4, dtype=np.int32))
+    m.Dihedral(pot, 0, 1, 2, 3)
+    u.force()
+    x = u.state()[0].astype(np.float64)
+    f = u.state()[2].astype(np.float64)
+    e_ref, c = _dihedral_energy(x, K, n, delta)
+    ep, _ = u.energies()
+    assert abs(ep - e_ref) <= 1e-3 * K
+    h = 1e-6
+    g = np.zeros_like(x)
+    for p in range(4):
+        for q in range(3):
+            xp, xm = x.copy(), x.copy()
+            xp[p, q] += h
+            xm[p, q] -= h
+            g[p, q] = (_dihedral_energy(xp, K, n, delta)[0] - _dihedral_energy(xm, K, n, delta)[0]) / (2 * h)
+    assert np.abs(f + g).max() <= 2e-3 * np.abs(g).max(), (f, -g)
+    assert np.abs(f.sum(axis=0)).max() <= 1e-5 * np.abs(f).max()

@@ -84,8 +84,16 @@ def test_tables_random_parameters_live():
         lo, hi = float(rng.uniform(0.0, 1.2)), float(rng.uniform(2.0, 3.4))
         cases.append(("harmonic_angle", (float(rng.uniform(0.5, 50)), float(rng.uniform(lo, hi)), lo, hi,
                                          0.005 * (hi - lo))))
+        cases.append(("harmonic_dihedral", (float(rng.uniform(0.5, 5)), int(rng.integers(1, 5)),
+                                            float(rng.choice([0.0, np.pi])), 0.001)))
+        cases.append(("harmonic_dihedral", (float(rng.uniform(0.5, 5)), int(rng.integers(1, 4)),
+                                            float(rng.uniform(0.1, 3.0)), 0.01)))
     for kind, params in cases:
         info, coef = reference_table(kind, params)
+        if info is None:  # the reference's fit fails: so must this one
+            with pytest.raises(m.EngineError):
+                S.make_potential(kind, params)
+            continue
         p = S.make_potential(kind, params)
         mine = p._info()
         assert mine["n"] == info["n"], (kind, params)
