@@ -20,6 +20,8 @@
  *   mxg_engine_addparts            engine_addpart           src/mdcore/src/engine.cpp:1726
  *   mxg_engine_addbonds            engine_bond_alloc + _bond_init src/mdcore/src/bond.cpp:497
  *   mxg_engine_addangles           engine_angle_alloc + angle_init src/mdcore/src/angle.cpp:659-707
+ *   mxg_engine_pairs_within        make_pairlist (the pair search of MxBond_PairwiseNew)
+ *                                  src/mdcore/src/bond.cpp:892-942
  *   mxg_engine_adddihedrals        engine_dihedral_addpot + engine_dihedral_add
  *                                  src/mdcore/src/engine_bonded.cpp:1049-1080, 1967-1991
  *   mxg_engine_start               engine_start             src/mdcore/include/engine.h:640
@@ -221,6 +223,15 @@ int mxg_engine_addangles(mxg_engine *e, int n, const int *i, const int *j, const
  * are balanced on k, which carries the energy. ids_out receives consecutive dihedral indices (may be NULL). */
 int mxg_engine_adddihedrals(mxg_engine *e, int n, const int *i, const int *j, const int *k, const int *l,
                             const mxg_potential *p, int *ids_out);
+/* The pair search of the pairwise bond constructor (make_pairlist, src/mdcore/src/bond.cpp:892-942), on
+ * the device over the current state of a started engine: the pairs (ids[a], ids[b]), b < a, of the n
+ * listed particles (one replica) whose global FP32 positions are within cutoff (|dx|^2 <= cutoff^2 summed
+ * x, y, z, no periodic image) and whose types ti, tj have type_mask[ti * ntypes + tj] != 0 (type_mask may
+ * be NULL: every pair of types; the reference's pair_check, bond.cpp:1134-1152), ordered by a, then b.
+ * *count receives the number of pairs; out_i/out_j (may be NULL to query the count) receive them when
+ * cap is large enough, else MXG_ERR_RANGE. */
+int mxg_engine_pairs_within(mxg_engine *e, int n, const int *ids, float cutoff, const unsigned char *type_mask,
+                            int ntypes, int *out_i, int *out_j, int cap, int *count);
 /* Builds the cell-pair lists and uploads the state. stream may be NULL (default stream). */
 int mxg_engine_start(mxg_engine *e, void *cuda_stream);
 /* Runs nsteps forward-Euler steps on the device (forces, bonds, integrate, re-bin). */

@@ -309,6 +309,24 @@ class Bond:
     def active(self):
         return bool(universe.bond_flags()[self.id] & 1)
 
+    @classmethod
+    def _handle(cls, bond_id, potential):
+        b = cls.__new__(cls)
+        b.id = bond_id
+        b.potential = potential
+        return b
+
+
+def _ids_of(particles):
+    """Particle ids of a particle, a list/tuple of particles or ids, or an id array."""
+    if isinstance(particles, Particle):
+        return np.array([particles.id], dtype=np.int32)
+    if isinstance(particles, np.ndarray):
+        return np.ascontiguousarray(particles, dtype=np.int32).ravel()
+    if isinstance(particles, (list, tuple)):
+        return np.array([_pid(p) for p in particles], dtype=np.int32)
+    raise TypeError("argument 1 is not a particle list")
+
 
 class Angle:
     """An angle p1-p2-p3 with its vertex at p2 and a potential in cos(theta)
@@ -358,6 +376,10 @@ class _ParticleMeta(type):
         v = np.zeros_like(x, dtype=np.float32) if velocities is None else np.asarray(velocities).reshape(-1, 3)
         ids = u._add_particles(x, v, np.full(len(x), cls.id, dtype=np.int32), replica)
         return ids
+
+    def items(cls):
+        """Ids of this type's particles, in id order (ParticleType.items)."""
+        return np.flatnonzero(_require()._t == cls.id).astype(np.int32)
 
 
 class Particle(metaclass=_ParticleMeta):
@@ -539,6 +561,41 @@ class _Universe:
         self._sync_state()
         self._dirty = True
         return list(range(first, first + len(ii)))
+
+    def bind_pairwise(self, potential, particles, cutoff, pairs=None, half_life=None, bond_energy=None, flags=0):
+        """Bonds every pair of the listed particles within cutoff of each other
+        (Universe.bind_pairwise, MxUniverse.cpp:669-733; MxBond_PairwiseNew,
+        bond.cpp:944-989). The pair search runs on the device over the current
+        state (global FP32 positions, no periodic image, pairs (a, b) with b
+        before a in the list, ordered by a then b); pairs: optional list of
+        (type, type) tuples that restricts the bonded type pairs. bond_energy is
+        the bonds' dissociation energy (default: never break). Returns the new
+        Bond handles."""
+        if not isinstance(potential, Potential):
+            raise TypeError("argument 0 is not a potential")
+        ids = _ids_of(particles)
+        self._ensure()
+        nt, mask = 0, None
+        if pairs is not None:
+            nt = len(self._types)
+            mask = np.zeros((nt, nt), dtype=np.uint8)
+            for (ta, tb) in pairs:
+                a = ta.id if isinstance(ta, type) else int(ta)
+                b = tb.id if isinstance(tb, type) else int(tb)
+                mask[a, b] = mask[b, a] = 1
+        mptr = None if mask is None else mask.ctypes.data_as(ctypes.c_void_p)
+        count = ctypes.c_int()
+        check(lib().mxg_engine_pairs_within(self._e, len(ids), ptr(ids, ctypes.c_int), float(cutoff), mptr, nt,
+                                            None, None, 0, ctypes.byref(count)), "pairs_within")
+        bi = np.zeros(count.value, dtype=np.int32)
+        bj = np.zeros(count.value, dtype=np.int32)
+        if count.value:
+            check(lib().mxg_engine_pairs_within(self._e, len(ids), ptr(ids, ctypes.c_int), float(cutoff), mptr, nt,
+                                                ptr(bi, ctypes.c_int), ptr(bj, ctypes.c_int), count.value,
+                                                ctypes.byref(count)), "pairs_within")
+        d = np.finfo(np.float64).max if bond_energy is None else float(bond_energy)
+        new = self._add_bonds(potential, bi, bj, d) if count.value else []
+        return [Bond._handle(k, potential) for k in new]
 
     def bind(self, obj, a, b=None, replica=0):
         """Binds a potential to a pair of types, or a force to a type (MxBind.cpp:18-100)."""

@@ -1492,6 +1492,28 @@ int mxg_engine_adddihedrals(mxg_engine *e, int n, const int *i, const int *j, co
     return MXG_OK;
 }
 
+int mxg_engine_pairs_within(mxg_engine *e, int n, const int *ids, float cutoff, const unsigned char *type_mask,
+                            int ntypes, int *out_i, int *out_j, int cap, int *count) {
+    if (!e || !count || (n > 0 && !ids)) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    if (!(cutoff >= 0.0f) || (type_mask && ntypes <= 0)) return MXG_ERR_ARG;
+    *count = 0;
+    if (n < 2) return MXG_OK;
+    for (int q = 0; q < n; ++q)
+        if (ids[q] < 0 || ids[q] >= e->nparts) return MXG_ERR_RANGE;
+    const Space &sp = e->spaces[e->prep[ids[0]]];
+    std::vector<int> a, b;
+    const int rc = find_pairs_within(e->view(e->cur), e->d_slot_of_id, e->nparts, sp.origin, sp.dim, n, ids, cutoff,
+                                     type_mask, ntypes, a, b, e->stream);
+    if (rc == -2) return MXG_ERR_MALLOC;
+    if (rc != 0) return MXG_ERR_CUDA;
+    *count = (int)a.size();
+    if (!out_i || !out_j || cap < (int)a.size()) return out_i || out_j ? MXG_ERR_RANGE : MXG_OK;
+    std::copy(a.begin(), a.end(), out_i);
+    std::copy(b.begin(), b.end(), out_j);
+    return MXG_OK;
+}
+
 int mxg_engine_start(mxg_engine *e, void *cuda_stream) {
     if (!e) return MXG_ERR_NULL;
     if (e->started) return MXG_ERR_STATE;

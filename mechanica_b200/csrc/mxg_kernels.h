@@ -1,5 +1,7 @@
 /* Host-callable launchers for the engine kernels (mxg_kernels.cu). */
 #pragma once
+#include <vector>
+
 #include "mxg_device.cuh"
 
 namespace mxg {
@@ -31,5 +33,13 @@ void launch_scatter(const EngineView &v, const float4 *pos, const float4 *vel, c
 void launch_energy(int ncells, const double *epot_cell, int nparts, const double *ebond_slot, const float4 *vel,
                    const float4 *pos, const DevType *types, double *partials, int nblocks, double *out,
                    cudaStream_t st);
+
+/* The pairwise bond constructor's pair search (mxg_pairs.cu): pairs (a, b), b < a, of the list ids
+ * with |x_a - x_b|^2 <= cutoff^2 in global FP32 coordinates (no periodic image) whose type pair has a
+ * nonzero mask entry (mask may be null), in the reference's order. lo, hi bound the replica's box.
+ * first/second receive the ids of a and b. Returns 0 or a negative status. */
+int find_pairs_within(const EngineView &v, const int *slot_of_id, int nids, const double lo[3], const double hi[3],
+                      int n, const int *ids_host, float cutoff, const unsigned char *mask_host, int ntypes,
+                      std::vector<int> &first, std::vector<int> &second, cudaStream_t st);
 
 }  // namespace mxg

@@ -19,6 +19,7 @@
  *                         (src/mdcore/src/MxForce.cpp:508-519, engine.cpp:983-1003)
  *   mxref_add_bonds       _bond_init (src/mdcore/src/bond.cpp:497-529)
  *   mxref_add_angles      angle_init (src/mdcore/src/angle.cpp:659-707)
+ *   mxref_pairwise        MxBond_PairwiseNew (src/mdcore/src/bond.cpp:944-989)
  *   mxref_add_dihedrals   engine_dihedral_addpot + engine_dihedral_add
  *                         (src/mdcore/src/engine_bonded.cpp:1049-1080, 1967-1991)
  *   mxref_step            engine_step (src/mdcore/src/engine.cpp:1198)
@@ -34,6 +35,7 @@
 #include "potential_eval.hpp"
 #include "bond.h"
 #include "angle.h"
+#include "MxParticleList.hpp"
 #include "task.h"
 #include "MxForce.h"
 #include "../../rendering/NOMStyle.hpp"
@@ -41,6 +43,7 @@
 
 extern PyTypeObject MxConstantForce_Type;
 extern PyTypeObject MxAngle_Type;
+extern PyTypeObject MxBondHandle_Type;
 MxPotential *potential_create_morse(double d, double a, double r0, double min, double max, double tol);
 MxPotential *potential_create_power(double k, double r0, double alpha, double a, double b, double tol);
 
@@ -277,6 +280,45 @@ int mxref_add_dihedrals(int n, const int *pi, const int *pj, const int *pk, cons
 }
 
 double mxref_epot_dihedral(void) { return _Engine.s.epot_dihedral; }
+
+/* The pairwise bond constructor, MxBond_PairwiseNew (src/mdcore/src/bond.cpp:944-989), on a
+ * particle list of n ids with potential pot; npairs (a[q], b[q]) type pairs restrict the bonded
+ * types as Universe.bind_pairwise's pairs argument does (none: every pair). The new bonds are
+ * appended to the engine's bond array; returns their number or a negative status. */
+int mxref_pairwise(int n, const int *ids, float cutoff, void *pot, int npairs, const int *ta, const int *tb) {
+    if (PyType_Ready(&MxBondHandle_Type) < 0) return -1;
+    MxParticleList list;
+    memset((void *)&list, 0, sizeof(list));
+    std::vector<int32_t> parts(ids, ids + n);
+    list.parts = parts.data();
+    list.nr_parts = n;
+    list.size_parts = n;
+    PyObject *pairs = NULL;
+    if (npairs > 0) {
+        pairs = PyList_New(npairs);
+        for (int q = 0; q < npairs; ++q)
+            PyList_SET_ITEM(pairs, q, PyTuple_Pack(2, (PyObject *)&engine::types[ta[q]],
+                                                   (PyObject *)&engine::types[tb[q]]));
+    }
+    const int before = _Engine.nr_bonds;
+    PyObject *args = PyTuple_New(0);
+    PyObject *bonds = MxBond_PairwiseNew((MxPotential *)pot, &list, cutoff, pairs, args, NULL);
+    Py_DECREF(args);
+    // the pair list is kept: its tuples hold the engine's type records, which
+    // are plain structs here and must never reach a zero reference count
+    if (!bonds) return -1;
+    Py_DECREF(bonds);
+    return _Engine.nr_bonds - before;
+}
+
+/* Particle ids of the engine's bonds in creation order. */
+int mxref_bond_ids(int *bi, int *bj, int cap) {
+    for (int k = 0; k < _Engine.nr_bonds && k < cap; ++k) {
+        bi[k] = _Engine.bonds[k].i;
+        bj[k] = _Engine.bonds[k].j;
+    }
+    return _Engine.nr_bonds;
+}
 
 int mxref_start(int nr_runners) { return engine_start(&_Engine, nr_runners, nr_runners); }
 

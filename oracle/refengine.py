@@ -16,7 +16,9 @@ A scenario is a dict:
     bonds (optional): bi, bj, bond_pot (kind, params), dissociation,
     angles (optional): ai, aj, ak (vertex aj), angle_pot ("harmonic_angle", (k, theta0, min, max, tol)),
     dihedrals (optional): di, dj, dk, dl, dihedral_pot ("harmonic_dihedral", (k, n, delta, tol)),
-    action: "force" | "steps", nsteps, runners (threads), time_it (bool),
+    action: "force" | "steps" | "pairwise", nsteps, runners (threads), time_it (bool),
+    pairwise (action "pairwise"): pw_ids (list order), pw_cutoff, pw_ta/pw_tb (type pairs, optional)
+        -> pw_i, pw_j: the bonds MxBond_PairwiseNew creates, in order,
     integrator (0 forward Euler, 1 Runge-Kutta 4),
     sbforces [(type, "berendsen" | "random" | "friction", params)] with the forces module's
     arguments: berenderson_tstat(tau), random(std, mean, durration),
@@ -177,6 +179,41 @@ def _execute(scn):
         if L.mxref_add_dihedrals(len(scn["di"]), a(scn["di"], ci), a(scn["dj"], ci), a(scn["dk"], ci),
                                  a(scn["dl"], ci), dp) != 0:
             raise RuntimeError("mxref_add_dihedrals")
+    if scn.get("action") == "pairwise":
+        hp = make_pot("harmonic", (1.0, 0.5, 0.1, 1.0, 0.009))
+        keep.append(hp)
+        ta = np.asarray(scn.get("pw_ta", []), dtype=np.int32)
+        tb = np.asarray(scn.get("pw_tb", []), dtype=np.int32)
+        ids = np.asarray(scn["pw_ids"], dtype=np.int32)
+        L.mxref_pairwise.argtypes = [ci, P(ci), ctypes.c_float, vp, ci, P(ci), P(ci)]
+        t0 = time.perf_counter()
+        cnt = L.mxref_pairwise(len(ids), a(ids, ci), float(scn["pw_cutoff"]), hp, len(ta), a(ta, ci), a(tb, ci))
+        seconds = time.perf_counter() - t0
+        if cnt < 0:
+            raise RuntimeError("mxref_pairwise")
+        nb0 = len(scn["bi"]) if "bi" in scn else 0
+        tot = nb0 + cnt
+        bi = np.zeros(max(tot, 1), dtype=np.int32)
+        bj = np.zeros(max(tot, 1), dtype=np.int32)
+        L.mxref_bond_ids.argtypes = [P(ci), P(ci), ci]
+        L.mxref_bond_ids(a(bi, ci), a(bj, ci), len(bi))
+        n = len(scn["t"])
+        xr = np.zeros((n, 3), dtype=np.float32)
+        xa = np.zeros((n, 3))
+        vv = np.zeros((n, 3), dtype=np.float32)
+        ff = np.zeros((n, 3), dtype=np.float32)
+        cc = np.zeros(n, dtype=np.int32)
+        tt = np.zeros(n, dtype=np.int32)
+        L.mxref_get_state(n, xr.ctypes.data_as(P(ctypes.c_float)), xa.ctypes.data_as(P(cd)),
+                          vv.ctypes.data_as(P(ctypes.c_float)), ff.ctypes.data_as(P(ctypes.c_float)),
+                          cc.ctypes.data_as(P(ci)), tt.ctypes.data_as(P(ci)))
+        cdim = np.zeros(3, dtype=np.int32)
+        h = np.zeros(3)
+        nc, nt, per = ci(), ci(), ctypes.c_uint()
+        L.mxref_space_info(cdim.ctypes.data_as(P(ci)), h.ctypes.data_as(P(cd)), ctypes.byref(nc), ctypes.byref(nt),
+                           ctypes.byref(per))
+        return {"pw_i": bi[nb0:tot].copy(), "pw_j": bj[nb0:tot].copy(), "seconds": np.float64(seconds),
+                "xrel": xr, "cell": cc, "cdim": cdim}
     L.mxref_start(int(scn.get("runners", 1)))
     t0 = time.perf_counter()
     if scn.get("action", "force") == "force":

@@ -93,6 +93,32 @@ def cell_origins(dim, cdim, origin=(0.0, 0.0, 0.0)):
     return out
 
 
+def pairlist(ids, xrel, cell, origins, types, cutoff, type_pairs=None):
+    """make_pairlist (src/mdcore/src/bond.cpp:892-942) restated: for list
+    entries a = 1..n-1 and b = 0..a-1, global positions float(x_rel + cell
+    origin), r2 = (dx*dx + dy*dy) + dz*dz in FP32 against float(cutoff)^2, type
+    pair accepted by pair_check (bond.cpp:1134-1152). Returns (ids[a], ids[b])
+    in the double loop's order."""
+    f32 = np.float32
+    g = (xrel.astype(np.float64) + origins[cell]).astype(f32)[ids]
+    t = np.asarray(types)[ids]
+    c2 = f32(cutoff) * f32(cutoff)
+    allowed = None
+    if type_pairs:
+        allowed = {(int(a), int(b)) for a, b in type_pairs} | {(int(b), int(a)) for a, b in type_pairs}
+    fi, fj = [], []
+    for a in range(1, len(ids)):
+        d = g[a] - g[:a]
+        r2 = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]
+        ok = r2 <= c2
+        if allowed is not None:
+            ok &= np.array([(int(t[a]), int(tb)) in allowed for tb in t[:a]], dtype=bool)
+        b = np.flatnonzero(ok)
+        fi.extend([ids[a]] * len(b))
+        fj.extend(ids[b].tolist())
+    return np.array(fi, dtype=np.int32), np.array(fj, dtype=np.int32)
+
+
 def nonbond(scn, xrel, vel, cell, tasks, cdim, precision=64, tables=None, second=None, pruning=0, virial=False):
     """Forces (N,3) float64, energy, counts for a configuration.
 

@@ -111,6 +111,37 @@ def make_tables():
     np.savez_compressed(os.path.join(OUT, "tables.npz"), **out)
 
 
+# pairwise bond constructor cases: (name, scenario, list-order seed, list size,
+# cutoff, type pairs or None)
+PAIRWISE = [
+    ("pw_morse_short", lambda: S.morse2(n=2000, seed=31), 1, 1500, 1.2, None),
+    ("pw_morse_long_ab", lambda: S.morse2(n=2000, seed=32), 2, 2000, 3.0, [(0, 1)]),
+    ("pw_lattice", lambda: S.lattice(nx=6, seed=33, noise=2e-2), 3, 216, 0.55, None),
+]
+
+
+def make_pairwise():
+    out = {}
+    for name, fac, seed, n, cutoff, tp in PAIRWISE:
+        scn = fac()
+        ids = np.random.default_rng(seed).permutation(len(scn["t"]))[:n].astype(np.int32)
+        extra = dict(action="pairwise", pw_ids=ids, pw_cutoff=cutoff)
+        if tp:
+            extra.update(pw_ta=[a for a, _ in tp], pw_tb=[b for _, b in tp])
+        r = refengine.run(dict(scn, **extra))
+        out[f"{name}__ids"] = ids
+        out[f"{name}__cutoff"] = np.float64(cutoff)
+        out[f"{name}__pairs"] = np.array(tp if tp else [], dtype=np.int32).reshape(-1, 2)
+        out[f"{name}__i"] = r["pw_i"]
+        out[f"{name}__j"] = r["pw_j"]
+        out[f"{name}__xrel"] = r["xrel"]
+        out[f"{name}__cell"] = r["cell"]
+        out[f"{name}__cdim"] = r["cdim"]
+        out[f"{name}__dim"] = np.asarray(scn["dim"], dtype=np.float64)
+        out[f"{name}__t"] = np.asarray(scn["t"], dtype=np.int32)
+    np.savez_compressed(os.path.join(OUT, "pairwise.npz"), **out)
+
+
 def scenario_arrays(scn):
     d = {}
     for k, v in scn.items():
@@ -160,6 +191,8 @@ if __name__ == "__main__":
     want = set(sys.argv[1:])
     if not want or "tables" in want:
         make_tables()
+    if not want or "pairwise" in want:
+        make_pairwise()
     for name, fac, ns in CASES:
         if not want or name in want:
             make_case(name, fac, ns)

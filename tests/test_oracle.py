@@ -40,3 +40,18 @@ def test_tier_b_bonds_excluded_lattice_nonbonded():
     bond = np.asarray(z["force_f"], dtype=np.float64) - f
     # bonds at (nearly) rest length contribute little compared with the Morse forces
     assert np.sqrt((bond ** 2).mean()) < 0.5 * np.sqrt((f ** 2).mean())
+
+
+@pytest.mark.parametrize("name", ["pw_morse_short", "pw_morse_long_ab", "pw_lattice"])
+def test_pairlist_restatement_matches_reference(name):
+    """The numpy restatement of make_pairlist reproduces the reference's
+    pairwise bonds (ids and order) on the fixture's placement."""
+    import os
+    from golden_util import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "pairwise.npz"))
+    origins = R.cell_origins(z[f"{name}__dim"], z[f"{name}__cdim"])
+    pairs = [tuple(p) for p in z[f"{name}__pairs"]] or None
+    fi, fj = R.pairlist(z[f"{name}__ids"], z[f"{name}__xrel"], z[f"{name}__cell"], origins, z[f"{name}__t"],
+                        float(z[f"{name}__cutoff"]), pairs)
+    assert np.array_equal(fi, z[f"{name}__i"])
+    assert np.array_equal(fj, z[f"{name}__j"])
