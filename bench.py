@@ -39,6 +39,7 @@ WORKLOAD = ("DPD fluid with body force: 200,000 particles, 40x20x20 box, periodi
             "DPD a=25 gamma=4.5 sigma=3 rc=1 kT=1; constant force 0.02 +x; FP32, dt=0.01")
 # algorithmic FP32 operations per candidate pair and per interacting DPD pair
 # (counted from the reference's scalar pair loop and dpd_eval)
+FORCE_TRAFFIC_BYTES = 17182208 + 518656  # DRAM read + write of one force launch, 200,000-particle DPD
 F_CAND = 9
 F_INT_DPD = 40
 F_INT_TABLE = 44
@@ -442,7 +443,10 @@ def main():
                 "algorithmic_flops_per_launch": flops, "candidate_pairs": cand.value,
                 "interacting_pairs": inter.value,
                 "flops_per_pair": {"candidate": F_CAND, "interacting_dpd": F_INT_DPD},
-                "force_ms_per_launch": force_ms, "traffic": None}
+                "force_ms_per_launch": force_ms,
+                # dram__bytes_read.sum + dram__bytes_write.sum of one force launch of this workload
+                # (ncu capture summarised in profiles/force_kernel_dpd200k.md)
+                "traffic": FORCE_TRAFFIC_BYTES if n == 200000 else None, "traffic_unit": "bytes per launch"}
 
     # ---- CPU baseline and accuracy (reference engine, rank 0, N=1 only) ----
     cpu = None
