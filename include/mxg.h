@@ -20,6 +20,8 @@
  *   mxg_engine_addparts            engine_addpart           src/mdcore/src/engine.cpp:1726
  *   mxg_engine_addbonds            engine_bond_alloc + _bond_init src/mdcore/src/bond.cpp:497
  *   mxg_engine_addangles           engine_angle_alloc + angle_init src/mdcore/src/angle.cpp:659-707
+ *   mxg_engine_set_boundary_potential MxBoundaryCondition(s)::set_potential
+ *                                  src/mdcore/src/MxBoundaryConditions.cpp:771-836, via bind (MxBind.cpp:74-96)
  *   mxg_engine_pairs_within        make_pairlist (the pair search of MxBond_PairwiseNew)
  *                                  src/mdcore/src/bond.cpp:892-942
  *   mxg_engine_adddihedrals        engine_dihedral_addpot + engine_dihedral_add
@@ -82,6 +84,7 @@ extern "C" {
 #define MXG_BOUNDARY_VELOCITY (1 << 0)
 #define MXG_BOUNDARY_PERIODIC (1 << 1)
 #define MXG_BOUNDARY_FREESLIP (1 << 2)
+#define MXG_BOUNDARY_POTENTIAL (1 << 3) /* with FREESLIP: the "potential" kind */
 #define MXG_BOUNDARY_NO_SLIP (1 << 4)
 
 /* faces, in the order the bc arrays use */
@@ -223,6 +226,14 @@ int mxg_engine_addangles(mxg_engine *e, int n, const int *i, const int *j, const
  * are balanced on k, which carries the energy. ids_out receives consecutive dihedral indices (may be NULL). */
 int mxg_engine_adddihedrals(mxg_engine *e, int n, const int *i, const int *j, const int *k, const int *l,
                             const mxg_potential *p, int *ids_out);
+/* Binds potential p between particles of `type` and a wall: face 0..5 (MXG_FACE_*) or -1 for all six
+ * (MxBoundaryCondition::set_potential / MxBoundaryConditions::set_potential,
+ * src/mdcore/src/MxBoundaryConditions.cpp:771-836). Evaluated for particles in cells next to a non-periodic
+ * face as boundary_eval does (src/mdcore/src/boundary_eval.hpp:124-223): distance r to the face, kept when
+ * r <= the potential's b; r^2 below the potential's a (sic, not a^2) is replaced by a^2 along the face
+ * normal; tables get potential_eval_ex with wall radius 0, DPD potentials dpd_boundary_eval against the
+ * wall velocity. */
+int mxg_engine_set_boundary_potential(mxg_engine *e, int face, int type, const mxg_potential *p);
 /* The pair search of the pairwise bond constructor (make_pairlist, src/mdcore/src/bond.cpp:892-942), on
  * the device over the current state of a started engine: the pairs (ids[a], ids[b]), b < a, of the n
  * listed particles (one replica) whose global FP32 positions are within cutoff (|dx|^2 <= cutoff^2 summed

@@ -49,7 +49,7 @@ FREESLIP_Y = 1 << 7
 FREESLIP_Z = 1 << 8
 FREESLIP_FULL = FREESLIP_X | FREESLIP_Y | FREESLIP_Z
 
-_BC_VELOCITY, _BC_PERIODIC, _BC_FREESLIP, _BC_NOSLIP = 1, 2, 4, 16
+_BC_VELOCITY, _BC_PERIODIC, _BC_FREESLIP, _BC_POTENTIAL, _BC_NOSLIP = 1, 2, 4, 8, 16
 _FACES = ["left", "right", "front", "back", "bottom", "top"]
 _AXIS_FACES = {"x": (0, 1), "y": (2, 3), "z": (4, 5)}
 
@@ -63,7 +63,7 @@ def _bc_kind_of(value):
     if s in ("NO_SLIP", "NOSLIP"):
         return _BC_NOSLIP
     if s == "POTENTIAL":
-        return _BC_FREESLIP  # wall potentials are not on this path; the wall reflects
+        return _BC_FREESLIP | _BC_POTENTIAL  # a free-slip wall that potentials are usually bound to
     raise ValueError(f"invalid boundary condition {value!r}")
 
 
@@ -358,6 +358,28 @@ class Dihedral:
         self.potential = potential
 
 
+class BoundaryCondition:
+    """One face of the box (MxBoundaryCondition, MxBoundaryConditions.hpp:25-52);
+    ``bind(potential, face, Type)`` puts a wall potential between the face and
+    the type's particles."""
+
+    _NORMALS = ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1))
+
+    def __init__(self, face):
+        self.face = face
+        self.name = _FACES[face]
+        self.normal = np.array(self._NORMALS[face], dtype=np.float32)
+
+
+class BoundaryConditions:
+    """The six faces (MxBoundaryConditions); ``bind(potential, universe.boundary_conditions,
+    Type)`` binds the wall potential on every face (MxBoundaryConditions.cpp:828-837)."""
+
+    def __init__(self):
+        for f, name in enumerate(_FACES):
+            setattr(self, name, BoundaryCondition(f))
+
+
 def _pid(p):
     return p.id if isinstance(p, Particle) else int(p)
 
@@ -442,6 +464,7 @@ class _Universe:
         self._bonds = []        # (potential, i[], j[], dissociation)
         self._angles = []       # (potential, i[], j[], k[])
         self._dihedrals = []    # (potential, i[], j[], k[], l[])
+        self._bpots = []        # wall potentials: (potential, face or -1, type)
         self._x = np.zeros((0, 3))
         self._v = np.zeros((0, 3), dtype=np.float32)
         self._t = np.zeros(0, dtype=np.int32)
@@ -498,6 +521,8 @@ class _Universe:
         for (p, ii, jj, kk) in self._angles:
             check(lib().mxg_engine_addangles(self._e, len(ii), ptr(ii, ctypes.c_int), ptr(jj, ctypes.c_int),
                                              ptr(kk, ctypes.c_int), p._h, None), "addangles")
+        for (p, face, t) in self._bpots:
+            check(lib().mxg_engine_set_boundary_potential(self._e, face, t, p._h), "set_boundary_potential")
         for (p, ii, jj, kk, ll) in self._dihedrals:
             check(lib().mxg_engine_adddihedrals(self._e, len(ii), ptr(ii, ctypes.c_int), ptr(jj, ctypes.c_int),
                                                 ptr(kk, ctypes.c_int), ptr(ll, ctypes.c_int), p._h, None),
@@ -545,6 +570,11 @@ class _Universe:
         self._sync_state()
         self._dirty = True
         return list(range(first, first + len(ii)))
+
+    @property
+    def boundary_conditions(self):
+        """The box faces, for binding wall potentials (Universe.boundary_conditions)."""
+        return BoundaryConditions()
 
     def _add_angles(self, pot, i, j, k):
         ii, jj, kk = i32(i), i32(j), i32(k)
@@ -598,7 +628,17 @@ class _Universe:
         return [Bond._handle(k, potential) for k in new]
 
     def bind(self, obj, a, b=None, replica=0):
-        """Binds a potential to a pair of types, or a force to a type (MxBind.cpp:18-100)."""
+        """Binds a potential to a pair of types, to a type and a wall (a
+        BoundaryCondition face or all of BoundaryConditions), or a force to a type
+        (MxBind.cpp:18-100)."""
+        walls = (BoundaryCondition, BoundaryConditions)
+        if isinstance(obj, Potential) and (isinstance(a, walls) or isinstance(b, walls)):
+            bc, t = (a, b) if isinstance(a, walls) else (b, a)
+            ti = t.id if isinstance(t, type) else int(t)
+            self._sync_state()
+            self._bpots.append((obj, bc.face if isinstance(bc, BoundaryCondition) else -1, ti))
+            self._dirty = True
+            return
         ta = a.id if isinstance(a, type) else int(a)
         if isinstance(obj, (Potential, PotentialSum)):
             tb = ta if b is None else (b.id if isinstance(b, type) else int(b))

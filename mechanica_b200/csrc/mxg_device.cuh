@@ -75,6 +75,9 @@ struct DevType {
     int sb_steps;        // random/friction: redraw interval in steps, ceil(duration / dt)
     float sb_a, sb_b, sb_c, sb_pad;  // Berendsen: 1/tau; random: mean, std; friction: coef, mean, std
     double target;       // Berendsen: the type's target temperature
+    int bpot[6];         // wall potential per face (left, right, front, back, bottom, top), -1 if none
+    unsigned wall_mask;  // active-cell bits of the faces with a wall potential
+    int bpad;
 };
 
 struct DevSpace {        // one per replica
@@ -175,6 +178,7 @@ struct EngineView {      // everything a kernel needs, passed by value
     const int *sec_count;    // per cell: SECOND entries, i.e. planes of received sums
     const int *cell_planes;  // per cell: received planes plus own-side planes of its later work items
     float4 *planes;          // [plane][slot] neighbour-side force sums of once-evaluated pairs
+    double *wall_e;          // per slot: wall energy of the last pass; null when no type has a wall potential
     const int4 *items;       // force work items: (cell, first entry, end entry, part)
     int nitems;
 };

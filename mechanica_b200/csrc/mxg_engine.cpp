@@ -83,6 +83,7 @@ struct TypeInfo {
     int sb_kind = 0;            // 2 Berendsen, 3 random, 4 friction (the type's one single-body force)
     float sb[4] = {0, 0, 0, 0};  // Berendsen: tau; random: mean, std, duration; friction: coef, mean, std, duration
     double target = 0.0;        // target temperature (Berendsen)
+    int bpot[6] = {-1, -1, -1, -1, -1, -1};  // wall potential per face (index into pots), -1 if none
 };
 
 struct BondInfo {
@@ -406,6 +407,8 @@ struct mxg_engine {
     int energy_blocks = 64;
     bool has_dpd = false;
     bool has_sb = false;                // a type has a Berendsen, random or friction force
+    bool has_walls = false;             // a type has a wall potential
+    double *d_wall_e = nullptr;         // per slot: wall energy of the last pass
     double *d_type_ke = nullptr;
     float4 *d_persist = nullptr;
     int integrator = 0;                 // 0 forward Euler, 1 Runge-Kutta 4 (engine.h EngineIntegrator)
@@ -575,6 +578,7 @@ struct mxg_engine {
         v.items = d_items;
         v.nitems = nitems;
         v.planes = d_planes;
+        v.wall_e = has_walls ? d_wall_e : nullptr;
         return v;
     }
 
@@ -852,6 +856,7 @@ int mxg_engine::start(cudaStream_t st) {
         hs.push_back(space_desc(r, r * tt));
     }
     has_sb = false;
+    has_walls = false;
     std::vector<DevType> ht(ntypes);
     for (int a = 0; a < (int)types.size(); ++a) {
         DevType &d = ht[a];
@@ -878,6 +883,15 @@ int mxg_engine::start(cudaStream_t st) {
             d.sb_steps = std::max(1, (int)std::ceil(dur / dt));  // durration_steps (MxForce.cpp:403,417)
         }
         if (ti.sb_kind) has_sb = true;
+        const unsigned face_bits[6] = {kCellActiveLeft, kCellActiveRight, kCellActiveFront,
+                                       kCellActiveBack, kCellActiveBottom, kCellActiveTop};
+        for (int f = 0; f < 6; ++f) {
+            d.bpot[f] = ti.bpot[f];
+            if (ti.bpot[f] >= 0) {
+                d.wall_mask |= face_bits[f];
+                has_walls = true;
+            }
+        }
     }
     std::vector<SortAxes> haxes(1);
     for (int q = 0; q < 13; ++q)
@@ -1001,6 +1015,7 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_sort_bounds, (size_t)ncells * 13);
     rc |= alloc(&d_epot_cell, nitems);
     rc |= alloc(&d_ebond_slot, nparts);
+    rc |= alloc(&d_wall_e, nparts);
     rc |= alloc(&d_bonds, hb.size());
     rc |= alloc(&d_bond_flags, hbf.size());
     rc |= alloc(&d_bond_off, boff.size());
@@ -1023,6 +1038,7 @@ int mxg_engine::start(cudaStream_t st) {
     CUDA_TRY(cudaMemsetAsync(d_step, 0, sizeof(unsigned long long), stream));
     CUDA_TRY(cudaMemsetAsync(d_epot_cell, 0, sizeof(double) * std::max(1, nitems), stream));
     CUDA_TRY(cudaMemsetAsync(d_ebond_slot, 0, sizeof(double) * std::max(1, nparts), stream));
+    CUDA_TRY(cudaMemsetAsync(d_wall_e, 0, sizeof(double) * std::max(1, nparts), stream));
     CUDA_TRY(cudaMemsetAsync(d_force, 0, sizeof(float4) * std::max(1, nparts), stream));
     CUDA_TRY(cudaMemsetAsync(d_persist, 0, sizeof(float4) * std::max(1, nparts), stream));
     CUDA_TRY(cudaMemsetAsync(d_type_ke, 0, sizeof(double) * ht.size(), stream));
@@ -1514,6 +1530,17 @@ int mxg_engine_pairs_within(mxg_engine *e, int n, const int *ids, float cutoff, 
     return MXG_OK;
 }
 
+int mxg_engine_set_boundary_potential(mxg_engine *e, int face, int type, const mxg_potential *p) {
+    if (!e || !p) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    if (face < -1 || face > 5 || type < 0 || type >= (int)e->types.size()) return MXG_ERR_RANGE;
+    e->pots.push_back(p->t);
+    const int idx = (int)e->pots.size() - 1;
+    for (int f = 0; f < 6; ++f)
+        if (face < 0 || f == face) e->types[type].bpot[f] = idx;
+    return MXG_OK;
+}
+
 int mxg_engine_start(mxg_engine *e, void *cuda_stream) {
     if (!e) return MXG_ERR_NULL;
     if (e->started) return MXG_ERR_STATE;
@@ -1627,7 +1654,7 @@ int mxg_engine_energy(mxg_engine *e, double *epot, double *ekin, double *virial9
     if (!e) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
     launch_energy(e->nitems, e->d_epot_cell, e->nparts, e->has_bonded() ? e->d_ebond_slot : nullptr,
-                  e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
+                  e->has_walls ? e->d_wall_e : nullptr, e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
                   e->stream);
     double out[2];
     CUDA_TRY(cudaMemcpyAsync(out, e->d_energy, sizeof(out), cudaMemcpyDeviceToHost, e->stream));
@@ -1726,7 +1753,7 @@ int mxg_engine_energy_async(mxg_engine *e, double *host_out2) {
     if (!e || !host_out2) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
     launch_energy(e->nitems, e->d_epot_cell, e->nparts, e->has_bonded() ? e->d_ebond_slot : nullptr,
-                  e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
+                  e->has_walls ? e->d_wall_e : nullptr, e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
                   e->stream);
     CUDA_TRY(cudaMemcpyAsync(host_out2, e->d_energy, 2 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     return MXG_OK;
@@ -1790,7 +1817,8 @@ int mxg_engine_adjoint_params(mxg_engine *e, int n, const int *pot, const int *p
 int mxg_engine_vjp_step(mxg_engine *e, void *lam_x, void *lam_v, double *grad) {
     if (!e || !lam_x || !lam_v || !grad) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
-    if (e->has_bonded() || e->has_sb) return MXG_ERR_ARG;  // bonded and single-body forces are not differentiated
+    // bonded, single-body and wall forces are not differentiated
+    if (e->has_bonded() || e->has_sb || e->has_walls) return MXG_ERR_ARG;
     if (e->nparts == 0) return MXG_OK;
     if (e->adjoint_stale) {
         const int rc = e->build_adjoint();

@@ -167,6 +167,61 @@ __device__ __forceinline__ void pair_contribution(const EngineView &v, const Dev
     }
 }
 
+/*
+ * Wall potentials of one particle (boundary_eval, boundary_eval.hpp:124-223),
+ * faces in the reference's order left, right, front, back, bottom, top: the
+ * distance r to the face from the cell-relative position (r = x for a low
+ * face, float(h - x) for a high one), kept when r <= b; r^2 < a (the
+ * reference compares with a, not a^2) becomes a^2 along the face normal.
+ * Tables: potential_eval_ex with the wall's radius 0, f -= f dx. DPD:
+ * dpd_boundary_eval against the wall velocity, f += f e (energy 0).
+ */
+__device__ __noinline__ void boundary_forces(const EngineView &v, const DevSpace &S, unsigned cflags, const DevType &T, float radius,
+                                const float4 &x, const float4 &u, float4 &f, double &epot) {
+    const unsigned bits[6] = {kCellActiveLeft, kCellActiveRight, kCellActiveFront,
+                              kCellActiveBack, kCellActiveBottom, kCellActiveTop};
+    const float xr[3] = {x.x, x.y, x.z};
+    for (int face = 0; face < 6; ++face) {
+        if (!(cflags & bits[face]) || T.bpot[face] < 0) continue;
+        const DevPot &p = v.pots[T.bpot[face]];
+        const int ax = face >> 1;
+        const bool high = face & 1;
+        const float r = high ? (float)__dsub_rn(S.hd[ax], (double)xr[ax]) : xr[ax];
+        if (!(r <= p.b)) continue;
+        float dx[3] = {0.f, 0.f, 0.f};
+        dx[ax] = high ? -r : r;
+        float r2 = __fmul_rn(r, r);
+        if (r2 < p.a) {
+            r2 = __fmul_rn(p.a, p.a);
+            dx[ax] = high ? -p.a : p.a;  // the face normal times a
+        }
+        if (p.kind == 1) {
+            if (r2 > __fmul_rn(p.b, p.b)) continue;
+            const float rr = sqrtf(r2);
+            const float e[3] = {__fdiv_rn(dx[0], rr), __fdiv_rn(dx[1], rr), __fdiv_rn(dx[2], rr)};
+            const float w[3] = {__fsub_rn(u.x, S.bc_vel[face][0]), __fsub_rn(u.y, S.bc_vel[face][1]),
+                                __fsub_rn(u.z, S.bc_vel[face][2])};
+            const float oc = __fsub_rn(1.0f, __fdiv_rn(rr, p.b));
+            const float fc = __fmul_rn(p.dpd_alpha, oc);
+            const float od = __fmul_rn(oc, oc);
+            const float ev = __fadd_rn(__fadd_rn(__fmul_rn(e[0], w[0]), __fmul_rn(e[1], w[1])), __fmul_rn(e[2], w[2]));
+            const float fd = __fmul_rn(__fmul_rn(-p.dpd_gamma, od), ev);
+            const float fr = __fmul_rn(__fmul_rn(p.dpd_sigma, oc), p.dpd_delta);
+            const float ff = __fadd_rn(__fadd_rn(fc, fd), fr);
+            f.x = __fadd_rn(f.x, __fmul_rn(ff, e[0]));
+            f.y = __fadd_rn(f.y, __fmul_rn(ff, e[1]));
+            f.z = __fadd_rn(f.z, __fmul_rn(ff, e[2]));
+        } else {
+            float ee, ff;
+            if (!table_eval_ex(p, v.coef, radius, 0.0f, r2, ee, ff)) continue;
+            f.x = __fsub_rn(f.x, __fmul_rn(ff, dx[0]));
+            f.y = __fsub_rn(f.y, __fmul_rn(ff, dx[1]));
+            f.z = __fsub_rn(f.z, __fmul_rn(ff, dx[2]));
+            epot += (double)ee;
+        }
+    }
+}
+
 constexpr int kOwn = 32;            // own particles staged at a time
 constexpr int kCap = 128;           // neighbour particles staged at a time
 constexpr int kChunks = kCap / 32;  // candidate steps per own particle
@@ -631,6 +686,17 @@ __device__ __forceinline__ float4 total_force(const EngineView &v, int s) {
         f.x += g.x;
         f.y += g.y;
         f.z += g.z;
+    }
+    if (v.wall_e) {
+        // wall potentials of particles in cells next to a bound face (runner_doself's
+        // boundary_eval, runner_dopair.cpp:533-535); the energy goes to the slot's entry
+        const float4 x = v.pos[s];
+        const DevType &T = v.types[__float_as_int(x.w)];
+        const int c = v.cell_of[s];
+        const unsigned cflags = v.cell_flags[c];
+        double ew = 0.0;
+        if (cflags & T.wall_mask) boundary_forces(v, v.spaces[v.cell_rep[c]], cflags, T, T.radius, x, v.vel[s], f, ew);
+        v.wall_e[s] = ew;
     }
     if (v.has_sb) {
         // the velocity-dependent and random single-body forces (MxForce.cpp:330-386)
@@ -1373,7 +1439,8 @@ __global__ void scatter_kernel(EngineView v, int ncells, const float4 *__restric
 
 /* Deterministic two-stage sums: block partials, then one block. */
 __global__ void reduce_energy_kernel(int ncells, const double *__restrict__ epot_cell, int nparts,
-                                     const double *__restrict__ ebond_slot, const float4 *__restrict__ vel,
+                                     const double *__restrict__ ebond_slot, const double *__restrict__ wall_e,
+                                     const float4 *__restrict__ vel,
                                      const float4 *__restrict__ pos, const DevType *__restrict__ types,
                                      double *partials) {
     __shared__ double s_pot[256], s_kin[256];
@@ -1381,6 +1448,7 @@ __global__ void reduce_energy_kernel(int ncells, const double *__restrict__ epot
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += gridDim.x * blockDim.x) ep += epot_cell[c];
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nparts; s += gridDim.x * blockDim.x) {
         if (ebond_slot) ep += ebond_slot[s];
+        if (wall_e) ep += wall_e[s];
         const float4 u = vel[s];
         const DevType &T = types[__float_as_int(pos[s].w)];
         // engine_kinetic_energy (engine.cpp:1698-1719): float e = 0.5*mass*|v|^2
@@ -1511,10 +1579,11 @@ void launch_scatter(const EngineView &v, const float4 *pos, const float4 *vel, c
                                          out_count, new_start, pos_out, vel_out, cell_out, slot_of_id);
 }
 
-void launch_energy(int ncells, const double *epot_cell, int nparts, const double *ebond_slot, const float4 *vel,
-                   const float4 *pos, const DevType *types, double *partials, int nblocks, double *out,
-                   cudaStream_t st) {
-    reduce_energy_kernel<<<nblocks, 256, 0, st>>>(ncells, epot_cell, nparts, ebond_slot, vel, pos, types, partials);
+void launch_energy(int ncells, const double *epot_cell, int nparts, const double *ebond_slot, const double *wall_e,
+                   const float4 *vel, const float4 *pos, const DevType *types, double *partials, int nblocks,
+                   double *out, cudaStream_t st) {
+    reduce_energy_kernel<<<nblocks, 256, 0, st>>>(ncells, epot_cell, nparts, ebond_slot, wall_e, vel, pos, types,
+                                                  partials);
     reduce_final_kernel<<<1, 32, 0, st>>>(nblocks, partials, out);
 }
 

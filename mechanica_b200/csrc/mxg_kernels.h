@@ -30,9 +30,10 @@ void launch_scatter(const EngineView &v, const float4 *pos, const float4 *vel, c
                     const int *old_start, const int *old_count, int *in_count, const int *in_list, int *out_count,
                     const int *new_start, float4 *pos_out, float4 *vel_out, int *cell_out, int *slot_of_id,
                     cudaStream_t st);
-void launch_energy(int ncells, const double *epot_cell, int nparts, const double *ebond_slot, const float4 *vel,
-                   const float4 *pos, const DevType *types, double *partials, int nblocks, double *out,
-                   cudaStream_t st);
+/* ebond_slot, wall_e: per-slot bonded and wall energies of the last pass (null when absent) */
+void launch_energy(int ncells, const double *epot_cell, int nparts, const double *ebond_slot, const double *wall_e,
+                   const float4 *vel, const float4 *pos, const DevType *types, double *partials, int nblocks,
+                   double *out, cudaStream_t st);
 
 /* The pairwise bond constructor's pair search (mxg_pairs.cu): pairs (a, b), b < a, of the list ids
  * with |x_a - x_b|^2 <= cutoff^2 in global FP32 coordinates (no periodic image) whose type pair has a

@@ -120,6 +120,38 @@ def lattice(nx=32, spacing=0.5, seed=3, dt=0.005, pull=0.05, dissociation=2.0, k
                 bi=bi, bj=bj, bond_pot=("harmonic", (k, spacing, 0.1, 1.0, 0.009)), dissociation=dissociation)
 
 
+def walls(n=3000, L=8.0, seed=6, dt=0.005, kind="lj", bc_z="potential", temperature=0.5):
+    """A two-type fluid between z walls with wall potentials (the box's other
+    axes periodic). kind "lj": Morse pairs, a repulsive r^-12 wall on both z
+    faces for type 0 and a Morse wall on the top face only for type 1.
+    kind "dpd": a DPD fluid with a DPD wall potential on every face (only the
+    non-periodic z faces act)."""
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0, L, size=(n, 3))
+    x[:, 2] = rng.uniform(0.05, L - 0.05, size=n)
+    x = np.minimum(x, L * (1 - 1e-6)).astype(np.float32).astype(np.float64)
+    t = (np.arange(n) % 2).astype(np.int32)
+    v = rng.normal(0, np.sqrt(temperature), size=(n, 3))
+    v -= v.mean(axis=0)
+    v = v.astype(np.float32).astype(np.float64)
+    cut = 1.0
+    cells = [int(L // cut)] * 3
+    if kind == "dpd":
+        pots = [("dpd", (25.0, 4.5, 3.0, cut, 0), 0, 0), ("dpd", (25.0, 4.5, 3.0, cut, 0), 0, 1),
+                ("dpd", (25.0, 4.5, 3.0, cut, 0), 1, 1)]
+        wall = [(-1, 0, "dpd", (25.0, 4.5, 3.0, cut, 0)), (-1, 1, "dpd", (40.0, 4.5, 3.0, cut, 0))]
+        types = [(1.0, 0.5, m.Newtonian), (1.0, 0.5, m.Newtonian)]
+    else:
+        # shifted Morse tables span r - (ri + rj) + r0 + 1, so max covers the cutoff
+        morse = (0.3, 5.0, 0.6, 1e-4, 2.0, 1e-3)
+        pots = [("morse", morse, 0, 0), ("morse", morse, 0, 1), ("morse", morse, 1, 1)]
+        wall = [(4, 0, "lj126", (0.3, 1.0, 1e-6, 0.0, 1e-3)), (5, 0, "lj126", (0.3, 1.0, 1e-6, 0.0, 1e-3)),
+                (5, 1, "morse", (0.5, 4.0, 0.3, 1e-4, 2.0, 1e-3))]
+        types = [(1.0, 0.3, m.Newtonian), (1.0, 0.3, m.Newtonian)]
+    return dict(dim=[L, L, L], cells=cells, cutoff=cut, dt=dt, bc=("periodic", "periodic", bc_z), types=types,
+                pots=pots, forces=[], x=x, v=v, t=t, wall_pots=wall)
+
+
 def chains(nchains=64, length=32, bond=0.5, L=8.0, seed=5, dt=0.002, k_bond=100.0, k_angle=5.0, theta0=2.0,
            pair=None, cut=1.0, temperature=0.1, dihedral=None):
     """Bead-spring chains in a periodic cube: harmonic bonds between consecutive
@@ -220,6 +252,9 @@ def build_gpu(scn, rng_mode="reference"):
         m.bind(make_potential(kind, params), types[ti], types[tj])
     for (ti, fx, fy, fz) in scn["forces"]:
         m.bind(m.forces.ConstantForce([fx, fy, fz]), types[ti])
+    for (face, ti, kind, params) in scn.get("wall_pots", []):
+        bcs = m.universe.boundary_conditions
+        m.bind(make_potential(kind, params), bcs if face < 0 else getattr(bcs, m._FACES[face]), types[ti])
     x, v, t = scn["x"], scn["v"], scn["t"]
     # create in id order, type by type, keeping ids equal to the scenario's indices
     assert np.all(np.diff(np.flatnonzero(t == t[0])) >= 1)

@@ -20,6 +20,8 @@
  *   mxref_add_bonds       _bond_init (src/mdcore/src/bond.cpp:497-529)
  *   mxref_add_angles      angle_init (src/mdcore/src/angle.cpp:659-707)
  *   mxref_pairwise        MxBond_PairwiseNew (src/mdcore/src/bond.cpp:944-989)
+ *   mxref_bind_boundary_potential  MxBoundaryCondition(s)::set_potential
+ *                         (src/mdcore/src/MxBoundaryConditions.cpp:771-836)
  *   mxref_add_dihedrals   engine_dihedral_addpot + engine_dihedral_add
  *                         (src/mdcore/src/engine_bonded.cpp:1049-1080, 1967-1991)
  *   mxref_step            engine_step (src/mdcore/src/engine.cpp:1198)
@@ -309,6 +311,23 @@ int mxref_pairwise(int n, const int *ids, float cutoff, void *pot, int npairs, c
     if (!bonds) return -1;
     Py_DECREF(bonds);
     return _Engine.nr_bonds - before;
+}
+
+/* bind(pot, boundary condition, type) (src/mdcore/src/MxBind.cpp:74-96): face 0..5 in the order left,
+ * right, front, back, bottom, top (MxBoundaryCondition::set_potential), or -1 for all six
+ * (MxBoundaryConditions::set_potential). */
+int mxref_bind_boundary_potential(int face, int type, void *pot) {
+    if (type < 0 || type >= engine::nr_types) return -1;
+    MxBoundaryConditions &bc = _Engine.boundary_conditions;
+    MxBoundaryCondition *faces[6] = {&bc.left, &bc.right, &bc.front, &bc.back, &bc.bottom, &bc.top};
+    MxParticleType *t = &engine::types[type];
+    if (face < 0)
+        bc.set_potential(t, (MxPotential *)pot);
+    else if (face < 6)
+        faces[face]->set_potential(t, (MxPotential *)pot);
+    else
+        return -1;
+    return 0;
 }
 
 /* Particle ids of the engine's bonds in creation order. */

@@ -23,7 +23,8 @@ A scenario is a dict:
     sbforces [(type, "berendsen" | "random" | "friction", params)] with the forces module's
     arguments: berenderson_tstat(tau), random(std, mean, durration),
     friction(coef, std, mean, durration) (MxForce.cpp:213-259),
-    target_temperature {type: T}
+    target_temperature {type: T},
+    wall_pots [(face or -1, type, kind, params)] (bind(pot, boundary condition, type))
 Results: xabs, xrel, v, f, cell (per id), tasks (rows type, sid, i, j),
     cdim, h, epot, epot_angle, epot_dihedral, ekin, bond_flags, seconds (wall time of the steps).
 """
@@ -48,7 +49,7 @@ def _pack(scn):
     flat = {}
     for k, v in scn.items():
         if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc", "sbforces",
-                 "target_temperature"):
+                 "target_temperature", "wall_pots"):
             flat[k] = np.array(repr(v))
         else:
             flat[k] = np.asarray(v)
@@ -60,7 +61,7 @@ def _unpack(npz):
     for k in npz.files:
         v = npz[k]
         if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc", "sbforces",
-                 "target_temperature"):
+                 "target_temperature", "wall_pots"):
             out[k] = eval(str(v))  # written by _pack from plain literals
         elif v.shape == ():
             out[k] = v.item()
@@ -153,6 +154,12 @@ def _execute(scn):
         q = list(params) + [0.0] * (4 - len(params))
         if L.mxref_bind_singlebody(int(t), code, *[float(v) for v in q]) < 0:
             raise RuntimeError("mxref_bind_singlebody")
+    L.mxref_bind_boundary_potential.argtypes = [ci, ci, vp]
+    for (face, t, kind, params) in scn.get("wall_pots", []):
+        wp = make_pot(kind, params)
+        keep.append(wp)
+        if L.mxref_bind_boundary_potential(int(face), int(t), wp) != 0:
+            raise RuntimeError("mxref_bind_boundary_potential")
     for t, temp in scn.get("target_temperature", {}).items():
         L.mxref_set_target_temperature(int(t), float(temp))
     x = np.ascontiguousarray(scn["x"], dtype=np.float64)

@@ -44,6 +44,9 @@ CASES = [
     ("chains_dihedral", lambda: S.chains(nchains=16, length=24, seed=23, dihedral=(1.5, 3, 0.0, 0.001)), 10),
     ("chains_dihedral_shift", lambda: S.chains(nchains=16, length=24, seed=24, dihedral=(0.8, 2, 1.0, 0.01),
                                                pair=(0.2, 6.0, 0.5, 1e-4, 1.0, 1e-3)), 10),
+    # wall potentials: LJ and Morse walls on "potential" z faces; DPD walls on no-slip z faces
+    ("walls_lj", lambda: S.walls(kind="lj", bc_z="potential", seed=41), 10),
+    ("walls_dpd", lambda: S.walls(kind="dpd", bc_z="no_slip", seed=42), 10),
 ]
 
 TABLES = [
@@ -145,7 +148,7 @@ def make_pairwise():
 def scenario_arrays(scn):
     d = {}
     for k, v in scn.items():
-        if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc"):
+        if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc", "wall_pots"):
             d["scn_" + k] = np.array(repr(v))
         else:
             d["scn_" + k] = np.asarray(v)
@@ -177,7 +180,7 @@ def load_scenario(z):
             continue
         v = z[k]
         key = k[4:]
-        if key in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc"):
+        if key in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc", "wall_pots"):
             scn[key] = eval(str(v))  # plain literals written by scenario_arrays
         elif v.shape == ():
             scn[key] = v.item()
