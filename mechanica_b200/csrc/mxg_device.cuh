@@ -77,7 +77,7 @@ struct DevType {
     double target;       // Berendsen: the type's target temperature
     int bpot[6];         // wall potential per face (left, right, front, back, bottom, top), -1 if none
     unsigned wall_mask;  // active-cell bits of the faces with a wall potential
-    int bpad;
+    int large;           // radius > cutoff: the reference's PARTICLE_LARGE (static, interacts with all)
 };
 
 struct DevSpace {        // one per replica
@@ -178,7 +178,12 @@ struct EngineView {      // everything a kernel needs, passed by value
     const int *sec_count;    // per cell: SECOND entries, i.e. planes of received sums
     const int *cell_planes;  // per cell: received planes plus own-side planes of its later work items
     float4 *planes;          // [plane][slot] neighbour-side force sums of once-evaluated pairs
-    double *wall_e;          // per slot: wall energy of the last pass; null when no type has a wall potential
+    double *body_e;          // per slot: wall and large-particle energy of the last pass; null when neither exists
+    const float4 *large_x;   // large particles: position relative to the replica origin, w = type
+    const float4 *large_v;   // large particles: velocity, w = id
+    const int *large_rep;    // large particles: replica
+    const int *large_pot;    // per replica [ntypes*ntypes]: potential of a (normal, large) type pair, or -1
+    int nlarge;
     const int4 *items;       // force work items: (cell, first entry, end entry, part)
     int nitems;
 };

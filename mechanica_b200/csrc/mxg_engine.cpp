@@ -408,7 +408,10 @@ struct mxg_engine {
     bool has_dpd = false;
     bool has_sb = false;                // a type has a Berendsen, random or friction force
     bool has_walls = false;             // a type has a wall potential
-    double *d_wall_e = nullptr;         // per slot: wall energy of the last pass
+    int nlarge = 0;                     // large particles (radius > cutoff)
+    float4 *d_large_x = nullptr, *d_large_v = nullptr;
+    int *d_large_rep = nullptr, *d_large_pot = nullptr;
+    double *d_body_e = nullptr;         // per slot: wall energy of the last pass
     double *d_type_ke = nullptr;
     float4 *d_persist = nullptr;
     int integrator = 0;                 // 0 forward Euler, 1 Runge-Kutta 4 (engine.h EngineIntegrator)
@@ -578,7 +581,12 @@ struct mxg_engine {
         v.items = d_items;
         v.nitems = nitems;
         v.planes = d_planes;
-        v.wall_e = has_walls ? d_wall_e : nullptr;
+        v.body_e = (has_walls || nlarge) ? d_body_e : nullptr;
+        v.large_x = d_large_x;
+        v.large_v = d_large_v;
+        v.large_rep = d_large_rep;
+        v.large_pot = d_large_pot;
+        v.nlarge = nlarge;
         return v;
     }
 
@@ -855,6 +863,38 @@ int mxg_engine::start(cudaStream_t st) {
             }
         hs.push_back(space_desc(r, r * tt));
     }
+    // ---- large particles (radius > cutoff: PARTICLE_LARGE, MxParticle.cpp:2091-2093): kept in
+    // their cells but static and out of the cell-pair loop; every other particle of the replica
+    // interacts with them through the potential of the type pair (particle_largecell_force)
+    std::vector<char> is_large(ntypes, 0);
+    for (int a = 0; a < (int)types.size(); ++a) is_large[a] = (double)(float)types[a].radius > cutoff;
+    std::vector<float4> hlx, hlv;
+    std::vector<int> hlrep, hlpot((size_t)tt * spaces.size(), -1);
+    for (int id = 0; id < nparts; ++id) {
+        if (!is_large[ptype[id]]) continue;
+        const Space &sp = spaces[prep[id]];
+        float4 q;
+        q.x = (float)(px[3 * (size_t)id] - sp.origin[0]);  // position local to the large-particle cell
+        q.y = (float)(px[3 * (size_t)id + 1] - sp.origin[1]);
+        q.z = (float)(px[3 * (size_t)id + 2] - sp.origin[2]);
+        int t = ptype[id];
+        memcpy(&q.w, &t, 4);
+        hlx.push_back(q);
+        float4 w = make_float4(pv[3 * (size_t)id], pv[3 * (size_t)id + 1], pv[3 * (size_t)id + 2], 0.f);
+        memcpy(&w.w, &id, 4);
+        hlv.push_back(w);
+        hlrep.push_back(prep[id]);
+    }
+    nlarge = (int)hlx.size();
+    for (size_t r = 0; r < spaces.size(); ++r)
+        for (int a = 0; a < ntypes; ++a)
+            for (int b = 0; b < ntypes; ++b) {
+                const size_t k = r * tt + (size_t)a * ntypes + b;
+                if (!is_large[a] && !is_large[b]) continue;
+                if (!is_large[a] && is_large[b]) hlpot[k] = hpidx[k];
+                hpidx[k] = -1;  // large particles take no part in the cell-pair loop
+                hpidx2[k] = -1;
+            }
     has_sb = false;
     has_walls = false;
     std::vector<DevType> ht(ntypes);
@@ -883,6 +923,10 @@ int mxg_engine::start(cudaStream_t st) {
             d.sb_steps = std::max(1, (int)std::ceil(dur / dt));  // durration_steps (MxForce.cpp:403,417)
         }
         if (ti.sb_kind) has_sb = true;
+        if (is_large[a]) {
+            d.large = 1;
+            d.flags |= (1u << 2) | (1u << 3) | (1u << 4);  // never integrated (not in any cell of the reference)
+        }
         const unsigned face_bits[6] = {kCellActiveLeft, kCellActiveRight, kCellActiveFront,
                                        kCellActiveBack, kCellActiveBottom, kCellActiveTop};
         for (int f = 0; f < 6; ++f) {
@@ -1015,7 +1059,11 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_sort_bounds, (size_t)ncells * 13);
     rc |= alloc(&d_epot_cell, nitems);
     rc |= alloc(&d_ebond_slot, nparts);
-    rc |= alloc(&d_wall_e, nparts);
+    rc |= alloc(&d_body_e, nparts);
+    rc |= alloc(&d_large_x, hlx.size());
+    rc |= alloc(&d_large_v, hlv.size());
+    rc |= alloc(&d_large_rep, hlrep.size());
+    rc |= alloc(&d_large_pot, hlpot.size());
     rc |= alloc(&d_bonds, hb.size());
     rc |= alloc(&d_bond_flags, hbf.size());
     rc |= alloc(&d_bond_off, boff.size());
@@ -1038,7 +1086,7 @@ int mxg_engine::start(cudaStream_t st) {
     CUDA_TRY(cudaMemsetAsync(d_step, 0, sizeof(unsigned long long), stream));
     CUDA_TRY(cudaMemsetAsync(d_epot_cell, 0, sizeof(double) * std::max(1, nitems), stream));
     CUDA_TRY(cudaMemsetAsync(d_ebond_slot, 0, sizeof(double) * std::max(1, nparts), stream));
-    CUDA_TRY(cudaMemsetAsync(d_wall_e, 0, sizeof(double) * std::max(1, nparts), stream));
+    CUDA_TRY(cudaMemsetAsync(d_body_e, 0, sizeof(double) * std::max(1, nparts), stream));
     CUDA_TRY(cudaMemsetAsync(d_force, 0, sizeof(float4) * std::max(1, nparts), stream));
     CUDA_TRY(cudaMemsetAsync(d_persist, 0, sizeof(float4) * std::max(1, nparts), stream));
     CUDA_TRY(cudaMemsetAsync(d_type_ke, 0, sizeof(double) * ht.size(), stream));
@@ -1057,6 +1105,8 @@ int mxg_engine::start(cudaStream_t st) {
         (rc = upload(d_bond_off, boff, stream)) || (rc = upload(d_bond_list, blist, stream)) ||
         (rc = upload(d_angles, ha, stream)) || (rc = upload(d_angle_off, aoff, stream)) ||
         (rc = upload(d_angle_list, alist, stream)) || (rc = upload(d_dihedrals, hd, stream)) ||
+        (rc = upload(d_large_x, hlx, stream)) || (rc = upload(d_large_v, hlv, stream)) ||
+        (rc = upload(d_large_rep, hlrep, stream)) || (rc = upload(d_large_pot, hlpot, stream)) ||
         (rc = upload(d_dihedral_off, doff, stream)) || (rc = upload(d_dihedral_list, dlist, stream)))
         return rc;
     CUDA_TRY(cudaStreamSynchronize(stream));
@@ -1654,7 +1704,7 @@ int mxg_engine_energy(mxg_engine *e, double *epot, double *ekin, double *virial9
     if (!e) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
     launch_energy(e->nitems, e->d_epot_cell, e->nparts, e->has_bonded() ? e->d_ebond_slot : nullptr,
-                  e->has_walls ? e->d_wall_e : nullptr, e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
+                  (e->has_walls || e->nlarge) ? e->d_body_e : nullptr, e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
                   e->stream);
     double out[2];
     CUDA_TRY(cudaMemcpyAsync(out, e->d_energy, sizeof(out), cudaMemcpyDeviceToHost, e->stream));
@@ -1753,7 +1803,7 @@ int mxg_engine_energy_async(mxg_engine *e, double *host_out2) {
     if (!e || !host_out2) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
     launch_energy(e->nitems, e->d_epot_cell, e->nparts, e->has_bonded() ? e->d_ebond_slot : nullptr,
-                  e->has_walls ? e->d_wall_e : nullptr, e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
+                  (e->has_walls || e->nlarge) ? e->d_body_e : nullptr, e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
                   e->stream);
     CUDA_TRY(cudaMemcpyAsync(host_out2, e->d_energy, 2 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     return MXG_OK;
@@ -1817,8 +1867,8 @@ int mxg_engine_adjoint_params(mxg_engine *e, int n, const int *pot, const int *p
 int mxg_engine_vjp_step(mxg_engine *e, void *lam_x, void *lam_v, double *grad) {
     if (!e || !lam_x || !lam_v || !grad) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
-    // bonded, single-body and wall forces are not differentiated
-    if (e->has_bonded() || e->has_sb || e->has_walls) return MXG_ERR_ARG;
+    // bonded, single-body, wall and large-particle forces are not differentiated
+    if (e->has_bonded() || e->has_sb || e->has_walls || e->nlarge) return MXG_ERR_ARG;
     if (e->nparts == 0) return MXG_OK;
     if (e->adjoint_stale) {
         const int rc = e->build_adjoint();

@@ -222,6 +222,61 @@ __device__ __noinline__ void boundary_forces(const EngineView &v, const DevSpace
     }
 }
 
+/*
+ * Interactions of one particle with the large particles of its replica
+ * (particle_largecell_force, runner_dopair.cpp:342-434, run from
+ * runner_doself for every particle): the particle's global FP32 position
+ * x_rel + cell origin against each large particle's position, no cutoff other
+ * than the potential's range, the pair evaluated as potential_eval_super_ex
+ * with the particle first (a pair closer than the table minimum gets a Philox
+ * direction of length a instead of the per-cell mt19937 draw). Only the
+ * particle's side is applied: large particles are static.
+ */
+__device__ __noinline__ void large_forces(const EngineView &v, int s, const float4 &x, const float4 &u, float radius,
+                                          float4 &f, double &epot) {
+    const int c = v.cell_of[s];
+    const int rep = v.cell_rep[c];
+    const DevSpace &S = v.spaces[rep];
+    const int l = c - S.cell_offset;
+    const int loc[3] = {l / (S.cdim[1] * S.cdim[2]), (l / S.cdim[2]) % S.cdim[1], l % S.cdim[2]};
+    const float xr[3] = {x.x, x.y, x.z};
+    float pix[3];
+    for (int k = 0; k < 3; ++k)
+        pix[k] = (float)__dadd_rn((double)xr[k], __dadd_rn(S.origin[k], __dmul_rn((double)loc[k], S.hd[k])));
+    const int ti = __float_as_int(x.w);
+    for (int j = 0; j < v.nlarge; ++j) {
+        if (v.large_rep[j] != rep) continue;
+        const float4 xl = v.large_x[j];
+        const int tj = __float_as_int(xl.w);
+        const int q = v.large_pot[S.pot_offset + ti * v.ntypes + tj];
+        if (q < 0) continue;
+        const DevPot &p = v.pots[q];
+        float dx = __fsub_rn(pix[0], xl.x), dy = __fsub_rn(pix[1], xl.y), dz = __fsub_rn(pix[2], xl.z);
+        float r2 = dot3_rn(dx, dy, dz);
+        const float4 ul = v.large_v[j];
+        if (r2 < p.a2) {
+            const unsigned idi = __float_as_uint(u.w), idj = __float_as_uint(ul.w);
+            const unsigned lo = idi < idj ? idi : idj, hi = idi < idj ? idj : idi;
+            float g0, g1, g2;
+            philox_normal3(*v.step, lo, hi, g0, g1, g2);
+            const float len = sqrtf(g0 * g0 + g1 * g1 + g2 * g2);
+            const float sgn = idi == lo ? 1.0f : -1.0f;
+            dx = sgn * g0 * p.a / len;
+            dy = sgn * g1 * p.a / len;
+            dz = sgn * g2 * p.a / len;
+            r2 = p.a2;
+        }
+        float cx, cy, cz, pe;
+        bool counted;
+        pair_contribution<true>(v, p, kRoleFirst, true, dx, dy, dz, r2, radius, v.types[tj].radius, u, ul, S.rng_mode,
+                                cx, cy, cz, pe, counted);
+        f.x += cx;
+        f.y += cy;
+        f.z += cz;
+        epot += (double)pe;
+    }
+}
+
 constexpr int kOwn = 32;            // own particles staged at a time
 constexpr int kCap = 128;           // neighbour particles staged at a time
 constexpr int kChunks = kCap / 32;  // candidate steps per own particle
@@ -687,16 +742,19 @@ __device__ __forceinline__ float4 total_force(const EngineView &v, int s) {
         f.y += g.y;
         f.z += g.z;
     }
-    if (v.wall_e) {
-        // wall potentials of particles in cells next to a bound face (runner_doself's
-        // boundary_eval, runner_dopair.cpp:533-535); the energy goes to the slot's entry
+    if (v.body_e) {
+        // wall potentials of particles in cells next to a bound face and the large
+        // particles' interactions (runner_doself's boundary_eval and
+        // particle_largecell_force, runner_dopair.cpp:526-535); the energy goes to the
+        // slot's entry
         const float4 x = v.pos[s];
         const DevType &T = v.types[__float_as_int(x.w)];
         const int c = v.cell_of[s];
         const unsigned cflags = v.cell_flags[c];
         double ew = 0.0;
         if (cflags & T.wall_mask) boundary_forces(v, v.spaces[v.cell_rep[c]], cflags, T, T.radius, x, v.vel[s], f, ew);
-        v.wall_e[s] = ew;
+        if (v.nlarge && !T.large) large_forces(v, s, x, v.vel[s], T.radius, f, ew);
+        v.body_e[s] = ew;
     }
     if (v.has_sb) {
         // the velocity-dependent and random single-body forces (MxForce.cpp:330-386)
@@ -1439,7 +1497,7 @@ __global__ void scatter_kernel(EngineView v, int ncells, const float4 *__restric
 
 /* Deterministic two-stage sums: block partials, then one block. */
 __global__ void reduce_energy_kernel(int ncells, const double *__restrict__ epot_cell, int nparts,
-                                     const double *__restrict__ ebond_slot, const double *__restrict__ wall_e,
+                                     const double *__restrict__ ebond_slot, const double *__restrict__ body_e,
                                      const float4 *__restrict__ vel,
                                      const float4 *__restrict__ pos, const DevType *__restrict__ types,
                                      double *partials) {
@@ -1448,7 +1506,7 @@ __global__ void reduce_energy_kernel(int ncells, const double *__restrict__ epot
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += gridDim.x * blockDim.x) ep += epot_cell[c];
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nparts; s += gridDim.x * blockDim.x) {
         if (ebond_slot) ep += ebond_slot[s];
-        if (wall_e) ep += wall_e[s];
+        if (body_e) ep += body_e[s];
         const float4 u = vel[s];
         const DevType &T = types[__float_as_int(pos[s].w)];
         // engine_kinetic_energy (engine.cpp:1698-1719): float e = 0.5*mass*|v|^2
@@ -1579,10 +1637,10 @@ void launch_scatter(const EngineView &v, const float4 *pos, const float4 *vel, c
                                          out_count, new_start, pos_out, vel_out, cell_out, slot_of_id);
 }
 
-void launch_energy(int ncells, const double *epot_cell, int nparts, const double *ebond_slot, const double *wall_e,
+void launch_energy(int ncells, const double *epot_cell, int nparts, const double *ebond_slot, const double *body_e,
                    const float4 *vel, const float4 *pos, const DevType *types, double *partials, int nblocks,
                    double *out, cudaStream_t st) {
-    reduce_energy_kernel<<<nblocks, 256, 0, st>>>(ncells, epot_cell, nparts, ebond_slot, wall_e, vel, pos, types,
+    reduce_energy_kernel<<<nblocks, 256, 0, st>>>(ncells, epot_cell, nparts, ebond_slot, body_e, vel, pos, types,
                                                   partials);
     reduce_final_kernel<<<1, 32, 0, st>>>(nblocks, partials, out);
 }

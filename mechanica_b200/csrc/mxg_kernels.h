@@ -30,8 +30,8 @@ void launch_scatter(const EngineView &v, const float4 *pos, const float4 *vel, c
                     const int *old_start, const int *old_count, int *in_count, const int *in_list, int *out_count,
                     const int *new_start, float4 *pos_out, float4 *vel_out, int *cell_out, int *slot_of_id,
                     cudaStream_t st);
-/* ebond_slot, wall_e: per-slot bonded and wall energies of the last pass (null when absent) */
-void launch_energy(int ncells, const double *epot_cell, int nparts, const double *ebond_slot, const double *wall_e,
+/* ebond_slot, body_e: per-slot bonded and wall energies of the last pass (null when absent) */
+void launch_energy(int ncells, const double *epot_cell, int nparts, const double *ebond_slot, const double *body_e,
                    const float4 *vel, const float4 *pos, const DevType *types, double *partials, int nblocks,
                    double *out, cudaStream_t st);
 

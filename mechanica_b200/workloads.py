@@ -152,6 +152,32 @@ def walls(n=3000, L=8.0, seed=6, dt=0.005, kind="lj", bc_z="potential", temperat
                 pots=pots, forces=[], x=x, v=v, t=t, wall_pots=wall)
 
 
+def large(n=3000, L=10.0, nlarge=3, seed=7, dt=0.005, big=2.0, temperature=0.3):
+    """A fluid of small particles (radius 0.3, Morse pairs) around a few large
+    particles (radius big > cutoff 1.0: the reference's PARTICLE_LARGE), which
+    stay put and act on every small particle through a shifted Morse
+    potential. Small particles start outside the large ones' radius."""
+    rng = np.random.default_rng(seed)
+    xl = rng.uniform(big + 0.5, L - big - 0.5, size=(nlarge, 3))
+    x = rng.uniform(0, L, size=(4 * n, 3))
+    keep = np.ones(len(x), dtype=bool)
+    for c in xl:
+        keep &= np.linalg.norm(x - c, axis=1) > big + 0.3
+    x = x[keep][:n]
+    x = np.concatenate([x, xl])
+    x = np.minimum(x, L * (1 - 1e-6)).astype(np.float32).astype(np.float64)
+    t = np.concatenate([np.zeros(len(x) - nlarge, dtype=np.int32), np.ones(nlarge, dtype=np.int32)])
+    v = rng.normal(0, np.sqrt(temperature), size=x.shape)
+    v[t == 1] = 0.0
+    v = v.astype(np.float32).astype(np.float64)
+    cut = 1.0
+    small = (0.3, 5.0, 0.6, 1e-4, 2.0, 1e-3)
+    return dict(dim=[L, L, L], cells=[int(L // cut)] * 3, cutoff=cut, dt=dt, bc=("periodic", "periodic", "periodic"),
+                types=[(1.0, 0.3, m.Newtonian), (10.0, big, m.Newtonian)],
+                pots=[("morse", small, 0, 0), ("morse", (0.5, 3.0, 0.2, 1e-4, 3.0, 1e-3), 0, 1)],
+                forces=[], x=x, v=v, t=t)
+
+
 def chains(nchains=64, length=32, bond=0.5, L=8.0, seed=5, dt=0.002, k_bond=100.0, k_angle=5.0, theta0=2.0,
            pair=None, cut=1.0, temperature=0.1, dihedral=None):
     """Bead-spring chains in a periodic cube: harmonic bonds between consecutive

@@ -47,6 +47,8 @@ CASES = [
     # wall potentials: LJ and Morse walls on "potential" z faces; DPD walls on no-slip z faces
     ("walls_lj", lambda: S.walls(kind="lj", bc_z="potential", seed=41), 10),
     ("walls_dpd", lambda: S.walls(kind="dpd", bc_z="no_slip", seed=42), 10),
+    # a fluid around three static large particles (radius > cutoff)
+    ("large_fluid", lambda: S.large(seed=51), 10),
 ]
 
 TABLES = [
