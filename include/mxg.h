@@ -22,6 +22,9 @@
  *   mxg_engine_addangles           engine_angle_alloc + angle_init src/mdcore/src/angle.cpp:659-707
  *   mxg_engine_set_boundary_potential MxBoundaryCondition(s)::set_potential
  *                                  src/mdcore/src/MxBoundaryConditions.cpp:771-836, via bind (MxBind.cpp:74-96)
+ *   mxg_engine_set_type_species    a particle type's species list (state vector layout)
+ *   mxg_engine_add_flux            MxFluxes_FluxEx src/mdcore/src/Flux.cpp:161-211 (flux, secrete, uptake)
+ *   mxg_engine_set_species / mxg_engine_get_species  the particles' species values
  *   mxg_engine_pairs_within        make_pairlist (the pair search of MxBond_PairwiseNew)
  *                                  src/mdcore/src/bond.cpp:892-942
  *   mxg_engine_adddihedrals        engine_dihedral_addpot + engine_dihedral_add
@@ -234,6 +237,22 @@ int mxg_engine_adddihedrals(mxg_engine *e, int n, const int *i, const int *j, co
  * normal; tables get potential_eval_ex with wall radius 0, DPD potentials dpd_boundary_eval against the
  * wall velocity. */
 int mxg_engine_set_boundary_potential(mxg_engine *e, int face, int type, const mxg_potential *p);
+/* Species (chemical cargo) of a particle type: nspec values per particle (at most 8), flags per species
+ * (bit 2: constant, SPECIES_KONSTANT: not integrated). Before mxg_engine_start. */
+int mxg_engine_set_type_species(mxg_engine *e, int type, int nspec, const unsigned *flags);
+/* A flux between types ta and tb on species ia (of ta) and ib (of tb) (MxFluxes_FluxEx,
+ * src/mdcore/src/Flux.cpp:161-211): kind 0 Fick, k (s_a - s_b); 1 secrete, max(k (s_a - target), 0);
+ * 2 uptake, max(k (target - s_b) s_a, 0); each times (1 - r/cutoff)^2 for every pair within the cutoff
+ * (flux_eval_ex, src/mdcore/src/flux_eval.hpp:33-84); decay removes decay/2 s per pair from each side.
+ * Both orders of a type pair share one list of at most 7 entries (MxFluxes_AddFlux, Flux.cpp:289-317).
+ * After each forward-Euler step, values += dt * rates unless constant, for the particles that kept their
+ * cell in that step; the others carry their rates to the next step (MxFluxes_Integrate, Flux.cpp:261-285,
+ * run per cell after the cell's particles moved). Before mxg_engine_start. */
+int mxg_engine_add_flux(mxg_engine *e, int kind, int ta, int tb, int ia, int ib, float k, float decay, float target);
+/* Species values by particle id, values[id * smax + k] for the type's first nspec species. Before start
+ * they are staged; after, they replace the device values. */
+int mxg_engine_set_species(mxg_engine *e, int n, int smax, const float *values);
+int mxg_engine_get_species(mxg_engine *e, int n, int smax, float *out);
 /* The pair search of the pairwise bond constructor (make_pairlist, src/mdcore/src/bond.cpp:892-942), on
  * the device over the current state of a started engine: the pairs (ids[a], ids[b]), b < a, of the n
  * listed particles (one replica) whose global FP32 positions are within cutoff (|dx|^2 <= cutoff^2 summed

@@ -27,7 +27,7 @@ from . import _native
 from ._native import EngineError, check, f32, f64, i32, lib, ptr
 
 __all__ = [
-    "init", "Universe", "universe", "Particle", "Potential", "Bond", "Angle", "Dihedral", "bind", "forces", "step", "run",
+    "init", "Universe", "universe", "Particle", "Potential", "Bond", "Angle", "Dihedral", "flux", "fick", "secrete", "uptake", "bind", "forces", "step", "run",
     "Newtonian", "Overdamped", "FORWARD_EULER", "RUNGE_KUTTA_4", "BOUNDARY_NONE", "PERIODIC_X", "PERIODIC_Y", "PERIODIC_Z",
     "PERIODIC_FULL", "FREESLIP_X", "FREESLIP_Y", "FREESLIP_Z", "FREESLIP_FULL", "EngineError",
 ]
@@ -384,12 +384,52 @@ def _pid(p):
     return p.id if isinstance(p, Particle) else int(p)
 
 
+class _SpeciesView:
+    """A particle's species values by name (``p.species.S1``, ``p.species.S1 = 0.5``)."""
+
+    def __init__(self, pid, tid):
+        object.__setattr__(self, "_pid", pid)
+        object.__setattr__(self, "_tid", tid)
+
+    def _index(self, name):
+        return universe._species_index(self._tid, name)[1]
+
+    def __getattr__(self, name):
+        if name.startswith("_"):
+            raise AttributeError(name)
+        k = self._index(name)
+        if universe._started and not universe._dirty:
+            return float(universe.species_values()[self._pid, k])
+        return float(universe._spec[self._pid, k])
+
+    def __setattr__(self, name, value):
+        k = self._index(name)
+        universe._sync_state()
+        universe._spec[self._pid, k] = float(value)
+        if universe._started and not universe._dirty:
+            universe.set_species_values(universe._spec)
+
+
+class _SpeciesAttr:
+    """``Type.species`` is the type's species list; ``particle.species`` its values."""
+
+    def __init__(self, names):
+        self.names = list(names)
+
+    def __get__(self, obj, cls=None):
+        if obj is None:
+            return self.names
+        return _SpeciesView(obj.id, type(obj).id)
+
+
 class _ParticleMeta(type):
     def __init__(cls, name, bases, ns):
         super().__init__(name, bases, ns)
         if bases and any(isinstance(b, _ParticleMeta) for b in bases):
             u = _require()
             cls.id = u._add_type(cls)
+            if isinstance(ns.get("species"), (list, tuple)):
+                cls.species = _SpeciesAttr(ns["species"])
 
     def factory(cls, positions=None, velocities=None, nr_parts=None, replica=0):
         """Bulk creation of particles of this type from arrays (N x 3)."""
@@ -465,6 +505,10 @@ class _Universe:
         self._angles = []       # (potential, i[], j[], k[])
         self._dihedrals = []    # (potential, i[], j[], k[], l[])
         self._bpots = []        # wall potentials: (potential, face or -1, type)
+        self._species = {}      # type -> (species names, flags)
+        self._spec_width = 0
+        self._spec = np.zeros((0, 0), dtype=np.float32)  # species values by particle id
+        self._fluxes = []       # (kind, type a, type b, species a, species b, k, decay, target)
         self._x = np.zeros((0, 3))
         self._v = np.zeros((0, 3), dtype=np.float32)
         self._t = np.zeros(0, dtype=np.int32)
@@ -521,6 +565,12 @@ class _Universe:
         for (p, ii, jj, kk) in self._angles:
             check(lib().mxg_engine_addangles(self._e, len(ii), ptr(ii, ctypes.c_int), ptr(jj, ctypes.c_int),
                                              ptr(kk, ctypes.c_int), p._h, None), "addangles")
+        for t, (names, flags) in self._species.items():
+            fl = np.asarray(flags, dtype=np.uint32)
+            check(lib().mxg_engine_set_type_species(self._e, t, len(names), fl.ctypes.data_as(ctypes.c_void_p)),
+                  "set_type_species")
+        for f in self._fluxes:
+            check(lib().mxg_engine_add_flux(self._e, *f), "add_flux")
         for (p, face, t) in self._bpots:
             check(lib().mxg_engine_set_boundary_potential(self._e, face, t, p._h), "set_boundary_potential")
         for (p, ii, jj, kk, ll) in self._dihedrals:
@@ -537,6 +587,17 @@ class _Universe:
         if tid is None:
             self._dirty = True
             tid = len(self._types) - 1
+        names = getattr(cls, "species", None)
+        if isinstance(names, _SpeciesAttr):
+            names = names.names
+        if names:
+            # species list ("$" marks a constant species, SPECIES_KONSTANT)
+            names = [str(s) for s in names]
+            self._species[tid] = ([s.lstrip("$") for s in names], [4 if s.startswith("$") else 0 for s in names])
+            self._spec_width = max(self._spec_width, len(names))
+            if self._spec.shape[1] < self._spec_width:
+                self._spec = np.pad(self._spec, ((0, 0), (0, self._spec_width - self._spec.shape[1])))
+            self._dirty = True
         if getattr(cls, "target_temperature", None) is not None:
             self._targets[tid] = float(cls.target_temperature)
             if self._started:
@@ -548,6 +609,7 @@ class _Universe:
     def _add_particles(self, x, v, t, replica=0):
         first = len(self._t)
         self._sync_state()
+        self._spec = np.concatenate([self._spec, np.zeros((len(t), self._spec.shape[1]), dtype=np.float32)])
         self._x = np.concatenate([self._x, np.asarray(x, dtype=np.float64)])
         self._v = np.concatenate([self._v, np.asarray(v, dtype=np.float32)])
         self._t = np.concatenate([self._t, np.asarray(t, dtype=np.int32)])
@@ -570,6 +632,44 @@ class _Universe:
         self._sync_state()
         self._dirty = True
         return list(range(first, first + len(ii)))
+
+    # ---- species (chemical cargo) and fluxes ----
+    def _species_index(self, cls, name):
+        t = cls.id if isinstance(cls, type) else int(cls)
+        if t not in self._species:
+            raise ValueError(f"particle type {getattr(cls, '__name__', t)} does not have any defined species")
+        names = self._species[t][0]
+        if name not in names:
+            raise ValueError(f"particle type {getattr(cls, '__name__', t)} does not have species {name}")
+        return t, names.index(name)
+
+    def _add_flux(self, kind, a, b, name, k, decay, target):
+        ta, ia = self._species_index(a, name)
+        tb, ib = self._species_index(b, name)
+        key = (min(ta, tb), max(ta, tb))
+        if sum(1 for f in self._fluxes if (min(f[1], f[2]), max(f[1], f[2])) == key) + 1 >= 8:
+            raise ValueError("at most 7 fluxes per pair of types")  # MxFluxes_AddFlux's limit
+        self._sync_state()
+        self._fluxes.append((int(kind), ta, tb, ia, ib, float(k), float(decay), float(target)))
+        self._dirty = True
+
+    def species_values(self):
+        """Species values by particle id (N x the widest type's species count)."""
+        self._ensure()
+        if not self._spec_width:
+            return np.zeros((len(self._t), 0), dtype=np.float32)
+        out = np.zeros((len(self._t), self._spec.shape[1]), dtype=np.float32)
+        check(lib().mxg_engine_get_species(self._e, len(self._t), out.shape[1], ptr(out, ctypes.c_float)),
+              "get_species")
+        return out
+
+    def set_species_values(self, values):
+        """Replaces the species values (N x width, by particle id)."""
+        vals = np.ascontiguousarray(values, dtype=np.float32)
+        self._spec = vals.copy()
+        if self._started and not self._dirty:
+            check(lib().mxg_engine_set_species(self._e, vals.shape[0], vals.shape[1], ptr(vals, ctypes.c_float)),
+                  "set_species")
 
     @property
     def boundary_conditions(self):
@@ -688,6 +788,10 @@ class _Universe:
             check(lib().mxg_engine_unload(self._e, n, ptr(x, ctypes.c_double), ptr(v, ctypes.c_float), None, None,
                                           None), "unload")
             self._x, self._v = x, v
+            if self._spec_width and self._spec.shape[1]:
+                sp = np.zeros((n, self._spec.shape[1]), dtype=np.float32)
+                check(lib().mxg_engine_get_species(self._e, n, sp.shape[1], ptr(sp, ctypes.c_float)), "get_species")
+                self._spec = sp
 
     def _ensure(self):
         if self._started and not self._dirty:
@@ -706,6 +810,9 @@ class _Universe:
                                                     ptr(f32(self._v[k:e]), ctypes.c_float),
                                                     ptr(i32(self._t[k:e]), ctypes.c_int), None), "addparts")
             k = e
+        if self._spec_width:
+            sp = np.ascontiguousarray(self._spec, dtype=np.float32)
+            check(lib().mxg_engine_set_species(self._e, n, sp.shape[1], ptr(sp, ctypes.c_float)), "set_species")
         check(lib().mxg_engine_start(self._e, ctypes.c_void_p(self.stream) if self.stream else None),
               "engine_start")
         self._started = True
@@ -864,6 +971,25 @@ def init(dim=(10.0, 10.0, 10.0), cutoff=1.0, cells=(4, 4, 4), dt=0.01, bc=None, 
 
 def bind(obj, a, b=None, replica=0):
     return _require().bind(obj, a, b, replica)
+
+
+def flux(A, B, name, k, decay=0.0):
+    """Fickian flux of species `name` between types A and B: k (s_a - s_b) (1 - r/cutoff)^2 per
+    pair within the cutoff (MxFluxes_Fick, Flux.cpp:213-227)."""
+    _require()._add_flux(0, A, B, name, k, decay, 0.0)
+
+
+fick = flux
+
+
+def secrete(A, B, name, k, target, decay=0.0):
+    """Secretion of `name` from A to B: max(k (s_a - target), 0) per pair (MxFluxes_Secrete)."""
+    _require()._add_flux(1, A, B, name, k, decay, target)
+
+
+def uptake(A, B, name, k, target, decay=0.0):
+    """Uptake of `name` by B from A: max(k (target - s_b) s_a, 0) per pair (MxFluxes_Uptake)."""
+    _require()._add_flux(2, A, B, name, k, decay, target)
 
 
 def step(until=0, dt=0):

@@ -79,6 +79,10 @@ _SIGS = {
     "mxg_engine_addbonds": ([_vp, ctypes.c_int, _c_int_p, _c_int_p, _vp, ctypes.c_double, _c_int_p], ctypes.c_int),
     "mxg_engine_addangles": ([_vp, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p, _vp, _c_int_p], ctypes.c_int),
     "mxg_engine_set_boundary_potential": ([_vp, ctypes.c_int, ctypes.c_int, _vp], ctypes.c_int),
+    "mxg_engine_set_type_species": ([_vp, ctypes.c_int, ctypes.c_int, _vp], ctypes.c_int),
+    "mxg_engine_add_flux": ([_vp] + [ctypes.c_int] * 5 + [ctypes.c_float] * 3, ctypes.c_int),
+    "mxg_engine_set_species": ([_vp, ctypes.c_int, ctypes.c_int, _c_float_p], ctypes.c_int),
+    "mxg_engine_get_species": ([_vp, ctypes.c_int, ctypes.c_int, _c_float_p], ctypes.c_int),
     "mxg_engine_pairs_within": ([_vp, ctypes.c_int, _c_int_p, ctypes.c_float, _vp, ctypes.c_int, _c_int_p, _c_int_p,
                                  ctypes.c_int, _c_int_p], ctypes.c_int),
     "mxg_engine_adddihedrals": ([_vp, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p, _c_int_p, _vp, _c_int_p],

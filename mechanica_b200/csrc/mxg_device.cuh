@@ -100,6 +100,8 @@ struct DevSpace {        // one per replica
     float sort_dscale;   // SHRT_MAX / (2 |h|)
     int dmaxdist;        // 2 + dscale * cutoff
     int pad2;
+    double dt_d;         // the engine's dt in double (species integration)
+    double cutoff_d;     // the space's cutoff in double (flux weight)
 };
 
 /* normalised sort directions of the 13 sort lists (space_cell.cpp:82-96) */
@@ -141,6 +143,28 @@ struct BondedView {
     const int *dihedral_list;
     const int *slot_of_id;
     double *e_slot;      // per slot: bonded energy of the last pass
+};
+
+struct DevFlux {         // one flux entry of a type pair's flux list (MxFlux, Flux.hpp)
+    int kind;            // 0 Fick, 1 secrete, 2 uptake
+    int ta, tb;          // the entry's type pair (a: loses, b: gains for a positive q)
+    int ia, ib;          // species index in a's and b's state vectors
+    float k, decay, target;
+};
+
+/* Species state vectors and fluxes, by particle id (values and rates are
+ * smax floats per particle; a type uses the first nspec of them). */
+struct SpeciesView {
+    float *value;            // [id * smax + k]
+    float *rate;             // [id * smax + k]: flux sum not yet integrated
+    const int *nspec;        // per type
+    const unsigned *flags;   // per type and species: bit 2 = constant (not integrated)
+    const int *flux_off;     // per type pair [ntypes*ntypes + 1]: the pair's entries
+    const DevFlux *flux;
+    const int *fx_off;       // per cell: full neighbour list (SELF, FIRST and SECOND entries)
+    const int *fx_cell;
+    const float4 *fx_shift;  // xyz shift of the task, w = role | sort id << 2 | key shift << 8
+    int smax;
 };
 
 struct EngineView {      // everything a kernel needs, passed by value

@@ -346,6 +346,18 @@ struct mxg_engine {
     std::vector<BondInfo> bonds;
     std::vector<AngleInfo> angles;
     std::vector<DihedralInfo> dihedrals;
+    // ---- species and fluxes ----
+    std::vector<int> type_nspec;               // per type (0: no state vector)
+    std::vector<std::vector<unsigned>> type_sflags;  // per type and species (bit 2: constant)
+    std::vector<std::vector<DevFlux>> flux_lists;    // per unordered type pair (a <= b): a * max_type + b
+    std::vector<float> spec_host;              // staged values, nparts * smax
+    int smax = 0;
+    float *d_spec = nullptr, *d_rate = nullptr;
+    int *d_nspec = nullptr, *d_flux_off = nullptr, *d_fx_off = nullptr, *d_fx_cell = nullptr;
+    unsigned *d_sflags = nullptr;
+    DevFlux *d_flux = nullptr;
+    float4 *d_fx_shift = nullptr;
+    bool has_fluxes = false;
 
     // ---- device ----
     bool started = false;
@@ -483,6 +495,8 @@ struct mxg_engine {
             S.origin[k] = sp.origin[k];
         }
         S.dt = dtf;
+        S.dt_d = dt;
+        S.cutoff_d = cutoff;
         const float cf = (float)cutoff;
         S.cut2_pair = cf * cf;                  // runner_dopair: float cutoff squared
         S.cut2_self = (float)(cutoff * cutoff);  // runner_doself: s->cutoff2 (double) as float
@@ -617,6 +631,22 @@ struct mxg_engine {
         if (has_sb) launch_singlebody_prep(v, ntypes, d_type_ke, d_persist, false, stream);
         launch_force(v, has_dpd, force_grid, !has_bonded(), stream);
         if (has_bonded()) launch_bonded(v, bonded_view(), stream);
+        if (has_fluxes) launch_fluxes(v, species_view(), stream);
+    }
+
+    SpeciesView species_view() const {
+        SpeciesView sp;
+        sp.value = d_spec;
+        sp.rate = d_rate;
+        sp.nspec = d_nspec;
+        sp.flags = d_sflags;
+        sp.flux_off = d_flux_off;
+        sp.flux = d_flux;
+        sp.fx_off = d_fx_off;
+        sp.fx_cell = d_fx_cell;
+        sp.fx_shift = d_fx_shift;
+        sp.smax = smax;
+        return sp;
     }
 
     /* One step (engine_step): force pass, bonded pass, integrator and re-binning;
@@ -633,8 +663,10 @@ struct mxg_engine {
         if (has_sb) launch_singlebody_prep(v, ntypes, d_type_ke, d_persist, true, stream);
         launch_force(v, has_dpd, force_grid, false, stream);
         if (has_bonded()) launch_bonded(v, bonded_view(), stream);
+        if (has_fluxes) launch_fluxes(v, species_view(), stream);
         launch_integrate(v, d_pos[b], d_vel[b], d_new_cell, d_in_count, d_in_list, d_out_count, !has_bonded(),
                          stream);
+        if (has_fluxes) launch_species_integrate(v, species_view(), d_new_cell, stream);  // MxFluxes_Integrate
         launch_scan(ncells, d_cell_count[b], d_out_count, d_in_count, d_cell_start[nb], d_cell_count[nb], d_step,
                     stream);
         launch_scatter(v, d_pos[b], d_vel[b], d_new_cell, d_cell_start[b], d_cell_count[b], d_in_count, d_in_list,
@@ -801,6 +833,39 @@ int mxg_engine::start(cudaStream_t st) {
             }
         }
     }
+    // ---- species fluxes: every task of each cell (SELF, FIRST and SECOND entries) for the
+    // full-shell flux pass, per-type species tables and the type pairs' flux lists ----
+    std::vector<int> fx_off(ncells + 1, 0), fx_cell, hnspec(ntypes, 0), hfoff((size_t)ntypes * ntypes + 1, 0);
+    std::vector<float4> fx_shift;
+    std::vector<unsigned> hsflags;
+    std::vector<DevFlux> hflux;
+    smax = 0;
+    for (int a = 0; a < (int)type_nspec.size() && a < ntypes; ++a) {
+        hnspec[a] = type_nspec[a];
+        smax = std::max(smax, type_nspec[a]);
+    }
+    hsflags.assign((size_t)ntypes * std::max(1, smax), 0u);
+    for (int a = 0; a < (int)type_sflags.size() && a < ntypes; ++a)
+        for (int k = 0; k < (int)type_sflags[a].size() && k < smax; ++k) hsflags[(size_t)a * smax + k] = type_sflags[a][k];
+    for (int a = 0; a < ntypes; ++a)
+        for (int b = 0; b < ntypes; ++b) {
+            const size_t key = (size_t)std::min(a, b) * max_type + std::max(a, b);
+            if (smax > 0 && key < flux_lists.size())
+                for (const DevFlux &f : flux_lists[key]) hflux.push_back(f);
+            hfoff[(size_t)a * ntypes + b + 1] = (int)hflux.size();
+        }
+    has_fluxes = smax > 0 && !hflux.empty();
+    if (has_fluxes) {
+        for (int c = 0; c < ncells; ++c) {
+            for (const NbEntry &e : nb[c]) {
+                fx_cell.push_back(e.cell);
+                fx_shift.push_back(e.shift);  // w: role | sort id << 2 | key shift << 8
+            }
+            fx_off[c + 1] = (int)fx_cell.size();
+        }
+    }
+    if (smax > 0 && spec_host.size() != (size_t)nparts * smax) spec_host.resize((size_t)nparts * smax, 0.0f);
+
     // ---- work items: each cell's SELF and FIRST entries split into up to `parts`
     // groups (one warp each) when there are too few cells to fill the GPU. Item k > 0
     // of a cell sums its own-side forces into plane sec_count + k - 1 of the cell.
@@ -1060,6 +1125,15 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_epot_cell, nitems);
     rc |= alloc(&d_ebond_slot, nparts);
     rc |= alloc(&d_body_e, nparts);
+    rc |= alloc(&d_spec, (size_t)nparts * smax);
+    rc |= alloc(&d_rate, (size_t)nparts * smax);
+    rc |= alloc(&d_nspec, hnspec.size());
+    rc |= alloc(&d_sflags, hsflags.size());
+    rc |= alloc(&d_flux_off, hfoff.size());
+    rc |= alloc(&d_flux, hflux.size());
+    rc |= alloc(&d_fx_off, fx_off.size());
+    rc |= alloc(&d_fx_cell, fx_cell.size());
+    rc |= alloc(&d_fx_shift, fx_shift.size());
     rc |= alloc(&d_large_x, hlx.size());
     rc |= alloc(&d_large_v, hlv.size());
     rc |= alloc(&d_large_rep, hlrep.size());
@@ -1087,6 +1161,7 @@ int mxg_engine::start(cudaStream_t st) {
     CUDA_TRY(cudaMemsetAsync(d_epot_cell, 0, sizeof(double) * std::max(1, nitems), stream));
     CUDA_TRY(cudaMemsetAsync(d_ebond_slot, 0, sizeof(double) * std::max(1, nparts), stream));
     CUDA_TRY(cudaMemsetAsync(d_body_e, 0, sizeof(double) * std::max(1, nparts), stream));
+    if (smax > 0) CUDA_TRY(cudaMemsetAsync(d_rate, 0, sizeof(float) * (size_t)nparts * smax, stream));
     CUDA_TRY(cudaMemsetAsync(d_force, 0, sizeof(float4) * std::max(1, nparts), stream));
     CUDA_TRY(cudaMemsetAsync(d_persist, 0, sizeof(float4) * std::max(1, nparts), stream));
     CUDA_TRY(cudaMemsetAsync(d_type_ke, 0, sizeof(double) * ht.size(), stream));
@@ -1106,6 +1181,10 @@ int mxg_engine::start(cudaStream_t st) {
         (rc = upload(d_angles, ha, stream)) || (rc = upload(d_angle_off, aoff, stream)) ||
         (rc = upload(d_angle_list, alist, stream)) || (rc = upload(d_dihedrals, hd, stream)) ||
         (rc = upload(d_large_x, hlx, stream)) || (rc = upload(d_large_v, hlv, stream)) ||
+        (rc = upload(d_spec, spec_host, stream)) || (rc = upload(d_nspec, hnspec, stream)) ||
+        (rc = upload(d_sflags, hsflags, stream)) || (rc = upload(d_flux_off, hfoff, stream)) ||
+        (rc = upload(d_flux, hflux, stream)) || (rc = upload(d_fx_off, fx_off, stream)) ||
+        (rc = upload(d_fx_cell, fx_cell, stream)) || (rc = upload(d_fx_shift, fx_shift, stream)) ||
         (rc = upload(d_large_rep, hlrep, stream)) || (rc = upload(d_large_pot, hlpot, stream)) ||
         (rc = upload(d_dihedral_off, doff, stream)) || (rc = upload(d_dihedral_list, dlist, stream)))
         return rc;
@@ -1588,6 +1667,82 @@ int mxg_engine_set_boundary_potential(mxg_engine *e, int face, int type, const m
     const int idx = (int)e->pots.size() - 1;
     for (int f = 0; f < 6; ++f)
         if (face < 0 || f == face) e->types[type].bpot[f] = idx;
+    return MXG_OK;
+}
+
+int mxg_engine_set_type_species(mxg_engine *e, int type, int nspec, const unsigned *flags) {
+    if (!e || (nspec > 0 && !flags)) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    if (type < 0 || type >= (int)e->types.size()) return MXG_ERR_RANGE;
+    if (nspec < 0 || nspec > 8) return MXG_ERR_ARG;  // state vectors of up to 8 species
+    if ((int)e->type_nspec.size() <= type) {
+        e->type_nspec.resize(type + 1, 0);
+        e->type_sflags.resize(type + 1);
+    }
+    e->type_nspec[type] = nspec;
+    e->type_sflags[type].assign(flags, flags + nspec);
+    return MXG_OK;
+}
+
+int mxg_engine_add_flux(mxg_engine *e, int kind, int ta, int tb, int ia, int ib, float k, float decay, float target) {
+    if (!e) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    const int nt = (int)e->types.size();
+    if (kind < 0 || kind > 2 || ta < 0 || tb < 0 || ta >= nt || tb >= nt) return MXG_ERR_ARG;
+    auto nsp = [&](int t) { return t < (int)e->type_nspec.size() ? e->type_nspec[t] : 0; };
+    if (ia < 0 || ib < 0 || ia >= nsp(ta) || ib >= nsp(tb)) return MXG_ERR_RANGE;
+    const size_t key = (size_t)std::min(ta, tb) * e->max_type + std::max(ta, tb);
+    if (e->flux_lists.size() <= key) e->flux_lists.resize(key + 1);
+    // one flux object of 8 slots per type pair holds at most 7 entries (MxFluxes_AddFlux, Flux.cpp:294-303)
+    if (e->flux_lists[key].size() + 1 >= 8) return MXG_ERR_RANGE;
+    DevFlux f;
+    f.kind = kind;
+    f.ta = ta;
+    f.tb = tb;
+    f.ia = ia;
+    f.ib = ib;
+    f.k = k;
+    f.decay = decay;
+    f.target = target;
+    e->flux_lists[key].push_back(f);
+    return MXG_OK;
+}
+
+int mxg_engine_set_species(mxg_engine *e, int n, int smax, const float *values) {
+    if (!e || (n > 0 && !values)) return MXG_ERR_NULL;
+    if (smax <= 0 || smax > 8) return MXG_ERR_ARG;
+    if (!e->started) {
+        // staged by particle id, at the width the start will use
+        int width = 0;
+        for (int t : e->type_nspec) width = std::max(width, t);
+        if (width == 0) return MXG_ERR_STATE;
+        const int np = (int)e->ptype.size();
+        e->spec_host.assign((size_t)np * width, 0.0f);
+        for (int id = 0; id < n && id < np; ++id)
+            for (int k = 0; k < std::min(smax, width); ++k) e->spec_host[(size_t)id * width + k] = values[(size_t)id * smax + k];
+        return MXG_OK;
+    }
+    if (e->smax == 0) return MXG_ERR_STATE;
+    std::vector<float> buf((size_t)e->nparts * e->smax, 0.0f);
+    CUDA_TRY(cudaMemcpyAsync(buf.data(), e->d_spec, sizeof(float) * buf.size(), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    for (int id = 0; id < n && id < e->nparts; ++id)
+        for (int k = 0; k < std::min(smax, e->smax); ++k) buf[(size_t)id * e->smax + k] = values[(size_t)id * smax + k];
+    CUDA_TRY(cudaMemcpyAsync(e->d_spec, buf.data(), sizeof(float) * buf.size(), cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return MXG_OK;
+}
+
+int mxg_engine_get_species(mxg_engine *e, int n, int smax, float *out) {
+    if (!e || (n > 0 && !out)) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    if (smax <= 0) return MXG_ERR_ARG;
+    if (e->smax == 0) return MXG_OK;
+    std::vector<float> buf((size_t)e->nparts * e->smax);
+    CUDA_TRY(cudaMemcpyAsync(buf.data(), e->d_spec, sizeof(float) * buf.size(), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    for (int id = 0; id < n && id < e->nparts; ++id)
+        for (int k = 0; k < std::min(smax, e->smax); ++k) out[(size_t)id * smax + k] = buf[(size_t)id * e->smax + k];
     return MXG_OK;
 }
 

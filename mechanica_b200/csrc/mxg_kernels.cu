@@ -790,6 +790,130 @@ __device__ __forceinline__ float4 total_force(const EngineView &v, int s) {
     return f;
 }
 
+/* ------------------------------------------------------------------------ */
+/* species fluxes                                                            */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Flux rates of one particle (flux_eval_ex, flux_eval.hpp:33-84, evaluated in
+ * the reference's pair loops for every pair within the cutoff whose types have
+ * fluxes, runner_dopair.cpp:197-252, 555-611). One thread per particle visits
+ * all its neighbour cells (full shell). Each pair is evaluated in the
+ * reference's orientation (the FIRST cell's particle first; in a cell, the
+ * lower slot first), so both of its particles compute the same weight
+ * (1 - r/cutoff)^2 and the same q for every entry of the pair's flux list and
+ * each applies its own share: the entry's a particle q_a = q_a - q - decay/2 s_a,
+ * its b particle q_b = q_b + q - decay/2 s_b. A cell pair that the reference's
+ * sorted loop skips as a whole (its unsigned exit test, runner_dopair.cpp:
+ * 167-171) carries no fluxes either. The rates accumulate on top of what the
+ * particle carries (cleared when its values are integrated).
+ */
+__global__ void flux_kernel(EngineView v, SpeciesView sp) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= v.nparts) return;
+    const float4 xo = v.pos[s];
+    const int to = __float_as_int(xo.w);
+    const int id = __float_as_int(v.vel[s].w);
+    const int nso = sp.nspec[to];
+    if (nso <= 0) return;
+    float *rate = sp.rate + (size_t)id * sp.smax;
+    float acc[8];
+    for (int k = 0; k < 8; ++k) acc[k] = k < sp.smax ? rate[k] : 0.f;
+    const int c = v.cell_of[s];
+    const DevSpace &S = v.spaces[v.cell_rep[c]];
+    const bool exit_test = (S.prune & 2) != 0;
+    for (int e = sp.fx_off[c]; e < sp.fx_off[c + 1]; ++e) {
+        const int nc = sp.fx_cell[e];
+        const float4 sh = sp.fx_shift[e];
+        const int pk = __float_as_int(sh.w);
+        const int role = pk & 3;
+        if (exit_test && role != kRoleSelf) {
+            // kmin(second) + dnshift - kmax(first) in unsigned arithmetic, as the force pass
+            const int sid = (pk >> 2) & 15;
+            const int cf = role == kRoleFirst ? c : nc, cs = role == kRoleFirst ? nc : c;
+            const int2 bf = v.sort_bounds[cf * 13 + sid], bs = v.sort_bounds[cs * 13 + sid];
+            const int gap = bs.x + (pk >> 8) - bf.y;
+            if (v.cell_count[cf] > 0 && v.cell_count[cs] > 0 && (gap < 0 || gap > S.dmaxdist)) continue;
+        }
+        const int j0 = v.cell_start[nc], j1 = j0 + v.cell_count[nc];
+        for (int j = j0; j < j1; ++j) {
+            if (j == s) continue;
+            const float4 xj = v.pos[j];
+            const int tj = __float_as_int(xj.w);
+            bool own_first;
+            float dx, dy, dz;
+            if (role == kRoleSelf) {
+                own_first = s < j;
+                const float4 &a = own_first ? xo : xj, &b = own_first ? xj : xo;
+                dx = __fsub_rn(a.x, b.x);
+                dy = __fsub_rn(a.y, b.y);
+                dz = __fsub_rn(a.z, b.z);
+            } else {
+                own_first = role == kRoleFirst;
+                const float4 &a = own_first ? xo : xj, &b = own_first ? xj : xo;
+                dx = __fsub_rn(__fsub_rn(a.x, sh.x), b.x);
+                dy = __fsub_rn(__fsub_rn(a.y, sh.y), b.y);
+                dz = __fsub_rn(__fsub_rn(a.z, sh.z), b.z);
+            }
+            const float r2 = dot3_rn(dx, dy, dz);
+            // the pair loop's float cutoff squared; the cell loop's double one as float
+            if (r2 > (role == kRoleSelf ? S.cut2_self : S.cut2_pair)) continue;
+            const int t1 = own_first ? to : tj, t2 = own_first ? tj : to;
+            const int f0 = sp.flux_off[t1 * v.ntypes + t2], f1 = sp.flux_off[t1 * v.ntypes + t2 + 1];
+            if (f0 == f1) continue;
+            const int id_j = __float_as_int(v.vel[j].w);
+            const int id1 = own_first ? id : id_j, id2 = own_first ? id_j : id;
+            const float r = __fsqrt_rn(r2);
+            float w = (float)__dsub_rn(1.0, __ddiv_rn((double)r, S.cutoff_d));
+            w = __fmul_rn(w, w);
+            for (int q = f0; q < f1; ++q) {
+                const DevFlux F = sp.flux[q];
+                // flux_eval_ex: pi is the pair's particle of type a (the first when both are),
+                // pj the one of type b (the second when both are)
+                const int ida = t1 == F.ta ? id1 : id2, idb = t2 == F.tb ? id2 : id1;
+                const float sa = sp.value[(size_t)ida * sp.smax + F.ia], sb = sp.value[(size_t)idb * sp.smax + F.ib];
+                float g;
+                if (F.kind == 0) {
+                    g = __fmul_rn(F.k, __fsub_rn(sa, sb));
+                } else if (F.kind == 1) {
+                    const float u = __fmul_rn(F.k, __fsub_rn(sa, F.target));
+                    g = __fmul_rn(u > 0.f ? 1.f : 0.f, u);
+                } else {
+                    const float u = __fmul_rn(__fmul_rn(F.k, __fsub_rn(F.target, sb)), sa);
+                    g = __fmul_rn(u > 0.f ? 1.f : 0.f, u);
+                }
+                const float qq = __fmul_rn(w, g);
+                const float hd = __fdiv_rn(F.decay, 2.f);
+                if (ida == id && F.ia < 8) acc[F.ia] = __fsub_rn(__fsub_rn(acc[F.ia], qq), __fmul_rn(hd, sa));
+                if (idb == id && F.ib < 8) acc[F.ib] = __fsub_rn(__fadd_rn(acc[F.ib], qq), __fmul_rn(hd, sb));
+            }
+        }
+    }
+    for (int k = 0; k < sp.smax && k < 8; ++k) rate[k] = acc[k];
+}
+
+/* Species update after a forward-Euler step (integrate_statevector,
+ * Flux.cpp:261-267): value += dt * rate (in double, rounded to float) unless
+ * the species is constant, then the rate is cleared. The reference runs it per
+ * cell after that cell's particles have moved (engine_advance.cpp:339-343), so
+ * a particle that changed cells in this step is in no cell's list at that
+ * moment: its values stay and its rates carry over to the next step. */
+__global__ void species_integrate_kernel(EngineView v, SpeciesView sp, const int *__restrict__ new_cell) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= v.nparts) return;
+    if (new_cell[s] != v.cell_of[s]) return;
+    const int t = __float_as_int(v.pos[s].w);
+    const int id = __float_as_int(v.vel[s].w);
+    const DevSpace &S = v.spaces[v.cell_rep[v.cell_of[s]]];
+    for (int k = 0; k < sp.nspec[t]; ++k) {
+        const float konst = (sp.flags[t * sp.smax + k] & 4u) ? 0.f : 1.f;
+        float &x = sp.value[(size_t)id * sp.smax + k];
+        x = (float)__dadd_rn((double)x, __dmul_rn(__dmul_rn(S.dt_d, (double)sp.rate[(size_t)id * sp.smax + k]),
+                                                  (double)konst));
+    }
+    for (int k = 0; k < sp.smax; ++k) sp.rate[(size_t)id * sp.smax + k] = 0.f;
+}
+
 /* Per type: the summed kinetic energy 0.5 m v^2 (each particle's term in FP32,
  * summed in FP64, engine_kinetic_energy, engine.cpp:1698-1719), the quantity
  * berendsen_force reads. One block per type, fixed summation order. */
@@ -1595,6 +1719,16 @@ void launch_singlebody_prep(const EngineView &v, int ntypes, double *type_ke, fl
 
 void launch_virial_reduce(const double *partials, int nwarps, double *out9, cudaStream_t st) {
     virial_reduce_kernel<<<1, 32, 0, st>>>(partials, nwarps, out9);
+}
+
+void launch_fluxes(const EngineView &v, const SpeciesView &sp, cudaStream_t st) {
+    const int tb = 128;
+    flux_kernel<<<(v.nparts + tb - 1) / tb, tb, 0, st>>>(v, sp);
+}
+
+void launch_species_integrate(const EngineView &v, const SpeciesView &sp, const int *new_cell, cudaStream_t st) {
+    const int tb = 256;
+    species_integrate_kernel<<<(v.nparts + tb - 1) / tb, tb, 0, st>>>(v, sp, new_cell);
 }
 
 void launch_bonded(const EngineView &v, const BondedView &bv, cudaStream_t st) {

@@ -15,6 +15,11 @@ void launch_singlebody_prep(const EngineView &v, int ntypes, double *type_ke, fl
 void launch_virial_reduce(const double *partials, int nwarps, double *out9, cudaStream_t st);
 /* combine: add the received planes here (no bond or integrator pass follows) */
 void launch_force(const EngineView &v, bool has_dpd, int grid, bool combine, cudaStream_t st);
+/* species flux rates of the current positions (full shell, by particle id), added to the carried rates */
+void launch_fluxes(const EngineView &v, const SpeciesView &sp, cudaStream_t st);
+/* species values += dt * rates after a forward-Euler step for particles that kept their cell (new_cell
+ * from the integrator); v is the state the rates belong to */
+void launch_species_integrate(const EngineView &v, const SpeciesView &sp, const int *new_cell, cudaStream_t st);
 /* bonds then angles; also adds the received planes (the force pass ran without combine) */
 void launch_bonded(const EngineView &v, const BondedView &bv, cudaStream_t st);
 void launch_integrate(const EngineView &v, float4 *pos, float4 *vel, int *new_cell, int *in_count, int *in_list,

@@ -178,6 +178,33 @@ def large(n=3000, L=10.0, nlarge=3, seed=7, dt=0.005, big=2.0, temperature=0.3):
                 forces=[], x=x, v=v, t=t)
 
 
+def species(n=2000, L=8.0, seed=8, dt=0.01, temperature=0.3):
+    """Two particle types carrying species (A: S1, S2, S3 with S3 constant; B:
+    S1, S2), with a Fick flux of S1 among A particles, secretion of S2 from B to
+    A and uptake of S1 by B from A, over a Morse fluid in a periodic box.
+    sp_* arrays describe the state vectors; fluxes lists (kind, type a, type b,
+    species index in a, species index in b, k, decay, target)."""
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0, L, size=(n, 3))
+    x = np.minimum(x, L * (1 - 1e-6)).astype(np.float32).astype(np.float64)
+    t = (rng.uniform(size=n) < 0.3).astype(np.int32)  # 0: A, 1: B
+    v = rng.normal(0, np.sqrt(temperature), size=(n, 3))
+    v = v.astype(np.float32).astype(np.float64)
+    cut = 1.0
+    morse = (0.2, 5.0, 0.6, 1e-4, 2.0, 1e-3)
+    smax = 3
+    values = rng.uniform(0, 1, size=(n, smax)).astype(np.float32)
+    values[t == 1, 2] = 0.0
+    return dict(dim=[L, L, L], cells=[int(L // cut)] * 3, cutoff=cut, dt=dt, bc=("periodic", "periodic", "periodic"),
+                types=[(1.0, 0.3, m.Newtonian), (1.0, 0.3, m.Newtonian)],
+                pots=[("morse", morse, 0, 0), ("morse", morse, 0, 1), ("morse", morse, 1, 1)],
+                forces=[], x=x, v=v, t=t,
+                sp_nspec=np.array([3, 2], dtype=np.int32), sp_names=[["S1", "S2", "$S3"], ["S1", "S2"]],
+                sp_flags=np.array([[0, 0, 4], [0, 0, 0]], dtype=np.uint32), sp_values=values,
+                fluxes=[(0, 0, 0, 0, 0, 2.0, 0.1, 0.0), (1, 1, 0, 1, 1, 1.0, 0.0, 0.5),
+                        (2, 0, 1, 0, 0, 0.5, 0.05, 1.0), (0, 0, 0, 2, 2, 1.0, 0.0, 0.0)])
+
+
 def chains(nchains=64, length=32, bond=0.5, L=8.0, seed=5, dt=0.002, k_bond=100.0, k_angle=5.0, theta0=2.0,
            pair=None, cut=1.0, temperature=0.1, dihedral=None):
     """Bead-spring chains in a periodic cube: harmonic bonds between consecutive
@@ -273,7 +300,10 @@ def build_gpu(scn, rng_mode="reference"):
            max_distance=scn.get("max_distance"), integrator=scn.get("integrator", m.FORWARD_EULER))
     types = []
     for k, (mass, radius, dyn) in enumerate(scn["types"]):
-        types.append(type(f"T{k}", (m.Particle,), {"mass": mass, "radius": radius, "dynamics": dyn}))
+        attrs = {"mass": mass, "radius": radius, "dynamics": dyn}
+        if "sp_names" in scn and scn["sp_nspec"][k] > 0:
+            attrs["species"] = list(scn["sp_names"][k])
+        types.append(type(f"T{k}", (m.Particle,), attrs))
     for (kind, params, ti, tj) in scn["pots"]:
         m.bind(make_potential(kind, params), types[ti], types[tj])
     for (ti, fx, fy, fz) in scn["forces"]:
@@ -291,6 +321,12 @@ def build_gpu(scn, rng_mode="reference"):
         u._add_bonds(make_potential(kind, params), scn["bi"], scn["bj"], scn["dissociation"])
     if "ai" in scn and len(scn["ai"]):
         u._add_angles(make_potential(*scn["angle_pot"]), scn["ai"], scn["aj"], scn["ak"])
+    for (kind, ta, tb, ia, ib, k, decay, target) in scn.get("fluxes", []):
+        name = scn["sp_names"][ta][ia].lstrip("$")
+        assert scn["sp_names"][tb][ib].lstrip("$") == name
+        u._add_flux(kind, types[ta], types[tb], name, k, decay, target)
+    if "sp_values" in scn:
+        u.set_species_values(np.asarray(scn["sp_values"], dtype=np.float32))
     if "di" in scn and len(scn["di"]):
         u._add_dihedrals(make_potential(*scn["dihedral_pot"]), scn["di"], scn["dj"], scn["dk"], scn["dl"])
     return u

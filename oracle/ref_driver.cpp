@@ -20,6 +20,8 @@
  *   mxref_add_bonds       _bond_init (src/mdcore/src/bond.cpp:497-529)
  *   mxref_add_angles      angle_init (src/mdcore/src/angle.cpp:659-707)
  *   mxref_pairwise        MxBond_PairwiseNew (src/mdcore/src/bond.cpp:944-989)
+ *   mxref_add_flux        MxFluxes_FluxEx (src/mdcore/src/Flux.cpp:161-211)
+ *   mxref_set_species     the particles' species state vectors (values and flags)
  *   mxref_bind_boundary_potential  MxBoundaryCondition(s)::set_potential
  *                         (src/mdcore/src/MxBoundaryConditions.cpp:771-836)
  *   mxref_add_dihedrals   engine_dihedral_addpot + engine_dihedral_add
@@ -38,6 +40,8 @@
 #include "bond.h"
 #include "angle.h"
 #include "MxParticleList.hpp"
+#include "Flux.hpp"
+#include "CStateVector.hpp"
 #include "task.h"
 #include "MxForce.h"
 #include "../../rendering/NOMStyle.hpp"
@@ -327,6 +331,55 @@ int mxref_bind_boundary_potential(int face, int type, void *pot) {
         faces[face]->set_potential(t, (MxPotential *)pot);
     else
         return -1;
+    return 0;
+}
+
+/* One flux between types ta and tb on their species ia and ib, as MxFluxes_FluxEx
+ * (src/mdcore/src/Flux.cpp:161-211) registers it without the species-name lookup:
+ * kind 0 Fick, 1 secrete, 2 uptake; one MxFluxes object shared by (ta, tb) and (tb, ta). */
+int mxref_add_flux(int kind, int ta, int tb, int ia, int ib, float k, float decay, float target) {
+    if (ta < 0 || tb < 0 || ta >= engine::nr_types || tb >= engine::nr_types) return -1;
+    const int i1 = _Engine.max_type * ta + tb, i2 = _Engine.max_type * tb + ta;
+    MxFluxes *f = _Engine.fluxes[i1];
+    if (!f) f = MxFluxes_New(8);
+    if (!f) return -2;
+    f = MxFluxes_AddFlux((FluxKind)kind, f, (int16_t)ta, (int16_t)tb, ia, ib, k, decay, target);
+    _Engine.fluxes[i1] = f;
+    _Engine.fluxes[i2] = f;
+    return 0;
+}
+
+/* Species state vectors (values, zero rates, the type's per-species flags) for particles
+ * 0..n-1: nspec[type] species each, values[id * smax + k], flags[type * smax + k]. */
+int mxref_set_species(int n, int smax, const int *nspec, const unsigned *flags, const float *values) {
+    space *s = &_Engine.s;
+    for (int id = 0; id < n; ++id) {
+        MxParticle *p = id < s->nr_parts ? s->partlist[id] : NULL;
+        if (!p) continue;
+        const int ns = nspec[p->typeId];
+        if (ns <= 0) continue;
+        CStateVector *sv = new CStateVector();
+        sv->size = ns;
+        sv->fvec = new float[ns];
+        sv->q = new float[ns]();
+        sv->species_flags = new uint32_t[ns];
+        for (int k = 0; k < ns; ++k) {
+            sv->fvec[k] = values[(size_t)id * smax + k];
+            sv->species_flags[k] = flags[(size_t)p->typeId * smax + k];
+        }
+        p->state_vector = sv;
+    }
+    return 0;
+}
+
+/* Species values by particle id (out[id * smax + k]); missing entries are left alone. */
+int mxref_get_species(int n, int smax, float *out) {
+    space *s = &_Engine.s;
+    for (int id = 0; id < n; ++id) {
+        MxParticle *p = id < s->nr_parts ? s->partlist[id] : NULL;
+        if (!p || !p->state_vector) continue;
+        for (int k = 0; k < p->state_vector->size && k < smax; ++k) out[(size_t)id * smax + k] = p->state_vector->fvec[k];
+    }
     return 0;
 }
 

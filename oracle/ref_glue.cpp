@@ -4,13 +4,13 @@
  * TEST INFRASTRUCTURE ONLY. Nothing in the product links or loads this.
  *
  * The reference's hot-path translation units (space, runners, pair loops,
- * integrator, bonds, angles, dihedrals, potentials) are compiled unmodified
+ * integrator, bonds, angles, dihedrals, fluxes, potentials) are compiled unmodified
  * from the reference checkout. They reference a handful of symbols that live
  * in subsystems that are outside the force-and-step path (rendering styles,
- * clusters, fluxes, events, timers, rigid constraints, exclusions, Verlet
+ * clusters, events, timers, rigid constraints, exclusions, Verlet
  * lists). This file defines those symbols as inert stand-ins so the engine
  * links; none of them is reached by the configurations the oracle runs (no
- * clusters, fluxes, exclusions, rigids or events).
+ * clusters, exclusions, rigids or events).
  */
 #include <random>
 
@@ -54,7 +54,6 @@ MxParticleType *MxParticleType_ForEngine(struct engine *, double, double, const 
 PyObject *MxParticleList_Pack(Py_ssize_t, ...) { return nullptr; }
 MxParticleList *MxParticleList_All() { return nullptr; }
 
-HRESULT MxFluxes_Integrate(int) { return S_OK; }
 void MxCuboid_UpdateAABB(MxCuboid *) {}
 MxCuboid::MxCuboid() {}
 int MxCluster_ComputeAggregateQuantities(struct MxCluster *) { return 0; }
@@ -67,6 +66,7 @@ CMulticastTimeEvent *CMulticastTimeEvent_New() { return nullptr; }
 HRESULT CMulticastTimeEvent_Invoke(CMulticastTimeEvent *, double) { return S_OK; }
 PyObject *MxPotential_Bind(MxPotential *, PyObject *, PyObject *) { Py_RETURN_NONE; }
 int MxParticle_Check(PyObject *) { return 0; }
+MxParticleType *MxParticleType_Get(PyObject *) { return nullptr; }
 /* MxRandomVector (src/mdcore/src/MxParticle.cpp:1782-1793, a file this build
  * does not compile): a normal magnitude N(mean, std) in a uniformly random
  * direction, restated with the same construction on a default-seeded mt19937

@@ -13,6 +13,9 @@
 #include <random>
 
 #define CAPI_FUNC(RTYPE) RTYPE
+/* carbon's spellings of the CPython type-object header initialisers */
+#define CObject_HEAD_INIT(type) PyVarObject_HEAD_INIT(type, 0)
+#define CVarObject_HEAD_INIT(type, size) PyVarObject_HEAD_INIT(type, size)
 #define CAPI_DATA(RTYPE) extern RTYPE
 #define CAPI_STRUCT(NAME) struct NAME
 
@@ -68,11 +71,12 @@ template <> inline std::string cast<std::string>(PyObject *o) { const char *s = 
 inline std::string str(PyObject *o) { PyObject *s = PyObject_Str(o); std::string r = s ? PyUnicode_AsUTF8(s) : "<object>"; Py_XDECREF(s); return r; }
 }
 
-/* Species state vector attached to particles (chemical cargo); the configs
- * here bind no species, so only the layout the engine touches is declared. */
+/* Species state vector attached to particles (chemical cargo): the layout the
+ * engine's flux code touches (values, rates, per-species flags). */
 struct CStateVector {
     float *fvec = nullptr;
     float *q = nullptr;
+    uint32_t *species_flags = nullptr;
     struct CSpeciesList *species = nullptr;
     int size = 0;
     void reset() {}

@@ -24,7 +24,9 @@ A scenario is a dict:
     arguments: berenderson_tstat(tau), random(std, mean, durration),
     friction(coef, std, mean, durration) (MxForce.cpp:213-259),
     target_temperature {type: T},
-    wall_pots [(face or -1, type, kind, params)] (bind(pot, boundary condition, type))
+    wall_pots [(face or -1, type, kind, params)] (bind(pot, boundary condition, type)),
+    species (optional): sp_nspec (per type), sp_flags (types x smax), sp_values (N x smax),
+    fluxes [(kind 0 fick | 1 secrete | 2 uptake, type a, type b, species a, species b, k, decay, target)]
 Results: xabs, xrel, v, f, cell (per id), tasks (rows type, sid, i, j),
     cdim, h, epot, epot_angle, epot_dihedral, ekin, bond_flags, seconds (wall time of the steps).
 """
@@ -49,7 +51,8 @@ def _pack(scn):
     flat = {}
     for k, v in scn.items():
         if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc", "sbforces",
-                 "target_temperature", "wall_pots"):
+                 "target_temperature", "wall_pots", "fluxes",
+                 "sp_names"):
             flat[k] = np.array(repr(v))
         else:
             flat[k] = np.asarray(v)
@@ -61,7 +64,8 @@ def _unpack(npz):
     for k in npz.files:
         v = npz[k]
         if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc", "sbforces",
-                 "target_temperature", "wall_pots"):
+                 "target_temperature", "wall_pots", "fluxes",
+                 "sp_names"):
             out[k] = eval(str(v))  # written by _pack from plain literals
         elif v.shape == ():
             out[k] = v.item()
@@ -221,6 +225,18 @@ def _execute(scn):
                            ctypes.byref(per))
         return {"pw_i": bi[nb0:tot].copy(), "pw_j": bj[nb0:tot].copy(), "seconds": np.float64(seconds),
                 "xrel": xr, "cell": cc, "cdim": cdim}
+    L.mxref_add_flux.argtypes = [ci] * 5 + [ctypes.c_float] * 3
+    for (kind, ta, tb, ia, ib, kk, dec, tgt) in scn.get("fluxes", []):
+        if L.mxref_add_flux(int(kind), int(ta), int(tb), int(ia), int(ib), float(kk), float(dec), float(tgt)) != 0:
+            raise RuntimeError("mxref_add_flux")
+    smax = 0
+    if "sp_values" in scn:
+        sv = np.ascontiguousarray(scn["sp_values"], dtype=np.float32)
+        smax = sv.shape[1]
+        L.mxref_set_species.argtypes = [ci, ci, P(ci), P(ctypes.c_uint), P(ctypes.c_float)]
+        L.mxref_set_species(n, smax, a(scn["sp_nspec"], ci),
+                            np.ascontiguousarray(scn["sp_flags"], dtype=np.uint32).ctypes.data_as(P(ctypes.c_uint)),
+                            sv.ctypes.data_as(P(ctypes.c_float)))
     L.mxref_start(int(scn.get("runners", 1)))
     t0 = time.perf_counter()
     if scn.get("action", "force") == "force":
@@ -268,6 +284,11 @@ def _execute(scn):
     out["epot_nonbond"] = np.float64(e[1].value)
     out["epot_bond"] = np.float64(e[2].value)
     out["ekin"] = np.float64(e[3].value)
+    if smax:
+        spo = np.zeros((n, smax), dtype=np.float32)
+        L.mxref_get_species.argtypes = [ci, ci, P(ctypes.c_float)]
+        L.mxref_get_species(n, smax, spo.ctypes.data_as(P(ctypes.c_float)))
+        out["species"] = spo
     L.mxref_epot_angle.restype = cd
     out["epot_angle"] = np.float64(L.mxref_epot_angle())
     L.mxref_epot_dihedral.restype = cd

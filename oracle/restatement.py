@@ -119,6 +119,50 @@ def pairlist(ids, xrel, cell, origins, types, cutoff, type_pairs=None):
     return np.array(fi, dtype=np.int32), np.array(fj, dtype=np.int32)
 
 
+def flux_step(x, t, L, cutoff, dt, values, fluxes, konst, moved):
+    """One forward-Euler species update under fluxes, in FP64 (flux_eval_ex,
+    src/mdcore/src/flux_eval.hpp:33-84; MxFluxes_Integrate, src/mdcore/src/
+    Flux.cpp:261-285): for every pair within the cutoff (minimum image in a
+    periodic box L) and every flux entry (kind, type a, type b, species a,
+    species b, k, decay, target) of its type pair, q = (1 - r/cutoff)^2 times
+    k (s_a - s_b) (Fick), max(k (s_a - target), 0) (secrete) or
+    max(k (target - s_b) s_a, 0) (uptake); rate_a -= q + decay/2 s_a,
+    rate_b += q - decay/2 s_b. values += dt * rate where konst is 0 and the
+    particle did not change cells (moved), else the values stay. Pairs of one
+    type take the lower id as a, which matters only for secretion and uptake
+    within one type."""
+    x = np.asarray(x, dtype=np.float64)
+    sv = np.asarray(values, dtype=np.float64)
+    rate = np.zeros_like(sv)
+    n = len(t)
+    for a in range(n - 1):
+        d = x[a] - x[a + 1:]
+        d -= L * np.round(d / L)
+        r2 = (d ** 2).sum(1)
+        for bb in np.flatnonzero(r2 <= cutoff * cutoff):
+            b = a + 1 + bb
+            w = (1 - np.sqrt(r2[bb]) / cutoff) ** 2
+            for (kind, ta, tb, ia, ib, k, dec, tgt) in fluxes:
+                if sorted((t[a], t[b])) != sorted((ta, tb)):
+                    continue
+                if ta == tb:
+                    pi, pj = a, b
+                else:
+                    pi, pj = (a, b) if t[a] == ta else (b, a)
+                si, sj = sv[pi, ia], sv[pj, ib]
+                if kind == 0:
+                    g = k * (si - sj)
+                elif kind == 1:
+                    g = max(k * (si - tgt), 0.0)
+                else:
+                    g = max(k * (tgt - sj) * si, 0.0)
+                rate[pi, ia] += -w * g - dec / 2 * si
+                rate[pj, ib] += w * g - dec / 2 * sj
+    out = sv + dt * rate * (1 - np.asarray(konst))
+    out[np.asarray(moved)] = sv[np.asarray(moved)]
+    return out
+
+
 def nonbond(scn, xrel, vel, cell, tasks, cdim, precision=64, tables=None, second=None, pruning=0, virial=False):
     """Forces (N,3) float64, energy, counts for a configuration.
 

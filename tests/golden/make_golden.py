@@ -49,6 +49,8 @@ CASES = [
     ("walls_dpd", lambda: S.walls(kind="dpd", bc_z="no_slip", seed=42), 10),
     # a fluid around three static large particles (radius > cutoff)
     ("large_fluid", lambda: S.large(seed=51), 10),
+    # species fluxes (Fick, secretion, uptake, a constant species) over a Morse fluid
+    ("species_fluxes", lambda: S.species(seed=61), 10),
 ]
 
 TABLES = [
@@ -150,7 +152,8 @@ def make_pairwise():
 def scenario_arrays(scn):
     d = {}
     for k, v in scn.items():
-        if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc", "wall_pots"):
+        if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc", "wall_pots", "fluxes",
+                 "sp_names"):
             d["scn_" + k] = np.array(repr(v))
         else:
             d["scn_" + k] = np.asarray(v)
@@ -165,13 +168,15 @@ def make_case(name, factory, nsteps):
     for k in ("f", "cell", "xrel", "epot", "ekin", "tasks", "cdim", "h", "bond_flags", "epot_angle",
               "epot_dihedral"):
         out["force_" + k] = f1[k]
-    for k in ("xrel", "xabs", "v", "cell", "epot", "ekin", "bond_flags"):
-        out["traj_" + k] = tr[k]
+    for k in ("xrel", "xabs", "v", "cell", "epot", "ekin", "bond_flags", "species"):
+        if k in tr:
+            out["traj_" + k] = tr[k]
     out["traj_nsteps"] = np.int64(nsteps)
     for ns in (1, 2):
         t = refengine.run(dict(scn, action="steps", nsteps=ns, runners=1))
-        for k in ("xrel", "xabs", "v", "cell", "epot", "ekin", "bond_flags"):
-            out[f"step{ns}_" + k] = t[k]
+        for k in ("xrel", "xabs", "v", "cell", "epot", "ekin", "bond_flags", "species"):
+            if k in t:
+                out[f"step{ns}_" + k] = t[k]
     np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **out)
 
 
@@ -182,7 +187,8 @@ def load_scenario(z):
             continue
         v = z[k]
         key = k[4:]
-        if key in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc", "wall_pots"):
+        if key in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc", "wall_pots", "fluxes",
+                   "sp_names"):
             scn[key] = eval(str(v))  # plain literals written by scenario_arrays
         elif v.shape == ():
             scn[key] = v.item()
