@@ -278,7 +278,7 @@ __device__ __noinline__ void large_forces(const EngineView &v, int s, const floa
 }
 
 constexpr int kOwn = 32;            // own particles staged at a time
-constexpr int kCap = 128;           // neighbour particles staged at a time
+constexpr int kCap = 96;            // neighbour particles staged at a time
 constexpr int kChunks = kCap / 32;  // candidate steps per own particle
 constexpr int kQueue = 256;         // ring buffer of queued pairs (holds kCap + 31)
 constexpr int kEnt = 32;            // neighbour entries cached at a time
@@ -448,7 +448,7 @@ constexpr size_t force_smem_bytes() {
 }
 
 template <bool kDPD, int kMode>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) force_kernel(EngineView v) {
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 5) force_kernel(EngineView v) {
     unsigned long long npair = 0;  // interacting pairs counted once (statistics launch only)
     double vir[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // pair virial (virial launch only)
     extern __shared__ float4 force_smem[];
