@@ -27,6 +27,8 @@
  *   mxg_engine_set_species / mxg_engine_get_species  the particles' species values
  *   mxg_engine_pairs_within        make_pairlist (the pair search of MxBond_PairwiseNew)
  *                                  src/mdcore/src/bond.cpp:892-942
+ *   mxg_engine_add_exclusions      engine_exclusion_add src/mdcore/src/engine_bonded.cpp:1277-1310
+ *   mxg_engine_exclusion_shrink    engine_exclusion_shrink src/mdcore/src/engine_bonded.cpp:1235-1262
  *   mxg_engine_adddihedrals        engine_dihedral_addpot + engine_dihedral_add
  *                                  src/mdcore/src/engine_bonded.cpp:1049-1080, 1967-1991
  *   mxg_engine_start               engine_start             src/mdcore/include/engine.h:640
@@ -224,6 +226,14 @@ int mxg_engine_addbonds(mxg_engine *e, int n, const int *i, const int *j, const 
  * the energy. ids_out receives consecutive angle indices (may be NULL). */
 int mxg_engine_addangles(mxg_engine *e, int n, const int *i, const int *j, const int *k, const mxg_potential *p,
                          int *ids_out);
+/* Adds n exclusions (i[q], j[q]): each force pass, before the bonds, the pair's table potential is
+ * taken back as exclusion_eval does (src/mdcore/src/exclusion.cpp:83-282): dx = (x_i - x_j) + h shift,
+ * kept within the cutoff, potential_eval without the radii shift, f_i += eff dx, f_j -= eff dx, its
+ * energy subtracted; pairs
+ * whose potential is DPD are skipped. Stored with i <= j (engine_exclusion_add). */
+int mxg_engine_add_exclusions(mxg_engine *e, int n, const int *i, const int *j);
+/* Sorts the exclusions and drops duplicates (engine_exclusion_shrink). */
+int mxg_engine_exclusion_shrink(mxg_engine *e);
 /* Adds n dihedrals i[q]-j[q]-k[q]-l[q], all with table potential p in cos(phi), evaluated each force pass
  * after the angles as dihedral_eval does (src/mdcore/src/dihedral.cpp:81-392): the forces on i, j and l
  * are balanced on k, which carries the energy. ids_out receives consecutive dihedral indices (may be NULL). */

@@ -504,6 +504,7 @@ class _Universe:
         self._bonds = []        # (potential, i[], j[], dissociation)
         self._angles = []       # (potential, i[], j[], k[])
         self._dihedrals = []    # (potential, i[], j[], k[], l[])
+        self._exclusions = []   # (i[], j[])
         self._bpots = []        # wall potentials: (potential, face or -1, type)
         self._species = {}      # type -> (species names, flags)
         self._spec_width = 0
@@ -573,6 +574,9 @@ class _Universe:
             check(lib().mxg_engine_add_flux(self._e, *f), "add_flux")
         for (p, face, t) in self._bpots:
             check(lib().mxg_engine_set_boundary_potential(self._e, face, t, p._h), "set_boundary_potential")
+        for (ii, jj) in self._exclusions:
+            check(lib().mxg_engine_add_exclusions(self._e, len(ii), ptr(ii, ctypes.c_int), ptr(jj, ctypes.c_int)),
+                  "add_exclusions")
         for (p, ii, jj, kk, ll) in self._dihedrals:
             check(lib().mxg_engine_adddihedrals(self._e, len(ii), ptr(ii, ctypes.c_int), ptr(jj, ctypes.c_int),
                                                 ptr(kk, ctypes.c_int), ptr(ll, ctypes.c_int), p._h, None),
@@ -683,6 +687,16 @@ class _Universe:
         self._sync_state()
         self._dirty = True
         return list(range(first, first + len(ii)))
+
+    def add_exclusions(self, i, j):
+        """Excludes the pairs (i[q], j[q]) from the pair potential: each force pass takes the
+        pair's table potential back (engine_exclusion_add and exclusion_eval; the reference
+        reaches them from C and its file readers only)."""
+        ii = i32([_pid(p) for p in np.atleast_1d(i)])
+        jj = i32([_pid(p) for p in np.atleast_1d(j)])
+        self._sync_state()
+        self._exclusions.append((ii, jj))
+        self._dirty = True
 
     def _add_dihedrals(self, pot, i, j, k, l):
         ii, jj, kk, ll = i32(i), i32(j), i32(k), i32(l)

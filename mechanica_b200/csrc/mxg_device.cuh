@@ -131,6 +131,9 @@ struct DevDihedral {
  * angle_list holds angle * 4 + role (0: i, 1: j, 2: k); dihedral_list holds
  * dihedral * 4 + role (0: i, 1: j, 2: k, 3: l). */
 struct BondedView {
+    const int2 *excl;        // exclusions (i <= j): the pair potential taken back
+    const int *excl_off;
+    const int *excl_list;    // exclusion * 2 + role (0: i, 1: j)
     const DevBond *bonds;
     unsigned *bond_flags;
     const int *bond_off;

@@ -95,6 +95,12 @@ struct AngleInfo {
     int i, j, k, pot;
 };
 
+struct ExclusionInfo {
+    int i, j;  // i <= j
+    bool operator<(const ExclusionInfo &o) const { return i < o.i || (i == o.i && j < o.j); }
+    bool operator==(const ExclusionInfo &o) const { return i == o.i && j == o.j; }
+};
+
 struct DihedralInfo {
     int i, j, k, l, pot;
 };
@@ -345,6 +351,7 @@ struct mxg_engine {
     std::vector<int> prep;                  // replica of each particle
     std::vector<BondInfo> bonds;
     std::vector<AngleInfo> angles;
+    std::vector<ExclusionInfo> exclusions;
     std::vector<DihedralInfo> dihedrals;
     // ---- species and fluxes ----
     std::vector<int> type_nspec;               // per type (0: no state vector)
@@ -409,6 +416,8 @@ struct mxg_engine {
     double *d_virial_partials = nullptr, *d_virial_out = nullptr;
     int virial_cap = 0;
     int *d_bond_off = nullptr, *d_bond_list = nullptr;
+    int2 *d_excl = nullptr;
+    int *d_excl_off = nullptr, *d_excl_list = nullptr;
     DevAngle *d_angles = nullptr;
     int *d_angle_off = nullptr, *d_angle_list = nullptr;
     DevDihedral *d_dihedrals = nullptr;
@@ -604,10 +613,15 @@ struct mxg_engine {
         return v;
     }
 
-    bool has_bonded() const { return !bonds.empty() || !angles.empty() || !dihedrals.empty(); }
+    bool has_bonded() const {
+        return !bonds.empty() || !angles.empty() || !dihedrals.empty() || !exclusions.empty();
+    }
 
     BondedView bonded_view() const {
         BondedView bv;
+        bv.excl = d_excl;
+        bv.excl_off = d_excl_off;
+        bv.excl_list = d_excl_list;
         bv.bonds = d_bonds;
         bv.bond_flags = d_bond_flags;
         bv.bond_off = d_bond_off;
@@ -1034,6 +1048,25 @@ int mxg_engine::start(cudaStream_t st) {
         }
     }
 
+    // ---- exclusions: CSR by particle id, entries exclusion * 2 + role ----
+    std::vector<int2> hx;
+    std::vector<int> xoff(nparts + 1, 0), xlist;
+    for (const ExclusionInfo &x : exclusions) {
+        if (x.i < 0 || x.j >= nparts || prep[x.i] != prep[x.j]) return MXG_ERR_BOND;
+        xoff[x.i + 1]++;
+        if (x.j != x.i) xoff[x.j + 1]++;
+    }
+    for (int p = 0; p < nparts; ++p) xoff[p + 1] += xoff[p];
+    xlist.assign(xoff[nparts], 0);
+    {
+        std::vector<int> fill(xoff.begin(), xoff.end() - 1);
+        for (int k = 0; k < (int)exclusions.size(); ++k) {
+            xlist[fill[exclusions[k].i]++] = 2 * k;
+            if (exclusions[k].j != exclusions[k].i) xlist[fill[exclusions[k].j]++] = 2 * k + 1;
+            hx.push_back(make_int2(exclusions[k].i, exclusions[k].j));
+        }
+    }
+
     // ---- angles: CSR by particle id, entries angle * 4 + role ----
     std::vector<DevAngle> ha;
     std::vector<int> aoff(nparts + 1, 0), alist;
@@ -1142,6 +1175,9 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_bond_flags, hbf.size());
     rc |= alloc(&d_bond_off, boff.size());
     rc |= alloc(&d_bond_list, blist.size());
+    rc |= alloc(&d_excl, hx.size());
+    rc |= alloc(&d_excl_off, xoff.size());
+    rc |= alloc(&d_excl_list, xlist.size());
     rc |= alloc(&d_angles, ha.size());
     rc |= alloc(&d_angle_off, aoff.size());
     rc |= alloc(&d_angle_list, alist.size());
@@ -1178,7 +1214,8 @@ int mxg_engine::start(cudaStream_t st) {
         (rc = upload(d_types, ht, stream)) || (rc = upload(d_spaces, hs, stream)) || (rc = upload(d_axes, haxes, stream)) ||
         (rc = upload(d_bonds, hb, stream)) || (rc = upload(d_bond_flags, hbf, stream)) ||
         (rc = upload(d_bond_off, boff, stream)) || (rc = upload(d_bond_list, blist, stream)) ||
-        (rc = upload(d_angles, ha, stream)) || (rc = upload(d_angle_off, aoff, stream)) ||
+        (rc = upload(d_excl, hx, stream)) || (rc = upload(d_excl_off, xoff, stream)) ||
+        (rc = upload(d_excl_list, xlist, stream)) || (rc = upload(d_angles, ha, stream)) || (rc = upload(d_angle_off, aoff, stream)) ||
         (rc = upload(d_angle_list, alist, stream)) || (rc = upload(d_dihedrals, hd, stream)) ||
         (rc = upload(d_large_x, hlx, stream)) || (rc = upload(d_large_v, hlv, stream)) ||
         (rc = upload(d_spec, spec_host, stream)) || (rc = upload(d_nspec, hnspec, stream)) ||
@@ -1743,6 +1780,21 @@ int mxg_engine_get_species(mxg_engine *e, int n, int smax, float *out) {
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     for (int id = 0; id < n && id < e->nparts; ++id)
         for (int k = 0; k < std::min(smax, e->smax); ++k) out[(size_t)id * smax + k] = buf[(size_t)id * e->smax + k];
+    return MXG_OK;
+}
+
+int mxg_engine_add_exclusions(mxg_engine *e, int n, const int *i, const int *j) {
+    if (!e || (n > 0 && (!i || !j))) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    for (int q = 0; q < n; ++q) e->exclusions.push_back({std::min(i[q], j[q]), std::max(i[q], j[q])});
+    return MXG_OK;
+}
+
+int mxg_engine_exclusion_shrink(mxg_engine *e) {
+    if (!e) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    std::sort(e->exclusions.begin(), e->exclusions.end());
+    e->exclusions.erase(std::unique(e->exclusions.begin(), e->exclusions.end()), e->exclusions.end());
     return MXG_OK;
 }
 

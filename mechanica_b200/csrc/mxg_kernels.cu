@@ -1140,8 +1140,8 @@ __device__ bool dihedral_terms(const EngineView &v, const BondedView &bv, int di
 }
 
 /*
- * The bonded pass (engine_bonded_eval, engine_bonded.cpp:1373-1543: bonds,
- * then angles, then dihedrals). One thread per particle slot; each thread evaluates every
+ * The bonded pass (engine_bonded_eval, engine_bonded.cpp:1373-1543:
+ * exclusions, bonds, angles, dihedrals). One thread per particle slot; each thread evaluates every
  * bond and angle its particle takes part in and applies its own share, in the
  * bonded lists' index order, so its force receives the same sequence of
  * updates as in the reference's serial loops.
@@ -1159,6 +1159,45 @@ __global__ void bonded_kernel(EngineView v, BondedView bv) {
     const int id = __float_as_int(v.vel[s].w);
     double eb = 0.0;
     float4 f = total_force(v, s);  // the bonded pass completes the nonbonded force
+    // exclusions (exclusion_eval, exclusion.cpp:83-282): the pair's table potential evaluated
+    // with potential_eval (no radii shift) on dx = (x_i - x_j) + h shift and taken back,
+    // f_i += eff dx, f_j -= eff dx and its energy subtracted, for pairs within the cutoff
+    const int x0 = bv.excl_off[id], x1 = bv.excl_off[id + 1];
+    for (int k = x0; k < x1; ++k) {
+        const int code = bv.excl_list[k];
+        const int2 X = bv.excl[code >> 1];
+        const int si = bv.slot_of_id[X.x], sj = bv.slot_of_id[X.y];
+        if (si < 0 || sj < 0) continue;
+        const float4 xi = v.pos[si], xj = v.pos[sj];
+        const int ti = __float_as_int(xi.w), tj = __float_as_int(xj.w);
+        const int ci = v.cell_of[si], cj = v.cell_of[sj];
+        const DevSpace &S = v.spaces[v.cell_rep[ci]];
+        const int q = v.pot_idx[S.pot_offset + tj * v.ntypes + ti];
+        if (q < 0 || v.pots[q].kind != 0) continue;
+        int loci[3], locj[3];
+        cell_loc(S, ci, loci);
+        cell_loc(S, cj, locj);
+        const float xiv[3] = {xi.x, xi.y, xi.z}, xjv[3] = {xj.x, xj.y, xj.z};
+        float d[3];
+        for (int c3 = 0; c3 < 3; ++c3)
+            d[c3] = (float)__dadd_rn((double)__fsub_rn(xiv[c3], xjv[c3]),
+                                     __dmul_rn(S.hd[c3], (double)wrap_shift(loci[c3] - locj[c3])));
+        const float r2 = dot3_rn(d[0], d[1], d[2]);
+        if (r2 > S.cut2_self) continue;
+        float ee, eff;
+        table_eval(v.pots[q], v.coef, r2, ee, eff);
+        const float wx = __fmul_rn(eff, d[0]), wy = __fmul_rn(eff, d[1]), wz = __fmul_rn(eff, d[2]);
+        if ((code & 1) == 0) {
+            f.x = __fadd_rn(f.x, wx);
+            f.y = __fadd_rn(f.y, wy);
+            f.z = __fadd_rn(f.z, wz);
+            eb -= (double)ee;  // the pair's energy is taken back (exclusion.cpp:279-280)
+        } else {
+            f.x = __fsub_rn(f.x, wx);
+            f.y = __fsub_rn(f.y, wy);
+            f.z = __fsub_rn(f.z, wz);
+        }
+    }
     const int k0 = bv.bond_off[id], k1 = bv.bond_off[id + 1];
     for (int k = k0; k < k1; ++k) {
         const int b = bv.bond_list[k];

@@ -206,15 +206,16 @@ def species(n=2000, L=8.0, seed=8, dt=0.01, temperature=0.3):
 
 
 def chains(nchains=64, length=32, bond=0.5, L=8.0, seed=5, dt=0.002, k_bond=100.0, k_angle=5.0, theta0=2.0,
-           pair=None, cut=1.0, temperature=0.1, dihedral=None):
+           pair=None, cut=1.0, temperature=0.1, dihedral=None, exclude_bonded=False):
     """Bead-spring chains in a periodic cube: harmonic bonds between consecutive
     beads (k_bond (r - bond)^2, never breaking) and harmonic angles on
     consecutive triples (k_angle (theta - theta0)^2, vertex at the middle bead).
     Chains are random walks with bond-length steps whose turning angle stays
     near pi - theta0, wrapped into the box, so bonds and angles cross the
-    periodic faces. pair: None (bonded forces only) or the parameters of a Morse
-    potential bound on the bead type. dihedral: None or (k, n, delta, tol) of a
-    harmonic dihedral on consecutive quadruples. Newtonian, mass 1."""
+    periodic faces. pair: None (bonded forces only), the parameters of a Morse
+    potential bound on the bead type, or (kind, parameters). dihedral: None or (k, n, delta, tol) of a
+    harmonic dihedral on consecutive quadruples. exclude_bonded: exclusions
+    between bonded neighbours (the pair potential taken back). Newtonian, mass 1."""
     rng = np.random.default_rng(seed)
     xs = []
     for _ in range(nchains):
@@ -244,8 +245,15 @@ def chains(nchains=64, length=32, bond=0.5, L=8.0, seed=5, dt=0.002, k_bond=100.
     v = rng.normal(0, np.sqrt(temperature), size=(n, 3))
     v -= v.mean(axis=0)
     cells = int(L // cut)
-    pots = [] if pair is None else [("morse", tuple(pair), 0, 0)]
+    if pair is None:
+        pots = []
+    elif isinstance(pair[0], str):  # (kind, params)
+        pots = [(pair[0], tuple(pair[1]), 0, 0)]
+    else:
+        pots = [("morse", tuple(pair), 0, 0)]
     extra = {}
+    if exclude_bonded:
+        extra.update(ex_i=bi.copy(), ex_j=bj.copy())
     if dihedral is not None:
         kd, nd, dd, tol = dihedral
         extra = dict(di=idx[:, :-3].ravel().astype(np.int32), dj=idx[:, 1:-2].ravel().astype(np.int32),
@@ -327,6 +335,8 @@ def build_gpu(scn, rng_mode="reference"):
         u._add_flux(kind, types[ta], types[tb], name, k, decay, target)
     if "sp_values" in scn:
         u.set_species_values(np.asarray(scn["sp_values"], dtype=np.float32))
+    if "ex_i" in scn and len(scn["ex_i"]):
+        u.add_exclusions(scn["ex_i"], scn["ex_j"])
     if "di" in scn and len(scn["di"]):
         u._add_dihedrals(make_potential(*scn["dihedral_pot"]), scn["di"], scn["dj"], scn["dk"], scn["dl"])
     return u

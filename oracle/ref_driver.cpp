@@ -21,6 +21,7 @@
  *   mxref_add_angles      angle_init (src/mdcore/src/angle.cpp:659-707)
  *   mxref_pairwise        MxBond_PairwiseNew (src/mdcore/src/bond.cpp:944-989)
  *   mxref_add_flux        MxFluxes_FluxEx (src/mdcore/src/Flux.cpp:161-211)
+ *   mxref_add_exclusions  engine_exclusion_add (src/mdcore/src/engine_bonded.cpp:1277-1310)
  *   mxref_set_species     the particles' species state vectors (values and flags)
  *   mxref_bind_boundary_potential  MxBoundaryCondition(s)::set_potential
  *                         (src/mdcore/src/MxBoundaryConditions.cpp:771-836)
@@ -379,6 +380,15 @@ int mxref_get_species(int n, int smax, float *out) {
         MxParticle *p = id < s->nr_parts ? s->partlist[id] : NULL;
         if (!p || !p->state_vector) continue;
         for (int k = 0; k < p->state_vector->size && k < smax; ++k) out[(size_t)id * smax + k] = p->state_vector->fvec[k];
+    }
+    return 0;
+}
+
+/* engine_exclusion_add (src/mdcore/src/engine_bonded.cpp:1277-1310) for n pairs. */
+int mxref_add_exclusions(int n, const int *pi, const int *pj) {
+    for (int q = 0; q < n; ++q) {
+        int rc = engine_exclusion_add(&_Engine, pi[q], pj[q]);
+        if (rc < 0) return rc;
     }
     return 0;
 }

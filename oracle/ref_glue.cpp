@@ -4,13 +4,13 @@
  * TEST INFRASTRUCTURE ONLY. Nothing in the product links or loads this.
  *
  * The reference's hot-path translation units (space, runners, pair loops,
- * integrator, bonds, angles, dihedrals, fluxes, potentials) are compiled unmodified
+ * integrator, exclusions, bonds, angles, dihedrals, fluxes, potentials) are compiled unmodified
  * from the reference checkout. They reference a handful of symbols that live
  * in subsystems that are outside the force-and-step path (rendering styles,
- * clusters, events, timers, rigid constraints, exclusions, Verlet
+ * clusters, events, timers, rigid constraints, Verlet
  * lists). This file defines those symbols as inert stand-ins so the engine
  * links; none of them is reached by the configurations the oracle runs (no
- * clusters, exclusions, rigids or events).
+ * clusters, rigids or events).
  */
 #include <random>
 
@@ -38,7 +38,6 @@ WallTime::WallTime() : start(0) {}
 WallTime::~WallTime() {}
 double MxWallTime() { return 0.0; }
 
-extern "C" int exclusion_eval(struct exclusion *, int, struct engine *, double *) { return 0; }
 int engine_rigid_eval(struct engine *) { return 0; }
 extern "C" int runner_verlet_fill(struct runner *, struct space_cell *, struct space_cell *, FPTYPE *) { return 0; }
 extern "C" int runner_verlet_eval(struct runner *, struct space_cell *, FPTYPE *) { return 0; }

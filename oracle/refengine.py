@@ -16,6 +16,7 @@ A scenario is a dict:
     bonds (optional): bi, bj, bond_pot (kind, params), dissociation,
     angles (optional): ai, aj, ak (vertex aj), angle_pot ("harmonic_angle", (k, theta0, min, max, tol)),
     dihedrals (optional): di, dj, dk, dl, dihedral_pot ("harmonic_dihedral", (k, n, delta, tol)),
+    exclusions (optional): ex_i, ex_j (engine_exclusion_add pairs),
     action: "force" | "steps" | "pairwise", nsteps, runners (threads), time_it (bool),
     pairwise (action "pairwise"): pw_ids (list order), pw_cutoff, pw_ta/pw_tb (type pairs, optional)
         -> pw_i, pw_j: the bonds MxBond_PairwiseNew creates, in order,
@@ -183,6 +184,10 @@ def _execute(scn):
         L.mxref_add_angles.argtypes = [ci, P(ci), P(ci), P(ci), vp]
         if L.mxref_add_angles(len(scn["ai"]), a(scn["ai"], ci), a(scn["aj"], ci), a(scn["ak"], ci), ap) != 0:
             raise RuntimeError("mxref_add_angles")
+    if "ex_i" in scn and len(scn["ex_i"]):
+        L.mxref_add_exclusions.argtypes = [ci, P(ci), P(ci)]
+        if L.mxref_add_exclusions(len(scn["ex_i"]), a(scn["ex_i"], ci), a(scn["ex_j"], ci)) != 0:
+            raise RuntimeError("mxref_add_exclusions")
     if "di" in scn and len(scn["di"]):
         dp = make_pot(*scn["dihedral_pot"])
         keep.append(dp)

@@ -44,6 +44,9 @@ CASES = [
     ("chains_dihedral", lambda: S.chains(nchains=16, length=24, seed=23, dihedral=(1.5, 3, 0.0, 0.001)), 10),
     ("chains_dihedral_shift", lambda: S.chains(nchains=16, length=24, seed=24, dihedral=(0.8, 2, 1.0, 0.01),
                                                pair=(0.2, 6.0, 0.5, 1e-4, 1.0, 1e-3)), 10),
+    # exclusions between bonded neighbours of the Morse chains
+    ("chains_excl", lambda: S.chains(nchains=16, length=24, seed=25,
+                                     pair=("lj126", (0.2, 1.0, 1e-8, 1e-4, 1e-3)), exclude_bonded=True), 10),
     # wall potentials: LJ and Morse walls on "potential" z faces; DPD walls on no-slip z faces
     ("walls_lj", lambda: S.walls(kind="lj", bc_z="potential", seed=41), 10),
     ("walls_dpd", lambda: S.walls(kind="dpd", bc_z="no_slip", seed=42), 10),

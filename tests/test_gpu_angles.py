@@ -225,3 +225,40 @@ def test_single_dihedral_against_central_differences():
             g[p, q] = (_dihedral_energy(xp, K, n, delta)[0] - _dihedral_energy(xm, K, n, delta)[0]) / (2 * h)
     assert np.abs(f + g).max() <= 2e-3 * np.abs(g).max(), (f, -g)
     assert np.abs(f.sum(axis=0)).max() <= 1e-5 * np.abs(f).max()
+
+
+# ---- exclusions (exclusion_eval, src/mdcore/src/exclusion.cpp:83-282) ----
+
+def test_exclusions_match_reference():
+    """LJ chains with the bonded neighbours excluded from the pair potential:
+    the force pass and one step against the reference engine. Beads
+    of different chains that start closer than the table minimum get a random
+    pair direction (a Philox draw here, an mt19937 draw there) and are left
+    out, as in the other parity tests."""
+    from test_gpu_parity import _close_pairs
+    z, scn = load("chains_excl")
+    keep = ~_close_pairs(scn, scn["x"])
+    assert keep.mean() > 0.9
+    u = S.build_gpu(scn)
+    u.force()
+    x, v, f, c, xr = u.state()
+    assert rel_rms(f[keep], z["force_f"][keep]) <= 1e-5
+    ep, _ = u.energies()  # a random direction keeps the pair at distance a: same energy
+    ref = float(z["force_epot"])
+    assert abs(ep - ref) <= 1e-6 * abs(ref)
+    scn_no = dict(scn)
+    scn_no.pop("ex_i")
+    scn_no.pop("ex_j")
+    u2 = S.build_gpu(scn_no)
+    u2.force()
+    # the exclusions change the forces
+    assert rel_rms(u2.state()[2][keep], z["force_f"][keep]) > 1e-3
+    L = np.asarray(scn["dim"])
+    for nsteps in (1,):
+        u = S.build_gpu(scn)
+        u.steps(nsteps)
+        x, v, f, c, xr = u.state()
+        k = f"step{nsteps}_"
+        d = x - z[k + "xabs"]
+        d -= L * np.round(d / L)
+        assert np.abs(d[keep]).max() < 1e-5
