@@ -206,6 +206,7 @@ struct EngineView {      // everything a kernel needs, passed by value
     const int *cell_planes;  // per cell: received planes plus own-side planes of its later work items
     float4 *planes;          // [plane][slot] neighbour-side force sums of once-evaluated pairs
     double *body_e;          // per slot: wall and large-particle energy of the last pass; null when neither exists
+    const float4 *body_f;    // per slot: wall and large-particle force of the pass; null when neither exists
     const float4 *large_x;   // large particles: position relative to the replica origin, w = type
     const float4 *large_v;   // large particles: velocity, w = id
     const int *large_rep;    // large particles: replica

@@ -432,7 +432,9 @@ struct mxg_engine {
     int nlarge = 0;                     // large particles (radius > cutoff)
     float4 *d_large_x = nullptr, *d_large_v = nullptr;
     int *d_large_rep = nullptr, *d_large_pot = nullptr;
-    double *d_body_e = nullptr;         // per slot: wall energy of the last pass
+    double *d_body_e = nullptr;         // per slot: wall and large-particle energy of the last pass
+    float4 *d_body_f = nullptr;         // per slot: wall and large-particle force of the pass
+    bool has_body() const { return has_walls || nlarge > 0; }
     double *d_type_ke = nullptr;
     float4 *d_persist = nullptr;
     int integrator = 0;                 // 0 forward Euler, 1 Runge-Kutta 4 (engine.h EngineIntegrator)
@@ -605,6 +607,7 @@ struct mxg_engine {
         v.nitems = nitems;
         v.planes = d_planes;
         v.body_e = (has_walls || nlarge) ? d_body_e : nullptr;
+        v.body_f = (has_walls || nlarge) ? d_body_f : nullptr;
         v.large_x = d_large_x;
         v.large_v = d_large_v;
         v.large_rep = d_large_rep;
@@ -643,6 +646,7 @@ struct mxg_engine {
         force_layout = b;
         const EngineView v = view(b);
         if (has_sb) launch_singlebody_prep(v, ntypes, d_type_ke, d_persist, false, stream);
+        if (has_body()) launch_body(v, d_body_f, stream);
         launch_force(v, has_dpd, force_grid, !has_bonded(), stream);
         if (has_bonded()) launch_bonded(v, bonded_view(), stream);
         if (has_fluxes) launch_fluxes(v, species_view(), stream);
@@ -675,6 +679,7 @@ struct mxg_engine {
         const int nb = 1 - b;
         const EngineView v = view(b);
         if (has_sb) launch_singlebody_prep(v, ntypes, d_type_ke, d_persist, true, stream);
+        if (has_body()) launch_body(v, d_body_f, stream);
         launch_force(v, has_dpd, force_grid, false, stream);
         if (has_bonded()) launch_bonded(v, bonded_view(), stream);
         if (has_fluxes) launch_fluxes(v, species_view(), stream);
@@ -697,6 +702,7 @@ struct mxg_engine {
         for (int stage = 0; stage < 4; ++stage) {
             // persistent random forces are redrawn in the first stage only (INTEGRATOR_UPDATE_PERSISTENTFORCE)
             if (has_sb) launch_singlebody_prep(v, ntypes, d_type_ke, d_persist, stage == 0, stream);
+            if (has_body()) launch_body(v, d_body_f, stream);
             launch_force(v, has_dpd, force_grid, false, stream);
             if (has_bonded()) launch_bonded(v, bonded_view(), stream);
             if (stage < 3) {
@@ -1158,6 +1164,7 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_epot_cell, nitems);
     rc |= alloc(&d_ebond_slot, nparts);
     rc |= alloc(&d_body_e, nparts);
+    rc |= alloc(&d_body_f, nparts);
     rc |= alloc(&d_spec, (size_t)nparts * smax);
     rc |= alloc(&d_rate, (size_t)nparts * smax);
     rc |= alloc(&d_nspec, hnspec.size());
@@ -2238,6 +2245,7 @@ int mxg_engine_pair_counts(mxg_engine *e, long long *candidates, long long *inte
         CUDA_TRY(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), e->stream));
         EngineView v = e->view(e->cur);
         v.pair_stats = d_cnt;
+        if (e->has_body()) launch_body(v, e->d_body_f, e->stream);
         launch_force(v, e->has_dpd, e->force_grid, true, e->stream);
         e->force_layout = e->cur;
         unsigned long long n = 0;

@@ -742,19 +742,11 @@ __device__ __forceinline__ float4 total_force(const EngineView &v, int s) {
         f.y += g.y;
         f.z += g.z;
     }
-    if (v.body_e) {
-        // wall potentials of particles in cells next to a bound face and the large
-        // particles' interactions (runner_doself's boundary_eval and
-        // particle_largecell_force, runner_dopair.cpp:526-535); the energy goes to the
-        // slot's entry
-        const float4 x = v.pos[s];
-        const DevType &T = v.types[__float_as_int(x.w)];
-        const int c = v.cell_of[s];
-        const unsigned cflags = v.cell_flags[c];
-        double ew = 0.0;
-        if (cflags & T.wall_mask) boundary_forces(v, v.spaces[v.cell_rep[c]], cflags, T, T.radius, x, v.vel[s], f, ew);
-        if (v.nlarge && !T.large) large_forces(v, s, x, v.vel[s], T.radius, f, ew);
-        v.body_e[s] = ew;
+    if (v.body_f) {  // walls and large particles of this pass (body_kernel)
+        const float4 b = v.body_f[s];
+        f.x += b.x;
+        f.y += b.y;
+        f.z += b.z;
     }
     if (v.has_sb) {
         // the velocity-dependent and random single-body forces (MxForce.cpp:330-386)
@@ -912,6 +904,26 @@ __global__ void species_integrate_kernel(EngineView v, SpeciesView sp, const int
                                                   (double)konst));
     }
     for (int k = 0; k < sp.smax; ++k) sp.rate[(size_t)id * sp.smax + k] = 0.f;
+}
+
+/* Wall potentials of particles in cells next to a bound face and the large
+ * particles' interactions (runner_doself's boundary_eval and
+ * particle_largecell_force, runner_dopair.cpp:526-535), one thread per slot,
+ * before the pass's force kernel; total_force adds the force, the energy goes
+ * to the slot's entry. */
+__global__ void body_kernel(EngineView v, float4 *body_f) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= v.nparts) return;
+    const float4 x = v.pos[s];
+    const DevType &T = v.types[__float_as_int(x.w)];
+    const int c = v.cell_of[s];
+    const unsigned cflags = v.cell_flags[c];
+    float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+    double ew = 0.0;
+    if (cflags & T.wall_mask) boundary_forces(v, v.spaces[v.cell_rep[c]], cflags, T, T.radius, x, v.vel[s], f, ew);
+    if (v.nlarge && !T.large) large_forces(v, s, x, v.vel[s], T.radius, f, ew);
+    body_f[s] = f;
+    v.body_e[s] = ew;
 }
 
 /* Per type: the summed kinetic energy 0.5 m v^2 (each particle's term in FP32,
@@ -1758,6 +1770,11 @@ void launch_singlebody_prep(const EngineView &v, int ntypes, double *type_ke, fl
 
 void launch_virial_reduce(const double *partials, int nwarps, double *out9, cudaStream_t st) {
     virial_reduce_kernel<<<1, 32, 0, st>>>(partials, nwarps, out9);
+}
+
+void launch_body(const EngineView &v, float4 *body_f, cudaStream_t st) {
+    const int tb = 128;
+    body_kernel<<<(v.nparts + tb - 1) / tb, tb, 0, st>>>(v, body_f);
 }
 
 void launch_fluxes(const EngineView &v, const SpeciesView &sp, cudaStream_t st) {

@@ -15,6 +15,9 @@ void launch_singlebody_prep(const EngineView &v, int ntypes, double *type_ke, fl
 void launch_virial_reduce(const double *partials, int nwarps, double *out9, cudaStream_t st);
 /* combine: add the received planes here (no bond or integrator pass follows) */
 void launch_force(const EngineView &v, bool has_dpd, int grid, bool combine, cudaStream_t st);
+/* wall and large-particle forces (into body_f) and energies (v.body_e) of the current positions; before
+ * the pass's force kernel */
+void launch_body(const EngineView &v, float4 *body_f, cudaStream_t st);
 /* species flux rates of the current positions (full shell, by particle id), added to the carried rates */
 void launch_fluxes(const EngineView &v, const SpeciesView &sp, cudaStream_t st);
 /* species values += dt * rates after a forward-Euler step for particles that kept their cell (new_cell
