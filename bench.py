@@ -447,6 +447,18 @@ def main():
                 # dram__bytes_read.sum + dram__bytes_write.sum of one force launch of this workload
                 # (ncu capture summarised in profiles/force_kernel_dpd200k.md)
                 "traffic": FORCE_TRAFFIC_BYTES if n == 200000 else None, "traffic_unit": "bytes per launch"}
+    # the same launch against the measured HBM copy bandwidth: compulsory state bytes (position and
+    # velocity read, force written, 16 B each per particle) over the launch time, and the captured
+    # DRAM traffic over the same time; both far below the bound, so HBM does not limit this kernel
+    hbm_peak = (peaks or {}).get("hbm_gbs")
+    if hbm_peak:
+        state_bytes = 48 * n
+        roofline["hbm_view"] = {
+            "peak": hbm_peak, "unit": "GB/s", "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
+            "algorithmic_bytes_per_launch": state_bytes,
+            "achieved": state_bytes / (force_ms / 1e3) / 1e9,
+            "frac": state_bytes / (force_ms / 1e3) / 1e9 / hbm_peak,
+            "traffic_rate": (FORCE_TRAFFIC_BYTES / (force_ms / 1e3) / 1e9) if n == 200000 else None}
 
     # ---- CPU baseline and accuracy (reference engine, rank 0, N=1 only) ----
     cpu = None
