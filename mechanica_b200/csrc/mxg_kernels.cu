@@ -1529,37 +1529,46 @@ __global__ void rk_final_kernel(EngineView v, float4 *pos, float4 *vel, RkState 
 /* re-binning                                                                */
 /* ------------------------------------------------------------------------ */
 
-/* New occupancy count_old - out + in, exclusive scan into new_start. One block
- * of 1024 threads walks the cells in chunks of kScanChunk: the counts go
- * through shared memory so that every global load and store is coalesced; each
- * thread scans eight consecutive cells of the chunk, warp-shuffle scans join
- * the threads, and a carry joins the chunks. */
-constexpr int kScanChunk = 8192;
-__device__ __forceinline__ int scan_pad(int i) { return i + (i >> 5); }  // conflict-free 8-cell runs
+constexpr int kScanPer = 16;                  // cells per thread
+constexpr int kScanChunk = 1024 * kScanPer;   // cells per pass of the block
 
+/* New occupancy (old - movers out + movers in) and its exclusive scan, one
+ * block: each thread owns 16 consecutive cells of a chunk, read and written
+ * as int4 vectors where the chunk is full, so the chunk's loads are all in
+ * flight at once; warp and block scans of the per-thread sums; the step
+ * counter that keys the Philox streams advances here. */
 __global__ void __launch_bounds__(1024) scan_kernel(int ncells, const int *__restrict__ old_count,
                                                    const int *__restrict__ out_count, const int *__restrict__ in_count,
                                                    int *new_start, int *new_count, unsigned long long *step) {
-    __shared__ int cnt[kScanChunk + kScanChunk / 32];
     __shared__ int warp_total[32];
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
     int carry = 0;
     for (int c0 = 0; c0 < ncells; c0 += kScanChunk) {
-        const int m = min(kScanChunk, ncells - c0);
-        for (int k = t; k < m; k += blockDim.x) {
-            const int c = c0 + k;
-            const int n = old_count[c] - out_count[c] + min(in_count[c], kBucket);
-            new_count[c] = n;
-            cnt[scan_pad(k)] = n;
-        }
-        __syncthreads();
-        int v[8], sum = 0;
+        const int base = c0 + kScanPer * t;
+        int v[kScanPer];
+        if (base + kScanPer <= ncells) {
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int idx = 8 * t + q;
-            v[q] = idx < m ? cnt[scan_pad(idx)] : 0;
-            sum += v[q];
+            for (int q = 0; q < kScanPer; q += 4) {
+                const int4 o = *reinterpret_cast<const int4 *>(old_count + base + q);
+                const int4 u = *reinterpret_cast<const int4 *>(out_count + base + q);
+                const int4 w = *reinterpret_cast<const int4 *>(in_count + base + q);
+                v[q] = o.x - u.x + min(w.x, kBucket);
+                v[q + 1] = o.y - u.y + min(w.y, kBucket);
+                v[q + 2] = o.z - u.z + min(w.z, kBucket);
+                v[q + 3] = o.w - u.w + min(w.w, kBucket);
+                *reinterpret_cast<int4 *>(new_count + base + q) = make_int4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < kScanPer; ++q) {
+                const int c = base + q;
+                v[q] = c < ncells ? old_count[c] - out_count[c] + min(in_count[c], kBucket) : 0;
+                if (c < ncells) new_count[c] = v[q];
+            }
         }
+        int sum = 0;
+#pragma unroll
+        for (int q = 0; q < kScanPer; ++q) sum += v[q];
         int incl = sum;
         for (int off = 1; off < 32; off <<= 1) {
             const int o = __shfl_up_sync(kFull, incl, off);
@@ -1577,15 +1586,21 @@ __global__ void __launch_bounds__(1024) scan_kernel(int ncells, const int *__res
         }
         __syncthreads();
         int run = carry + (wid > 0 ? warp_total[wid - 1] : 0) + incl - sum;
+        if (base + kScanPer <= ncells) {
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int idx = 8 * t + q;
-            if (idx < m) cnt[scan_pad(idx)] = run;
-            run += v[q];
+            for (int q = 0; q < kScanPer; q += 4) {
+                const int a0 = run, a1 = a0 + v[q], a2 = a1 + v[q + 1], a3 = a2 + v[q + 2];
+                *reinterpret_cast<int4 *>(new_start + base + q) = make_int4(a0, a1, a2, a3);
+                run = a3 + v[q + 3];
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < kScanPer; ++q) {
+                if (base + q < ncells) new_start[base + q] = run;
+                run += v[q];
+            }
         }
         carry += warp_total[31];
-        __syncthreads();
-        for (int k = t; k < m; k += blockDim.x) new_start[c0 + k] = cnt[scan_pad(k)];
         __syncthreads();
     }
     if (t == 0) {
