@@ -34,6 +34,7 @@
  *   mxg_engine_start               engine_start             src/mdcore/include/engine.h:640
  *   mxg_engine_step                engine_step              src/mdcore/src/engine.cpp:1198
  *   mxg_engine_force               engine_force             src/mdcore/src/engine.cpp:1230
+ *   mxg_engine_step_timed          engine_step with the engine timers (engine.h:113-135)
  *   mxg_engine_load                engine_load              src/mdcore/include/engine.h:612
  *   mxg_engine_unload              engine_unload            src/mdcore/include/engine.h:646
  *   mxg_engine_kinetic_energy      engine_kinetic_energy    src/mdcore/src/engine.cpp:1698
@@ -276,6 +277,11 @@ int mxg_engine_pairs_within(mxg_engine *e, int n, const int *ids, float cutoff, 
 int mxg_engine_start(mxg_engine *e, void *cuda_stream);
 /* Runs nsteps forward-Euler steps on the device (forces, bonds, integrate, re-bin). */
 int mxg_engine_step(mxg_engine *e, int nsteps);
+/* nsteps steps launched one kernel at a time with CUDA events at the phase boundaries; ms[n] (n >= 15)
+ * receives the summed milliseconds at the reference's timer ids (engine.h:113-135): 0 step, 1 prepare
+ * (single-body and wall/large-particle passes), 4 nonbond, 5 bonded (with species fluxes), 11 advance,
+ * 14 shuffle (re-binning); under Runge-Kutta 4 the whole step is counted as advance. */
+int mxg_engine_step_timed(mxg_engine *e, int nsteps, double *ms, int n);
 /* Computes forces (and energies) for the current positions without advancing. */
 int mxg_engine_force(mxg_engine *e);
 /* Waits for the engine's stream and returns the device status word as a status code. */

@@ -847,6 +847,18 @@ class _Universe:
         self.time += int(n)
         check(lib().mxg_engine_status(self._e), "engine_step")
 
+    def timers(self, n=1):
+        """Steps n times launching kernel by kernel and returns the milliseconds per step of each
+        phase, named after the reference's engine timers (engine.h:113-135)."""
+        self._ensure()
+        ms = np.zeros(16)
+        check(lib().mxg_engine_step_timed(self._e, int(n), ptr(ms, ctypes.c_double), len(ms)), "step_timed")
+        self.time += int(n)
+        check(lib().mxg_engine_status(self._e), "engine_step")
+        k = max(1, int(n))
+        return {"step": ms[0] / k, "prepare": ms[1] / k, "nonbond": ms[4] / k, "bonded": ms[5] / k,
+                "advance": ms[11] / k, "shuffle": ms[14] / k}
+
     def force(self):
         self._ensure()
         check(lib().mxg_engine_force(self._e), "engine_force")

@@ -671,25 +671,42 @@ struct mxg_engine {
      * the received planes are added by the bonded kernel or, without bonded
      * interactions, by the integrator; the re-binning pass computes the new key
      * bounds. */
-    void enqueue_step(int b) {
+    /* ev (optional, 6 events): recorded at the phase boundaries prepare | nonbond | bonded |
+     * advance | shuffle (the reference's engine timers). */
+    void enqueue_step(int b, cudaEvent_t *ev = nullptr) {
+        auto mark = [&](int k) {
+            if (ev) cudaEventRecord(ev[k], stream);
+        };
         if (integrator == 1) {
+            mark(0);
+            mark(1);
+            mark(2);
+            mark(3);
             enqueue_step_rk4(b);
+            mark(4);
+            mark(5);
             return;
         }
         const int nb = 1 - b;
         const EngineView v = view(b);
+        mark(0);
         if (has_sb) launch_singlebody_prep(v, ntypes, d_type_ke, d_persist, true, stream);
         if (has_body()) launch_body(v, d_body_f, stream);
+        mark(1);
         launch_force(v, has_dpd, force_grid, false, stream);
+        mark(2);
         if (has_bonded()) launch_bonded(v, bonded_view(), stream);
         if (has_fluxes) launch_fluxes(v, species_view(), stream);
+        mark(3);
         launch_integrate(v, d_pos[b], d_vel[b], d_new_cell, d_in_count, d_in_list, d_out_count, !has_bonded(),
                          stream);
         if (has_fluxes) launch_species_integrate(v, species_view(), d_new_cell, stream);  // MxFluxes_Integrate
+        mark(4);
         launch_scan(ncells, d_cell_count[b], d_out_count, d_in_count, d_cell_start[nb], d_cell_count[nb], d_step,
                     stream);
         launch_scatter(v, d_pos[b], d_vel[b], d_new_cell, d_cell_start[b], d_cell_count[b], d_in_count, d_in_list,
                        d_out_count, d_cell_start[nb], d_pos[nb], d_vel[nb], d_cell_of[nb], d_slot_of_id, stream);
+        mark(5);
     }
 
     /* One Runge-Kutta 4 step (engine_advance_runge_kutta_4): four force passes (with
@@ -1828,6 +1845,38 @@ int mxg_engine_step(mxg_engine *e, int nsteps) {
         e->force_layout = 1 - e->cur;
     }
     return MXG_OK;
+}
+
+int mxg_engine_step_timed(mxg_engine *e, int nsteps, double *ms, int n) {
+    if (!e || !ms) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    if (n < 15 || nsteps < 0) return MXG_ERR_ARG;
+    for (int k = 0; k < n; ++k) ms[k] = 0.0;
+    if (e->nparts == 0) return MXG_OK;
+    cudaEvent_t ev[6];
+    for (int k = 0; k < 6; ++k) CUDA_TRY(cudaEventCreate(&ev[k]));
+    // timer ids of the reference (engine.h:113-135): step 0, prepare 1, nonbond 4, bonded 5,
+    // advance 11, shuffle 14
+    const int slot[5] = {1, 4, 5, 11, 14};
+    int rc = MXG_OK;
+    for (int s = 0; s < nsteps && rc == MXG_OK; ++s) {
+        e->enqueue_step(e->cur, ev);
+        if (cudaGetLastError() != cudaSuccess || cudaEventSynchronize(ev[5]) != cudaSuccess) {
+            rc = MXG_ERR_CUDA;
+            break;
+        }
+        float t;
+        for (int k = 0; k < 5; ++k) {
+            cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+            ms[slot[k]] += t;
+        }
+        cudaEventElapsedTime(&t, ev[0], ev[5]);
+        ms[0] += t;
+        e->cur = 1 - e->cur;
+        e->force_layout = 1 - e->cur;
+    }
+    for (int k = 0; k < 6; ++k) cudaEventDestroy(ev[k]);
+    return rc;
 }
 
 int mxg_engine_force(mxg_engine *e) {
