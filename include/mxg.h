@@ -319,7 +319,8 @@ int mxg_engine_energy_async(mxg_engine *e, double *host_out2);
 int mxg_engine_finalize(mxg_engine *e);
 
 /* ---- adjoint (reverse-mode gradients of trajectories) ---- No counterpart in the reference. ---- */
-/* Bytes of a state snapshot (positions, velocities, cell lists, id map, step counter, bond flags). */
+/* Bytes of a state snapshot (positions, velocities, cell lists, id map, step counter, bond flags, species
+ * values and rates, persistent random single-body forces). */
 int mxg_engine_snapshot_bytes(const mxg_engine *e, size_t *bytes);
 /* save = 1: copies the current state into dev_buf (device memory, 16-byte aligned); save = 0: makes
  * dev_buf's state current. Ordered on the engine stream; restoring then stepping reproduces the

@@ -847,6 +847,47 @@ class _Universe:
         self.time += int(n)
         check(lib().mxg_engine_status(self._e), "engine_step")
 
+    def checkpoint(self, path=None):
+        """The exact engine state: positions and velocities in the engine's cell frame, cell
+        lists, id map, step counter (which keys the random streams), bond flags, species values
+        and rates and the persistent random single-body forces. Restoring it into a universe
+        built the same way resumes the trajectory bit for bit. Returns a dict of arrays and
+        writes it to `path` (.npz) when given. The reference has no checkpoint."""
+        import torch
+        self._ensure()
+        b = ctypes.c_size_t()
+        check(lib().mxg_engine_snapshot_bytes(self._e, ctypes.byref(b)), "snapshot_bytes")
+        buf = torch.empty(b.value, dtype=torch.uint8, device="cuda")
+        check(lib().mxg_engine_snapshot(self._e, ctypes.c_void_p(buf.data_ptr()), 1), "snapshot")
+        check(lib().mxg_engine_status(self._e), "snapshot")  # the engine stream is done with it
+        data = {"snapshot": buf.cpu().numpy(), "species": self.species_values(), "time": np.int64(self.time),
+                "nparts": np.int64(len(self._t))}
+        if path is not None:
+            np.savez(path, **data)
+        return data
+
+    def restore(self, data):
+        """Makes a checkpoint (the dict or an .npz path) the current state; the universe must
+        have been built the same way (types, particles, potentials, bonds, box)."""
+        import torch
+        if not isinstance(data, dict):
+            with np.load(data) as z:
+                data = {k: z[k] for k in z.files}
+        self._ensure()
+        if int(data["nparts"]) != len(self._t):
+            raise ValueError("the checkpoint holds a different number of particles")
+        b = ctypes.c_size_t()
+        check(lib().mxg_engine_snapshot_bytes(self._e, ctypes.byref(b)), "snapshot_bytes")
+        snap = np.ascontiguousarray(data["snapshot"], dtype=np.uint8)
+        if snap.size != b.value:
+            raise ValueError("the checkpoint was taken from a differently built universe")
+        buf = torch.from_numpy(snap).to("cuda")
+        torch.cuda.synchronize()
+        check(lib().mxg_engine_snapshot(self._e, ctypes.c_void_p(buf.data_ptr()), 0), "restore")
+        check(lib().mxg_engine_status(self._e), "restore")
+        self._spec = np.ascontiguousarray(data["species"], dtype=np.float32).copy()
+        self.time = int(data["time"])
+
     def timers(self, n=1):
         """Steps n times launching kernel by kernel and returns the milliseconds per step of each
         phase, named after the reference's engine timers (engine.h:113-135)."""

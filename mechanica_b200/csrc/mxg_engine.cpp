@@ -787,7 +787,7 @@ struct mxg_engine {
 
     /* Layout of a state snapshot: byte offsets of its sections (16-byte aligned). */
     struct SnapLayout {
-        size_t pos, vel, cell_of, slot_of_id, start, count, step, bonds, total;
+        size_t pos, vel, cell_of, slot_of_id, start, count, step, bonds, spec, rate, persist, total;
     };
     SnapLayout snap_layout() const {
         SnapLayout L;
@@ -805,6 +805,9 @@ struct mxg_engine {
         L.count = take(sizeof(int) * (size_t)ncells);
         L.step = take(sizeof(unsigned long long));
         L.bonds = take(sizeof(unsigned) * bonds.size());
+        L.spec = take(sizeof(float) * (size_t)nparts * smax);
+        L.rate = take(sizeof(float) * (size_t)nparts * smax);
+        L.persist = take(has_sb ? sizeof(float4) * (size_t)nparts : 0);
         L.total = o;
         return L;
     }
@@ -2098,6 +2101,9 @@ int mxg_engine_snapshot(mxg_engine *e, void *dev_buf, int save) {
         {e->d_cell_count[c], L.count, sizeof(int) * (size_t)e->ncells},
         {e->d_step, L.step, sizeof(unsigned long long)},
         {e->d_bond_flags, L.bonds, sizeof(unsigned) * e->bonds.size()},
+        {e->d_spec, L.spec, sizeof(float) * (size_t)e->nparts * e->smax},
+        {e->d_rate, L.rate, sizeof(float) * (size_t)e->nparts * e->smax},
+        {e->d_persist, L.persist, e->has_sb ? sizeof(float4) * (size_t)e->nparts : 0},
     };
     for (const Sec &q : secs) {
         if (q.bytes == 0) continue;
