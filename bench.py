@@ -216,6 +216,20 @@ def forms_and_configs(args, stream, flush):
         out[name] = {"value": n * K / (ms / 1e3), "unit": "particle-steps/s", "particles": n, "steps": K,
                      "ms_per_step": ms / K}
         m.universe.close()
+        if not args.no_cpu_baseline:
+            # the reference engine on the host cores, a bounded sample of the same workload
+            try:
+                from oracle import refengine
+                if refengine.available():
+                    cores = os.cpu_count() or 1
+                    ks = 100 if name.startswith("lj") else 10
+                    r = refengine.run(dict(scn, action="steps", nsteps=ks, warmup=2, runners=cores))
+                    ref = n * ks / float(r["seconds"])
+                    out[name]["cpu_reference"] = {"value": ref, "unit": "particle-steps/s", "cores": cores,
+                                                  "kind": "reference", "sample": f"{ks} engine_step calls"}
+                    out[name]["speedup_vs_cpu_reference"] = out[name]["value"] / ref
+            except Exception as exc:
+                out[name]["cpu_reference"] = {"error": str(exc)[:200]}
 
     # batched ensemble: all replicas in one engine, one set of launches per step
     specs = W.cell_sorting_specs(nrep=256, seed=5)
