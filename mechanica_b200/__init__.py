@@ -847,6 +847,30 @@ class _Universe:
         self.time += int(n)
         check(lib().mxg_engine_status(self._e), "engine_step")
 
+    def device_state(self):
+        """Zero-copy torch views of the device-resident state in slot order (cells in order,
+        ascending id inside a cell): "pos" (N, 4) float32 cell-relative x, y, z and the type id's
+        bits in w; "vel" (N, 4) v and the particle id's bits in w; "force" (N, 4); "cell" (N,)
+        int32. Read the w columns with .view(torch.int32). The views follow the engine's double
+        buffers, so they are valid until the next step or force pass."""
+        import torch
+        self._ensure()
+        p, v, f, c = (ctypes.c_void_p() for _ in range(4))
+        check(lib().mxg_engine_device_state(self._e, ctypes.byref(p), ctypes.byref(v), ctypes.byref(f),
+                                            ctypes.byref(c)), "device_state")
+        n = len(self._t)
+
+        class _View:
+            def __init__(self, ptr, shape, typestr):
+                self.__cuda_array_interface__ = {"shape": shape, "typestr": typestr, "data": (ptr, False),
+                                                 "version": 3, "strides": None}
+
+        out = {}
+        for name, ptr_, shape, ts in (("pos", p, (n, 4), "<f4"), ("vel", v, (n, 4), "<f4"),
+                                      ("force", f, (n, 4), "<f4"), ("cell", c, (n,), "<i4")):
+            out[name] = torch.as_tensor(_View(ptr_.value or 0, shape, ts), device="cuda")
+        return out
+
     def checkpoint(self, path=None):
         """The exact engine state: positions and velocities in the engine's cell frame, cell
         lists, id map, step counter (which keys the random streams), bond flags, species values

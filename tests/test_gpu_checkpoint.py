@@ -45,3 +45,19 @@ def test_restore_rejects_another_universe(tmp_path):
     u2 = S.build_gpu(scn2)
     with pytest.raises(ValueError):
         u2.restore(ck)
+
+
+def test_device_state_views_match_state():
+    """The zero-copy device views hold the same state as the host copies."""
+    import torch
+    z, scn = load("argon_small")
+    u = S.build_gpu(scn)
+    u.steps(2)
+    d = u.device_state()
+    torch.cuda.synchronize()
+    x, v, f, c, xr = u.state()
+    ids = d["vel"].view(torch.int32)[:, 3].cpu().numpy()
+    assert sorted(ids.tolist()) == list(range(len(x)))
+    assert np.array_equal(d["pos"][:, :3].cpu().numpy(), xr[ids].astype(np.float32))
+    assert np.array_equal(d["vel"][:, :3].cpu().numpy(), v[ids])
+    assert np.array_equal(d["cell"].cpu().numpy(), c[ids])
