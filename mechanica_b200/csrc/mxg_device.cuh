@@ -23,7 +23,7 @@ constexpr int kChunk = 8;           // floats per table interval
 constexpr int kBucket = 32;         // max particles entering one cell per step
 constexpr int kMaxTypes = 64;       // types per engine
 constexpr int kWarpsPerBlock = 4;   // force kernel: warps (work items) per block
-constexpr int kMaxCellParts = 4;    // force work items per cell at most
+constexpr int kMaxCellParts = 8;    // force work items per cell at most
 
 /* neighbour-entry roles, relative to the reference's (flipped) cell pair */
 enum : int { kRoleSelf = 0, kRoleFirst = 1, kRoleSecond = 2 };
@@ -213,6 +213,7 @@ struct EngineView {      // everything a kernel needs, passed by value
     const int *large_pot;    // per replica [ntypes*ntypes]: potential of a (normal, large) type pair, or -1
     int nlarge;
     const int4 *items;       // force work items: (cell, first entry, end entry, part)
+    int *item_ctr;           // [0] next work item, [1] warps done (dynamic fetch; zero between launches)
     int nitems;
 };
 

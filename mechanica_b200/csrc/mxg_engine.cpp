@@ -387,6 +387,7 @@ struct mxg_engine {
     float4 *d_planes = nullptr;
     int nplanes = 0;
     int4 *d_items = nullptr;            // force work items: (cell, first entry, end entry, part)
+    int *d_item_ctr = nullptr;          // the force kernel's work-item counter and finished-warp count
     int *d_cell_planes = nullptr;       // planes summed into each cell's forces
     int nitems = 0;
     DevPot *d_pots = nullptr;
@@ -604,6 +605,7 @@ struct mxg_engine {
         v.sec_count = d_sec_count;
         v.cell_planes = d_cell_planes;
         v.items = d_items;
+        v.item_ctr = d_item_ctr;
         v.nitems = nitems;
         v.planes = d_planes;
         v.body_e = (has_walls || nlarge) ? d_body_e : nullptr;
@@ -907,15 +909,17 @@ int mxg_engine::start(cudaStream_t st) {
     if (smax > 0 && spec_host.size() != (size_t)nparts * smax) spec_host.resize((size_t)nparts * smax, 0.0f);
 
     // ---- work items: each cell's SELF and FIRST entries split into up to `parts`
-    // groups (one warp each) when there are too few cells to fill the GPU. Item k > 0
-    // of a cell sums its own-side forces into plane sec_count + k - 1 of the cell.
+    // groups (one warp each) when there are too few cells for about three waves of
+    // items (warps fetch items from a counter, so finer items shorten the tail that the
+    // most crowded cells leave). Item k > 0 of a cell sums its own-side forces into
+    // plane sec_count + k - 1 of the cell.
     {
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         num_sms = sms;
     }
-    const int want_warps = num_sms * 32;
+    const int want_warps = num_sms * 64;
     const int parts = std::max(1, std::min(kMaxCellParts, (want_warps + ncells - 1) / std::max(1, ncells)));
     std::vector<int> nb_off(ncells + 1, 0), nb_cell, nb_rev, hplanes(ncells, 0);
     std::vector<float4> nb_shift;
@@ -1170,6 +1174,7 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_sec_count, ncells);
     rc |= alloc(&d_cell_planes, ncells);
     rc |= alloc(&d_items, hitems.size());
+    rc |= alloc(&d_item_ctr, 2);
     rc |= alloc(&d_planes, (size_t)nplanes * nparts);
     rc |= alloc(&d_pots, hp.size());
     rc |= alloc(&d_coef, coef.size() + 8);
@@ -1221,6 +1226,7 @@ int mxg_engine::start(cudaStream_t st) {
     CUDA_TRY(cudaMemsetAsync(d_out_count, 0, sizeof(int) * ncells, stream));
     CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
     CUDA_TRY(cudaMemsetAsync(d_step, 0, sizeof(unsigned long long), stream));
+    CUDA_TRY(cudaMemsetAsync(d_item_ctr, 0, 2 * sizeof(int), stream));
     CUDA_TRY(cudaMemsetAsync(d_epot_cell, 0, sizeof(double) * std::max(1, nitems), stream));
     CUDA_TRY(cudaMemsetAsync(d_ebond_slot, 0, sizeof(double) * std::max(1, nparts), stream));
     CUDA_TRY(cudaMemsetAsync(d_body_e, 0, sizeof(double) * std::max(1, nparts), stream));

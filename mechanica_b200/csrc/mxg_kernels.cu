@@ -463,7 +463,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 5) force_kernel(EngineVie
         tinfo[t] = T.has_force ? make_float4(T.fx, T.fy, T.fz, T.radius) : make_float4(0.f, 0.f, 0.f, T.radius);
     }
     __syncthreads();
-    for (int it = blockIdx.x * kWarpsPerBlock + w; it < v.nitems; it += gridDim.x * kWarpsPerBlock) {
+    // work items: fetched from a counter (the crowded cells' items would otherwise hold
+    // their block's slot while the other warps idle); the virial launch keeps a fixed
+    // grid-stride assignment, so that its per-warp FP64 partials sum in a fixed order.
+    // Every item writes only its own outputs, so the fetch order changes no result.
+    const int nwarps = gridDim.x * kWarpsPerBlock;
+    auto fetch = [&](int prev) -> int {
+        if (kMode == 2) return prev < 0 ? blockIdx.x * kWarpsPerBlock + w : prev + nwarps;
+        int t = 0;
+        if (lane == 0) t = atomicAdd(v.item_ctr, 1);
+        return __shfl_sync(kFull, t, 0);
+    };
+    for (int it = fetch(-1); it < v.nitems; it = fetch(it)) {
         const int4 item = v.items[it];
         const int c = item.x, nb0 = item.y, nb1 = item.z, part = item.w;
         const int n = v.cell_count[c];
@@ -705,6 +716,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 5) force_kernel(EngineVie
         }
         for (int off = 16; off > 0; off >>= 1) ecell += __shfl_xor_sync(kFull, ecell, off);
         if (lane == 0 && kMode != 2) v.epot_cell[it] = ecell;
+    }
+    if (kMode != 2 && lane == 0) {
+        // every warp has drawn its last ticket once the done count reaches the grid's warps:
+        // the last one re-arms both counters for the next launch on the stream
+        if (atomicAdd(v.item_ctr + 1, 1) == nwarps - 1) {
+            atomicExch(v.item_ctr, 0);
+            atomicExch(v.item_ctr + 1, 0);
+        }
     }
     if (kMode == 1) {
         for (int off = 16; off > 0; off >>= 1) npair += __shfl_xor_sync(kFull, npair, off);
