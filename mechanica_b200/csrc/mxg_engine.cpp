@@ -932,18 +932,27 @@ int mxg_engine::start(cudaStream_t st) {
             ((pk & 3) == kRoleSelf ? self_e : (pk & 3) == kRoleFirst ? first_e : second_e).push_back(&e);
         }
         const int nf = (int)first_e.size();
-        const int groups = std::max(1, std::min(parts, nf));
         auto push = [&](const NbEntry *e) {
             nb_cell.push_back(e->cell);
             nb_shift.push_back(e->shift);
             nb_rev.push_back(e->rev);
         };
-        for (int g = 0; g < groups; ++g) {
+        // a split cell's SELF entry is an item of its own (the crowded cells' n^2 own pairs
+        // would otherwise make their first item the longest of the launch)
+        const bool self_alone = parts > 1 && !self_e.empty() && nf >= 2;
+        const int fgroups = std::max(1, std::min(self_alone ? parts - 1 : parts, nf));
+        const int groups = fgroups + (self_alone ? 1 : 0);
+        if (self_alone) {
             const int e0 = (int)nb_cell.size();
-            if (g == 0)
+            for (auto *e : self_e) push(e);
+            hitems.push_back(make_int4(c, e0, (int)nb_cell.size(), 0));
+        }
+        for (int g = 0; g < fgroups; ++g) {
+            const int e0 = (int)nb_cell.size();
+            if (g == 0 && !self_alone)
                 for (auto *e : self_e) push(e);
-            for (int k = g * nf / groups; k < (g + 1) * nf / groups; ++k) push(first_e[k]);
-            hitems.push_back(make_int4(c, e0, (int)nb_cell.size(), g));
+            for (int k = g * nf / fgroups; k < (g + 1) * nf / fgroups; ++k) push(first_e[k]);
+            hitems.push_back(make_int4(c, e0, (int)nb_cell.size(), g + (self_alone ? 1 : 0)));
         }
         for (auto *e : second_e) push(e);
         nb_off[c + 1] = (int)nb_cell.size();
