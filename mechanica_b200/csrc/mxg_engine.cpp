@@ -388,6 +388,8 @@ struct mxg_engine {
     int nplanes = 0;
     int4 *d_items = nullptr;            // force work items: (cell, first entry, end entry, part)
     int *d_item_ctr = nullptr;          // the force kernel's work-item counter and finished-warp count
+    int *d_item_order = nullptr;        // work items, most crowded cells first (when cells are split)
+    bool order_items = false;
     int *d_cell_planes = nullptr;       // planes summed into each cell's forces
     int nitems = 0;
     DevPot *d_pots = nullptr;
@@ -606,6 +608,7 @@ struct mxg_engine {
         v.cell_planes = d_cell_planes;
         v.items = d_items;
         v.item_ctr = d_item_ctr;
+        v.item_order = order_items ? d_item_order : nullptr;
         v.nitems = nitems;
         v.planes = d_planes;
         v.body_e = (has_walls || nlarge) ? d_body_e : nullptr;
@@ -959,6 +962,11 @@ int mxg_engine::start(cudaStream_t st) {
         hplanes[c] = hsec[c] + groups - 1;
     }
     nitems = (int)hitems.size();
+    // few crowded cells, split into several items each: the launch's length is set by the
+    // most crowded cells' items, so they are handed out first (reordered before every force
+    // pass). With sparse cells (mean occupancy below 16) the items are short and the
+    // ordering launch costs more than the tail it removes.
+    order_items = parts > 1 && (long long)nparts >= 16LL * ncells;
     nplanes = 0;
     for (int c = 0; c < ncells; ++c) nplanes = std::max(nplanes, hplanes[c]);
 
@@ -1184,6 +1192,7 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_cell_planes, ncells);
     rc |= alloc(&d_items, hitems.size());
     rc |= alloc(&d_item_ctr, 2);
+    rc |= alloc(&d_item_order, hitems.size());
     rc |= alloc(&d_planes, (size_t)nplanes * nparts);
     rc |= alloc(&d_pots, hp.size());
     rc |= alloc(&d_coef, coef.size() + 8);

@@ -471,7 +471,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 5) force_kernel(EngineVie
     auto fetch = [&](int prev) -> int {
         if (kMode == 2) return prev < 0 ? blockIdx.x * kWarpsPerBlock + w : prev + nwarps;
         int t = 0;
-        if (lane == 0) t = atomicAdd(v.item_ctr, 1);
+        if (lane == 0) {
+            t = atomicAdd(v.item_ctr, 1);
+            if (v.item_order && t < v.nitems) t = v.item_order[t];
+        }
         return __shfl_sync(kFull, t, 0);
     };
     for (int it = fetch(-1); it < v.nitems; it = fetch(it)) {
@@ -1788,7 +1791,42 @@ void launch_force_mode(const EngineView &v, int grid, cudaStream_t st) {
         force_kernel<kDPD, 0><<<grid, kWarpsPerBlock * 32, bytes, st>>>(v);
 }
 
+/* Work items by decreasing occupancy of their cell (counting sort on the count, capped
+ * at 255; ties in any order, which changes no result: each item writes only its own
+ * outputs). One block; launched before a force pass when cells are split into several
+ * items, so that the most crowded cells' items start first. */
+__global__ void item_order_kernel(EngineView v) {
+    __shared__ int bin[256];
+    for (int k = threadIdx.x; k < 256; k += blockDim.x) bin[k] = 0;
+    __syncthreads();
+    for (int it = threadIdx.x; it < v.nitems; it += blockDim.x)
+        atomicAdd(&bin[255 - min(v.cell_count[v.items[it].x], 255)], 1);
+    __syncthreads();
+    if (threadIdx.x < 32) {  // exclusive scan of the 256 bins, one warp, 8 bins a lane
+        const int lane = threadIdx.x;
+        int c[8], s = 0;
+        for (int k = 0; k < 8; ++k) {
+            c[k] = bin[lane * 8 + k];
+            s += c[k];
+        }
+        int incl = s;
+        for (int off = 1; off < 32; off <<= 1) {
+            const int o = __shfl_up_sync(kFull, incl, off);
+            if (lane >= off) incl += o;
+        }
+        int run = incl - s;
+        for (int k = 0; k < 8; ++k) {
+            bin[lane * 8 + k] = run;
+            run += c[k];
+        }
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < v.nitems; it += blockDim.x)
+        v.item_order[atomicAdd(&bin[255 - min(v.cell_count[v.items[it].x], 255)], 1)] = it;
+}
+
 void launch_force(const EngineView &v, bool has_dpd, int grid, bool combine, cudaStream_t st) {
+    if (v.item_order && v.nitems > 0 && !v.virial_partials) item_order_kernel<<<1, 1024, 0, st>>>(v);
     if (has_dpd)
         launch_force_mode<true>(v, grid, st);
     else
