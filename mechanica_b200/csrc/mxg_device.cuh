@@ -24,6 +24,7 @@ constexpr int kBucket = 32;         // max particles entering one cell per step
 constexpr int kMaxTypes = 64;       // types per engine
 constexpr int kWarpsPerBlock = 4;   // force kernel: warps (work items) per block
 constexpr int kMaxCellParts = 8;    // force work items per cell at most
+constexpr int kOrderMaxItems = 32768;  // work items the occupancy ordering handles at most
 
 /* neighbour-entry roles, relative to the reference's (flipped) cell pair */
 enum : int { kRoleSelf = 0, kRoleFirst = 1, kRoleSecond = 2 };

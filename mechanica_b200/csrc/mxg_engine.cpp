@@ -966,7 +966,7 @@ int mxg_engine::start(cudaStream_t st) {
     // most crowded cells' items, so they are handed out first (reordered before every force
     // pass). With sparse cells (mean occupancy below 16) the items are short and the
     // ordering launch costs more than the tail it removes.
-    order_items = parts > 1 && (long long)nparts >= 16LL * ncells;
+    order_items = parts > 1 && (long long)nparts >= 16LL * ncells && nitems <= kOrderMaxItems;
     nplanes = 0;
     for (int c = 0; c < ncells; ++c) nplanes = std::max(nplanes, hplanes[c]);
 

@@ -1797,32 +1797,50 @@ void launch_force_mode(const EngineView &v, int grid, cudaStream_t st) {
  * items, so that the most crowded cells' items start first. */
 __global__ void item_order_kernel(EngineView v) {
     __shared__ int bin[256];
+    __shared__ unsigned char key_s[kOrderMaxItems];  // 255 - min(count, 255) per item
+    const int lane = threadIdx.x & 31;
     for (int k = threadIdx.x; k < 256; k += blockDim.x) bin[k] = 0;
-    __syncthreads();
+    // the keys first, with independent loads in flight (the host orders at most
+    // kOrderMaxItems items)
+#pragma unroll 8
     for (int it = threadIdx.x; it < v.nitems; it += blockDim.x)
-        atomicAdd(&bin[255 - min(v.cell_count[v.items[it].x], 255)], 1);
+        key_s[it] = (unsigned char)(255 - min(v.cell_count[v.items[it].x], 255));
     __syncthreads();
-    if (threadIdx.x < 32) {  // exclusive scan of the 256 bins, one warp, 8 bins a lane
-        const int lane = threadIdx.x;
-        int c[8], s = 0;
-        for (int k = 0; k < 8; ++k) {
-            c[k] = bin[lane * 8 + k];
-            s += c[k];
+    // consecutive items mostly share a cell: the lanes of a warp with equal keys take
+    // one shared-memory atomic between them (the leader's), the others their rank
+    const int nround = (v.nitems + blockDim.x - 1) / blockDim.x;
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int r = 0; r < nround; ++r) {
+            const int it = r * blockDim.x + threadIdx.x;
+            const bool live = it < v.nitems;
+            const int key = live ? (int)key_s[it] : 256;
+            const unsigned peers = __match_any_sync(kFull, key);
+            const int leader = __ffs(peers) - 1;
+            int base = 0;
+            if (lane == leader && live) base = atomicAdd(&bin[key], __popc(peers));
+            base = __shfl_sync(kFull, base, leader);
+            if (pass == 1 && live) v.item_order[base + __popc(peers & ((1u << lane) - 1u))] = it;
         }
-        int incl = s;
-        for (int off = 1; off < 32; off <<= 1) {
-            const int o = __shfl_up_sync(kFull, incl, off);
-            if (lane >= off) incl += o;
+        __syncthreads();
+        if (pass == 0 && threadIdx.x < 32) {  // exclusive scan of the 256 bins, 8 bins a lane
+            int c[8], sum = 0;
+            for (int k = 0; k < 8; ++k) {
+                c[k] = bin[lane * 8 + k];
+                sum += c[k];
+            }
+            int incl = sum;
+            for (int off = 1; off < 32; off <<= 1) {
+                const int o = __shfl_up_sync(kFull, incl, off);
+                if (lane >= off) incl += o;
+            }
+            int run = incl - sum;
+            for (int k = 0; k < 8; ++k) {
+                bin[lane * 8 + k] = run;
+                run += c[k];
+            }
         }
-        int run = incl - s;
-        for (int k = 0; k < 8; ++k) {
-            bin[lane * 8 + k] = run;
-            run += c[k];
-        }
+        __syncthreads();
     }
-    __syncthreads();
-    for (int it = threadIdx.x; it < v.nitems; it += blockDim.x)
-        v.item_order[atomicAdd(&bin[255 - min(v.cell_count[v.items[it].x], 255)], 1)] = it;
 }
 
 void launch_force(const EngineView &v, bool has_dpd, int grid, bool combine, cudaStream_t st) {
