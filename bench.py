@@ -58,6 +58,25 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(x, world, device=None):
+    """The largest of a per-rank float over all ranks (a MAX all-reduce in FP64). Every
+    rank calls it at the same point; with one rank it returns x."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, n, steps, ms):
+    """Whole-job particle-steps/s: each of `world` ranks advances its own n-particle
+    replica `steps` times, and the job lasts as long as its slowest rank (`ms`, the max
+    over ranks of the device-timed milliseconds)."""
+    return world * n * steps / (ms / 1e3)
+
+
 def workload(n):
     from mechanica_b200 import workloads as W
     scale = (n / 200000.0) ** (1.0 / 3.0)
@@ -398,12 +417,8 @@ def main():
     rc = L.mxg_engine_status(e)
     if rc < 0:
         raise RuntimeError(f"engine status {rc} after the timed steps")
-    ms = sum(s.elapsed_time(t) for s, t in zip(starts, ends))
-    if world > 1:
-        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-    value = world * n * K / (ms / 1e3)
+    ms = max_over_ranks(sum(s.elapsed_time(t) for s, t in zip(starts, ends)), world, dev)
+    value = job_rate(world, n, K, ms)
 
     # ---- e2e through the C ABI with pinned host buffers ----
     hpos = torch.empty(n * 16, dtype=torch.uint8, pin_memory=True)
@@ -427,12 +442,8 @@ def main():
             e2[k].record(stream)
             flush.zero_()
     barrier()
-    ms_e2e = sum(s.elapsed_time(t) for s, t in zip(s2, e2))
-    if world > 1:
-        tt = torch.tensor([ms_e2e], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_e2e = float(tt.item())
-    e2e = world * n * Ke / (ms_e2e / 1e3)
+    ms_e2e = max_over_ranks(sum(s.elapsed_time(t) for s, t in zip(s2, e2)), world, dev)
+    e2e = job_rate(world, n, Ke, ms_e2e)
 
     # ---- roofline of the dominant kernel (nonbonded forces) ----
     R = 50
