@@ -27,6 +27,9 @@
  *   mxg_engine_set_species / mxg_engine_get_species  the particles' species values
  *   mxg_engine_pairs_within        make_pairlist (the pair search of MxBond_PairwiseNew)
  *                                  src/mdcore/src/bond.cpp:892-942
+ *   mxg_engine_group_metrics       MxParticles_CenterOfMass / _CenterOfGeometry / _RadiusOfGyration /
+ *                                  _MomentOfInertia src/mdcore/src/metrics.cpp:330-466 (the
+ *                                  MxParticleList methods, MxParticleList.cpp:406-458)
  *   mxg_engine_add_exclusions      engine_exclusion_add src/mdcore/src/engine_bonded.cpp:1277-1310
  *   mxg_engine_exclusion_shrink    engine_exclusion_shrink src/mdcore/src/engine_bonded.cpp:1235-1262
  *   mxg_engine_adddihedrals        engine_dihedral_addpot + engine_dihedral_add
@@ -273,6 +276,11 @@ int mxg_engine_get_species(mxg_engine *e, int n, int smax, float *out);
  * cap is large enough, else MXG_ERR_RANGE. */
 int mxg_engine_pairs_within(mxg_engine *e, int n, const int *ids, float cutoff, const unsigned char *type_mask,
                             int ntypes, int *out_i, int *out_j, int cap, int *count);
+/* Metrics of a particle group over the current state of a started engine (metrics.cpp:330-466): out[0]
+ * total mass, out[1..3] centre of mass, out[4..6] centroid, out[7] radius of gyration (the reference's
+ * sqrt of the summed distances to the centroid), out[8..16] moment of inertia about the centre of mass
+ * (row-major; off-diagonals + sum m dx dy as in the reference). ids: n >= 1 particle ids. Sums in FP64. */
+int mxg_engine_group_metrics(mxg_engine *e, int n, const int *ids, double *out);
 /* Builds the cell-pair lists and uploads the state. stream may be NULL (default stream). */
 int mxg_engine_start(mxg_engine *e, void *cuda_stream);
 /* Runs nsteps forward-Euler steps on the device (forces, bonds, integrate, re-bin). */

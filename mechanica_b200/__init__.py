@@ -29,7 +29,7 @@ from ._native import EngineError, check, f32, f64, i32, lib, ptr
 __all__ = [
     "init", "Universe", "universe", "Particle", "Potential", "Bond", "Angle", "Dihedral", "flux", "fick", "secrete", "uptake", "bind", "forces", "step", "run",
     "Newtonian", "Overdamped", "FORWARD_EULER", "RUNGE_KUTTA_4", "BOUNDARY_NONE", "PERIODIC_X", "PERIODIC_Y", "PERIODIC_Z",
-    "PERIODIC_FULL", "FREESLIP_X", "FREESLIP_Y", "FREESLIP_Z", "FREESLIP_FULL", "EngineError",
+    "PERIODIC_FULL", "FREESLIP_X", "FREESLIP_Y", "FREESLIP_Z", "FREESLIP_FULL", "EngineError", "ParticleList",
 ]
 
 # particle dynamics (src/mdcore/include/MxParticle.h:48-49)
@@ -440,8 +440,60 @@ class _ParticleMeta(type):
         return ids
 
     def items(cls):
-        """Ids of this type's particles, in id order (ParticleType.items)."""
-        return np.flatnonzero(_require()._t == cls.id).astype(np.int32)
+        """This type's particles, in id order, as a ParticleList (ParticleType.items)."""
+        return ParticleList(np.flatnonzero(_require()._t == cls.id).astype(np.int32))
+
+
+class ParticleList:
+    """A list of particle ids with the reference's group metrics (MxParticleList,
+    src/mdcore/src/MxParticleList.cpp:193-199), computed on the device over the
+    current state: centre of mass, centroid, radius of gyration and moment of
+    inertia with the formulas of src/mdcore/src/metrics.cpp:330-466 (the radius of
+    gyration is the square root of the summed distances to the centroid, and the
+    inertia's off-diagonal terms are + sum m dx dy, as there). Behaves as an int32
+    array of the ids."""
+
+    def __init__(self, ids):
+        self.ids = np.ascontiguousarray(np.asarray(ids, dtype=np.int32).reshape(-1))
+
+    def __len__(self):
+        return len(self.ids)
+
+    def __iter__(self):
+        return iter(self.ids.tolist())
+
+    def __getitem__(self, k):
+        return self.ids[k]
+
+    def __array__(self, dtype=None, copy=None):
+        return self.ids if dtype is None else self.ids.astype(dtype)
+
+    def __repr__(self):
+        return f"ParticleList({self.ids.tolist()!r})"
+
+    def _metrics(self):
+        if len(self.ids) == 0:
+            raise ValueError("empty particle list")
+        u = _require()
+        u._ensure()
+        out = np.zeros(17)
+        check(lib().mxg_engine_group_metrics(u._e, len(self.ids), ptr(self.ids, ctypes.c_int),
+                                             out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "group_metrics")
+        return out
+
+    def center_of_mass(self):
+        return self._metrics()[1:4]
+
+    def centroid(self):
+        return self._metrics()[4:7]
+
+    def radius_of_gyration(self):
+        return float(self._metrics()[7])
+
+    def moment_of_inertia(self):
+        return self._metrics()[8:17].reshape(3, 3)
+
+    inertia = moment_of_inertia
 
 
 class Particle(metaclass=_ParticleMeta):

@@ -85,6 +85,7 @@ _SIGS = {
     "mxg_engine_get_species": ([_vp, ctypes.c_int, ctypes.c_int, _c_float_p], ctypes.c_int),
     "mxg_engine_pairs_within": ([_vp, ctypes.c_int, _c_int_p, ctypes.c_float, _vp, ctypes.c_int, _c_int_p, _c_int_p,
                                  ctypes.c_int, _c_int_p], ctypes.c_int),
+    "mxg_engine_group_metrics": ([_vp, ctypes.c_int, _c_int_p, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "mxg_engine_step_timed": ([_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_int], ctypes.c_int),
     "mxg_engine_add_exclusions": ([_vp, ctypes.c_int, _c_int_p, _c_int_p], ctypes.c_int),
     "mxg_engine_exclusion_shrink": ([_vp], ctypes.c_int),

@@ -13,7 +13,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmxg.so")
 
-SOURCES = ["mxg_kernels.cu", "mxg_adjoint.cu", "mxg_pairs.cu", "mxg_engine.cpp", "potential_table.cpp", "mxg_noalloc.cu"]
+SOURCES = ["mxg_kernels.cu", "mxg_adjoint.cu", "mxg_pairs.cu", "mxg_metrics.cu", "mxg_engine.cpp", "potential_table.cpp",
+           "mxg_noalloc.cu"]
 HEADERS = ["mxg_device.cuh", "mxg_kernels.h", "potential_table.h", "mxg_adjoint.h"]
 
 

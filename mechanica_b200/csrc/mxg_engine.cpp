@@ -1747,6 +1747,30 @@ int mxg_engine_pairs_within(mxg_engine *e, int n, const int *ids, float cutoff, 
     return MXG_OK;
 }
 
+int mxg_engine_group_metrics(mxg_engine *e, int n, const int *ids, double *out) {
+    if (!e || !ids || !out) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    if (n < 1) return MXG_ERR_ARG;
+    for (int q = 0; q < n; ++q)
+        if (ids[q] < 0 || ids[q] >= e->nparts) return MXG_ERR_RANGE;
+    int *d_ids = nullptr;
+    double *d_out = nullptr;
+    if (cudaMalloc(&d_ids, sizeof(int) * (size_t)n) != cudaSuccess) return MXG_ERR_MALLOC;
+    if (cudaMalloc(&d_out, sizeof(double) * 17) != cudaSuccess) {
+        cudaFree(d_ids);
+        return MXG_ERR_MALLOC;
+    }
+    cudaError_t err = cudaMemcpyAsync(d_ids, ids, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, e->stream);
+    if (err == cudaSuccess) {
+        launch_group_metrics(e->view(e->cur), d_ids, n, e->d_slot_of_id, d_out, e->stream);
+        err = cudaMemcpyAsync(out, d_out, sizeof(double) * 17, cudaMemcpyDeviceToHost, e->stream);
+    }
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    cudaFree(d_ids);
+    cudaFree(d_out);
+    return err == cudaSuccess ? MXG_OK : MXG_ERR_CUDA;
+}
+
 int mxg_engine_set_boundary_potential(mxg_engine *e, int face, int type, const mxg_potential *p) {
     if (!e || !p) return MXG_ERR_NULL;
     if (e->started) return MXG_ERR_STATE;

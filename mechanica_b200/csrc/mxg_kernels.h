@@ -7,6 +7,9 @@
 namespace mxg {
 
 void configure_force_kernels();
+/* particle-group metrics (mxg_metrics.cu): out[17] as mxg_engine_group_metrics */
+void launch_group_metrics(const EngineView &v, const int *ids, int n, const int *slot_of_id, double *out,
+                          cudaStream_t st);
 void launch_sort_bounds(const EngineView &v, cudaStream_t st);
 /* Before a force pass: the per-type kinetic energy (Berendsen) and, when redraw is set (the
  * step's first force pass), the persistent random forces due at this step. */

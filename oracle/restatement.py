@@ -163,6 +163,64 @@ def flux_step(x, t, L, cutoff, dt, values, fluxes, konst, moved):
     return out
 
 
+def group_metrics(x, mass, fp32=False):
+    """Particle-group metrics as the reference computes them (src/mdcore/src/metrics.cpp):
+    centre of mass (:366-389), centroid (:391-412), radius of gyration (:330-364: the
+    square root of the SUM of the distances to the centroid) and moment of inertia about
+    the centre of mass (:414-466: diagonal sum m (dy^2 + dz^2) ..., off-diagonal + sum m
+    dx dy ...). x: global positions in list order (the reference's p->x[k] + o[k], in
+    double); mass: per entry. fp32=True repeats the reference's FP32 running sums in list
+    order (Magnum float vectors, `float m`); otherwise every sum is FP64.
+    Returns (total mass, com[3], centroid[3], rog, inertia[3x3])."""
+    x = np.asarray(x, dtype=np.float64)
+    mass = np.asarray(mass, dtype=np.float64)
+    n = len(x)
+    if not fp32:
+        M = mass.sum()
+        com = (mass[:, None] * x).sum(axis=0) / M
+        cen = x.sum(axis=0) / n
+        rog = np.sqrt(np.linalg.norm(cen - x, axis=1).sum())
+        d = x - com
+        I = np.zeros((3, 3))
+        I[0, 0] = ((d[:, 1] ** 2 + d[:, 2] ** 2) * mass).sum()
+        I[1, 1] = ((d[:, 0] ** 2 + d[:, 2] ** 2) * mass).sum()
+        I[2, 2] = ((d[:, 1] ** 2 + d[:, 0] ** 2) * mass).sum()
+        I[0, 1] = I[1, 0] = (d[:, 0] * d[:, 1] * mass).sum()
+        I[1, 2] = I[2, 1] = (d[:, 1] * d[:, 2] * mass).sum()
+        I[0, 2] = I[2, 0] = (d[:, 0] * d[:, 2] * mass).sum()
+        return M, com, cen, float(rog), I
+    f = np.float32
+    r = [f(0)] * 3
+    M = f(0)
+    for i in range(n):  # `r[k] += p->mass * (x + o)`: double product, rounded on the float store
+        M = f(float(M) + mass[i])
+        for k in range(3):
+            r[k] = f(float(r[k]) + mass[i] * x[i, k])
+    com = np.array([f(r[k] / M) for k in range(3)], dtype=np.float32)
+    c = [f(0)] * 3
+    for i in range(n):
+        for k in range(3):
+            c[k] = f(float(c[k]) + x[i, k])
+    cen = np.array([f(c[k] / f(n)) for k in range(3)], dtype=np.float32)
+    r2 = f(0)
+    for i in range(n):
+        dx = [f(float(cen[k]) - x[i, k]) for k in range(3)]
+        r2 = f(r2 + f(np.sqrt(f(f(dx[0] * dx[0] + dx[1] * dx[1]) + dx[2] * dx[2]))))
+    rog = float(np.sqrt(r2))
+    I = np.zeros((3, 3), dtype=np.float32)
+    for i in range(n):
+        d = [f(f(x[i, k]) - com[k]) for k in range(3)]  # pix is a float vector: rounded first
+        m = mass[i]
+        I[0, 0] = f(float(I[0, 0]) + float(f(d[1] * d[1] + d[2] * d[2])) * m)
+        I[1, 1] = f(float(I[1, 1]) + float(f(d[0] * d[0] + d[2] * d[2])) * m)
+        I[2, 2] = f(float(I[2, 2]) + float(f(d[1] * d[1] + d[0] * d[0])) * m)
+        I[0, 1] = f(float(I[0, 1]) + float(f(d[0] * d[1])) * m)
+        I[1, 2] = f(float(I[1, 2]) + float(f(d[1] * d[2])) * m)
+        I[0, 2] = f(float(I[0, 2]) + float(f(d[0] * d[2])) * m)
+    I[1, 0], I[2, 1], I[2, 0] = I[0, 1], I[1, 2], I[0, 2]
+    return float(M), com.astype(np.float64), cen.astype(np.float64), rog, I.astype(np.float64)
+
+
 def nonbond(scn, xrel, vel, cell, tasks, cdim, precision=64, tables=None, second=None, pruning=0, virial=False):
     """Forces (N,3) float64, energy, counts for a configuration.
 

@@ -74,3 +74,38 @@ def test_flux_restatement_matches_reference():
                       scn["fluxes"], konst, moved)
     assert moved.sum() > 0
     assert np.abs(out - z["step1_species"]).max() <= 1e-6
+
+
+def test_group_metrics_restatement_known_answer():
+    """Two particles at x = 0 and 2 with masses 1 and 3 (metrics.cpp:330-466): centroid
+    1, centre of mass 1.5, radius of gyration sqrt(|1 - 0| + |1 - 2|) = sqrt(2) (the
+    reference sums distances, not squares), inertia about the centre of mass
+    diag(0, 3, 3); the FP32 running sums give the same values here."""
+    import numpy as np
+    from oracle import restatement as R
+    x = np.array([[0.0, 0.0, 0.0], [2.0, 0.0, 0.0]])
+    m = np.array([1.0, 3.0])
+    for fp32 in (False, True):
+        M, com, cen, rog, I = R.group_metrics(x, m, fp32=fp32)
+        assert M == 4.0
+        assert np.allclose(com, [1.5, 0, 0]) and np.allclose(cen, [1.0, 0, 0])
+        assert abs(rog - np.sqrt(2.0)) < 1e-7
+        assert np.allclose(I, np.diag([0.0, 3.0, 3.0]))
+    # an off-diagonal term keeps the reference's + sign
+    x = np.array([[1.0, 1.0, 0.0], [-1.0, -1.0, 0.0]])
+    I = R.group_metrics(x, np.ones(2))[4]
+    assert I[0, 1] == 2.0 and I[1, 0] == 2.0
+
+
+def test_group_metrics_fp32_close_to_fp64():
+    import numpy as np
+    from oracle import restatement as R
+    rng = np.random.default_rng(4)
+    x = rng.uniform(0, 10, size=(400, 3))
+    m = rng.uniform(1, 3, size=400)
+    a, b = R.group_metrics(x, m), R.group_metrics(x, m, fp32=True)
+    assert abs(a[0] - b[0]) <= 1e-6 * a[0]
+    assert np.abs(a[1] - b[1]).max() <= 1e-6 * np.abs(a[1]).max()
+    assert np.abs(a[2] - b[2]).max() <= 1e-6 * np.abs(a[2]).max()
+    assert abs(a[3] - b[3]) <= 1e-6 * a[3]
+    assert np.abs(a[4] - b[4]).max() <= 1e-5 * np.abs(a[4]).max()
