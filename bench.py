@@ -37,9 +37,12 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-steps/s (1 B200) plain vs batched/adjoint; force rel-err <=1e-5"
 WORKLOAD = ("DPD fluid with body force: 200,000 particles, 40x20x20 box, periodic x/y, no-slip z; "
             "DPD a=25 gamma=4.5 sigma=3 rc=1 kT=1; constant force 0.02 +x; FP32, dt=0.01")
+# one force launch of the 200,000-particle DPD workload, from the ncu capture summarised in
+# profiles/force_kernel_dpd200k.md: DRAM read + write bytes, and warp instructions executed
+FORCE_TRAFFIC_BYTES = 17175296 + 393984
+FORCE_WARP_INSTRUCTIONS = 137756726
 # algorithmic FP32 operations per candidate pair and per interacting DPD pair
 # (counted from the reference's scalar pair loop and dpd_eval)
-FORCE_TRAFFIC_BYTES = 17182208 + 518656  # DRAM read + write of one force launch, 200,000-particle DPD
 F_CAND = 9
 F_INT_DPD = 40
 F_INT_TABLE = 44
@@ -487,6 +490,15 @@ def main():
             "achieved": state_bytes / (force_ms / 1e3) / 1e9,
             "frac": state_bytes / (force_ms / 1e3) / 1e9 / hbm_peak,
             "traffic_rate": (FORCE_TRAFFIC_BYTES / (force_ms / 1e3) / 1e9) if n == 200000 else None}
+    if n == 200000:
+        # the limiter the counters show: instruction issue (one warp instruction per scheduler
+        # per clock, four schedulers per SM)
+        issue_peak = sm_count * 4 * max_mhz * 1e6 / 1e9
+        issue = FORCE_WARP_INSTRUCTIONS / (force_ms / 1e3) / 1e9
+        roofline["issue_view"] = {
+            "warp_instructions_per_launch": FORCE_WARP_INSTRUCTIONS, "achieved": issue, "peak": issue_peak,
+            "unit": "G warp-instructions/s", "frac": issue / issue_peak,
+            "peak_source": f"{sm_count} SMs x 4 schedulers x {max_mhz:.0f} MHz (nominal issue rate)"}
 
     # ---- CPU baseline and accuracy (reference engine, rank 0, N=1 only) ----
     cpu = None
