@@ -644,52 +644,52 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 5) force_kernel(EngineVie
                         // ---- pass 1: each own particle against the region, kChunks steps of
                         // 32 candidates, then pass 2 on every full batch of 32 queued pairs
                         int qhead = 0, qtail = 0;
-                        for (int il = 0; il < ni; ++il) {
-                            const float4 xi = sm.own_x[il];
-                            const int i = i0 + il;
-                            const unsigned long long mk = sm.own_mask[il];
-                            unsigned hb[kChunks];
+                        // il == ni adds no candidates and flushes the queue: one call site of
+                        // eval_batch keeps the kernel's instruction footprint small
+                        for (int il = 0; il <= ni; ++il) {
+                            if (il < ni) {
+                                const float4 xi = sm.own_x[il];
+                                const int i = i0 + il;
+                                const unsigned long long mk = sm.own_mask[il];
+                                unsigned hb[kChunks];
 #pragma unroll
-                            for (int u = 0; u < kChunks; ++u) {
-                                hb[u] = 0u;
-                                if (u * 32 < M) {
-                                    const float dx = __fsub_rn(__fsub_rn(xi.x, rsx[u]), rbx[u]);
-                                    const float dy = __fsub_rn(__fsub_rn(xi.y, rsy[u]), rby[u]);
-                                    const float dz = __fsub_rn(__fsub_rn(xi.z, rsz[u]), rbz[u]);
-                                    const float r2 = dot3_rn(dx, dy, dz);
-                                    bool hit = (r2 <= rc2[u]) & (((mk >> rtj[u]) & 1ull) != 0ull) & (rself[u] != i);
-                                    if (prune && hit && rself[u] < 0) {
-                                        // runner_dopair's pruning: a pair (first, second) is evaluated
-                                        // only when key_second + dnshift - key_first < dmaxdist
-                                        // (runner_dopair.cpp:167-182)
-                                        const int jj = u * 32 + lane;
-                                        const int meta = __float_as_int(sm.nb_s[jj].w);
-                                        const int epk = __float_as_int(sm.ent_sh[(meta >> 2) & 31].w);
-                                        const int okey =
-                                            sort_key(xi.x, xi.y, xi.z, v.axes->n[(epk >> 2) & 15], sbias, sdscale);
-                                        hit = sm.nb_key[jj] + (epk >> 8) - okey < dmaxdist;
+                                for (int u = 0; u < kChunks; ++u) {
+                                    hb[u] = 0u;
+                                    if (u * 32 < M) {
+                                        const float dx = __fsub_rn(__fsub_rn(xi.x, rsx[u]), rbx[u]);
+                                        const float dy = __fsub_rn(__fsub_rn(xi.y, rsy[u]), rby[u]);
+                                        const float dz = __fsub_rn(__fsub_rn(xi.z, rsz[u]), rbz[u]);
+                                        const float r2 = dot3_rn(dx, dy, dz);
+                                        bool hit = (r2 <= rc2[u]) & (((mk >> rtj[u]) & 1ull) != 0ull) & (rself[u] != i);
+                                        if (prune && hit && rself[u] < 0) {
+                                            // runner_dopair's pruning: a pair (first, second) is evaluated
+                                            // only when key_second + dnshift - key_first < dmaxdist
+                                            // (runner_dopair.cpp:167-182)
+                                            const int jj = u * 32 + lane;
+                                            const int meta = __float_as_int(sm.nb_s[jj].w);
+                                            const int epk = __float_as_int(sm.ent_sh[(meta >> 2) & 31].w);
+                                            const int okey = sort_key(xi.x, xi.y, xi.z, v.axes->n[(epk >> 2) & 15],
+                                                                      sbias, sdscale);
+                                            hit = sm.nb_key[jj] + (epk >> 8) - okey < dmaxdist;
+                                        }
+                                        hb[u] = __ballot_sync(kFull, hit);
                                     }
-                                    hb[u] = __ballot_sync(kFull, hit);
+                                }
+#pragma unroll
+                                for (int u = 0; u < kChunks; ++u) {
+                                    if ((hb[u] >> lane) & 1u)
+                                        sm.queue[(qtail + __popc(hb[u] & lt_mask)) & (kQueue - 1)] =
+                                            (unsigned short)((il << 8) | (u * 32 + lane));
+                                    qtail += __popc(hb[u]);
                                 }
                             }
-#pragma unroll
-                            for (int u = 0; u < kChunks; ++u) {
-                                if ((hb[u] >> lane) & 1u)
-                                    sm.queue[(qtail + __popc(hb[u] & lt_mask)) & (kQueue - 1)] =
-                                        (unsigned short)((il << 8) | (u * 32 + lane));
-                                qtail += __popc(hb[u]);
-                            }
-                            while (qtail - qhead >= 32) {
+                            while (qtail - qhead >= 32 || (il == ni && qtail > qhead)) {
+                                const int nb = min(32, qtail - qhead);
                                 __syncwarp();
-                                eval_batch<kDPD, kMode>(v, sm, tinfo, qhead, 32, i0, start, pot_base, rng_mode,
-                                                        ecell, npair, vir);
-                                qhead += 32;
+                                eval_batch<kDPD, kMode>(v, sm, tinfo, qhead, nb, i0, start, pot_base, rng_mode, ecell,
+                                                        npair, vir);
+                                qhead += nb;
                             }
-                        }
-                        if (qtail > qhead) {
-                            __syncwarp();
-                            eval_batch<kDPD, kMode>(v, sm, tinfo, qhead, qtail - qhead, i0, start, pot_base,
-                                                    rng_mode, ecell, npair, vir);
                         }
                         __syncwarp();
                         // ---- neighbour-side sums of FIRST entries into their planes
