@@ -39,8 +39,8 @@ WORKLOAD = ("DPD fluid with body force: 200,000 particles, 40x20x20 box, periodi
             "DPD a=25 gamma=4.5 sigma=3 rc=1 kT=1; constant force 0.02 +x; FP32, dt=0.01")
 # one force launch of the 200,000-particle DPD workload, from the ncu capture summarised in
 # profiles/force_kernel_dpd200k.md: DRAM read + write bytes, and warp instructions executed
-FORCE_TRAFFIC_BYTES = 17175296 + 393984
-FORCE_WARP_INSTRUCTIONS = 137756726
+FORCE_TRAFFIC_BYTES = 17170688 + 1504768
+FORCE_WARP_INSTRUCTIONS = 137576112
 # algorithmic FP32 operations per candidate pair and per interacting DPD pair
 # (counted from the reference's scalar pair loop and dpd_eval)
 F_CAND = 9
@@ -449,18 +449,14 @@ def main():
     e2e = job_rate(world, n, Ke, ms_e2e)
 
     # ---- roofline of the dominant kernel (nonbonded forces) ----
+    # the force kernel alone, per launch, L2 flushed before each launch; the median
     R = 50
-    fs = [torch.cuda.Event(enable_timing=True) for _ in range(R)]
-    fe = [torch.cuda.Event(enable_timing=True) for _ in range(R)]
+    per = np.zeros(R)
     barrier()
-    with torch.cuda.stream(stream):
-        for k in range(R):
-            flush.zero_()
-            fs[k].record(stream)
-            L.mxg_engine_force(e)
-            fe[k].record(stream)
+    check(L.mxg_engine_time_force_launches(e, R, ctypes.c_void_p(flush.data_ptr()), flush.numel(),
+                                           per.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "time_force")
     barrier()
-    force_ms = sum(a.elapsed_time(b) for a, b in zip(fs, fe)) / R
+    force_ms = float(np.median(per))
     flops = F_CAND * cand.value + F_INT_DPD * inter.value
     peaks = measured_peaks()
     sm_count = torch.cuda.get_device_properties(dev).multi_processor_count

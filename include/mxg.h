@@ -385,12 +385,13 @@ int mxg_engine_clear_status(mxg_engine *e);
  * mean CUDA-event duration of one launch in milliseconds (state is not advanced). */
 int mxg_engine_time_force(mxg_engine *e, int reps, double *ms);
 
-/* ---- timing of the engine's own kernels (for roofline reporting) ---- */
-/* Enables per-kernel CUDA-event timing on the engine stream (off by default). */
-int mxg_engine_enable_timing(mxg_engine *e, int on);
-/* Accumulated milliseconds and launch counts for kernels: 0 force, 1 bonds, 2 integrate, 3 scan,
- * 4 scatter. */
-int mxg_engine_kernel_times(mxg_engine *e, double *ms, long long *launches, int nkernels);
+/* ---- timing of the force kernel (for roofline reporting) ---- */
+/* reps launches of the nonbonded force kernel alone (with the occupancy ordering when the engine
+ * uses it), each between its own pair of CUDA events on the engine stream, flush_bytes of device
+ * memory at flush (may be NULL with 0 bytes) zeroed before every launch outside the events so that
+ * each launch starts with a cold L2; ms[r] receives launch r's milliseconds. The forces of the
+ * state are recomputed in full afterwards; the state is not advanced. */
+int mxg_engine_time_force_launches(mxg_engine *e, int reps, void *flush, size_t flush_bytes, double *ms);
 /* Pair statistics for the last force evaluation: candidate and interacting pair counts as the
  * reference's task list defines them (counted on the device when enabled). */
 int mxg_engine_pair_counts(mxg_engine *e, long long *candidates, long long *interacting);

@@ -110,9 +110,8 @@ _SIGS = {
     "mxg_engine_copy_state": ([_vp, _vp, _vp, ctypes.c_int], ctypes.c_int),
     "mxg_engine_energy_async": ([_vp, _c_double_p], ctypes.c_int),
     "mxg_engine_finalize": ([_vp], ctypes.c_int),
-    "mxg_engine_enable_timing": ([_vp, ctypes.c_int], ctypes.c_int),
     "mxg_engine_time_force": ([_vp, ctypes.c_int, _c_double_p], ctypes.c_int),
-    "mxg_engine_kernel_times": ([_vp, _c_double_p, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int], ctypes.c_int),
+    "mxg_engine_time_force_launches": ([_vp, ctypes.c_int, _vp, ctypes.c_size_t, _c_double_p], ctypes.c_int),
     "mxg_engine_pair_counts": ([_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)],
                                ctypes.c_int),
     "mxg_engine_add_replica": ([_vp, _c_double_p, _c_double_p, _c_int_p, _c_int_p, _c_float_p, _c_float_p],

@@ -216,6 +216,7 @@ struct EngineView {      // everything a kernel needs, passed by value
     const int4 *items;       // force work items: (cell, first entry, end entry, part)
     int *item_ctr;           // [0] next work item, [1] warps done (dynamic fetch; zero between launches)
     int *item_order;         // items by decreasing cell occupancy (split cells only), else null
+    int dpd_pure;            // every pair potential is DPD with the reference's random term: DPD-only kernel
     int nitems;
 };
 

@@ -390,6 +390,7 @@ struct mxg_engine {
     int *d_item_ctr = nullptr;          // the force kernel's work-item counter and finished-warp count
     int *d_item_order = nullptr;        // work items, most crowded cells first (when cells are split)
     bool order_items = false;
+    bool dpd_pure = false;              // every pair potential DPD, no summed second term, no Philox
     int *d_cell_planes = nullptr;       // planes summed into each cell's forces
     int nitems = 0;
     DevPot *d_pots = nullptr;
@@ -609,6 +610,7 @@ struct mxg_engine {
         v.items = d_items;
         v.item_ctr = d_item_ctr;
         v.item_order = order_items ? d_item_order : nullptr;
+        v.dpd_pure = dpd_pure ? 1 : 0;
         v.nitems = nitems;
         v.planes = d_planes;
         v.body_e = (has_walls || nlarge) ? d_body_e : nullptr;
@@ -1021,6 +1023,11 @@ int mxg_engine::start(cudaStream_t st) {
                 hpidx[k] = -1;  // large particles take no part in the cell-pair loop
                 hpidx2[k] = -1;
             }
+    dpd_pure = has_dpd && rng_mode == 0;
+    for (int k : hpidx)
+        if (k >= 0 && pots[k].kind != kKindDPD) dpd_pure = false;
+    for (int k : hpidx2)
+        if (k >= 0) dpd_pure = false;
     has_sb = false;
     has_walls = false;
     std::vector<DevType> ht(ntypes);
@@ -2246,12 +2253,6 @@ int mxg_engine_finalize(mxg_engine *e) {
     return MXG_OK;
 }
 
-int mxg_engine_enable_timing(mxg_engine *e, int on) {
-    if (!e) return MXG_ERR_NULL;
-    (void)on;
-    return MXG_OK;
-}
-
 /* Launches the force kernel reps times on the engine stream between two events
  * and returns the mean duration in milliseconds. */
 int mxg_engine_time_force(mxg_engine *e, int reps, double *ms) {
@@ -2272,6 +2273,35 @@ int mxg_engine_time_force(mxg_engine *e, int reps, double *ms) {
     cudaEventDestroy(b);
     *ms = t / std::max(1, reps);
     return MXG_OK;
+}
+
+int mxg_engine_time_force_launches(mxg_engine *e, int reps, void *flush, size_t flush_bytes, double *ms) {
+    if (!e || !ms) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    if (reps < 1 || (flush_bytes > 0 && !flush)) return MXG_ERR_ARG;
+    std::vector<cudaEvent_t> ev(2 * (size_t)reps, nullptr);
+    cudaError_t err = cudaSuccess;
+    for (auto &x : ev)
+        if (err == cudaSuccess) err = cudaEventCreate(&x);
+    const EngineView v = e->view(e->cur);
+    for (int r = 0; r < reps && err == cudaSuccess; ++r) {
+        if (flush_bytes > 0) err = cudaMemsetAsync(flush, 0, flush_bytes, e->stream);
+        if (err == cudaSuccess) err = cudaEventRecord(ev[2 * r], e->stream);
+        if (err == cudaSuccess) launch_force(v, e->has_dpd, e->force_grid, false, e->stream);
+        if (err == cudaSuccess) err = cudaEventRecord(ev[2 * r + 1], e->stream);
+    }
+    if (err == cudaSuccess) {
+        e->enqueue_force(e->cur);  // the complete forces of the state, as engine_force leaves them
+        err = cudaStreamSynchronize(e->stream);
+    }
+    for (int r = 0; r < reps && err == cudaSuccess; ++r) {
+        float t = 0.f;
+        err = cudaEventElapsedTime(&t, ev[2 * r], ev[2 * r + 1]);
+        ms[r] = t;
+    }
+    for (auto &x : ev)
+        if (x) cudaEventDestroy(x);
+    return err == cudaSuccess ? MXG_OK : MXG_ERR_CUDA;
 }
 
 /* A small autotuner for the force kernel's grid: candidate CTAs per SM are
@@ -2311,15 +2341,6 @@ int mxg_engine_autotune(mxg_engine *e) {
     e->force_grid = best;
     const int rc = e->build_graphs();
     return rc != MXG_OK ? rc : best_per_sm;
-}
-
-int mxg_engine_kernel_times(mxg_engine *e, double *ms, long long *launches, int nkernels) {
-    if (!e) return MXG_ERR_NULL;
-    for (int k = 0; k < nkernels; ++k) {
-        if (ms) ms[k] = 0.0;
-        if (launches) launches[k] = 0;
-    }
-    return MXG_OK;
 }
 
 int mxg_engine_pair_counts(mxg_engine *e, long long *candidates, long long *interacting) {

@@ -109,7 +109,9 @@ __global__ void sort_bounds_kernel(EngineView v) {
  * its exact negation for a self pair whose first particle is j): r2 and the
  * per-pair force are bit-identical to the reference's.
  */
-template <bool kDPD>
+// kPure: every pair potential is DPD and the random term is the reference's (no Philox):
+// the table and Philox code is left out of the kernel (a smaller instruction footprint)
+template <bool kDPD, bool kPure = false>
 __device__ __forceinline__ void pair_contribution(const EngineView &v, const DevPot &p, int role, bool i_first,
                                                   float dx, float dy, float dz, float r2, float radi, float radj,
                                                   const float4 &vi, const float4 &vj, unsigned rng_mode,
@@ -117,7 +119,7 @@ __device__ __forceinline__ void pair_contribution(const EngineView &v, const Dev
     cx = cy = cz = 0.f;
     pe = 0.f;
     counted = false;
-    if (kDPD && p.kind == 1) {
+    if (kDPD && (kPure || p.kind == 1)) {
         // dpd_eval (dpd_eval.hpp:21-69), in the reference's orientation
         const float r_first = i_first ? radi : radj;
         const float r_second = i_first ? radj : radi;
@@ -143,7 +145,7 @@ __device__ __forceinline__ void pair_contribution(const EngineView &v, const Dev
         const float ev = __fadd_rn(__fadd_rn(__fmul_rn(ex, wx), __fmul_rn(ey, wy)), __fmul_rn(ez, wz));
         const float fd = __fmul_rn(__fmul_rn(-p.dpd_gamma, od), ev);
         float fr = __fmul_rn(__fmul_rn(p.dpd_sigma, oc), p.dpd_delta);
-        if (rng_mode) {
+        if (!kPure && rng_mode) {
             const unsigned idi = __float_as_uint(vi.w), idj = __float_as_uint(vj.w);
             fr = fr * philox_pair_xi(*v.step, idi < idj ? idi : idj, idi < idj ? idj : idi);
         }
@@ -154,7 +156,7 @@ __device__ __forceinline__ void pair_contribution(const EngineView &v, const Dev
         cy = sg * __fmul_rn(f, ey);
         cz = sg * __fmul_rn(f, ez);
         counted = i_first;
-    } else {
+    } else if (!kPure) {
         float e, f;
         if (!table_eval_ex(p, v.coef, i_first ? radi : radj, i_first ? radj : radi, r2, e, f)) return;
         // first particle gets -f dx, second +f dx
@@ -307,7 +309,7 @@ struct ForceSmem {
  * lane; own-side segmented sums into own_f, neighbour-side sums into nb_f.
  * kMode 1 counts the pairs (once each), kMode 2 sums the pair virial
  * (x_first - x_second) (x) F_first in FP64 (xx, yy, zz, xy, xz, yz). */
-template <bool kDPD, int kMode>
+template <bool kDPD, int kMode, bool kPure = false>
 __device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD> &sm, const float4 *tinfo, int qhead,
                                            int nb, int i0, int own_start, int pot_base, unsigned rng_mode,
                                            double &ecell, unsigned long long &npair, double *vir) {
@@ -361,11 +363,11 @@ __device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD> 
         const float4 vj = kDPD ? sm.nb_v[jj] : make_float4(0.f, 0.f, 0.f, 0.f);
         float pe;
         bool counted;
-        pair_contribution<kDPD>(v, p, role, i_first, dx, dy, dz, r2, tinfo[ti].w, tinfo[tj].w, vi, vj, rng_mode,
+        pair_contribution<kDPD, kPure>(v, p, role, i_first, dx, dy, dz, r2, tinfo[ti].w, tinfo[tj].w, vi, vj, rng_mode,
                                 cx, cy, cz, pe, counted);
         ecell += (double)pe;
         if (kMode == 1 && counted) ++npair;
-        if (v.pot_idx2) {
+        if (!kPure && v.pot_idx2) {
             // a second potential summed on the same pair (a table potential plus a DPD
             // thermostat), evaluated on the pair's own displacement
             const int q2 = v.pot_idx2[pot_base + ti * v.ntypes + tj];
@@ -447,7 +449,7 @@ constexpr size_t force_smem_bytes() {
     return sizeof(ForceSmem<kDPD>) * kWarpsPerBlock;
 }
 
-template <bool kDPD, int kMode>
+template <bool kDPD, int kMode, bool kPure = false>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 5) force_kernel(EngineView v) {
     unsigned long long npair = 0;  // interacting pairs counted once (statistics launch only)
     double vir[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // pair virial (virial launch only)
@@ -686,7 +688,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 5) force_kernel(EngineVie
                             while (qtail - qhead >= 32 || (il == ni && qtail > qhead)) {
                                 const int nb = min(32, qtail - qhead);
                                 __syncwarp();
-                                eval_batch<kDPD, kMode>(v, sm, tinfo, qhead, nb, i0, start, pot_base, rng_mode, ecell,
+                                eval_batch<kDPD, kMode, kPure>(v, sm, tinfo, qhead, nb, i0, start, pot_base, rng_mode, ecell,
                                                         npair, vir);
                                 qhead += nb;
                             }
@@ -1757,11 +1759,11 @@ __global__ void reduce_final_kernel(int nblocks, const double *partials, double 
 /* launchers                                                                 */
 /* ------------------------------------------------------------------------ */
 
-template <bool kDPD, int kMode>
+template <bool kDPD, int kMode, bool kPure = false>
 void configure_one() {
     const int bytes = (int)force_smem_bytes<kDPD>();
-    cudaFuncSetAttribute(force_kernel<kDPD, kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    cudaFuncSetAttribute(force_kernel<kDPD, kMode>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    cudaFuncSetAttribute(force_kernel<kDPD, kMode, kPure>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(force_kernel<kDPD, kMode, kPure>, cudaFuncAttributePreferredSharedMemoryCarveout,
                          cudaSharedmemCarveoutMaxShared);
 }
 
@@ -1769,6 +1771,7 @@ void configure_force_kernels() {
     // the force kernel's occupancy is bounded by shared memory: allow its dynamic
     // shared memory and ask for the largest carveout of the unified L1/shared storage
     configure_one<true, 0>();
+    configure_one<true, 0, true>();
     configure_one<true, 1>();
     configure_one<true, 2>();
     configure_one<false, 0>();
@@ -1787,6 +1790,8 @@ void launch_force_mode(const EngineView &v, int grid, cudaStream_t st) {
         force_kernel<kDPD, 1><<<grid, kWarpsPerBlock * 32, bytes, st>>>(v);
     else if (v.virial_partials)
         force_kernel<kDPD, 2><<<grid, kWarpsPerBlock * 32, bytes, st>>>(v);
+    else if (kDPD && v.dpd_pure)
+        force_kernel<true, 0, true><<<grid, kWarpsPerBlock * 32, force_smem_bytes<true>(), st>>>(v);
     else
         force_kernel<kDPD, 0><<<grid, kWarpsPerBlock * 32, bytes, st>>>(v);
 }
