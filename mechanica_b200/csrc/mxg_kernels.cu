@@ -83,7 +83,8 @@ __global__ void sort_bounds_kernel(EngineView v) {
 /* ------------------------------------------------------------------------ */
 
 /*
- * One warp per cell (grid-stride). Every cell pair is evaluated once, by the
+ * One warp per work item (a cell with a group of its entries; warps take items
+ * from a device counter). Every cell pair is evaluated once, by the
  * cell that is FIRST in the reference's flipped pair (runner_dopair.cpp:91-340);
  * the cell's own pairs (runner_doself, :446-682) are evaluated from both sides.
  * The warp stages up to kOwn of the cell's particles and then, region by
