@@ -914,17 +914,21 @@ int mxg_engine::start(cudaStream_t st) {
     if (smax > 0 && spec_host.size() != (size_t)nparts * smax) spec_host.resize((size_t)nparts * smax, 0.0f);
 
     // ---- work items: each cell's SELF and FIRST entries split into up to `parts`
-    // groups (one warp each) when there are too few cells for about three waves of
-    // items (warps fetch items from a counter, so finer items shorten the tail that the
-    // most crowded cells leave). Item k > 0 of a cell sums its own-side forces into
-    // plane sec_count + k - 1 of the cell.
+    // groups (one warp each) when there are too few cells to fill the GPU. Crowded cells
+    // (mean occupancy 16 or more) aim at about three waves of items: their items are long
+    // and uneven, and warps fetch items from a counter, so finer items shorten the tail
+    // that the most crowded cells leave. Sparse cells aim at one wave of resident warps
+    // (5 blocks of kWarpsPerBlock per SM): their items are short and each split adds a
+    // staging of the cell's own particles. Item k > 0 of a cell sums its own-side forces
+    // into plane sec_count + k - 1 of the cell.
     {
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         num_sms = sms;
     }
-    const int want_warps = num_sms * 64;
+    const bool crowded = (long long)nparts >= 16LL * std::max(1, ncells);
+    const int want_warps = num_sms * (crowded ? 64 : 5 * kWarpsPerBlock);
     const int parts = std::max(1, std::min(kMaxCellParts, (want_warps + ncells - 1) / std::max(1, ncells)));
     std::vector<int> nb_off(ncells + 1, 0), nb_cell, nb_rev, hplanes(ncells, 0);
     std::vector<float4> nb_shift;
@@ -968,7 +972,7 @@ int mxg_engine::start(cudaStream_t st) {
     // most crowded cells' items, so they are handed out first (reordered before every force
     // pass). With sparse cells (mean occupancy below 16) the items are short and the
     // ordering launch costs more than the tail it removes.
-    order_items = parts > 1 && (long long)nparts >= 16LL * ncells && nitems <= kOrderMaxItems;
+    order_items = parts > 1 && crowded && nitems <= kOrderMaxItems;
     nplanes = 0;
     for (int c = 0; c < ncells; ++c) nplanes = std::max(nplanes, hplanes[c]);
 
