@@ -25,3 +25,21 @@ def test_timed_steps_match_plain_steps():
         assert t[k] > 0.0, (k, t)
     parts = t["prepare"] + t["nonbond"] + t["bonded"] + t["advance"] + t["shuffle"]
     assert parts <= t["step"] * 1.0001 + 1e-6
+
+
+def test_force_launch_timing_leaves_the_forces_of_a_force_pass():
+    """mxg_engine_time_force_launches times launches of the force kernel alone and then
+    recomputes the forces in full: the state's forces are bit-identical to those of a
+    plain force pass, and every launch reports a positive duration."""
+    import ctypes
+    from mechanica_b200._native import check, lib
+    z, scn = load("dpd_small")
+    u = S.build_gpu(scn)
+    u.force()
+    f0 = np.ascontiguousarray(u.state()[2], dtype=np.float32).copy()
+    ms = np.zeros(3)
+    check(lib().mxg_engine_time_force_launches(u._e, 3, None, 0, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+          "time_force_launches")
+    assert np.all(ms > 0.0), ms
+    f1 = np.ascontiguousarray(u.state()[2], dtype=np.float32)
+    assert np.array_equal(f0.view(np.uint32), f1.view(np.uint32))
