@@ -11,10 +11,12 @@ pair forces by brute force over minimum-image pairs within the cutoff, with
   - the DPD force of dpd_eval.hpp:21-69 with the random term times a Philox
     draw xi keyed on (step, lower id, higher id), the stream the engine's
     Philox mode uses (Philox4x32-10, Salmon et al., SC'11),
-as a sum of two terms per type pair; forward Euler with the speed clamp of
-engine_advance.cpp:164-173; and the Gaussian-smoothed A-B radial distribution
-loss. Central finite differences of this model, with tables re-fitted on their
-frozen nodes at theta +- h, are the reference gradient.
+as a sum of two terms per type pair; bonds with bond_eval's table semantics
+(bond.cpp:99-312: length clamp, break test on f = V'(r)/r); forward Euler with
+the speed clamp of engine_advance.cpp:164-173 or its overdamped form with the
+step clamp (:174-182); and the Gaussian-smoothed A-B radial distribution loss.
+Central finite differences of this model, with tables re-fitted on their frozen
+nodes at theta +- h, are the reference gradient.
 """
 import numpy as np
 
@@ -82,6 +84,46 @@ class Table:
             ee = ee * x + c[:, k]
         return np.where(ok, eff * c[:, 1] / ro, 0.0)
 
+    def bond_force_over_r(self, r):
+        """potential_eval semantics of a bond (bond.cpp:174-178, potential_eval.hpp:67-104):
+        the length clamped to [a, b], no radius shift, the interval index clamped to n;
+        returns f with F_i = -f (x_i - x_j)."""
+        rc = np.clip(r, self.a, self.b)
+        t = self.alpha[0] + rc * (self.alpha[1] + rc * self.alpha[2])
+        ind = np.minimum(np.maximum(0.0, t).astype(np.int64), self.n)
+        c = self.c[ind]
+        x = (rc - c[:, 0]) * c[:, 1]
+        ee = c[:, 2] * x + c[:, 3]
+        eff = c[:, 2].copy()
+        for k in range(4, 8):
+            eff = eff * x + ee
+            ee = ee * x + c[:, k]
+        return eff * c[:, 1] / rc
+
+
+class Bonds:
+    """Harmonic/table bonds (i[k], j[k]) with one table, per-bond dissociation energies
+    and active flags; a bond whose f = V'(r)/r reaches its dissociation energy is
+    destroyed before it acts (bond.cpp:227-242), and stays destroyed."""
+
+    def __init__(self, i, j, table, dissociation, active=None):
+        self.i, self.j = np.asarray(i, dtype=np.int64), np.asarray(j, dtype=np.int64)
+        self.table = table
+        self.dissociation = np.broadcast_to(np.asarray(dissociation, dtype=np.float64), self.i.shape)
+        self.active = np.ones(len(self.i), dtype=bool) if active is None else np.asarray(active, dtype=bool).copy()
+
+    def forces(self, x, box):
+        d = x[self.i] - x[self.j]
+        d -= box * np.rint(d / box)
+        r = np.sqrt((d * d).sum(1))
+        f = self.table.bond_force_over_r(r)
+        self.active &= ~(f >= self.dissociation)
+        fi = np.where(self.active[:, None], -f[:, None] * d, 0.0)
+        out = np.zeros_like(x)
+        np.add.at(out, self.i, fi)
+        np.add.at(out, self.j, -fi)
+        return out
+
 
 class Dpd:
     def __init__(self, alpha, gamma, sigma, cutoff, delta):
@@ -125,9 +167,11 @@ def forces(x, v, types, ids, box, radius, terms, cutoff, step, philox=True):
     return f
 
 
-def run(x0, v0, types, ids, box, mass, radius, terms, cutoff, dt, nsteps, step0, maxv, philox=True, body=None):
-    """FP64 forward Euler (engine_advance.cpp:164-173); returns the final positions
-    (unwrapped: minimum image is applied inside the force pass)."""
+def run(x0, v0, types, ids, box, mass, radius, terms, cutoff, dt, nsteps, step0, maxv, philox=True, body=None,
+        bonds=None, overdamped=False, maxx=None):
+    """FP64 forward Euler (engine_advance.cpp:164-182); returns the final positions
+    (unwrapped: minimum image is applied inside the force pass). bonds: a Bonds set
+    (its flags change as bonds break). overdamped: x += clamp(dt f imass, maxx)."""
     x = np.array(x0, dtype=np.float64)
     v = np.array(v0, dtype=np.float64)
     imass = 1.0 / mass[types]
@@ -135,6 +179,11 @@ def run(x0, v0, types, ids, box, mass, radius, terms, cutoff, dt, nsteps, step0,
         f = forces(x, v, types, ids, box, radius, terms, cutoff, step0 + s, philox)
         if body is not None:
             f = f + body[types]
+        if bonds is not None:
+            f = f + bonds.forces(x, box)
+        if overdamped:
+            x = x + np.clip(dt * f * imass[:, None], -maxx, maxx)
+            continue
         v = v + dt * f * imass[:, None]
         v = np.clip(v, -maxv, maxv)
         x = x + dt * v

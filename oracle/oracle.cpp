@@ -68,9 +68,13 @@ struct Pot {
     T dpd_alpha, dpd_gamma, dpd_sigma, dpd_delta;
 };
 
-/* potential_eval_ex in type T; coefficients widened from float */
+/* potential_eval_ex in type T; coefficients widened from float. Its integer
+ * decisions (the range test and the interval index) are taken as the FP32 code
+ * takes them, from the pair's FP32 r2f (equal to r2 when T is float): they are
+ * part of the tabulated model, and an FP64 decision flips pairs that lie on a
+ * table edge (a lattice's second neighbours sit on the lattice's Morse edge). */
 template <typename T>
-bool table_eval_ex(const Pot<T> &p, T ri, T rj, T r2, T &e, T &f) {
+bool table_eval_ex(const Pot<T> &p, T ri, T rj, T r2, float r2f, T &e, T &f) {
     const T eps = (T)FLT_EPSILON;
     T r = std::sqrt(r2);
     const T ro = r < eps ? eps : r;
@@ -79,9 +83,16 @@ bool table_eval_ex(const Pot<T> &p, T ri, T rj, T r2, T &e, T &f) {
         r = r / (ri + rj);
     else if (p.flags & (1u << 12))
         r = r - (ri + rj) + p.r0p1;
-    const T t = p.alpha[0] + r * (p.alpha[1] + r * p.alpha[2]);
-    const unsigned ind = (unsigned)std::max((T)0, t);
-    if (r > p.b || ind > (unsigned)p.n) return false;
+    float rf = std::sqrt(r2f);
+    const float af = (float)p.a;
+    rf = rf < af ? af : rf;
+    if (p.flags & (1u << 11))
+        rf = rf / ((float)ri + (float)rj);
+    else if (p.flags & (1u << 12))
+        rf = rf - ((float)ri + (float)rj) + (float)p.r0p1;
+    const float t = (float)p.alpha[0] + rf * ((float)p.alpha[1] + rf * (float)p.alpha[2]);
+    const unsigned ind = (unsigned)std::max(0.0f, t);
+    if (rf > (float)p.b || ind > (unsigned)p.n) return false;
     const float *c = p.c + ind * 8;
     const T x = (r - (T)c[0]) * (T)c[1];
     T ee = (T)c[2] * x + (T)c[3];
@@ -105,6 +116,7 @@ struct Setup {
     const double *origin;
     double dim[3];
     T cut2_pair, cut2_self;
+    float cut2f_pair, cut2f_self;  // the FP32 cutoff tests (float(cutoff)^2; float(cutoff^2))
     int ntypes;
     std::vector<T> radius;
     const int *pot_of_pair;
@@ -118,9 +130,10 @@ struct Setup {
     float axes[13][3];
 };
 
+/* r2f: the pair's r2 in the reference's FP32 arithmetic, for its integer decisions */
 template <typename T>
-void pair_force(const Setup<T> &S, int pi, int pj, const T *dx_in, T r2, std::vector<T> &f, double &epot,
-                long long &nint, long long &nrand, double *vir) {
+void pair_force(const Setup<T> &S, int pi, int pj, const T *dx_in, T r2, float r2f, std::vector<T> &f,
+                double &epot, long long &nint, long long &nrand, double *vir) {
     const int ti = S.type[pi], tj = S.type[pj];
     const int pidx = S.pot_of_pair[ti * S.ntypes + tj];
     const int didx = S.dpd_of_pair ? S.dpd_of_pair[ti * S.ntypes + tj] : -1;
@@ -128,7 +141,7 @@ void pair_force(const Setup<T> &S, int pi, int pj, const T *dx_in, T r2, std::ve
         const int idx = which == 0 ? pidx : didx;
         if (idx < 0) continue;
         const Pot<T> &p = S.pots[idx];
-        if (r2 < p.a * p.a) {
+        if (r2f < (float)p.a * (float)p.a) {
             ++nrand;
             continue;
         }
@@ -137,7 +150,8 @@ void pair_force(const Setup<T> &S, int pi, int pj, const T *dx_in, T r2, std::ve
             const T ri = S.radius[ti], rj = S.radius[tj];
             const bool shifted = p.flags & (1u << 12);
             const T cutoff = shifted ? (p.b + ri + rj) : p.b;
-            if (r2 > cutoff * cutoff) continue;
+            const float cutf = shifted ? ((float)p.b + (float)ri) + (float)rj : (float)p.b;
+            if (r2f > cutf * cutf) continue;
             const T r = std::sqrt(r2);
             const T e[3] = {dx[0] / r, dx[1] / r, dx[2] / r};
             const T w[3] = {S.v[3 * pi] - S.v[3 * pj], S.v[3 * pi + 1] - S.v[3 * pj + 1], S.v[3 * pi + 2] - S.v[3 * pj + 2]};
@@ -158,7 +172,7 @@ void pair_force(const Setup<T> &S, int pi, int pj, const T *dx_in, T r2, std::ve
             ++nint;
         } else {
             T ee, ff;
-            if (!table_eval_ex(p, S.radius[ti], S.radius[tj], r2, ee, ff)) continue;
+            if (!table_eval_ex(p, S.radius[ti], S.radius[tj], r2, r2f, ee, ff)) continue;
             for (int k = 0; k < 3; ++k) {
                 const T wk = ff * dx[k];
                 f[3 * pi + k] -= wk;
@@ -194,11 +208,16 @@ int run(const Setup<T> &S, const int *tasks, int ntasks, double *f_out, double *
                 for (size_t b = a + 1; b < mem.size(); ++b) {
                     const int pi = mem[a], pj = mem[b];
                     T dx[3];
-                    for (int k = 0; k < 3; ++k) dx[k] = S.x[3 * pi + k] - S.x[3 * pj + k];
+                    float dxf[3];
+                    for (int k = 0; k < 3; ++k) {
+                        dx[k] = S.x[3 * pi + k] - S.x[3 * pj + k];
+                        dxf[k] = S.xf[3 * pi + k] - S.xf[3 * pj + k];
+                    }
                     const T r2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
+                    const float r2f = dxf[0] * dxf[0] + dxf[1] * dxf[1] + dxf[2] * dxf[2];
                     ++ncand;
-                    if (r2 > S.cut2_self) continue;
-                    pair_force(S, pi, pj, dx, r2, f, epot, nint, nrand, vir);
+                    if (r2f > S.cut2f_self) continue;
+                    pair_force(S, pi, pj, dx, r2, r2f, f, epot, nint, nrand, vir);
                 }
         } else if (type == 2) {  // pair, shift and flip as space_getsid
             int ci = ci0, cj = cj0;
@@ -256,14 +275,17 @@ int run(const Setup<T> &S, const int *tasks, int ntasks, double *f_out, double *
                         continue;
                     }
                     T pix[3], dx[3];
+                    float dxf[3];
                     for (int k = 0; k < 3; ++k) {
                         pix[k] = S.x[3 * pi + k] - shift[k];
                         dx[k] = pix[k] - S.x[3 * pj + k];
+                        dxf[k] = (S.xf[3 * pi + k] - fshift[k]) - S.xf[3 * pj + k];
                     }
                     const T r2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
+                    const float r2f = dxf[0] * dxf[0] + dxf[1] * dxf[1] + dxf[2] * dxf[2];
                     ++ncand;
-                    if (r2 > S.cut2_pair) continue;
-                    pair_force(S, pi, pj, dx, r2, f, epot, nint, nrand, vir);
+                    if (r2f > S.cut2f_pair) continue;
+                    pair_force(S, pi, pj, dx, r2, r2f, f, epot, nint, nrand, vir);
                 }
         }
     }
@@ -293,6 +315,8 @@ int build_and_run(const OrcInput *in, double *f_out, double *epot_out, long long
     S.origin = in->cell_origin;
     for (int k = 0; k < 3; ++k) S.dim[k] = in->dim[k];
     const float cf = (float)in->cutoff;
+    S.cut2f_pair = cf * cf;
+    S.cut2f_self = (float)(in->cutoff * in->cutoff);
     if (sizeof(T) == sizeof(float)) {
         S.cut2_pair = (T)(cf * cf);
         S.cut2_self = (T)(float)(in->cutoff * in->cutoff);

@@ -47,6 +47,11 @@
 #include "MxForce.h"
 #include "../../rendering/NOMStyle.hpp"
 #include <vector>
+#include <cstring>
+#include <limits>
+#include <algorithm>
+#include <cmath>
+#include "MxCuboid.hpp"
 
 extern PyTypeObject MxConstantForce_Type;
 extern PyTypeObject MxAngle_Type;
@@ -439,6 +444,64 @@ int mxref_get_state(int n, float *xrel, double *xabs, float *v, float *f, int *c
             v[3 * id + k] = p->v[k];
             f[3 * id + k] = p->f[k];
         }
+    }
+    return 0;
+}
+
+/* Adds a static cuboid the way cuboid_init does (MxCuboid.cpp:40-76; that file is not
+ * compiled here): the orientation qx qy qz from Quaternion::rotation's formula
+ * (axis sin(a/2), cos(a/2)), its inverse as conjugated() / dot(), the bounding box as
+ * MxCuboid_UpdateAABB forms it (its upper bound starting at the smallest positive float);
+ * then the reference's own engine_addcuboid. */
+int mxref_add_cuboid(const float *pos, const float *size, const float *angles) {
+    MxCuboid c;
+    memset((void *)&c, 0, sizeof(c));
+    c.position = Magnum::Vector3(pos[0], pos[1], pos[2]);
+    c.size = Magnum::Vector3(size[0], size[1], size[2]);
+    const Magnum::Vector3 axes[3] = {Magnum::Vector3::xAxis(), Magnum::Vector3::yAxis(), Magnum::Vector3::zAxis()};
+    Magnum::Quaternion q[3];
+    for (int k = 0; k < 3; ++k) {
+        const float half = angles[k] / 2;
+        q[k] = Magnum::Quaternion(axes[k] * std::sin(half), std::cos(half));
+    }
+    c.orientation = q[0] * q[1] * q[2];
+    const float dot = Magnum::Math::dot(c.orientation.vector(), c.orientation.vector()) +
+                      c.orientation.scalar() * c.orientation.scalar();
+    c.inv_orientation = Magnum::Quaternion(-c.orientation.vector() / dot, c.orientation.scalar() / dot);
+    Magnum::Vector3 mn = Magnum::Vector3(std::numeric_limits<float>::max());
+    Magnum::Vector3 mx = Magnum::Vector3(std::numeric_limits<float>::min());
+    const Magnum::Vector3 h = 0.5 * c.size;
+    const Magnum::Vector3 pts[8] = {
+        c.orientation.transformVector({h[0], h[1], h[2]}) + c.position,
+        c.orientation.transformVector({h[0], -h[1], h[2]}) + c.position,
+        c.orientation.transformVector({-h[0], -h[1], h[2]}) + c.position,
+        c.orientation.transformVector({-h[0], h[1], h[2]}) + c.position,
+        c.orientation.transformVector({h[0], h[1], -h[2]}) + c.position,
+        c.orientation.transformVector({h[0], -h[1], -h[2]}) + c.position,
+        c.orientation.transformVector({-h[0], -h[1], -h[2]}) + c.position,
+        c.orientation.transformVector({-h[0], h[1], -h[2]}) + c.position,
+    };
+    for (int i = 0; i < 8; ++i)
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = std::min(mn[k], pts[i][k]);
+            mx[k] = std::max(mx[k], pts[i][k]);
+        }
+    c.aabb._min = mn;
+    c.aabb._max = mx;
+    MxCuboid *res = NULL;
+    return engine_addcuboid(&_Engine, &c, &res);
+}
+
+int mxref_bind_cuboid(void *pot, int type) {
+    return engine_add_cuboid_potential(&_Engine, (MxPotential *)pot, type);
+}
+
+/* Per-id number density f[3] (MxParticle::number_density) of the last force pass. */
+int mxref_number_density(int n, float *out) {
+    space *s = &_Engine.s;
+    for (int id = 0; id < n; ++id) {
+        MxParticle *p = id < s->nr_parts ? s->partlist[id] : NULL;
+        out[id] = p ? p->f[3] : 0.f;
     }
     return 0;
 }

@@ -26,9 +26,10 @@ A scenario is a dict:
     friction(coef, std, mean, durration) (MxForce.cpp:213-259),
     target_temperature {type: T},
     wall_pots [(face or -1, type, kind, params)] (bind(pot, boundary condition, type)),
+    cuboids [(pos, size, angles)] (static cuboids), cuboid_pots [(type, kind, params)] (bind(pot, Cuboid, type)),
     species (optional): sp_nspec (per type), sp_flags (types x smax), sp_values (N x smax),
     fluxes [(kind 0 fick | 1 secrete | 2 uptake, type a, type b, species a, species b, k, decay, target)]
-Results: xabs, xrel, v, f, cell (per id), tasks (rows type, sid, i, j),
+Results: xabs, xrel, v, f, cell, number_density (per id), tasks (rows type, sid, i, j),
     cdim, h, epot, epot_angle, epot_dihedral, ekin, bond_flags, seconds (wall time of the steps).
 """
 import ctypes
@@ -53,7 +54,7 @@ def _pack(scn):
     for k, v in scn.items():
         if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc", "sbforces",
                  "target_temperature", "wall_pots", "fluxes",
-                 "sp_names"):
+                 "sp_names", "cuboids", "cuboid_pots"):
             flat[k] = np.array(repr(v))
         else:
             flat[k] = np.asarray(v)
@@ -66,7 +67,7 @@ def _unpack(npz):
         v = npz[k]
         if k in ("types", "pots", "forces", "bond_pot", "angle_pot", "dihedral_pot", "bc", "sbforces",
                  "target_temperature", "wall_pots", "fluxes",
-                 "sp_names"):
+                 "sp_names", "cuboids", "cuboid_pots"):
             out[k] = eval(str(v))  # written by _pack from plain literals
         elif v.shape == ():
             out[k] = v.item()
@@ -167,6 +168,18 @@ def _execute(scn):
             raise RuntimeError("mxref_bind_boundary_potential")
     for t, temp in scn.get("target_temperature", {}).items():
         L.mxref_set_target_temperature(int(t), float(temp))
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.mxref_add_cuboid.argtypes = [fp, fp, fp]
+    L.mxref_bind_cuboid.argtypes = [vp, ci]
+    for (pos, size, ang) in scn.get("cuboids", []):
+        pa, sa, aa = (np.ascontiguousarray(q, dtype=np.float32) for q in (pos, size, ang))
+        if L.mxref_add_cuboid(pa.ctypes.data_as(fp), sa.ctypes.data_as(fp), aa.ctypes.data_as(fp)) != 0:
+            raise RuntimeError("mxref_add_cuboid")
+    for (t, kind, params) in scn.get("cuboid_pots", []):
+        cp = make_pot(kind, params)
+        keep.append(cp)
+        if L.mxref_bind_cuboid(cp, int(t)) != 0:
+            raise RuntimeError("mxref_bind_cuboid")
     x = np.ascontiguousarray(scn["x"], dtype=np.float64)
     v = np.ascontiguousarray(scn["v"], dtype=np.float64)
     t = np.ascontiguousarray(scn["t"], dtype=np.int32)
@@ -266,6 +279,9 @@ def _execute(scn):
                       vv.ctypes.data_as(P(ctypes.c_float)), ff.ctypes.data_as(P(ctypes.c_float)),
                       cc.ctypes.data_as(P(ci)), tt.ctypes.data_as(P(ci)))
     out.update(xrel=xr, xabs=xa, v=vv, f=ff, cell=cc)
+    nd = np.zeros(n, dtype=np.float32)
+    L.mxref_number_density(n, nd.ctypes.data_as(P(ctypes.c_float)))
+    out["number_density"] = nd
     cdim = np.zeros(3, dtype=np.int32)
     h = np.zeros(3)
     nc, nt, per = ci(), ci(), ctypes.c_uint()

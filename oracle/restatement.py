@@ -314,3 +314,152 @@ def nonbond(scn, xrel, vel, cell, tasks, cdim, precision=64, tables=None, second
     if rc != 0:
         raise RuntimeError(f"orc_nonbond {rc}")
     return f, ep.value, counts
+
+
+def _table_index(info, s):
+    """The interval of s as the FP32 code picks it (potential_eval.hpp:83-86: the quadratic
+    map in float, truncated, at most n): an integer decision of the tabulated model, so the
+    FP64 evaluation uses the same polynomial piece as the FP32 one."""
+    f32 = np.float32
+    a = np.asarray(info["alpha"], dtype=f32)
+    s32 = np.asarray(s, dtype=f32)
+    t = a[0] + s32 * (a[1] + s32 * a[2])
+    return np.minimum(np.maximum(f32(0), t).astype(np.int64), info["n"])
+
+
+def _table_poly(coef, ind, s):
+    """Value and derivative of the table's interval polynomial at s, in FP64
+    (the Horner scheme of potential_eval.hpp:67-104 without its rounding)."""
+    c = np.asarray(coef, dtype=np.float64).reshape(-1, 8)[ind]
+    x = (s - c[..., 0]) * c[..., 1]
+    ee = c[..., 2] * x + c[..., 3]
+    eff = c[..., 2].copy()
+    for k in range(4, 8):
+        eff = eff * x + ee
+        ee = ee * x + c[..., k]
+    return ee, eff * c[..., 1]
+
+
+def _min_image(d, dim, periodic):
+    d = np.array(d, dtype=np.float64)
+    for k in range(3):
+        if periodic[k]:
+            d[..., k] -= dim[k] * np.round(d[..., k] / dim[k])
+    return d
+
+
+def _cos_grad(u, w):
+    """c = u.w / (|u| |w|) and its gradients with respect to u and w."""
+    nu, nw = np.linalg.norm(u, axis=-1, keepdims=True), np.linalg.norm(w, axis=-1, keepdims=True)
+    c = (u * w).sum(-1, keepdims=True) / (nu * nw)
+    return c[..., 0], (w / nw - c * u / nu) / nu, (u / nu - c * w / nw) / nw
+
+
+def bonded(scn, xabs, bond_flags=None, tables=None, virial=False):
+    """FP64 bonded forces (N, 3) and energy of a configuration, in the order of
+    engine_bonded_eval (src/mdcore/src/engine_bonded.cpp:1373-1543) on the
+    reference builder's FP32 tables:
+      exclusions (exclusion.cpp:83-282): the pair's table potential without the
+        radius shift taken back for excluded pairs within the cutoff;
+      bonds (bond.cpp:99-312): r^2 clamped to [a^2, b^2], F_i = -V'(r)/r d; bond_flags
+        (after the pass) select the bonds that acted;
+      angles (angle.cpp:92-352): V(cos theta) at the vertex j, cos clamped to [a, b],
+        F = -V'(c) dc/dx;
+      dihedrals (dihedral.cpp:81-392): V(c), c = -(b1 x b2).(b2 x b3) / (|b1 x b2| |b2 x b3|)
+        with b1 = x_i - x_j, b2 = x_k - x_j, b3 = x_l - x_k, clamped to [a, b].
+    Positions are global (FP64), pairs by minimum image on periodic axes.
+    tables: optional {"bond"/"angle"/"dihedral"/(ti, tj): (info, coef)}.
+    virial: also return the terms' virial sum (x_m - x_ref) (x) F_m (bonds and
+    exclusions d (x) F_i, angles about the vertex, dihedrals about j)."""
+    tables = dict(tables or {})
+    x = np.asarray(xabs, dtype=np.float64)
+    n = len(x)
+    dim = np.asarray(scn["dim"], dtype=np.float64)
+    periodic = [b == "periodic" for b in scn["bc"]]
+    f = np.zeros((n, 3))
+    ep = 0.0
+    W = np.zeros((3, 3))
+
+    def vir(r, F):
+        W[...] += np.einsum("na,nb->ab", np.atleast_2d(r), np.atleast_2d(F))
+
+    def table(key, kind_params):
+        if key not in tables:
+            tables[key] = reference_table(*kind_params)
+        return tables[key]
+
+    t = np.asarray(scn["t"])
+    if "ex_i" in scn and len(scn["ex_i"]):
+        pots = {}
+        for (kind, params, ti, tj) in scn["pots"]:
+            pots[(ti, tj)] = pots[(tj, ti)] = (kind, params)
+        cut2 = float(scn["cutoff"]) ** 2
+        for i, j in zip(scn["ex_i"], scn["ex_j"]):
+            kp = pots.get((int(t[i]), int(t[j])))
+            if kp is None or kp[0] == "dpd":
+                continue
+            d = _min_image(x[i] - x[j], dim, periodic)
+            r2 = float(d @ d)
+            if r2 > cut2:
+                continue
+            info, coef = table(("pair",) + tuple(sorted((int(t[i]), int(t[j])))), kp)
+            r = np.sqrt(r2)
+            e, dv = _table_poly(coef, _table_index(info, r), r)
+            f[i] += dv / r * d
+            f[j] -= dv / r * d
+            ep -= float(e)
+            vir(d, dv / r * d)
+    if "bi" in scn and len(scn["bi"]):
+        info, coef = table("bond", scn["bond_pot"])
+        bi, bj = np.asarray(scn["bi"]), np.asarray(scn["bj"])
+        act = np.ones(len(bi), bool) if bond_flags is None else (np.asarray(bond_flags) & 1).astype(bool)
+        bi, bj = bi[act], bj[act]
+        d = _min_image(x[bi] - x[bj], dim, periodic)
+        r = np.sqrt(np.clip((d * d).sum(1), info["a"] ** 2, info["b"] ** 2))
+        e, dv = _table_poly(coef, _table_index(info, r), r)
+        fi = -(dv / r)[:, None] * d
+        np.add.at(f, bi, fi)
+        np.add.at(f, bj, -fi)
+        ep += float(e.sum())
+        vir(d, fi)
+    if "ai" in scn and len(scn["ai"]):
+        info, coef = table("angle", scn["angle_pot"])
+        ai, aj, ak = (np.asarray(scn[k]) for k in ("ai", "aj", "ak"))
+        rji = _min_image(x[ai] - x[aj], dim, periodic)
+        rjk = _min_image(x[ak] - x[aj], dim, periodic)
+        c, gi, gk = _cos_grad(rji, rjk)
+        cc = np.clip(np.clip(c, -1.0, 1.0), info["a"], info["b"])
+        e, dv = _table_poly(coef, _table_index(info, cc), cc)
+        wi, wk = dv[:, None] * gi, dv[:, None] * gk
+        np.add.at(f, ai, -wi)
+        np.add.at(f, ak, -wk)
+        np.add.at(f, aj, wi + wk)
+        ep += float(e.sum())
+        vir(rji, -wi)
+        vir(rjk, -wk)
+    if "di" in scn and len(scn["di"]):
+        info, coef = table("dihedral", scn["dihedral_pot"])
+        di, dj, dk, dl = (np.asarray(scn[k]) for k in ("di", "dj", "dk", "dl"))
+        b1 = _min_image(x[di] - x[dj], dim, periodic)
+        b2 = _min_image(x[dk] - x[dj], dim, periodic)
+        b3 = _min_image(x[dl] - x[dk], dim, periodic)
+        A, B = np.cross(b1, b2), np.cross(b2, b3)
+        c, gA, gB = _cos_grad(A, B)
+        c, gA, gB = -c, -gA, -gB
+        g1 = np.cross(b2, gA)                        # dc/db1 through A = b1 x b2
+        g2 = np.cross(gA, b1) + np.cross(b3, gB)     # dc/db2 through A and B = b2 x b3
+        g3 = np.cross(gB, b2)                        # dc/db3 through B
+        cc = np.clip(np.clip(c, -1.0, 1.0), info["a"], info["b"])
+        e, dv = _table_poly(coef, _table_index(info, cc), cc)
+        wi, wj, wl = dv[:, None] * g1, dv[:, None] * (-g1 - g2), dv[:, None] * g3
+        np.add.at(f, di, -wi)
+        np.add.at(f, dj, -wj)
+        np.add.at(f, dl, -wl)
+        np.add.at(f, dk, wi + wj + wl)
+        ep += float(e.sum())
+        vir(b1, -wi)
+        vir(b2, wi + wj + wl)
+        vir(b2 + b3, -wl)
+    if virial:
+        return f, ep, W
+    return f, ep

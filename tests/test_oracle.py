@@ -5,7 +5,7 @@ import pytest
 
 from oracle import restatement as R
 
-from golden_util import CASES, load, ref_tasks, rel_rms
+from golden_util import CASES, fp64_total, load, ref_tasks, rel_rms
 
 NONBONDED = [c for c in CASES if not c.startswith("lattice")]
 
@@ -29,6 +29,27 @@ def test_tier_b_fp64_close_to_reference(name):
     f64, ep64, _ = R.nonbond(scn, z["force_xrel"], scn["v"], z["force_cell"], ref_tasks(z), z["force_cdim"],
                              precision=64)
     assert rel_rms(z["force_f"], f64) < 1e-5
+
+
+BONDED = ["lattice_small", "lattice_break", "lattice_noisy", "chains_bonded", "chains_morse", "chains_dihedral",
+          "chains_dihedral_shift", "chains_excl"]
+
+
+@pytest.mark.parametrize("name", BONDED)
+def test_fp64_bonded_restatement_matches_reference(name):
+    """The FP64 oracle with bonded terms (tier B nonbonded + the bonded restatement) against
+    the reference engine's FP32 force pass: forces within the reference's own FP32 error
+    (1e-5 relative RMS), energies within 1e-6. Particles in pairs closer than the table
+    minimum (a random direction in the reference) are left out of the force comparison;
+    their energy is not restated, so the energy check skips cases that have them."""
+    from test_gpu_parity import _close_pairs
+    z, scn = load(name)
+    f64, ep64 = fp64_total(scn, z["force_xrel"], scn["v"], z["force_cell"], z, z["force_bond_flags"])
+    keep = ~_close_pairs(scn, scn["x"])
+    assert rel_rms(z["force_f"][keep], f64[keep]) < 1e-5
+    if keep.all():
+        ref = float(z["force_epot"])
+        assert abs(ep64 - ref) <= 1e-6 * abs(ref)
 
 
 def test_tier_b_bonds_excluded_lattice_nonbonded():
