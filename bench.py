@@ -6,12 +6,14 @@ Default workload (N=1): the DPD fluid with a body force -- 200,000 particles in 
 sigma=3, cutoff 1, constant force 0.02 in +x, dt=0.01 -- seeded synthetic
 positions (uniform) and velocities (Maxwell-Boltzmann, kT=1).
 
-One step = one engine_step: nonbonded forces, integrator, re-binning (four
+One step = one engine_step: nonbonded forces, integrator, re-binning (three
 kernels replayed from a CUDA graph). value = particles x timed steps / device
 time (per-step CUDA events on the engine stream, L2 flushed between steps with
-a 256 MiB write). e2e = the same metric through the C ABI with host buffers:
-every step uploads the state from pinned host memory, steps, downloads the
-state and the FP64 energies.
+a 256 MiB write). e2e = the same metric through the C ABI in the reference's
+data format with host buffers: every step engine_load's the absolute positions
+and velocities by particle id from pinned host memory, steps, and
+engine_unload's them back (host clock); the raw slot-order state copy is
+reported beside it.
 
 --impl reference times the reference's own CPU engine (compiled in place from
 the reference sources, oracle/_ref) on this host's cores for the same workload.
@@ -37,15 +39,52 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-steps/s (1 B200) plain vs batched/adjoint; force rel-err <=1e-5"
 WORKLOAD = ("DPD fluid with body force: 200,000 particles, 40x20x20 box, periodic x/y, no-slip z; "
             "DPD a=25 gamma=4.5 sigma=3 rc=1 kT=1; constant force 0.02 +x; FP32, dt=0.01")
-# one force launch of the 200,000-particle DPD workload, from the ncu capture summarised in
-# profiles/force_kernel_dpd200k.md: DRAM read + write bytes, and warp instructions executed
-FORCE_TRAFFIC_BYTES = 17170688 + 1504768
-FORCE_WARP_INSTRUCTIONS = 137576112
+# counters of one force launch of the 200,000-particle DPD workload from an ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum, smsp__inst_executed.sum), with the hash of the
+# kernel sources they were captured on; used only while that hash matches the current sources
+COUNTERS = os.path.join(ROOT, "profiles", "force_kernel_dpd200k.counters.txt")
 # algorithmic FP32 operations per candidate pair and per interacting DPD pair
 # (counted from the reference's scalar pair loop and dpd_eval)
 F_CAND = 9
 F_INT_DPD = 40
 F_INT_TABLE = 44
+
+
+# the sources that decide what a force launch does: its kernels and device structures, the host
+# engine that builds its work items, tables and launch configuration, and the build flags
+FORCE_SOURCES = ("mechanica_b200/csrc/mxg_kernels.cu", "mechanica_b200/csrc/mxg_kernels.h",
+                 "mechanica_b200/csrc/mxg_device.cuh", "mechanica_b200/csrc/mxg_engine.cpp",
+                 "mechanica_b200/csrc/potential_table.cpp", "mechanica_b200/csrc/potential_table.h",
+                 "mechanica_b200/build.py")
+
+
+def sources_sha16():
+    """Hash of the sources that decide what a force launch does: identifies the build whose
+    launches a capture measured."""
+    import hashlib
+    h = hashlib.sha256()
+    for path in (os.path.join(ROOT, f) for f in FORCE_SOURCES):
+        h.update(os.path.basename(path).encode())
+        with open(path, "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()[:16]
+
+
+def captured_counters():
+    """(counters dict, note): the force launch's captured counters when they were taken on the
+    current sources, else (None, why not)."""
+    if not os.path.exists(COUNTERS):
+        return None, "no capture recorded"
+    rec = {}
+    with open(COUNTERS) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) >= 2 and not line.startswith("#"):
+                rec[parts[0]] = parts[1]
+    want = sources_sha16()
+    if rec.get("sources_sha16") != want:
+        return None, f"capture of sources {rec.get('sources_sha16')} is stale (current {want})"
+    return {k: int(v) for k, v in rec.items() if k != "sources_sha16" and v.isdigit()}, "captured on these sources"
 
 
 def parse():
@@ -88,18 +127,44 @@ def workload(n):
 
 
 class Clocks:
-    """Samples nvidia-smi clocks and throttle reasons every 200 ms."""
+    """Samples the SM clock and the clock-event (throttle) reasons during a timed region:
+    NVML polled every half millisecond in a thread (a 20-step region lasts a few
+    milliseconds), else nvidia-smi every 200 ms. Reads only; changes no setting."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
         self.index = index
         self.proc = None
         self.f = None
+        self.thread = None
+        self.samples = []
+        self.max_mhz = None
 
     def start(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            bits = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
+            self.stop_flag = threading.Event()
+
+            def poll():
+                while not self.stop_flag.is_set():
+                    mhz = float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                    r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((mhz, [n for n, bit in bits.items() if r & bit]))
+                    time.sleep(0.0005)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         try:
             self.f = tempfile.NamedTemporaryFile("w+", delete=False, suffix=".csv")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
@@ -109,8 +174,15 @@ class Clocks:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join()
+            sm = [m for m, _ in self.samples]
+            reasons = sorted({n for _, rs in self.samples for n in rs})
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                    "samples": len(sm), "source": "NVML, 0.5 ms period"}
         if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock source"]}
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -121,18 +193,17 @@ class Clocks:
         rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
         os.unlink(self.f.name)
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             try:
                 sm.append(float(r[1]))
                 mx = float(r[2])
-                for k, name in enumerate(names):
+                for k, name in enumerate(self.NAMES):
                     if r[5 + k].strip().lower() == "active":
                         reasons.add(name)
             except Exception:
                 continue
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 200 ms period"}
 
 
 def measured_peaks():
@@ -268,6 +339,7 @@ def forms_and_configs(args, stream, flush):
         check(L.mxg_engine_step(e, 3), "warm-up")
     ms_b = _time_steps(L, e, Kb, stream, flush)
     check(L.mxg_engine_status(e), "batched")
+    batched_roofline = force_roofline(L, e, flush, F_INT_TABLE, "Morse tables over all replicas")
     u.close()
     # the same replicas, one plain engine each, run one after another
     ms_s = 0.0
@@ -280,12 +352,42 @@ def forms_and_configs(args, stream, flush):
         check(L.mxg_engine_status(e), "sequential")
         m.universe.close()
     out["adjoint_32k"] = adjoint_form(stream)
+    out["adjoint_bonded_32k"] = adjoint_bonded_form(stream)
     out["batched_256"] = {"value": ntot * Kb / (ms_b / 1e3), "unit": "particle-steps/s", "replicas": len(specs),
                           "particles": ntot, "steps": Kb, "ms_per_step": ms_b / Kb,
                           "force_ctas_per_sm": per_sm,
                           "sequential_plain_value": ntot * Kb / (ms_s / 1e3),
-                          "speedup_vs_sequential": ms_s / ms_b}
+                          "speedup_vs_sequential": ms_s / ms_b, "roofline": batched_roofline}
     return out
+
+
+def fp32_peak_tflops():
+    """Nominal FP32 pipe of the current device (MEASURED_PEAKS.json holds no FP32 figure):
+    SMs x 128 lanes x 2 FLOP x the measured maximum SM clock."""
+    import torch
+    sm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = (measured_peaks() or {}).get("sm_max_mhz", 1965.0)
+    return sm * 128 * 2 * mhz * 1e6 / 1e12, f"nominal FP32 pipe: {sm} SMs x 128 lanes x 2 x {mhz:.0f} MHz"
+
+
+def force_roofline(L, e, flush, f_int, what, reps=20):
+    """The engine's force launch against the FP32 pipe: algorithmic FLOPs (F_CAND per
+    candidate pair of the reference's task lists, f_int per interacting pair, counted on the
+    current state) over the median CUDA-event time of reps launches, L2 flushed before each."""
+    from mechanica_b200._native import check
+    cand, inter = ctypes.c_longlong(), ctypes.c_longlong()
+    check(L.mxg_engine_pair_counts(e, ctypes.byref(cand), ctypes.byref(inter)), "pair_counts")
+    per = np.zeros(reps)
+    check(L.mxg_engine_time_force_launches(e, reps, ctypes.c_void_p(flush.data_ptr()), flush.numel(),
+                                           per.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "time_force")
+    ms = float(np.median(per))
+    flops = F_CAND * cand.value + f_int * inter.value
+    peak, src = fp32_peak_tflops()
+    achieved = flops / (ms / 1e3) / 1e12
+    return {"bound": "fp32", "kernel": f"force_kernel ({what})", "achieved": achieved, "peak": peak,
+            "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": src, "force_ms_per_launch": ms,
+            "algorithmic_flops_per_launch": flops, "candidate_pairs": cand.value, "interacting_pairs": inter.value,
+            "flops_per_pair": {"candidate": F_CAND, "interacting": f_int}}
 
 
 def adjoint_form(stream, nsteps=200, every=20):
@@ -326,7 +428,76 @@ def adjoint_form(stream, nsteps=200, every=20):
            "forward_value": n * nsteps / (fwd / 1e3), "loss": float(loss.item()),
            "grad_theta": [float(g) for g in theta.grad.numpy()],
            "params": "Morse (d, a, r0) of AA, AB, BB; DPD gamma shared",
-           "check": "gradients vs FP64 central differences: tests/test_gpu_adjoint.py (512 particles, 12 steps)"}
+           "check": "gradients vs FP64 central differences: tests/test_gpu_adjoint.py (512 particles; a = 8 over "
+                    "12 steps; the workload's own a = 5 over 4 steps with h = 1e-4, where Morse r0's difference "
+                    "spreads by ~1e-3 over h as its table edge crosses pairs at the cutoff)",
+           "roofline": adjoint_roofline(u._e, tot, nsteps, F_INT_TABLE + F_INT_DPD)}
+    u.close()
+    return out
+
+
+# the VJP of a pair term is counted as twice its forward arithmetic (the polynomial's value
+# and derivative for each term of the force and of its parameters)
+F_VJP_FACTOR = 2
+
+
+def adjoint_roofline(e, ms_total, nsteps, f_int):
+    """Forward + backward against the FP32 pipe. Algorithmic FLOPs per step: the forward force
+    pass and its recompute in the backward sweep (F_CAND per candidate, f_int per interacting
+    pair each) and the VJP (F_CAND per candidate, F_VJP_FACTOR x f_int per interacting pair);
+    pairs counted on the starting state (the density is constant), steps x that over the
+    CUDA-event time of forward + loss + backward."""
+    from mechanica_b200._native import check, lib
+    cand, inter = ctypes.c_longlong(), ctypes.c_longlong()
+    check(lib().mxg_engine_pair_counts(e, ctypes.byref(cand), ctypes.byref(inter)), "pair_counts")
+    per_step = 2 * (F_CAND * cand.value + f_int * inter.value) + F_CAND * cand.value + F_VJP_FACTOR * f_int * inter.value
+    flops = nsteps * per_step
+    peak, src = fp32_peak_tflops()
+    achieved = flops / (ms_total / 1e3) / 1e12
+    return {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "peak_source": src, "algorithmic_flops": flops, "candidate_pairs": cand.value,
+            "interacting_pairs": inter.value,
+            "flops_per_step": "2 x (9 cand + f_int int) + (9 cand + 2 f_int int)", "f_int": f_int}
+
+
+def adjoint_bonded_form(stream, nsteps=200, every=20):
+    """The adjoint through bonds: a 32^3 harmonic-bonded block (98,304 bonds, k = 20,
+    r0 = 0.5, starting stretched at 0.51) with a weak Morse term, overdamped, dt = 0.002;
+    200 steps, snapshots every 20; loss = a seeded linear functional of the final positions;
+    gradients with respect to harmonic k and r0 and Morse d and a (the FD-checked model of
+    tests/test_gpu_adjoint_bonds.py, scaled up)."""
+    import torch
+    from mechanica_b200 import adjoint as A
+    from mechanica_b200 import workloads as W
+    spec = W.bonded_block(nx=32)
+    n = len(spec["t"])
+    with torch.cuda.stream(stream):
+        u, P = W.build_bonded_adjoint(spec, stream=stream.cuda_stream)
+        c = torch.tensor(np.random.default_rng(3).normal(size=(n, 3)), dtype=torch.float64, device="cuda")
+        theta = torch.tensor(P.theta(), dtype=torch.float64, requires_grad=True)
+        x0 = torch.tensor(spec["x"], dtype=torch.float64, requires_grad=True)
+        v0 = torch.zeros_like(x0)
+        x4 = A.trajectory(theta, x0, v0, A.Simulation(u, P, nsteps=every, checkpoint_every=every, step0=0))
+        (x4[:, :3].double() * c).sum().backward()
+        theta.grad = None
+        sim = A.Simulation(u, P, nsteps=nsteps, checkpoint_every=every, step0=0)
+        torch.cuda.synchronize()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        x4 = A.trajectory(theta, x0, v0, sim)
+        loss = (x4[:, :3].double() * c).sum()
+        e1.record(stream)
+        loss.backward()
+        e2.record(stream)
+        torch.cuda.synchronize()
+    fwd, tot = e0.elapsed_time(e1), e0.elapsed_time(e2)
+    out = {"value": n * nsteps / (tot / 1e3), "unit": "particle-steps/s (forward + backward)", "particles": n,
+           "bonds": int(len(spec["bi"])), "steps": nsteps, "checkpoint_every": every, "ms_forward": fwd,
+           "ms_forward_backward": tot, "forward_value": n * nsteps / (fwd / 1e3),
+           "grad_theta": [float(g) for g in theta.grad.numpy()], "params": "harmonic k, r0; Morse d, a",
+           "check": "bond-k, r0, Morse and position gradients vs FP64 central differences: "
+                    "tests/test_gpu_adjoint_bonds.py (6^3 block, 10 steps)",
+           "roofline": adjoint_roofline(u._e, tot, nsteps, F_INT_TABLE)}
     u.close()
     return out
 
@@ -446,7 +617,28 @@ def main():
             flush.zero_()
     barrier()
     ms_e2e = max_over_ranks(sum(s.elapsed_time(t) for s, t in zip(s2, e2)), world, dev)
-    e2e = job_rate(world, n, Ke, ms_e2e)
+    e2e_raw = job_rate(world, n, Ke, ms_e2e)
+
+    # ---- e2e through the reference's own data format: engine_load (absolute positions and
+    # velocities by particle id, from pinned host memory), engine_step, engine_unload (the same
+    # arrays back), on the host's clock around the synchronised calls ----
+    hx = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
+    hv = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+    xp = ctypes.cast(ctypes.c_void_p(hx.data_ptr()), ctypes.POINTER(ctypes.c_double))
+    vp = ctypes.cast(ctypes.c_void_p(hv.data_ptr()), ctypes.POINTER(ctypes.c_float))
+    check(L.mxg_engine_unload(e, n, xp, vp, None, None, None), "unload")
+    Kl = max(1, min(K, 200))
+    barrier()
+    t_l = time.perf_counter()
+    for k in range(Kl):
+        check(L.mxg_engine_load(e, n, xp, vp), "load")
+        check(L.mxg_engine_step(e, 1), "step")
+        check(L.mxg_engine_unload(e, n, xp, vp, None, None, None), "unload")
+    torch.cuda.synchronize(dev)
+    ms_l = max_over_ranks(1e3 * (time.perf_counter() - t_l), world, dev)
+    barrier()
+    check(L.mxg_engine_status(e), "e2e status")
+    e2e = job_rate(world, n, Kl, ms_l)
 
     # ---- roofline of the dominant kernel (nonbonded forces) ----
     # the force kernel alone, per launch, L2 flushed before each launch; the median
@@ -470,10 +662,11 @@ def main():
                 "algorithmic_flops_per_launch": flops, "candidate_pairs": cand.value,
                 "interacting_pairs": inter.value,
                 "flops_per_pair": {"candidate": F_CAND, "interacting_dpd": F_INT_DPD},
-                "force_ms_per_launch": force_ms,
-                # dram__bytes_read.sum + dram__bytes_write.sum of one force launch of this workload
-                # (ncu capture summarised in profiles/force_kernel_dpd200k.md)
-                "traffic": FORCE_TRAFFIC_BYTES if n == 200000 else None, "traffic_unit": "bytes per launch"}
+                "force_ms_per_launch": force_ms}
+    counters, counters_note = captured_counters() if n == 200000 else (None, "no capture of this size")
+    traffic = counters.get("dram_bytes_per_launch") if counters else None
+    roofline.update({"traffic": traffic, "traffic_unit": "bytes per launch", "traffic_source": counters_note,
+                     "sources_sha16": sources_sha16()})
     # the same launch against the measured HBM copy bandwidth: compulsory state bytes (position and
     # velocity read, force written, 16 B each per particle) over the launch time, and the captured
     # DRAM traffic over the same time; both far below the bound, so HBM does not limit this kernel
@@ -485,14 +678,15 @@ def main():
             "algorithmic_bytes_per_launch": state_bytes,
             "achieved": state_bytes / (force_ms / 1e3) / 1e9,
             "frac": state_bytes / (force_ms / 1e3) / 1e9 / hbm_peak,
-            "traffic_rate": (FORCE_TRAFFIC_BYTES / (force_ms / 1e3) / 1e9) if n == 200000 else None}
-    if n == 200000:
+            "traffic_rate": (traffic / (force_ms / 1e3) / 1e9) if traffic else None}
+    if counters and counters.get("warp_instructions_per_launch"):
         # the limiter the counters show: instruction issue (one warp instruction per scheduler
-        # per clock, four schedulers per SM)
+        # per clock, four schedulers per SM), from the capture of these sources
+        wi = counters["warp_instructions_per_launch"]
         issue_peak = sm_count * 4 * max_mhz * 1e6 / 1e9
-        issue = FORCE_WARP_INSTRUCTIONS / (force_ms / 1e3) / 1e9
+        issue = wi / (force_ms / 1e3) / 1e9
         roofline["issue_view"] = {
-            "warp_instructions_per_launch": FORCE_WARP_INSTRUCTIONS, "achieved": issue, "peak": issue_peak,
+            "warp_instructions_per_launch": wi, "achieved": issue, "peak": issue_peak,
             "unit": "G warp-instructions/s", "frac": issue / issue_peak,
             "peak_source": f"{sm_count} SMs x 4 schedulers x {max_mhz:.0f} MHz (nominal issue rate)"}
 
@@ -523,11 +717,16 @@ def main():
             "config": {"workload": WORKLOAD, "particles_per_gpu": n, "cells": scn["cells"],
                        "l2": "flushed between steps (256 MiB write outside the per-step CUDA events)",
                        "rng": "reference DPD random term (xi = 1)", "parallelism": f"replicas x{world}"},
-            "clocks": clocks, "gpu_launches": 4 * K,
-            "e2e": {"value": e2e, "unit": "particle-steps/s", "steps": Ke, "h2d_bytes_per_step": 32 * n,
-                    "d2h_bytes_per_step": 32 * n + 16,
-                    "path": "mxg_engine_copy_state (pinned host -> device), mxg_engine_step, "
-                            "mxg_engine_copy_state (device -> pinned host), mxg_engine_energy_async"},
+            "clocks": clocks, "gpu_launches": 3 * K,
+            "e2e": {"value": e2e, "unit": "particle-steps/s", "steps": Kl, "h2d_bytes_per_step": 36 * n,
+                    "d2h_bytes_per_step": 36 * n,
+                    "path": "mxg_engine_load (absolute x double[3], v float[3] by id, pinned host -> device; "
+                            "placement and (cell, id) ordering on the device), mxg_engine_step, "
+                            "mxg_engine_unload (x, v by id, device -> pinned host); host wall clock",
+                    "raw_state_copy": {"value": e2e_raw, "steps": Ke, "h2d_bytes_per_step": 32 * n,
+                                       "d2h_bytes_per_step": 32 * n + 16,
+                                       "path": "mxg_engine_copy_state (slot-order float4 pos, vel), mxg_engine_step, "
+                                               "mxg_engine_copy_state back, mxg_engine_energy_async; CUDA events"}},
             "roofline": roofline, "cpu_baseline": cpu, "accuracy": accuracy,
             "forms": forms, "wall_s_timed_region": t_wall}
     if rank == 0:

@@ -38,6 +38,10 @@
  *   mxg_engine_step                engine_step              src/mdcore/src/engine.cpp:1198
  *   mxg_engine_force               engine_force             src/mdcore/src/engine.cpp:1230
  *   mxg_engine_step_timed          engine_step with the engine timers (engine.h:113-135)
+ *   mxg_engine_add_cuboid          engine_addcuboid         src/mdcore/src/engine.cpp:1742
+ *   mxg_engine_set_cuboid_potential engine_add_cuboid_potential src/mdcore/src/engine.cpp:1816
+ *   mxg_engine_number_density      MxParticle::f[3]: space_prepare's self term (space.cpp:216-236) plus
+ *                                  the runners' W(r2, cutoff) per pair (runner_dopair.cpp:194-203)
  *   mxg_engine_load                engine_load              src/mdcore/include/engine.h:612
  *   mxg_engine_unload              engine_unload            src/mdcore/include/engine.h:646
  *   mxg_engine_kinetic_energy      engine_kinetic_energy    src/mdcore/src/engine.cpp:1698
@@ -72,7 +76,8 @@ extern "C" {
 #define MXG_ERR_NOCUDA -22
 #define MXG_ERR_TOOFAST -29
 /* GPU-specific status codes */
-#define MXG_ERR_CELL_OVERFLOW -101 /* more particles entered a cell in one step than its bucket holds */
+#define MXG_ERR_CELL_OVERFLOW -101 /* kept for ABI stability: no longer raised (any number of particles may
+                                      enter a cell in one step) */
 #define MXG_ERR_NONFINITE -102     /* a position or velocity became NaN/Inf */
 #define MXG_ERR_STATE -103         /* call made in the wrong engine state */
 #define MXG_ERR_ARG -104           /* invalid argument */
@@ -195,9 +200,17 @@ int mxg_engine_pot_index(mxg_engine *e, int replica, int type_i, int type_j, int
  * engine the device copy is updated in place, ordered on the engine stream. No counterpart in the
  * reference. */
 int mxg_engine_set_pot_params(mxg_engine *e, int idx, const double *params, int nparams);
-/* Chooses the force kernel's grid (CTAs per SM) by timing candidate launches on the current state;
- * returns the chosen blocks per SM. Call after mxg_engine_start. */
+/* Chooses the force kernel's tile shape (own and neighbour particles staged per region: 32/96,
+ * 32/64, 64/96 or 32/128) and grid (CTAs per SM) by timing candidate launches on the current state,
+ * so the choice follows the state's density; returns the chosen blocks per SM. Call after
+ * mxg_engine_start. Tile shapes differ in the order of the FP32 force sums, so two engines compare
+ * bit for bit only with the same configuration (mxg_engine_force_config). No counterpart in the
+ * reference. */
 int mxg_engine_autotune(mxg_engine *e);
+/* set = 0: reads the force kernel's tile variant (0-3) and grid (CTAs); set = 1: pins them (after
+ * mxg_engine_start; the grid is clamped to the blocks the work items can occupy and written back;
+ * the step graphs are re-captured). */
+int mxg_engine_force_config(mxg_engine *e, int *variant, int *grid, int set);
 
 /* dt, max-distance fraction (reference default 0.05) */
 int mxg_engine_set_dt(mxg_engine *e, double dt, double max_dist_fraction);
@@ -251,6 +264,19 @@ int mxg_engine_adddihedrals(mxg_engine *e, int n, const int *i, const int *j, co
  * normal; tables get potential_eval_ex with wall radius 0, DPD potentials dpd_boundary_eval against the
  * wall velocity. */
 int mxg_engine_set_boundary_potential(mxg_engine *e, int face, int type, const mxg_potential *p);
+/* Adds a static cuboid to replica rep (engine_addcuboid, src/mdcore/src/engine.cpp:1742; Cuboid(pos, size,
+ * orientation), src/mdcore/src/MxCuboid.cpp:40-76): centre pos (NULL: the box centre dim / 2, as
+ * engine_center), size, orientation angles about x, y, z (the quaternion qx qy qz). Its bounding box is
+ * formed as MxCuboid_UpdateAABB does (MxCuboid.cpp:190-221). id (may be NULL) receives its index. */
+int mxg_engine_add_cuboid(mxg_engine *e, int rep, const float *pos, const float *size, const float *angles, int *id);
+/* The potential between particles of a type and every cuboid (engine_add_cuboid_potential,
+ * src/mdcore/src/engine.cpp:1816-1830; bind(pot, Cuboid, type), MxBind.cpp:67-73), evaluated per particle
+ * as potential_eval_cuboid_particle (src/mdcore/src/cuboid_eval.hpp:73-188): the particle's distance from
+ * the cuboid's centre along the axis of the face it is nearest to (inside) or above (outside), in the
+ * cuboid's frame, through potential_eval_ex with r0 = half the size on that axis. No energy. */
+int mxg_engine_set_cuboid_potential(mxg_engine *e, int type, const mxg_potential *p);
+/* Cuboid id's geometry: out16 = centre[3], size[3], orientation quaternion (x, y, z, w), box min[3], max[3]. */
+int mxg_engine_cuboid_info(const mxg_engine *e, int id, float *out16);
 /* Species (chemical cargo) of a particle type: nspec values per particle (at most 8), flags per species
  * (bit 2: constant, SPECIES_KONSTANT: not integrated). Before mxg_engine_start. */
 int mxg_engine_set_type_species(mxg_engine *e, int type, int nspec, const unsigned *flags);
@@ -299,20 +325,42 @@ int mxg_engine_nr_cells(const mxg_engine *e);
 /* Per-id host copies: absolute positions (double[3n]), velocities, forces (float[3n]), cell index,
  * cell-relative positions. Any pointer may be NULL. */
 int mxg_engine_unload(mxg_engine *e, int n, double *x, float *v, float *f, int *cell, float *xrel);
-/* Per-id upload of positions (double[3n], global coordinates) and velocities (float[3n]);
- * particles are re-binned as engine_addpart would place them. */
+/* Per-id upload of positions (double[3n], global coordinates) and velocities (float[3n]; NULL keeps
+ * each particle's velocity); particles are placed as engine_addpart would place them and ordered by
+ * (cell, id), both on the device. A position outside its replica's box returns MXG_ERR_SPACE and
+ * changes no state. */
 int mxg_engine_load(mxg_engine *e, int n, const double *x, const float *v);
 /* Potential energy (nonbonded + bonded) of the last force evaluation and the current kinetic energy,
- * both reduced in FP64 on the device. virial9 (may be NULL): the nonbonded pair virial
- * sum over pairs of (x_first - x_second) (x) F_first of the current positions, reduced in FP64 (one
- * extra force pass that changes no engine state); the reference's MxCalculateVirial returns zeros
- * (metrics.cpp:183,246). */
+ * both reduced in FP64 on the device. virial9 (may be NULL): the virial of the current positions,
+ * reduced in FP64: the nonbonded pair sum of (x_first - x_second) (x) F_first (one extra force pass
+ * that changes no engine state) plus the bonded terms' sum of (x_m - x_ref) (x) F_m (bonds active
+ * after the last pass, exclusions, angles about their vertex, dihedrals about their j particle); the
+ * reference's MxCalculateVirial returns zeros (metrics.cpp:183,246). */
 int mxg_engine_energy(mxg_engine *e, double *epot, double *ekin, double *virial9);
 double mxg_engine_kinetic_energy(mxg_engine *e);
 /* Cell-pair task list rows (type, sid, i, j) as space_init builds them. */
 int mxg_engine_tasks(const mxg_engine *e, int *out, int cap);
 /* Bond flags (bit 0 = active); returns the number of bonds. */
 int mxg_engine_bond_flags(mxg_engine *e, unsigned *out, int cap);
+/* The number density of the particles for the current positions (the reference's
+ * MxParticle::number_density, f[3], as a force pass leaves it: space_prepare's W(0, cutoff),
+ * src/mdcore/src/space.cpp:216-236, plus W(r^2, cutoff) for every pair the pair loops reach
+ * within the cutoff whose type pair has no potential and no flux, or whose potential evaluates
+ * in range, src/mdcore/src/runner_dopair.cpp:194-203 and dpd_eval.hpp:133-166; W the cubic
+ * spline of smoothing_kernel.hpp:37-56). out: float[n] by particle id (may be NULL); volume (may
+ * be NULL): engine_advance's computed volume, the sum of 1 / number density
+ * (engine_advance.cpp:184-185), in FP64. The reference forms r with a 12-bit reciprocal
+ * square-root approximation; here r = sqrtf(r^2). Large particles, wall potentials and second
+ * summed potentials add nothing. Synchronous. */
+int mxg_engine_number_density(mxg_engine *e, int n, float *out, double *volume);
+/* Replaces the bond flags (n = the number of bonds; bit 0 = active). The reference keeps the flag in
+ * each bond (MxBond.flags, src/mdcore/include/bond.h:47-70) and re-creates destroyed bonds through
+ * _bond_init (src/mdcore/src/bond.cpp:497); here a trajectory restarted from its first state
+ * re-activates the bonds it had then. Ordered on the engine stream. */
+int mxg_engine_set_bond_flags(mxg_engine *e, const unsigned *flags, int n);
+/* The engine's index of bond k's potential (for mxg_engine_set_pot_params and
+ * mxg_engine_adjoint_params). */
+int mxg_engine_bond_pot_index(const mxg_engine *e, int k, int *idx);
 /* Space description: cdim[3], h[3], nr_cells, period bitmask. */
 int mxg_engine_space_info(const mxg_engine *e, int *cdim, double *h, int *nr_cells, unsigned *period);
 /* Raw device-resident state in slot order (cell-sorted): pos float4 (xrel, type bits),
@@ -343,7 +391,11 @@ int mxg_engine_adjoint_params(mxg_engine *e, int n, const int *pot, const int *p
  * arrays indexed by particle id, holding the adjoints of the positions and velocities after the step;
  * on return (stream-ordered) they hold the adjoints of the state before it. grad: device double array
  * of the gradient slots, to which the step's parameter terms are added. Periodic boxes, nonbonded
- * potentials (tables, DPD, summed pairs) and constant forces; bonds are refused (MXG_ERR_ARG). */
+ * potentials (tables, DPD, summed pairs), bonds (bond_eval, src/mdcore/src/bond.cpp:99-312: the
+ * table through its length clamp, harmonic k and r0 as parameters; break flags held fixed: a bond
+ * broken before or during the step adds nothing) and constant forces; angles, dihedrals, exclusions,
+ * wall potentials, large particles and Berendsen/random/friction forces are refused (MXG_ERR_ARG).
+ * Wall reflections of the integrator are not differentiated. */
 int mxg_engine_vjp_step(mxg_engine *e, void *lam_x, void *lam_v, double *grad);
 /* Device float4 arrays by particle id: absolute positions (x, y, z, type bits) and velocities
  * (v, id bits); either pointer may be NULL. Stream-ordered. */
@@ -406,10 +458,14 @@ int mxg_engine_pair_counts(mxg_engine *e, long long *candidates, long long *inte
  * doubles; out is a device array of 1 + ntypes doubles receiving the total and the per-type sums.
  * Work is enqueued on stream (NULL = default stream). The reduction's scratch is a file-scope
  * device array of 256 x 64 doubles (128 KiB, held by every GPU that loads the library until the
- * process exits): ntypes above 64 is rejected with MXG_ERR_RANGE. The first call on a device looks
- * the array's address up for that device (cudaGetSymbolAddress); make that first call before any
- * stream capture. Calls that overlap on the GPU share the array and race; serialise them. Nothing
- * is allocated: no cudaMalloc, cudaFree or allocating library routine is called. */
+ * process exits): ntypes above 64 is rejected with MXG_ERR_RANGE. Type ids outside [0, ntypes)
+ * contribute nothing. The first call on a device looks the array's address up for that device
+ * (cudaGetSymbolAddress); with CUDA's lazy module loading (the default since CUDA 12) that first
+ * call, or the first launch, may also load this library's device code, which allocates device
+ * memory for the code and the array and can synchronise the device: make the first call per device
+ * during set-up, outside any allocation-free or latency-critical region and before any stream
+ * capture. After it, calls allocate nothing: no cudaMalloc, cudaFree or allocating library routine
+ * is called. Calls that overlap on the GPU share the array and race; serialise them. */
 int mxg_kinetic_energy_noalloc(const void *vel, const void *pos, int nparts, const double *type_mass, int ntypes,
                                double *out, void *stream);
 

@@ -18,8 +18,10 @@ factories, src/mdcore/src/bond.cpp:535-560 for ``Bond``):
 Everything below the Python layer is the C ABI of libmxg.so (include/mxg.h);
 all force, bond and integration work runs in CUDA kernels on the device.
 """
+import atexit
 import ctypes
 import math
+import weakref
 
 import numpy as np
 
@@ -27,7 +29,7 @@ from . import _native
 from ._native import EngineError, check, f32, f64, i32, lib, ptr
 
 __all__ = [
-    "init", "Universe", "universe", "Particle", "Potential", "Bond", "Angle", "Dihedral", "flux", "fick", "secrete", "uptake", "bind", "forces", "step", "run",
+    "init", "Universe", "universe", "Particle", "Potential", "Bond", "Angle", "Dihedral", "Cuboid", "flux", "fick", "secrete", "uptake", "bind", "forces", "step", "run",
     "Newtonian", "Overdamped", "FORWARD_EULER", "RUNGE_KUTTA_4", "BOUNDARY_NONE", "PERIODIC_X", "PERIODIC_Y", "PERIODIC_Z",
     "PERIODIC_FULL", "FREESLIP_X", "FREESLIP_Y", "FREESLIP_Z", "FREESLIP_FULL", "EngineError", "ParticleList",
 ]
@@ -358,6 +360,20 @@ class Dihedral:
         self.potential = potential
 
 
+class Cuboid:
+    """A static box that particles of a bound type are pushed from (the reference's Cuboid,
+    MxCuboid.cpp:40-76): centre pos (default the box centre, engine_center), size and the
+    orientation angles about x, y and z. Bind a potential to it with
+    bind(potential, Cuboid, ParticleType)."""
+
+    def __init__(self, pos=None, size=(1.0, 1.0, 1.0), orientation=(0.0, 0.0, 0.0), replica=0):
+        self.id = _require()._add_cuboid(pos, size, orientation, replica)
+
+    @property
+    def geometry(self):
+        return universe.cuboid_info(self.id)
+
+
 class BoundaryCondition:
     """One face of the box (MxBoundaryCondition, MxBoundaryConditions.hpp:25-52);
     ``bind(potential, face, Type)`` puts a wall potential between the face and
@@ -558,6 +574,8 @@ class _Universe:
         self._dihedrals = []    # (potential, i[], j[], k[], l[])
         self._exclusions = []   # (i[], j[])
         self._bpots = []        # wall potentials: (potential, face or -1, type)
+        self._cuboids = []      # (replica, pos or None, size, angles)
+        self._cuboid_pots = []  # (potential, type)
         self._species = {}      # type -> (species names, flags)
         self._spec_width = 0
         self._spec = np.zeros((0, 0), dtype=np.float32)  # species values by particle id
@@ -581,6 +599,7 @@ class _Universe:
                                     ptr(f32(vel), ctypes.c_float), ptr(f32(restore), ctypes.c_float),
                                     self.max_types, 0, ctypes.byref(h)), "engine_init")
         self._e = h
+        _LIVE.add(self)
         frac = -1.0
         if self.max_distance is not None and self.max_distance >= 0:
             hh = self.space_info()[1]
@@ -626,6 +645,12 @@ class _Universe:
             check(lib().mxg_engine_add_flux(self._e, *f), "add_flux")
         for (p, face, t) in self._bpots:
             check(lib().mxg_engine_set_boundary_potential(self._e, face, t, p._h), "set_boundary_potential")
+        for (rep, pos, size, ang) in self._cuboids:
+            check(lib().mxg_engine_add_cuboid(self._e, rep, None if pos is None else ptr(f32(pos), ctypes.c_float),
+                                              ptr(f32(size), ctypes.c_float), ptr(f32(ang), ctypes.c_float), None),
+                  "add_cuboid")
+        for (p, t) in self._cuboid_pots:
+            check(lib().mxg_engine_set_cuboid_potential(self._e, t, p._h), "set_cuboid_potential")
         for (ii, jj) in self._exclusions:
             check(lib().mxg_engine_add_exclusions(self._e, len(ii), ptr(ii, ctypes.c_int), ptr(jj, ctypes.c_int)),
                   "add_exclusions")
@@ -793,10 +818,31 @@ class _Universe:
         new = self._add_bonds(potential, bi, bj, d) if count.value else []
         return [Bond._handle(k, potential) for k in new]
 
+    def _add_cuboid(self, pos, size, orientation, replica=0):
+        self._sync_state()
+        self._cuboids.append((int(replica), None if pos is None else [float(q) for q in pos],
+                              [float(q) for q in size], [float(q) for q in orientation]))
+        self._dirty = True
+        return len(self._cuboids) - 1
+
+    def cuboid_info(self, k):
+        """(centre, size, orientation quaternion (x, y, z, w), box min, box max) of cuboid k."""
+        self._ensure()
+        out = np.zeros(16, dtype=np.float32)
+        check(lib().mxg_engine_cuboid_info(self._e, int(k), ptr(out, ctypes.c_float)), "cuboid_info")
+        return out[0:3], out[3:6], out[6:10], out[10:13], out[13:16]
+
     def bind(self, obj, a, b=None, replica=0):
         """Binds a potential to a pair of types, to a type and a wall (a
-        BoundaryCondition face or all of BoundaryConditions), or a force to a type
-        (MxBind.cpp:18-100)."""
+        BoundaryCondition face or all of BoundaryConditions), to a type and the cuboids
+        (bind(pot, Cuboid, type)), or a force to a type (MxBind.cpp:18-100)."""
+        if isinstance(obj, Potential) and (a is Cuboid or b is Cuboid):
+            t = b if a is Cuboid else a
+            self._sync_state()
+            self._cuboid_pots = [(p, q) for (p, q) in self._cuboid_pots if q != t.id]  # one per type
+            self._cuboid_pots.append((obj, t.id if isinstance(t, type) else int(t)))
+            self._dirty = True
+            return
         walls = (BoundaryCondition, BoundaryConditions)
         if isinstance(obj, Potential) and (isinstance(a, walls) or isinstance(b, walls)):
             bc, t = (a, b) if isinstance(a, walls) else (b, a)
@@ -830,19 +876,37 @@ class _Universe:
         check(lib().mxg_engine_pot_index(self._e, int(replica), ta, tb, int(which), ctypes.byref(idx)), "pot_index")
         return idx.value
 
+    def bond_potential_indices(self, pot):
+        """The engine's indices of the copies of pot that bonds use (one per group of bonds
+        created together)."""
+        self._ensure()
+        out, first = [], 0
+        for (p, ii, jj, d) in self._bonds:
+            if p is pot and len(ii):
+                idx = ctypes.c_int()
+                check(lib().mxg_engine_bond_pot_index(self._e, first, ctypes.byref(idx)), "bond_pot_index")
+                out.append(idx.value)
+            first += len(ii)
+        return out
+
+    def set_bond_flags(self, flags):
+        """Replaces the bonds' active flags (one per bond, in creation order)."""
+        self._ensure()
+        f = np.ascontiguousarray(flags, dtype=np.uint32)
+        check(lib().mxg_engine_set_bond_flags(self._e, ptr(f, ctypes.c_uint), len(f)), "set_bond_flags")
+
     def set_potential_params(self, pot, params):
         """New construction parameters for a bound potential: the host object is
-        re-fitted on its frozen nodes and every engine copy of it is updated in place."""
+        re-fitted on its frozen nodes and every engine copy of it (type pairs and
+        bonds) is updated in place."""
         q = np.ascontiguousarray(params, dtype=np.float64)
         pot.refit(q)
         if self._e is None or self._dirty or not self._started:
             self._dirty = True
             return
-        for (p, a, b, rep, which) in self._pots:
-            if p is pot:
-                idx = self.potential_index(a, b, rep, which)
-                check(lib().mxg_engine_set_pot_params(self._e, idx, ptr(q, ctypes.c_double), len(q)),
-                      "set_pot_params")
+        idxs = [self.potential_index(a, b, rep, which) for (p, a, b, rep, which) in self._pots if p is pot]
+        for idx in idxs + self.bond_potential_indices(pot):
+            check(lib().mxg_engine_set_pot_params(self._e, idx, ptr(q, ctypes.c_double), len(q)), "set_pot_params")
 
     # ---- engine lifecycle ----
     def _sync_state(self):
@@ -898,6 +962,28 @@ class _Universe:
         check(lib().mxg_engine_step(self._e, int(n)), "engine_step")
         self.time += int(n)
         check(lib().mxg_engine_status(self._e), "engine_step")
+
+    def number_density(self):
+        """(number density by particle id, computed volume) for the current positions: the
+        reference's per-particle f[3] (W(0, cutoff) plus W(r^2, cutoff) over the pairs the
+        pair loops reach) and the sum of its inverses (engine_advance.cpp:184-185)."""
+        self._ensure()
+        n = len(self._t)
+        out = np.zeros(n, dtype=np.float32)
+        vol = ctypes.c_double()
+        check(lib().mxg_engine_number_density(self._e, n, ptr(out, ctypes.c_float), ctypes.byref(vol)),
+              "number_density")
+        return out, vol.value
+
+    def load(self, x, v=None):
+        """Replaces every particle's position (global coordinates, by id) and, when given, its
+        velocity (engine_load, engine.cpp:472-618): the particles are re-placed in their
+        cells on the device as engine_addpart places them."""
+        self._ensure()
+        xx = f64(np.asarray(x).reshape(-1, 3))
+        vv = None if v is None else f32(np.asarray(v).reshape(-1, 3))
+        check(lib().mxg_engine_load(self._e, len(xx), ptr(xx, ctypes.c_double),
+                                    None if vv is None else ptr(vv, ctypes.c_float)), "engine_load")
 
     def device_state(self):
         """Zero-copy torch views of the device-resident state in slot order (cells in order,
@@ -1059,9 +1145,19 @@ class _Universe:
         return ms.value
 
     def autotune(self):
-        """Picks the force kernel's grid by timing candidates on the current state."""
+        """Picks the force kernel's tile shape and grid by timing candidates on the current
+        state; returns the chosen CTAs per SM (force_config() gives the variant and grid)."""
         self._ensure()
         return check(lib().mxg_engine_autotune(self._e), "autotune")
+
+    def force_config(self, variant=None, grid=None):
+        """(tile variant, grid) of the force kernel; with both arguments, pins them."""
+        self._ensure()
+        vv, gg = ctypes.c_int(0 if variant is None else int(variant)), ctypes.c_int(0 if grid is None else int(grid))
+        setting = variant is not None and grid is not None
+        check(lib().mxg_engine_force_config(self._e, ctypes.byref(vv), ctypes.byref(gg), 1 if setting else 0),
+              "force_config")
+        return vv.value, gg.value
 
     def candidate_pairs(self):
         self._ensure()
@@ -1080,6 +1176,20 @@ class _UniverseNamespace:
 
     def __getattr__(self, name):
         return getattr(universe, name)
+
+
+# universes holding an engine: finalized at interpreter exit while the CUDA runtime is still up
+# (an engine left to the runtime's own teardown can outlive the context its memory belongs to)
+_LIVE = weakref.WeakSet()
+
+
+@atexit.register
+def _close_live_universes():
+    for u in list(_LIVE):
+        try:
+            u.close()
+        except Exception:
+            pass
 
 
 universe = _Universe()

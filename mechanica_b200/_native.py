@@ -31,7 +31,7 @@ ERRORS = {
     -21: "CUDA error",
     -22: "no CUDA device",
     -29: "particle moving too fast (moved more than one cell in a step)",
-    -101: "cell bucket overflow (too many particles entered one cell in a step)",
+    -101: "cell bucket overflow (no longer raised)",
     -102: "non-finite position or velocity",
     -103: "call made in the wrong engine state",
     -104: "invalid argument",
@@ -79,6 +79,9 @@ _SIGS = {
     "mxg_engine_addbonds": ([_vp, ctypes.c_int, _c_int_p, _c_int_p, _vp, ctypes.c_double, _c_int_p], ctypes.c_int),
     "mxg_engine_addangles": ([_vp, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p, _vp, _c_int_p], ctypes.c_int),
     "mxg_engine_set_boundary_potential": ([_vp, ctypes.c_int, ctypes.c_int, _vp], ctypes.c_int),
+    "mxg_engine_add_cuboid": ([_vp, ctypes.c_int, _c_float_p, _c_float_p, _c_float_p, _c_int_p], ctypes.c_int),
+    "mxg_engine_set_cuboid_potential": ([_vp, ctypes.c_int, _vp], ctypes.c_int),
+    "mxg_engine_cuboid_info": ([_vp, ctypes.c_int, _c_float_p], ctypes.c_int),
     "mxg_engine_set_type_species": ([_vp, ctypes.c_int, ctypes.c_int, _vp], ctypes.c_int),
     "mxg_engine_add_flux": ([_vp] + [ctypes.c_int] * 5 + [ctypes.c_float] * 3, ctypes.c_int),
     "mxg_engine_set_species": ([_vp, ctypes.c_int, ctypes.c_int, _c_float_p], ctypes.c_int),
@@ -105,6 +108,9 @@ _SIGS = {
     "mxg_engine_kinetic_energy": ([_vp], ctypes.c_double),
     "mxg_engine_tasks": ([_vp, _c_int_p, ctypes.c_int], ctypes.c_int),
     "mxg_engine_bond_flags": ([_vp, _c_uint_p, ctypes.c_int], ctypes.c_int),
+    "mxg_engine_set_bond_flags": ([_vp, _c_uint_p, ctypes.c_int], ctypes.c_int),
+    "mxg_engine_number_density": ([_vp, ctypes.c_int, _c_float_p, _c_double_p], ctypes.c_int),
+    "mxg_engine_bond_pot_index": ([_vp, ctypes.c_int, _c_int_p], ctypes.c_int),
     "mxg_engine_space_info": ([_vp, _c_int_p, _c_double_p, _c_int_p, _c_uint_p], ctypes.c_int),
     "mxg_engine_device_state": ([_vp, _vpp, _vpp, _vpp, _vpp], ctypes.c_int),
     "mxg_engine_copy_state": ([_vp, _vp, _vp, ctypes.c_int], ctypes.c_int),
@@ -140,6 +146,7 @@ _SIGS = {
     "mxg_engine_addparts_replica": ([_vp, ctypes.c_int, ctypes.c_int, _c_double_p, _c_float_p, _c_int_p, _c_int_p],
                                     ctypes.c_int),
     "mxg_engine_autotune": ([_vp], ctypes.c_int),
+    "mxg_engine_force_config": ([_vp, _c_int_p, _c_int_p, ctypes.c_int], ctypes.c_int),
     "mxg_kinetic_energy_noalloc": ([_vp, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp], ctypes.c_int),
 }
 

@@ -5,8 +5,8 @@ final state of an n-step run (absolute positions by particle id, float4 with
 the type in w). Its forward pass steps the engine and keeps a snapshot of the
 whole device state every K steps; its backward pass recomputes each segment
 from its snapshot, keeping the segment's per-step states, and walks back
-through them with ``mxg_engine_vjp_step`` (the adjoint of the force pass and of
-the integrator), which also accumulates d loss / d theta. The DPD random term
+through them with ``mxg_engine_vjp_step`` (the adjoint of the force pass, the
+bonds and the integrator), which also accumulates d loss / d theta. The DPD random term
 is replayed exactly: its Philox stream is keyed on the step counter, which the
 snapshots carry.
 
@@ -63,15 +63,17 @@ class Parameters:
                 self.u.set_potential_params(pot, q)
 
     def register(self):
-        """Tells the engine which (engine potential, parameter) feeds which slot."""
+        """Tells the engine which (engine potential, parameter) feeds which slot: every
+        copy of the potential bound to a type pair or used by bonds."""
         pots, params, slots = [], [], []
         for k, entries in enumerate(self.slots):
             for pot, j in entries:
-                for (p, a, b, rep, which) in self.u._pots:
-                    if p is pot:
-                        pots.append(self.u.potential_index(a, b, rep, which))
-                        params.append(j)
-                        slots.append(k)
+                idxs = [self.u.potential_index(a, b, rep, which) for (p, a, b, rep, which) in self.u._pots
+                        if p is pot]
+                for idx in idxs + self.u.bond_potential_indices(pot):
+                    pots.append(idx)
+                    params.append(j)
+                    slots.append(k)
         n = len(pots)
         arr = lambda v: (ctypes.c_int * max(1, n))(*v)
         check(lib().mxg_engine_adjoint_params(self.u.handle, n, arr(pots), arr(params), arr(slots)), "adjoint_params")
@@ -88,6 +90,8 @@ class Simulation:
         self.K = int(checkpoint_every)
         self.step0 = int(step0)
         self._bytes = None
+        # the bonds' active flags at the start: every run from (x0, v0) starts from them
+        self.bond_flags0 = universe.bond_flags() if universe._bonds else None
 
     def _engine(self):
         return self.u.handle
@@ -112,6 +116,8 @@ class Simulation:
         check(lib().mxg_engine_load(e, len(x), x.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                     v.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), "load")
         check(lib().mxg_engine_set_step_counter(e, self.step0), "set_step_counter")
+        if self.bond_flags0 is not None:
+            self.u.set_bond_flags(self.bond_flags0)
 
     def positions(self):
         """Absolute positions by id, (N, 4) float32 with the type in w; waits for the

@@ -22,9 +22,11 @@
  * The derivative of a tabulated potential is that of the piecewise polynomial
  * itself, and parameter derivatives use tables of dV/dtheta fitted on the same
  * frozen nodes (the fit is linear in the sampled function), so the gradients
- * are those of the tabulated model the forward pass integrates. Wall
- * reflections and bonds are not differentiated (the adjoint covers periodic
- * boxes and nonbonded potentials plus constant forces).
+ * are those of the tabulated model the forward pass integrates. Bonds add
+ * their terms in vjp_bond_kernel (the break flags held fixed). Wall
+ * reflections, angles, dihedrals and exclusions are not differentiated (the
+ * adjoint covers periodic boxes, nonbonded potentials, bonds and constant
+ * forces).
  */
 #include "mxg_adjoint.h"
 #include "mxg_device.cuh"
@@ -453,6 +455,86 @@ __global__ void __launch_bounds__(kWarpsA * 32, 4) vjp_pair_kernel(EngineView v,
     }
 }
 
+constexpr int kBondVjpThreads = 128;
+constexpr int kGradPad = kMaxGradSlots + 1;  // shared row stride (doubles): fewer bank conflicts
+
+/*
+ * Bond terms of the step's VJP (bond_eval, bond.cpp:99-312, with potential_eval's
+ * table semantics). One thread per particle slot visits the bonds of its
+ * particle that acted in the step's bond pass: the flags are read after that
+ * pass, so a bond broken before the step or by it contributes nothing (the
+ * break decision is a step function of the state and is held fixed). With
+ * d = x_i - x_j (x_i in x_j's cell frame, as the forward pass forms it) and
+ * f = V'(r_c)/r_c at the clamped length r_c = sqrt(clamp(|d|^2, a^2, b^2)),
+ * the bond's forces are F_i = -f d = -F_j. For u = w_i - w_j (the force
+ * adjoints) its share of the position adjoint is -A u at i and +A u at j, with
+ * A = f I + (f'(r)/r) d d^T (f' = 0 where the length is clamped). The
+ * parameter terms -(df/dtheta)(d.u) are counted once, at the bond's i end;
+ * df/dtheta comes from the tables of dV/dtheta fitted on the bond table's
+ * frozen nodes (harmonic k and r0). Parameter sums: per thread in shared
+ * memory, then per block in thread order (deterministic).
+ */
+__global__ void __launch_bounds__(kBondVjpThreads) vjp_bond_kernel(EngineView v, BondedView bv, AdjointView a) {
+    __shared__ double gsum[kBondVjpThreads * kGradPad];
+    double *g = gsum + threadIdx.x * kGradPad;
+    for (int q = 0; q < kMaxGradSlots; ++q) g[q] = 0.0;
+    const int stride = gridDim.x * blockDim.x;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < v.nparts; s += stride) {
+        const int id = __float_as_int(v.vel[s].w);
+        const int k0 = bv.bond_off[id], k1 = bv.bond_off[id + 1];
+        if (k0 == k1) continue;
+        float gx[3] = {0.f, 0.f, 0.f};
+        for (int k = k0; k < k1; ++k) {
+            const int b = bv.bond_list[k];
+            if (!(bv.bond_flags[b] & 1u)) continue;
+            const DevBond B = bv.bonds[b];
+            const int si = bv.slot_of_id[B.i], sj = bv.slot_of_id[B.j];
+            if (si < 0 || sj < 0 || si == sj) continue;
+            const int ci = v.cell_of[si];
+            const DevSpace &S = v.spaces[v.cell_rep[ci]];
+            float d[3];
+            bond_vector(S, ci, v.cell_of[sj], v.pos[si], v.pos[sj], d);
+            const DevPot &p = v.pots[B.pot];
+            const float r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+            const float a2 = p.a * p.a, b2 = p.b * p.b;
+            const bool clamped = r2 < a2 || r2 > b2;
+            const float rc = sqrtf(fmaxf(a2, fminf(b2, r2)));
+            const float t = p.alpha0 + rc * (p.alpha1 + rc * p.alpha2);
+            const int ind = min((int)fmaxf(0.0f, t), p.n);
+            const float *c = v.coef + p.coef_off + ind * kChunk;
+            const float x = (rc - c[0]) * c[1];
+            float P, dP, ddP;
+            poly3(c, x, P, dP, ddP);
+            const float vp = dP * c[1], vpp = ddP * c[1] * c[1];
+            const float f = vp / rc;
+            const float dfdr = clamped ? 0.f : vpp / rc - vp / (rc * rc);
+            const float4 wi = a.w[si], wj = a.w[sj];
+            const float u[3] = {wi.x - wj.x, wi.y - wj.y, wi.z - wj.z};
+            const float du = d[0] * u[0] + d[1] * u[1] + d[2] * u[2];
+            const float kk = dfdr / rc * du;  // r = r_c wherever dfdr is not zero
+            const float sg = s == si ? -1.f : 1.f;
+            for (int q = 0; q < 3; ++q) gx[q] += sg * (f * u[q] + kk * d[q]);
+            if (s != si) continue;
+            const DevPotGrad &pg = a.pot_grad[B.pot];
+            for (int q = 0; q < pg.n; ++q) {
+                if (pg.mode[q] != kGradTable) continue;
+                const float *cd = a.dcoef + pg.coef_off[q] + ind * kChunk;
+                float Pq, dPq, ddPq;
+                poly3(cd, x, Pq, dPq, ddPq);
+                g[pg.slot[q]] += (double)(-(dPq * c[1] / rc) * du);
+            }
+        }
+        const float4 o = a.gx[s];
+        a.gx[s] = make_float4(o.x + gx[0], o.y + gx[1], o.z + gx[2], 0.f);
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < a.nslots) {
+        double t = 0.0;
+        for (int r = 0; r < (int)blockDim.x; ++r) t += gsum[r * kGradPad + threadIdx.x];
+        a.bond_partials[(size_t)blockIdx.x * kMaxGradSlots + threadIdx.x] = t;
+    }
+}
+
 /* Per slot: the adjoints back into id order. */
 __global__ void adj_finish_kernel(EngineView v, AdjointView a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -462,12 +544,14 @@ __global__ void adj_finish_kernel(EngineView v, AdjointView a) {
     a.lam_v[id] = a.gv[s];
 }
 
-/* grad[k] += sum of the warps' partials, in warp order. */
-__global__ void adj_grad_kernel(AdjointView a, int nwarps, double *grad) {
+/* grad[k] += sum of the pair kernel's warp partials, in warp order, then of the
+ * bond kernel's block partials, in block order. */
+__global__ void adj_grad_kernel(AdjointView a, int nwarps, int nbond_blocks, double *grad) {
     const int k = threadIdx.x;
     if (k >= a.nslots) return;
     double t = 0.0;
     for (int q = 0; q < nwarps; ++q) t += a.partials[(size_t)q * kMaxGradSlots + k];
+    for (int q = 0; q < nbond_blocks; ++q) t += a.bond_partials[(size_t)q * kMaxGradSlots + k];
     grad[k] += t;
 }
 
@@ -613,6 +697,7 @@ int launch_rdf(const float4 *x, int n, const double *box, int ta, int tb, int nb
 
 int adjoint_grid(int num_sms) { return num_sms * 4; }
 int adjoint_partials(int num_sms) { return adjoint_grid(num_sms) * kWarpsA; }
+int adjoint_bond_blocks(int num_sms) { return num_sms * 2; }
 
 void configure_adjoint_kernels() {
     cudaFuncSetAttribute(vjp_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adj_smem_bytes());
@@ -620,13 +705,16 @@ void configure_adjoint_kernels() {
                          cudaSharedmemCarveoutMaxShared);
 }
 
-void launch_vjp_step(const EngineView &v, const AdjointView &a, int num_sms, double *grad, cudaStream_t st) {
+void launch_vjp_step(const EngineView &v, const AdjointView &a, const BondedView *bv, int num_sms, double *grad,
+                     cudaStream_t st) {
     const int tb = 256;
     adj_prep_kernel<<<(v.nparts + tb - 1) / tb, tb, 0, st>>>(v, a);
     const int grid = adjoint_grid(num_sms);
     vjp_pair_kernel<<<grid, kWarpsA * 32, adj_smem_bytes(), st>>>(v, a);
+    const int bblocks = bv ? adjoint_bond_blocks(num_sms) : 0;
+    if (bv) vjp_bond_kernel<<<bblocks, kBondVjpThreads, 0, st>>>(v, *bv, a);
     adj_finish_kernel<<<(v.nparts + tb - 1) / tb, tb, 0, st>>>(v, a);
-    adj_grad_kernel<<<1, 64, 0, st>>>(a, grid * kWarpsA, grad);
+    adj_grad_kernel<<<1, 64, 0, st>>>(a, grid * kWarpsA, bblocks, grad);
 }
 
 }  // namespace mxg

@@ -21,7 +21,8 @@ struct AdjointView {
     float4 *w, *gx, *gv;         // [slot] scratch: force adjoint and the partial sums
     const DevPotGrad *pot_grad;  // per potential
     const float *dcoef;          // derivative tables' coefficient pool
-    double *partials;            // [warp][kMaxGradSlots] FP64 parameter sums
+    double *partials;            // [warp][kMaxGradSlots] FP64 parameter sums of the pair terms
+    double *bond_partials;       // [block][kMaxGradSlots] FP64 parameter sums of the bond terms
     int nslots;
 };
 
@@ -30,8 +31,13 @@ void launch_positions(const EngineView &v, float4 *x_out, float4 *v_out, cudaStr
 int launch_rdf(const float4 *x, int n, const double *box, int ta, int tb, int nbins, double dr, double sigma,
                unsigned long long *hist, const double *coef, float4 *grad, cudaStream_t st);
 int adjoint_partials(int num_sms);
+/* blocks of the bond-term kernel (each writes kMaxGradSlots partial sums) */
+int adjoint_bond_blocks(int num_sms);
 void configure_adjoint_kernels();
-/* Enqueues the VJP of one step at the engine's current state, whose forces v.force must hold. */
-void launch_vjp_step(const EngineView &v, const AdjointView &a, int num_sms, double *grad, cudaStream_t st);
+/* Enqueues the VJP of one step at the engine's current state, whose forces v.force must hold
+ * (with the bond pass of that state applied when bv is not null: its flags then mark the bonds
+ * that acted in the step). */
+void launch_vjp_step(const EngineView &v, const AdjointView &a, const BondedView *bv, int num_sms, double *grad,
+                     cudaStream_t st);
 
 }  // namespace mxg

@@ -20,7 +20,9 @@
 namespace mxg {
 
 constexpr int kChunk = 8;           // floats per table interval
-constexpr int kBucket = 32;         // max particles entering one cell per step
+constexpr int kBucket = 32;         // movers per cell per step kept in the cell's bucket (more go to the overflow list)
+constexpr int kChunkShift = 8;      // the re-binning's net mover counts per chunk of 256 consecutive cells
+constexpr int kScatterWarps = 8;    // re-binning: cells (one warp each) per block
 constexpr int kMaxTypes = 64;       // types per engine
 constexpr int kWarpsPerBlock = 4;   // force kernel: warps (work items) per block
 constexpr int kMaxCellParts = 8;    // force work items per cell at most
@@ -46,8 +48,23 @@ enum : unsigned { kBcVelocity = 1u << 0, kBcPeriodic = 1u << 1, kBcFreeslip = 1u
 /* status word bits */
 enum : unsigned {
     kStatusTooFast = 1u << 0,
-    kStatusBucketOverflow = 1u << 1,
     kStatusNonFinite = 1u << 2,
+};
+
+/* device-side load (engine_load): staging arrays by particle id */
+struct LoadView {
+    const double *x;         // [3n] global positions
+    const float *v;          // [3n] velocities, or null: keep the current ones
+    const int *type_of_id;
+    const int *rep_of_id;
+    float4 *xr;              // cell-relative position, w = type bits
+    float4 *vel;             // velocity, w = id bits
+    int *cell;               // destination cell, -1 outside the replica's box
+    int *fill;               // per cell: particles placed so far
+    int *ids;                // slot -> id, before the per-cell ordering
+    int *err;                // set when a particle lies outside its box
+    const int *slot_now;     // current slot of each id (velocities kept when v is null)
+    int n;
 };
 
 struct DevPot {          // one per potential, 64 B
@@ -79,15 +96,32 @@ struct DevType {
     int bpot[6];         // wall potential per face (left, right, front, back, bottom, top), -1 if none
     unsigned wall_mask;  // active-cell bits of the faces with a wall potential
     int large;           // radius > cutoff: the reference's PARTICLE_LARGE (static, interacts with all)
+    int cpot;            // potential between this type and the cuboids (engine_add_cuboid_potential), -1 if none
+    int pad3;
+};
+
+/* A static cuboid (MxCuboid, MxCuboid.hpp; a body with a box shape): centre, half extents,
+ * orientation and its inverse as quaternions (x, y, z, w), its axis-aligned bounding box as
+ * MxCuboid_UpdateAABB (MxCuboid.cpp:190-221) forms it, and its replica. */
+struct DevCuboid {
+    float pos[3];
+    float size[3];
+    float q[4];
+    float qi[4];
+    float lo[3], hi[3];
+    int rep;
+    int pad;
 };
 
 struct DevSpace {        // one per replica
     double origin[3];    // the box's lower corner
     double hd[3];        // cell size (double, as space.h keeps it)
+    double ih[3];        // 1 / cell size (double)
     float h[3], h2[3];   // float(h), float(2h)
     float maxv[3], maxv2[3], maxx[3], maxx2[3];
     float dt;
     float cut2_pair, cut2_self;
+    float cut2w_pair, cut2w_self;  // the candidate pass's widened cutoffs (covers the one rounding it skips)
     int cdim[3];
     int cell_offset;
     int ncells;
@@ -217,7 +251,15 @@ struct EngineView {      // everything a kernel needs, passed by value
     int *item_ctr;           // [0] next work item, [1] warps done (dynamic fetch; zero between launches)
     int *item_order;         // items by decreasing cell occupancy (split cells only), else null
     int dpd_pure;            // every pair potential is DPD with the reference's random term: DPD-only kernel
+    int force_variant;       // the force kernel's tile shape (see Tile), chosen by the autotuner
     int nitems;
+    const DevCuboid *cuboids;  // static cuboids (all replicas)
+    int ncuboids;
+    const float4 *dpd_pair;  // DPD-only kernel, per replica and type pair: (rc, alpha, gamma, sigma delta),
+                             // (a^2, a, 1/rc, alpha + sigma delta); null otherwise
+    int *ovf_list;           // movers beyond their destination's bucket this step: old slot (capacity nparts)
+    int *ovf_count;          // entries of ovf_list (re-armed by the re-binning launch)
+    int *chunk_delta;        // per chunk of 1 << kChunkShift cells: movers in minus movers out this step
 };
 
 #ifdef __CUDACC__
@@ -245,6 +287,35 @@ __device__ __forceinline__ uint4 philox4x32(uint4 c, uint2 k) {
 __device__ __forceinline__ int sort_key(float x, float y, float z, const float *n, float bias, float dscale) {
     const float proj = __fadd_rn(__fadd_rn(__fadd_rn(bias, __fmul_rn(x, n[0])), __fmul_rn(y, n[1])), __fmul_rn(z, n[2]));
     return (int)(unsigned)__fmul_rn(dscale, proj);
+}
+
+/* Cell coordinates of global cell c in its replica's grid. */
+__device__ __forceinline__ void cell_loc(const DevSpace &S, int c, int loc[3]) {
+    const int l = c - S.cell_offset;
+    loc[0] = l / (S.cdim[1] * S.cdim[2]);
+    loc[1] = (l / S.cdim[2]) % S.cdim[1];
+    loc[2] = l % S.cdim[2];
+}
+
+/* The bonded code's neighbour-cell shift (bond.cpp:163-170, angle.cpp:155-168):
+ * a cell difference of more than one is a periodic wrap. */
+__device__ __forceinline__ int wrap_shift(int d) { return d > 1 ? -1 : (d < -1 ? 1 : d); }
+
+/* x + shift*h formed in double and rounded to float, as the reference writes
+ * the double product into a float position. */
+__device__ __forceinline__ float shifted(float x, int sh, double h) {
+    return (float)__dadd_rn((double)x, __dmul_rn(h, (double)sh));
+}
+
+/* The bond vector d = x_i - x_j of bond_eval (bond.cpp:163-178): x_i moved into
+ * x_j's cell frame by the wrapped cell shift, in the reference's rounding. */
+__device__ __forceinline__ void bond_vector(const DevSpace &S, int ci, int cj, const float4 &xi, const float4 &xj,
+                                            float d[3]) {
+    int loci[3], locj[3];
+    cell_loc(S, ci, loci);
+    cell_loc(S, cj, locj);
+    const float xiv[3] = {xi.x, xi.y, xi.z}, xjv[3] = {xj.x, xj.y, xj.z};
+    for (int q = 0; q < 3; ++q) d[q] = __fsub_rn(shifted(xiv[q], wrap_shift(loci[q] - locj[q]), S.hd[q]), xjv[q]);
 }
 
 /* uniform in (0,1) from 32 random bits */

@@ -29,6 +29,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <numeric>
 #include <vector>
@@ -84,7 +85,80 @@ struct TypeInfo {
     float sb[4] = {0, 0, 0, 0};  // Berendsen: tau; random: mean, std, duration; friction: coef, mean, std, duration
     double target = 0.0;        // target temperature (Berendsen)
     int bpot[6] = {-1, -1, -1, -1, -1, -1};  // wall potential per face (index into pots), -1 if none
+    int cpot = -1;                           // potential with the cuboids (index into pots), -1 if none
 };
+
+/* A static cuboid: centre, size, orientation qx qy qz from the three angles, its
+ * inverse and its axis-aligned bounding box, in the reference's float arithmetic
+ * (cuboid_init and MxCuboid_UpdateAABB, MxCuboid.cpp:40-76 and 190-221). */
+struct CuboidInfo {
+    int rep;
+    float pos[3], size[3], q[4], qi[4], lo[3], hi[3];
+};
+
+/* quaternion product (x, y, z, w) as the vector form forms it: b.v a.w + a.v b.w + a.v x b.v,
+ * a.w b.w - a.v . b.v */
+void quat_mul_host(const float *a, const float *b, float *o) {
+    const float cx = a[1] * b[2] - a[2] * b[1], cy = a[2] * b[0] - a[0] * b[2], cz = a[0] * b[1] - a[1] * b[0];
+    float r[4];
+    r[0] = (b[0] * a[3] + a[0] * b[3]) + cx;
+    r[1] = (b[1] * a[3] + a[1] * b[3]) + cy;
+    r[2] = (b[2] * a[3] + a[2] * b[3]) + cz;
+    r[3] = a[3] * b[3] - ((a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]);
+    for (int k = 0; k < 4; ++k) o[k] = r[k];
+}
+
+void quat_rotate_host(const float *q, const float *v, float *out) {
+    const float p[4] = {v[0], v[1], v[2], 0.f}, qc[4] = {-q[0], -q[1], -q[2], q[3]};
+    float t[4], r[4];
+    quat_mul_host(q, p, t);
+    quat_mul_host(t, qc, r);
+    for (int k = 0; k < 3; ++k) out[k] = r[k];
+}
+
+CuboidInfo make_cuboid(int rep, const float *pos, const float *size, const float *angles) {
+    CuboidInfo c;
+    c.rep = rep;
+    for (int k = 0; k < 3; ++k) {
+        c.pos[k] = pos[k];
+        c.size[k] = size[k];
+    }
+    // Quaternion::rotation(angle, axis) = (axis sin(angle / 2), cos(angle / 2)); orientation = qx qy qz
+    float qa[3][4];
+    for (int k = 0; k < 3; ++k) {
+        const float half = angles[k] / 2;
+        for (int q = 0; q < 3; ++q) qa[k][q] = q == k ? std::sin(half) : 0.f * std::sin(half);
+        qa[k][3] = std::cos(half);
+    }
+    float qxy[4];
+    quat_mul_host(qa[0], qa[1], qxy);
+    quat_mul_host(qxy, qa[2], c.q);
+    // inverted() = conjugated() / dot()
+    const float dot = ((c.q[0] * c.q[0] + c.q[1] * c.q[1]) + c.q[2] * c.q[2]) + c.q[3] * c.q[3];
+    for (int q = 0; q < 3; ++q) c.qi[q] = -c.q[q] / dot;
+    c.qi[3] = c.q[3] / dot;
+    // bounding box of the eight rotated corners; the upper bound starts at the smallest positive
+    // float, as the reference initialises it
+    float half[3];
+    for (int k = 0; k < 3; ++k) {
+        half[k] = 0.5f * size[k];
+        c.lo[k] = std::numeric_limits<float>::max();
+        c.hi[k] = std::numeric_limits<float>::min();
+    }
+    const float sgn[8][3] = {{1, 1, 1}, {1, -1, 1}, {-1, -1, 1}, {-1, 1, 1},
+                             {1, 1, -1}, {1, -1, -1}, {-1, -1, -1}, {-1, 1, -1}};
+    for (int i = 0; i < 8; ++i) {
+        const float corner[3] = {sgn[i][0] * half[0], sgn[i][1] * half[1], sgn[i][2] * half[2]};
+        float r[3];
+        quat_rotate_host(c.q, corner, r);
+        for (int k = 0; k < 3; ++k) {
+            const float pt = r[k] + pos[k];
+            c.lo[k] = std::min(c.lo[k], pt);
+            c.hi[k] = std::max(c.hi[k], pt);
+        }
+    }
+    return c;
+}
 
 struct BondInfo {
     int i, j, pot;
@@ -353,6 +427,7 @@ struct mxg_engine {
     std::vector<AngleInfo> angles;
     std::vector<ExclusionInfo> exclusions;
     std::vector<DihedralInfo> dihedrals;
+    std::vector<CuboidInfo> cuboids;
     // ---- species and fluxes ----
     std::vector<int> type_nspec;               // per type (0: no state vector)
     std::vector<std::vector<unsigned>> type_sflags;  // per type and species (bit 2: constant)
@@ -378,7 +453,20 @@ struct mxg_engine {
     int *d_cell_of[2] = {nullptr, nullptr};
     int *d_new_cell = nullptr;
     int *d_cell_start[2] = {nullptr, nullptr}, *d_cell_count[2] = {nullptr, nullptr};
-    int *d_in_count = nullptr, *d_out_count = nullptr, *d_in_list = nullptr;
+    // movers per cell and per chunk of cells, by step parity: a step counts into its own parity and
+    // its re-binning clears the other one, so the counts of the parity about to step are zero
+    int *d_in_count[2] = {nullptr, nullptr}, *d_out_count[2] = {nullptr, nullptr};
+    int *d_chunk_delta[2] = {nullptr, nullptr};
+    int nchunks = 0;
+    int *d_in_list = nullptr;
+    int *d_ovf_list = nullptr, *d_ovf_count = nullptr;  // movers beyond their destination's bucket
+    unsigned *d_rebin_ctl = nullptr;                    // re-binning: finished blocks of the scatter
+    // device-side load and unload (allocated at the first call)
+    double *d_ld_x = nullptr, *d_ul_x = nullptr;
+    float *d_ld_v = nullptr, *d_ul_v = nullptr, *d_ul_f = nullptr, *d_ul_xrel = nullptr;
+    float4 *d_ld_xr = nullptr, *d_ld_vel = nullptr;
+    int *d_ld_cell = nullptr, *d_ld_ids = nullptr, *d_ld_count = nullptr, *d_ld_fill = nullptr, *d_ld_err = nullptr;
+    int *d_type_of_id = nullptr, *d_rep_of_id = nullptr, *d_ul_cell = nullptr;
     int *d_slot_of_id = nullptr;
     int *d_cell_rep = nullptr;
     unsigned *d_cell_flags = nullptr;
@@ -397,6 +485,8 @@ struct mxg_engine {
     float *d_coef = nullptr;
     int *d_pot_idx = nullptr;
     int *d_pot_idx2 = nullptr;   // second summed potential per type pair, or -1
+    float4 *d_dpd_pair = nullptr;  // DPD-only kernel: two records per replica and type pair
+    std::vector<int> h_pot_idx;    // the device's potential index per replica and type pair
     bool has_second = false;
     DevType *d_types = nullptr;
     DevSpace *d_spaces = nullptr;
@@ -417,7 +507,10 @@ struct mxg_engine {
     size_t dcoef_cap = 0;
     float4 *d_adj_w = nullptr, *d_adj_gx = nullptr, *d_adj_gv = nullptr;
     double *d_adj_partials = nullptr;
+    double *d_adj_bond_partials = nullptr;
     double *d_virial_partials = nullptr, *d_virial_out = nullptr;
+    double *d_bvirial_partials = nullptr;  // bonded virial: per block, 9 components
+    float *d_nd = nullptr;                  // number density by id (allocated at the first request)
     int virial_cap = 0;
     int *d_bond_off = nullptr, *d_bond_list = nullptr;
     int2 *d_excl = nullptr;
@@ -438,13 +531,16 @@ struct mxg_engine {
     int *d_large_rep = nullptr, *d_large_pot = nullptr;
     double *d_body_e = nullptr;         // per slot: wall and large-particle energy of the last pass
     float4 *d_body_f = nullptr;         // per slot: wall and large-particle force of the pass
-    bool has_body() const { return has_walls || nlarge > 0; }
+    bool has_cuboid_forces = false;     // a cuboid exists and a type has a cuboid potential
+    DevCuboid *d_cuboids = nullptr;
+    bool has_body() const { return has_walls || nlarge > 0 || has_cuboid_forces; }
     double *d_type_ke = nullptr;
     float4 *d_persist = nullptr;
     int integrator = 0;                 // 0 forward Euler, 1 Runge-Kutta 4 (engine.h EngineIntegrator)
     int force_layout = 0;               // the buffer whose slot order the force array follows
     float4 *d_rk[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // RK4 per-slot stage state
     int force_grid = 0;
+    int force_variant = 0;              // tile shape of the force kernel (autotuned)
     int num_sms = 148;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool use_graphs = true;
@@ -455,6 +551,21 @@ struct mxg_engine {
             if (graph[k]) cudaGraphExecDestroy(graph[k]);
         for (void *p : allocations) cudaFree(p);
         if (own_stream) cudaStreamDestroy(own_stream);
+    }
+
+    /* The DPD-only kernel's constants, two records per replica and type pair (see
+     * EngineView::dpd_pair); one empty record when that kernel is not used. */
+    std::vector<float4> dpd_records(const std::vector<DevPot> &hp) const {
+        std::vector<float4> out(dpd_pure ? 2 * h_pot_idx.size() : 1, make_float4(0.f, 0.f, 0.f, 0.f));
+        if (!dpd_pure) return out;
+        for (size_t k = 0; k < h_pot_idx.size(); ++k) {
+            if (h_pot_idx[k] < 0) continue;
+            const DevPot &d = hp[h_pot_idx[k]];
+            const float sd = d.dpd_sigma * d.dpd_delta;
+            out[2 * k] = make_float4(d.b, d.dpd_alpha, d.dpd_gamma, sd);
+            out[2 * k + 1] = make_float4(d.a2, d.a, 1.0f / d.b, d.dpd_alpha + sd);
+        }
+        return out;
     }
 
     /* Device form of the potentials: one DevPot each and the pooled coefficients. */
@@ -500,6 +611,7 @@ struct mxg_engine {
         const float dtf = (float)dt;
         for (int k = 0; k < 3; ++k) {
             S.hd[k] = sp.h[k];
+            S.ih[k] = sp.ih[k];
             S.h[k] = (float)sp.h[k];
             S.h2[k] = (float)(2. * sp.h[k]);
             S.maxv[k] = (S.h[k] * max_dist_fraction) / dtf;
@@ -515,6 +627,12 @@ struct mxg_engine {
         const float cf = (float)cutoff;
         S.cut2_pair = cf * cf;                  // runner_dopair: float cutoff squared
         S.cut2_self = (float)(cutoff * cutoff);  // runner_doself: s->cutoff2 (double) as float
+        // the candidate pass forms x_i - (x_j + s) instead of (x_i - s) - x_j: one rounding of
+        // coordinates below 2h apart, covered by a margin far above it (the exact test follows)
+        const double hmax = std::max(sp.h[0], std::max(sp.h[1], sp.h[2]));
+        const double margin = 2e-5 * (3 * hmax * hmax + cutoff * cutoff);
+        S.cut2w_pair = (float)((double)S.cut2_pair + margin);
+        S.cut2w_self = (float)((double)S.cut2_self + margin);
         S.cell_offset = sp.cell_offset;
         S.ncells = sp.ncells;
         S.pot_offset = pot_offset;
@@ -611,15 +729,22 @@ struct mxg_engine {
         v.item_ctr = d_item_ctr;
         v.item_order = order_items ? d_item_order : nullptr;
         v.dpd_pure = dpd_pure ? 1 : 0;
+        v.force_variant = force_variant;
         v.nitems = nitems;
         v.planes = d_planes;
-        v.body_e = (has_walls || nlarge) ? d_body_e : nullptr;
-        v.body_f = (has_walls || nlarge) ? d_body_f : nullptr;
+        v.body_e = has_body() ? d_body_e : nullptr;
+        v.body_f = has_body() ? d_body_f : nullptr;
         v.large_x = d_large_x;
         v.large_v = d_large_v;
         v.large_rep = d_large_rep;
         v.large_pot = d_large_pot;
         v.nlarge = nlarge;
+        v.cuboids = d_cuboids;
+        v.ncuboids = has_cuboid_forces ? (int)cuboids.size() : 0;
+        v.dpd_pair = dpd_pure ? d_dpd_pair : nullptr;
+        v.chunk_delta = d_chunk_delta[b];
+        v.ovf_list = d_ovf_list;
+        v.ovf_count = d_ovf_count;
         return v;
     }
 
@@ -694,7 +819,6 @@ struct mxg_engine {
             mark(5);
             return;
         }
-        const int nb = 1 - b;
         const EngineView v = view(b);
         mark(0);
         if (has_sb) launch_singlebody_prep(v, ntypes, d_type_ke, d_persist, true, stream);
@@ -705,15 +829,20 @@ struct mxg_engine {
         if (has_bonded()) launch_bonded(v, bonded_view(), stream);
         if (has_fluxes) launch_fluxes(v, species_view(), stream);
         mark(3);
-        launch_integrate(v, d_pos[b], d_vel[b], d_new_cell, d_in_count, d_in_list, d_out_count, !has_bonded(),
+        launch_integrate(v, d_pos[b], d_vel[b], d_new_cell, d_in_count[b], d_in_list, d_out_count[b], !has_bonded(),
                          stream);
         if (has_fluxes) launch_species_integrate(v, species_view(), d_new_cell, stream);  // MxFluxes_Integrate
         mark(4);
-        launch_scan(ncells, d_cell_count[b], d_out_count, d_in_count, d_cell_start[nb], d_cell_count[nb], d_step,
-                    stream);
-        launch_scatter(v, d_pos[b], d_vel[b], d_new_cell, d_cell_start[b], d_cell_count[b], d_in_count, d_in_list,
-                       d_out_count, d_cell_start[nb], d_pos[nb], d_vel[nb], d_cell_of[nb], d_slot_of_id, stream);
+        enqueue_scatter(v, b);
         mark(5);
+    }
+
+    void enqueue_scatter(const EngineView &v, int b) {
+        const int nb = 1 - b;
+        launch_scatter(v, d_pos[b], d_vel[b], d_new_cell, d_cell_start[b], d_cell_count[b], d_in_count[b], d_in_list,
+                       d_out_count[b], d_cell_start[nb], d_cell_count[nb], d_pos[nb], d_vel[nb], d_cell_of[nb],
+                       d_slot_of_id, d_in_count[nb], d_out_count[nb], d_chunk_delta[nb], nchunks, d_rebin_ctl,
+                       d_step, stream);
     }
 
     /* One Runge-Kutta 4 step (engine_advance_runge_kutta_4): four force passes (with
@@ -721,7 +850,6 @@ struct mxg_engine {
      * bounds before each intermediate pass, then the final update, re-binning as
      * for Euler. */
     void enqueue_step_rk4(int b) {
-        const int nb = 1 - b;
         const EngineView v = view(b);
         for (int stage = 0; stage < 4; ++stage) {
             // persistent random forces are redrawn in the first stage only (INTEGRATOR_UPDATE_PERSISTENTFORCE)
@@ -733,14 +861,11 @@ struct mxg_engine {
                 launch_rk_stage(v, d_pos[b], d_rk, stage, !has_bonded(), stream);
                 launch_sort_bounds(v, stream);
             } else {
-                launch_rk_final(v, d_pos[b], d_vel[b], d_rk, d_new_cell, d_in_count, d_in_list, d_out_count,
+                launch_rk_final(v, d_pos[b], d_vel[b], d_rk, d_new_cell, d_in_count[b], d_in_list, d_out_count[b],
                                 !has_bonded(), stream);
             }
         }
-        launch_scan(ncells, d_cell_count[b], d_out_count, d_in_count, d_cell_start[nb], d_cell_count[nb], d_step,
-                    stream);
-        launch_scatter(v, d_pos[b], d_vel[b], d_new_cell, d_cell_start[b], d_cell_count[b], d_in_count, d_in_list,
-                       d_out_count, d_cell_start[nb], d_pos[nb], d_vel[nb], d_cell_of[nb], d_slot_of_id, stream);
+        enqueue_scatter(v, b);
     }
 
     /* Key bounds for a state that did not come from the re-binning pass. */
@@ -779,6 +904,7 @@ struct mxg_engine {
             rc |= alloc(&d_adj_gx, (size_t)nparts);
             rc |= alloc(&d_adj_gv, (size_t)nparts);
             rc |= alloc(&d_adj_partials, (size_t)adjoint_partials(num_sms) * kMaxGradSlots);
+            rc |= alloc(&d_adj_bond_partials, (size_t)adjoint_bond_blocks(num_sms) * kMaxGradSlots);
             if (rc != MXG_OK) return MXG_ERR_MALLOC;
             configure_adjoint_kernels();
         }
@@ -1029,12 +1155,16 @@ int mxg_engine::start(cudaStream_t st) {
             }
     dpd_pure = has_dpd && rng_mode == 0;
     for (int k : hpidx)
-        if (k >= 0 && pots[k].kind != kKindDPD) dpd_pure = false;
+        if (k >= 0 && (pots[k].kind != kKindDPD || (pots[k].flags & kFlagShifted))) dpd_pure = false;
     for (int k : hpidx2)
         if (k >= 0) dpd_pure = false;
+    h_pot_idx = hpidx;
+    const std::vector<float4> hdpd = dpd_records(hp);
     has_sb = false;
     has_walls = false;
+    has_cuboid_forces = false;
     std::vector<DevType> ht(ntypes);
+    for (DevType &d : ht) d.cpot = -1;
     for (int a = 0; a < (int)types.size(); ++a) {
         DevType &d = ht[a];
         memset(&d, 0, sizeof(d));
@@ -1064,6 +1194,8 @@ int mxg_engine::start(cudaStream_t st) {
             d.large = 1;
             d.flags |= (1u << 2) | (1u << 3) | (1u << 4);  // never integrated (not in any cell of the reference)
         }
+        d.cpot = is_large[a] ? -1 : ti.cpot;
+        if (d.cpot >= 0 && !cuboids.empty()) has_cuboid_forces = true;
         const unsigned face_bits[6] = {kCellActiveLeft, kCellActiveRight, kCellActiveFront,
                                        kCellActiveBack, kCellActiveBottom, kCellActiveTop};
         for (int f = 0; f < 6; ++f) {
@@ -1189,9 +1321,16 @@ int mxg_engine::start(cudaStream_t st) {
     if (integrator == 1)
         for (int k = 0; k < 5; ++k) rc |= alloc(&d_rk[k], nparts);
     rc |= alloc(&d_new_cell, nparts);
-    rc |= alloc(&d_in_count, ncells);
-    rc |= alloc(&d_out_count, ncells);
+    nchunks = (ncells + (1 << kChunkShift) - 1) >> kChunkShift;
+    for (int p = 0; p < 2; ++p) {
+        rc |= alloc(&d_in_count[p], ncells);
+        rc |= alloc(&d_out_count[p], ncells);
+        rc |= alloc(&d_chunk_delta[p], nchunks);
+    }
     rc |= alloc(&d_in_list, (size_t)ncells * kBucket);
+    rc |= alloc(&d_ovf_list, (size_t)nparts);
+    rc |= alloc(&d_ovf_count, 1);
+    rc |= alloc(&d_rebin_ctl, 1);
     rc |= alloc(&d_slot_of_id, nparts);
     rc |= alloc(&d_cell_rep, ncells);
     rc |= alloc(&d_cell_flags, ncells);
@@ -1209,6 +1348,25 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_coef, coef.size() + 8);
     rc |= alloc(&d_pot_idx, hpidx.size());
     rc |= alloc(&d_pot_idx2, hpidx2.size());
+    rc |= alloc(&d_dpd_pair, hdpd.size());
+    std::vector<DevCuboid> hcub;
+    for (const CuboidInfo &ci : cuboids) {
+        DevCuboid d;
+        memset(&d, 0, sizeof(d));
+        for (int k = 0; k < 3; ++k) {
+            d.pos[k] = ci.pos[k];
+            d.size[k] = ci.size[k];
+            d.lo[k] = ci.lo[k];
+            d.hi[k] = ci.hi[k];
+        }
+        for (int k = 0; k < 4; ++k) {
+            d.q[k] = ci.q[k];
+            d.qi[k] = ci.qi[k];
+        }
+        d.rep = ci.rep;
+        hcub.push_back(d);
+    }
+    rc |= alloc(&d_cuboids, hcub.size());
     rc |= alloc(&d_types, ht.size());
     rc |= alloc(&d_type_ke, ht.size());
     rc |= alloc(&d_persist, (size_t)nparts);
@@ -1251,8 +1409,13 @@ int mxg_engine::start(cudaStream_t st) {
     rc |= alloc(&d_energy, 2);
     if (rc != MXG_OK) return MXG_ERR_MALLOC;
 
-    CUDA_TRY(cudaMemsetAsync(d_in_count, 0, sizeof(int) * ncells, stream));
-    CUDA_TRY(cudaMemsetAsync(d_out_count, 0, sizeof(int) * ncells, stream));
+    for (int p = 0; p < 2; ++p) {
+        CUDA_TRY(cudaMemsetAsync(d_in_count[p], 0, sizeof(int) * ncells, stream));
+        CUDA_TRY(cudaMemsetAsync(d_out_count[p], 0, sizeof(int) * ncells, stream));
+        CUDA_TRY(cudaMemsetAsync(d_chunk_delta[p], 0, sizeof(int) * nchunks, stream));
+    }
+    CUDA_TRY(cudaMemsetAsync(d_ovf_count, 0, sizeof(int), stream));
+    CUDA_TRY(cudaMemsetAsync(d_rebin_ctl, 0, sizeof(unsigned), stream));
     CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
     CUDA_TRY(cudaMemsetAsync(d_step, 0, sizeof(unsigned long long), stream));
     CUDA_TRY(cudaMemsetAsync(d_item_ctr, 0, 2 * sizeof(int), stream));
@@ -1272,7 +1435,8 @@ int mxg_engine::start(cudaStream_t st) {
         (rc = upload(d_sec_count, hsec, stream)) || (rc = upload(d_cell_planes, hplanes, stream)) ||
         (rc = upload(d_items, hitems, stream)) || (rc = upload(d_pots, hp, stream)) ||
         (rc = upload(d_coef, coef, stream)) || (rc = upload(d_pot_idx, hpidx, stream)) ||
-        (rc = upload(d_pot_idx2, hpidx2, stream)) ||
+        (rc = upload(d_pot_idx2, hpidx2, stream)) || (rc = upload(d_dpd_pair, hdpd, stream)) ||
+        (rc = upload(d_cuboids, hcub, stream)) ||
         (rc = upload(d_types, ht, stream)) || (rc = upload(d_spaces, hs, stream)) || (rc = upload(d_axes, haxes, stream)) ||
         (rc = upload(d_bonds, hb, stream)) || (rc = upload(d_bond_flags, hbf, stream)) ||
         (rc = upload(d_bond_off, boff, stream)) || (rc = upload(d_bond_list, blist, stream)) ||
@@ -1316,24 +1480,58 @@ int mxg_engine::build_graphs() {
     return MXG_OK;
 }
 
-/* Re-places all particles from global positions (per id) and velocities. */
+/* Re-places all particles from global positions (per id) and velocities (per id, or the
+ * current ones when v is null), on the device: the host arrays are copied once and the
+ * placement, counting, scan and (cell, id) ordering run as kernels with the host
+ * placement's arithmetic. A particle outside its box leaves the state unchanged and returns
+ * MXG_ERR_SPACE. */
 int mxg_engine::load_state(const double *x, const float *v, int n) {
     if (n != nparts) return MXG_ERR_ARG;
-    for (int p = 0; p < n; ++p) {
-        for (int k = 0; k < 3; ++k) px[3 * (size_t)p + k] = x[3 * (size_t)p + k];
-        if (v)
-            for (int k = 0; k < 3; ++k) pv[3 * (size_t)p + k] = v[3 * (size_t)p + k];
+    if (nparts == 0) return MXG_OK;
+    if (!d_ld_x) {
+        int rc = alloc(&d_ld_x, 3 * (size_t)nparts);
+        rc |= alloc(&d_ld_v, 3 * (size_t)nparts);
+        rc |= alloc(&d_ld_xr, (size_t)nparts);
+        rc |= alloc(&d_ld_vel, (size_t)nparts);
+        rc |= alloc(&d_ld_cell, (size_t)nparts);
+        rc |= alloc(&d_ld_ids, (size_t)nparts);
+        rc |= alloc(&d_ld_count, (size_t)ncells);
+        rc |= alloc(&d_ld_fill, (size_t)ncells);
+        rc |= alloc(&d_ld_err, 1);
+        rc |= alloc(&d_type_of_id, (size_t)nparts);
+        rc |= alloc(&d_rep_of_id, (size_t)nparts);
+        if (rc != MXG_OK) return MXG_ERR_MALLOC;
+        if ((rc = upload(d_type_of_id, ptype, stream)) || (rc = upload(d_rep_of_id, prep, stream))) return rc;
     }
-    std::vector<float4> hpos, hvel;
-    std::vector<int> hcell_of, hslot, hcount, hstart;
-    int rc = stage(hpos, hvel, hcell_of, hslot, hcount, hstart);
-    if (rc != MXG_OK) return rc;
-    if ((rc = upload(d_pos[cur], hpos, stream)) || (rc = upload(d_vel[cur], hvel, stream)) ||
-        (rc = upload(d_cell_of[cur], hcell_of, stream)) || (rc = upload(d_cell_start[cur], hstart, stream)) ||
-        (rc = upload(d_cell_count[cur], hcount, stream)) || (rc = upload(d_slot_of_id, hslot, stream)))
-        return rc;
-    refresh_bounds();
-    CUDA_TRY(cudaStreamSynchronize(stream));
+    CUDA_TRY(cudaMemcpyAsync(d_ld_x, x, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, stream));
+    if (v) CUDA_TRY(cudaMemcpyAsync(d_ld_v, v, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaMemsetAsync(d_ld_count, 0, sizeof(int) * (size_t)ncells, stream));
+    CUDA_TRY(cudaMemsetAsync(d_ld_fill, 0, sizeof(int) * (size_t)ncells, stream));
+    CUDA_TRY(cudaMemsetAsync(d_ld_err, 0, sizeof(int), stream));
+    LoadView ld;
+    ld.x = d_ld_x;
+    ld.v = v ? d_ld_v : nullptr;
+    ld.type_of_id = d_type_of_id;
+    ld.rep_of_id = d_rep_of_id;
+    ld.xr = d_ld_xr;
+    ld.vel = d_ld_vel;
+    ld.cell = d_ld_cell;
+    ld.fill = d_ld_fill;
+    ld.ids = d_ld_ids;
+    ld.err = d_ld_err;
+    ld.slot_now = d_slot_of_id;
+    ld.n = n;
+    const EngineView ev = view(cur);
+    launch_load_place(ev, ld, d_ld_count, stream);
+    int err = 0;
+    CUDA_TRY(cudaMemcpyAsync(&err, d_ld_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CUDA_TRY(cudaStreamSynchronize(stream));  // also: the caller's host arrays are free again
+    if (err) return MXG_ERR_SPACE;
+    CUDA_TRY(cudaMemcpyAsync(d_cell_count[cur], d_ld_count, sizeof(int) * (size_t)ncells, cudaMemcpyDeviceToDevice,
+                             stream));
+    launch_load_order(ev, ld, d_ld_count, d_cell_start[cur], d_pos[cur], d_vel[cur], d_cell_of[cur], d_slot_of_id,
+                      stream);
+    CUDA_TRY(cudaGetLastError());
     return MXG_OK;
 }
 
@@ -1644,7 +1842,11 @@ int mxg_engine_set_pot_params(mxg_engine *e, int idx, const double *params, int 
     std::vector<DevPot> hp;
     std::vector<float> coef;
     e->pot_arrays(hp, coef);  // same sizes: a frozen-node refit keeps every table's length
-    if ((rc = upload(e->d_pots, hp, e->stream)) || (rc = upload(e->d_coef, coef, e->stream))) return rc;
+    const std::vector<float4> hdpd = e->dpd_records(hp);
+    if ((rc = upload(e->d_pots, hp, e->stream)) || (rc = upload(e->d_coef, coef, e->stream)) ||
+        (rc = upload(e->d_dpd_pair, hdpd, e->stream)))
+        return rc;
+    CUDA_TRY(cudaStreamSynchronize(e->stream));  // the host vectors go out of scope
     return MXG_OK;
 }
 
@@ -1780,6 +1982,41 @@ int mxg_engine_group_metrics(mxg_engine *e, int n, const int *ids, double *out) 
     cudaFree(d_ids);
     cudaFree(d_out);
     return err == cudaSuccess ? MXG_OK : MXG_ERR_CUDA;
+}
+
+int mxg_engine_add_cuboid(mxg_engine *e, int rep, const float *pos, const float *size, const float *angles, int *id) {
+    if (!e || !size || !angles) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    if (rep < 0 || rep >= (int)e->spaces.size()) return MXG_ERR_RANGE;
+    float centre[3];
+    for (int k = 0; k < 3; ++k) centre[k] = pos ? pos[k] : (float)e->spaces[rep].dim[k] / 2.f;  // engine_center
+    e->cuboids.push_back(make_cuboid(rep, centre, size, angles));
+    if (id) *id = (int)e->cuboids.size() - 1;
+    return MXG_OK;
+}
+
+int mxg_engine_set_cuboid_potential(mxg_engine *e, int type, const mxg_potential *p) {
+    if (!e || !p) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    if (type < 0 || type >= (int)e->types.size()) return MXG_ERR_RANGE;
+    if (p->t.kind != kKindTable) return MXG_ERR_POTENTIAL;
+    e->pots.push_back(p->t);
+    e->types[type].cpot = (int)e->pots.size() - 1;
+    return MXG_OK;
+}
+
+int mxg_engine_cuboid_info(const mxg_engine *e, int id, float *out16) {
+    if (!e || !out16) return MXG_ERR_NULL;
+    if (id < 0 || id >= (int)e->cuboids.size()) return MXG_ERR_RANGE;
+    const CuboidInfo &c = e->cuboids[id];
+    for (int k = 0; k < 3; ++k) {
+        out16[k] = c.pos[k];
+        out16[3 + k] = c.size[k];
+        out16[10 + k] = c.lo[k];
+        out16[13 + k] = c.hi[k];
+    }
+    for (int k = 0; k < 4; ++k) out16[6 + k] = c.q[k];
+    return MXG_OK;
 }
 
 int mxg_engine_set_boundary_potential(mxg_engine *e, int face, int type, const mxg_potential *p) {
@@ -1957,7 +2194,6 @@ int mxg_engine_status(mxg_engine *e) {
     unsigned st = 0;
     CUDA_TRY(cudaMemcpy(&st, e->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
     if (st & kStatusNonFinite) return MXG_ERR_NONFINITE;
-    if (st & kStatusBucketOverflow) return MXG_ERR_CELL_OVERFLOW;
     if (st & kStatusTooFast) return MXG_ERR_TOOFAST;
     return MXG_OK;
 }
@@ -1975,46 +2211,27 @@ int mxg_engine_nr_cells(const mxg_engine *e) { return e ? e->ncells : MXG_ERR_NU
 int mxg_engine_unload(mxg_engine *e, int n, double *x, float *v, float *f, int *cell, float *xrel) {
     if (!e) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
-    if (n > e->nparts) return MXG_ERR_RANGE;
-    const int N = e->nparts;
-    std::vector<float4> hp(N), hv(N), hf(N), hfv(N);
-    std::vector<int> hc(N);
-    CUDA_TRY(cudaStreamSynchronize(e->stream));
-    CUDA_TRY(cudaMemcpy(hp.data(), e->d_pos[e->cur], sizeof(float4) * N, cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(hv.data(), e->d_vel[e->cur], sizeof(float4) * N, cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(hf.data(), e->d_force, sizeof(float4) * N, cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(hc.data(), e->d_cell_of[e->cur], sizeof(int) * N, cudaMemcpyDeviceToHost));
+    if (n > e->nparts || n < 0) return MXG_ERR_RANGE;
+    if (n == 0) return MXG_OK;
+    const size_t N = (size_t)e->nparts;
+    // by id on the device (positions: cell origin + x_rel in double), then one copy per array
+    if (x && !e->d_ul_x && e->alloc(&e->d_ul_x, 3 * N) != MXG_OK) return MXG_ERR_MALLOC;
+    if (v && !e->d_ul_v && e->alloc(&e->d_ul_v, 3 * N) != MXG_OK) return MXG_ERR_MALLOC;
+    if (f && !e->d_ul_f && e->alloc(&e->d_ul_f, 3 * N) != MXG_OK) return MXG_ERR_MALLOC;
+    if (cell && !e->d_ul_cell && e->alloc(&e->d_ul_cell, N) != MXG_OK) return MXG_ERR_MALLOC;
+    if (xrel && !e->d_ul_xrel && e->alloc(&e->d_ul_xrel, 3 * N) != MXG_OK) return MXG_ERR_MALLOC;
     // after a step the forces are in the slot order of the step's starting buffer, whose
     // velocity array still carries the ids in that order
-    CUDA_TRY(cudaMemcpy(hfv.data(), e->d_vel[e->force_layout], sizeof(float4) * N, cudaMemcpyDeviceToHost));
-    if (f)
-        for (int s = 0; s < N; ++s) {
-            int id;
-            memcpy(&id, &hfv[s].w, 4);
-            if (id < 0 || id >= n) continue;
-            f[3 * (size_t)id] = hf[s].x;
-            f[3 * (size_t)id + 1] = hf[s].y;
-            f[3 * (size_t)id + 2] = hf[s].z;
-        }
-    for (int s = 0; s < N; ++s) {
-        int id;
-        memcpy(&id, &hv[s].w, 4);
-        if (id < 0 || id >= n) continue;
-        const int c = hc[s];
-        const Space &sp = e->spaces[e->prep[id]];
-        const int lc = c - sp.cell_offset;
-        const float xr[3] = {hp[s].x, hp[s].y, hp[s].z};
-        for (int k = 0; k < 3; ++k) {
-            if (x) x[3 * (size_t)id + k] = sp.cell_origin[3 * (size_t)lc + k] + xr[k];
-            if (xrel) xrel[3 * (size_t)id + k] = xr[k];
-        }
-        if (v) {
-            v[3 * (size_t)id] = hv[s].x;
-            v[3 * (size_t)id + 1] = hv[s].y;
-            v[3 * (size_t)id + 2] = hv[s].z;
-        }
-        if (cell) cell[id] = c;
-    }
+    launch_unload(e->view(e->cur), e->d_vel[e->force_layout], x ? e->d_ul_x : nullptr, v ? e->d_ul_v : nullptr,
+                  f ? e->d_ul_f : nullptr, cell ? e->d_ul_cell : nullptr, xrel ? e->d_ul_xrel : nullptr, e->stream);
+    const size_t m = (size_t)n;
+    if (x) CUDA_TRY(cudaMemcpyAsync(x, e->d_ul_x, sizeof(double) * 3 * m, cudaMemcpyDeviceToHost, e->stream));
+    if (v) CUDA_TRY(cudaMemcpyAsync(v, e->d_ul_v, sizeof(float) * 3 * m, cudaMemcpyDeviceToHost, e->stream));
+    if (f) CUDA_TRY(cudaMemcpyAsync(f, e->d_ul_f, sizeof(float) * 3 * m, cudaMemcpyDeviceToHost, e->stream));
+    if (cell) CUDA_TRY(cudaMemcpyAsync(cell, e->d_ul_cell, sizeof(int) * m, cudaMemcpyDeviceToHost, e->stream));
+    if (xrel) CUDA_TRY(cudaMemcpyAsync(xrel, e->d_ul_xrel, sizeof(float) * 3 * m, cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    CUDA_TRY(cudaGetLastError());
     return MXG_OK;
 }
 
@@ -2029,7 +2246,7 @@ int mxg_engine_energy(mxg_engine *e, double *epot, double *ekin, double *virial9
     if (!e) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
     launch_energy(e->nitems, e->d_epot_cell, e->nparts, e->has_bonded() ? e->d_ebond_slot : nullptr,
-                  (e->has_walls || e->nlarge) ? e->d_body_e : nullptr, e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
+                  e->has_body() ? e->d_body_e : nullptr, e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
                   e->stream);
     double out[2];
     CUDA_TRY(cudaMemcpyAsync(out, e->d_energy, sizeof(out), cudaMemcpyDeviceToHost, e->stream));
@@ -2049,6 +2266,15 @@ int mxg_engine_energy(mxg_engine *e, double *epot, double *ekin, double *virial9
         v.virial_partials = e->d_virial_partials;
         launch_force(v, e->has_dpd, e->force_grid, false, e->stream);
         launch_virial_reduce(e->d_virial_partials, nwarps, e->d_virial_out, e->stream);
+        if (e->has_bonded()) {
+            // the bonded terms' share (bonds active after the last pass, exclusions, angles, dihedrals)
+            const int nblk = bonded_virial_blocks(e->num_sms);
+            if (!e->d_bvirial_partials && e->alloc(&e->d_bvirial_partials, (size_t)nblk * 9) != MXG_OK)
+                return MXG_ERR_MALLOC;
+            launch_bonded_virial(e->view(e->cur), e->bonded_view(), (int)e->bonds.size(), (int)e->exclusions.size(),
+                                 (int)e->angles.size(), (int)e->dihedrals.size(), nblk, e->d_bvirial_partials,
+                                 e->d_virial_out, e->stream);
+        }
         CUDA_TRY(cudaMemcpyAsync(virial9, e->d_virial_out, 9 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
         CUDA_TRY(cudaStreamSynchronize(e->stream));
         CUDA_TRY(cudaGetLastError());
@@ -2085,6 +2311,26 @@ int mxg_engine_bond_flags(mxg_engine *e, unsigned *out, int cap) {
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     if (n) CUDA_TRY(cudaMemcpy(out, e->d_bond_flags, sizeof(unsigned) * n, cudaMemcpyDeviceToHost));
     return n;
+}
+
+int mxg_engine_set_bond_flags(mxg_engine *e, const unsigned *flags, int n) {
+    if (!e || (n > 0 && !flags)) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    if (n != (int)e->bonds.size()) return MXG_ERR_RANGE;
+    if (n == 0) return MXG_OK;
+    std::vector<unsigned> f(flags, flags + n);
+    for (unsigned &x : f) x &= 1u;
+    int rc = upload(e->d_bond_flags, f, e->stream);
+    if (rc != MXG_OK) return rc;
+    CUDA_TRY(cudaStreamSynchronize(e->stream));  // the host vector goes out of scope
+    return MXG_OK;
+}
+
+int mxg_engine_bond_pot_index(const mxg_engine *e, int k, int *idx) {
+    if (!e || !idx) return MXG_ERR_NULL;
+    if (k < 0 || k >= (int)e->bonds.size()) return MXG_ERR_RANGE;
+    *idx = e->bonds[k].pot;
+    return MXG_OK;
 }
 
 int mxg_engine_space_info(const mxg_engine *e, int *cdim, double *h, int *nr_cells, unsigned *period) {
@@ -2128,7 +2374,7 @@ int mxg_engine_energy_async(mxg_engine *e, double *host_out2) {
     if (!e || !host_out2) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
     launch_energy(e->nitems, e->d_epot_cell, e->nparts, e->has_bonded() ? e->d_ebond_slot : nullptr,
-                  (e->has_walls || e->nlarge) ? e->d_body_e : nullptr, e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
+                  e->has_body() ? e->d_body_e : nullptr, e->d_vel[e->cur], e->d_pos[e->cur], e->d_types, e->d_partials, e->energy_blocks, e->d_energy,
                   e->stream);
     CUDA_TRY(cudaMemcpyAsync(host_out2, e->d_energy, 2 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     return MXG_OK;
@@ -2195,15 +2441,26 @@ int mxg_engine_adjoint_params(mxg_engine *e, int n, const int *pot, const int *p
 int mxg_engine_vjp_step(mxg_engine *e, void *lam_x, void *lam_v, double *grad) {
     if (!e || !lam_x || !lam_v || !grad) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
-    // bonded, single-body, wall and large-particle forces are not differentiated
-    if (e->has_bonded() || e->has_sb || e->has_walls || e->nlarge) return MXG_ERR_ARG;
+    // angles, dihedrals, exclusions, single-body, wall and large-particle forces are not
+    // differentiated; bonds are
+    if (!e->angles.empty() || !e->dihedrals.empty() || !e->exclusions.empty() || e->has_sb || e->has_walls ||
+        e->nlarge)
+        return MXG_ERR_ARG;
     if (e->nparts == 0) return MXG_OK;
     if (e->adjoint_stale) {
         const int rc = e->build_adjoint();
         if (rc != MXG_OK) return rc;
     }
     const EngineView v = e->view(e->cur);
-    launch_force(v, e->has_dpd, e->force_grid, true, e->stream);  // forces of the step's state
+    // forces of the step's state; with bonds, the bond pass of the state completes them and
+    // leaves the flags of the bonds that acted in the step (as the forward step's pass did)
+    const bool bonded = !e->bonds.empty();
+    launch_force(v, e->has_dpd, e->force_grid, !bonded, e->stream);
+    BondedView bv;
+    if (bonded) {
+        bv = e->bonded_view();
+        launch_bonded(v, bv, e->stream);
+    }
     e->force_layout = e->cur;
     AdjointView a;
     a.lam_x = static_cast<float4 *>(lam_x);
@@ -2214,8 +2471,9 @@ int mxg_engine_vjp_step(mxg_engine *e, void *lam_x, void *lam_v, double *grad) {
     a.pot_grad = e->d_pot_grad;
     a.dcoef = e->d_dcoef;
     a.partials = e->d_adj_partials;
+    a.bond_partials = e->d_adj_bond_partials;
     a.nslots = e->grad_slots;
-    launch_vjp_step(v, a, e->num_sms, grad, e->stream);
+    launch_vjp_step(v, a, bonded ? &bv : nullptr, e->num_sms, grad, e->stream);
     CUDA_TRY(cudaGetLastError());
     return MXG_OK;
 }
@@ -2308,43 +2566,90 @@ int mxg_engine_time_force_launches(mxg_engine *e, int reps, void *flush, size_t 
     return err == cudaSuccess ? MXG_OK : MXG_ERR_CUDA;
 }
 
-/* A small autotuner for the force kernel's grid: candidate CTAs per SM are
- * timed on the current state (mean of a few launches each) and the fastest is
- * kept; the step graphs are re-captured with it. */
+/* The force kernel's autotuner: every tile shape (own particles and neighbour particles staged
+ * per region, see the force kernel's Tile) with candidate CTAs per SM is timed on the current
+ * state (the median of five launches each, after one warm launch) and the fastest pair is
+ * kept; the step graphs are re-captured with it. The state's occupancy (its density) decides. */
 int mxg_engine_autotune(mxg_engine *e) {
     if (!e) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
     if (e->nparts == 0) return MXG_OK;
     const int cands[] = {2, 4, 6, 8, 12, 16, 24, 32};
     const int max_grid = (e->nitems + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    int best = e->force_grid, best_per_sm = 0;
+    int best = e->force_grid, best_per_sm = 0, best_variant = e->force_variant;
     float best_ms = 1e30f;
-    cudaEvent_t a, b;
-    CUDA_TRY(cudaEventCreate(&a));
-    CUDA_TRY(cudaEventCreate(&b));
-    const EngineView v = e->view(e->cur);
-    for (int per_sm : cands) {
-        const int grid = std::max(1, std::min(max_grid, e->num_sms * per_sm));
-        launch_force(v, e->has_dpd, grid, true, e->stream);  // warm
-        e->force_layout = e->cur;
-        CUDA_TRY(cudaEventRecord(a, e->stream));
-        for (int r = 0; r < 5; ++r) launch_force(v, e->has_dpd, grid, true, e->stream);
-        CUDA_TRY(cudaEventRecord(b, e->stream));
-        CUDA_TRY(cudaEventSynchronize(b));
-        float t = 0.f;
-        cudaEventElapsedTime(&t, a, b);
-        if (t < best_ms) {
-            best_ms = t;
-            best = grid;
-            best_per_sm = per_sm;
+    cudaEvent_t ev[6];
+    for (auto &x : ev) CUDA_TRY(cudaEventCreate(&x));
+    for (int variant = 0; variant < force_variants(); ++variant) {
+        e->force_variant = variant;
+        const EngineView v = e->view(e->cur);
+        for (int per_sm : cands) {
+            const int grid = std::max(1, std::min(max_grid, e->num_sms * per_sm));
+            launch_force(v, e->has_dpd, grid, true, e->stream);  // warm
+            float t[5];
+            for (int r = 0; r < 5; ++r) {
+                CUDA_TRY(cudaEventRecord(ev[r], e->stream));
+                launch_force(v, e->has_dpd, grid, true, e->stream);
+                CUDA_TRY(cudaEventRecord(ev[5], e->stream));
+                CUDA_TRY(cudaEventSynchronize(ev[5]));
+                cudaEventElapsedTime(&t[r], ev[r], ev[5]);
+            }
+            std::sort(t, t + 5);
+            if (t[2] < best_ms) {
+                best_ms = t[2];
+                best = grid;
+                best_per_sm = per_sm;
+                best_variant = variant;
+            }
+            if (grid == max_grid) break;
         }
-        if (grid == max_grid) break;
     }
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
+    for (auto &x : ev) cudaEventDestroy(x);
+    e->force_layout = e->cur;
     e->force_grid = best;
+    e->force_variant = best_variant;
     const int rc = e->build_graphs();
     return rc != MXG_OK ? rc : best_per_sm;
+}
+
+int mxg_engine_force_config(mxg_engine *e, int *variant, int *grid, int set) {
+    if (!e || !variant || !grid) return MXG_ERR_NULL;
+    if (!set) {
+        *variant = e->force_variant;
+        *grid = e->force_grid;
+        return MXG_OK;
+    }
+    if (!e->started) return MXG_ERR_STATE;
+    if (*variant < 0 || *variant >= force_variants() || *grid < 1) return MXG_ERR_ARG;
+    // no more blocks than the work items can occupy (the autotuner's bound too)
+    *grid = std::min(*grid, std::max(1, (e->nitems + kWarpsPerBlock - 1) / kWarpsPerBlock));
+    e->force_variant = *variant;
+    e->force_grid = *grid;
+    return e->build_graphs();
+}
+
+int mxg_engine_number_density(mxg_engine *e, int n, float *out, double *volume) {
+    if (!e || (!out && !volume)) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    if (n < 0 || n > e->nparts) return MXG_ERR_RANGE;
+    if (e->nparts == 0) {
+        if (volume) *volume = 0.0;
+        return MXG_OK;
+    }
+    if (!e->d_nd && e->alloc(&e->d_nd, (size_t)e->nparts) != MXG_OK) return MXG_ERR_MALLOC;
+    launch_number_density(e->view(e->cur), e->has_fluxes ? e->d_flux_off : nullptr, e->d_nd, e->stream);
+    std::vector<float> h((size_t)e->nparts);
+    CUDA_TRY(cudaMemcpyAsync(h.data(), e->d_nd, sizeof(float) * h.size(), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    CUDA_TRY(cudaGetLastError());
+    if (out) std::copy(h.begin(), h.begin() + n, out);
+    if (volume) {
+        // engine_advance's computed volume: the sum over particles of 1 / number density
+        double vol = 0.0;
+        for (float x : h) vol += x > 0.f ? (double)(1.f / x) : 0.0;
+        *volume = vol;
+    }
+    return MXG_OK;
 }
 
 int mxg_engine_pair_counts(mxg_engine *e, long long *candidates, long long *interacting) {

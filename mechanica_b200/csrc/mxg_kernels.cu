@@ -6,8 +6,8 @@
  *   bonded_kernel     harmonic/table bonds with dissociation flags, angles.
  *   integrate_kernel  forward Euler (Newtonian / overdamped), speed clamp,
  *                     wall reflection, relocation; counts the next binning.
- *   scan_kernel       exclusive scan of the new cell occupancy.
- *   scatter_kernel    stable re-binning (ascending id inside each cell).
+ *   scatter_kernel    stable re-binning (ascending id inside each cell); each
+ *                     cell's new start from chunked net mover counts.
  *   energy kernels    FP64 reductions of potential and kinetic energy.
  *
  * Compiled with -fmad=false: every FP32/FP64 operation on the pair, bond and
@@ -88,7 +88,7 @@ __global__ void sort_bounds_kernel(EngineView v) {
  * cell that is FIRST in the reference's flipped pair (runner_dopair.cpp:91-340);
  * the cell's own pairs (runner_doself, :446-682) are evaluated from both sides.
  * The warp stages up to kOwn of the cell's particles and then, region by
- * region, up to kCap particles of its SELF and FIRST neighbour entries (whole
+ * region, up to kCap particles (the tile shape, Tile) of its SELF and FIRST neighbour entries (whole
  * entries where they fit) in shared memory. Each own particle is tested
  * against the staged neighbours one per lane, 32 candidates per step, for the
  * cutoff, the reference's pruning and the existence of a potential (pass 1).
@@ -280,14 +280,32 @@ __device__ __noinline__ void large_forces(const EngineView &v, int s, const floa
     }
 }
 
-constexpr int kOwn = 32;            // own particles staged at a time
-constexpr int kCap = 96;            // neighbour particles staged at a time
-constexpr int kChunks = kCap / 32;  // candidate steps per own particle
-constexpr int kQueue = 256;         // ring buffer of queued pairs (holds kCap + 31)
+/* A force-kernel tile shape: own particles staged at a time, neighbour particles staged
+ * per region (a multiple of 32: the candidate pass keeps kCap / 32 of them per lane in
+ * registers) and the resident blocks per SM its register budget allows. The autotuner
+ * picks one per engine (force_variant); variant 0 is the default. */
+template <int kOwnT, int kCapT, int kBlocksT>
+struct Tile {
+    static constexpr int kOwn = kOwnT, kCap = kCapT, kChunks = kCapT / 32, kBlocks = kBlocksT;
+    // a queued pair is (own index << 8 | staged index) in 16 bits; one own particle queues at most
+    // kCap pairs on top of fewer than 32 waiting ones
+    static_assert(kOwnT >= 1 && kOwnT <= 255 && kCapT % 32 == 0 && kCapT >= 32 && kCapT <= 256, "tile shape");
+};
+using Tile0 = Tile<32, 96, 5>;
+using Tile1 = Tile<32, 64, 6>;
+using Tile2 = Tile<64, 96, 5>;
+using Tile3 = Tile<32, 128, 4>;
+constexpr int kForceVariants = 4;
+
+constexpr int kQueue = 256;         // ring buffer of queued pairs (holds kCap + 31 for every tile)
+static_assert(Tile0::kCap + 31 <= kQueue && Tile1::kCap + 31 <= kQueue && Tile2::kCap + 31 <= kQueue &&
+                  Tile3::kCap + 31 <= kQueue,
+              "queue");
 constexpr int kEnt = 32;            // neighbour entries cached at a time
 
-template <bool kDPD>
+template <bool kDPD, class TS>
 struct ForceSmem {
+    static constexpr int kOwn = TS::kOwn, kCap = TS::kCap;
     float4 nb_x[kCap];              // neighbour position; w = type
     float4 nb_s[kCap];              // shift of FIRST entries, else 0; w = role | entry << 2 | index << 8
     float4 nb_f[kCap];              // neighbour-side force sums of the region
@@ -306,14 +324,46 @@ struct ForceSmem {
     unsigned short queue[kQueue];   // own index << 8 | staged index, in candidate order
 };
 
+/*
+ * dpd_eval (dpd_eval.hpp:21-69) for the DPD-only kernel, the reference's random term (no
+ * random number), non-shifted potentials: q0 = (cutoff, alpha, gamma, sigma delta),
+ * q1 = (a^2, a, 1 / cutoff, alpha + sigma delta) of the type pair. The cutoff test is the
+ * reference's exact one on r2; the force magnitude is formed from one reciprocal square root
+ * and fused multiply-adds, f = oc (alpha + sigma delta - gamma oc (e.v)) with oc = 1 - r/rc,
+ * e = dx/r (a few units in the last place from the reference's divisions; the force
+ * tolerance is 1e-5). The first particle gets +f e, the second -f e.
+ */
+__device__ __forceinline__ void dpd_fast(const float4 &q0, const float4 &q1, bool i_first, float dx, float dy,
+                                         float dz, float r2, const float4 &vi, const float4 &vj, float &cx, float &cy,
+                                         float &cz, bool &counted) {
+    cx = cy = cz = 0.f;
+    counted = false;
+    if (r2 > __fmul_rn(q0.x, q0.x)) return;
+    const float ir = rsqrtf(r2);
+    const float r = __fmul_rn(r2, ir);
+    const float ex = __fmul_rn(dx, ir), ey = __fmul_rn(dy, ir), ez = __fmul_rn(dz, ir);
+    const float wx = __fsub_rn(vi.x, vj.x), wy = __fsub_rn(vi.y, vj.y), wz = __fsub_rn(vi.z, vj.z);
+    // e.(v_first - v_second): dx is first minus second, w is i minus j
+    const float ev0 = __fmaf_rn(ex, wx, __fmaf_rn(ey, wy, __fmul_rn(ez, wz)));
+    const float ev = i_first ? ev0 : -ev0;
+    const float oc = __fmaf_rn(-r, q1.z, 1.0f);
+    const float f = __fmul_rn(oc, __fmaf_rn(__fmul_rn(-q0.z, oc), ev, q1.w));
+    const float fs = i_first ? f : -f;
+    cx = __fmul_rn(fs, ex);
+    cy = __fmul_rn(fs, ey);
+    cz = __fmul_rn(fs, ez);
+    counted = i_first;
+}
+
 /* Pass 2 over the nb <= 32 queued pairs from qhead: one interacting pair per
  * lane; own-side segmented sums into own_f, neighbour-side sums into nb_f.
  * kMode 1 counts the pairs (once each), kMode 2 sums the pair virial
  * (x_first - x_second) (x) F_first in FP64 (xx, yy, zz, xy, xz, yz). */
-template <bool kDPD, int kMode, bool kPure = false>
-__device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD> &sm, const float4 *tinfo, int qhead,
+template <bool kDPD, int kMode, bool kPure, class TS>
+__device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD, TS> &sm, const float4 *tinfo, int qhead,
                                            int nb, int i0, int own_start, int pot_base, unsigned rng_mode,
-                                           double &ecell, unsigned long long &npair, double *vir) {
+                                           float cut2_pair, float cut2_self, double &ecell, unsigned long long &npair,
+                                           double *vir) {
     const int lane = threadIdx.x & 31;
     float cx = 0.f, cy = 0.f, cz = 0.f;
     int il = -1, jj = 0;
@@ -340,50 +390,76 @@ __device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD> 
         float r2 = dot3_rn(dx, dy, dz);
         const float dxo = dx, dyo = dy, dzo = dz;  // before the r < a substitution
         const int ti = __float_as_int(xi.w), tj = __float_as_int(b.w);
-        const DevPot &p = v.pots[v.pot_idx[pot_base + ti * v.ntypes + tj]];
         const bool i_first = role == kRoleFirst || (role == kRoleSelf && i < jl);
         nbside = role == kRoleFirst;
-        if (r2 < p.a2) {
-            // potential_eval_super_ex (dpd_eval.hpp:122-131): random direction of
-            // length a; here a Philox draw keyed on the step and the id pair
-            const unsigned idi = __float_as_uint(kDPD ? sm.own_v[il].w : v.vel[own_start + i].w);
-            const unsigned idj =
-                __float_as_uint(kDPD ? sm.nb_v[jj].w : v.vel[sm.ent_slot[(meta >> 2) & 31] + jl].w);
-            const unsigned lo = idi < idj ? idi : idj, hi = idi < idj ? idj : idi;
-            float g0, g1, g2;
-            philox_normal3(*v.step, lo, hi, g0, g1, g2);
-            const float len = sqrtf(g0 * g0 + g1 * g1 + g2 * g2);
-            // the draw is the displacement first-minus-second for (lo, hi)
-            const float sgn = ((idi == lo) == i_first) ? 1.0f : -1.0f;
-            dx = sgn * g0 * p.a / len;
-            dy = sgn * g1 * p.a / len;
-            dz = sgn * g2 * p.a / len;
-            r2 = p.a2;
+        // the exact cutoff test of the pair loops (pass 1 queued a superset)
+        const bool inside = r2 <= (role == kRoleSelf ? cut2_self : cut2_pair);
+        if (kPure && inside) {
+            // every pair potential is a DPD potential with the reference's random term: its
+            // constants from one compact record per type pair
+            const int pk = 2 * (pot_base + ti * v.ntypes + tj);
+            const float4 q0 = __ldg(v.dpd_pair + pk), q1 = __ldg(v.dpd_pair + pk + 1);
+            if (r2 < q1.x) {
+                // potential_eval_super_ex's random direction of length a (Philox here)
+                const unsigned idi = __float_as_uint(sm.own_v[il].w), idj = __float_as_uint(sm.nb_v[jj].w);
+                const unsigned lo = idi < idj ? idi : idj, hi = idi < idj ? idj : idi;
+                float g0, g1, g2;
+                philox_normal3(*v.step, lo, hi, g0, g1, g2);
+                const float len = sqrtf(g0 * g0 + g1 * g1 + g2 * g2);
+                const float sgn = ((idi == lo) == i_first) ? 1.0f : -1.0f;
+                dx = sgn * g0 * q1.y / len;
+                dy = sgn * g1 * q1.y / len;
+                dz = sgn * g2 * q1.y / len;
+                r2 = q1.x;
+            }
+            bool counted;
+            dpd_fast(q0, q1, i_first, dx, dy, dz, r2, sm.own_v[il], sm.nb_v[jj], cx, cy, cz, counted);
+            if (kMode == 1 && counted) ++npair;
         }
-        const float4 vi = kDPD ? sm.own_v[il] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 vj = kDPD ? sm.nb_v[jj] : make_float4(0.f, 0.f, 0.f, 0.f);
-        float pe;
-        bool counted;
-        pair_contribution<kDPD, kPure>(v, p, role, i_first, dx, dy, dz, r2, tinfo[ti].w, tinfo[tj].w, vi, vj, rng_mode,
-                                cx, cy, cz, pe, counted);
-        ecell += (double)pe;
-        if (kMode == 1 && counted) ++npair;
-        if (!kPure && v.pot_idx2) {
-            // a second potential summed on the same pair (a table potential plus a DPD
-            // thermostat), evaluated on the pair's own displacement
-            const int q2 = v.pot_idx2[pot_base + ti * v.ntypes + tj];
-            if (q2 >= 0) {
-                const DevPot &p2 = v.pots[q2];
-                float r2b = dot3_rn(dxo, dyo, dzo);
-                if (!(r2b < p2.a2)) {
-                    float c2x, c2y, c2z, pe2;
-                    bool counted2;
-                    pair_contribution<kDPD>(v, p2, role, i_first, dxo, dyo, dzo, r2b, tinfo[ti].w, tinfo[tj].w, vi,
-                                            vj, rng_mode, c2x, c2y, c2z, pe2, counted2);
-                    cx = cx + c2x;
-                    cy = cy + c2y;
-                    cz = cz + c2z;
-                    ecell += (double)pe2;
+        if (!kPure && inside) {
+            const DevPot &p = v.pots[v.pot_idx[pot_base + ti * v.ntypes + tj]];
+            if (r2 < p.a2) {
+                // potential_eval_super_ex (dpd_eval.hpp:122-131): random direction of
+                // length a; here a Philox draw keyed on the step and the id pair
+                const unsigned idi = __float_as_uint(kDPD ? sm.own_v[il].w : v.vel[own_start + i].w);
+                const unsigned idj =
+                    __float_as_uint(kDPD ? sm.nb_v[jj].w : v.vel[sm.ent_slot[(meta >> 2) & 31] + jl].w);
+                const unsigned lo = idi < idj ? idi : idj, hi = idi < idj ? idj : idi;
+                float g0, g1, g2;
+                philox_normal3(*v.step, lo, hi, g0, g1, g2);
+                const float len = sqrtf(g0 * g0 + g1 * g1 + g2 * g2);
+                // the draw is the displacement first-minus-second for (lo, hi)
+                const float sgn = ((idi == lo) == i_first) ? 1.0f : -1.0f;
+                dx = sgn * g0 * p.a / len;
+                dy = sgn * g1 * p.a / len;
+                dz = sgn * g2 * p.a / len;
+                r2 = p.a2;
+            }
+            const float4 vi = kDPD ? sm.own_v[il] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 vj = kDPD ? sm.nb_v[jj] : make_float4(0.f, 0.f, 0.f, 0.f);
+            float pe;
+            bool counted;
+            pair_contribution<kDPD, kPure>(v, p, role, i_first, dx, dy, dz, r2, tinfo[ti].w, tinfo[tj].w, vi, vj, rng_mode,
+                                    cx, cy, cz, pe, counted);
+            ecell += (double)pe;
+            if (kMode == 1 && counted) ++npair;
+            if (!kPure && v.pot_idx2) {
+                // a second potential summed on the same pair (a table potential plus a DPD
+                // thermostat), evaluated on the pair's own displacement
+                const int q2 = v.pot_idx2[pot_base + ti * v.ntypes + tj];
+                if (q2 >= 0) {
+                    const DevPot &p2 = v.pots[q2];
+                    float r2b = dot3_rn(dxo, dyo, dzo);
+                    if (!(r2b < p2.a2)) {
+                        float c2x, c2y, c2z, pe2;
+                        bool counted2;
+                        pair_contribution<kDPD>(v, p2, role, i_first, dxo, dyo, dzo, r2b, tinfo[ti].w, tinfo[tj].w, vi,
+                                                vj, rng_mode, c2x, c2y, c2z, pe2, counted2);
+                        cx = cx + c2x;
+                        cy = cy + c2y;
+                        cz = cz + c2z;
+                        ecell += (double)pe2;
+                    }
                 }
             }
         }
@@ -445,19 +521,20 @@ __device__ __forceinline__ void zero_plane(const EngineView &v, int rev, int nst
     for (int k = lane; k < ncount; k += 32) dst[k] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
-template <bool kDPD>
+template <bool kDPD, class TS>
 constexpr size_t force_smem_bytes() {
-    return sizeof(ForceSmem<kDPD>) * kWarpsPerBlock;
+    return sizeof(ForceSmem<kDPD, TS>) * kWarpsPerBlock;
 }
 
-template <bool kDPD, int kMode, bool kPure = false>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 5) force_kernel(EngineView v) {
+template <bool kDPD, int kMode, bool kPure, class TS>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, TS::kBlocks) force_kernel(EngineView v) {
+    constexpr int kOwn = TS::kOwn, kCap = TS::kCap, kChunks = TS::kChunks;
     unsigned long long npair = 0;  // interacting pairs counted once (statistics launch only)
     double vir[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // pair virial (virial launch only)
     extern __shared__ float4 force_smem[];
     __shared__ float4 tinfo[kMaxTypes];  // per type: constant force (zero if none), radius
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    ForceSmem<kDPD> &sm = reinterpret_cast<ForceSmem<kDPD> *>(force_smem)[w];
+    ForceSmem<kDPD, TS> &sm = reinterpret_cast<ForceSmem<kDPD, TS> *>(force_smem)[w];
     const unsigned lt_mask = (1u << lane) - 1u;
     const int ntypes = v.ntypes;
     for (int t = threadIdx.x; t < ntypes; t += blockDim.x) {
@@ -497,6 +574,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 5) force_kernel(EngineVie
             const DevSpace &S = v.spaces[v.cell_rep[c]];
             const int pot_base = S.pot_offset;
             const float cut2_pair = S.cut2_pair, cut2_self = S.cut2_self;
+            const float cut2w_pair = S.cut2w_pair, cut2w_self = S.cut2w_self;
             const unsigned rng_mode = S.rng_mode;
             const bool prune = (S.prune & 1) != 0;      // per-pair projection test
             const bool exit_test = (S.prune & 2) != 0;  // cell-pair exit test
@@ -505,17 +583,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 5) force_kernel(EngineVie
             for (int i0 = 0; i0 < n; i0 += kOwn) {
                 const int ni = min(kOwn, n - i0);
                 __syncwarp();
-                if (lane < ni) {
-                    const float4 x = v.pos[start + i0 + lane];
-                    sm.own_x[lane] = x;
+                for (int k = lane; k < ni; k += 32) {  // kOwn may exceed the warp
+                    const float4 x = v.pos[start + i0 + k];
+                    sm.own_x[k] = x;
                     const int ti = __float_as_int(x.w);
                     const float4 T = tinfo[ti];  // the body force goes with the cell's first work item
-                    sm.own_f[lane] = part == 0 ? make_float4(T.x, T.y, T.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (kDPD) sm.own_v[lane] = v.vel[start + i0 + lane];
+                    sm.own_f[k] = part == 0 ? make_float4(T.x, T.y, T.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (kDPD) sm.own_v[k] = v.vel[start + i0 + k];
                     unsigned long long mk = 0ull;
                     for (int t = 0; t < ntypes; ++t)
                         if (v.pot_idx[pot_base + ti * ntypes + t] >= 0) mk |= 1ull << t;  // a lone second term is moved here
-                    sm.own_mask[lane] = mk;
+                    sm.own_mask[k] = mk;
                 }
                 for (int g0 = nb0; g0 < nb1; g0 += kEnt) {
                     // ---- entries g0 .. g0+31: lane k loads entry g0 + k; SELF and FIRST entries
@@ -597,14 +675,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 5) force_kernel(EngineVie
                         __syncwarp();
                         // ---- stage the region's neighbour particles; lane's chunk-u neighbour
                         // (staged index u * 32 + lane) is also kept in registers for pass 1
-                        float rbx[kChunks], rby[kChunks], rbz[kChunks], rsx[kChunks], rsy[kChunks], rsz[kChunks];
-                        float rc2[kChunks];   // cutoff squared; -1 for an empty position
+                        // neighbour position plus the entry's shift (one rounding away from the
+                        // reference's (x_i - s) - x_j): pass 1 is a superset filter with a widened
+                        // cutoff; pass 2 applies the exact test on the exact displacement
+                        float rbx[kChunks], rby[kChunks], rbz[kChunks];
+                        float rc2[kChunks];   // widened cutoff squared; -1 for an empty position
                         int rself[kChunks];   // index of a SELF neighbour within the cell, else -1
                         int rtj[kChunks];     // neighbour type
 #pragma unroll
                         for (int u = 0; u < kChunks; ++u) {
                             const int idx = u * 32 + lane;
-                            rbx[u] = rby[u] = rbz[u] = rsx[u] = rsy[u] = rsz[u] = 0.f;
+                            rbx[u] = rby[u] = rbz[u] = 0.f;
                             rc2[u] = -1.f;
                             rself[u] = -1;
                             rtj[u] = 0;
@@ -632,13 +713,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 5) force_kernel(EngineVie
                                 sm.nb_s[idx] = s4;
                                 sm.nb_f[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
                                 if (kDPD) sm.nb_v[idx] = v.vel[slot];
-                                rbx[u] = q.x;
-                                rby[u] = q.y;
-                                rbz[u] = q.z;
-                                rsx[u] = s4.x;
-                                rsy[u] = s4.y;
-                                rsz[u] = s4.z;
-                                rc2[u] = role == kRoleSelf ? cut2_self : cut2_pair;
+                                rbx[u] = __fadd_rn(q.x, s4.x);
+                                rby[u] = __fadd_rn(q.y, s4.y);
+                                rbz[u] = __fadd_rn(q.z, s4.z);
+                                rc2[u] = role == kRoleSelf ? cut2w_self : cut2w_pair;
                                 rself[u] = role == kRoleSelf ? jl : -1;
                                 rtj[u] = __float_as_int(q.w);
                             }
@@ -659,9 +737,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 5) force_kernel(EngineVie
                                 for (int u = 0; u < kChunks; ++u) {
                                     hb[u] = 0u;
                                     if (u * 32 < M) {
-                                        const float dx = __fsub_rn(__fsub_rn(xi.x, rsx[u]), rbx[u]);
-                                        const float dy = __fsub_rn(__fsub_rn(xi.y, rsy[u]), rby[u]);
-                                        const float dz = __fsub_rn(__fsub_rn(xi.z, rsz[u]), rbz[u]);
+                                        const float dx = __fsub_rn(xi.x, rbx[u]);
+                                        const float dy = __fsub_rn(xi.y, rby[u]);
+                                        const float dz = __fsub_rn(xi.z, rbz[u]);
                                         const float r2 = dot3_rn(dx, dy, dz);
                                         bool hit = (r2 <= rc2[u]) & (((mk >> rtj[u]) & 1ull) != 0ull) & (rself[u] != i);
                                         if (prune && hit && rself[u] < 0) {
@@ -689,8 +767,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 5) force_kernel(EngineVie
                             while (qtail - qhead >= 32 || (il == ni && qtail > qhead)) {
                                 const int nb = min(32, qtail - qhead);
                                 __syncwarp();
-                                eval_batch<kDPD, kMode, kPure>(v, sm, tinfo, qhead, nb, i0, start, pot_base, rng_mode, ecell,
-                                                        npair, vir);
+                                eval_batch<kDPD, kMode, kPure, TS>(v, sm, tinfo, qhead, nb, i0, start, pot_base, rng_mode, cut2_pair,
+                                               cut2_self, ecell, npair, vir);
                                 qhead += nb;
                             }
                         }
@@ -712,11 +790,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 5) force_kernel(EngineVie
                     }
                 }
                 __syncwarp();
-                if (lane < ni) {
-                    const float4 f = sm.own_f[lane];
+                for (int k = lane; k < ni; k += 32) {
+                    const float4 f = sm.own_f[k];
                     // the cell's first work item writes the force, later ones their own plane
                     float4 *dst = part == 0 ? v.force : v.planes + (size_t)(v.sec_count[c] + part - 1) * v.nparts;
-                    if (kMode != 2) dst[start + i0 + lane] = make_float4(f.x, f.y, f.z, 0.f);
+                    if (kMode != 2) dst[start + i0 + k] = make_float4(f.x, f.y, f.z, 0.f);
                 }
             }
         }
@@ -761,11 +839,20 @@ __global__ void virial_reduce_kernel(const double *partials, int nwarps, double 
 __device__ __forceinline__ float4 total_force(const EngineView &v, int s) {
     float4 f = v.force[s];
     const int np = v.cell_planes[v.cell_of[s]];
-    for (int k = 0; k < np; ++k) {
-        const float4 g = v.planes[(size_t)k * v.nparts + s];
-        f.x += g.x;
-        f.y += g.y;
-        f.z += g.z;
+    // the planes are read once: eight independent streaming loads in flight, then the
+    // additions in plane order (the same sums, bit for bit)
+    for (int k0 = 0; k0 < np; k0 += 8) {
+        float4 g[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            if (k0 + q < np) g[q] = __ldcs(v.planes + (size_t)(k0 + q) * v.nparts + s);
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            if (k0 + q < np) {
+                f.x += g[q].x;
+                f.y += g[q].y;
+                f.z += g[q].z;
+            }
     }
     if (v.body_f) {  // walls and large particles of this pass (body_kernel)
         const float4 b = v.body_f[s];
@@ -931,11 +1018,199 @@ __global__ void species_integrate_kernel(EngineView v, SpeciesView sp, const int
     for (int k = 0; k < sp.smax; ++k) sp.rate[(size_t)id * sp.smax + k] = 0.f;
 }
 
-/* Wall potentials of particles in cells next to a bound face and the large
- * particles' interactions (runner_doself's boundary_eval and
- * particle_largecell_force, runner_dopair.cpp:526-535), one thread per slot,
- * before the pass's force kernel; total_force adds the force, the energy goes
- * to the slot's entry. */
+/*
+ * The number density f[3] of the particles (the reference's MxParticle::number_density),
+ * for the current positions, as a force pass leaves it: W(0, rc) from space_prepare
+ * (space.cpp:216-236) plus W(r2, rc) for every pair the pair loops reach within the cutoff
+ * (runner_dopair.cpp:194-203, 552-559) whose type pair has no potential and no flux, or
+ * whose potential evaluates in range (potential_eval_super_ex adds it on success,
+ * dpd_eval.hpp:133-166; a pair closer than the table minimum counts at distance a). W is
+ * the cubic spline of smoothing_kernel.hpp:37-56 with h = rc; the reference forms r with
+ * a 12-bit reciprocal square-root approximation (qsqrt, :19-24), here sqrtf. One thread per
+ * particle visits the full shell of its cell (SELF, FIRST and SECOND entries, each pair in
+ * the reference's orientation for its r2, the same pruning tests as the force pass), so the
+ * sums have a fixed order. Large particles, walls and second summed potentials add nothing.
+ */
+__device__ __forceinline__ float w_cubic(float r2, float h) {
+    const float r = sqrtf(r2);
+    const float x = r / h;
+    float y;
+    if (x < 1.f) {
+        const float x2 = x * x;
+        y = 1.f - (3.f / 2.f) * x2 + (3.f / 4.f) * x2 * x;
+    } else if (x < 2.f) {
+        const float a = 2.f - x;
+        y = (1.f / 4.f) * a * a * a;
+    } else {
+        y = 0.f;
+    }
+    return (float)((double)y / (M_PI * (double)h * (double)h * (double)h));
+}
+
+__global__ void number_density_kernel(EngineView v, const int *flux_off, float *nd_out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= v.nparts) return;
+    const float4 xo = v.pos[s];
+    const int to = __float_as_int(xo.w);
+    const int c = v.cell_of[s];
+    const DevSpace &S = v.spaces[v.cell_rep[c]];
+    const float h = (float)S.cutoff_d;
+    float nd = w_cubic(0.f, h);
+    if (v.types[to].large) {
+        nd_out[__float_as_int(v.vel[s].w)] = nd;
+        return;
+    }
+    const bool prune = (S.prune & 1) != 0, exit_test = (S.prune & 2) != 0;
+    for (int e = v.nb_off[c]; e < v.nb_off[c + 1]; ++e) {
+        const int nc = v.nb_cell[e];
+        const float4 sh = v.nb_shift[e];
+        const int pk = __float_as_int(sh.w);
+        const int role = pk & 3;
+        const int sid = (pk >> 2) & 15;
+        if (exit_test && role != kRoleSelf) {
+            const int cf = role == kRoleFirst ? c : nc, cs = role == kRoleFirst ? nc : c;
+            const int2 bf = v.sort_bounds[cf * 13 + sid], bs = v.sort_bounds[cs * 13 + sid];
+            const int gap = bs.x + (pk >> 8) - bf.y;
+            if (v.cell_count[cf] > 0 && v.cell_count[cs] > 0 && (gap < 0 || gap > S.dmaxdist)) continue;
+        }
+        const int j0 = v.cell_start[nc], j1 = j0 + v.cell_count[nc];
+        for (int j = j0; j < j1; ++j) {
+            if (j == s) continue;
+            const float4 xj = v.pos[j];
+            const float4 &a = role == kRoleSecond ? xj : xo, &b = role == kRoleSecond ? xo : xj;
+            float dx, dy, dz;
+            if (role == kRoleSelf) {
+                dx = __fsub_rn(a.x, b.x);
+                dy = __fsub_rn(a.y, b.y);
+                dz = __fsub_rn(a.z, b.z);
+            } else {
+                dx = __fsub_rn(__fsub_rn(a.x, sh.x), b.x);
+                dy = __fsub_rn(__fsub_rn(a.y, sh.y), b.y);
+                dz = __fsub_rn(__fsub_rn(a.z, sh.z), b.z);
+            }
+            const float r2 = dot3_rn(dx, dy, dz);
+            if (r2 > (role == kRoleSelf ? S.cut2_self : S.cut2_pair)) continue;
+            if (prune && role != kRoleSelf) {
+                const float *n = v.axes->n[sid];
+                const int kf = sort_key(a.x, a.y, a.z, n, S.sort_bias, S.sort_dscale);
+                const int ks = sort_key(b.x, b.y, b.z, n, S.sort_bias, S.sort_dscale);
+                if (!(ks + (pk >> 8) - kf < S.dmaxdist)) continue;
+            }
+            const int tj = __float_as_int(xj.w);
+            if (v.types[tj].large) continue;
+            const int q = v.pot_idx[S.pot_offset + to * v.ntypes + tj];
+            bool counts;
+            if (q < 0) {
+                counts = !flux_off || flux_off[to * v.ntypes + tj] == flux_off[to * v.ntypes + tj + 1];
+            } else {
+                const DevPot &p = v.pots[q];
+                const float rr2 = r2 < p.a2 ? p.a2 : r2;
+                const float ra = role == kRoleSecond ? v.types[tj].radius : v.types[to].radius;
+                const float rb = role == kRoleSecond ? v.types[to].radius : v.types[tj].radius;
+                if (p.kind == 1) {
+                    const float cut = (p.flags & (1u << 12)) ? __fadd_rn(__fadd_rn(p.b, ra), rb) : p.b;
+                    counts = !(rr2 > __fmul_rn(cut, cut));
+                } else {
+                    float ee, ff;
+                    counts = table_eval_ex(p, v.coef, ra, rb, rr2, ee, ff);
+                }
+            }
+            if (counts) nd = __fadd_rn(nd, w_cubic(r2, h));
+        }
+    }
+    nd_out[__float_as_int(v.vel[s].w)] = nd;
+}
+
+/* Quaternion product a b, components (x, y, z, w), in the arithmetic order of the
+ * vector form (b.v a.w + a.v b.w + a.v x b.v, a.w b.w - a.v . b.v). */
+__device__ __forceinline__ void quat_mul(const float *a, const float *b, float *o) {
+    const float cx = a[1] * b[2] - a[2] * b[1], cy = a[2] * b[0] - a[0] * b[2], cz = a[0] * b[1] - a[1] * b[0];
+    o[0] = (b[0] * a[3] + a[0] * b[3]) + cx;
+    o[1] = (b[1] * a[3] + a[1] * b[3]) + cy;
+    o[2] = (b[2] * a[3] + a[2] * b[3]) + cz;
+    o[3] = a[3] * b[3] - ((a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]);
+}
+
+/* q v q* : v rotated by the unit quaternion q. */
+__device__ __forceinline__ void quat_rotate(const float *q, const float *v, float *out) {
+    const float p[4] = {v[0], v[1], v[2], 0.f}, qc[4] = {-q[0], -q[1], -q[2], q[3]};
+    float t[4], r[4];
+    quat_mul(q, p, t);
+    quat_mul(t, qc, r);
+    out[0] = r[0];
+    out[1] = r[1];
+    out[2] = r[2];
+}
+
+/*
+ * Cuboid forces on one particle (potential_eval_cuboid_particle, cuboid_eval.hpp:73-188,
+ * called from runner_doself for the cuboids whose bounding box, widened by the cutoff,
+ * meets the particle's cell, :190-201 and :37-55): the particle's global point
+ * x_rel + float(cell origin) inside the widened box is taken into the cuboid's frame, and
+ * the face it is nearest to (inside) or above (outside) gives the axis: the potential
+ * potential_eval_ex(pot, r0 = half size on that axis, radius, distance^2) along that axis,
+ * rotated back. No energy is tabulated, as in the reference.
+ */
+__device__ __noinline__ void cuboid_forces(const EngineView &v, int c, const float4 &x, const DevType &T, float4 &f) {
+    const DevSpace &S = v.spaces[v.cell_rep[c]];
+    int loc[3];
+    cell_loc(S, c, loc);
+    const float cut = (float)S.cutoff_d;
+    float org[3], bmin[3], bmax[3], pt[3];
+    const float xr[3] = {x.x, x.y, x.z};
+    for (int k = 0; k < 3; ++k) {
+        org[k] = (float)__dadd_rn(S.origin[k], __dmul_rn((double)loc[k], S.hd[k]));
+        bmin[k] = org[k] - cut;
+        bmax[k] = (org[k] + (float)S.hd[k]) + cut;
+        pt[k] = xr[k] + org[k];
+    }
+    const DevPot &p = v.pots[T.cpot];
+    for (int q = 0; q < v.ncuboids; ++q) {
+        const DevCuboid &C = v.cuboids[q];
+        if (C.rep != v.cell_rep[c]) continue;
+        bool meets = true, inside = true;
+        for (int k = 0; k < 3; ++k) {
+            meets = meets && C.lo[k] <= bmax[k] && C.hi[k] >= bmin[k];
+            inside = inside && pt[k] >= C.lo[k] - cut && pt[k] <= C.hi[k] + cut;
+        }
+        if (!meets || !inside) continue;
+        float rel[3] = {pt[0] - C.pos[0], pt[1] - C.pos[1], pt[2] - C.pos[2]}, pl[3];
+        quat_rotate(C.qi, rel, pl);
+        float dv[3], half[3];
+        for (int k = 0; k < 3; ++k) {
+            half[k] = C.size[k] / 2.f;
+            dv[k] = fabsf(pl[k]) - half[k];
+        }
+        int ax;
+        if (dv[0] < 0 && dv[1] < 0 && dv[2] < 0) {  // inside: the nearest face
+            ax = (dv[0] > dv[1] && dv[0] > dv[2]) ? 0 : ((dv[1] > dv[0] && dv[1] > dv[2]) ? 1 : 2);
+        } else if (dv[0] < 0 && dv[1] < 0) {
+            ax = 2;
+        } else if (dv[0] < 0 && dv[2] < 0) {
+            ax = 1;
+        } else if (dv[1] < 0 && dv[2] < 0) {
+            ax = 0;
+        } else {
+            continue;
+        }
+        const float dist = fabsf(pl[ax]);
+        float ee, ff;
+        if (!table_eval_ex(p, v.coef, half[ax], T.radius, __fmul_rn(dist, dist), ee, ff)) continue;
+        // -forceVec * force with forceVec zero off the axis (signed zeros kept as the reference forms them)
+        float fv[3], fg[3];
+        for (int k = 0; k < 3; ++k) fv[k] = (k == ax ? -pl[ax] : -0.f) * ff;
+        quat_rotate(C.q, fv, fg);
+        f.x += fg[0];
+        f.y += fg[1];
+        f.z += fg[2];
+    }
+}
+
+/* Wall potentials of particles in cells next to a bound face, the large particles'
+ * interactions and the cuboids' forces (runner_doself's boundary_eval,
+ * particle_largecell_force and potential_eval_cuboid_particle, runner_dopair.cpp:
+ * 526-535), one thread per slot, before the pass's force kernel; total_force adds the
+ * force, the energy goes to the slot's entry. */
 __global__ void body_kernel(EngineView v, float4 *body_f) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= v.nparts) return;
@@ -947,6 +1222,7 @@ __global__ void body_kernel(EngineView v, float4 *body_f) {
     double ew = 0.0;
     if (cflags & T.wall_mask) boundary_forces(v, v.spaces[v.cell_rep[c]], cflags, T, T.radius, x, v.vel[s], f, ew);
     if (v.nlarge && !T.large) large_forces(v, s, x, v.vel[s], T.radius, f, ew);
+    if (v.ncuboids && T.cpot >= 0) cuboid_forces(v, c, x, T, f);
     body_f[s] = f;
     v.body_e[s] = ew;
 }
@@ -1008,24 +1284,6 @@ __global__ void combine_kernel(EngineView v) {
 /* ------------------------------------------------------------------------ */
 /* bonds                                                                     */
 /* ------------------------------------------------------------------------ */
-
-/* Cell coordinates of global cell c in its replica's grid. */
-__device__ __forceinline__ void cell_loc(const DevSpace &S, int c, int loc[3]) {
-    const int l = c - S.cell_offset;
-    loc[0] = l / (S.cdim[1] * S.cdim[2]);
-    loc[1] = (l / S.cdim[2]) % S.cdim[1];
-    loc[2] = l % S.cdim[2];
-}
-
-/* The bonded code's neighbour-cell shift (bond.cpp:163-170, angle.cpp:155-168):
- * a cell difference of more than one is a periodic wrap. */
-__device__ __forceinline__ int wrap_shift(int d) { return d > 1 ? -1 : (d < -1 ? 1 : d); }
-
-/* x + shift*h formed in double and rounded to float, as the reference writes
- * the double product into a float position. */
-__device__ __forceinline__ float shifted(float x, int sh, double h) {
-    return (float)__dadd_rn((double)x, __dmul_rn(h, (double)sh));
-}
 
 /*
  * The force terms of angle aid exactly as angle_eval computes them
@@ -1242,15 +1500,10 @@ __global__ void bonded_kernel(EngineView v, BondedView bv) {
         const DevBond B = bv.bonds[b];
         const int si = bv.slot_of_id[B.i], sj = bv.slot_of_id[B.j];
         if (si < 0 || sj < 0) continue;
-        const int ci = v.cell_of[si], cj = v.cell_of[sj];
+        const int ci = v.cell_of[si];
         const DevSpace &S = v.spaces[v.cell_rep[ci]];
-        int loci[3], locj[3];
-        cell_loc(S, ci, loci);
-        cell_loc(S, cj, locj);
-        const float4 xi = v.pos[si], xj = v.pos[sj];
-        const float xiv[3] = {xi.x, xi.y, xi.z}, xjv[3] = {xj.x, xj.y, xj.z};
         float d[3];
-        for (int q = 0; q < 3; ++q) d[q] = __fsub_rn(shifted(xiv[q], wrap_shift(loci[q] - locj[q]), S.hd[q]), xjv[q]);
+        bond_vector(S, ci, v.cell_of[sj], v.pos[si], v.pos[sj], d);
         float r2 = dot3_rn(d[0], d[1], d[2]);
         const DevPot &p = v.pots[B.pot];
         const float a2 = __fmul_rn(p.a, p.a), b2 = __fmul_rn(p.b, p.b);
@@ -1317,6 +1570,194 @@ __global__ void bonded_kernel(EngineView v, BondedView bv) {
     bv.e_slot[s] = eb;
 }
 
+constexpr int kVirThreads = 128;
+
+/* A table's value and derivative at s in FP64 on its FP32 coefficients, the interval
+ * picked from float(s) as the FP32 code picks it (an integer decision of the model). */
+__device__ __forceinline__ void table_value64(const DevPot &p, const float *coef, double sd, double &e, double &dv) {
+    const float sf = (float)sd;
+    const float t = __fadd_rn(p.alpha0, __fmul_rn(sf, __fadd_rn(p.alpha1, __fmul_rn(sf, p.alpha2))));
+    const int ind = min((int)fmaxf(0.0f, t), p.n);
+    const float *c = coef + p.coef_off + ind * kChunk;
+    const double x = (sd - (double)c[0]) * (double)c[1];
+    double ee = (double)c[2] * x + (double)c[3], eff = (double)c[2];
+    for (int k = 4; k < 8; ++k) {
+        eff = eff * x + ee;
+        ee = ee * x + (double)c[k];
+    }
+    e = ee;
+    dv = eff * (double)c[1];
+}
+
+/* x_i - x_j in FP64 for particles in cells ci, cj (x_i taken into x_j's frame by the
+ * bonded code's wrapped cell shift). */
+__device__ __forceinline__ void rel64(const EngineView &v, int si, int sj, double d[3]) {
+    const int ci = v.cell_of[si], cj = v.cell_of[sj];
+    const DevSpace &S = v.spaces[v.cell_rep[ci]];
+    int li[3], lj[3];
+    cell_loc(S, ci, li);
+    cell_loc(S, cj, lj);
+    const float4 a = v.pos[si], b = v.pos[sj];
+    const float av[3] = {a.x, a.y, a.z}, bv[3] = {b.x, b.y, b.z};
+    for (int q = 0; q < 3; ++q) d[q] = ((double)av[q] + (double)wrap_shift(li[q] - lj[q]) * S.hd[q]) - (double)bv[q];
+}
+
+__device__ __forceinline__ void cross64(const double *a, const double *b, double *o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* c = u.w / (|u| |w|) and its gradients with respect to u and w. */
+__device__ __forceinline__ double cos_grad64(const double *u, const double *w, double *gu, double *gw) {
+    const double nu = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    const double nw = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+    const double c = (u[0] * w[0] + u[1] * w[1] + u[2] * w[2]) / (nu * nw);
+    for (int q = 0; q < 3; ++q) {
+        gu[q] = (w[q] / nw - c * u[q] / nu) / nu;
+        gw[q] = (u[q] / nu - c * w[q] / nw) / nw;
+    }
+    return c;
+}
+
+/*
+ * The bonded terms' virial, sum over the terms' members of (x_m - x_ref) (x) F_m for the
+ * current positions: active bonds (flags after the last pass; a bond whose FP32 f reaches its
+ * dissociation energy at these positions would break and adds nothing), d (x) F_i with
+ * F_i = -V'(r)/r d; exclusions within the cutoff, d (x) (+V'(r)/r d) (the pair potential taken
+ * back, so the pair's term in the nonbonded virial cancels); angles about their vertex,
+ * r_ji (x) F_i + r_jk (x) F_k; dihedrals about their j particle,
+ * b1 (x) F_i + b2 (x) F_k + (b2 + b3) (x) F_l. Each term is evaluated in FP64 from the FP32
+ * positions (the table's interval and clamps decided as in FP32): the FP32 force of a bond
+ * near its rest length carries a relative error far above 1e-6 (r - r0 cancels), as the
+ * reference's does, and the virial is reported to 1e-6. Degenerate angles (cos = 0 or -1,
+ * a random plane in the force pass) add nothing. One thread per term, FP64 sums per thread,
+ * per block in thread order; launched only by the energy call.
+ */
+__global__ void __launch_bounds__(kVirThreads) bonded_virial_kernel(EngineView v, BondedView bv, int nb, int nx,
+                                                                    int na, int nd, double *partials) {
+    __shared__ double part[kVirThreads * 9];
+    double w[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    auto add = [&](const double *r, const double *F) {
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) w[3 * a + b] += r[a] * F[b];
+    };
+    const int total = nb + nx + na + nd;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        if (t < nb) {
+            if (!(bv.bond_flags[t] & 1u)) continue;
+            const DevBond B = bv.bonds[t];
+            const int si = bv.slot_of_id[B.i], sj = bv.slot_of_id[B.j];
+            if (si < 0 || sj < 0) continue;
+            const DevPot &p = v.pots[B.pot];
+            // the FP32 pass's break decision
+            const int ci = v.cell_of[si];
+            float df[3];
+            bond_vector(v.spaces[v.cell_rep[ci]], ci, v.cell_of[sj], v.pos[si], v.pos[sj], df);
+            float r2f = dot3_rn(df[0], df[1], df[2]);
+            const float a2 = __fmul_rn(p.a, p.a), b2 = __fmul_rn(p.b, p.b);
+            if (r2f < a2 || r2f > b2) r2f = fmaxf(a2, fminf(b2, r2f));
+            float ee, eff;
+            table_eval(p, v.coef, r2f, ee, eff);
+            if ((double)eff >= B.dissociation) continue;
+            double d[3];
+            rel64(v, si, sj, d);
+            const double r = fmin(fmax(sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]), (double)p.a), (double)p.b);
+            double e64, dv;
+            table_value64(p, v.coef, r, e64, dv);
+            const double F[3] = {-dv / r * d[0], -dv / r * d[1], -dv / r * d[2]};
+            add(d, F);
+        } else if (t < nb + nx) {
+            const int2 X = bv.excl[t - nb];
+            const int si = bv.slot_of_id[X.x], sj = bv.slot_of_id[X.y];
+            if (si < 0 || sj < 0) continue;
+            const float4 xi = v.pos[si], xj = v.pos[sj];
+            const DevSpace &S = v.spaces[v.cell_rep[v.cell_of[si]]];
+            const int q = v.pot_idx[S.pot_offset + __float_as_int(xj.w) * v.ntypes + __float_as_int(xi.w)];
+            if (q < 0 || v.pots[q].kind != 0) continue;
+            double d[3];
+            rel64(v, si, sj, d);
+            const float df[3] = {(float)d[0], (float)d[1], (float)d[2]};
+            if (dot3_rn(df[0], df[1], df[2]) > S.cut2_self) continue;
+            const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            double e64, dv;
+            table_value64(v.pots[q], v.coef, r, e64, dv);
+            const double F[3] = {dv / r * d[0], dv / r * d[1], dv / r * d[2]};
+            add(d, F);
+        } else if (t < nb + nx + na) {
+            const DevAngle A = bv.angles[t - nb - nx];
+            if (A.pot < 0) continue;
+            const int si = bv.slot_of_id[A.i], sj = bv.slot_of_id[A.j], sk = bv.slot_of_id[A.k];
+            if (si < 0 || sj < 0 || sk < 0) continue;
+            double rji[3], rjk[3], gi[3], gk[3];
+            rel64(v, si, sj, rji);
+            rel64(v, sk, sj, rjk);
+            double c = cos_grad64(rji, rjk, gi, gk);
+            if (c == 0.0 || c == -1.0) continue;
+            const DevPot &p = v.pots[A.pot];
+            c = fmin(fmax(fmin(fmax(c, -1.0), 1.0), (double)p.a), (double)p.b);
+            double e64, dv;
+            table_value64(p, v.coef, c, e64, dv);
+            const double Fi[3] = {-dv * gi[0], -dv * gi[1], -dv * gi[2]}, Fk[3] = {-dv * gk[0], -dv * gk[1], -dv * gk[2]};
+            add(rji, Fi);
+            add(rjk, Fk);
+        } else {
+            const DevDihedral D = bv.dihedrals[t - nb - nx - na];
+            if (D.pot < 0) continue;
+            const int si = bv.slot_of_id[D.i], sj = bv.slot_of_id[D.j], sk = bv.slot_of_id[D.k],
+                      sl = bv.slot_of_id[D.l];
+            if (si < 0 || sj < 0 || sk < 0 || sl < 0) continue;
+            double b1[3], b2[3], b3[3], A3[3], B3[3], gA[3], gB[3];
+            rel64(v, si, sj, b1);
+            rel64(v, sk, sj, b2);
+            rel64(v, sl, sk, b3);
+            cross64(b1, b2, A3);
+            cross64(b2, b3, B3);
+            double c = -cos_grad64(A3, B3, gA, gB);
+            for (int q = 0; q < 3; ++q) {
+                gA[q] = -gA[q];
+                gB[q] = -gB[q];
+            }
+            double g1[3], g2a[3], g2b[3], g3[3];
+            cross64(b2, gA, g1);   // dc/db1 through A = b1 x b2
+            cross64(gA, b1, g2a);  // dc/db2 through A
+            cross64(b3, gB, g2b);  // dc/db2 through B = b2 x b3
+            cross64(gB, b2, g3);   // dc/db3 through B
+            const DevPot &p = v.pots[D.pot];
+            c = fmin(fmax(fmin(fmax(c, -1.0), 1.0), (double)p.a), (double)p.b);
+            double e64, dv;
+            table_value64(p, v.coef, c, e64, dv);
+            double Fi[3], Fk[3], Fl[3], rl[3];
+            for (int q = 0; q < 3; ++q) {
+                const double wi = dv * g1[q], wj = dv * (-g1[q] - g2a[q] - g2b[q]), wl = dv * g3[q];
+                Fi[q] = -wi;
+                Fl[q] = -wl;
+                Fk[q] = wi + wj + wl;
+                rl[q] = b2[q] + b3[q];
+            }
+            add(b1, Fi);
+            add(b2, Fk);
+            add(rl, Fl);
+        }
+    }
+    for (int k = 0; k < 9; ++k) part[threadIdx.x * 9 + k] = w[k];
+    __syncthreads();
+    if (threadIdx.x < 9) {
+        double s9 = 0.0;
+        for (int r = 0; r < (int)blockDim.x; ++r) s9 += part[r * 9 + threadIdx.x];
+        partials[(size_t)blockIdx.x * 9 + threadIdx.x] = s9;
+    }
+}
+
+/* out9 += the bonded virial from the blocks' partials, in block order. */
+__global__ void bonded_virial_reduce_kernel(const double *partials, int nblocks, double *out9) {
+    const int k = threadIdx.x;
+    if (k >= 9) return;
+    double t = 0.0;
+    for (int q = 0; q < nblocks; ++q) t += partials[(size_t)q * 9 + k];
+    out9[k] += t;
+}
+
 /* ------------------------------------------------------------------------ */
 /* integrator                                                                */
 /* ------------------------------------------------------------------------ */
@@ -1341,15 +1782,25 @@ __device__ __forceinline__ int relocate(const DevSpace &S, int c, float *xv, int
     return S.cell_offset + (loc[0] * S.cdim[1] + loc[1]) * S.cdim[2] + loc[2];
 }
 
-/* Appends a particle that moved from cell c to dest to dest's bucket. */
+/* Appends a particle that moved from cell c to dest to dest's bucket, or, when
+ * the bucket is full, to the step's overflow list (at most one entry per
+ * particle, so nparts entries always suffice). The reference has no limit on
+ * the particles entering a cell (space_cell_add_incomming, space_cell.cpp:
+ * 260-290), and neither has this engine. A move between chunks of cells also
+ * updates the two chunks' net counts, from which the re-binning forms each
+ * cell's new start without a scan over all cells. */
 __device__ __forceinline__ void bucket_move(const EngineView &v, int s, int c, int dest, int *in_count, int *in_list,
                                             int *out_count) {
     const int k = atomicAdd(&in_count[dest], 1);
     if (k < kBucket)
         in_list[dest * kBucket + k] = s;
     else
-        atomicOr(v.status, kStatusBucketOverflow);
+        v.ovf_list[atomicAdd(v.ovf_count, 1)] = s;
     atomicAdd(&out_count[c], 1);
+    if ((c >> kChunkShift) != (dest >> kChunkShift)) {
+        atomicAdd(&v.chunk_delta[dest >> kChunkShift], 1);
+        atomicSub(&v.chunk_delta[c >> kChunkShift], 1);
+    }
 }
 
 /*
@@ -1358,12 +1809,11 @@ __device__ __forceinline__ void bucket_move(const EngineView &v, int s, int c, i
  * wall reflection (boundary_eval.hpp:30-122), and the move to a neighbour cell
  * with x -= delta*h. The next step's space_shuffle_local rule is applied once
  * more to the moved particle, as engine_force does before the next force pass.
- * Moved particles are appended to the destination cell's bucket; stayers are
- * counted implicitly (count_old - out + in).
+ * Moved particles are appended to the destination cell's bucket (or the overflow list);
+ * stayers are counted implicitly (count_old - out + in).
  */
-__global__ void integrate_kernel(EngineView v, float4 *pos, float4 *vel, int *new_cell, int *in_count,
-                                 int *in_list, int *out_count, bool add_planes) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void integrate_one(int s, const EngineView &v, float4 *pos, float4 *vel, int *new_cell,
+                                              int *in_count, int *in_list, int *out_count, bool add_planes) {
     if (s >= v.nparts) return;
     const int c = v.cell_of[s];
     const DevSpace &S = v.spaces[v.cell_rep[c]];
@@ -1512,9 +1962,9 @@ __global__ void rk_stage_kernel(EngineView v, float4 *pos, RkState rk, int stage
     pos[s] = make_float4(nx[0], nx[1], nx[2], x.w);
 }
 
-__global__ void rk_final_kernel(EngineView v, float4 *pos, float4 *vel, RkState rk, int *new_cell, int *in_count,
-                                int *in_list, int *out_count, bool add_planes) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void rk_final_one(int s, const EngineView &v, float4 *pos, float4 *vel, const RkState &rk,
+                                             int *new_cell, int *in_count, int *in_list, int *out_count,
+                                             bool add_planes) {
     if (s >= v.nparts) return;
     const int c = v.cell_of[s];
     const DevSpace &S = v.spaces[v.cell_rep[c]];
@@ -1554,103 +2004,93 @@ __global__ void rk_final_kernel(EngineView v, float4 *pos, float4 *vel, RkState 
 /* re-binning                                                                */
 /* ------------------------------------------------------------------------ */
 
-constexpr int kScanPer = 16;                  // cells per thread
-constexpr int kScanChunk = 1024 * kScanPer;   // cells per pass of the block
+constexpr int kAdvThreads = 256;   // integrator blocks
 
-/* New occupancy (old - movers out + movers in) and its exclusive scan, one
- * block: each thread owns 16 consecutive cells of a chunk, read and written
- * as int4 vectors where the chunk is full, so the chunk's loads are all in
- * flight at once; warp and block scans of the per-thread sums; the step
- * counter that keys the Philox streams advances here. */
-__global__ void __launch_bounds__(1024) scan_kernel(int ncells, const int *__restrict__ old_count,
-                                                   const int *__restrict__ out_count, const int *__restrict__ in_count,
-                                                   int *new_start, int *new_count, unsigned long long *step) {
-    __shared__ int warp_total[32];
-    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-    int carry = 0;
-    for (int c0 = 0; c0 < ncells; c0 += kScanChunk) {
-        const int base = c0 + kScanPer * t;
-        int v[kScanPer];
-        if (base + kScanPer <= ncells) {
-#pragma unroll
-            for (int q = 0; q < kScanPer; q += 4) {
-                const int4 o = *reinterpret_cast<const int4 *>(old_count + base + q);
-                const int4 u = *reinterpret_cast<const int4 *>(out_count + base + q);
-                const int4 w = *reinterpret_cast<const int4 *>(in_count + base + q);
-                v[q] = o.x - u.x + min(w.x, kBucket);
-                v[q + 1] = o.y - u.y + min(w.y, kBucket);
-                v[q + 2] = o.z - u.z + min(w.z, kBucket);
-                v[q + 3] = o.w - u.w + min(w.w, kBucket);
-                *reinterpret_cast<int4 *>(new_count + base + q) = make_int4(v[q], v[q + 1], v[q + 2], v[q + 3]);
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < kScanPer; ++q) {
-                const int c = base + q;
-                v[q] = c < ncells ? old_count[c] - out_count[c] + min(in_count[c], kBucket) : 0;
-                if (c < ncells) new_count[c] = v[q];
-            }
-        }
-        int sum = 0;
-#pragma unroll
-        for (int q = 0; q < kScanPer; ++q) sum += v[q];
-        int incl = sum;
-        for (int off = 1; off < 32; off <<= 1) {
-            const int o = __shfl_up_sync(kFull, incl, off);
-            if (lane >= off) incl += o;
-        }
-        if (lane == 31) warp_total[wid] = incl;
-        __syncthreads();
-        if (wid == 0) {
-            int x = lane < (int)(blockDim.x >> 5) ? warp_total[lane] : 0;
-            for (int off = 1; off < 32; off <<= 1) {
-                const int o = __shfl_up_sync(kFull, x, off);
-                if (lane >= off) x += o;
-            }
-            warp_total[lane] = x;
-        }
-        __syncthreads();
-        int run = carry + (wid > 0 ? warp_total[wid - 1] : 0) + incl - sum;
-        if (base + kScanPer <= ncells) {
-#pragma unroll
-            for (int q = 0; q < kScanPer; q += 4) {
-                const int a0 = run, a1 = a0 + v[q], a2 = a1 + v[q + 1], a3 = a2 + v[q + 2];
-                *reinterpret_cast<int4 *>(new_start + base + q) = make_int4(a0, a1, a2, a3);
-                run = a3 + v[q + 3];
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < kScanPer; ++q) {
-                if (base + q < ncells) new_start[base + q] = run;
-                run += v[q];
-            }
-        }
-        carry += warp_total[31];
-        __syncthreads();
-    }
-    if (t == 0) {
-        new_start[ncells] = carry;
-        *step += 1;  // the step counter keying the Philox streams
-    }
+__global__ void __launch_bounds__(kAdvThreads, 4) integrate_kernel(EngineView v, float4 *pos, float4 *vel,
+                                                                int *new_cell, int *in_count, int *in_list,
+                                                                int *out_count, bool add_planes) {
+    integrate_one(blockIdx.x * blockDim.x + threadIdx.x, v, pos, vel, new_cell, in_count, in_list, out_count,
+                  add_planes);
+}
+
+__global__ void __launch_bounds__(kAdvThreads, 4) rk_final_kernel(EngineView v, float4 *pos, float4 *vel, RkState rk,
+                                                               int *new_cell, int *in_count, int *in_list,
+                                                               int *out_count, bool add_planes) {
+    rk_final_one(blockIdx.x * blockDim.x + threadIdx.x, v, pos, vel, rk, new_cell, in_count, in_list, out_count,
+                 add_planes);
 }
 
 /*
- * One warp per destination cell. Stayers keep their relative order (ascending
- * id); movers are merged in by id, so every cell stays sorted by id and the
- * layout is independent of thread scheduling. The warp then computes the new
- * cell's projection-key bounds for the next force pass.
+ * The stable re-binning into the other buffer: one warp per destination cell, kScatterWarps
+ * consecutive cells per block. The cell's new start needs no scan over all cells: it is its
+ * old start plus the net number of movers into the cells before it, which the block sums from
+ * the integrator's per-chunk net counts (chunks before the block's own) and the per-cell
+ * counts of its chunk before its first cell; the block's cells then add up their new counts
+ * in order. Stayers keep their relative order (ascending id); movers from the cell's bucket
+ * and from the overflow list are merged in by id, so every cell stays sorted by id and the
+ * layout does not depend on thread scheduling. The warp then computes the new cell's
+ * projection-key bounds for the next force pass.
+ *
+ * The counts of this step are read by other blocks and stay as they are; the block clears its
+ * cells' counts of the other buffer parity (and the grid that parity's chunk counts), which the
+ * next step uses. The block that finishes last re-arms its done counter and the overflow list
+ * and advances the step counter that keys the Philox streams.
  */
-__global__ void scatter_kernel(EngineView v, int ncells, const float4 *__restrict__ pos, const float4 *__restrict__ vel,
-                               const int *__restrict__ new_cell, const int *__restrict__ old_start,
-                               const int *__restrict__ old_count, int *in_count, const int *__restrict__ in_list,
-                               int *out_count, const int *__restrict__ new_start, float4 *pos_out, float4 *vel_out,
-                               int *cell_out, int *slot_of_id) {
-    const int lane = threadIdx.x & 31;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < ncells; c += warps) {
+__global__ void __launch_bounds__(kScatterWarps * 32, 5) scatter_kernel(
+    EngineView v, int ncells, const float4 *__restrict__ pos, const float4 *__restrict__ vel,
+    const int *__restrict__ new_cell, const int *__restrict__ old_start, const int *__restrict__ old_count,
+    const int *__restrict__ in_count, const int *__restrict__ in_list, const int *__restrict__ out_count,
+    int *new_start, int *new_count, float4 *pos_out, float4 *vel_out, int *cell_out, int *slot_of_id,
+    int *clear_in, int *clear_out, int *clear_chunk, int nchunks, unsigned *done, unsigned long long *step) {
+    __shared__ int s_net[kScatterWarps], s_n[kScatterWarps];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int c0 = blockIdx.x * kScatterWarps, c = c0 + wid;
+    {
+        // net movers into the cells [0, c0): whole chunks, then the cells of c0's chunk before c0
+        const int k0 = c0 >> kChunkShift, cb = k0 << kChunkShift;
+        int net = 0;
+        for (int j = tid; j < k0; j += blockDim.x) net += v.chunk_delta[j];
+        for (int q = cb + 4 * tid; q < c0; q += 4 * blockDim.x) {  // [cb, c0) holds whole int4 groups
+            const int4 a = *reinterpret_cast<const int4 *>(in_count + q);
+            const int4 b = *reinterpret_cast<const int4 *>(out_count + q);
+            net += ((a.x + a.y) + (a.z + a.w)) - ((b.x + b.y) + (b.z + b.w));
+        }
+        net = __reduce_add_sync(kFull, net);
+        if (lane == 0) {
+            s_net[wid] = net;
+            s_n[wid] = c < ncells ? old_count[c] - out_count[c] + in_count[c] : 0;
+        }
+        for (int j = blockIdx.x * blockDim.x + tid; j < nchunks; j += gridDim.x * blockDim.x) clear_chunk[j] = 0;
+        __syncthreads();
+    }
+    if (c < ncells) {
+        int base = old_start[c0];
+        for (int w = 0; w < kScatterWarps; ++w) base += s_net[w] + (w < wid ? s_n[w] : 0);
         const int os = old_start[c], on = old_count[c];
-        const int m = min(in_count[c], kBucket);
-        const int base = new_start[c];
+        const int mtot = in_count[c];
+        const int m = min(mtot, kBucket);
+        const int nov = mtot > kBucket ? *v.ovf_count : 0;  // the overflow list is scanned only when needed
+        // movers into c with an id below myid: from the bucket, then from the overflow list
+        auto movers_below = [&](int myid) {
+            int r = 0;
+            for (int q = 0; q < m; ++q) r += __float_as_int(vel[in_list[c * kBucket + q]].w) < myid;
+            for (int q = 0; q < nov; ++q) {
+                const int src = v.ovf_list[q];
+                r += new_cell[src] == c && __float_as_int(vel[src].w) < myid;
+            }
+            return r;
+        };
+        auto stayers_below = [&](int myid) {
+            int r = 0;
+            for (int k = 0; k < on; ++k) r += (new_cell[os + k] == c) && (__float_as_int(vel[os + k].w) < myid);
+            return r;
+        };
+        auto place = [&](int src, int myid, int dst) {
+            pos_out[dst] = pos[src];
+            vel_out[dst] = vel[src];
+            cell_out[dst] = c;
+            slot_of_id[myid] = dst;
+        };
         // stayers
         int stay_before = 0;
         for (int k0 = 0; k0 < on; k0 += 32) {
@@ -1662,47 +2102,207 @@ __global__ void scatter_kernel(EngineView v, int ncells, const float4 *__restric
                 myid = __float_as_int(vel[os + k].w);
             }
             const unsigned bal = __ballot_sync(kFull, stay);
-            if (stay) {
-                int rank = stay_before + __popc(bal & ((1u << lane) - 1u));
-                for (int q = 0; q < m; ++q) {
-                    const int src = in_list[c * kBucket + q];
-                    rank += __float_as_int(vel[src].w) < myid;
-                }
-                const int dst = base + rank;
-                pos_out[dst] = pos[os + k];
-                vel_out[dst] = vel[os + k];
-                cell_out[dst] = c;
-                slot_of_id[myid] = dst;
-            }
+            if (stay) place(os + k, myid, base + stay_before + __popc(bal & ((1u << lane) - 1u)) + movers_below(myid));
             stay_before += __popc(bal);
         }
-        // movers
+        // movers of the bucket
         for (int q0 = 0; q0 < m; q0 += 32) {
             const int q = q0 + lane;
             if (q < m) {
                 const int src = in_list[c * kBucket + q];
                 const int myid = __float_as_int(vel[src].w);
-                int rank = 0;
-                for (int k = 0; k < on; ++k)
-                    rank += (new_cell[os + k] == c) && (__float_as_int(vel[os + k].w) < myid);
-                for (int r = 0; r < m; ++r) rank += __float_as_int(vel[in_list[c * kBucket + r]].w) < myid;
-                const int dst = base + rank;
-                pos_out[dst] = pos[src];
-                vel_out[dst] = vel[src];
-                cell_out[dst] = c;
-                slot_of_id[myid] = dst;
+                place(src, myid, base + stayers_below(myid) + movers_below(myid));
             }
         }
-        __syncwarp();
+        // movers of the overflow list
+        for (int q0 = 0; q0 < nov; q0 += 32) {
+            const int q = q0 + lane;
+            if (q < nov) {
+                const int src = v.ovf_list[q];
+                if (new_cell[src] == c) {
+                    const int myid = __float_as_int(vel[src].w);
+                    place(src, myid, base + stayers_below(myid) + movers_below(myid));
+                }
+            }
+        }
+        const int nn = stay_before + mtot;
         if (lane == 0) {
-            in_count[c] = 0;
-            out_count[c] = 0;
+            new_start[c] = base;
+            new_count[c] = nn;
+            if (c == ncells - 1) new_start[ncells] = base + nn;
+            clear_in[c] = 0;
+            clear_out[c] = 0;
         }
         // the next force pass's cell-pair exit test reads the new cell's key bounds
-        const int nn = new_start[c + 1] - base;
         const DevSpace &S = v.spaces[v.cell_rep[c]];
         if (nn > 0 && (S.prune & 2))
             cell_sort_bounds(pos_out, base, nn, S.sort_bias, S.sort_dscale, v.axes, v.sort_bounds + c * 13);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        if (atomicAdd(done, 1u) == gridDim.x - 1) {  // every block is done with the overflow list
+            *v.ovf_count = 0;
+            *done = 0u;
+            *step += 1;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* device-side load and unload                                               */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * engine_load's placement (space_addpart, space.cpp:431-451, and the first
+ * shuffle's rule, space.cpp:352-371) per particle id, on the device: the cell
+ * index (int)((x - origin) ih), the cell-relative position float(x - (origin +
+ * l h)) in double, one move by delta = (x >= h) - (x < 0) in float; counts
+ * the new occupancy. Same arithmetic as the host placement, so the cells and
+ * the FP32 positions are bit-identical to it.
+ */
+__global__ void place_kernel(EngineView v, LoadView ld, int *count) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ld.n) return;
+    const DevSpace &S = v.spaces[ld.rep_of_id[p]];
+    int ind[3];
+    double x[3];
+    for (int k = 0; k < 3; ++k) {
+        x[k] = ld.x[3 * (size_t)p + k];
+        ind[k] = (int)__dmul_rn(__dsub_rn(x[k], S.origin[k]), S.ih[k]);
+    }
+    if (ind[0] < 0 || ind[0] >= S.cdim[0] || ind[1] < 0 || ind[1] >= S.cdim[1] || ind[2] < 0 || ind[2] >= S.cdim[2]) {
+        ld.cell[p] = -1;
+        atomicExch(ld.err, 1);
+        return;
+    }
+    float xr[3];
+    int delta[3];
+    for (int k = 0; k < 3; ++k) {
+        xr[k] = (float)__dsub_rn(x[k], __dadd_rn(S.origin[k], __dmul_rn((double)ind[k], S.hd[k])));
+        delta[k] = cell_delta(xr[k], S.h[k]);
+    }
+    if (delta[0] | delta[1] | delta[2])
+        for (int k = 0; k < 3; ++k) {
+            xr[k] = __fsub_rn(xr[k], __fmul_rn((float)delta[k], S.h[k]));
+            ind[k] = (ind[k] + delta[k] + S.cdim[k]) % S.cdim[k];
+        }
+    const int c = S.cell_offset + (ind[0] * S.cdim[1] + ind[1]) * S.cdim[2] + ind[2];
+    ld.cell[p] = c;
+    ld.xr[p] = make_float4(xr[0], xr[1], xr[2], __int_as_float(ld.type_of_id[p]));
+    // the given velocity, or the particle's current one
+    float4 u = ld.v ? make_float4(ld.v[3 * (size_t)p], ld.v[3 * (size_t)p + 1], ld.v[3 * (size_t)p + 2], 0.f)
+                    : v.vel[ld.slot_now[p]];
+    u.w = __int_as_float(p);
+    ld.vel[p] = u;
+    atomicAdd(&count[c], 1);
+}
+
+/* Exclusive scan of the new occupancy into start[0..ncells] (one block). */
+__global__ void __launch_bounds__(1024) load_scan_kernel(const int *__restrict__ count, int ncells, int *start) {
+    __shared__ int warp_sums[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int base = 0; base < ncells; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int x = i < ncells ? count[i] : 0;
+        int incl = x;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int t = __shfl_up_sync(kFull, incl, d);
+            if (lane >= d) incl += t;
+        }
+        if (lane == 31) warp_sums[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            int w = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+            for (int d = 1; d < 32; d <<= 1) {
+                const int t = __shfl_up_sync(kFull, w, d);
+                if (lane >= d) w += t;
+            }
+            warp_sums[lane] = w;
+        }
+        __syncthreads();
+        const int excl = carry + (wid ? warp_sums[wid - 1] : 0) + incl - x;
+        if (i < ncells) start[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = excl + x;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) start[ncells] = carry;
+}
+
+/* Each particle takes a place in its cell's range (in any order; ordered next). */
+__global__ void load_fill_kernel(LoadView ld, const int *__restrict__ start) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ld.n) return;
+    const int c = ld.cell[p];
+    ld.ids[start[c] + atomicAdd(&ld.fill[c], 1)] = p;
+}
+
+/* One warp per cell: its particles in ascending id (rank = number of smaller ids in the
+ * cell), written to the slot arrays, then the cell's projection-key bounds. */
+__global__ void load_order_kernel(EngineView v, LoadView ld, const int *__restrict__ start, float4 *pos_out,
+                                  float4 *vel_out, int *cell_out, int *slot_of_id, int2 *sort_bounds) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < v.ncells; c += warps) {
+        const int s0 = start[c], n = start[c + 1] - s0;
+        for (int k0 = 0; k0 < n; k0 += 32) {
+            const int k = k0 + lane;
+            if (k < n) {
+                const int id = ld.ids[s0 + k];
+                int rank = 0;
+                for (int q = 0; q < n; ++q) rank += ld.ids[s0 + q] < id;
+                const int dst = s0 + rank;
+                pos_out[dst] = ld.xr[id];
+                vel_out[dst] = ld.vel[id];
+                cell_out[dst] = c;
+                slot_of_id[id] = dst;
+            }
+        }
+        __syncwarp();
+        const DevSpace &S = v.spaces[v.cell_rep[c]];
+        if (n > 0 && (S.prune & 2)) cell_sort_bounds(pos_out, s0, n, S.sort_bias, S.sort_dscale, v.axes, sort_bounds + c * 13);
+    }
+}
+
+/* engine_unload's arrays by particle id (engine.cpp:620-784): the global position
+ * cell origin + x_rel in double, the velocity, the force of the last pass (from the slot
+ * order it was computed in: force_ids = that layout's velocities, w = id), the cell and
+ * the cell-relative position. Any output may be null. */
+__global__ void unload_kernel(EngineView v, const float4 *__restrict__ force_ids, double *x_out, float *v_out,
+                              float *f_out, int *cell_out, float *xrel_out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= v.nparts) return;
+    const float4 q = v.pos[s], u = v.vel[s];
+    const int id = __float_as_int(u.w);
+    const int c = v.cell_of[s];
+    if (x_out || xrel_out) {
+        const DevSpace &S = v.spaces[v.cell_rep[c]];
+        int loc[3];
+        cell_loc(S, c, loc);
+        const float xr[3] = {q.x, q.y, q.z};
+        for (int k = 0; k < 3; ++k) {
+            if (x_out)
+                x_out[3 * (size_t)id + k] =
+                    __dadd_rn(__dadd_rn(S.origin[k], __dmul_rn((double)loc[k], S.hd[k])), (double)xr[k]);
+            if (xrel_out) xrel_out[3 * (size_t)id + k] = xr[k];
+        }
+    }
+    if (v_out) {
+        v_out[3 * (size_t)id] = u.x;
+        v_out[3 * (size_t)id + 1] = u.y;
+        v_out[3 * (size_t)id + 2] = u.z;
+    }
+    if (cell_out) cell_out[id] = c;
+    if (f_out) {
+        const float4 f = v.force[s];
+        const int fid = __float_as_int(force_ids[s].w);
+        f_out[3 * (size_t)fid] = f.x;
+        f_out[3 * (size_t)fid + 1] = f.y;
+        f_out[3 * (size_t)fid + 2] = f.z;
     }
 }
 
@@ -1760,41 +2360,64 @@ __global__ void reduce_final_kernel(int nblocks, const double *partials, double 
 /* launchers                                                                 */
 /* ------------------------------------------------------------------------ */
 
-template <bool kDPD, int kMode, bool kPure = false>
+template <bool kDPD, int kMode, bool kPure, class TS>
 void configure_one() {
-    const int bytes = (int)force_smem_bytes<kDPD>();
-    cudaFuncSetAttribute(force_kernel<kDPD, kMode, kPure>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    cudaFuncSetAttribute(force_kernel<kDPD, kMode, kPure>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    const int bytes = (int)force_smem_bytes<kDPD, TS>();
+    cudaFuncSetAttribute(force_kernel<kDPD, kMode, kPure, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(force_kernel<kDPD, kMode, kPure, TS>, cudaFuncAttributePreferredSharedMemoryCarveout,
                          cudaSharedmemCarveoutMaxShared);
+}
+
+template <class TS>
+void configure_tile() {
+    configure_one<true, 0, false, TS>();
+    configure_one<true, 0, true, TS>();
+    configure_one<false, 0, false, TS>();
 }
 
 void configure_force_kernels() {
     // the force kernel's occupancy is bounded by shared memory: allow its dynamic
     // shared memory and ask for the largest carveout of the unified L1/shared storage
-    configure_one<true, 0>();
-    configure_one<true, 0, true>();
-    configure_one<true, 1>();
-    configure_one<true, 2>();
-    configure_one<false, 0>();
-    configure_one<false, 1>();
-    configure_one<false, 2>();
+    configure_tile<Tile0>();
+    configure_tile<Tile1>();
+    configure_tile<Tile2>();
+    configure_tile<Tile3>();
+    configure_one<true, 1, false, Tile0>();
+    configure_one<true, 2, false, Tile0>();
+    configure_one<false, 1, false, Tile0>();
+    configure_one<false, 2, false, Tile0>();
 }
 
 void launch_sort_bounds(const EngineView &v, cudaStream_t st) {
     sort_bounds_kernel<<<(v.ncells * 32 + 255) / 256, 256, 0, st>>>(v);
 }
 
-template <bool kDPD>
-void launch_force_mode(const EngineView &v, int grid, cudaStream_t st) {
-    const size_t bytes = force_smem_bytes<kDPD>();
-    if (v.pair_stats)
-        force_kernel<kDPD, 1><<<grid, kWarpsPerBlock * 32, bytes, st>>>(v);
-    else if (v.virial_partials)
-        force_kernel<kDPD, 2><<<grid, kWarpsPerBlock * 32, bytes, st>>>(v);
-    else if (kDPD && v.dpd_pure)
-        force_kernel<true, 0, true><<<grid, kWarpsPerBlock * 32, force_smem_bytes<true>(), st>>>(v);
+template <bool kDPD, class TS>
+void launch_force_tile(const EngineView &v, int grid, cudaStream_t st) {
+    const size_t bytes = force_smem_bytes<kDPD, TS>();
+    if (kDPD && v.dpd_pure)
+        force_kernel<true, 0, true, TS><<<grid, kWarpsPerBlock * 32, force_smem_bytes<true, TS>(), st>>>(v);
     else
-        force_kernel<kDPD, 0><<<grid, kWarpsPerBlock * 32, bytes, st>>>(v);
+        force_kernel<kDPD, 0, false, TS><<<grid, kWarpsPerBlock * 32, bytes, st>>>(v);
+}
+
+/* The statistics and virial launches use the default tile; the force pass the engine's
+ * variant (0 to kForceVariants - 1). */
+template <bool kDPD>
+void launch_force_mode(const EngineView &v, int grid, int variant, cudaStream_t st) {
+    const size_t bytes = force_smem_bytes<kDPD, Tile0>();
+    if (v.pair_stats)
+        force_kernel<kDPD, 1, false, Tile0><<<grid, kWarpsPerBlock * 32, bytes, st>>>(v);
+    else if (v.virial_partials)
+        force_kernel<kDPD, 2, false, Tile0><<<grid, kWarpsPerBlock * 32, bytes, st>>>(v);
+    else if (variant == 1)
+        launch_force_tile<kDPD, Tile1>(v, grid, st);
+    else if (variant == 2)
+        launch_force_tile<kDPD, Tile2>(v, grid, st);
+    else if (variant == 3)
+        launch_force_tile<kDPD, Tile3>(v, grid, st);
+    else
+        launch_force_tile<kDPD, Tile0>(v, grid, st);
 }
 
 /* Work items by decreasing occupancy of their cell (counting sort on the count, capped
@@ -1849,12 +2472,14 @@ __global__ void item_order_kernel(EngineView v) {
     }
 }
 
+int force_variants() { return kForceVariants; }
+
 void launch_force(const EngineView &v, bool has_dpd, int grid, bool combine, cudaStream_t st) {
     if (v.item_order && v.nitems > 0 && !v.virial_partials) item_order_kernel<<<1, 1024, 0, st>>>(v);
     if (has_dpd)
-        launch_force_mode<true>(v, grid, st);
+        launch_force_mode<true>(v, grid, v.force_variant, st);
     else
-        launch_force_mode<false>(v, grid, st);
+        launch_force_mode<false>(v, grid, v.force_variant, st);
     if (combine) combine_kernel<<<(v.nparts + 255) / 256, 256, 0, st>>>(v);
 }
 
@@ -1866,6 +2491,14 @@ void launch_singlebody_prep(const EngineView &v, int ntypes, double *type_ke, fl
 
 void launch_virial_reduce(const double *partials, int nwarps, double *out9, cudaStream_t st) {
     virial_reduce_kernel<<<1, 32, 0, st>>>(partials, nwarps, out9);
+}
+
+int bonded_virial_blocks(int num_sms) { return num_sms * 2; }
+
+void launch_bonded_virial(const EngineView &v, const BondedView &bv, int nb, int nx, int na, int nd, int nblocks,
+                          double *partials, double *out9, cudaStream_t st) {
+    bonded_virial_kernel<<<nblocks, kVirThreads, 0, st>>>(v, bv, nb, nx, na, nd, partials);
+    bonded_virial_reduce_kernel<<<1, 32, 0, st>>>(partials, nblocks, out9);
 }
 
 void launch_body(const EngineView &v, float4 *body_f, cudaStream_t st) {
@@ -1890,9 +2523,8 @@ void launch_bonded(const EngineView &v, const BondedView &bv, cudaStream_t st) {
 
 void launch_integrate(const EngineView &v, float4 *pos, float4 *vel, int *new_cell, int *in_count, int *in_list,
                       int *out_count, bool add_planes, cudaStream_t st) {
-    const int tb = 256;
-    integrate_kernel<<<(v.nparts + tb - 1) / tb, tb, 0, st>>>(v, pos, vel, new_cell, in_count, in_list, out_count,
-                                                             add_planes);
+    integrate_kernel<<<(v.nparts + kAdvThreads - 1) / kAdvThreads, kAdvThreads, 0, st>>>(
+        v, pos, vel, new_cell, in_count, in_list, out_count, add_planes);
 }
 
 void launch_rk_stage(const EngineView &v, float4 *pos, float4 *const *rk, int stage, bool add_planes,
@@ -1904,23 +2536,42 @@ void launch_rk_stage(const EngineView &v, float4 *pos, float4 *const *rk, int st
 void launch_rk_final(const EngineView &v, float4 *pos, float4 *vel, float4 *const *rk, int *new_cell, int *in_count,
                      int *in_list, int *out_count, bool add_planes, cudaStream_t st) {
     const RkState r{rk[0], rk[1], rk[2], rk[3], rk[4]};
-    rk_final_kernel<<<(v.nparts + 255) / 256, 256, 0, st>>>(v, pos, vel, r, new_cell, in_count, in_list, out_count,
-                                                           add_planes);
-}
-
-void launch_scan(int ncells, const int *old_count, const int *out_count, const int *in_count, int *new_start,
-                 int *new_count, unsigned long long *step, cudaStream_t st) {
-    scan_kernel<<<1, 1024, 0, st>>>(ncells, old_count, out_count, in_count, new_start, new_count, step);
+    rk_final_kernel<<<(v.nparts + kAdvThreads - 1) / kAdvThreads, kAdvThreads, 0, st>>>(
+        v, pos, vel, r, new_cell, in_count, in_list, out_count, add_planes);
 }
 
 void launch_scatter(const EngineView &v, const float4 *pos, const float4 *vel, const int *new_cell,
-                    const int *old_start, const int *old_count, int *in_count, const int *in_list, int *out_count,
-                    const int *new_start, float4 *pos_out, float4 *vel_out, int *cell_out, int *slot_of_id,
-                    cudaStream_t st) {
+                    const int *old_start, const int *old_count, const int *in_count, const int *in_list,
+                    const int *out_count, int *new_start, int *new_count, float4 *pos_out, float4 *vel_out,
+                    int *cell_out, int *slot_of_id, int *clear_in, int *clear_out, int *clear_chunk, int nchunks,
+                    unsigned *ctl, unsigned long long *step, cudaStream_t st) {
+    const int grid = (v.ncells + kScatterWarps - 1) / kScatterWarps;
+    scatter_kernel<<<grid, kScatterWarps * 32, 0, st>>>(v, v.ncells, pos, vel, new_cell, old_start, old_count,
+                                                        in_count, in_list, out_count, new_start, new_count, pos_out,
+                                                        vel_out, cell_out, slot_of_id, clear_in, clear_out,
+                                                        clear_chunk, nchunks, ctl, step);
+}
+
+void launch_number_density(const EngineView &v, const int *flux_off, float *nd_by_id, cudaStream_t st) {
+    number_density_kernel<<<(v.nparts + 127) / 128, 128, 0, st>>>(v, flux_off, nd_by_id);
+}
+
+void launch_load_place(const EngineView &v, const LoadView &ld, int *count, cudaStream_t st) {
+    place_kernel<<<(ld.n + 255) / 256, 256, 0, st>>>(v, ld, count);
+}
+
+void launch_load_order(const EngineView &v, const LoadView &ld, const int *count, int *start, float4 *pos_out,
+                       float4 *vel_out, int *cell_out, int *slot_of_id, cudaStream_t st) {
+    load_scan_kernel<<<1, 1024, 0, st>>>(count, v.ncells, start);
+    load_fill_kernel<<<(ld.n + 255) / 256, 256, 0, st>>>(ld, start);
     const int tb = 256;
-    const int grid = (v.ncells * 32 + tb - 1) / tb;
-    scatter_kernel<<<grid, tb, 0, st>>>(v, v.ncells, pos, vel, new_cell, old_start, old_count, in_count, in_list,
-                                         out_count, new_start, pos_out, vel_out, cell_out, slot_of_id);
+    load_order_kernel<<<(v.ncells * 32 + tb - 1) / tb, tb, 0, st>>>(v, ld, start, pos_out, vel_out, cell_out,
+                                                                     slot_of_id, v.sort_bounds);
+}
+
+void launch_unload(const EngineView &v, const float4 *force_ids, double *x, float *vel, float *f, int *cell,
+                   float *xrel, cudaStream_t st) {
+    unload_kernel<<<(v.nparts + 255) / 256, 256, 0, st>>>(v, force_ids, x, vel, f, cell, xrel);
 }
 
 void launch_energy(int ncells, const double *epot_cell, int nparts, const double *ebond_slot, const double *body_e,

@@ -90,7 +90,9 @@ __global__ void ke_final_kernel(const double *partials, int nblocks, int ntypes,
 }
 
 /* Looks up the device address of the scratch array for the current device,
- * once per device. */
+ * once per device. Under lazy module loading this first lookup may also load the
+ * module (allocating its code and the array), so callers make the first call at
+ * set-up. */
 int scratch_for_current_device(double **ptr) {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MXG_ERR_CUDA;

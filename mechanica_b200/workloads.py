@@ -316,6 +316,10 @@ def build_gpu(scn, rng_mode="reference"):
         m.bind(make_potential(kind, params), types[ti], types[tj])
     for (ti, fx, fy, fz) in scn["forces"]:
         m.bind(m.forces.ConstantForce([fx, fy, fz]), types[ti])
+    for (pos, size, ang) in scn.get("cuboids", []):
+        m.Cuboid(pos, size, ang)
+    for (ti, kind, params) in scn.get("cuboid_pots", []):
+        m.bind(make_potential(kind, params), m.Cuboid, types[ti])
     for (face, ti, kind, params) in scn.get("wall_pots", []):
         bcs = m.universe.boundary_conditions
         m.bind(make_potential(kind, params), bcs if face < 0 else getattr(bcs, m._FACES[face]), types[ti])
@@ -445,3 +449,48 @@ def build_adjoint(spec, stream=None):
     slots.append(dpds)
     u._add_particles(np.asarray(spec["x"]), np.asarray(spec["v"], dtype=np.float32), np.asarray(spec["t"], dtype=np.int32))
     return u, A.Parameters(u, slots)
+
+
+def bonded_block(nx=32, spacing=0.51, r0=0.5, k=20.0, d=0.05, a=6.0, margin=3.0, seed=17, noise=0.005, dt=0.002):
+    """A simple-cubic block of nx^3 particles with harmonic bonds to the six nearest
+    neighbours (k, r0; the block starts at `spacing`, stretched when spacing > r0) and a weak
+    form of the lattice's Morse nonbonded term (d, a, r0 = 0.5, radius 0.5; its table ends at
+    r = 0.95, between the third and fourth neighbour shells), overdamped, in the middle of a
+    periodic box with `margin` of free space on each side. dt keeps overdamped Euler inside
+    its stability limit dt 8 (2k + V''_Morse) < 2. Returns a spec dict (x, bonds, potentials'
+    construction parameters, box)."""
+    rng = np.random.default_rng(seed)
+    L = nx * spacing + 2 * margin
+    g = (np.arange(nx) - (nx - 1) / 2) * spacing + L / 2
+    x = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    x = (x + rng.normal(0, noise, size=x.shape)).astype(np.float32).astype(np.float64)
+    idx = np.arange(len(x)).reshape(nx, nx, nx)
+    bi, bj = [], []
+    for ax in range(3):
+        sa, sb = [slice(None)] * 3, [slice(None)] * 3
+        sa[ax], sb[ax] = slice(0, nx - 1), slice(1, nx)
+        bi.append(idx[tuple(sa)].ravel())
+        bj.append(idx[tuple(sb)].ravel())
+    cut = 1.0
+    cells = int(L // cut)
+    return dict(dim=[L, L, L], cells=[cells] * 3, cutoff=cut, dt=dt, bc=("periodic",) * 3, x=x,
+                t=np.zeros(len(x), dtype=np.int32), bi=np.concatenate(bi).astype(np.int32),
+                bj=np.concatenate(bj).astype(np.int32), morse=(d, a, 0.5, 1e-4, 1.45, 1e-3),
+                harmonic=(k, r0, 0.1, 1.2, 0.009), radius=0.5)
+
+
+def build_bonded_adjoint(spec, stream=None):
+    """The bonded block in the engine; returns the universe and the four differentiated
+    parameters: harmonic k and r0 of the bonds, Morse d and a."""
+    from . import adjoint as A
+    bc = {"x": spec["bc"][0], "y": spec["bc"][1], "z": spec["bc"][2]}
+    m.init(dim=spec["dim"], cells=spec["cells"], cutoff=spec["cutoff"], dt=spec["dt"], bc=bc, stream=stream)
+    Tp = type("Bead", (m.Particle,), {"mass": 1.0, "radius": spec["radius"], "dynamics": m.Overdamped})
+    u = m.universe
+    mp = m.Potential.morse(*spec["morse"])
+    m.bind(mp, Tp, Tp)
+    hp = m.Potential.harmonic(*spec["harmonic"])
+    x = np.asarray(spec["x"])
+    u._add_particles(x, np.zeros_like(x, dtype=np.float32), np.asarray(spec["t"], dtype=np.int32))
+    u._add_bonds(hp, spec["bi"], spec["bj"], 1e30)
+    return u, A.Parameters(u, [[(hp, 0)], [(hp, 1)], [(mp, 0)], [(mp, 1)]])

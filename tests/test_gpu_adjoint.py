@@ -167,3 +167,46 @@ def test_rdf_loss_gradient_matches_finite_differences():
         fd = (R.rdf_loss(xp, spec["t"], box, 0, 1, W.rdf_target()) -
               R.rdf_loss(xm, spec["t"], box, 0, 1, W.rdf_target())) / (2 * h)
         assert abs(gx[i, kk] - fd) <= 1e-3 * abs(fd) + 1e-4 * np.abs(gx).max(), (i, kk, gx[i, kk], fd)
+
+
+def test_adjoint_at_the_workload_parameters():
+    """The same check at the adjoint workload's own Morse steepness (a = 5; 512 particles, 4
+    steps, a snapshot every 2) with the workload's finite-difference step h = 1e-4. The Morse
+    d and a and the DPD gamma gradients agree with FP64 central differences within 1e-3.
+    r0 moves the table's range edge (s = r - 2 radius + r0 + 1 <= cutoff) across the pairs
+    that sit at the cutoff, so its finite difference carries O(jump / h) terms: its spread
+    over h = 1e-4, 1e-5, 1e-6 is measured here, and the adjoint must agree with the h = 1e-4
+    difference within that spread (or 1e-3, whichever is larger)."""
+    global T
+    saved = T
+    T = 4
+    try:
+        spec = W.adjoint_spec(n=N, seed=3, a=5.0)
+        target = W.rdf_target()
+        u, P = W.build_adjoint(spec, stream=torch.cuda.current_stream().cuda_stream)
+        sim = A.Simulation(u, P, nsteps=T, checkpoint_every=2, step0=0)
+        theta0 = P.theta()
+        theta = torch.tensor(theta0, dtype=torch.float64, requires_grad=True)
+        x0 = torch.tensor(spec["x"], dtype=torch.float64)
+        v0 = torch.tensor(spec["v"], dtype=torch.float64)
+        x4 = A.trajectory(theta, x0, v0, sim)
+        loss, _ = A.rdf_loss(x4, torch.tensor(target, dtype=torch.float64, device="cuda"), spec["dim"], 0, 1)
+        loss.backward()
+        adj = theta.grad.numpy()
+
+        def fd(k, h):
+            tp, tm = theta0.copy(), theta0.copy()
+            tp[k] += h
+            tm[k] -= h
+            return (_reference_loss(spec, tp, target=target)[0] - _reference_loss(spec, tm, target=target)[0]) / (2 * h)
+
+        for k in range(10):
+            f4 = fd(k, 1e-4)
+            if k in (2, 5, 8):  # Morse r0
+                spread = max(abs(f4 - fd(k, 1e-5)), abs(f4 - fd(k, 1e-6)))
+                assert abs(adj[k] - f4) <= max(GRAD_TOL * abs(f4), 2 * spread), (k, adj[k], f4, spread)
+            else:
+                assert abs(adj[k] - f4) <= GRAD_TOL * abs(f4) + 1e-6, (k, adj[k], f4)
+        u.close()
+    finally:
+        T = saved

@@ -50,11 +50,66 @@ def test_batched_force_pass_matches_reference_per_replica():
 
 
 def test_autotune_keeps_results():
+    """The autotuner picks a tile shape and grid on the state; forces stay within the FP32
+    summation bar of the default configuration, and every tile variant pinned by hand gives
+    the same bits on two engines built alike."""
     specs = _small_specs()
     u = W.build_gpu_batch(specs)
     u.force()
     f0 = u.state()[2]
     per_sm = u.autotune()
     assert per_sm > 0
+    variant, grid = u.force_config()
+    assert 0 <= variant < 4 and grid >= 1
     u.force()
-    assert np.array_equal(u.state()[2], f0)
+    assert rel_rms(u.state()[2], f0) <= 1e-6
+    for variant in range(4):
+        bits = []
+        for _ in range(2):
+            u = W.build_gpu_batch(specs)
+            u.force_config(variant, 148 * 4)
+            u.force()
+            bits.append(u.state()[2].view(np.uint32).copy())
+        assert np.array_equal(bits[0], bits[1])
+        assert rel_rms(bits[0].view(np.float32), f0) <= 1e-6
+
+
+@pytest.mark.skipif(not refengine.available(), reason="reference library not built")
+def test_cell_sorting_ensemble_sample_matches_reference_per_replica():
+    """Replicas drawn from the batched workload itself (256 cell-sorting replicas, seed 5:
+    N uniform in [1000, 20000], density 0.8, cutoff 2.5, Morse a = 5): the largest replica,
+    the one with the smallest d_AB, and two more picked by a seeded draw, in one engine.
+    Per replica against the reference engine: cell-relative positions bit-exact after the
+    placement, forces of the first pass within 1e-5 relative RMS, and after one step the
+    cells identical and the positions within 1e-5."""
+    specs = W.cell_sorting_specs(nrep=256, seed=5)
+    n = np.array([len(s["t"]) for s in specs])
+    dab = np.array([s["pots"][1][1][0] for s in specs])
+    pick = [int(np.argmax(n)), int(np.argmin(dab))]
+    rng = np.random.default_rng(1)
+    pick += [int(k) for k in rng.choice([k for k in range(len(specs)) if k not in pick], size=2, replace=False)]
+    sample = [specs[k] for k in pick]
+    assert max(len(s["t"]) for s in sample) > 19000 and min(dab[pick]) < 0.06
+    u = W.build_gpu_batch(sample)
+    u.force()
+    x, v, f, c, xr = u.state()
+    refs = [refengine.run(dict(sc, action="force", runners=8)) for sc in sample]
+    off = 0
+    for sc, ref in zip(sample, refs):
+        k = len(sc["t"])
+        assert rel_rms(f[off:off + k], ref["f"]) <= 1e-5
+        assert np.array_equal(xr[off:off + k].view(np.uint32), ref["xrel"].view(np.uint32))
+        off += k
+    u.steps(1)
+    x, v, f, c, xr = u.state()
+    off, coff = 0, 0
+    for sc in sample:
+        k = len(sc["t"])
+        ref = refengine.run(dict(sc, action="steps", nsteps=1, runners=8))
+        assert np.array_equal(c[off:off + k] - coff, ref["cell"])
+        L = np.asarray(sc["dim"])
+        d = x[off:off + k] - ref["xabs"]
+        d -= L * np.round(d / L)
+        assert np.abs(d).max() < 1e-5
+        off += k
+        coff += int(np.prod(ref["cdim"]))

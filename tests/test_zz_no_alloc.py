@@ -77,3 +77,37 @@ def test_noalloc_rejects_too_many_types():
     rc = lib().mxg_kinetic_energy_noalloc(p, p, 8, ctypes.c_void_p(mass.data_ptr()), 65,
                                           ctypes.c_void_p(out.data_ptr()), None)
     assert rc == -6  # MXG_ERR_RANGE: more types than the scratch array holds
+
+
+def test_noalloc_on_a_stream_and_with_unlisted_types():
+    """On a caller's stream (not the default one), and with ntypes smaller than the largest
+    type id present: particles whose type is outside [0, ntypes) add nothing, so the total
+    is the sum over the types that remain."""
+    import torch
+    from mechanica_b200._native import lib
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(7)
+    n = 5000
+    types = rng.integers(0, 4, size=n).astype(np.int32)
+    v = rng.normal(size=(n, 3)).astype(np.float32)
+    pos = np.zeros((n, 4), dtype=np.float32)
+    pos[:, 3] = types.view(np.float32)
+    vel = np.zeros((n, 4), dtype=np.float32)
+    vel[:, :3] = v
+    masses = [1.0, 2.5, 0.5, 4.0]
+    pd, vd = torch.from_numpy(pos).to(dev), torch.from_numpy(vel).to(dev)
+    st = torch.cuda.Stream(device=dev)
+    for ntypes in (4, 2):
+        tm = torch.tensor(masses[:ntypes], dtype=torch.float64, device=dev)
+        out = torch.full((1 + ntypes,), -1.0, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize(dev)
+        rc = lib().mxg_kinetic_energy_noalloc(ctypes.c_void_p(vd.data_ptr()), ctypes.c_void_p(pd.data_ptr()), n,
+                                              ctypes.c_void_p(tm.data_ptr()), ntypes,
+                                              ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(st.cuda_stream))
+        assert rc == 0
+        st.synchronize()
+        res = out.cpu().numpy()
+        want = _per_type_host(v, types, masses[:ntypes])
+        assert np.allclose(res[1:], want, rtol=1e-12, atol=1e-12)
+        assert abs(res[0] - want.sum()) <= 1e-12 * abs(want.sum())
