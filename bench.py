@@ -13,7 +13,9 @@ a 256 MiB write). e2e = the same metric through the C ABI in the reference's
 data format with host buffers: every step engine_load's the absolute positions
 and velocities by particle id from pinned host memory, steps, and
 engine_unload's them back (host clock); the raw slot-order state copy is
-reported beside it.
+reported beside it. roofline: the force kernel against the FP32 pipe (and, as
+hbm_view, against the measured copy bandwidth); rebin_view: the integrator and
+the re-binning scatter against the measured copy bandwidth.
 
 --impl reference times the reference's own CPU engine (compiled in place from
 the reference sources, oracle/_ref) on this host's cores for the same workload.
@@ -97,7 +99,46 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-forms", action="store_true", help="skip the other configurations (batched, LJ, lattice)")
+    ap.add_argument("--record-counters", metavar="CSV",
+                    help="write the force-launch counters file from an ncu --csv capture of one force launch "
+                         "(dram__bytes_read.sum, dram__bytes_write.sum, smsp__inst_executed.sum) and exit")
     return ap.parse_args()
+
+
+def record_counters(csv_path):
+    """Writes COUNTERS from an ncu CSV capture of one force launch of the default workload, with
+    the hash of the current sources (the capture must have run these sources)."""
+    import csv
+    vals = {}
+    kernel = None
+    with open(csv_path) as f:
+        rows = [r for r in csv.reader(f)]
+    hdr = next(i for i, r in enumerate(rows) if "Metric Name" in r)
+    cols = rows[hdr]
+    for r in rows[hdr + 1:]:
+        if len(r) != len(cols):
+            continue
+        d = dict(zip(cols, r))
+        if "force_kernel" not in d["Kernel Name"]:
+            continue
+        if kernel is None:
+            kernel = (d["ID"], d["Kernel Name"])
+        if (d["ID"], d["Kernel Name"]) != kernel:
+            continue
+        vals[d["Metric Name"]] = int(float(d["Metric Value"].replace(",", "")))
+    need = ("dram__bytes_read.sum", "dram__bytes_write.sum", "smsp__inst_executed.sum")
+    missing = [k for k in need if k not in vals]
+    if missing:
+        raise SystemExit(f"{csv_path}: no {missing} for a force_kernel launch")
+    with open(COUNTERS, "w") as f:
+        f.write(f"# one force launch of the default workload (ncu capture {os.path.basename(csv_path)}: "
+                f"{kernel[1].split('(')[0]})\n")
+        f.write(f"sources_sha16 {sources_sha16()}\n")
+        f.write(f"dram_bytes_per_launch {vals['dram__bytes_read.sum'] + vals['dram__bytes_write.sum']}\n")
+        f.write(f"dram_bytes_read {vals['dram__bytes_read.sum']}\n")
+        f.write(f"dram_bytes_write {vals['dram__bytes_write.sum']}\n")
+        f.write(f"warp_instructions_per_launch {vals['smsp__inst_executed.sum']}\n")
+    print(open(COUNTERS).read(), end="")
 
 
 def max_over_ranks(x, world, device=None):
@@ -516,6 +557,9 @@ class torch_stream:
 
 def main():
     args = parse()
+    if args.record_counters:
+        record_counters(args.record_counters)
+        return
     if args.impl == "reference":
         reference_arm(args)
         return
@@ -689,6 +733,26 @@ def main():
             "warp_instructions_per_launch": wi, "achieved": issue, "peak": issue_peak,
             "unit": "G warp-instructions/s", "frac": issue / issue_peak,
             "peak_source": f"{sm_count} SMs x 4 schedulers x {max_mhz:.0f} MHz (nominal issue rate)"}
+
+    # ---- re-binning against the measured HBM bandwidth: the integrator (advance + mover counts)
+    # and the scatter (re-binning + next key bounds), each timed with CUDA events at the phase
+    # boundaries of whole steps (kernel by kernel, no L2 flush: the integrator reads the received
+    # planes the force pass just wrote); algorithmic bytes 88 per particle for each (integrate:
+    # pos, vel, force, type read, pos, vel, cell written; scatter: key, pos, vel, id, type read
+    # and written) ----
+    tm = (ctypes.c_double * 16)()
+    Kt = 20
+    barrier()
+    check(L.mxg_engine_step_timed(e, Kt, tm, 16), "step_timed")
+    barrier()
+    if hbm_peak:
+        rb = {"peak": hbm_peak, "unit": "GB/s", "bytes_per_particle": 88,
+              "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)", "steps": Kt}
+        for name, slot in (("integrate_kernel", 11), ("scatter_kernel", 14)):
+            t = tm[slot] / Kt
+            rate = 88 * n / (t / 1e3) / 1e9
+            rb[name] = {"ms_per_launch": t, "achieved": rate, "frac": rate / hbm_peak}
+        roofline["rebin_view"] = rb
 
     # ---- CPU baseline and accuracy (reference engine, rank 0, N=1 only) ----
     cpu = None

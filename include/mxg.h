@@ -235,6 +235,13 @@ int mxg_engine_set_target_temperature(mxg_engine *e, int type, double temperatur
 /* Adds n particles (positions double[3n] in global coordinates, velocities float[3n]); ids_out
  * receives consecutive ids (may be NULL). */
 int mxg_engine_addparts(mxg_engine *e, int n, const double *x, const float *v, const int *type, int *ids_out);
+/* Adds particles of replica rep by cell (replica-local index, as the engine numbers cells: x-major)
+ * and FP32 cell-relative position, kept exactly as given (space_cell's own representation, the
+ * state the re-binning leaves): a state taken from another engine with the same space continues
+ * bit for bit. Used to hand particles between slabs of a decomposed box. No counterpart call in
+ * the reference (its particles enter through engine_addpart's global positions). */
+int mxg_engine_addparts_cellrel(mxg_engine *e, int rep, int n, const int *cell, const float *xrel, const float *v,
+                                const int *type, int *ids_out);
 /* Adds n harmonic/table bonds between particle ids i[k], j[k], all with potential p. */
 int mxg_engine_addbonds(mxg_engine *e, int n, const int *i, const int *j, const mxg_potential *p,
                         double dissociation_energy, int *ids_out);

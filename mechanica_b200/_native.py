@@ -76,6 +76,8 @@ _SIGS = {
     "mxg_engine_add_singlebody_force": ([_vp, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float],
                                         ctypes.c_int),
     "mxg_engine_addparts": ([_vp, ctypes.c_int, _c_double_p, _c_float_p, _c_int_p, _c_int_p], ctypes.c_int),
+    "mxg_engine_addparts_cellrel": ([_vp, ctypes.c_int, ctypes.c_int, _c_int_p, _c_float_p, _c_float_p, _c_int_p,
+                                     _c_int_p], ctypes.c_int),
     "mxg_engine_addbonds": ([_vp, ctypes.c_int, _c_int_p, _c_int_p, _vp, ctypes.c_double, _c_int_p], ctypes.c_int),
     "mxg_engine_addangles": ([_vp, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p, _vp, _c_int_p], ctypes.c_int),
     "mxg_engine_set_boundary_potential": ([_vp, ctypes.c_int, ctypes.c_int, _vp], ctypes.c_int),

@@ -423,6 +423,8 @@ struct mxg_engine {
     std::vector<float> pv;
     std::vector<int> ptype;
     std::vector<int> prep;                  // replica of each particle
+    std::vector<int> pcell;                 // given cell (replica-local) of each particle, or -1: placed from px
+    std::vector<float> pxr;                 // given cell-relative position (3 per particle) where pcell >= 0
     std::vector<BondInfo> bonds;
     std::vector<AngleInfo> angles;
     std::vector<ExclusionInfo> exclusions;
@@ -661,6 +663,11 @@ struct mxg_engine {
         std::vector<float> xr(3 * (size_t)n);
         for (int p = 0; p < n; ++p) {
             const Space &sp = spaces[prep[p]];
+            if (pcell[p] >= 0) {  // added with its cell and cell-relative position: kept as given
+                cell[p] = sp.cell_offset + pcell[p];
+                for (int k = 0; k < 3; ++k) xr[3 * (size_t)p + k] = pxr[3 * (size_t)p + k];
+                continue;
+            }
             int lc;
             int rc = sp.place(&px[3 * (size_t)p], lc, &xr[3 * (size_t)p]);
             if (rc != MXG_OK) return rc;
@@ -1887,6 +1894,36 @@ int mxg_engine_addparts_replica(mxg_engine *e, int rep, int n, const double *x, 
         }
         e->ptype.push_back(type[k]);
         e->prep.push_back(rep);
+        e->pcell.push_back(-1);
+        for (int q = 0; q < 3; ++q) e->pxr.push_back(0.f);
+        if (ids_out) ids_out[k] = first + k;
+    }
+    return MXG_OK;
+}
+
+int mxg_engine_addparts_cellrel(mxg_engine *e, int rep, int n, const int *cell, const float *xrel, const float *v,
+                                const int *type, int *ids_out) {
+    if (!e || (n > 0 && (!cell || !xrel || !type))) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    if (rep < 0 || rep >= (int)e->spaces.size()) return MXG_ERR_RANGE;
+    const Space &sp = e->spaces[rep];
+    for (int k = 0; k < n; ++k) {
+        if (type[k] < 0 || type[k] >= (int)e->types.size()) return MXG_ERR_RANGE;
+        if (cell[k] < 0 || cell[k] >= sp.ncells) return MXG_ERR_CELL;
+        for (int q = 0; q < 3; ++q)
+            if (!std::isfinite(xrel[3 * (size_t)k + q])) return MXG_ERR_ARG;
+    }
+    const int first = (int)e->ptype.size();
+    for (int k = 0; k < n; ++k) {
+        for (int q = 0; q < 3; ++q) {
+            // the global position the cell-relative one stands for (reported before the start)
+            e->px.push_back(sp.cell_origin[3 * (size_t)cell[k] + q] + (double)xrel[3 * (size_t)k + q]);
+            e->pv.push_back(v ? v[3 * (size_t)k + q] : 0.f);
+            e->pxr.push_back(xrel[3 * (size_t)k + q]);
+        }
+        e->ptype.push_back(type[k]);
+        e->prep.push_back(rep);
+        e->pcell.push_back(cell[k]);
         if (ids_out) ids_out[k] = first + k;
     }
     return MXG_OK;

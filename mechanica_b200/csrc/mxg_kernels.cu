@@ -362,7 +362,8 @@ __device__ __forceinline__ void dpd_fast(const float4 &q0, const float4 &q1, boo
 template <bool kDPD, int kMode, bool kPure, class TS>
 __device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD, TS> &sm, const float4 *tinfo, int qhead,
                                            int nb, int i0, int own_start, int pot_base, unsigned rng_mode,
-                                           float cut2_pair, float cut2_self, double &ecell, unsigned long long &npair,
+                                           float cut2_pair, float cut2_self, bool self_once, double &ecell,
+                                           unsigned long long &npair,
                                            double *vir) {
     const int lane = threadIdx.x & 31;
     float cx = 0.f, cy = 0.f, cz = 0.f;
@@ -391,7 +392,9 @@ __device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD, 
         const float dxo = dx, dyo = dy, dzo = dz;  // before the r < a substitution
         const int ti = __float_as_int(xi.w), tj = __float_as_int(b.w);
         const bool i_first = role == kRoleFirst || (role == kRoleSelf && i < jl);
-        nbside = role == kRoleFirst;
+        // FIRST pairs, and a cell's own pairs when each is evaluated once (by its lower index),
+        // put the second particle's share into the staged neighbour's sums
+        nbside = role == kRoleFirst || (role == kRoleSelf && self_once);
         // the exact cutoff test of the pair loops (pass 1 queued a superset)
         const bool inside = r2 <= (role == kRoleSelf ? cut2_self : cut2_pair);
         if (kPure && inside) {
@@ -580,6 +583,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, TS::kBlocks) force_kernel
             const bool exit_test = (S.prune & 2) != 0;  // cell-pair exit test
             const float sbias = S.sort_bias, sdscale = S.sort_dscale;
             const int dmaxdist = S.dmaxdist;
+            // a cell whose particles fit one own pass evaluates each of its own pairs once
+            const bool self_once = n <= kOwn;
             for (int i0 = 0; i0 < n; i0 += kOwn) {
                 const int ni = min(kOwn, n - i0);
                 __syncwarp();
@@ -733,15 +738,21 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, TS::kBlocks) force_kernel
                                 const int i = i0 + il;
                                 const unsigned long long mk = sm.own_mask[il];
                                 unsigned hb[kChunks];
+                                bool hv[kChunks];
 #pragma unroll
                                 for (int u = 0; u < kChunks; ++u) {
                                     hb[u] = 0u;
+                                    hv[u] = false;
                                     if (u * 32 < M) {
                                         const float dx = __fsub_rn(xi.x, rbx[u]);
                                         const float dy = __fsub_rn(xi.y, rby[u]);
                                         const float dz = __fsub_rn(xi.z, rbz[u]);
                                         const float r2 = dot3_rn(dx, dy, dz);
-                                        bool hit = (r2 <= rc2[u]) & (((mk >> rtj[u]) & 1ull) != 0ull) & (rself[u] != i);
+                                        // a cell's own pair once (neighbour index above the own one; -1, not
+                                        // a SELF neighbour, compares as the largest unsigned value), or from
+                                        // both sides when the cell takes several own-particle passes
+                                        const bool pair_ok = self_once ? (unsigned)rself[u] > (unsigned)i : rself[u] != i;
+                                        bool hit = (r2 <= rc2[u]) & (((mk >> rtj[u]) & 1ull) != 0ull) & pair_ok;
                                         if (prune && hit && rself[u] < 0) {
                                             // runner_dopair's pruning: a pair (first, second) is evaluated
                                             // only when key_second + dnshift - key_first < dmaxdist
@@ -754,11 +765,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, TS::kBlocks) force_kernel
                                             hit = sm.nb_key[jj] + (epk >> 8) - okey < dmaxdist;
                                         }
                                         hb[u] = __ballot_sync(kFull, hit);
+                                        hv[u] = hit;
                                     }
                                 }
 #pragma unroll
                                 for (int u = 0; u < kChunks; ++u) {
-                                    if ((hb[u] >> lane) & 1u)
+                                    if (hv[u])
                                         sm.queue[(qtail + __popc(hb[u] & lt_mask)) & (kQueue - 1)] =
                                             (unsigned short)((il << 8) | (u * 32 + lane));
                                     qtail += __popc(hb[u]);
@@ -768,14 +780,23 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, TS::kBlocks) force_kernel
                                 const int nb = min(32, qtail - qhead);
                                 __syncwarp();
                                 eval_batch<kDPD, kMode, kPure, TS>(v, sm, tinfo, qhead, nb, i0, start, pot_base, rng_mode, cut2_pair,
-                                               cut2_self, ecell, npair, vir);
+                                               cut2_self, self_once, ecell, npair, vir);
                                 qhead += nb;
                             }
                         }
                         __syncwarp();
-                        // ---- neighbour-side sums of FIRST entries into their planes
+                        // ---- neighbour-side sums of FIRST entries into their planes; those of a
+                        // cell's own particles (pairs evaluated once) into their own sums
                         for (int idx = lane; idx < M && kMode != 2; idx += 32) {
                             const int meta = __float_as_int(sm.nb_s[idx].w);
+                            if (self_once && (meta & 3) == kRoleSelf) {
+                                const float4 g = sm.nb_f[idx];
+                                float4 &o = sm.own_f[meta >> 8];  // one own pass: own index = index in the cell
+                                o.x += g.x;
+                                o.y += g.y;
+                                o.z += g.z;
+                                continue;
+                            }
                             if ((meta & 3) != kRoleFirst) continue;
                             const int ke = (meta >> 2) & 31;
                             float4 *dst = v.planes + (size_t)sm.ent_rev[ke] * v.nparts + sm.ent_slot[ke] + (meta >> 8);
@@ -2133,8 +2154,10 @@ __global__ void __launch_bounds__(kScatterWarps * 32, 5) scatter_kernel(
             clear_in[c] = 0;
             clear_out[c] = 0;
         }
-        // the next force pass's cell-pair exit test reads the new cell's key bounds
+        // the next force pass's cell-pair exit test reads the new cell's key bounds from the slots
+        // just written (the barrier makes the lanes' stores visible to the whole warp)
         const DevSpace &S = v.spaces[v.cell_rep[c]];
+        __syncwarp();
         if (nn > 0 && (S.prune & 2))
             cell_sort_bounds(pos_out, base, nn, S.sort_bias, S.sort_dscale, v.axes, v.sort_bounds + c * 13);
     }

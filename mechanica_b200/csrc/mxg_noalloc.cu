@@ -41,13 +41,17 @@ std::mutex g_scratch_mutex;
 
 /* Stage 1: each block walks its share of the particles in chunks of blockDim;
  * for every chunk the per-particle energies go to shared memory and thread t
- * (t < ntypes) adds the chunk's type-t energies in index order. */
+ * (t < ntypes) adds the chunk's type-t energies in index order. With one type,
+ * every thread keeps a running sum over its chunks and the block adds them in a
+ * fixed tree at the end (warp shuffles, then the warps in order): no serial scan. */
 __global__ void __launch_bounds__(kNoallocThreads)
     ke_partials_kernel(const float4 *__restrict__ vel, const float4 *__restrict__ pos, int n,
                        const double *__restrict__ type_mass, int ntypes, double *partials) {
     __shared__ float se[kNoallocThreads];
     __shared__ int stype[kNoallocThreads];
-    double acc = 0.0;  // thread t < ntypes: running sum of type t
+    __shared__ double swarp[kNoallocThreads / 32];
+    double acc = 0.0;  // thread t < ntypes: running sum of type t (one type: this thread's particles)
+    const bool one_type = ntypes == 1;
     for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const int s = base + threadIdx.x;
         float e = 0.0f;
@@ -61,6 +65,10 @@ __global__ void __launch_bounds__(kNoallocThreads)
             const float v2 = __fadd_rn(__fadd_rn(__fmul_rn(u.x, u.x), __fmul_rn(u.y, u.y)), __fmul_rn(u.z, u.z));
             e = (float)__dmul_rn(__dmul_rn(0.5, type_mass[t]), (double)v2);
         }
+        if (one_type) {
+            acc += (double)e;
+            continue;
+        }
         se[threadIdx.x] = e;
         stype[threadIdx.x] = t;
         __syncthreads();
@@ -68,6 +76,17 @@ __global__ void __launch_bounds__(kNoallocThreads)
             for (int k = 0; k < (int)blockDim.x; ++k)
                 if (stype[k] == (int)threadIdx.x) acc += (double)se[k];
         __syncthreads();
+    }
+    if (one_type) {
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+        if ((threadIdx.x & 31) == 0) swarp[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double b = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b += swarp[w];
+            partials[blockIdx.x] = b;
+        }
+        return;
     }
     if ((int)threadIdx.x < ntypes) partials[blockIdx.x * ntypes + threadIdx.x] = acc;
 }
