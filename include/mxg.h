@@ -242,6 +242,12 @@ int mxg_engine_addparts(mxg_engine *e, int n, const double *x, const float *v, c
  * the reference (its particles enter through engine_addpart's global positions). */
 int mxg_engine_addparts_cellrel(mxg_engine *e, int rep, int n, const int *cell, const float *xrel, const float *v,
                                 const int *type, int *ids_out);
+/* Before mxg_engine_start: the particle count on which the force pass's work-item split (cells split
+ * into several items when they are too few to fill the GPU, finer when the mean occupancy is 16 or
+ * more) is decided, instead of this engine's own; 0 restores the default. A slab of a decomposed box
+ * passes the whole box's count, so that its cells are split, and their sums ordered, as in the
+ * undivided box. */
+int mxg_engine_set_occupancy_hint(mxg_engine *e, long long nparts);
 /* Adds n harmonic/table bonds between particle ids i[k], j[k], all with potential p. */
 int mxg_engine_addbonds(mxg_engine *e, int n, const int *i, const int *j, const mxg_potential *p,
                         double dissociation_energy, int *ids_out);

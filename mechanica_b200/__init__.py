@@ -584,6 +584,9 @@ class _Universe:
         self._v = np.zeros((0, 3), dtype=np.float32)
         self._t = np.zeros(0, dtype=np.int32)
         self._r = np.zeros(0, dtype=np.int32)
+        self._c = np.zeros(0, dtype=np.int32)  # given cell of a particle added cell-relative, else -1
+        self._xr = np.zeros((0, 3), dtype=np.float32)  # its cell-relative position
+        self.occupancy_hint = 0  # particle count the force pass's work-item split is decided on (0: own)
         self._started = False
         self._dirty = False
         self._new_engine()
@@ -695,8 +698,34 @@ class _Universe:
         self._v = np.concatenate([self._v, np.asarray(v, dtype=np.float32)])
         self._t = np.concatenate([self._t, np.asarray(t, dtype=np.int32)])
         self._r = np.concatenate([self._r, np.full(len(t), int(replica), dtype=np.int32)])
+        self._c = np.concatenate([self._c, np.full(len(t), -1, dtype=np.int32)])
+        self._xr = np.concatenate([self._xr, np.zeros((len(t), 3), dtype=np.float32)])
         self._dirty = True
         return list(range(first, first + len(t)))
+
+    def _add_particles_cellrel(self, cell, xrel, v, t, replica=0):
+        """Adds particles by cell (the engine's cell index in the replica) and FP32 cell-relative
+        position, kept exactly as given (mxg_engine_addparts_cellrel): a state handed over from
+        another engine over the same space continues bit for bit."""
+        cell = np.asarray(cell, dtype=np.int32)
+        xrel = np.asarray(xrel, dtype=np.float32).reshape(-1, 3)
+        cdim, h = self.cell_grid()
+        loc = np.stack([cell // (cdim[1] * cdim[2]), (cell // cdim[2]) % cdim[1], cell % cdim[2]], axis=1)
+        x = np.asarray(self.origin) + loc * h + xrel.astype(np.float64)  # the global positions they stand for
+        k0 = len(self._t)
+        first = self._add_particles(x, v, t, replica)
+        self._c[k0:] = cell
+        self._xr[k0:] = xrel
+        return first
+
+    def cell_grid(self):
+        """(cells per axis, cell edge) of the engine's grid (space_init's cdim and h)."""
+        cdim = (ctypes.c_int * 3)()
+        h = (ctypes.c_double * 3)()
+        nc = ctypes.c_int()
+        per = ctypes.c_uint()
+        check(lib().mxg_engine_space_info(self._e, cdim, h, ctypes.byref(nc), ctypes.byref(per)), "space_info")
+        return np.array(cdim[:], dtype=np.int64), np.array(h[:])
 
     def add_replica(self, dim, cells, bc=None, origin=(0.0, 0.0, 0.0)):
         """Adds an independent simulation box that steps together with the others
@@ -918,6 +947,7 @@ class _Universe:
             check(lib().mxg_engine_unload(self._e, n, ptr(x, ctypes.c_double), ptr(v, ctypes.c_float), None, None,
                                           None), "unload")
             self._x, self._v = x, v
+            self._c[:] = -1  # the pulled global positions now stand for every particle
             if self._spec_width and self._spec.shape[1]:
                 sp = np.zeros((n, self._spec.shape[1]), dtype=np.float32)
                 check(lib().mxg_engine_get_species(self._e, n, sp.shape[1], ptr(sp, ctypes.c_float)), "get_species")
@@ -929,17 +959,27 @@ class _Universe:
         if self._started or self._dirty:
             self._new_engine()
         n = len(self._t)
-        # particles go in id order; consecutive runs of one replica are added together
+        # particles go in id order; consecutive runs of one replica (and of one way of placing them)
+        # are added together
         k = 0
         while k < n:
             rep = int(self._r[k])
+            given = self._c[k] >= 0
             e = k
-            while e < n and self._r[e] == rep:
+            while e < n and self._r[e] == rep and (self._c[e] >= 0) == given:
                 e += 1
-            check(lib().mxg_engine_addparts_replica(self._e, rep, e - k, ptr(f64(self._x[k:e]), ctypes.c_double),
-                                                    ptr(f32(self._v[k:e]), ctypes.c_float),
-                                                    ptr(i32(self._t[k:e]), ctypes.c_int), None), "addparts")
+            if given:
+                check(lib().mxg_engine_addparts_cellrel(self._e, rep, e - k, ptr(i32(self._c[k:e]), ctypes.c_int),
+                                                        ptr(f32(self._xr[k:e]), ctypes.c_float),
+                                                        ptr(f32(self._v[k:e]), ctypes.c_float),
+                                                        ptr(i32(self._t[k:e]), ctypes.c_int), None), "addparts")
+            else:
+                check(lib().mxg_engine_addparts_replica(self._e, rep, e - k, ptr(f64(self._x[k:e]), ctypes.c_double),
+                                                        ptr(f32(self._v[k:e]), ctypes.c_float),
+                                                        ptr(i32(self._t[k:e]), ctypes.c_int), None), "addparts")
             k = e
+        if self.occupancy_hint:
+            check(lib().mxg_engine_set_occupancy_hint(self._e, int(self.occupancy_hint)), "occupancy_hint")
         if self._spec_width:
             sp = np.ascontiguousarray(self._spec, dtype=np.float32)
             check(lib().mxg_engine_set_species(self._e, n, sp.shape[1], ptr(sp, ctypes.c_float)), "set_species")

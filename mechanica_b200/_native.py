@@ -78,6 +78,7 @@ _SIGS = {
     "mxg_engine_addparts": ([_vp, ctypes.c_int, _c_double_p, _c_float_p, _c_int_p, _c_int_p], ctypes.c_int),
     "mxg_engine_addparts_cellrel": ([_vp, ctypes.c_int, ctypes.c_int, _c_int_p, _c_float_p, _c_float_p, _c_int_p,
                                      _c_int_p], ctypes.c_int),
+    "mxg_engine_set_occupancy_hint": ([_vp, ctypes.c_longlong], ctypes.c_int),
     "mxg_engine_addbonds": ([_vp, ctypes.c_int, _c_int_p, _c_int_p, _vp, ctypes.c_double, _c_int_p], ctypes.c_int),
     "mxg_engine_addangles": ([_vp, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p, _vp, _c_int_p], ctypes.c_int),
     "mxg_engine_set_boundary_potential": ([_vp, ctypes.c_int, ctypes.c_int, _vp], ctypes.c_int),

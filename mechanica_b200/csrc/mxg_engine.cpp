@@ -480,6 +480,7 @@ struct mxg_engine {
     int *d_item_ctr = nullptr;          // the force kernel's work-item counter and finished-warp count
     int *d_item_order = nullptr;        // work items, most crowded cells first (when cells are split)
     bool order_items = false;
+    long long occupancy_hint = 0;       // particle count the work-item split is decided on (0: nparts)
     bool dpd_pure = false;              // every pair potential DPD, no summed second term, no Philox
     int *d_cell_planes = nullptr;       // planes summed into each cell's forces
     int nitems = 0;
@@ -1060,7 +1061,7 @@ int mxg_engine::start(cudaStream_t st) {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         num_sms = sms;
     }
-    const bool crowded = (long long)nparts >= 16LL * std::max(1, ncells);
+    const bool crowded = (occupancy_hint > 0 ? occupancy_hint : (long long)nparts) >= 16LL * std::max(1, ncells);
     const int want_warps = num_sms * (crowded ? 64 : 5 * kWarpsPerBlock);
     const int parts = std::max(1, std::min(kMaxCellParts, (want_warps + ncells - 1) / std::max(1, ncells)));
     std::vector<int> nb_off(ncells + 1, 0), nb_cell, nb_rev, hplanes(ncells, 0);
@@ -1926,6 +1927,14 @@ int mxg_engine_addparts_cellrel(mxg_engine *e, int rep, int n, const int *cell, 
         e->pcell.push_back(cell[k]);
         if (ids_out) ids_out[k] = first + k;
     }
+    return MXG_OK;
+}
+
+int mxg_engine_set_occupancy_hint(mxg_engine *e, long long nparts) {
+    if (!e) return MXG_ERR_NULL;
+    if (e->started) return MXG_ERR_STATE;
+    if (nparts < 0) return MXG_ERR_ARG;
+    e->occupancy_hint = nparts;
     return MXG_OK;
 }
 
