@@ -289,6 +289,30 @@ __device__ __forceinline__ int sort_key(float x, float y, float z, const float *
     return (int)(unsigned)__fmul_rn(dscale, proj);
 }
 
+/* sort_key along the reference's sort direction sid (runner_dosort.cpp's 13 normalised cell
+ * shifts, the same FP32 values as SortAxes holds); with sid known at compile time the direction
+ * is three immediates. */
+__device__ __forceinline__ int sort_key_sid(int sid, float x, float y, float z, float bias, float dscale) {
+    constexpr float a = (float)5.773502691896258e-01, b = (float)7.071067811865475e-01;
+    float n[3];
+    switch (sid) {
+        case 0: n[0] = a; n[1] = a; n[2] = a; break;
+        case 1: n[0] = b; n[1] = b; n[2] = 0.f; break;
+        case 2: n[0] = a; n[1] = a; n[2] = -a; break;
+        case 3: n[0] = b; n[1] = 0.f; n[2] = b; break;
+        case 4: n[0] = 1.f; n[1] = 0.f; n[2] = 0.f; break;
+        case 5: n[0] = b; n[1] = 0.f; n[2] = -b; break;
+        case 6: n[0] = a; n[1] = -a; n[2] = a; break;
+        case 7: n[0] = b; n[1] = -b; n[2] = 0.f; break;
+        case 8: n[0] = a; n[1] = -a; n[2] = -a; break;
+        case 9: n[0] = 0.f; n[1] = b; n[2] = b; break;
+        case 10: n[0] = 0.f; n[1] = 1.f; n[2] = 0.f; break;
+        case 11: n[0] = 0.f; n[1] = b; n[2] = -b; break;
+        default: n[0] = 0.f; n[1] = 0.f; n[2] = 1.f; break;
+    }
+    return sort_key(x, y, z, n, bias, dscale);
+}
+
 /* Cell coordinates of global cell c in its replica's grid. */
 __device__ __forceinline__ void cell_loc(const DevSpace &S, int c, int loc[3]) {
     const int l = c - S.cell_offset;

@@ -468,6 +468,7 @@ struct mxg_engine {
     float *d_ld_v = nullptr, *d_ul_v = nullptr, *d_ul_f = nullptr, *d_ul_xrel = nullptr;
     float4 *d_ld_xr = nullptr, *d_ld_vel = nullptr;
     int *d_ld_cell = nullptr, *d_ld_ids = nullptr, *d_ld_count = nullptr, *d_ld_fill = nullptr, *d_ld_err = nullptr;
+    int *h_ld_err = nullptr;  // pinned: the load's out-of-box flag, read back without a staging copy
     int *d_type_of_id = nullptr, *d_rep_of_id = nullptr, *d_ul_cell = nullptr;
     int *d_slot_of_id = nullptr;
     int *d_cell_rep = nullptr;
@@ -553,6 +554,7 @@ struct mxg_engine {
         for (int k = 0; k < 2; ++k)
             if (graph[k]) cudaGraphExecDestroy(graph[k]);
         for (void *p : allocations) cudaFree(p);
+        if (h_ld_err) cudaFreeHost(h_ld_err);
         if (own_stream) cudaStreamDestroy(own_stream);
     }
 
@@ -1496,6 +1498,10 @@ int mxg_engine::build_graphs() {
 int mxg_engine::load_state(const double *x, const float *v, int n) {
     if (n != nparts) return MXG_ERR_ARG;
     if (nparts == 0) return MXG_OK;
+    if (!h_ld_err && cudaMallocHost((void **)&h_ld_err, sizeof(int)) != cudaSuccess) {
+        h_ld_err = nullptr;
+        return MXG_ERR_MALLOC;
+    }
     if (!d_ld_x) {
         int rc = alloc(&d_ld_x, 3 * (size_t)nparts);
         rc |= alloc(&d_ld_v, 3 * (size_t)nparts);
@@ -1531,10 +1537,9 @@ int mxg_engine::load_state(const double *x, const float *v, int n) {
     ld.n = n;
     const EngineView ev = view(cur);
     launch_load_place(ev, ld, d_ld_count, stream);
-    int err = 0;
-    CUDA_TRY(cudaMemcpyAsync(&err, d_ld_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CUDA_TRY(cudaMemcpyAsync(h_ld_err, d_ld_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
     CUDA_TRY(cudaStreamSynchronize(stream));  // also: the caller's host arrays are free again
-    if (err) return MXG_ERR_SPACE;
+    if (*h_ld_err) return MXG_ERR_SPACE;
     CUDA_TRY(cudaMemcpyAsync(d_cell_count[cur], d_ld_count, sizeof(int) * (size_t)ncells, cudaMemcpyDeviceToDevice,
                              stream));
     launch_load_order(ev, ld, d_ld_count, d_cell_start[cur], d_pos[cur], d_vel[cur], d_cell_of[cur], d_slot_of_id,
@@ -2284,7 +2289,6 @@ int mxg_engine_unload(mxg_engine *e, int n, double *x, float *v, float *f, int *
 int mxg_engine_load(mxg_engine *e, int n, const double *x, const float *v) {
     if (!e || !x) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
-    CUDA_TRY(cudaStreamSynchronize(e->stream));
     return e->load_state(x, v, n);
 }
 

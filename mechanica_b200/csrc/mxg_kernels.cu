@@ -43,19 +43,21 @@ __device__ __forceinline__ void cell_sort_bounds(const float4 *__restrict__ pos,
     if (n <= 32) {  // one particle per lane
         const bool live = lane < n;
         const float4 q = live ? pos[start + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
         for (int sid = 0; sid < 13; ++sid) {
-            const int key = sort_key(q.x, q.y, q.z, axes->n[sid], bias, dscale);
+            const int key = sort_key_sid(sid, q.x, q.y, q.z, bias, dscale);
             const int kmin = __reduce_min_sync(kFull, live ? key : 0x7fffffff);
             const int kmax = __reduce_max_sync(kFull, live ? key : -1);
             if (lane == 0) out[sid] = make_int2(kmin, kmax);
         }
         return;
     }
+#pragma unroll
     for (int sid = 0; sid < 13; ++sid) {
         int kmin = 0x7fffffff, kmax = -1;
         for (int k = lane; k < n; k += 32) {
             const float4 q = pos[start + k];
-            const int key = sort_key(q.x, q.y, q.z, axes->n[sid], bias, dscale);
+            const int key = sort_key_sid(sid, q.x, q.y, q.z, bias, dscale);
             kmin = min(kmin, key);
             kmax = max(kmax, key);
         }
@@ -302,6 +304,14 @@ static_assert(Tile0::kCap + 31 <= kQueue && Tile1::kCap + 31 <= kQueue && Tile2:
                   Tile3::kCap + 31 <= kQueue,
               "queue");
 constexpr int kEnt = 32;            // neighbour entries cached at a time
+
+/* 16-byte asynchronous copy from global to shared memory (cp.async, cached in L1) and the
+ * wait for every copy this thread has issued. */
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 template <bool kDPD, class TS>
 struct ForceSmem {
@@ -678,15 +688,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, TS::kBlocks) force_kernel
                         }
                         if (lane == 0) sm.reg_beg[nent] = M;
                         __syncwarp();
-                        // ---- stage the region's neighbour particles; lane's chunk-u neighbour
-                        // (staged index u * 32 + lane) is also kept in registers for pass 1
+                        // ---- stage the region's neighbour particles: positions and velocities go
+                        // straight from global to shared memory (cp.async, every load of the region in
+                        // flight at once, none through registers); then lane's chunk-u neighbour
+                        // (staged index u * 32 + lane) is also kept in registers for pass 1:
                         // neighbour position plus the entry's shift (one rounding away from the
                         // reference's (x_i - s) - x_j): pass 1 is a superset filter with a widened
                         // cutoff; pass 2 applies the exact test on the exact displacement
                         float rbx[kChunks], rby[kChunks], rbz[kChunks];
                         float rc2[kChunks];   // widened cutoff squared; -1 for an empty position
                         int rself[kChunks];   // index of a SELF neighbour within the cell, else -1
-                        int rtj[kChunks];     // neighbour type
+                        int rtj[kChunks];     // neighbour type (the entry's sort direction until staged)
 #pragma unroll
                         for (int u = 0; u < kChunks; ++u) {
                             const int idx = u * 32 + lane;
@@ -704,25 +716,35 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, TS::kBlocks) force_kernel
                                 const float4 es = sm.ent_sh[ke];
                                 const int epk = __float_as_int(es.w);
                                 const int role = epk & 3;
-                                const float4 q = v.pos[slot];
-                                if (prune)
-                                    sm.nb_key[idx] =
-                                        sort_key(q.x, q.y, q.z, v.axes->n[(epk >> 2) & 15], sbias, sdscale);
+                                cp_async16(&sm.nb_x[idx], v.pos + slot);
+                                if (kDPD) cp_async16(&sm.nb_v[idx], v.vel + slot);
                                 float4 s4 = make_float4(0.f, 0.f, 0.f, __int_as_float(role | (ke << 2) | (jl << 8)));
                                 if (role == kRoleFirst) {
                                     s4.x = es.x;
                                     s4.y = es.y;
                                     s4.z = es.z;
                                 }
-                                sm.nb_x[idx] = q;
                                 sm.nb_s[idx] = s4;
                                 sm.nb_f[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
-                                if (kDPD) sm.nb_v[idx] = v.vel[slot];
-                                rbx[u] = __fadd_rn(q.x, s4.x);
-                                rby[u] = __fadd_rn(q.y, s4.y);
-                                rbz[u] = __fadd_rn(q.z, s4.z);
+                                rbx[u] = s4.x;
+                                rby[u] = s4.y;
+                                rbz[u] = s4.z;
                                 rc2[u] = role == kRoleSelf ? cut2w_self : cut2w_pair;
                                 rself[u] = role == kRoleSelf ? jl : -1;
+                                rtj[u] = (epk >> 2) & 15;
+                            }
+                        }
+                        cp_async_wait_all();
+                        __syncwarp();
+#pragma unroll
+                        for (int u = 0; u < kChunks; ++u) {
+                            const int idx = u * 32 + lane;
+                            if (idx < M) {
+                                const float4 q = sm.nb_x[idx];
+                                if (prune) sm.nb_key[idx] = sort_key(q.x, q.y, q.z, v.axes->n[rtj[u]], sbias, sdscale);
+                                rbx[u] = __fadd_rn(q.x, rbx[u]);
+                                rby[u] = __fadd_rn(q.y, rby[u]);
+                                rbz[u] = __fadd_rn(q.z, rbz[u]);
                                 rtj[u] = __float_as_int(q.w);
                             }
                         }
