@@ -646,7 +646,13 @@ def main():
     ve = ctypes.c_void_p(hvel.data_ptr())
     ee = ctypes.cast(ctypes.c_void_p(hen.data_ptr()), ctypes.POINTER(ctypes.c_double))
     check(L.mxg_engine_copy_state(e, pe, ve, 0), "copy_state")
-    Ke = max(1, min(K, 500))
+    with torch.cuda.stream(stream):  # warm-up of this path (untimed)
+        for _ in range(3):
+            L.mxg_engine_copy_state(e, pe, ve, 1)
+            L.mxg_engine_step(e, 1)
+            L.mxg_engine_copy_state(e, pe, ve, 0)
+            L.mxg_engine_energy_async(e, ee)
+    Ke = max(100, min(K, 500))
     s2 = [torch.cuda.Event(enable_timing=True) for _ in range(Ke)]
     e2 = [torch.cuda.Event(enable_timing=True) for _ in range(Ke)]
     barrier()
@@ -671,7 +677,12 @@ def main():
     xp = ctypes.cast(ctypes.c_void_p(hx.data_ptr()), ctypes.POINTER(ctypes.c_double))
     vp = ctypes.cast(ctypes.c_void_p(hv.data_ptr()), ctypes.POINTER(ctypes.c_float))
     check(L.mxg_engine_unload(e, n, xp, vp, None, None, None), "unload")
-    Kl = max(1, min(K, 200))
+    # warm-up of this path (untimed): the first load allocates the engine's staging buffers
+    for _ in range(3):
+        check(L.mxg_engine_load(e, n, xp, vp), "load")
+        check(L.mxg_engine_step(e, 1), "step")
+        check(L.mxg_engine_unload(e, n, xp, vp, None, None, None), "unload")
+    Kl = max(100, min(K, 200))  # at least 100 round trips: one host hiccup must not set the figure
     barrier()
     t_l = time.perf_counter()
     for k in range(Kl):
