@@ -2243,39 +2243,38 @@ __global__ void place_kernel(EngineView v, LoadView ld, int *count) {
     atomicAdd(&count[c], 1);
 }
 
-/* Exclusive scan of the new occupancy into start[0..ncells] (one block). */
+/* Exclusive scan of the new occupancy into start[0..ncells] (one block, one pass): thread t
+ * sums its own run of consecutive cells, the block scans the 1024 run totals (warp shuffles,
+ * then the warp totals), and each thread writes its run's prefixes. */
 __global__ void __launch_bounds__(1024) load_scan_kernel(const int *__restrict__ count, int ncells, int *start) {
     __shared__ int warp_sums[32];
-    __shared__ int carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int base = 0; base < ncells; base += blockDim.x) {
-        const int i = base + threadIdx.x;
-        const int x = i < ncells ? count[i] : 0;
-        int incl = x;
-        for (int d = 1; d < 32; d <<= 1) {
-            const int t = __shfl_up_sync(kFull, incl, d);
-            if (lane >= d) incl += t;
-        }
-        if (lane == 31) warp_sums[wid] = incl;
-        __syncthreads();
-        if (wid == 0) {
-            int w = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
-            for (int d = 1; d < 32; d <<= 1) {
-                const int t = __shfl_up_sync(kFull, w, d);
-                if (lane >= d) w += t;
-            }
-            warp_sums[lane] = w;
-        }
-        __syncthreads();
-        const int excl = carry + (wid ? warp_sums[wid - 1] : 0) + incl - x;
-        if (i < ncells) start[i] = excl;
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) carry = excl + x;
-        __syncthreads();
+    const int per = (ncells + blockDim.x - 1) / blockDim.x;
+    const int b0 = min(ncells, (int)threadIdx.x * per), b1 = min(ncells, b0 + per);
+    int run = 0;
+    for (int i = b0; i < b1; ++i) run += count[i];
+    int incl = run;
+    for (int d = 1; d < 32; d <<= 1) {
+        const int t = __shfl_up_sync(kFull, incl, d);
+        if (lane >= d) incl += t;
     }
-    if (threadIdx.x == 0) start[ncells] = carry;
+    if (lane == 31) warp_sums[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int w = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int t = __shfl_up_sync(kFull, w, d);
+            if (lane >= d) w += t;
+        }
+        warp_sums[lane] = w;
+    }
+    __syncthreads();
+    int excl = (wid ? warp_sums[wid - 1] : 0) + incl - run;
+    for (int i = b0; i < b1; ++i) {
+        start[i] = excl;
+        excl += count[i];
+    }
+    if (threadIdx.x == blockDim.x - 1) start[ncells] = warp_sums[(blockDim.x >> 5) - 1];
 }
 
 /* Each particle takes a place in its cell's range (in any order; ordered next). */
