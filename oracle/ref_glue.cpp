@@ -66,7 +66,7 @@ HRESULT CMulticastTimeEvent_Invoke(CMulticastTimeEvent *, double) { return S_OK;
 PyObject *MxPotential_Bind(MxPotential *, PyObject *, PyObject *) { Py_RETURN_NONE; }
 int MxParticle_Check(PyObject *) { return 0; }
 MxParticleType *MxParticleType_Get(PyObject *) { return nullptr; }
-/* MxRandomVector (src/mdcore/src/MxParticle.cpp:1782-1793, a file this build
+/* MxRandomVector (src/mdcore/src/MxParticle.cpp:1782-1793, a file the oracle Makefile
  * does not compile): a normal magnitude N(mean, std) in a uniformly random
  * direction, restated with the same construction on a default-seeded mt19937
  * as carbon's global generator (the random-force tests compare
