@@ -589,6 +589,20 @@ constexpr double kRdfFixed = 4294967296.0;  // histogram fixed point: 2^32 per u
  * c_b = (b + 1/2) dr, minimum image in the periodic box, terms with
  * |r - c_b| > 4 sigma left out. Fixed-point sums make the result independent
  * of the order of the additions. One thread per particle i. */
+/* An FP32 minimum-image distance test that rejects the pairs far beyond the histogram's reach
+ * before the exact FP64 distance: its error (a few units in the last place of the box length)
+ * is far below kRdfMargin, so every pair the FP64 test keeps passes it, and the same pairs
+ * contribute, in the same order, as without it. */
+constexpr float kRdfMargin = 1e-2f;
+__device__ __forceinline__ bool rdf_may_reach(const float4 &a, const float4 &b, const float *L, const float *iL,
+                                              float r2max) {
+    float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    dx -= L[0] * rintf(dx * iL[0]);
+    dy -= L[1] * rintf(dy * iL[1]);
+    dz -= L[2] * rintf(dz * iL[2]);
+    return dx * dx + dy * dy + dz * dz < r2max;
+}
+
 __global__ void rdf_hist_kernel(const float4 *__restrict__ x, int n, double3 box, int ta, int tb, int nbins,
                                 double dr, double sigma, unsigned long long *hist) {
     __shared__ float4 tile[kRdfTile];
@@ -602,6 +616,9 @@ __global__ void rdf_hist_kernel(const float4 *__restrict__ x, int n, double3 box
         active = __float_as_int(xi.w) == ta;
     }
     const double rmax = nbins * dr + 4 * sigma;
+    const float Lf[3] = {(float)box.x, (float)box.y, (float)box.z};
+    const float iLf[3] = {1.0f / Lf[0], 1.0f / Lf[1], 1.0f / Lf[2]};
+    const float r2f = (float)((rmax + kRdfMargin) * (rmax + kRdfMargin));
     __syncthreads();
     for (int t0 = 0; t0 < n; t0 += kRdfTile) {
         const int j = t0 + threadIdx.x;
@@ -612,6 +629,7 @@ __global__ void rdf_hist_kernel(const float4 *__restrict__ x, int n, double3 box
             for (int k = 0; k < m; ++k) {
                 const float4 xj = tile[k];
                 if (__float_as_int(xj.w) != tb || t0 + k == i) continue;
+                if (!rdf_may_reach(xi, xj, Lf, iLf, r2f)) continue;
                 double d[3] = {(double)xi.x - xj.x, (double)xi.y - xj.y, (double)xi.z - xj.z};
                 const double L[3] = {box.x, box.y, box.z};
                 for (int q = 0; q < 3; ++q) d[q] -= L[q] * rint(d[q] / L[q]);
@@ -646,6 +664,9 @@ __global__ void rdf_grad_kernel(const float4 *__restrict__ x, int n, double3 box
         partner = ti == ta ? tb : (ti == tb ? ta : -2);
     }
     const double rmax = nbins * dr + 4 * sigma;
+    const float Lf[3] = {(float)box.x, (float)box.y, (float)box.z};
+    const float iLf[3] = {1.0f / Lf[0], 1.0f / Lf[1], 1.0f / Lf[2]};
+    const float r2f = (float)((rmax + kRdfMargin) * (rmax + kRdfMargin));
     double g[3] = {0.0, 0.0, 0.0};
     for (int t0 = 0; t0 < n; t0 += kRdfTile) {
         const int j = t0 + threadIdx.x;
@@ -656,6 +677,7 @@ __global__ void rdf_grad_kernel(const float4 *__restrict__ x, int n, double3 box
             for (int k = 0; k < m; ++k) {
                 const float4 xj = tile[k];
                 if (__float_as_int(xj.w) != partner || t0 + k == i) continue;
+                if (!rdf_may_reach(xi, xj, Lf, iLf, r2f)) continue;
                 double d[3] = {(double)xi.x - xj.x, (double)xi.y - xj.y, (double)xi.z - xj.z};
                 const double L[3] = {box.x, box.y, box.z};
                 for (int q = 0; q < 3; ++q) d[q] -= L[q] * rint(d[q] / L[q]);
