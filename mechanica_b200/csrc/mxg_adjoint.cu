@@ -546,13 +546,24 @@ __global__ void adj_finish_kernel(EngineView v, AdjointView a) {
 
 /* grad[k] += sum of the pair kernel's warp partials, in warp order, then of the
  * bond kernel's block partials, in block order. */
-__global__ void adj_grad_kernel(AdjointView a, int nwarps, int nbond_blocks, double *grad) {
-    const int k = threadIdx.x;
-    if (k >= a.nslots) return;
+/* grad[k] += the step's parameter-gradient partials of slot k: one block per slot, each thread
+ * summing a fixed stride of the warp and bond-block partials, then a fixed tree over the
+ * threads (the same order on every run). */
+constexpr int kGradThreads = 256;
+__global__ void __launch_bounds__(kGradThreads) adj_grad_kernel(AdjointView a, int nwarps, int nbond_blocks,
+                                                              double *grad) {
+    __shared__ double part[kGradThreads];
+    const int k = blockIdx.x;
     double t = 0.0;
-    for (int q = 0; q < nwarps; ++q) t += a.partials[(size_t)q * kMaxGradSlots + k];
-    for (int q = 0; q < nbond_blocks; ++q) t += a.bond_partials[(size_t)q * kMaxGradSlots + k];
-    grad[k] += t;
+    for (int q = threadIdx.x; q < nwarps; q += blockDim.x) t += a.partials[(size_t)q * kMaxGradSlots + k];
+    for (int q = threadIdx.x; q < nbond_blocks; q += blockDim.x) t += a.bond_partials[(size_t)q * kMaxGradSlots + k];
+    part[threadIdx.x] = t;
+    __syncthreads();
+    for (int h = blockDim.x >> 1; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) part[threadIdx.x] += part[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) grad[k] += part[0];
 }
 
 /* Absolute positions (x, y, z, type bits) and velocities (v, id bits) by id;
@@ -585,10 +596,6 @@ constexpr int kRdfTile = 256;
 constexpr int kRdfMaxBins = 256;
 constexpr double kRdfFixed = 4294967296.0;  // histogram fixed point: 2^32 per unit
 
-/* hist[b] += sum over (i of type ta, j of type tb, i != j) of K(r_ij - c_b),
- * c_b = (b + 1/2) dr, minimum image in the periodic box, terms with
- * |r - c_b| > 4 sigma left out. Fixed-point sums make the result independent
- * of the order of the additions. One thread per particle i. */
 /* An FP32 minimum-image distance test that rejects the pairs far beyond the histogram's reach
  * before the exact FP64 distance: its error (a few units in the last place of the box length)
  * is far below kRdfMargin, so every pair the FP64 test keeps passes it, and the same pairs
@@ -603,6 +610,10 @@ __device__ __forceinline__ bool rdf_may_reach(const float4 &a, const float4 &b, 
     return dx * dx + dy * dy + dz * dz < r2max;
 }
 
+/* hist[b] += sum over (i of type ta, j of type tb, i != j) of K(r_ij - c_b),
+ * c_b = (b + 1/2) dr, minimum image in the periodic box, terms with
+ * |r - c_b| > 4 sigma left out. Fixed-point sums make the result independent
+ * of the order of the additions. One thread per particle i. */
 __global__ void rdf_hist_kernel(const float4 *__restrict__ x, int n, double3 box, int ta, int tb, int nbins,
                                 double dr, double sigma, unsigned long long *hist) {
     __shared__ float4 tile[kRdfTile];
@@ -736,7 +747,7 @@ void launch_vjp_step(const EngineView &v, const AdjointView &a, const BondedView
     const int bblocks = bv ? adjoint_bond_blocks(num_sms) : 0;
     if (bv) vjp_bond_kernel<<<bblocks, kBondVjpThreads, 0, st>>>(v, *bv, a);
     adj_finish_kernel<<<(v.nparts + tb - 1) / tb, tb, 0, st>>>(v, a);
-    adj_grad_kernel<<<1, 64, 0, st>>>(a, grid * kWarpsA, bblocks, grad);
+    if (a.nslots > 0) adj_grad_kernel<<<a.nslots, kGradThreads, 0, st>>>(a, grid * kWarpsA, bblocks, grad);
 }
 
 }  // namespace mxg
