@@ -289,6 +289,9 @@ __device__ __noinline__ void large_forces(const EngineView &v, int s, const floa
 template <int kOwnT, int kCapT, int kBlocksT>
 struct Tile {
     static constexpr int kOwn = kOwnT, kCap = kCapT, kChunks = kCapT / 32, kBlocks = kBlocksT;
+    // the ring queue of pairs (a power of two holding kCap + 31: one own particle queues at
+    // most kCap pairs on top of fewer than 32 waiting ones)
+    static constexpr int kQ = kCapT + 31 <= 128 ? 128 : 256;
     // a queued pair is (own index << 8 | staged index) in 16 bits; one own particle queues at most
     // kCap pairs on top of fewer than 32 waiting ones
     static_assert(kOwnT >= 1 && kOwnT <= 255 && kCapT % 32 == 0 && kCapT >= 32 && kCapT <= 256, "tile shape");
@@ -299,10 +302,6 @@ using Tile2 = Tile<64, 96, 5>;
 using Tile3 = Tile<32, 128, 4>;
 constexpr int kForceVariants = 4;
 
-constexpr int kQueue = 256;         // ring buffer of queued pairs (holds kCap + 31 for every tile)
-static_assert(Tile0::kCap + 31 <= kQueue && Tile1::kCap + 31 <= kQueue && Tile2::kCap + 31 <= kQueue &&
-                  Tile3::kCap + 31 <= kQueue,
-              "queue");
 constexpr int kEnt = 32;            // neighbour entries cached at a time
 
 /* 16-byte asynchronous copy from global to shared memory (cp.async, cached in L1) and the
@@ -318,7 +317,8 @@ struct ForceSmem {
     static constexpr int kOwn = TS::kOwn, kCap = TS::kCap;
     float4 nb_x[kCap];              // neighbour position; w = type
     float4 nb_s[kCap];              // shift of FIRST entries, else 0; w = role | entry << 2 | index << 8
-    float4 nb_f[kCap];              // neighbour-side force sums of the region
+    float4 nb_f[kCap];              // neighbour-side force sums of the region: runs of even index
+    float4 nb_f1[kCap];             // and of odd index (summed at the region's end)
     float4 nb_v[kDPD ? kCap : 1];   // velocity; w = id
     float4 own_x[kOwn];
     float4 own_v[kDPD ? kOwn : 1];
@@ -331,7 +331,7 @@ struct ForceSmem {
     int reg_jb[kEnt];               // region: index within its cell of the entry's first staged particle
     unsigned long long own_mask[kOwn];  // bit t: a potential exists for (own type, t)
     int nb_key[kCap];               // sort key of the neighbour (per-pair pruning)
-    unsigned short queue[kQueue];   // own index << 8 | staged index, in candidate order
+    unsigned short queue[TS::kQ];   // own index << 8 | staged index, in candidate order
 };
 
 /*
@@ -380,7 +380,7 @@ __device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD, 
     int il = -1, jj = 0;
     bool nbside = false;
     if (lane < nb) {
-        const int cd = sm.queue[(qhead + lane) & (kQueue - 1)];
+        const int cd = sm.queue[(qhead + lane) & (TS::kQ - 1)];
         il = cd >> 8;
         jj = cd & 0xff;
         const int i = i0 + il;
@@ -488,18 +488,19 @@ __device__ __forceinline__ void eval_batch(const EngineView &v, ForceSmem<kDPD, 
     // segments: runs of equal own index (inactive lanes form the last one)
     const int il_prev = __shfl_up_sync(kFull, il, 1);
     const unsigned heads = __ballot_sync(kFull, lane == 0 || il != il_prev);
-    // neighbour side, one segment after another (neighbours are distinct inside one)
-    unsigned segs = heads & (nb == 32 ? kFull : ((1u << nb) - 1u));
-    while (segs) {
-        const int h = __ffs(segs) - 1;
-        segs &= segs - 1;
-        const int next = segs ? __ffs(segs) - 1 : nb;
-        if (nbside && lane >= h && lane < next) {
-            float4 f = sm.nb_f[jj];
+    // neighbour side: the runs in pairs, runs of even index into nb_f and of odd index into
+    // nb_f1 (the two runs of a pair cannot add to the same sum, and inside a run the
+    // neighbours are distinct), pair after pair: every sum has a fixed order
+    const int nseg = __popc(heads & (nb == 32 ? kFull : ((1u << nb) - 1u)));
+    const int sidx = __popc(heads & (0xffffffffu >> (31 - lane))) - 1;  // this lane's run
+    for (int pr = 0; 2 * pr < nseg; ++pr) {
+        if (nbside && lane < nb && (sidx >> 1) == pr) {
+            float4 *acc = (sidx & 1) ? sm.nb_f1 : sm.nb_f;
+            float4 f = acc[jj];
             f.x = __fsub_rn(f.x, cx);
             f.y = __fsub_rn(f.y, cy);
             f.z = __fsub_rn(f.z, cz);
-            sm.nb_f[jj] = f;
+            acc[jj] = f;
         }
         __syncwarp();
     }
@@ -545,7 +546,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, TS::kBlocks) force_kernel
     unsigned long long npair = 0;  // interacting pairs counted once (statistics launch only)
     double vir[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // pair virial (virial launch only)
     extern __shared__ float4 force_smem[];
-    __shared__ float4 tinfo[kMaxTypes];  // per type: constant force (zero if none), radius
+    // per type: constant force (zero if none), radius; after the warps' areas (v.ntypes entries)
+    float4 *tinfo = force_smem + sizeof(ForceSmem<kDPD, TS>) * kWarpsPerBlock / sizeof(float4);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     ForceSmem<kDPD, TS> &sm = reinterpret_cast<ForceSmem<kDPD, TS> *>(force_smem)[w];
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -726,6 +728,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, TS::kBlocks) force_kernel
                                 }
                                 sm.nb_s[idx] = s4;
                                 sm.nb_f[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+                                sm.nb_f1[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
                                 rbx[u] = s4.x;
                                 rby[u] = s4.y;
                                 rbz[u] = s4.z;
@@ -793,7 +796,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, TS::kBlocks) force_kernel
 #pragma unroll
                                 for (int u = 0; u < kChunks; ++u) {
                                     if (hv[u])
-                                        sm.queue[(qtail + __popc(hb[u] & lt_mask)) & (kQueue - 1)] =
+                                        sm.queue[(qtail + __popc(hb[u] & lt_mask)) & (TS::kQ - 1)] =
                                             (unsigned short)((il << 8) | (u * 32 + lane));
                                     qtail += __popc(hb[u]);
                                 }
@@ -811,8 +814,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, TS::kBlocks) force_kernel
                         // cell's own particles (pairs evaluated once) into their own sums
                         for (int idx = lane; idx < M && kMode != 2; idx += 32) {
                             const int meta = __float_as_int(sm.nb_s[idx].w);
+                            const float4 g0 = sm.nb_f[idx], g1 = sm.nb_f1[idx];
+                            const float4 g = make_float4(g0.x + g1.x, g0.y + g1.y, g0.z + g1.z, 0.f);
                             if (self_once && (meta & 3) == kRoleSelf) {
-                                const float4 g = sm.nb_f[idx];
                                 float4 &o = sm.own_f[meta >> 8];  // one own pass: own index = index in the cell
                                 o.x += g.x;
                                 o.y += g.y;
@@ -822,7 +826,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, TS::kBlocks) force_kernel
                             if ((meta & 3) != kRoleFirst) continue;
                             const int ke = (meta >> 2) & 31;
                             float4 *dst = v.planes + (size_t)sm.ent_rev[ke] * v.nparts + sm.ent_slot[ke] + (meta >> 8);
-                            float4 f = sm.nb_f[idx];
+                            float4 f = g;
                             if (i0 > 0) {  // later own chunks add to the first chunk's sums
                                 const float4 o = *dst;
                                 f = make_float4(o.x + f.x, o.y + f.y, o.z + f.z, 0.f);
@@ -2404,9 +2408,15 @@ __global__ void reduce_final_kernel(int nblocks, const double *partials, double 
 /* launchers                                                                 */
 /* ------------------------------------------------------------------------ */
 
+/* dynamic shared memory of a force launch: the warps' areas, then the per-type table */
+template <bool kDPD, class TS>
+size_t force_launch_bytes(const EngineView &v) {
+    return force_smem_bytes<kDPD, TS>() + sizeof(float4) * (size_t)v.ntypes;
+}
+
 template <bool kDPD, int kMode, bool kPure, class TS>
 void configure_one() {
-    const int bytes = (int)force_smem_bytes<kDPD, TS>();
+    const int bytes = (int)(force_smem_bytes<kDPD, TS>() + sizeof(float4) * kMaxTypes);
     cudaFuncSetAttribute(force_kernel<kDPD, kMode, kPure, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     cudaFuncSetAttribute(force_kernel<kDPD, kMode, kPure, TS>, cudaFuncAttributePreferredSharedMemoryCarveout,
                          cudaSharedmemCarveoutMaxShared);
@@ -2438,18 +2448,17 @@ void launch_sort_bounds(const EngineView &v, cudaStream_t st) {
 
 template <bool kDPD, class TS>
 void launch_force_tile(const EngineView &v, int grid, cudaStream_t st) {
-    const size_t bytes = force_smem_bytes<kDPD, TS>();
     if (kDPD && v.dpd_pure)
-        force_kernel<true, 0, true, TS><<<grid, kWarpsPerBlock * 32, force_smem_bytes<true, TS>(), st>>>(v);
+        force_kernel<true, 0, true, TS><<<grid, kWarpsPerBlock * 32, force_launch_bytes<true, TS>(v), st>>>(v);
     else
-        force_kernel<kDPD, 0, false, TS><<<grid, kWarpsPerBlock * 32, bytes, st>>>(v);
+        force_kernel<kDPD, 0, false, TS><<<grid, kWarpsPerBlock * 32, force_launch_bytes<kDPD, TS>(v), st>>>(v);
 }
 
 /* The statistics and virial launches use the default tile; the force pass the engine's
  * variant (0 to kForceVariants - 1). */
 template <bool kDPD>
 void launch_force_mode(const EngineView &v, int grid, int variant, cudaStream_t st) {
-    const size_t bytes = force_smem_bytes<kDPD, Tile0>();
+    const size_t bytes = force_launch_bytes<kDPD, Tile0>(v);
     if (v.pair_stats)
         force_kernel<kDPD, 1, false, Tile0><<<grid, kWarpsPerBlock * 32, bytes, st>>>(v);
     else if (v.virial_partials)
