@@ -410,6 +410,16 @@ int mxg_engine_adjoint_params(mxg_engine *e, int n, const int *pot, const int *p
  * wall potentials, large particles and Berendsen/random/friction forces are refused (MXG_ERR_ARG).
  * Wall reflections of the integrator are not differentiated. */
 int mxg_engine_vjp_step(mxg_engine *e, void *lam_x, void *lam_v, double *grad);
+/* mxg_engine_vjp_step with the forces of the current state given: forces is a device float4 array of
+ * nr_parts entries in the current slot order, as mxg_engine_save_forces left it after the step taken
+ * from this state. Without bonds the step's force pass is then not repeated (the forces are copied
+ * in); with bonds (whose pass also decides the break flags) or forces NULL it is. The adjoint
+ * workflow's recompute saves them anyway. */
+int mxg_engine_vjp_step_forces(mxg_engine *e, void *lam_x, void *lam_v, double *grad, const void *forces);
+/* Copies the forces of the last force pass (total forces, slot order of the state that pass ran on:
+ * after mxg_engine_step, the state the step started from) into dev_buf (nr_parts float4), ordered on
+ * the engine stream. */
+int mxg_engine_save_forces(mxg_engine *e, void *dev_buf);
 /* Device float4 arrays by particle id: absolute positions (x, y, z, type bits) and velocities
  * (v, id bits); either pointer may be NULL. Stream-ordered. */
 int mxg_engine_positions(mxg_engine *e, void *x4, void *v4);

@@ -138,6 +138,8 @@ _SIGS = {
     "mxg_engine_snapshot": ([_vp, _vp, ctypes.c_int], ctypes.c_int),
     "mxg_engine_adjoint_params": ([_vp, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p], ctypes.c_int),
     "mxg_engine_vjp_step": ([_vp, _vp, _vp, _vp], ctypes.c_int),
+    "mxg_engine_vjp_step_forces": ([_vp, _vp, _vp, _vp, _vp], ctypes.c_int),
+    "mxg_engine_save_forces": ([_vp, _vp], ctypes.c_int),
     "mxg_engine_positions": ([_vp, _vp, _vp], ctypes.c_int),
     "mxg_engine_set_step_counter": ([_vp, ctypes.c_ulonglong], ctypes.c_int),
     "mxg_rdf": ([_vp, ctypes.c_int, _c_double_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,

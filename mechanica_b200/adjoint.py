@@ -173,15 +173,18 @@ class Trajectory(torch.autograd.Function):
             s1 = min(sim.nsteps, s0 + sim.K)
             sim.restore(ctx.snaps[seg])
             states = []
-            for s in range(s0, s1):  # recompute the segment, keeping every state
+            for s in range(s0, s1):  # recompute the segment, keeping every state and its forces
                 buf = sim.snapshot_buffer()
                 sim.save(buf)
-                states.append(buf)
                 sim.step(1)
-            for buf in reversed(states):
+                fbuf = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+                check(lib().mxg_engine_save_forces(e, _dptr(fbuf)), "save_forces")
+                states.append((buf, fbuf))
+            for buf, fbuf in reversed(states):
                 sim.restore(buf)
-                check(lib().mxg_engine_vjp_step(e, _dptr(lam_x), _dptr(lam_v), ctypes.cast(grad.data_ptr(),
-                                                ctypes.POINTER(ctypes.c_double))), "vjp_step")
+                check(lib().mxg_engine_vjp_step_forces(e, _dptr(lam_x), _dptr(lam_v),
+                                                       ctypes.cast(grad.data_ptr(), ctypes.POINTER(ctypes.c_double)),
+                                                       _dptr(fbuf)), "vjp_step")
         torch.cuda.synchronize()
         check(lib().mxg_engine_status(e), "adjoint")
         tdt, xdt, vdt = ctx.dtypes

@@ -2489,6 +2489,19 @@ int mxg_engine_adjoint_params(mxg_engine *e, int n, const int *pot, const int *p
 }
 
 int mxg_engine_vjp_step(mxg_engine *e, void *lam_x, void *lam_v, double *grad) {
+    return mxg_engine_vjp_step_forces(e, lam_x, lam_v, grad, nullptr);
+}
+
+int mxg_engine_save_forces(mxg_engine *e, void *dev_buf) {
+    if (!e || !dev_buf) return MXG_ERR_NULL;
+    if (!e->started) return MXG_ERR_STATE;
+    if (e->nparts == 0) return MXG_OK;
+    CUDA_TRY(cudaMemcpyAsync(dev_buf, e->d_force, sizeof(float4) * (size_t)e->nparts, cudaMemcpyDeviceToDevice,
+                             e->stream));
+    return MXG_OK;
+}
+
+int mxg_engine_vjp_step_forces(mxg_engine *e, void *lam_x, void *lam_v, double *grad, const void *forces) {
     if (!e || !lam_x || !lam_v || !grad) return MXG_ERR_NULL;
     if (!e->started) return MXG_ERR_STATE;
     // angles, dihedrals, exclusions, single-body, wall and large-particle forces are not
@@ -2505,7 +2518,11 @@ int mxg_engine_vjp_step(mxg_engine *e, void *lam_x, void *lam_v, double *grad) {
     // forces of the step's state; with bonds, the bond pass of the state completes them and
     // leaves the flags of the bonds that acted in the step (as the forward step's pass did)
     const bool bonded = !e->bonds.empty();
-    launch_force(v, e->has_dpd, e->force_grid, !bonded, e->stream);
+    if (forces && !bonded)
+        CUDA_TRY(cudaMemcpyAsync(e->d_force, forces, sizeof(float4) * (size_t)e->nparts, cudaMemcpyDeviceToDevice,
+                                 e->stream));
+    else
+        launch_force(v, e->has_dpd, e->force_grid, !bonded, e->stream);
     BondedView bv;
     if (bonded) {
         bv = e->bonded_view();
