@@ -29,6 +29,8 @@
  * forces).
  */
 #include "mxg_adjoint.h"
+
+#include <algorithm>
 #include "mxg_device.cuh"
 
 namespace mxg {
@@ -41,7 +43,8 @@ constexpr int kCapA = 64;              // neighbour particles staged at a time
 constexpr int kChunksA = kCapA / 32;
 constexpr int kQueueA = 128;           // ring buffer of queued pairs (holds kCapA + 31)
 constexpr int kEntA = 32;              // neighbour entries cached at a time
-constexpr int kWarpsA = 4;             // warps (cells) per block
+constexpr int kWarpsA = 4;             // warps (work items) per block
+constexpr int kVjpParts = 4;           // work items per cell (contiguous groups of its entries)
 
 struct AdjSmem {
     float4 nb_x[kCapA];   // neighbour position (SECOND entries pre-shifted); w = type
@@ -245,15 +248,23 @@ __global__ void __launch_bounds__(kWarpsA * 32, 4) vjp_pair_kernel(EngineView v,
     for (int q = 0; q < kMaxGradSlots; ++q) gl[q] = 0.0;
     const unsigned lt_mask = (1u << lane) - 1u;
     const int ntypes = v.ntypes;
-    for (int c = blockIdx.x * kWarpsA + w; c < v.ncells; c += gridDim.x * kWarpsA) {
+    const int nwarps = gridDim.x * kWarpsA;
+    // work items from a counter (a cell's parts are items of their own, so no warp holds a
+    // crowded cell alone); every item writes only its own outputs and parameter partials
+    auto fetch = [&]() -> int {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(a.item_ctr, 1);
+        return __shfl_sync(kFull, t, 0);
+    };
+    for (int it = fetch(); it < a.nitems; it = fetch()) {
+        const int4 item = a.items[it];
+        const int c = item.x, nb0 = item.y, nb1 = item.z, part = item.w;
         const int n = v.cell_count[c];
-        if (n == 0) continue;
         const int start = v.cell_start[c];
         const DevSpace &S = v.spaces[v.cell_rep[c]];
         const int pot_base = S.pot_offset;
         const float cut2_pair = S.cut2_pair, cut2_self = S.cut2_self;
         const unsigned rng_mode = S.rng_mode;
-        const int nb0 = v.nb_off[c], nb1 = v.nb_off[c + 1];
         for (int i0 = 0; i0 < n; i0 += kOwnA) {
             const int ni = min(kOwnA, n - i0);
             __syncwarp();
@@ -438,20 +449,35 @@ __global__ void __launch_bounds__(kWarpsA * 32, 4) vjp_pair_kernel(EngineView v,
             if (lane < ni) {
                 const int sl = start + i0 + lane;
                 const float4 gx = sm.own_gx[lane], gv = sm.own_gv[lane];
-                const float4 bx = a.gx[sl], bv = a.gv[sl];
-                a.gx[sl] = make_float4(bx.x + gx.x, bx.y + gx.y, bx.z + gx.z, 0.f);
-                a.gv[sl] = make_float4(bv.x + gv.x, bv.y + gv.y, bv.z + gv.z, 0.f);
+                if (part == 0) {
+                    const float4 bx = a.gx[sl], bv = a.gv[sl];
+                    a.gx[sl] = make_float4(bx.x + gx.x, bx.y + gx.y, bx.z + gx.z, 0.f);
+                    a.gv[sl] = make_float4(bv.x + gv.x, bv.y + gv.y, bv.z + gv.z, 0.f);
+                } else {
+                    a.pgx[(size_t)(part - 1) * v.nparts + sl] = gx;
+                    a.pgv[(size_t)(part - 1) * v.nparts + sl] = gv;
+                }
             }
         }
+        // this item's parameter sums, lanes in order; then the lanes' sums start again
+        __syncwarp();
+        if (lane < kMaxGradSlots && lane < a.nslots) {
+            double *base = reinterpret_cast<double *>(reinterpret_cast<AdjSmem *>(adj_smem) + kWarpsA) +
+                           (size_t)(w * 32) * kMaxGradSlots;
+            double t = 0.0;
+            for (int l = 0; l < 32; ++l) t += base[(size_t)l * kMaxGradSlots + lane];
+            a.partials[(size_t)it * kMaxGradSlots + lane] = t;
+        }
+        __syncwarp();
+        for (int q = 0; q < kMaxGradSlots; ++q) gl[q] = 0.0;
     }
-    // this warp's parameter sums, lanes in order
-    __syncwarp();
-    if (lane < kMaxGradSlots && lane < a.nslots) {
-        double* base = reinterpret_cast<double *>(reinterpret_cast<AdjSmem *>(adj_smem) + kWarpsA) +
-                       (size_t)(w * 32) * kMaxGradSlots;
-        double t = 0.0;
-        for (int l = 0; l < 32; ++l) t += base[(size_t)l * kMaxGradSlots + lane];
-        a.partials[(size_t)(blockIdx.x * kWarpsA + w) * kMaxGradSlots + lane] = t;
+    if (lane == 0) {
+        // every warp has drawn its last ticket once the done count reaches the grid's warps:
+        // the last one re-arms both counters for the next launch on the stream
+        if (atomicAdd(a.item_ctr + 1, 1) == nwarps - 1) {
+            atomicExch(a.item_ctr, 0);
+            atomicExch(a.item_ctr + 1, 0);
+        }
     }
 }
 
@@ -540,15 +566,19 @@ __global__ void adj_finish_kernel(EngineView v, AdjointView a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= v.nparts) return;
     const int id = __float_as_int(v.vel[s].w);
-    a.lam_x[id] = a.gx[s];
-    a.lam_v[id] = a.gv[s];
+    float4 gx = a.gx[s], gv = a.gv[s];
+    for (int p = 0; p + 1 < kVjpParts; ++p) {  // the later parts' sums, in part order
+        const float4 px = a.pgx[(size_t)p * v.nparts + s], pv = a.pgv[(size_t)p * v.nparts + s];
+        gx = make_float4(gx.x + px.x, gx.y + px.y, gx.z + px.z, 0.f);
+        gv = make_float4(gv.x + pv.x, gv.y + pv.y, gv.z + pv.z, 0.f);
+    }
+    a.lam_x[id] = gx;
+    a.lam_v[id] = gv;
 }
 
-/* grad[k] += sum of the pair kernel's warp partials, in warp order, then of the
- * bond kernel's block partials, in block order. */
 /* grad[k] += the step's parameter-gradient partials of slot k: one block per slot, each thread
- * summing a fixed stride of the warp and bond-block partials, then a fixed tree over the
- * threads (the same order on every run). */
+ * summing a fixed stride of the pair items' and bond blocks' partials, then a fixed tree over
+ * the threads (the same order on every run). */
 constexpr int kGradThreads = 256;
 __global__ void __launch_bounds__(kGradThreads) adj_grad_kernel(AdjointView a, int nwarps, int nbond_blocks,
                                                               double *grad) {
@@ -728,8 +758,28 @@ int launch_rdf(const float4 *x, int n, const double *box, int ta, int tb, int nb
     return 0;
 }
 
+/* One thread per word over all sections in order (a section's words are consecutive). */
+__global__ void copy_sections_kernel(CopySections c, unsigned long long total) {
+    for (unsigned long long t = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; t < total;
+         t += (unsigned long long)gridDim.x * blockDim.x) {
+        unsigned long long r = t;
+        int k = 0;
+        while (k < c.n - 1 && r >= c.words[k]) r -= c.words[k++];
+        c.dst[k][r] = c.src[k][r];
+    }
+}
+
+void launch_copy_sections(const CopySections &c, cudaStream_t st) {
+    unsigned long long total = 0;
+    for (int k = 0; k < c.n; ++k) total += c.words[k];
+    if (total == 0) return;
+    const int tb = 256;
+    const unsigned long long blocks = std::min<unsigned long long>((total + tb - 1) / tb, 148ull * 16);
+    copy_sections_kernel<<<(unsigned)blocks, tb, 0, st>>>(c, total);
+}
+
 int adjoint_grid(int num_sms) { return num_sms * 4; }
-int adjoint_partials(int num_sms) { return adjoint_grid(num_sms) * kWarpsA; }
+int vjp_parts() { return kVjpParts; }
 int adjoint_bond_blocks(int num_sms) { return num_sms * 2; }
 
 void configure_adjoint_kernels() {
@@ -747,7 +797,7 @@ void launch_vjp_step(const EngineView &v, const AdjointView &a, const BondedView
     const int bblocks = bv ? adjoint_bond_blocks(num_sms) : 0;
     if (bv) vjp_bond_kernel<<<bblocks, kBondVjpThreads, 0, st>>>(v, *bv, a);
     adj_finish_kernel<<<(v.nparts + tb - 1) / tb, tb, 0, st>>>(v, a);
-    if (a.nslots > 0) adj_grad_kernel<<<a.nslots, kGradThreads, 0, st>>>(a, grid * kWarpsA, bblocks, grad);
+    if (a.nslots > 0) adj_grad_kernel<<<a.nslots, kGradThreads, 0, st>>>(a, a.nitems, bblocks, grad);
 }
 
 }  // namespace mxg

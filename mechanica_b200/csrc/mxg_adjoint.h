@@ -21,16 +21,33 @@ struct AdjointView {
     float4 *w, *gx, *gv;         // [slot] scratch: force adjoint and the partial sums
     const DevPotGrad *pot_grad;  // per potential
     const float *dcoef;          // derivative tables' coefficient pool
-    double *partials;            // [warp][kMaxGradSlots] FP64 parameter sums of the pair terms
+    double *partials;            // [item][kMaxGradSlots] FP64 parameter sums of the pair terms
     double *bond_partials;       // [block][kMaxGradSlots] FP64 parameter sums of the bond terms
     int nslots;
+    // the pair terms' work items: (cell, first entry, end entry, part), kVjpParts per cell; part 0
+    // adds its own-side sums to gx / gv, part p > 0 writes them to plane p - 1 of pgx / pgv
+    const int4 *items;
+    int nitems;
+    int *item_ctr;               // [0] next item, [1] warps done (zero between launches)
+    float4 *pgx, *pgv;           // [part - 1][slot]
 };
 
 void launch_positions(const EngineView &v, float4 *x_out, float4 *v_out, cudaStream_t st);
 /* Smoothed pair histogram of types (ta, tb) and/or its gradient (see mxg_rdf). */
 int launch_rdf(const float4 *x, int n, const double *box, int ta, int tb, int nbins, double dr, double sigma,
                unsigned long long *hist, const double *coef, float4 *grad, cudaStream_t st);
-int adjoint_partials(int num_sms);
+/* Up to kCopyMax device-to-device copies of whole 4-byte words in one launch (the sections of a
+ * state snapshot): section k copies words[k] words from src[k] to dst[k]. */
+constexpr int kCopyMax = 12;
+struct CopySections {
+    const unsigned *src[kCopyMax];
+    unsigned *dst[kCopyMax];
+    unsigned long long words[kCopyMax];
+    int n;
+};
+void launch_copy_sections(const CopySections &c, cudaStream_t st);
+/* parts per cell of the pair terms' work items (contiguous groups of the cell's entries) */
+int vjp_parts();
 /* blocks of the bond-term kernel (each writes kMaxGradSlots partial sums) */
 int adjoint_bond_blocks(int num_sms);
 void configure_adjoint_kernels();

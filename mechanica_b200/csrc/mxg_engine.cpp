@@ -511,6 +511,11 @@ struct mxg_engine {
     size_t dcoef_cap = 0;
     float4 *d_adj_w = nullptr, *d_adj_gx = nullptr, *d_adj_gv = nullptr;
     double *d_adj_partials = nullptr;
+    int4 *d_adj_items = nullptr;            // the pair VJP's work items
+    int *d_adj_ctr = nullptr;
+    float4 *d_adj_pgx = nullptr, *d_adj_pgv = nullptr;
+    int adj_nitems = 0;
+    std::vector<int> h_nb_off;              // per cell: first neighbour entry (host copy)
     double *d_adj_bond_partials = nullptr;
     double *d_virial_partials = nullptr, *d_virial_out = nullptr;
     double *d_bvirial_partials = nullptr;  // bonded virial: per block, 9 components
@@ -913,7 +918,24 @@ struct mxg_engine {
             rc |= alloc(&d_adj_w, (size_t)nparts);
             rc |= alloc(&d_adj_gx, (size_t)nparts);
             rc |= alloc(&d_adj_gv, (size_t)nparts);
-            rc |= alloc(&d_adj_partials, (size_t)adjoint_partials(num_sms) * kMaxGradSlots);
+            // the pair VJP's work items: each cell's entries in vjp_parts() contiguous groups
+            const int P = vjp_parts();
+            std::vector<int4> items;
+            for (int c = 0; c < ncells; ++c) {
+                const int e0 = h_nb_off[c], ne = h_nb_off[c + 1] - e0;
+                for (int g = 0; g < P; ++g) items.push_back(make_int4(c, e0 + g * ne / P, e0 + (g + 1) * ne / P, g));
+            }
+            adj_nitems = (int)items.size();
+            rc |= alloc(&d_adj_items, items.size());
+            rc |= alloc(&d_adj_ctr, 2);
+            rc |= alloc(&d_adj_pgx, (size_t)std::max(1, P - 1) * nparts);
+            rc |= alloc(&d_adj_pgv, (size_t)std::max(1, P - 1) * nparts);
+            rc |= alloc(&d_adj_partials, (size_t)std::max(1, adj_nitems) * kMaxGradSlots);
+            if (rc == MXG_OK) {
+                CUDA_TRY(cudaMemsetAsync(d_adj_ctr, 0, 2 * sizeof(int), stream));
+                rc = upload(d_adj_items, items, stream);
+                if (rc == MXG_OK) CUDA_TRY(cudaStreamSynchronize(stream));
+            }
             rc |= alloc(&d_adj_bond_partials, (size_t)adjoint_bond_blocks(num_sms) * kMaxGradSlots);
             if (rc != MXG_OK) return MXG_ERR_MALLOC;
             configure_adjoint_kernels();
@@ -1104,6 +1126,7 @@ int mxg_engine::start(cudaStream_t st) {
         hplanes[c] = hsec[c] + groups - 1;
     }
     nitems = (int)hitems.size();
+    h_nb_off = nb_off;
     // few crowded cells, split into several items each: the launch's length is set by the
     // most crowded cells' items, so they are handed out first (reordered before every force
     // pass). With sparse cells (mean occupancy below 16) the items are short and the
@@ -2460,13 +2483,19 @@ int mxg_engine_snapshot(mxg_engine *e, void *dev_buf, int save) {
         {e->d_rate, L.rate, sizeof(float) * (size_t)e->nparts * e->smax},
         {e->d_persist, L.persist, e->has_sb ? sizeof(float4) * (size_t)e->nparts : 0},
     };
+    // every section in one copy launch (whole 4-byte words: every section's size is a multiple of 4)
+    CopySections cs;
+    cs.n = 0;
     for (const Sec &q : secs) {
         if (q.bytes == 0) continue;
-        if (save)
-            CUDA_TRY(cudaMemcpyAsync(b + q.off, q.dev, q.bytes, cudaMemcpyDeviceToDevice, e->stream));
-        else
-            CUDA_TRY(cudaMemcpyAsync(q.dev, b + q.off, q.bytes, cudaMemcpyDeviceToDevice, e->stream));
+        unsigned *in = static_cast<unsigned *>(q.dev), *out = reinterpret_cast<unsigned *>(b + q.off);
+        cs.src[cs.n] = save ? in : out;
+        cs.dst[cs.n] = save ? out : in;
+        cs.words[cs.n] = q.bytes / 4;
+        ++cs.n;
     }
+    launch_copy_sections(cs, e->stream);
+    CUDA_TRY(cudaGetLastError());
     if (!save) e->refresh_bounds();
     return MXG_OK;
 }
@@ -2538,6 +2567,11 @@ int mxg_engine_vjp_step_forces(mxg_engine *e, void *lam_x, void *lam_v, double *
     a.pot_grad = e->d_pot_grad;
     a.dcoef = e->d_dcoef;
     a.partials = e->d_adj_partials;
+    a.items = e->d_adj_items;
+    a.nitems = e->adj_nitems;
+    a.item_ctr = e->d_adj_ctr;
+    a.pgx = e->d_adj_pgx;
+    a.pgv = e->d_adj_pgv;
     a.bond_partials = e->d_adj_bond_partials;
     a.nslots = e->grad_slots;
     launch_vjp_step(v, a, bonded ? &bv : nullptr, e->num_sms, grad, e->stream);
