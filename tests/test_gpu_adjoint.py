@@ -109,6 +109,44 @@ def test_snapshot_replays_bitwise():
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
 
 
+def test_vjp_step_with_saved_forces_matches_recomputed_forces():
+    """The VJP of a step taken with the forces that the step itself produced
+    (mxg_engine_save_forces, then mxg_engine_vjp_step_forces) gives the same adjoints and
+    parameter terms, bit for bit, as the VJP that repeats the step's force pass."""
+    spec = _spec()
+    u, P, sim = _gpu(spec)
+    P.register()
+    sim.load(spec["x"], spec["v"])
+    sim.step(2)
+    e = sim._engine()
+    buf = sim.snapshot_buffer()
+    sim.save(buf)
+    sim.step(1)
+    fbuf = torch.empty((N, 4), dtype=torch.float32, device="cuda")
+    assert lib().mxg_engine_save_forces(e, ctypes.c_void_p(fbuf.data_ptr())) == 0
+    rng = np.random.default_rng(11)
+    lam0 = torch.tensor(rng.normal(size=(N, 4)), dtype=torch.float32, device="cuda")
+    outs = []
+    for forces in (None, fbuf):
+        sim.restore(buf)
+        lx, lv = lam0.clone(), (0.5 * lam0).clone()
+        g = torch.zeros(16, dtype=torch.float64, device="cuda")
+        gp = ctypes.cast(g.data_ptr(), ctypes.POINTER(ctypes.c_double))
+        if forces is None:
+            rc = lib().mxg_engine_vjp_step(e, ctypes.c_void_p(lx.data_ptr()), ctypes.c_void_p(lv.data_ptr()), gp)
+        else:
+            rc = lib().mxg_engine_vjp_step_forces(e, ctypes.c_void_p(lx.data_ptr()), ctypes.c_void_p(lv.data_ptr()),
+                                                  gp, ctypes.c_void_p(forces.data_ptr()))
+        assert rc == 0
+        torch.cuda.synchronize()
+        outs.append((lx.cpu().numpy(), lv.cpu().numpy(), g.cpu().numpy()))
+    (x0, v0, g0), (x1, v1, g1) = outs
+    assert np.array_equal(x0.view(np.uint32), x1.view(np.uint32))
+    assert np.array_equal(v0.view(np.uint32), v1.view(np.uint32))
+    assert np.array_equal(g0.view(np.uint64), g1.view(np.uint64))
+    assert np.abs(g0[:len(P.slots)]).sum() > 0
+
+
 def test_adjoint_gradients_match_fp64_finite_differences():
     spec = _spec()
     target = W.rdf_target()
