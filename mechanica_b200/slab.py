@@ -17,8 +17,9 @@ never built. One step:
 3. one engine step; the rank keeps the particles that stayed in its slab and sends the ones that
    left it (into a ghost layer) to the rank that owns their new cell.
 
-Both exchanges are all-gathers over torch.distributed (gloo with host tensors, or NCCL with
-device tensors); every rank takes the same collective steps in the same order. The engine is
+Both exchanges are point-to-point with the two neighbouring slabs only (torch.distributed
+isend / irecv: gloo with host tensors, or NCCL with device tensors), counts first, then the
+records into the receiver's buffer; gather() collects the whole state with all-gathers. The engine is
 rebuilt every step (a slab's particle count changes from step to step), so this path gives the
 decomposition's results, not the speed of a resident multi-GPU engine. Not decomposed: bonds,
 angles, dihedrals, exclusions, species, large particles and cuboids (refused), and the Philox
@@ -114,6 +115,46 @@ def exchange(records, rank, world, group=None, device=None):
     return np.concatenate(out) if out else np.zeros(0, dtype=RECORD)
 
 
+def exchange_neighbours(records, rank, world, peers, group=None, device=None):
+    """Point-to-point exchange with the neighbouring slabs only (ghosts and leavers never go
+    further: a particle moves less than one cell layer per step, and every slab is at least two
+    layers wide). Every record must be addressed to one of `peers` (the distinct neighbour
+    ranks). Each pair of neighbours swaps the count, then the records, straight into the
+    receiver's buffer (torch.distributed isend / irecv: gloo with host tensors, NCCL with
+    device tensors). Returns the records received, in ascending source rank."""
+    import torch
+    import torch.distributed as dist
+    if world == 1 or not peers:
+        return records[records["dest"] == rank]
+    bad = ~np.isin(records["dest"], np.asarray(list(peers), dtype=np.int32))
+    if bad.any():
+        raise RuntimeError(f"slab rank {rank}: records addressed beyond the neighbouring slabs {sorted(peers)}")
+    dev = device or torch.device("cpu")
+    size = records.dtype.itemsize
+    peers = sorted(peers)
+    out_n = {p: torch.tensor([int((records["dest"] == p).sum())], dtype=torch.int64, device=dev) for p in peers}
+    in_n = {p: torch.zeros(1, dtype=torch.int64, device=dev) for p in peers}
+    reqs = [dist.irecv(in_n[p], src=p, group=group) for p in peers]
+    reqs += [dist.isend(out_n[p], dst=p, group=group) for p in peers]
+    for r in reqs:
+        r.wait()
+    sends, recvs, reqs = {}, {}, []
+    for p in peers:
+        n_in = int(in_n[p].item())
+        if n_in:
+            recvs[p] = torch.empty(n_in * size, dtype=torch.uint8, device=dev)
+            reqs.append(dist.irecv(recvs[p], src=p, group=group))
+    for p in peers:
+        sel = records[records["dest"] == p]
+        if len(sel):
+            sends[p] = torch.from_numpy(np.ascontiguousarray(sel).view(np.uint8).copy()).to(dev)
+            reqs.append(dist.isend(sends[p], dst=p, group=group))
+    for r in reqs:
+        r.wait()
+    got = [np.frombuffer(recvs[p].cpu().numpy().tobytes(), dtype=RECORD) for p in peers if p in recvs]
+    return np.concatenate(got) if got else np.zeros(0, dtype=RECORD)
+
+
 class Slab:
     """This rank's slab of a universe built for the whole box (types, potentials, forces and all
     particles, as on a single GPU; every rank builds the same one). The whole box is placed once
@@ -141,6 +182,8 @@ class Slab:
         self.ncx = int(self.cdim[0])
         self.ranges = slab_ranges(self.ncx, world)
         self.layer_owner = owner_of_layers(self.ranges, self.ncx)
+        x0, x1 = self.ranges[rank]
+        self.peers = sorted({int(self.layer_owner[(x0 - 1) % self.ncx]), int(self.layer_owner[x1 % self.ncx])} - {rank})
         x, v, f, cell, xr = u.state()
         self.n_total = len(cell)
         mine = self.layer_owner[cell // self.ncyz] == rank
@@ -173,7 +216,7 @@ class Slab:
         # 1. ghosts from the neighbouring slabs
         gi, gd = ghost_records(self.cells, self.layer_owner, rank, self.ranges, self.ncyz, self.ncx)
         sent = pack(gd, self.ids[gi], self.types[gi], self.cells[gi], self.xr[gi], self.v[gi])
-        ghosts = exchange(sent, rank, world, self.group, self.device)
+        ghosts = exchange_neighbours(sent, rank, world, self.peers, self.group, self.device)
         # 2. the rank's engine: own particles, then ghosts, placed in ascending id
         ids = np.concatenate([self.ids, ghosts["id"]])
         types = np.concatenate([self.types, ghosts["type"]])
@@ -191,7 +234,7 @@ class Slab:
         dest = self.layer_owner[nc // self.ncyz]
         stay = dest == rank
         leavers = pack(dest[~stay], self.ids[~stay], self.types[~stay], nc[~stay], nxr[~stay], nv[~stay])
-        arrived = exchange(leavers, rank, world, self.group, self.device)
+        arrived = exchange_neighbours(leavers, rank, world, self.peers, self.group, self.device)
         self.ids = np.concatenate([self.ids[stay], arrived["id"]]).astype(np.int32)
         self.types = np.concatenate([self.types[stay], arrived["type"]]).astype(np.int32)
         self.cells = np.concatenate([nc[stay], arrived["cell"]]).astype(np.int32)

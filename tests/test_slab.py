@@ -1,7 +1,8 @@
 """Slab decomposition bookkeeping on the CPU (mechanica_b200.slab): the slab ranges, the
 owners of the cell layers, which particles go to which neighbour as ghosts, and the record
 exchange between gloo ranks (world sizes 2 and 3) -- every rank receives exactly the records
-addressed to it, in source-rank order."""
+addressed to it, in source-rank order -- and the step's neighbour-only point-to-point exchange
+(world sizes 2, 3 and 4)."""
 import numpy as np
 import pytest
 
@@ -53,6 +54,17 @@ def test_one_slab_sends_no_ghosts():
 def test_exchange_over_gloo(tmp_path, world):
     out = str(tmp_path / "route")
     res = run_ranks(world, ["routing", out], timeout=180)
+    assert all(rc == 0 for rc, _ in res), res
+    for r in range(world):
+        assert open(f"{out}.{r}").read() == "ok"
+
+
+@pytest.mark.parametrize("world", [2, 3, 4])
+def test_neighbour_exchange_over_gloo(tmp_path, world):
+    """The slab step's exchange: point-to-point with the two neighbouring slabs only, counts then
+    records; every rank receives exactly what its neighbours addressed to it."""
+    out = str(tmp_path / "nb")
+    res = run_ranks(world, ["neighbours", out], timeout=180)
     assert all(rc == 0 for rc, _ in res), res
     for r in range(world):
         assert open(f"{out}.{r}").read() == "ok"
