@@ -751,9 +751,30 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, TS::kBlocks) force_kernel
                                 rtj[u] = __float_as_int(q.w);
                             }
                         }
+                        // the candidate test's form for the whole region: the type test is moot
+                        // when every own particle has a potential with every type staged, the
+                        // own-index test when no SELF neighbour is staged (2: the full test)
+                        int pmode = 2;
+                        if (!prune) {
+                            unsigned long long rtypes = 0ull;
+                            bool rs_any = false;
+#pragma unroll
+                            for (int u = 0; u < kChunks; ++u)
+                                if (u * 32 + lane < M) {
+                                    rtypes |= 1ull << rtj[u];
+                                    rs_any |= rself[u] >= 0;
+                                }
+                            rtypes = (unsigned long long)__reduce_or_sync(kFull, (unsigned)rtypes) |
+                                     ((unsigned long long)__reduce_or_sync(kFull, (unsigned)(rtypes >> 32)) << 32);
+                            bool full = true;
+                            for (int k = lane; k < ni; k += 32) full &= (sm.own_mask[k] & rtypes) == rtypes;
+                            if (__all_sync(kFull, full)) pmode = __any_sync(kFull, rs_any) ? 1 : 0;
+                        }
                         __syncwarp();
                         // ---- pass 1: each own particle against the region, kChunks steps of
-                        // 32 candidates, then pass 2 on every full batch of 32 queued pairs
+                        // 32 candidates, then pass 2 on every full batch of 32 queued pairs.
+                        // The squared distance is formed with fused multiply-adds: pass 1 is a
+                        // superset filter (widened cutoff), the exact test is pass 2's
                         int qhead = 0, qtail = 0;
                         // il == ni adds no candidates and flushes the queue: one call site of
                         // eval_batch keeps the kernel's instruction footprint small
@@ -761,36 +782,68 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, TS::kBlocks) force_kernel
                             if (il < ni) {
                                 const float4 xi = sm.own_x[il];
                                 const int i = i0 + il;
-                                const unsigned long long mk = sm.own_mask[il];
                                 unsigned hb[kChunks];
                                 bool hv[kChunks];
+                                if (pmode == 0) {
 #pragma unroll
-                                for (int u = 0; u < kChunks; ++u) {
-                                    hb[u] = 0u;
-                                    hv[u] = false;
-                                    if (u * 32 < M) {
-                                        const float dx = __fsub_rn(xi.x, rbx[u]);
-                                        const float dy = __fsub_rn(xi.y, rby[u]);
-                                        const float dz = __fsub_rn(xi.z, rbz[u]);
-                                        const float r2 = dot3_rn(dx, dy, dz);
-                                        // a cell's own pair once (neighbour index above the own one; -1, not
-                                        // a SELF neighbour, compares as the largest unsigned value), or from
-                                        // both sides when the cell takes several own-particle passes
-                                        const bool pair_ok = self_once ? (unsigned)rself[u] > (unsigned)i : rself[u] != i;
-                                        bool hit = (r2 <= rc2[u]) & (((mk >> rtj[u]) & 1ull) != 0ull) & pair_ok;
-                                        if (prune && hit && rself[u] < 0) {
-                                            // runner_dopair's pruning: a pair (first, second) is evaluated
-                                            // only when key_second + dnshift - key_first < dmaxdist
-                                            // (runner_dopair.cpp:167-182)
-                                            const int jj = u * 32 + lane;
-                                            const int meta = __float_as_int(sm.nb_s[jj].w);
-                                            const int epk = __float_as_int(sm.ent_sh[(meta >> 2) & 31].w);
-                                            const int okey = sort_key(xi.x, xi.y, xi.z, v.axes->n[(epk >> 2) & 15],
-                                                                      sbias, sdscale);
-                                            hit = sm.nb_key[jj] + (epk >> 8) - okey < dmaxdist;
+                                    for (int u = 0; u < kChunks; ++u) {
+                                        hb[u] = 0u;
+                                        hv[u] = false;
+                                        if (u * 32 < M) {
+                                            const float dx = __fsub_rn(xi.x, rbx[u]);
+                                            const float dy = __fsub_rn(xi.y, rby[u]);
+                                            const float dz = __fsub_rn(xi.z, rbz[u]);
+                                            const bool hit = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz))) <= rc2[u];
+                                            hb[u] = __ballot_sync(kFull, hit);
+                                            hv[u] = hit;
                                         }
-                                        hb[u] = __ballot_sync(kFull, hit);
-                                        hv[u] = hit;
+                                    }
+                                } else if (pmode == 1) {
+#pragma unroll
+                                    for (int u = 0; u < kChunks; ++u) {
+                                        hb[u] = 0u;
+                                        hv[u] = false;
+                                        if (u * 32 < M) {
+                                            const float dx = __fsub_rn(xi.x, rbx[u]);
+                                            const float dy = __fsub_rn(xi.y, rby[u]);
+                                            const float dz = __fsub_rn(xi.z, rbz[u]);
+                                            const float r2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+                                            const bool pair_ok = self_once ? (unsigned)rself[u] > (unsigned)i : rself[u] != i;
+                                            const bool hit = (r2 <= rc2[u]) & pair_ok;
+                                            hb[u] = __ballot_sync(kFull, hit);
+                                            hv[u] = hit;
+                                        }
+                                    }
+                                } else {
+                                    const unsigned long long mk = sm.own_mask[il];
+#pragma unroll
+                                    for (int u = 0; u < kChunks; ++u) {
+                                        hb[u] = 0u;
+                                        hv[u] = false;
+                                        if (u * 32 < M) {
+                                            const float dx = __fsub_rn(xi.x, rbx[u]);
+                                            const float dy = __fsub_rn(xi.y, rby[u]);
+                                            const float dz = __fsub_rn(xi.z, rbz[u]);
+                                            const float r2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+                                            // a cell's own pair once (neighbour index above the own one; -1, not
+                                            // a SELF neighbour, compares as the largest unsigned value), or from
+                                            // both sides when the cell takes several own-particle passes
+                                            const bool pair_ok = self_once ? (unsigned)rself[u] > (unsigned)i : rself[u] != i;
+                                            bool hit = (r2 <= rc2[u]) & (((mk >> rtj[u]) & 1ull) != 0ull) & pair_ok;
+                                            if (prune && hit && rself[u] < 0) {
+                                                // runner_dopair's pruning: a pair (first, second) is evaluated
+                                                // only when key_second + dnshift - key_first < dmaxdist
+                                                // (runner_dopair.cpp:167-182)
+                                                const int jj = u * 32 + lane;
+                                                const int meta = __float_as_int(sm.nb_s[jj].w);
+                                                const int epk = __float_as_int(sm.ent_sh[(meta >> 2) & 31].w);
+                                                const int okey = sort_key(xi.x, xi.y, xi.z, v.axes->n[(epk >> 2) & 15],
+                                                                          sbias, sdscale);
+                                                hit = sm.nb_key[jj] + (epk >> 8) - okey < dmaxdist;
+                                            }
+                                            hb[u] = __ballot_sync(kFull, hit);
+                                            hv[u] = hit;
+                                        }
                                     }
                                 }
 #pragma unroll
