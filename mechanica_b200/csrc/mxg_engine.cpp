@@ -469,6 +469,8 @@ struct mxg_engine {
     float4 *d_ld_xr = nullptr, *d_ld_vel = nullptr;
     int *d_ld_cell = nullptr, *d_ld_ids = nullptr, *d_ld_count = nullptr, *d_ld_fill = nullptr, *d_ld_err = nullptr;
     int *h_ld_err = nullptr;  // pinned: the load's out-of-box flag, read back without a staging copy
+    cudaStream_t ld_stream = nullptr;               // the load's velocity copy, beside the placement
+    cudaEvent_t ld_x_done = nullptr, ld_v_done = nullptr;
     int *d_type_of_id = nullptr, *d_rep_of_id = nullptr, *d_ul_cell = nullptr;
     int *d_slot_of_id = nullptr;
     int *d_cell_rep = nullptr;
@@ -560,6 +562,9 @@ struct mxg_engine {
             if (graph[k]) cudaGraphExecDestroy(graph[k]);
         for (void *p : allocations) cudaFree(p);
         if (h_ld_err) cudaFreeHost(h_ld_err);
+        if (ld_x_done) cudaEventDestroy(ld_x_done);
+        if (ld_v_done) cudaEventDestroy(ld_v_done);
+        if (ld_stream) cudaStreamDestroy(ld_stream);
         if (own_stream) cudaStreamDestroy(own_stream);
     }
 
@@ -1540,11 +1545,24 @@ int mxg_engine::load_state(const double *x, const float *v, int n) {
         if (rc != MXG_OK) return MXG_ERR_MALLOC;
         if ((rc = upload(d_type_of_id, ptype, stream)) || (rc = upload(d_rep_of_id, prep, stream))) return rc;
     }
-    CUDA_TRY(cudaMemcpyAsync(d_ld_x, x, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, stream));
-    if (v) CUDA_TRY(cudaMemcpyAsync(d_ld_v, v, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, stream));
+    if (v && !ld_stream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&ld_stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&ld_x_done, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&ld_v_done, cudaEventDisableTiming));
+    }
     CUDA_TRY(cudaMemsetAsync(d_ld_count, 0, sizeof(int) * (size_t)ncells, stream));
     CUDA_TRY(cudaMemsetAsync(d_ld_fill, 0, sizeof(int) * (size_t)ncells, stream));
     CUDA_TRY(cudaMemsetAsync(d_ld_err, 0, sizeof(int), stream));
+    CUDA_TRY(cudaMemcpyAsync(d_ld_x, x, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, stream));
+    if (v) {
+        // the velocities cross after the positions, on a second stream, while the placement,
+        // the scan, the fill and the ordering (which need only the positions) run; only the
+        // launch that writes the velocities into their slots waits for them
+        CUDA_TRY(cudaEventRecord(ld_x_done, stream));
+        CUDA_TRY(cudaStreamWaitEvent(ld_stream, ld_x_done, 0));
+        CUDA_TRY(cudaMemcpyAsync(d_ld_v, v, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, ld_stream));
+        CUDA_TRY(cudaEventRecord(ld_v_done, ld_stream));
+    }
     LoadView ld;
     ld.x = d_ld_x;
     ld.v = v ? d_ld_v : nullptr;
@@ -1560,15 +1578,14 @@ int mxg_engine::load_state(const double *x, const float *v, int n) {
     ld.n = n;
     const EngineView ev = view(cur);
     launch_load_place(ev, ld, d_ld_count, stream);
+    // the ordering launches write nothing when a particle lay outside its box, so one
+    // synchronisation at the end reports the error with the engine's state untouched
+    launch_load_order(ev, ld, d_ld_count, d_cell_start[cur], d_cell_count[cur], d_pos[cur], d_vel[cur],
+                      d_cell_of[cur], d_slot_of_id, v ? ld_v_done : nullptr, stream);
     CUDA_TRY(cudaMemcpyAsync(h_ld_err, d_ld_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
     CUDA_TRY(cudaStreamSynchronize(stream));  // also: the caller's host arrays are free again
-    if (*h_ld_err) return MXG_ERR_SPACE;
-    CUDA_TRY(cudaMemcpyAsync(d_cell_count[cur], d_ld_count, sizeof(int) * (size_t)ncells, cudaMemcpyDeviceToDevice,
-                             stream));
-    launch_load_order(ev, ld, d_ld_count, d_cell_start[cur], d_pos[cur], d_vel[cur], d_cell_of[cur], d_slot_of_id,
-                      stream);
     CUDA_TRY(cudaGetLastError());
-    return MXG_OK;
+    return *h_ld_err ? MXG_ERR_SPACE : MXG_OK;
 }
 
 /* ======================================================================== */

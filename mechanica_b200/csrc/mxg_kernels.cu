@@ -2292,73 +2292,113 @@ __global__ void place_kernel(EngineView v, LoadView ld, int *count) {
     const int c = S.cell_offset + (ind[0] * S.cdim[1] + ind[1]) * S.cdim[2] + ind[2];
     ld.cell[p] = c;
     ld.xr[p] = make_float4(xr[0], xr[1], xr[2], __int_as_float(ld.type_of_id[p]));
-    // the given velocity, or the particle's current one
-    float4 u = ld.v ? make_float4(ld.v[3 * (size_t)p], ld.v[3 * (size_t)p + 1], ld.v[3 * (size_t)p + 2], 0.f)
-                    : v.vel[ld.slot_now[p]];
-    u.w = __int_as_float(p);
-    ld.vel[p] = u;
+    // a kept velocity is copied out before the ordering overwrites the slot arrays (given
+    // velocities are read by the ordering itself)
+    if (!ld.v) {
+        float4 u = v.vel[ld.slot_now[p]];
+        u.w = __int_as_float(p);
+        ld.vel[p] = u;
+    }
     atomicAdd(&count[c], 1);
 }
 
-/* Exclusive scan of the new occupancy into start[0..ncells] (one block, one pass): thread t
- * sums its own run of consecutive cells, the block scans the 1024 run totals (warp shuffles,
- * then the warp totals), and each thread writes its run's prefixes. */
-__global__ void __launch_bounds__(1024) load_scan_kernel(const int *__restrict__ count, int ncells, int *start) {
+/* Exclusive scan of the new occupancy into start[0..ncells] and a copy of the counts (one
+ * block, tiles of 8192 cells): a tile's counts are loaded coalesced into shared memory
+ * (every load in flight at once; a padding word after each run of eight keeps a thread's
+ * run in distinct banks), each thread sums its run of eight, the block scans the run totals
+ * (warp shuffles, then the warp totals) and the starts go back out coalesced. Nothing is
+ * written when the placement found a particle outside its box. */
+constexpr int kScanPer = 8;
+constexpr int kScanTile = 1024 * kScanPer;
+__device__ __forceinline__ int scan_slot(int i) { return i + i / kScanPer; }
+__global__ void __launch_bounds__(1024) load_scan_kernel(const int *__restrict__ count, int ncells, int *start,
+                                                         int *count_out, const int *err) {
+    __shared__ int tile[kScanTile + kScanTile / kScanPer];
     __shared__ int warp_sums[32];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int per = (ncells + blockDim.x - 1) / blockDim.x;
-    const int b0 = min(ncells, (int)threadIdx.x * per), b1 = min(ncells, b0 + per);
-    int run = 0;
-    for (int i = b0; i < b1; ++i) run += count[i];
-    int incl = run;
-    for (int d = 1; d < 32; d <<= 1) {
-        const int t = __shfl_up_sync(kFull, incl, d);
-        if (lane >= d) incl += t;
-    }
-    if (lane == 31) warp_sums[wid] = incl;
-    __syncthreads();
-    if (wid == 0) {
-        int w = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
-        for (int d = 1; d < 32; d <<= 1) {
-            const int t = __shfl_up_sync(kFull, w, d);
-            if (lane >= d) w += t;
+    if (*err) return;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    int carry = 0;
+    for (int t0 = 0; t0 < ncells; t0 += kScanTile) {
+        const int m = min(kScanTile, ncells - t0);
+#pragma unroll
+        for (int k = 0; k < kScanPer; ++k) {
+            const int i = k * 1024 + tid;
+            const int ci = i < m ? count[t0 + i] : 0;
+            tile[scan_slot(i)] = ci;
+            if (i < m) count_out[t0 + i] = ci;
         }
-        warp_sums[lane] = w;
+        __syncthreads();
+        int c[kScanPer], run = 0;
+#pragma unroll
+        for (int k = 0; k < kScanPer; ++k) {
+            c[k] = tile[scan_slot(tid * kScanPer + k)];
+            run += c[k];
+        }
+        int incl = run;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int t = __shfl_up_sync(kFull, incl, d);
+            if (lane >= d) incl += t;
+        }
+        if (lane == 31) warp_sums[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            int w = warp_sums[lane];
+            for (int d = 1; d < 32; d <<= 1) {
+                const int t = __shfl_up_sync(kFull, w, d);
+                if (lane >= d) w += t;
+            }
+            warp_sums[lane] = w;
+        }
+        __syncthreads();
+        int excl = carry + (wid ? warp_sums[wid - 1] : 0) + incl - run;
+#pragma unroll
+        for (int k = 0; k < kScanPer; ++k) {
+            tile[scan_slot(tid * kScanPer + k)] = excl;
+            excl += c[k];
+        }
+        carry += warp_sums[31];
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kScanPer; ++k) {
+            const int i = k * 1024 + tid;
+            if (i < m) start[t0 + i] = tile[scan_slot(i)];
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    int excl = (wid ? warp_sums[wid - 1] : 0) + incl - run;
-    for (int i = b0; i < b1; ++i) {
-        start[i] = excl;
-        excl += count[i];
-    }
-    if (threadIdx.x == blockDim.x - 1) start[ncells] = warp_sums[(blockDim.x >> 5) - 1];
+    if (tid == 0) start[ncells] = carry;
 }
 
 /* Each particle takes a place in its cell's range (in any order; ordered next). */
 __global__ void load_fill_kernel(LoadView ld, const int *__restrict__ start) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= ld.n) return;
+    if (p >= ld.n || *ld.err) return;
     const int c = ld.cell[p];
     ld.ids[start[c] + atomicAdd(&ld.fill[c], 1)] = p;
 }
 
 /* One warp per cell: its particles in ascending id (rank = number of smaller ids in the
- * cell), written to the slot arrays, then the cell's projection-key bounds. */
+ * cell, compared through warp shuffles), written to the slot arrays, then the cell's
+ * projection-key bounds. Nothing is written when the placement failed. */
 __global__ void load_order_kernel(EngineView v, LoadView ld, const int *__restrict__ start, float4 *pos_out,
                                   float4 *vel_out, int *cell_out, int *slot_of_id, int2 *sort_bounds) {
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
+    if (*ld.err) return;
     for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < v.ncells; c += warps) {
         const int s0 = start[c], n = start[c + 1] - s0;
         for (int k0 = 0; k0 < n; k0 += 32) {
             const int k = k0 + lane;
+            const int id = k < n ? ld.ids[s0 + k] : 0x7fffffff;
+            int rank = 0;
+            for (int b0 = 0; b0 < n; b0 += 32) {
+                const int other = b0 == k0 ? id : (b0 + lane < n ? ld.ids[s0 + b0 + lane] : 0x7fffffff);
+                const int m = min(32, n - b0);
+                for (int q = 0; q < m; ++q) rank += __shfl_sync(kFull, other, q) < id;
+            }
             if (k < n) {
-                const int id = ld.ids[s0 + k];
-                int rank = 0;
-                for (int q = 0; q < n; ++q) rank += ld.ids[s0 + q] < id;
                 const int dst = s0 + rank;
                 pos_out[dst] = ld.xr[id];
-                vel_out[dst] = ld.vel[id];
+                if (!ld.v) vel_out[dst] = ld.vel[id];  // given velocities: load_vel_kernel
                 cell_out[dst] = c;
                 slot_of_id[id] = dst;
             }
@@ -2367,6 +2407,15 @@ __global__ void load_order_kernel(EngineView v, LoadView ld, const int *__restri
         const DevSpace &S = v.spaces[v.cell_rep[c]];
         if (n > 0 && (S.prune & 2)) cell_sort_bounds(pos_out, s0, n, S.sort_bias, S.sort_dscale, v.axes, sort_bounds + c * 13);
     }
+}
+
+/* Given velocities into their particles' new slots (after the ordering, once the copy of
+ * the velocities has arrived); w = id. */
+__global__ void load_vel_kernel(LoadView ld, const int *__restrict__ slot_of_id, float4 *vel_out) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ld.n || *ld.err) return;
+    vel_out[slot_of_id[p]] = make_float4(ld.v[3 * (size_t)p], ld.v[3 * (size_t)p + 1], ld.v[3 * (size_t)p + 2],
+                                         __int_as_float(p));
 }
 
 /* engine_unload's arrays by particle id (engine.cpp:620-784): the global position
@@ -2666,13 +2715,18 @@ void launch_load_place(const EngineView &v, const LoadView &ld, int *count, cuda
     place_kernel<<<(ld.n + 255) / 256, 256, 0, st>>>(v, ld, count);
 }
 
-void launch_load_order(const EngineView &v, const LoadView &ld, const int *count, int *start, float4 *pos_out,
-                       float4 *vel_out, int *cell_out, int *slot_of_id, cudaStream_t st) {
-    load_scan_kernel<<<1, 1024, 0, st>>>(count, v.ncells, start);
+void launch_load_order(const EngineView &v, const LoadView &ld, const int *count, int *start, int *count_out,
+                       float4 *pos_out, float4 *vel_out, int *cell_out, int *slot_of_id, cudaEvent_t vel_ready,
+                       cudaStream_t st) {
+    load_scan_kernel<<<1, 1024, 0, st>>>(count, v.ncells, start, count_out, ld.err);
     load_fill_kernel<<<(ld.n + 255) / 256, 256, 0, st>>>(ld, start);
     const int tb = 256;
     load_order_kernel<<<(v.ncells * 32 + tb - 1) / tb, tb, 0, st>>>(v, ld, start, pos_out, vel_out, cell_out,
                                                                      slot_of_id, v.sort_bounds);
+    if (ld.v) {  // the given velocities, once their copy has arrived
+        if (vel_ready) cudaStreamWaitEvent(st, vel_ready, 0);
+        load_vel_kernel<<<(ld.n + 255) / 256, 256, 0, st>>>(ld, slot_of_id, vel_out);
+    }
 }
 
 void launch_unload(const EngineView &v, const float4 *force_ids, double *x, float *vel, float *f, int *cell,

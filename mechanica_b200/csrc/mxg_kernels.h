@@ -61,8 +61,9 @@ void launch_number_density(const EngineView &v, const int *flux_off, float *nd_b
  * caller); ld.err is set when a particle lies outside its box. */
 void launch_load_place(const EngineView &v, const LoadView &ld, int *count, cudaStream_t st);
 /* The rest of the load: scan of count into start, the slot arrays in (cell, id) order, key bounds. */
-void launch_load_order(const EngineView &v, const LoadView &ld, const int *count, int *start, float4 *pos_out,
-                       float4 *vel_out, int *cell_out, int *slot_of_id, cudaStream_t st);
+void launch_load_order(const EngineView &v, const LoadView &ld, const int *count, int *start, int *count_out,
+                       float4 *pos_out, float4 *vel_out, int *cell_out, int *slot_of_id, cudaEvent_t vel_ready,
+                       cudaStream_t st);
 /* engine_unload's arrays by id on the device (any output may be null); force_ids: the velocities of the slot
  * order the forces were computed in */
 void launch_unload(const EngineView &v, const float4 *force_ids, double *x, float *vel, float *f, int *cell,

@@ -49,6 +49,29 @@ def test_device_load_matches_host_placement(name):
     assert np.array_equal(after_load.view(np.uint32), after_host.view(np.uint32))
 
 
+def test_device_load_matches_host_placement_on_a_large_grid():
+    """16,000 cells (two tiles of the device scan of the occupancy), a few of them empty,
+    velocities given (their copy overlaps the placement)."""
+    from mechanica_b200 import workloads as W
+    scn = W.dpd(n=60000, dims=(40.0, 20.0, 20.0), seed=4)
+    u = W.build_gpu(scn)
+    u.steps(3)
+    x, v, f, c, xr = u.state()
+    assert np.bincount(np.asarray(c), minlength=16000).min() == 0
+    u.load(x, v)
+    xl, vl, fl, cl, xrl = u.state()
+    pl, wl, cellsl = _slots(u)
+    u.close()
+    u = W.build_gpu(dict(scn, x=x, v=v))
+    x2, v2, f2, c2, xr2 = u.state()
+    p2, w2, cells2 = _slots(u)
+    u.close()
+    assert np.array_equal(cl, c2)
+    assert np.array_equal(xrl.view(np.uint32), xr2.view(np.uint32))
+    assert np.array_equal(xl, x2) and np.array_equal(vl, v2)
+    assert np.array_equal(pl, p2) and np.array_equal(wl, w2) and np.array_equal(cellsl, cells2)
+
+
 def test_load_keeps_velocities_and_rejects_outside_positions():
     z, scn = load("argon_small")
     u = S.build_gpu(scn)
