@@ -341,7 +341,9 @@ int mxg_engine_unload(mxg_engine *e, int n, double *x, float *v, float *f, int *
 /* Per-id upload of positions (double[3n], global coordinates) and velocities (float[3n]; NULL keeps
  * each particle's velocity); particles are placed as engine_addpart would place them and ordered by
  * (cell, id), both on the device. A position outside its replica's box returns MXG_ERR_SPACE and
- * changes no state. */
+ * changes no state. Returns once the engine's stream has finished the load, so the host arrays
+ * may be reused at once; the velocities cross on a second stream of the engine's while the
+ * placement runs. */
 int mxg_engine_load(mxg_engine *e, int n, const double *x, const float *v);
 /* Potential energy (nonbonded + bonded) of the last force evaluation and the current kinetic energy,
  * both reduced in FP64 on the device. virial9 (may be NULL): the virial of the current positions,
