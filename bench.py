@@ -12,8 +12,9 @@ time (per-step CUDA events on the engine stream, L2 flushed between steps with
 a 256 MiB write). e2e = the same metric through the C ABI in the reference's
 data format with host buffers: every step engine_load's the absolute positions
 and velocities by particle id from pinned host memory, steps, and
-engine_unload's them back (host clock); the raw slot-order state copy is
-reported beside it. roofline: the force kernel against the FP32 pipe (and, as
+engine_unload's them back (host clock; the median of five blocks of round
+trips, each block's mean); the raw slot-order state copy is reported beside
+it. roofline: the force kernel against the FP32 pipe (and, as
 hbm_view, against the measured copy bandwidth); rebin_view: the integrator and
 the re-binning scatter against the measured copy bandwidth.
 
@@ -682,18 +683,25 @@ def main():
         check(L.mxg_engine_load(e, n, xp, vp), "load")
         check(L.mxg_engine_step(e, 1), "step")
         check(L.mxg_engine_unload(e, n, xp, vp, None, None, None), "unload")
-    Kl = max(100, min(K, 200))  # at least 100 round trips: one host hiccup must not set the figure
+    # five blocks of round trips, each timed on the host clock as a whole (its mean per round
+    # trip); the figure is the median block, so that one stall of the host (another process
+    # scheduled on the core for some milliseconds) does not set it
+    NB, KB = 5, max(20, min(K, 40))
+    Kl = NB * KB
+    blocks = []
     barrier()
-    t_l = time.perf_counter()
-    for k in range(Kl):
-        check(L.mxg_engine_load(e, n, xp, vp), "load")
-        check(L.mxg_engine_step(e, 1), "step")
-        check(L.mxg_engine_unload(e, n, xp, vp, None, None, None), "unload")
-    torch.cuda.synchronize(dev)
-    ms_l = max_over_ranks(1e3 * (time.perf_counter() - t_l), world, dev)
+    for b in range(NB):
+        t_l = time.perf_counter()
+        for k in range(KB):
+            check(L.mxg_engine_load(e, n, xp, vp), "load")
+            check(L.mxg_engine_step(e, 1), "step")
+            check(L.mxg_engine_unload(e, n, xp, vp, None, None, None), "unload")
+        torch.cuda.synchronize(dev)
+        blocks.append(1e3 * (time.perf_counter() - t_l) / KB)
+    ms_l = max_over_ranks(float(np.median(blocks)), world, dev)
     barrier()
     check(L.mxg_engine_status(e), "e2e status")
-    e2e = job_rate(world, n, Kl, ms_l)
+    e2e = job_rate(world, n, 1, ms_l)
 
     # ---- roofline of the dominant kernel (nonbonded forces) ----
     # the force kernel alone, per launch, L2 flushed before each launch; the median
@@ -795,6 +803,9 @@ def main():
             "clocks": clocks, "gpu_launches": 3 * K,
             "e2e": {"value": e2e, "unit": "particle-steps/s", "steps": Kl, "h2d_bytes_per_step": 36 * n,
                     "d2h_bytes_per_step": 36 * n,
+                    "statistic": f"median of {NB} blocks of {KB} round trips, each block timed as a whole "
+                                 "on the host clock (its mean per round trip)",
+                    "block_ms_per_step": [round(x, 4) for x in blocks],
                     "path": "mxg_engine_load (absolute x double[3], v float[3] by id, pinned host -> device; "
                             "placement and (cell, id) ordering on the device), mxg_engine_step, "
                             "mxg_engine_unload (x, v by id, device -> pinned host); host wall clock",
