@@ -264,6 +264,7 @@ __global__ void __launch_bounds__(kWarpsA * 32, 4) vjp_pair_kernel(EngineView v,
         const DevSpace &S = v.spaces[v.cell_rep[c]];
         const int pot_base = S.pot_offset;
         const float cut2_pair = S.cut2_pair, cut2_self = S.cut2_self;
+        const float cut2w_pair = S.cut2w_pair, cut2w_self = S.cut2w_self;
         const unsigned rng_mode = S.rng_mode;
         for (int i0 = 0; i0 < n; i0 += kOwnA) {
             const int ni = min(kOwnA, n - i0);
@@ -332,30 +333,65 @@ __global__ void __launch_bounds__(kWarpsA * 32, 4) vjp_pair_kernel(EngineView v,
                     }
                     if (lane == 0) sm.reg_beg[nent] = M;
                     __syncwarp();
-                    for (int idx = lane; idx < M; idx += 32) {
-                        int r = 0;
-                        for (int step = 16; step > 0; step >>= 1)
-                            if (r + step < nent && sm.reg_beg[r + step] <= idx) r += step;
-                        const int ke = rce + r;
-                        const int jl = sm.reg_jb[r] + idx - sm.reg_beg[r];
-                        const int slot = sm.ent_slot[ke] + jl;
-                        const float4 es = sm.ent_sh[ke];
-                        const int role = __float_as_int(es.w) & 3;
-                        float4 q = v.pos[slot];
-                        float4 s4 = make_float4(0.f, 0.f, 0.f, __int_as_float(role | (ke << 2) | (jl << 8)));
-                        if (role == kRoleSecond) {
-                            q.x -= es.x;
-                            q.y -= es.y;
-                            q.z -= es.z;
-                        } else if (role == kRoleFirst) {
-                            s4.x = es.x;
-                            s4.y = es.y;
-                            s4.z = es.z;
+                    // lane's chunk-u neighbour (staged index u * 32 + lane) is also kept in registers
+                    // for the candidate pass: its position plus the entry's shift, a widened cutoff
+                    // (-1: empty), its index in the cell when it is a SELF neighbour (else -1) and its
+                    // type; the candidate pass is a superset filter, the drain applies the exact test
+                    float rbx[kChunksA], rby[kChunksA], rbz[kChunksA], rc2[kChunksA];
+                    int rself[kChunksA], rtj[kChunksA];
+                    unsigned long long rtypes = 0ull;
+                    bool rs_any = false;
+#pragma unroll
+                    for (int u = 0; u < kChunksA; ++u) {
+                        const int idx = u * 32 + lane;
+                        rbx[u] = rby[u] = rbz[u] = 0.f;
+                        rc2[u] = -1.f;
+                        rself[u] = -1;
+                        rtj[u] = 0;
+                        if (idx < M) {
+                            int r = 0;
+                            for (int step = 16; step > 0; step >>= 1)
+                                if (r + step < nent && sm.reg_beg[r + step] <= idx) r += step;
+                            const int ke = rce + r;
+                            const int jl = sm.reg_jb[r] + idx - sm.reg_beg[r];
+                            const int slot = sm.ent_slot[ke] + jl;
+                            const float4 es = sm.ent_sh[ke];
+                            const int role = __float_as_int(es.w) & 3;
+                            float4 q = v.pos[slot];
+                            float4 s4 = make_float4(0.f, 0.f, 0.f, __int_as_float(role | (ke << 2) | (jl << 8)));
+                            if (role == kRoleSecond) {
+                                q.x -= es.x;
+                                q.y -= es.y;
+                                q.z -= es.z;
+                            } else if (role == kRoleFirst) {
+                                s4.x = es.x;
+                                s4.y = es.y;
+                                s4.z = es.z;
+                            }
+                            sm.nb_x[idx] = q;
+                            sm.nb_s[idx] = s4;
+                            sm.nb_v[idx] = v.vel[slot];
+                            sm.nb_w[idx] = a.w[slot];
+                            rbx[u] = __fadd_rn(q.x, s4.x);
+                            rby[u] = __fadd_rn(q.y, s4.y);
+                            rbz[u] = __fadd_rn(q.z, s4.z);
+                            rc2[u] = role == kRoleSelf ? cut2w_self : cut2w_pair;
+                            rself[u] = role == kRoleSelf ? jl : -1;
+                            rtj[u] = __float_as_int(q.w);
+                            rtypes |= 1ull << rtj[u];
+                            rs_any |= role == kRoleSelf;
                         }
-                        sm.nb_x[idx] = q;
-                        sm.nb_s[idx] = s4;
-                        sm.nb_v[idx] = v.vel[slot];
-                        sm.nb_w[idx] = a.w[slot];
+                    }
+                    // the candidate test's form for the whole region: the type test is moot when every
+                    // own particle has a potential with every type staged, the own-index test when no
+                    // SELF neighbour is staged (2: the full test)
+                    int pmode = 2;
+                    {
+                        rtypes = (unsigned long long)__reduce_or_sync(kFull, (unsigned)rtypes) |
+                                 ((unsigned long long)__reduce_or_sync(kFull, (unsigned)(rtypes >> 32)) << 32);
+                        bool full = true;
+                        for (int k = lane; k < ni; k += 32) full &= (sm.own_mask[k] & rtypes) == rtypes;
+                        if (__all_sync(kFull, full)) pmode = __any_sync(kFull, rs_any) ? 1 : 0;
                     }
                     __syncwarp();
                     int qhead = 0, qtail = 0;
@@ -369,6 +405,8 @@ __global__ void __launch_bounds__(kWarpsA * 32, 4) vjp_pair_kernel(EngineView v,
                             const float4 xi = sm.own_x[il], b = sm.nb_x[jj], s = sm.nb_s[jj];
                             const float3 d = make_float3((xi.x - s.x) - b.x, (xi.y - s.y) - b.y, (xi.z - s.z) - b.z);
                             const float r2 = d.x * d.x + d.y * d.y + d.z * d.z;
+                            // the exact cutoff test of the pair loops (the candidate pass queued a superset)
+                            const bool inside = r2 <= ((__float_as_int(s.w) & 3) == kRoleSelf ? cut2_self : cut2_pair);
                             const float4 vi = sm.own_v[il], vj = sm.nb_v[jj];
                             const float4 wi = sm.own_w[il], wj = sm.nb_w[jj];
                             const float3 u = make_float3(wi.x - wj.x, wi.y - wj.y, wi.z - wj.z);
@@ -378,8 +416,8 @@ __global__ void __launch_bounds__(kWarpsA * 32, 4) vjp_pair_kernel(EngineView v,
                             const bool count = ida < idb;
                             const float radi = v.types[ti].radius, radj = v.types[tj].radius;
                             const int p1 = v.pot_idx[pot_base + ti * ntypes + tj];
-                            term_vjp(v, a, p1, radi, radj, d, r2, vij, ida, idb, rng_mode, u, count, gx, gv, gl);
-                            if (v.pot_idx2) {
+                            if (inside) term_vjp(v, a, p1, radi, radj, d, r2, vij, ida, idb, rng_mode, u, count, gx, gv, gl);
+                            if (inside && v.pot_idx2) {
                                 const int p2 = v.pot_idx2[pot_base + ti * ntypes + tj];
                                 if (p2 >= 0)
                                     term_vjp(v, a, p2, radi, radj, d, r2, vij, ida, idb, rng_mode, u, count, gx, gv,
@@ -413,23 +451,42 @@ __global__ void __launch_bounds__(kWarpsA * 32, 4) vjp_pair_kernel(EngineView v,
                     for (int il = 0; il < ni; ++il) {
                         const float4 xi = sm.own_x[il];
                         const int i = i0 + il;
-                        const unsigned long long mk = sm.own_mask[il];
+                        unsigned hb[kChunksA];
+                        bool hv[kChunksA];
+                        // squared distance by fused multiply-adds: a superset filter with a widened cutoff
+                        if (pmode == 0) {
+#pragma unroll
+                            for (int u = 0; u < kChunksA; ++u) {
+                                const float dx = __fsub_rn(xi.x, rbx[u]), dy = __fsub_rn(xi.y, rby[u]),
+                                            dz = __fsub_rn(xi.z, rbz[u]);
+                                hv[u] = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz))) <= rc2[u];
+                                hb[u] = __ballot_sync(kFull, hv[u]);
+                            }
+                        } else if (pmode == 1) {
+#pragma unroll
+                            for (int u = 0; u < kChunksA; ++u) {
+                                const float dx = __fsub_rn(xi.x, rbx[u]), dy = __fsub_rn(xi.y, rby[u]),
+                                            dz = __fsub_rn(xi.z, rbz[u]);
+                                hv[u] = (__fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz))) <= rc2[u]) & (rself[u] != i);
+                                hb[u] = __ballot_sync(kFull, hv[u]);
+                            }
+                        } else {
+                            const unsigned long long mk = sm.own_mask[il];
+#pragma unroll
+                            for (int u = 0; u < kChunksA; ++u) {
+                                const float dx = __fsub_rn(xi.x, rbx[u]), dy = __fsub_rn(xi.y, rby[u]),
+                                            dz = __fsub_rn(xi.z, rbz[u]);
+                                hv[u] = (__fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz))) <= rc2[u]) &
+                                        (rself[u] != i) & (((mk >> rtj[u]) & 1ull) != 0ull);
+                                hb[u] = __ballot_sync(kFull, hv[u]);
+                            }
+                        }
 #pragma unroll
                         for (int u = 0; u < kChunksA; ++u) {
-                            const int jj = u * 32 + lane;
-                            bool hit = false;
-                            if (jj < M) {
-                                const float4 b = sm.nb_x[jj], s = sm.nb_s[jj];
-                                const int meta = __float_as_int(s.w);
-                                const float dx = (xi.x - s.x) - b.x, dy = (xi.y - s.y) - b.y, dz = (xi.z - s.z) - b.z;
-                                const float r2 = dx * dx + dy * dy + dz * dz;
-                                const bool self = (meta & 3) == kRoleSelf;
-                                hit = r2 <= (self ? cut2_self : cut2_pair) && ((mk >> __float_as_int(b.w)) & 1ull) &&
-                                      !(self && (meta >> 8) == i);
-                            }
-                            const unsigned hb = __ballot_sync(kFull, hit);
-                            if (hit) sm.queue[(qtail + __popc(hb & lt_mask)) & (kQueueA - 1)] = (unsigned short)((il << 8) | jj);
-                            qtail += __popc(hb);
+                            if (hv[u])
+                                sm.queue[(qtail + __popc(hb[u] & lt_mask)) & (kQueueA - 1)] =
+                                    (unsigned short)((il << 8) | (u * 32 + lane));
+                            qtail += __popc(hb[u]);
                         }
                         while (qtail - qhead >= 32) {
                             __syncwarp();
