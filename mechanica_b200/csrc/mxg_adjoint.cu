@@ -523,7 +523,7 @@ __global__ void __launch_bounds__(kWarpsA * 32, 4) vjp_pair_kernel(EngineView v,
                            (size_t)(w * 32) * kMaxGradSlots;
             double t = 0.0;
             for (int l = 0; l < 32; ++l) t += base[(size_t)l * kMaxGradSlots + lane];
-            a.partials[(size_t)it * kMaxGradSlots + lane] = t;
+            a.partials[(size_t)lane * a.nitems + it] = t;
         }
         __syncwarp();
         for (int q = 0; q < kMaxGradSlots; ++q) gl[q] = 0.0;
@@ -634,16 +634,24 @@ __global__ void adj_finish_kernel(EngineView v, AdjointView a) {
 }
 
 /* grad[k] += the step's parameter-gradient partials of slot k: one block per slot, each thread
- * summing a fixed stride of the pair items' and bond blocks' partials, then a fixed tree over
- * the threads (the same order on every run). */
-constexpr int kGradThreads = 256;
-__global__ void __launch_bounds__(kGradThreads) adj_grad_kernel(AdjointView a, int nwarps, int nbond_blocks,
+ * summing a fixed stride of the pair items' partials (contiguous per slot, so a warp's loads
+ * are coalesced) and of the bond blocks' partials, then a fixed tree over the threads (the same
+ * order on every run). */
+constexpr int kGradThreads = 1024;
+__global__ void __launch_bounds__(kGradThreads) adj_grad_kernel(AdjointView a, int nitems, int nbond_blocks,
                                                               double *grad) {
     __shared__ double part[kGradThreads];
     const int k = blockIdx.x;
-    double t = 0.0;
-    for (int q = threadIdx.x; q < nwarps; q += blockDim.x) t += a.partials[(size_t)q * kMaxGradSlots + k];
-    for (int q = threadIdx.x; q < nbond_blocks; q += blockDim.x) t += a.bond_partials[(size_t)q * kMaxGradSlots + k];
+    const double *pk = a.partials + (size_t)k * nitems;
+    double t0 = 0.0, t1 = 0.0;  // two independent chains, added at the end
+    int q = threadIdx.x;
+    for (; q + (int)blockDim.x < nitems; q += 2 * blockDim.x) {
+        t0 += pk[q];
+        t1 += pk[q + blockDim.x];
+    }
+    if (q < nitems) t0 += pk[q];
+    double t = t0 + t1;
+    for (int r = threadIdx.x; r < nbond_blocks; r += blockDim.x) t += a.bond_partials[(size_t)r * kMaxGradSlots + k];
     part[threadIdx.x] = t;
     __syncthreads();
     for (int h = blockDim.x >> 1; h > 0; h >>= 1) {
@@ -697,14 +705,25 @@ __device__ __forceinline__ bool rdf_may_reach(const float4 &a, const float4 &b, 
     return dx * dx + dy * dy + dz * dz < r2max;
 }
 
+/* The pairs that pass the FP32 test are queued per warp (lane << 8 | tile index, in tile
+ * order, then lane order) and evaluated in FP64 32 at a time, one pair per lane, so that the
+ * expensive terms run on full warps instead of on the one lane of a warp that found a partner.
+ * A warp's queue is drained before the block loads its next tile of partners. */
+constexpr int kRdfWarps = kRdfTile / 32;
+constexpr int kRdfQueue = 64;  // ring: fewer than 32 waiting plus at most 32 from one partner
+
 /* hist[b] += sum over (i of type ta, j of type tb, i != j) of K(r_ij - c_b),
  * c_b = (b + 1/2) dr, minimum image in the periodic box, terms with
  * |r - c_b| > 4 sigma left out. Fixed-point sums make the result independent
- * of the order of the additions. One thread per particle i. */
-__global__ void rdf_hist_kernel(const float4 *__restrict__ x, int n, double3 box, int ta, int tb, int nbins,
-                                double dr, double sigma, unsigned long long *hist) {
+ * of the order of the additions. One lane per particle i. */
+__global__ void __launch_bounds__(kRdfTile) rdf_hist_kernel(const float4 *__restrict__ x, int n, double3 box, int ta,
+                                                          int tb, int nbins, double dr, double sigma,
+                                                          unsigned long long *hist) {
     __shared__ float4 tile[kRdfTile];
     __shared__ unsigned long long h[kRdfMaxBins];
+    __shared__ unsigned short queue[kRdfWarps][kRdfQueue];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt_mask = (1u << lane) - 1u;
     for (int b = threadIdx.x; b < nbins; b += blockDim.x) h[b] = 0ull;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -717,29 +736,54 @@ __global__ void rdf_hist_kernel(const float4 *__restrict__ x, int n, double3 box
     const float Lf[3] = {(float)box.x, (float)box.y, (float)box.z};
     const float iLf[3] = {1.0f / Lf[0], 1.0f / Lf[1], 1.0f / Lf[2]};
     const float r2f = (float)((rmax + kRdfMargin) * (rmax + kRdfMargin));
-    __syncthreads();
-    for (int t0 = 0; t0 < n; t0 += kRdfTile) {
-        const int j = t0 + threadIdx.x;
-        tile[threadIdx.x] = j < n ? x[j] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-        __syncthreads();
-        if (active) {
-            const int m = min(kRdfTile, n - t0);
-            for (int k = 0; k < m; ++k) {
-                const float4 xj = tile[k];
-                if (__float_as_int(xj.w) != tb || t0 + k == i) continue;
-                if (!rdf_may_reach(xi, xj, Lf, iLf, r2f)) continue;
-                double d[3] = {(double)xi.x - xj.x, (double)xi.y - xj.y, (double)xi.z - xj.z};
-                const double L[3] = {box.x, box.y, box.z};
-                for (int q = 0; q < 3; ++q) d[q] -= L[q] * rint(d[q] / L[q]);
-                const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-                if (r >= rmax) continue;
-                const int b0 = max(0, (int)floor((r - 4 * sigma) / dr)), b1 = min(nbins - 1, (int)floor((r + 4 * sigma) / dr));
+    const double L[3] = {box.x, box.y, box.z};
+    // the FP64 terms of nb <= 32 queued pairs from qh, one per lane
+    auto batch = [&](int qh, int nb) {
+        const int cd = lane < nb ? queue[w][(qh + lane) & (kRdfQueue - 1)] : 0;
+        const int src = cd >> 8;
+        const float ax = __shfl_sync(kFull, xi.x, src), ay = __shfl_sync(kFull, xi.y, src),
+                    az = __shfl_sync(kFull, xi.z, src);
+        if (lane < nb) {
+            const float4 xj = tile[cd & 0xff];
+            double d[3] = {(double)ax - xj.x, (double)ay - xj.y, (double)az - xj.z};
+            for (int q = 0; q < 3; ++q) d[q] -= L[q] * rint(d[q] / L[q]);
+            const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            if (r < rmax) {
+                const int b0 = max(0, (int)floor((r - 4 * sigma) / dr)),
+                          b1 = min(nbins - 1, (int)floor((r + 4 * sigma) / dr));
                 for (int b = b0; b <= b1; ++b) {
                     const double t = r - (b + 0.5) * dr;
                     if (fabs(t) > 4 * sigma) continue;
                     atomicAdd(&h[b], (unsigned long long)llrint(rdf_kernel_value(t, sigma) * kRdfFixed));
                 }
             }
+        }
+        __syncwarp();
+    };
+    __syncthreads();
+    int qh = 0, qt = 0;
+    for (int t0 = 0; t0 < n; t0 += kRdfTile) {
+        const int j = t0 + threadIdx.x;
+        tile[threadIdx.x] = j < n ? x[j] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+        __syncthreads();
+        const int m = min(kRdfTile, n - t0);
+        for (int k = 0; k < m; ++k) {
+            const float4 xj = tile[k];
+            if (__float_as_int(xj.w) != tb) continue;
+            const bool hit = active && t0 + k != i && rdf_may_reach(xi, xj, Lf, iLf, r2f);
+            const unsigned bal = __ballot_sync(kFull, hit);
+            if (hit) queue[w][(qt + __popc(bal & lt_mask)) & (kRdfQueue - 1)] = (unsigned short)((lane << 8) | k);
+            qt += __popc(bal);
+            if (qt - qh >= 32) {
+                __syncwarp();
+                batch(qh, 32);
+                qh += 32;
+            }
+        }
+        if (qt > qh) {  // the queue refers to this tile: drain it before the next one
+            __syncwarp();
+            batch(qh, qt - qh);
+            qh = qt;
         }
         __syncthreads();
     }
@@ -749,10 +793,16 @@ __global__ void rdf_hist_kernel(const float4 *__restrict__ x, int n, double3 box
 
 /* grad[i] = sum over partners j of sum_b coef[b] dK(r_ij - c_b)/dr (x_i - x_j)/r
  * for i of type ta (partners tb) and of type tb (partners ta): d loss / d x_i
- * for loss = sum_b G_b(hist) with coef[b] = dG/dhist_b. One thread per particle. */
-__global__ void rdf_grad_kernel(const float4 *__restrict__ x, int n, double3 box, int ta, int tb, int nbins,
-                                double dr, double sigma, const double *__restrict__ coef, float4 *grad) {
+ * for loss = sum_b G_b(hist) with coef[b] = dG/dhist_b. One lane per particle i; a pair's
+ * term is computed by whichever lane holds it in the batch and added by the lane of its i, in
+ * queue order, so each i sums its partners in ascending j. */
+__global__ void __launch_bounds__(kRdfTile) rdf_grad_kernel(const float4 *__restrict__ x, int n, double3 box, int ta,
+                                                          int tb, int nbins, double dr, double sigma,
+                                                          const double *__restrict__ coef, float4 *grad) {
     __shared__ float4 tile[kRdfTile];
+    __shared__ unsigned short queue[kRdfWarps][kRdfQueue];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt_mask = (1u << lane) - 1u;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
     int partner = -2;
@@ -765,23 +815,22 @@ __global__ void rdf_grad_kernel(const float4 *__restrict__ x, int n, double3 box
     const float Lf[3] = {(float)box.x, (float)box.y, (float)box.z};
     const float iLf[3] = {1.0f / Lf[0], 1.0f / Lf[1], 1.0f / Lf[2]};
     const float r2f = (float)((rmax + kRdfMargin) * (rmax + kRdfMargin));
+    const double L[3] = {box.x, box.y, box.z};
     double g[3] = {0.0, 0.0, 0.0};
-    for (int t0 = 0; t0 < n; t0 += kRdfTile) {
-        const int j = t0 + threadIdx.x;
-        tile[threadIdx.x] = j < n ? x[j] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-        __syncthreads();
-        if (partner != -2) {
-            const int m = min(kRdfTile, n - t0);
-            for (int k = 0; k < m; ++k) {
-                const float4 xj = tile[k];
-                if (__float_as_int(xj.w) != partner || t0 + k == i) continue;
-                if (!rdf_may_reach(xi, xj, Lf, iLf, r2f)) continue;
-                double d[3] = {(double)xi.x - xj.x, (double)xi.y - xj.y, (double)xi.z - xj.z};
-                const double L[3] = {box.x, box.y, box.z};
-                for (int q = 0; q < 3; ++q) d[q] -= L[q] * rint(d[q] / L[q]);
-                const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-                if (r >= rmax || r <= 0.0) continue;
-                const int b0 = max(0, (int)floor((r - 4 * sigma) / dr)), b1 = min(nbins - 1, (int)floor((r + 4 * sigma) / dr));
+    auto batch = [&](int qh, int nb) {
+        const int cd = lane < nb ? queue[w][(qh + lane) & (kRdfQueue - 1)] : 0;
+        const int src = cd >> 8;
+        const float ax = __shfl_sync(kFull, xi.x, src), ay = __shfl_sync(kFull, xi.y, src),
+                    az = __shfl_sync(kFull, xi.z, src);
+        double c[3] = {0.0, 0.0, 0.0};
+        if (lane < nb) {
+            const float4 xj = tile[cd & 0xff];
+            double d[3] = {(double)ax - xj.x, (double)ay - xj.y, (double)az - xj.z};
+            for (int q = 0; q < 3; ++q) d[q] -= L[q] * rint(d[q] / L[q]);
+            const double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            if (r < rmax && r > 0.0) {
+                const int b0 = max(0, (int)floor((r - 4 * sigma) / dr)),
+                          b1 = min(nbins - 1, (int)floor((r + 4 * sigma) / dr));
                 double s = 0.0;
                 for (int b = b0; b <= b1; ++b) {
                     const double t = r - (b + 0.5) * dr;
@@ -791,8 +840,46 @@ __global__ void rdf_grad_kernel(const float4 *__restrict__ x, int n, double3 box
                 }
                 // ta == tb counts each unordered pair twice in hist, as i and as j
                 const double f = s / r * (ta == tb ? 2.0 : 1.0);
-                for (int q = 0; q < 3; ++q) g[q] += f * d[q];
+                for (int q = 0; q < 3; ++q) c[q] = f * d[q];
             }
+        }
+        // each pair's term to the lane of its i, in queue order
+        for (int q = 0; q < nb; ++q) {
+            const int owner = __shfl_sync(kFull, src, q);
+            const double c0 = __shfl_sync(kFull, c[0], q), c1 = __shfl_sync(kFull, c[1], q),
+                         c2 = __shfl_sync(kFull, c[2], q);
+            if (lane == owner) {
+                g[0] += c0;
+                g[1] += c1;
+                g[2] += c2;
+            }
+        }
+        __syncwarp();
+    };
+    int qh = 0, qt = 0;
+    for (int t0 = 0; t0 < n; t0 += kRdfTile) {
+        const int j = t0 + threadIdx.x;
+        tile[threadIdx.x] = j < n ? x[j] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+        __syncthreads();
+        const int m = min(kRdfTile, n - t0);
+        for (int k = 0; k < m; ++k) {
+            const float4 xj = tile[k];
+            const int tj = __float_as_int(xj.w);
+            if (tj != ta && tj != tb) continue;
+            const bool hit = tj == partner && t0 + k != i && rdf_may_reach(xi, xj, Lf, iLf, r2f);
+            const unsigned bal = __ballot_sync(kFull, hit);
+            if (hit) queue[w][(qt + __popc(bal & lt_mask)) & (kRdfQueue - 1)] = (unsigned short)((lane << 8) | k);
+            qt += __popc(bal);
+            if (qt - qh >= 32) {
+                __syncwarp();
+                batch(qh, 32);
+                qh += 32;
+            }
+        }
+        if (qt > qh) {
+            __syncwarp();
+            batch(qh, qt - qh);
+            qh = qt;
         }
         __syncthreads();
     }

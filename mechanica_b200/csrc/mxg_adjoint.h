@@ -21,7 +21,7 @@ struct AdjointView {
     float4 *w, *gx, *gv;         // [slot] scratch: force adjoint and the partial sums
     const DevPotGrad *pot_grad;  // per potential
     const float *dcoef;          // derivative tables' coefficient pool
-    double *partials;            // [item][kMaxGradSlots] FP64 parameter sums of the pair terms
+    double *partials;            // [kMaxGradSlots][item] FP64 parameter sums of the pair terms
     double *bond_partials;       // [block][kMaxGradSlots] FP64 parameter sums of the bond terms
     int nslots;
     // the pair terms' work items: (cell, first entry, end entry, part), kVjpParts per cell; part 0
