@@ -717,7 +717,7 @@ constexpr int kRdfQueue = 64;  // ring: fewer than 32 waiting plus at most 32 fr
  * |r - c_b| > 4 sigma left out. Fixed-point sums make the result independent
  * of the order of the additions. One lane per particle i. */
 __global__ void __launch_bounds__(kRdfTile) rdf_hist_kernel(const float4 *__restrict__ x, int n, double3 box, int ta,
-                                                          int tb, int nbins, double dr, double sigma,
+                                                          int tb, int nbins, double dr, double sigma, int chunk,
                                                           unsigned long long *hist) {
     __shared__ float4 tile[kRdfTile];
     __shared__ unsigned long long h[kRdfMaxBins];
@@ -762,11 +762,13 @@ __global__ void __launch_bounds__(kRdfTile) rdf_hist_kernel(const float4 *__rest
     };
     __syncthreads();
     int qh = 0, qt = 0;
-    for (int t0 = 0; t0 < n; t0 += kRdfTile) {
+    // this block's partners: the tiles of its chunk of the particle range (blockIdx.y)
+    const int jend = min(n, (blockIdx.y + 1) * chunk);
+    for (int t0 = blockIdx.y * chunk; t0 < jend; t0 += kRdfTile) {
         const int j = t0 + threadIdx.x;
-        tile[threadIdx.x] = j < n ? x[j] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+        tile[threadIdx.x] = j < jend ? x[j] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
         __syncthreads();
-        const int m = min(kRdfTile, n - t0);
+        const int m = min(kRdfTile, jend - t0);
         for (int k = 0; k < m; ++k) {
             const float4 xj = tile[k];
             if (__float_as_int(xj.w) != tb) continue;
@@ -797,8 +799,8 @@ __global__ void __launch_bounds__(kRdfTile) rdf_hist_kernel(const float4 *__rest
  * term is computed by whichever lane holds it in the batch and added by the lane of its i, in
  * queue order, so each i sums its partners in ascending j. */
 __global__ void __launch_bounds__(kRdfTile) rdf_grad_kernel(const float4 *__restrict__ x, int n, double3 box, int ta,
-                                                          int tb, int nbins, double dr, double sigma,
-                                                          const double *__restrict__ coef, float4 *grad) {
+                                                          int tb, int nbins, double dr, double sigma, int chunk,
+                                                          const double *__restrict__ coef, double *gpart) {
     __shared__ float4 tile[kRdfTile];
     __shared__ unsigned short queue[kRdfWarps][kRdfQueue];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -857,11 +859,13 @@ __global__ void __launch_bounds__(kRdfTile) rdf_grad_kernel(const float4 *__rest
         __syncwarp();
     };
     int qh = 0, qt = 0;
-    for (int t0 = 0; t0 < n; t0 += kRdfTile) {
+    // this block's partners: the tiles of its chunk of the particle range (blockIdx.y)
+    const int jend = min(n, (blockIdx.y + 1) * chunk);
+    for (int t0 = blockIdx.y * chunk; t0 < jend; t0 += kRdfTile) {
         const int j = t0 + threadIdx.x;
-        tile[threadIdx.x] = j < n ? x[j] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+        tile[threadIdx.x] = j < jend ? x[j] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
         __syncthreads();
-        const int m = min(kRdfTile, n - t0);
+        const int m = min(kRdfTile, jend - t0);
         for (int k = 0; k < m; ++k) {
             const float4 xj = tile[k];
             const int tj = __float_as_int(xj.w);
@@ -883,7 +887,19 @@ __global__ void __launch_bounds__(kRdfTile) rdf_grad_kernel(const float4 *__rest
         }
         __syncthreads();
     }
-    if (i < n) grad[i] = make_float4((float)g[0], (float)g[1], (float)g[2], 0.f);
+    if (i < n)
+        for (int q = 0; q < 3; ++q) gpart[((size_t)blockIdx.y * n + i) * 3 + q] = g[q];
+}
+
+/* grad[i]: particle i's sums over the partner chunks, added in chunk order (so in ascending
+ * partner index, chunk by chunk). */
+__global__ void rdf_grad_sum_kernel(const double *__restrict__ gpart, int n, int nchunks, float4 *grad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double g[3] = {0.0, 0.0, 0.0};
+    for (int c = 0; c < nchunks; ++c)
+        for (int q = 0; q < 3; ++q) g[q] += gpart[((size_t)c * n + i) * 3 + q];
+    grad[i] = make_float4((float)g[0], (float)g[1], (float)g[2], 0.f);
 }
 
 }  // namespace
@@ -897,8 +913,25 @@ int launch_rdf(const float4 *x, int n, const double *box, int ta, int tb, int nb
     if (nbins < 1 || nbins > kRdfMaxBins) return -1;
     const double3 b = make_double3(box[0], box[1], box[2]);
     const int grid = (n + kRdfTile - 1) / kRdfTile;
-    if (hist) rdf_hist_kernel<<<grid, kRdfTile, 0, st>>>(x, n, b, ta, tb, nbins, dr, sigma, hist);
-    if (grad) rdf_grad_kernel<<<grid, kRdfTile, 0, st>>>(x, n, b, ta, tb, nbins, dr, sigma, coef, grad);
+    // the partner range split into chunks of whole tiles, one block per (particle tile, chunk),
+    // so that a few hundred blocks (not one per SM) hide the candidate test's latency
+    int sms = 148, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int ntiles = grid;
+    const int nchunks = std::max(1, std::min(ntiles, (6 * sms + grid - 1) / grid));
+    const int chunk = ((ntiles + nchunks - 1) / nchunks) * kRdfTile;
+    const int nch = (n + chunk - 1) / chunk;
+    const dim3 g2(grid, nch);
+    if (hist) rdf_hist_kernel<<<g2, kRdfTile, 0, st>>>(x, n, b, ta, tb, nbins, dr, sigma, chunk, hist);
+    if (grad) {
+        double *gpart = nullptr;
+        if (cudaMallocAsync(reinterpret_cast<void **>(&gpart), sizeof(double) * 3 * (size_t)n * nch, st) != cudaSuccess)
+            return -2;
+        rdf_grad_kernel<<<g2, kRdfTile, 0, st>>>(x, n, b, ta, tb, nbins, dr, sigma, chunk, coef, gpart);
+        rdf_grad_sum_kernel<<<(n + 255) / 256, 256, 0, st>>>(gpart, n, nch, grad);
+        cudaFreeAsync(gpart, st);
+    }
     return 0;
 }
 

@@ -2618,10 +2618,11 @@ int mxg_rdf(const void *x4, int n, const double *box, int type_a, int type_b, in
     if (!x4 || !box || (!hist && !grad4) || (grad4 && !coef)) return MXG_ERR_NULL;
     if (n < 0 || !(dr > 0) || !(sigma > 0)) return MXG_ERR_ARG;
     if (n == 0) return MXG_OK;
-    if (launch_rdf(static_cast<const float4 *>(x4), n, box, type_a, type_b, nbins, dr, sigma,
-                   static_cast<unsigned long long *>(hist), coef, static_cast<float4 *>(grad4),
-                   static_cast<cudaStream_t>(stream)) != 0)
-        return MXG_ERR_RANGE;
+    const int rc = launch_rdf(static_cast<const float4 *>(x4), n, box, type_a, type_b, nbins, dr, sigma,
+                              static_cast<unsigned long long *>(hist), coef, static_cast<float4 *>(grad4),
+                              static_cast<cudaStream_t>(stream));
+    if (rc == -1) return MXG_ERR_RANGE;
+    if (rc == -2) return MXG_ERR_MALLOC;
     CUDA_TRY(cudaGetLastError());
     return MXG_OK;
 }
