@@ -415,13 +415,15 @@ __global__ void __launch_bounds__(kWarpsA * 32, 4) vjp_pair_kernel(EngineView v,
                             const unsigned ida = __float_as_uint(vi.w), idb = __float_as_uint(vj.w);
                             const bool count = ida < idb;
                             const float radi = v.types[ti].radius, radj = v.types[tj].radius;
+                            // the pair's potential, then a second one summed on it: one call site, so
+                            // that the kernel's instruction footprint holds one copy of the terms
                             const int p1 = v.pot_idx[pot_base + ti * ntypes + tj];
-                            if (inside) term_vjp(v, a, p1, radi, radj, d, r2, vij, ida, idb, rng_mode, u, count, gx, gv, gl);
-                            if (inside && v.pot_idx2) {
-                                const int p2 = v.pot_idx2[pot_base + ti * ntypes + tj];
-                                if (p2 >= 0)
-                                    term_vjp(v, a, p2, radi, radj, d, r2, vij, ida, idb, rng_mode, u, count, gx, gv,
-                                             gl);
+                            const int p2 = v.pot_idx2 ? v.pot_idx2[pot_base + ti * ntypes + tj] : -1;
+#pragma unroll 1
+                            for (int k = 0; k < 2 && inside; ++k) {
+                                const int pk = k == 0 ? p1 : p2;
+                                if (pk >= 0)
+                                    term_vjp(v, a, pk, radi, radj, d, r2, vij, ida, idb, rng_mode, u, count, gx, gv, gl);
                             }
                         }
                         const int il_prev = __shfl_up_sync(kFull, il, 1);
